@@ -1,0 +1,257 @@
+/*
+ * dicegpu.h -- C ABI of the B200 subset-correlation library (libdicegpu.so).
+ *
+ * This header is the drop-in boundary for DICe's local subset-correlation hot
+ * path: warp of the subset pixels by the affine or quadratic shape function,
+ * Keys-4 / bicubic / bilinear interpolation of the deformed image and its
+ * gradients, the ZNSSD residual, the FP64 Gauss-Newton Hessian / right-hand
+ * side / LU solve, and the Nelder-Mead simplex fallback, followed by the
+ * per-subset epilogue (sigma, gamma, noise, contrast, active pixels, status).
+ *
+ * Every entry point returns int: 0 on success, a negative DICEGPU_ERR_* code
+ * otherwise.  Nothing throws across this boundary.  Per-subset outcomes are
+ * reported with the reference's Status_Flag integers (DICe.h:609-675).
+ *
+ * Reference interfaces replaced (paths inside the DICe project):
+ *   Schema::execute_correlation()          src/core/DICe_Schema.cpp:1622-1792
+ *   Schema::generic_correlation_routine()  src/core/DICe_Schema.cpp:2026-2368
+ *   Objective_ZNSSD::computeUpdateFast()   src/core/DICe_Objective.cpp:430-657
+ *   Objective::computeUpdateRobust()       src/core/DICe_Objective.cpp:369-388
+ *   Objective::gamma() / sigma()           src/core/DICe_Objective.cpp:58-76, 150-184
+ *   Subset::initialize() (DEF target)      src/base/DICe_Subset.cpp:373-440
+ *   Image_::interpolate_*_all()            src/base/DICe_Image.cpp:394-425, 493-636, 834-883
+ *   Image_::compute_gradients()            src/base/DICe_Image.cpp:1015-1093
+ *   dice_correlate() (C API precedent)     src/api/DICe_api.h:129-133, DICe_api.cpp:51-151
+ *
+ * Field layout: per-subset state lives in a double array of stride
+ * DICEGPU_FIELD_STRIDE, the analogue of the Schema's per-subset MultiField
+ * values (double, DICe_Schema.h:543-551).  Column indices are DICEGPU_F_*.
+ */
+#ifndef DICEGPU_H
+#define DICEGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DICEGPU_ABI_VERSION 1
+
+/* ---- error codes (return values) ---------------------------------------- */
+#define DICEGPU_OK              0
+#define DICEGPU_ERR_ARG        -1   /* bad argument (dice_correlate returns -1 too, DICe_api.cpp:71-76) */
+#define DICEGPU_ERR_CUDA       -2   /* a CUDA runtime call failed */
+#define DICEGPU_ERR_STATE      -3   /* call order: e.g. no reference image yet */
+#define DICEGPU_ERR_NOMEM      -4   /* device allocation failed */
+#define DICEGPU_ERR_TIMEOUT    -5   /* a bounded device wait gave up (status word) */
+#define DICEGPU_ERR_UNSUPPORTED -6  /* option outside the implemented path */
+#define DICEGPU_ERR_DEVICE     -7   /* the device status word recorded an error */
+
+/* ---- enums mirroring the reference (DICe.h) ------------------------------ */
+/* Status_Flag, DICe.h:609-675 (only the values the path produces are named) */
+#define DICEGPU_CORRELATION_SUCCESSFUL                 0
+#define DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL 1
+#define DICEGPU_INITIALIZE_USING_NEIGHBOR_VALUE_SUCCESSFUL 3
+#define DICEGPU_INITIALIZE_FAILED                      5
+#define DICEGPU_CORRELATION_FAILED                     8
+#define DICEGPU_SUBSET_CONSTRUCTION_FAILED             9
+#define DICEGPU_LINEAR_SOLVE_FAILED                   10
+#define DICEGPU_MAX_ITERATIONS_REACHED                11
+#define DICEGPU_INITIALIZE_FAILED_BY_EXCEPTION        12
+#define DICEGPU_JUMP_TOLERANCE_EXCEEDED               16
+#define DICEGPU_HESSIAN_SINGULAR                      21
+#define DICEGPU_FRAME_FAILED_DUE_TO_HIGH_GAMMA        23
+#define DICEGPU_FRAME_FAILED_DUE_TO_NEGATIVE_SIGMA    24
+
+/* Interpolation_Method, DICe.h:549-555 */
+#define DICEGPU_BILINEAR    0
+#define DICEGPU_BICUBIC     1
+#define DICEGPU_KEYS_FOURTH 2
+
+/* Optimization_Method, DICe.h:527-535 */
+#define DICEGPU_SIMPLEX                     0
+#define DICEGPU_GRADIENT_BASED              1
+#define DICEGPU_SIMPLEX_THEN_GRADIENT_BASED 3
+#define DICEGPU_GRADIENT_BASED_THEN_SIMPLEX 4
+
+/* Shape_Function_Type, DICe.h:509-516 */
+#define DICEGPU_AFFINE_SF    0
+#define DICEGPU_QUADRATIC_SF 1
+
+/* Gradient_Method, DICe.h:563-568 */
+#define DICEGPU_FINITE_DIFFERENCE   0
+#define DICEGPU_CONVOLUTION_5_POINT 1
+
+/* ---- per-subset field columns (double) ----------------------------------- */
+#define DICEGPU_FIELD_STRIDE   32
+#define DICEGPU_F_COORD_X       0   /* SUBSET_COORDINATES_X_FS */
+#define DICEGPU_F_COORD_Y       1   /* SUBSET_COORDINATES_Y_FS */
+#define DICEGPU_F_DISP_X        2   /* SUBSET_DISPLACEMENT_X_FS */
+#define DICEGPU_F_DISP_Y        3   /* SUBSET_DISPLACEMENT_Y_FS */
+#define DICEGPU_F_ROT_Z         4   /* ROTATION_Z_FS */
+#define DICEGPU_F_STRETCH_XX    5   /* NORMAL_STRETCH_XX_FS */
+#define DICEGPU_F_STRETCH_YY    6   /* NORMAL_STRETCH_YY_FS */
+#define DICEGPU_F_SHEAR_XY      7   /* SHEAR_STRETCH_XY_FS */
+#define DICEGPU_F_QUAD_A        8   /* QUAD_A_FS .. QUAD_L_FS = 8..19 */
+#define DICEGPU_F_SIGMA        20
+#define DICEGPU_F_GAMMA        21
+#define DICEGPU_F_BETA         22
+#define DICEGPU_F_NOISE        23
+#define DICEGPU_F_CONTRAST     24
+#define DICEGPU_F_ACTIVE_PIXELS 25
+#define DICEGPU_F_STATUS       26
+#define DICEGPU_F_ITERATIONS   27
+#define DICEGPU_F_MATCH        28
+#define DICEGPU_F_CONDITION    29   /* CONDITION_NUMBER_FS (2x2 displacement block) */
+#define DICEGPU_F_OMEGA        30
+
+/* dice_correlate's record, DICe_api.h:65: x, y, u, v, theta, sigma, gamma, beta, flag */
+#define DICEGPU_API_STRIDE 9
+
+/* ---- correlation parameters (POD stand-in for Teuchos::ParameterList) -----
+ * Defaults (dicegpu_default_params) are dice_default_params,
+ * src/core/DICe_ParameterUtilities.cpp:363-421. */
+typedef struct dicegpu_params {
+  int32_t shape_function;          /* DICEGPU_AFFINE_SF | DICEGPU_QUADRATIC_SF */
+  int32_t enable_translation;      /* must be 1 (DICe_LocalShapeFunction.cpp:164) */
+  int32_t enable_rotation;
+  int32_t enable_normal_strain;
+  int32_t enable_shear_strain;
+  int32_t interpolation;           /* DICEGPU_BILINEAR | BICUBIC | KEYS_FOURTH */
+  int32_t optimization;            /* DICEGPU_SIMPLEX ... GRADIENT_BASED_THEN_SIMPLEX */
+  int32_t gradient_method;         /* DICEGPU_FINITE_DIFFERENCE | CONVOLUTION_5_POINT */
+  int32_t max_solver_iterations_fast;    /* 25 */
+  int32_t max_solver_iterations_robust;  /* 1000 */
+  double  fast_solver_tolerance;         /* 1e-4 */
+  double  robust_solver_tolerance;       /* 1e-6 */
+  double  skip_solve_gamma_threshold;    /* 1e-10 */
+  double  robust_delta_disp;             /* 1.0 */
+  double  robust_delta_theta;            /* 0.1 */
+  double  disp_jump_tol;                 /* 1e4 */
+  double  theta_jump_tol;                /* 100 */
+  double  levenberg_marquardt_regularization_factor; /* -1 (off unless > 0) */
+  double  momentum_factor;               /* 0 (off unless != 0) */
+  double  initial_gamma_threshold;       /* -1 (off) */
+  double  final_gamma_threshold;         /* -1 (off) */
+  int32_t normalize_gamma_with_active_pixels; /* 0 */
+  int32_t output_beta;                   /* 0 */
+  /* 1: deformed-image gradients are computed and interpolated (images fed as
+   * arrays: Schema::set_def_image(w,h,array), DICe_Schema.cpp:339, so
+   * use_ref_grads=false).  0: the reference-image gradients at the reference
+   * pixel are used, rotated by theta (images fed from files,
+   * DICe_Schema.cpp:185; DICe_LocalShapeFunction.cpp:375-376). */
+  int32_t use_def_gradients;
+  int32_t subset_size;                   /* square subsets: side length (odd) */
+  int32_t reserved[4];
+} dicegpu_params;
+
+/* Fills *p with the reference defaults. Replaces dice_default_params. */
+int dicegpu_default_params(dicegpu_params* p);
+
+/* Number of shape-function parameters N for these params (2..6 affine, 12 quadratic). */
+int dicegpu_num_params(const dicegpu_params* p);
+
+/* ---- context -------------------------------------------------------------- */
+typedef struct dicegpu_ctx dicegpu_ctx;
+
+/* Creates a context on the current CUDA device.  The context owns the device
+ * images, gradients, subset tables and per-subset field buffers.  One context
+ * per host thread; calls on one context are serialised on its stream.
+ * Replaces the Schema constructor's role for the hot path (DICe_Schema.cpp:101-139). */
+int dicegpu_create(const dicegpu_params* params, dicegpu_ctx** out);
+int dicegpu_destroy(dicegpu_ctx* ctx);
+int dicegpu_set_params(dicegpu_ctx* ctx, const dicegpu_params* params);
+/* The stream every later call on ctx is issued on (a cudaStream_t; NULL = legacy default). */
+int dicegpu_set_stream(dicegpu_ctx* ctx, void* stream);
+
+/* Images are row-major float [h][w].  `on_device` = 1 when `pixels` is a device
+ * pointer (copied device to device), 0 for host memory.  The reference image
+ * gets finite-difference gradients (Image_::compute_gradients,
+ * DICe_Image.cpp:1015-1093); the deformed image gets them when
+ * params.use_def_gradients is 1.  Replaces Schema::set_ref_image /
+ * set_def_image(w,h,array) (DICe_Schema.cpp:328-349). */
+int dicegpu_set_ref_image(dicegpu_ctx* ctx, int w, int h, const float* pixels, int on_device);
+int dicegpu_set_def_image(dicegpu_ctx* ctx, int w, int h, const float* pixels, int on_device);
+
+/* Square subsets of params.subset_size centred on the COORD_X/COORD_Y field
+ * columns (Subset(cx,cy,w,h), DICe_Subset.cpp:78-113).  `fields` is a host
+ * array of n * DICEGPU_FIELD_STRIDE doubles: coordinates plus the initial
+ * shape-function fields (zeros for affine; QUAD_A = QUAD_H = 1 for quadratic,
+ * as Quadratic_Shape_Function::reset_fields).  SIGMA = -1 marks a subset whose
+ * initializer fails (DICe_Initializer.cpp:415-435). */
+int dicegpu_set_subsets(dicegpu_ctx* ctx, int n, const double* fields);
+
+/* Arbitrary-shape subsets (coordinate-array Subset ctor, DICe_Subset.cpp:49-76):
+ * subset i owns pixels [offsets[i], offsets[i+1]) of px/py (global pixel
+ * coordinates, row-major order).  Replaces params.subset_size for these subsets. */
+int dicegpu_set_subset_pixels(dicegpu_ctx* ctx, int n, const int32_t* offsets,
+                              const int32_t* px, const int32_t* py);
+/* Per-subset FORCE_SIMPLEX flags (DICe_Schema.cpp:2162-2165); NULL clears them. */
+int dicegpu_set_force_simplex(dicegpu_ctx* ctx, int n, const uint8_t* flags);
+
+/* Copies the n * DICEGPU_FIELD_STRIDE field array back to host memory
+ * (waits for the context's stream). */
+int dicegpu_get_fields(dicegpu_ctx* ctx, double* fields_out);
+/* Device pointer of the field array (n * DICEGPU_FIELD_STRIDE doubles). */
+int dicegpu_fields_device_ptr(dicegpu_ctx* ctx, double** dptr);
+
+/* One frame of local DIC over every subset: initial guess from the field
+ * values (USE_FIELD_VALUES), Gauss-Newton and/or simplex per
+ * params.optimization, jump / sigma / gamma tests, record_step.  Runs as one
+ * persistent work-stealing launch.  The first call after dicegpu_set_subsets
+ * is frame 0 (field-of-view check, DICe_Schema.cpp:2036-2048).
+ * Replaces Schema::execute_correlation() (DICe_Schema.cpp:1622). */
+int dicegpu_execute_correlation(dicegpu_ctx* ctx);
+
+/* The same frame run as one kernel launch per subset (the plain, unbatched
+ * GPU path the batched launch is compared with). */
+int dicegpu_execute_correlation_plain(dicegpu_ctx* ctx);
+
+/* Number of kernel launches this context issued since creation. */
+int dicegpu_launch_count(dicegpu_ctx* ctx, int64_t* count);
+
+/* Launch shape of the persistent kernel: warps (subsets in flight) per CTA
+ * and CTAs per SM; 0 keeps the current value.  The tile capacity is derived. */
+int dicegpu_set_launch_shape(dicegpu_ctx* ctx, int warps_per_cta, int ctas_per_sm);
+int dicegpu_get_launch_shape(dicegpu_ctx* ctx, int* warps_per_cta, int* ctas_per_sm);
+
+/* ---- stride-9 API (mirror of dice_correlate) ------------------------------
+ * points: n * 9 floats [x, y, u, v, theta, sigma, gamma, beta, flag]; on input
+ * sigma < 0 asks for an automatic guess (here: zero motion), otherwise u, v,
+ * theta are the guess.  Square subsets of `subset_size`.  Images are host
+ * arrays.  params may be NULL (tracking defaults as in DICe_api.cpp:96: affine
+ * u,v,theta, simplex, 8 px / 0.1 rad jump tolerances).
+ * Returns -1 on bad arguments like dice_correlate (DICe_api.cpp:71-76). */
+int dicegpu_correlate(float* points, int n_points, int subset_size,
+                      const float* ref_img, int ref_w, int ref_h,
+                      const float* def_img, int def_w, int def_h,
+                      const dicegpu_params* params);
+
+/* ---- per-call kernels for the Objective / Image interfaces --------------- */
+/* Interpolates the context's deformed image (and its gradients when present)
+ * at n points xy[2n] with `method`.  Device or host pointers per on_device.
+ * Replaces Image_::interpolate_{bilinear,bicubic,keys_fourth}_all. */
+int dicegpu_interpolate(dicegpu_ctx* ctx, int method, int n, const float* xy,
+                        float* intensity, float* grad_x, float* grad_y, int on_device);
+
+/* Finite-difference gradients of a float image (both device pointers).
+ * Replaces Image_::compute_gradients (DICe_Image.cpp:1015-1093). */
+int dicegpu_image_gradients(int w, int h, const float* d_img, float* d_gx, float* d_gy,
+                            int method, void* stream);
+
+/* Objective::gamma for every subset at the parameters in `fields` (host,
+ * n * stride): writes gamma per subset to gamma_out (host). */
+int dicegpu_gamma(dicegpu_ctx* ctx, const double* fields, double* gamma_out);
+
+/* Error word the device kernels write instead of trapping (0 = none). */
+int dicegpu_device_status(dicegpu_ctx* ctx, int32_t* status);
+
+/* Library version string. */
+const char* dicegpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DICEGPU_H */

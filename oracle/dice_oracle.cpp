@@ -1,0 +1,1143 @@
+// dice_oracle.cpp -- CPU oracle for the DICe local subset-correlation path.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for tests/, smoke() and the CPU
+// baseline leg of bench.py.  Never linked into or called by libdicegpu.so.
+//
+// It restates, function by function, the reference's CPU path with the
+// reference's precision contract: scalar_t = float for warp, interpolation,
+// residuals and products; double for the Gauss-Newton Hessian / RHS and the
+// LU factorisation (DICe.h:96-118, DICe_Objective.cpp:448-449).  It is built
+// with -ffp-contract=off so that no fused multiply-add changes a rounding the
+// reference's x86-64 build would not change.  Citations are paths inside the
+// DICe project.
+//
+// Deliberate reference behaviours kept here (each also kept by the GPU path):
+//  * pixel rounding (int)(x+0.5)==(int)x ? (int)x : (int)x+1 and the 4-pixel
+//    border deactivation (DICe_Subset.cpp:405-411);
+//  * GN runs solve_it = 0..max inclusive and reports the last index
+//    (DICe_Objective.cpp:494-495, 653);
+//  * the affine convergence test reads only u, v, theta
+//    (DICe_LocalShapeFunction.cpp:433-459);
+//  * the singular-Hessian test uses only the 2x2 displacement block
+//    (DICe_Objective.cpp:558-579) and the GETRF info code is ignored;
+//  * on success STATUS_FLAG is the initializer's status (DICe_Schema.cpp:2351);
+//  * SIGMA = -1 after a failed frame makes the next initial guess fail with
+//    INITIALIZE_FAILED (DICe_Initializer.cpp:415-435);
+//  * noise_std_dev's bounding-box quirks (DICe_Subset.cpp:664-684);
+//  * the simplex leaves the shape function at the last point it evaluated
+//    (the variables alias the parameters, DICe_LocalShapeFunction.h:259-261).
+#include "dice_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace oracle {
+
+static const double kPi = 3.14159265358979323846;
+static const double kTwoPi = 6.28318530717958647692;
+
+// ---------------------------------------------------------------------------
+// Image (DICe_Image.cpp)
+// ---------------------------------------------------------------------------
+struct Image {
+  int w = 0, h = 0;
+  const float* I = nullptr;
+  const float* gx = nullptr;
+  const float* gy = nullptr;
+  bool has_gradients = false;
+  // linear-index read: the reference indexes intensities_[y*w+x] without a
+  // bounds check; inside the array we read the same element, outside (only
+  // reachable through paths the subset border test excludes) we read 0.
+  inline float at(const float* a, long idx) const {
+    return (idx >= 0 && idx < (long)w * h) ? a[idx] : 0.0f;
+  }
+};
+
+// Keys fourth-order cubic convolution kernel pieces (DICe_Image.cpp:114-122).
+// The published Keys (1981) 6-point kernel: for s in [0,1): 4/3 s^3 - 7/3 s^2 + 1;
+// [1,2): -7/12 s^3 + 3 s^2 - 59/12 s + 5/2; [2,3): 1/12 s^3 - 2/3 s^2 + 7/4 s - 3/2.
+// Evaluated in double and rounded to float, as the reference's double literals do.
+static inline float keys_f0(float s) {
+  return (float)((4.0 / 3.0) * s * s * s - (7.0 / 3.0) * s * s + 1.0);
+}
+static inline float keys_f1(float s) {
+  return (float)(-(7.0 / 12.0) * s * s * s + 3.0 * s * s - (59.0 / 12.0) * s + 2.5);
+}
+static inline float keys_f2(float s) {
+  return (float)((1.0 / 12.0) * s * s * s - (2.0 / 3.0) * s * s + 1.75 * s - 1.5);
+}
+
+// Image_::interpolate_bilinear (DICe_Image.cpp:432-445) on one channel.
+static float bilinear(const Image& im, const float* a, float lx, float ly) {
+  if (lx < 0.0 || lx >= im.w - 1.5 || ly < 0.0 || ly >= im.h - 1.5) return 0.0f;
+  const int x1 = (int)lx, x2 = x1 + 1, y1 = (int)ly, y2 = y1 + 1;
+  const int w = im.w;
+  return a[y1 * w + x1] * (x2 - lx) * (y2 - ly) + a[y1 * w + x2] * (lx - x1) * (y2 - ly) +
+         a[y2 * w + x2] * (lx - x1) * (ly - y1) + a[y2 * w + x1] * (x2 - lx) * (ly - y1);
+}
+
+// Image_::interpolate_bilinear_all (DICe_Image.cpp:394-425).
+static void interp_bilinear_all(const Image& im, float& iv, float& gxv, float& gyv, bool grad,
+                                float lx, float ly) {
+  iv = bilinear(im, im.I, lx, ly);
+  if (grad) {
+    gxv = bilinear(im, im.gx, lx, ly);
+    gyv = bilinear(im, im.gy, lx, ly);
+  }
+}
+
+// Catmull-Rom (a = -1/2) cubic convolution weights: the separable form of the
+// 16-tap polynomial written out in Image_::interpolate_bicubic_all
+// (DICe_Image.cpp:493-636); same kernel, summed row by row.
+static inline void catmull_rom_weights(float t, float wgt[4]) {
+  const float t2 = t * t, t3 = t2 * t;
+  wgt[0] = 0.5f * (-t3 + 2.0f * t2 - t);
+  wgt[1] = 0.5f * (3.0f * t3 - 5.0f * t2 + 2.0f);
+  wgt[2] = 0.5f * (-3.0f * t3 + 4.0f * t2 + t);
+  wgt[3] = 0.5f * (t3 - t2);
+}
+
+static float bicubic_channel(const Image& im, const float* a, int x0, int y0, const float wx[4],
+                             const float wy[4]) {
+  float v = 0.0f;
+  for (int m = 0; m < 4; ++m) {
+    float row = 0.0f;
+    const long base = (long)(y0 - 1 + m) * im.w + (x0 - 1);
+    for (int n = 0; n < 4; ++n) row += wx[n] * im.at(a, base + n);
+    v += wy[m] * row;
+  }
+  return v;
+}
+
+// Image_::interpolate_bicubic_all (DICe_Image.cpp:493-636).  The reference
+// computes a bilinear fallback near the border and then falls through to the
+// bicubic expression, which overwrites it; we do the same.
+static void interp_bicubic_all(const Image& im, float& iv, float& gxv, float& gyv, bool grad,
+                               float lx, float ly) {
+  const int x0 = (int)lx, y0 = (int)ly;
+  float wx[4], wy[4];
+  catmull_rom_weights(lx - x0, wx);
+  catmull_rom_weights(ly - y0, wy);
+  iv = bicubic_channel(im, im.I, x0, y0, wx, wy);
+  if (grad) {
+    gxv = bicubic_channel(im, im.gx, x0, y0, wx, wy);
+    gyv = bicubic_channel(im, im.gy, x0, y0, wx, wy);
+  }
+}
+
+// Image_::interpolate_keys_fourth_all (DICe_Image.cpp:834-883): 6x6 taps,
+// cc = wy[m]*wx[n] in float, accumulated m-outer / n-inner in float.  As in
+// the reference the bilinear border value is overwritten by the Keys sum.
+static void interp_keys_all(const Image& im, float& iv, float& gxv, float& gyv, bool grad,
+                            float lx, float ly) {
+  iv = 0.0f;
+  if (grad) { gxv = 0.0f; gyv = 0.0f; }
+  const int ix = (int)lx, iy = (int)ly;
+  const float dx = lx - ix, dy = ly - iy;
+  float cx[6], cy[6];
+  cx[0] = keys_f2((float)(dx + 2.0));
+  cx[1] = keys_f1((float)(dx + 1.0));
+  cx[2] = keys_f0(dx);
+  cx[3] = keys_f0((float)(1.0 - dx));
+  cx[4] = keys_f1((float)(2.0 - dx));
+  cx[5] = keys_f2((float)(3.0 - dx));
+  cy[0] = keys_f2((float)(dy + 2.0));
+  cy[1] = keys_f1((float)(dy + 1.0));
+  cy[2] = keys_f0(dy);
+  cy[3] = keys_f0((float)(1.0 - dy));
+  cy[4] = keys_f1((float)(2.0 - dy));
+  cy[5] = keys_f2((float)(3.0 - dy));
+  for (int m = 0; m < 6; ++m) {
+    for (int n = 0; n < 6; ++n) {
+      const float cc = cy[m] * cx[n];
+      const long idx = (long)(iy - 2 + m) * im.w + ix - 2 + n;
+      iv += cc * im.at(im.I, idx);
+      if (grad) {
+        gxv += cc * im.at(im.gx, idx);
+        gyv += cc * im.at(im.gy, idx);
+      }
+    }
+  }
+}
+
+static void interpolate(const Image& im, int method, float& iv, float& gxv, float& gyv, bool grad,
+                        float lx, float ly) {
+  switch (method) {
+    case DICEGPU_BILINEAR: interp_bilinear_all(im, iv, gxv, gyv, grad, lx, ly); break;
+    case DICEGPU_BICUBIC: interp_bicubic_all(im, iv, gxv, gyv, grad, lx, ly); break;
+    default: interp_keys_all(im, iv, gxv, gyv, grad, lx, ly); break;
+  }
+}
+
+// Image_::compute_gradients_finite_difference (DICe_Image.cpp:1066-1093) with
+// grad_c1 = 1/12, grad_c2 = -8/12 stored as float (DICe_Image.cpp:214-215),
+// then optional 5x5 smoothing (smooth_gradients_convolution_5_point, :1034-1060).
+static void compute_gradients(int w, int h, const float* I, int method, float* gx, float* gy) {
+  const float c1 = (float)(1.0 / 12.0), c2 = (float)(-8.0 / 12.0);
+  for (int y = 0; y < h; ++y) {
+    for (int x = 0; x < w; ++x) {
+      const long i = (long)y * w + x;
+      if (x < 2) gx[i] = I[i + 1] - I[i];
+      else if (x >= w - 2) gx[i] = I[i] - I[i - 1];
+      else gx[i] = c1 * I[i - 2] + c2 * I[i - 1] - c2 * I[i + 1] - c1 * I[i + 2];
+      if (y < 2) gy[i] = I[i + w] - I[i];
+      else if (y >= h - 2) gy[i] = I[i] - I[i - w];
+      else gy[i] = c1 * I[i - 2 * w] + c2 * I[i - w] - c2 * I[i + w] - c1 * I[i + 2 * w];
+    }
+  }
+  if (method == DICEGPU_CONVOLUTION_5_POINT) {
+    // binomial 5-tap smoothing, outer product of (1,4,6,4,1)/16
+    static const float k[5] = {0.0625f, 0.25f, 0.375f, 0.25f, 0.0625f};
+    std::vector<float> tx(gx, gx + (long)w * h), ty(gy, gy + (long)w * h);
+    for (int y = 2; y < h - 2; ++y) {
+      for (int x = 2; x < w - 2; ++x) {
+        float vx = 0.0f, vy = 0.0f;
+        for (int i = 0; i < 5; ++i)
+          for (int j = 0; j < 5; ++j) {
+            const float c = k[i] * k[j];
+            const long idx = (long)(y + i - 2) * w + x + j - 2;
+            vx += c * tx[idx];
+            vy += c * ty[idx];
+          }
+        gx[(long)y * w + x] = vx;
+        gy[(long)y * w + x] = vy;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Local shape functions (DICe_LocalShapeFunction.cpp)
+// ---------------------------------------------------------------------------
+struct ShapeFn {
+  int type = DICEGPU_AFFINE_SF;
+  int N = 2;
+  // affine parameter slots in spec_map_ insertion order (init, :170-218)
+  int iu = 0, iv = 1, it = -1, iex = -1, iey = -1, ig = -1;
+  float p[12];
+  float deltas[12];
+
+  void init(const dicegpu_params& P) {
+    type = P.shape_function;
+    if (type == DICEGPU_QUADRATIC_SF) {
+      N = 12;
+      // Quadratic_Shape_Function ctor deltas (:481-492)
+      const float d[12] = {0.001f, 0.001f, 1.0e-6f, 1.0e-6f, 1.0e-6f, 1.0f,
+                           0.001f, 0.001f, 1.0e-6f, 1.0e-6f, 1.0e-6f, 1.0f};
+      for (int i = 0; i < 12; ++i) { deltas[i] = d[i]; p[i] = 0.0f; }
+      p[0] = 1.0f;  // QUAD_A
+      p[7] = 1.0f;  // QUAD_H
+      return;
+    }
+    int k = 2;
+    iu = 0; iv = 1; it = iex = iey = ig = -1;
+    if (P.enable_rotation) it = k++;
+    if (P.enable_normal_strain) { iex = k++; iey = k++; }
+    if (P.enable_shear_strain) ig = k++;
+    N = k;
+    for (int i = 0; i < N; ++i) { p[i] = 0.0f; deltas[i] = (float)P.robust_delta_theta; }
+    deltas[iu] = (float)P.robust_delta_disp;
+    deltas[iv] = (float)P.robust_delta_disp;
+  }
+
+  // Affine_Shape_Function::map (:220-248) / Quadratic_Shape_Function::map (:509-520)
+  void map(float x, float y, float cx, float cy, float& ox, float& oy) const {
+    const float dx = x - cx, dy = y - cy;
+    if (type == DICEGPU_QUADRATIC_SF) {
+      ox = p[0] * dx + p[1] * dy + p[2] * dx * dy + p[3] * dx * dx + p[4] * dy * dy + p[5] + cx;
+      oy = p[6] * dx + p[7] * dy + p[8] * dx * dy + p[9] * dx * dx + p[10] * dy * dy + p[11] + cy;
+      return;
+    }
+    const float theta = it >= 0 ? p[it] : 0.0f;
+    const float dudx = iex >= 0 ? p[iex] : 0.0f;
+    const float dvdy = iey >= 0 ? p[iey] : 0.0f;
+    const float gxy = ig >= 0 ? p[ig] : 0.0f;
+    const float cost = std::cos(theta), sint = std::sin(theta);
+    const float Dx = (float)((1.0 + dudx) * dx + gxy * dy);
+    const float Dy = (float)((1.0 + dvdy) * dy + gxy * dx);
+    ox = cost * Dx - sint * Dy + p[iu] + cx;
+    oy = sint * Dx + cost * Dy + p[iv] + cy;
+  }
+
+  // map_to_u_v_theta (affine :333-347; quadratic :552-578)
+  void map_to_u_v_theta(float cx, float cy, float& u, float& v, float& t) const {
+    if (type == DICEGPU_QUADRATIC_SF) {
+      float cxp, cyp, rxp, ryp;
+      map(cx, cy, cx, cy, cxp, cyp);
+      u = cxp - cx;
+      v = cyp - cy;
+      map((float)(cx + 5.0), cy, cx, cy, rxp, ryp);
+      const float ax = rxp - cxp, ay = ryp - cyp;
+      const float mag_a = std::sqrt(ax * ax + ay * ay);
+      const float bx = 5.0f, by = 0.0f, mag_b = 5.0f;
+      const float adb = (ax * bx + ay * by) / (mag_a * mag_b);
+      t = ay < 0.0f ? (float)(kTwoPi - std::acos(adb)) : std::acos(adb);
+      return;
+    }
+    u = p[iu];
+    v = p[iv];
+    t = it >= 0 ? p[it] : 0.0f;
+  }
+
+  // residuals (affine :350-396, quadratic :580-614)
+  void residuals(float x, float y, float cx, float cy, float gx, float gy, float* r,
+                 bool use_ref_grads) const {
+    if (type == DICEGPU_QUADRATIC_SF) {
+      const float dx = x - cx, dy = y - cy;
+      float Gx = gx, Gy = gy;
+      if (use_ref_grads) {
+        float u, v, th;
+        map_to_u_v_theta(cx, cy, u, v, th);
+        const float c = std::cos(th), s = std::sin(th);
+        Gx = c * gx - s * gy;
+        Gy = s * gx + c * gy;
+      }
+      r[0] = Gx * dx; r[1] = Gx * dy; r[2] = Gx * dx * dy; r[3] = Gx * dx * dx;
+      r[4] = Gx * dy * dy; r[5] = Gx;
+      r[6] = Gy * dx; r[7] = Gy * dy; r[8] = Gy * dx * dy; r[9] = Gy * dx * dx;
+      r[10] = Gy * dy * dy; r[11] = Gy;
+      return;
+    }
+    const float theta = it >= 0 ? p[it] : 0.0f;
+    const float dudx = iex >= 0 ? p[iex] : 0.0f;
+    const float dvdy = iey >= 0 ? p[iey] : 0.0f;
+    const float gxy = ig >= 0 ? p[ig] : 0.0f;
+    const float c = std::cos(theta), s = std::sin(theta);
+    const float dx = x - cx, dy = y - cy;
+    const float Dx = (float)((1.0 + dudx) * dx + gxy * dy);
+    const float Dy = (float)((1.0 + dvdy) * dy + gxy * dx);
+    const float Gx = use_ref_grads ? c * gx - s * gy : gx;
+    const float Gy = use_ref_grads ? s * gx + c * gy : gy;
+    r[iu] = Gx;
+    r[iv] = Gy;
+    if (it >= 0) r[it] = Gx * (-s * Dx - c * Dy) + Gy * (c * Dx - s * Dy);
+    if (iex >= 0) r[iex] = Gx * dx * c + Gy * dx * s;
+    if (iey >= 0) r[iey] = -Gx * dy * s + Gy * dy * c;
+    if (ig >= 0) r[ig] = Gx * (c * dy - s * dx) + Gy * (s * dy + c * dx);
+  }
+
+  // test_for_convergence (base :91-102 for quadratic; affine :433-459)
+  bool converged(const float* old, float tol) const {
+    bool conv = true;
+    if (type == DICEGPU_QUADRATIC_SF) {
+      for (int i = 0; i < N; ++i)
+        if (std::abs(p[i] - old[i]) >= tol) conv = false;
+      return conv;
+    }
+    if (std::abs(p[iu] - old[iu]) >= tol) conv = false;
+    if (std::abs(p[iv] - old[iv]) >= tol) conv = false;
+    if (it >= 0 && std::abs(p[it] - old[it]) >= tol) conv = false;
+    return conv;
+  }
+
+  // initialize_parameters_from_fields (affine :252-312, DISPLACEMENT_BASED
+  // projection; quadratic through the base class, :125-137)
+  void from_fields(const double* f) {
+    if (type == DICEGPU_QUADRATIC_SF) {
+      for (int i = 0; i < 12; ++i) p[i] = (float)f[DICEGPU_F_QUAD_A + i];
+      return;
+    }
+    p[iu] = (float)f[DICEGPU_F_DISP_X];
+    p[iv] = (float)f[DICEGPU_F_DISP_Y];
+    if (it >= 0) p[it] = (float)f[DICEGPU_F_ROT_Z];
+    if (iex >= 0) p[iex] = (float)f[DICEGPU_F_STRETCH_XX];
+    if (iey >= 0) p[iey] = (float)f[DICEGPU_F_STRETCH_YY];
+    if (ig >= 0) p[ig] = (float)f[DICEGPU_F_SHEAR_XY];
+  }
+
+  // save_fields (base :65-74; quadratic :616-629 also stores u, v, theta)
+  void to_fields(double* f, float cx, float cy) const {
+    if (type == DICEGPU_QUADRATIC_SF) {
+      for (int i = 0; i < 12; ++i) f[DICEGPU_F_QUAD_A + i] = p[i];
+      float u, v, t;
+      map_to_u_v_theta(cx, cy, u, v, t);
+      f[DICEGPU_F_DISP_X] = u;
+      f[DICEGPU_F_DISP_Y] = v;
+      f[DICEGPU_F_ROT_Z] = t;
+      return;
+    }
+    f[DICEGPU_F_DISP_X] = p[iu];
+    f[DICEGPU_F_DISP_Y] = p[iv];
+    if (it >= 0) f[DICEGPU_F_ROT_Z] = p[it];
+    if (iex >= 0) f[DICEGPU_F_STRETCH_XX] = p[iex];
+    if (iey >= 0) f[DICEGPU_F_STRETCH_YY] = p[iey];
+    if (ig >= 0) f[DICEGPU_F_SHEAR_XY] = p[ig];
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Subset (DICe_Subset.cpp)
+// ---------------------------------------------------------------------------
+struct Subset {
+  int cx = 0, cy = 0, npix = 0;
+  std::vector<int> x, y;
+  std::vector<float> ref, def, gx, gy;
+  std::vector<char> active, deact;
+  bool has_gradients = false;
+
+  // Subset(cx,cy,w,h) (:78-113): odd extent, negative coordinates clamped to 0.
+  void init_square(int cx_, int cy_, int size) {
+    cx = cx_; cy = cy_;
+    const int hw = size / 2;
+    npix = (2 * hw + 1) * (2 * hw + 1);
+    x.resize(npix); y.resize(npix);
+    int k = 0;
+    for (int yy = cy - hw; yy <= cy + hw; ++yy)
+      for (int xx = cx - hw; xx <= cx + hw; ++xx) {
+        x[k] = xx < 0 ? 0 : xx;
+        y[k] = yy < 0 ? 0 : yy;
+        ++k;
+      }
+    alloc();
+  }
+  // Subset(cx,cy,x[],y[]) (:49-76)
+  void init_list(int cx_, int cy_, const int32_t* px, const int32_t* py, int n) {
+    cx = cx_; cy = cy_; npix = n;
+    x.resize(n); y.resize(n);
+    for (int i = 0; i < n; ++i) {
+      x[i] = px[i] < 0 ? 0 : px[i];
+      y[i] = py[i] < 0 ? 0 : py[i];
+    }
+    alloc();
+  }
+  void alloc() {
+    ref.assign(npix, 0.0f); def.assign(npix, 0.0f);
+    gx.assign(npix, 0.0f); gy.assign(npix, 0.0f);
+    active.assign(npix, 1); deact.assign(npix, 0);
+  }
+  // initialize(ref_img) with no shape function (:385-389, :428-437)
+  void init_ref(const Image& im) {
+    for (int i = 0; i < npix; ++i) ref[i] = im.I[(long)y[i] * im.w + x[i]];
+    if (im.has_gradients) {
+      for (int i = 0; i < npix; ++i) {
+        gx[i] = im.gx[(long)y[i] * im.w + x[i]];
+        gy[i] = im.gy[(long)y[i] * im.w + x[i]];
+      }
+      has_gradients = true;
+    }
+  }
+  // initialize(def_img, DEF_INTENSITIES, shape_function, interp) (:390-426)
+  void init_def(const Image& im, const ShapeFn& sf, int interp) {
+    const float fcx = (float)cx, fcy = (float)cy;
+    for (int i = 0; i < npix; ++i) {
+      float mx, my;
+      sf.map((float)x[i], (float)y[i], fcx, fcy, mx, my);
+      const int px = ((int)(mx + 0.5) == (int)(mx)) ? (int)(mx) : (int)(mx) + 1;
+      const int py = ((int)(my + 0.5) == (int)(my)) ? (int)(my) : (int)(my) + 1;
+      if (px < 4 || px >= im.w - 4 || py < 4 || py >= im.h - 4) {
+        deact[i] = 1;
+        continue;
+      }
+      deact[i] = 0;
+      interpolate(im, interp, def[i], gx[i], gy[i], im.has_gradients, mx - 0.0f, my - 0.0f);
+    }
+  }
+  int num_active() const {
+    int n = 0;
+    for (int i = 0; i < npix; ++i) if (active[i] && !deact[i]) ++n;
+    return n;
+  }
+  // mean (:285-301)
+  float mean(bool def_target) const {
+    float m = 0.0f;
+    const int na = num_active();
+    const std::vector<float>& v = def_target ? def : ref;
+    for (int i = 0; i < npix; ++i) if (active[i] && !deact[i]) m += v[i];
+    return na != 0 ? m / na : 0.0f;
+  }
+  // mean with sum (:303-321)
+  float mean(bool def_target, float& sum) const {
+    const float m = mean(def_target);
+    const std::vector<float>& v = def_target ? def : ref;
+    sum = 0.0f;
+    for (int i = 0; i < npix; ++i)
+      if (active[i] && !deact[i]) sum += (v[i] - m) * (v[i] - m);
+    sum = std::sqrt(sum);
+    return m;
+  }
+  // gamma (:323-340)
+  float gamma() const {
+    float sr = 0.0f, sd = 0.0f;
+    const float mr = mean(false, sr);
+    const float md = mean(true, sd);
+    if (sr == 0.0f || sd == 0.0f) return -1.0f;
+    float g = 0.0f;
+    for (int i = 0; i < npix; ++i)
+      if (active[i] && !deact[i]) {
+        const float val = (def[i] - md) / sd - (ref[i] - mr) / sr;
+        g += val * val;
+      }
+    return g;
+  }
+  // contrast_std_dev (:607-620)
+  float contrast_std_dev() const {
+    const float m = mean(true);
+    float sd = 0.0f;
+    int na = 0;
+    for (int i = 0; i < npix; ++i)
+      if (active[i] && !deact[i]) { ++na; sd += (def[i] - m) * (def[i] - m); }
+    return na == 0 ? 0.0f : std::sqrt(sd / na);
+  }
+  // noise_std_dev (:622-703) on the deformed image
+  float noise_std_dev(const Image& im, const ShapeFn& sf) const {
+    static const float mask[3][3] = {{1, -2, 1}, {-2, 4, -2}, {1, -2, 1}};
+    int min_x = cx, max_x = cx, min_y = cy, max_y = cy, ndeact = 0;
+    for (int i = 0; i < npix; ++i) {
+      if (deact[i] || !active[i]) { ++ndeact; continue; }
+      if (x[i] < min_x) min_x = x[i];
+      if (x[i] > max_x) max_x = x[i];
+      if (y[i] < min_y) min_y = y[i];
+      if (y[i] > max_y) max_y = y[i];
+    }
+    if (ndeact == npix) return -1.0f;
+    float u, v, t;
+    sf.map_to_u_v_theta((float)cx, (float)cy, u, v, t);
+    min_x = (int)(min_x + u); max_x = (int)(max_x + u);
+    min_y = (int)(min_y + v); max_y = (int)(max_y + v);
+    const int img_h = im.h, img_w = im.w;
+    if (min_x < 0) min_x = 0;
+    if (min_y < 0) min_y = 0;
+    if (max_x >= img_w) min_x = 0;  // the reference resets min_x here (:667)
+    if (max_y >= img_h) min_y = 0;  // and min_y here (:668)
+    int hh = max_y - min_y + 1, ww = max_x - min_x + 1;
+    if (ww < 3) ww = 3;
+    if (hh < 3) hh = 3;
+    float variance = 0.0f;
+    for (int yy = min_y; yy < max_y; ++yy) {
+      for (int xx = min_x; xx < max_x; ++xx) {
+        if (xx < 1 || xx >= img_w - 1 || yy < 1 || yy >= img_h - 1) {
+          const float a = im.at(im.I, (long)yy * img_w + xx);
+          variance += std::sqrt(a * a);
+        } else {
+          float conv = 0.0f;
+          for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i)
+              conv += im.I[(long)(yy + j - 1) * img_w + xx + i - 1] * mask[i][j];
+          variance += std::abs(conv);
+        }
+      }
+    }
+    variance = (float)(variance * (std::sqrt(0.5 * kPi) / (6.0 * (ww - 2) * (hh - 2))));
+    return variance;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// LU factorisation + inverse standing in for LAPACK DGETRF/DGETRI
+// (DICe_Objective.cpp:571, 591).  Partial pivoting on the first maximal
+// |a_ij| (IDAMAX), column scaling by the reciprocal pivot, rank-1 trailing
+// update (the unblocked DGETF2 order).  A zero pivot leaves the column
+// unscaled and records info; DGETRI then returns early and leaves the LU
+// factors in place, which the reference goes on to use as the "inverse".
+// ---------------------------------------------------------------------------
+static int lu_factor(double* A, int N, int* piv) {  // row-major A[i*N+j]
+  int info = 0;
+  for (int j = 0; j < N; ++j) {
+    int p = j;
+    double best = std::abs(A[j * N + j]);
+    for (int i = j + 1; i < N; ++i)
+      if (std::abs(A[i * N + j]) > best) { best = std::abs(A[i * N + j]); p = i; }
+    piv[j] = p;
+    if (A[p * N + j] != 0.0) {
+      if (p != j)
+        for (int k = 0; k < N; ++k) std::swap(A[j * N + k], A[p * N + k]);
+      const double r = 1.0 / A[j * N + j];
+      for (int i = j + 1; i < N; ++i) A[i * N + j] *= r;
+    } else if (info == 0) {
+      info = j + 1;
+    }
+    for (int i = j + 1; i < N; ++i)
+      for (int k = j + 1; k < N; ++k) A[i * N + k] -= A[i * N + j] * A[j * N + k];
+  }
+  return info;
+}
+
+static void lu_inverse(const double* LU, const int* piv, int N, double* inv) {
+  // columns of inv(A) solve A x = e_k: x = U^-1 L^-1 P e_k
+  std::vector<double> col(N);
+  for (int k = 0; k < N; ++k) {
+    for (int i = 0; i < N; ++i) col[i] = (i == k) ? 1.0 : 0.0;
+    for (int j = 0; j < N; ++j)
+      if (piv[j] != j) std::swap(col[j], col[piv[j]]);
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < i; ++j) col[i] -= LU[i * N + j] * col[j];
+    for (int i = N - 1; i >= 0; --i) {
+      for (int j = i + 1; j < N; ++j) col[i] -= LU[i * N + j] * col[j];
+      col[i] /= LU[i * N + i];
+    }
+    for (int i = 0; i < N; ++i) inv[i * N + k] = col[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Objective (DICe_Objective.cpp) + simplex (DICe_Simplex.cpp)
+// ---------------------------------------------------------------------------
+struct Ctx {
+  dicegpu_params P;
+  Image ref, def;
+};
+
+struct Counters {
+  int gn_iters = 0;
+  int simplex_evals = 0;
+};
+
+// Objective::gamma (:58-76)
+static float objective_gamma(const Ctx& C, Subset& s, const ShapeFn& sf, Counters* cnt) {
+  s.init_def(C.def, sf, C.P.interpolation);
+  if (cnt) cnt->simplex_evals++;
+  float g = s.gamma();
+  if (C.P.normalize_gamma_with_active_pixels) {
+    int na = 0;
+    for (int i = 0; i < s.npix; ++i) if (s.active[i]) ++na;
+    if (na > 0) g /= na;
+  }
+  return g;
+}
+
+// Objective::sigma (:150-184)
+static float objective_sigma(const Ctx& C, const Subset& s, const ShapeFn& sf, float& noise) {
+  if (!s.has_gradients) return 0.0f;
+  noise = s.noise_std_dev(C.def, sf);
+  if (noise < 0.0f) return -1.0f;
+  float sgx = 0.0f, sgy = 0.0f;
+  for (int i = 0; i < s.npix; ++i) {
+    if (!s.active[i] || s.deact[i]) continue;
+    sgx += s.gx[i] * s.gx[i];
+    sgy += s.gy[i] * s.gy[i];
+  }
+  const float sg = sgx > sgy ? sgy : sgx;
+  return sg > 0.0f ? (float)std::sqrt(2.0 * noise * noise / sg) : -1.0f;
+}
+
+// Objective_ZNSSD::computeUpdateFast (:430-657)
+static int compute_update_fast(const Ctx& C, Subset& s, ShapeFn& sf, int& num_iterations,
+                               double* cond_out, Counters* cnt) {
+  const int N = sf.N;
+  const float tol = (float)C.P.fast_solver_tolerance;
+  const int max_its = C.P.max_solver_iterations_fast;
+  const bool use_ref_grads = !C.def.has_gradients;
+  double H[144], q[12], Hinv[144];
+  float r[12], def_old[12], def_update[12], def_update_old[12];
+  int piv[12];
+  for (int i = 0; i < N; ++i) def_update_old[i] = 0.0f;
+  const float fcx = (float)s.cx, fcy = (float)s.cy;
+  const float meanF = s.mean(false);
+  int solve_it = 0;
+  for (; solve_it <= max_its; ++solve_it) {
+    num_iterations = solve_it;
+    s.init_def(C.def, sf, C.P.interpolation);
+    if (cnt) cnt->gn_iters++;
+    const float meanG = s.mean(true);
+    for (int i = 0; i < N * N; ++i) H[i] = 0.0;
+    for (int i = 0; i < N; ++i) q[i] = 0.0;
+    for (int idx = 0; idx < s.npix; ++idx) {
+      if (s.deact[idx] || !s.active[idx]) continue;
+      const float GmF = (s.def[idx] - meanG) - (s.ref[idx] - meanF);
+      for (int i = 0; i < N; ++i) r[i] = 0.0f;
+      sf.residuals((float)s.x[idx], (float)s.y[idx], fcx, fcy, s.gx[idx], s.gy[idx], r,
+                   use_ref_grads);
+      for (int i = 0; i < N; ++i) {
+        q[i] += GmF * r[i];
+        for (int j = 0; j < N; ++j) H[i * N + j] += r[i] * r[j];
+      }
+    }
+    if (C.P.levenberg_marquardt_regularization_factor > 0.0) {
+      const float alpha = (float)C.P.levenberg_marquardt_regularization_factor;
+      H[0] += alpha;
+      H[1 * N + 1] += alpha;
+    }
+    const float det_h = (float)(H[0] * H[N + 1] - H[N] * H[1]);
+    const double nsq = H[0] * H[0] + H[1] * H[1] + H[N] * H[N] + H[N + 1] * H[N + 1];
+    const float norm_H = (float)std::sqrt(nsq);
+    float cond = -1.0f;
+    if (det_h != 0.0f) {
+      const float norm_Hi = (float)std::sqrt((1.0 / (double)(det_h * det_h)) * nsq);
+      cond = norm_H * norm_Hi;
+    }
+    const int info = lu_factor(H, N, piv);
+    if (cond_out) *cond_out = cond;
+    if (cond > 1.0e12f) return DICEGPU_HESSIAN_SINGULAR;
+    const double* M = H;
+    if (info == 0) {
+      lu_inverse(H, piv, N, Hinv);
+      M = Hinv;
+    }
+    for (int i = 0; i < N; ++i) def_old[i] = sf.p[i];
+    for (int i = 0; i < N; ++i) def_update[i] = 0.0f;
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) def_update[i] += M[i * N + j] * (-1.0) * q[j];
+    if (C.P.momentum_factor != 0.0) {
+      const float mom = (float)C.P.momentum_factor;
+      for (int i = 0; i < N; ++i) {
+        def_update[i] += mom * def_update_old[i];
+        def_update_old[i] = def_update[i];
+      }
+    }
+    for (int i = 0; i < N; ++i) sf.p[i] += def_update[i];
+    if (sf.converged(def_old, tol)) break;
+  }
+  if (solve_it > max_its) return DICEGPU_MAX_ITERATIONS_REACHED;
+  return DICEGPU_CORRELATION_SUCCESSFUL;
+}
+
+// Simplex::minimize (DICe_Simplex.cpp:60-277) via Subset_Simplex::objective
+// (:298-302).  `last_eval` receives the parameters of the last evaluation (the
+// subset's deformed state belongs to that point).
+static int simplex_minimize(const Ctx& C, Subset& s, ShapeFn& sf, int& num_iterations,
+                            float threshold, Counters* cnt) {
+  const int nd = sf.N;
+  const int max_iterations = C.P.max_solver_iterations_robust;
+  const double tolerance = C.P.robust_solver_tolerance;
+  const float tiny = 1.0e-10f;
+  float* vars = sf.p;  // the variables alias the shape-function parameters
+  float init_vars[12];
+  for (int i = 0; i < nd; ++i) init_vars[i] = vars[i];
+  const int mpts = nd + 1;
+  float gv[13];
+  float pts[13][12];
+  for (int i = 0; i < mpts; ++i) {
+    for (int j = 0; j < nd; ++j) pts[i][j] = vars[j];
+    if (i > 0) pts[i][i - 1] += sf.deltas[i - 1];
+    for (int j = 0; j < nd; ++j) vars[j] = pts[i][j];
+    gv[i] = objective_gamma(C, s, sf, cnt);
+    if (i == 0 && gv[i] < threshold && gv[i] >= 0.0f) {
+      num_iterations = 0;
+      return DICEGPU_CORRELATION_SUCCESSFUL;
+    }
+    for (int j = 0; j < nd; ++j) vars[j] = init_vars[j];
+  }
+  int inhi = 0;
+  float ysave;
+  float psum[12], ptry[12];
+  for (int j = 0; j < nd; ++j) {
+    float sum = 0.0f;
+    for (int i = 0; i < mpts; ++i) sum += pts[i][j];
+    psum[j] = sum;
+  }
+  float old_rtol = 0.0f, gamma_new = 0.0f, gamma_old = -1.0f;
+  int gamma_repeats = 0;
+  const int gamma_repeats_allowed = 15;
+  const float gamma_tol = 1.0e-8f;
+  int iteration = 0;
+  for (iteration = 0; iteration < max_iterations; iteration++) {
+    if (iteration >= max_iterations - 1) {
+      num_iterations = iteration;
+      return DICEGPU_MAX_ITERATIONS_REACHED;
+    }
+    int ilo = 0;
+    int ihi = gv[0] > gv[1] ? (inhi = 1, 0) : (inhi = 0, 1);
+    for (int i = 0; i < mpts; i++) {
+      if (gv[i] <= gv[ilo]) ilo = i;
+      if (gv[i] > gv[ihi]) {
+        inhi = ihi;
+        ihi = i;
+      } else if (gv[i] > gv[inhi] && i != ihi)
+        inhi = i;
+    }
+    const float rtol = (float)(2.0 * std::abs(gv[ihi] - gv[ilo]) /
+                               (std::abs(gv[ihi]) + std::abs(gv[ilo]) + tiny));
+    const float rtol_diff = std::abs(rtol - old_rtol);
+    old_rtol = rtol;
+    if (std::abs(gamma_new - gamma_old) < gamma_tol) gamma_repeats++;
+    gamma_old = gamma_new;
+    if (rtol < tolerance || rtol_diff < tolerance || gamma_repeats > gamma_repeats_allowed) {
+      std::swap(gv[0], gv[ilo]);
+      for (int i = 0; i < nd; i++) std::swap(pts[0][i], pts[ilo][i]);
+      break;
+    }
+    float ytry, fac, fac1, fac2;
+    fac = -1.0f;
+    fac1 = (float)((1.0 - fac) / nd);
+    fac2 = fac1 - fac;
+    for (int j = 0; j < nd; j++) ptry[j] = psum[j] * fac1 - pts[ihi][j] * fac2;
+    for (int n = 0; n < nd; ++n) vars[n] = ptry[n];
+    ytry = objective_gamma(C, s, sf, cnt);
+    if (ytry < gv[ihi]) {
+      gv[ihi] = ytry;
+      for (int j = 0; j < nd; j++) {
+        psum[j] += ptry[j] - pts[ihi][j];
+        pts[ihi][j] = ptry[j];
+      }
+    }
+    if (ytry <= gv[ilo]) {
+      fac = 2.0f;
+      fac1 = (float)((1.0 - fac) / nd);
+      fac2 = fac1 - fac;
+      for (int j = 0; j < nd; j++) ptry[j] = psum[j] * fac1 - pts[ihi][j] * fac2;
+      for (int n = 0; n < nd; ++n) vars[n] = ptry[n];
+      ytry = objective_gamma(C, s, sf, cnt);
+      if (ytry < gv[ihi]) {
+        gv[ihi] = ytry;
+        for (int j = 0; j < nd; j++) {
+          psum[j] += ptry[j] - pts[ihi][j];
+          pts[ihi][j] = ptry[j];
+        }
+      }
+    } else if (ytry >= gv[inhi]) {
+      ysave = gv[ihi];
+      fac = 0.5f;
+      fac1 = (float)((1.0 - fac) / nd);
+      fac2 = fac1 - fac;
+      for (int j = 0; j < nd; j++) ptry[j] = psum[j] * fac1 - pts[ihi][j] * fac2;
+      for (int n = 0; n < nd; ++n) vars[n] = ptry[n];
+      ytry = objective_gamma(C, s, sf, cnt);
+      if (ytry < gv[ihi]) {
+        gv[ihi] = ytry;
+        for (int j = 0; j < nd; j++) {
+          psum[j] += ptry[j] - pts[ihi][j];
+          pts[ihi][j] = ptry[j];
+        }
+      }
+      if (ytry >= ysave) {
+        for (int i = 0; i < mpts; i++) {
+          if (i != ilo) {
+            for (int j = 0; j < nd; j++)
+              pts[i][j] = psum[j] = (float)(0.5 * (pts[i][j] + pts[ilo][j]));
+            for (int n = 0; n < nd; ++n) vars[n] = psum[n];
+            gv[i] = objective_gamma(C, s, sf, cnt);
+          }
+        }
+        for (int j = 0; j < nd; j++) {
+          float sum = 0.0f;
+          for (int i = 0; i < mpts; i++) sum += pts[i][j];
+          psum[j] = sum;
+        }
+      }
+    }
+    gamma_new = objective_gamma(C, s, sf, cnt);
+  }
+  num_iterations = iteration;
+  return DICEGPU_CORRELATION_SUCCESSFUL;
+}
+
+// Objective::computeUpdateRobust (:369-388)
+static int compute_update_robust(const Ctx& C, Subset& s, ShapeFn& sf, int& num_iterations,
+                                 Counters* cnt) {
+  return simplex_minimize(C, s, sf, num_iterations, (float)C.P.skip_solve_gamma_threshold, cnt);
+}
+
+// Schema::record_failed_step (DICe_Schema.cpp:1959-1983)
+static void record_failed_step(double* f, int status, int num_iterations) {
+  f[DICEGPU_F_SIGMA] = -1.0;
+  f[DICEGPU_F_MATCH] = -1.0;
+  f[DICEGPU_F_GAMMA] = -1.0;
+  f[DICEGPU_F_BETA] = -1.0;
+  f[DICEGPU_F_OMEGA] = -1.0;
+  f[DICEGPU_F_NOISE] = -1.0;
+  f[DICEGPU_F_CONTRAST] = -1.0;
+  f[DICEGPU_F_ACTIVE_PIXELS] = -1.0;
+  f[DICEGPU_F_STATUS] = status;
+  f[DICEGPU_F_ITERATIONS] = num_iterations;
+}
+
+// Field_Value_Initializer::initial_guess (DICe_Initializer.cpp:398-436), own id.
+static int initial_guess(const double* f, ShapeFn& sf) {
+  if (f[DICEGPU_F_SIGMA] != -1.0) {
+    sf.from_fields(f);
+    return DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+  }
+  return DICEGPU_INITIALIZE_FAILED;
+}
+
+// Objective::beta (DICe_Objective.cpp:78-148): finite-difference slope of gamma
+// in u, v (and theta when rotation is enabled), unnormalised.
+static float objective_beta(const Ctx& C, Subset& s, const ShapeFn& sf_in) {
+  Ctx C2 = C;
+  C2.P.normalize_gamma_with_active_pixels = 0;
+  const float eps[3] = {0.1f, 0.1f, 0.1f};
+  const float fac[3] = {1.0e-3f, 1.0e-3f, 1.0e-1f};
+  const float g0 = objective_gamma(C2, s, sf_in, nullptr);
+  float dir[3] = {0.0f, 0.0f, 0.0f};
+  const bool rot = C.P.enable_rotation != 0;
+  for (int i = 0; i < 3; ++i) {
+    ShapeFn t = sf_in;
+    float u, v, th;
+    t.map_to_u_v_theta((float)s.cx, (float)s.cy, u, v, th);
+    if (!rot && i == 2) continue;
+    if (i == 0) u += eps[i]; else if (i == 1) v += eps[i]; else th += eps[i];
+    auto insert = [&](ShapeFn& sfn) {
+      if (sfn.type == DICEGPU_QUADRATIC_SF) {
+        for (int k = 0; k < 12; ++k) sfn.p[k] = 0.0f;
+        sfn.p[0] = std::cos(th); sfn.p[1] = -std::sin(th);
+        sfn.p[6] = std::sin(th); sfn.p[7] = std::cos(th);
+        sfn.p[5] = u; sfn.p[11] = v;
+      } else {
+        sfn.p[sfn.iu] = u; sfn.p[sfn.iv] = v;
+        if (sfn.it >= 0) sfn.p[sfn.it] = th;
+      }
+    };
+    insert(t);
+    const float gp = objective_gamma(C2, s, t, nullptr);
+    if (i == 0) u -= 2 * eps[i]; else if (i == 1) v -= 2 * eps[i]; else th -= 2 * eps[i];
+    insert(t);
+    const float gm = objective_gamma(C2, s, t, nullptr);
+    if (std::abs(gm - g0) < 1.0e-10 || std::abs(gp - g0) < 1.0e-10) {
+      objective_gamma(C, s, sf_in, nullptr);
+      return -1.0f;
+    }
+    const float sm = std::abs(eps[i] / (gm - g0)) * fac[i];
+    const float sp = std::abs(eps[i] / (gp - g0)) * fac[i];
+    dir[i] = (float)((sm + sp) / 2.0);
+  }
+  float mag = 0.0f;
+  for (int i = 0; i < 3; ++i) {
+    if (!rot && i == 2) continue;
+    mag += dir[i] * dir[i];
+  }
+  mag = std::sqrt(mag);
+  objective_gamma(C, s, sf_in, nullptr);
+  return mag;
+}
+
+// Schema::generic_correlation_routine (DICe_Schema.cpp:2026-2368) for one subset,
+// restricted to the USE_FIELD_VALUES initializer and local DIC.
+static void correlate_subset(const Ctx& C, Subset& s, double* f, bool first_frame,
+                             bool force_simplex, Counters* cnt) {
+  const dicegpu_params& P = C.P;
+  if (P.subset_size > 0 && first_frame) {
+    const float cur_x = (float)(f[DICEGPU_F_COORD_X] + f[DICEGPU_F_DISP_X]);
+    const float cur_y = (float)(f[DICEGPU_F_COORD_Y] + f[DICEGPU_F_DISP_Y]);
+    const int hs = P.subset_size / 2;
+    if (cur_x < hs || cur_x > C.def.w - hs || cur_y < hs || cur_y > C.def.h - hs) {
+      record_failed_step(f, DICEGPU_INITIALIZE_FAILED_BY_EXCEPTION, -1);
+      return;
+    }
+  }
+  int num_iterations = -1;
+  ShapeFn sf;
+  sf.init(P);
+  int init_status = initial_guess(f, sf);
+  if (init_status == DICEGPU_INITIALIZE_FAILED) {
+    record_failed_step(f, init_status, num_iterations);
+    return;
+  }
+  if (P.initial_gamma_threshold != -1.0) {
+    const float g0 = objective_gamma(C, s, sf, cnt);
+    if (g0 > P.initial_gamma_threshold || g0 < 0.0f) {
+      record_failed_step(f, DICEGPU_INITIALIZE_FAILED, num_iterations);
+      return;
+    }
+  }
+  const float prev_u = (float)f[DICEGPU_F_DISP_X];
+  const float prev_v = (float)f[DICEGPU_F_DISP_Y];
+  const float prev_t = (float)f[DICEGPU_F_ROT_Z];
+  const int opt = P.optimization;
+  int corr_status = DICEGPU_CORRELATION_FAILED;
+  double cond = 0.0;
+  bool cond_set = false;
+  if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED || force_simplex) {
+    corr_status = compute_update_robust(C, s, sf, num_iterations, cnt);
+  } else {
+    corr_status = compute_update_fast(C, s, sf, num_iterations, &cond, cnt);
+    cond_set = true;
+  }
+  const float fcx = (float)f[DICEGPU_F_COORD_X], fcy = (float)f[DICEGPU_F_COORD_Y];
+  float nu, nv, nt;
+  sf.map_to_u_v_theta(fcx, fcy, nu, nv, nt);
+  bool jump_pass = true;
+  if (std::abs(nu - prev_u) > P.disp_jump_tol || std::abs(nv - prev_v) > P.disp_jump_tol ||
+      std::abs(nt - prev_t) > P.theta_jump_tol)
+    jump_pass = false;
+  if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL || !jump_pass) {
+    bool second_failed = false;
+    if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_GRADIENT_BASED || force_simplex) {
+      second_failed = true;
+    } else if (opt == DICEGPU_GRADIENT_BASED_THEN_SIMPLEX) {
+      init_status = initial_guess(f, sf);
+      corr_status = compute_update_robust(C, s, sf, num_iterations, cnt);
+      if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
+    } else if (opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED) {
+      init_status = initial_guess(f, sf);
+      corr_status = compute_update_fast(C, s, sf, num_iterations, &cond, cnt);
+      cond_set = true;
+      if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
+    }
+    if (second_failed && corr_status != DICEGPU_CORRELATION_SUCCESSFUL) {
+      if (cond_set) f[DICEGPU_F_CONDITION] = cond;
+      record_failed_step(f, corr_status, num_iterations);
+      return;
+    }
+  }
+  if (cond_set) f[DICEGPU_F_CONDITION] = cond;
+  float noise = 0.0f;
+  const float sigma = objective_sigma(C, s, sf, noise);
+  if (sigma < 0.0f) {
+    record_failed_step(f, DICEGPU_FRAME_FAILED_DUE_TO_NEGATIVE_SIGMA, num_iterations);
+    return;
+  }
+  const float gamma = objective_gamma(C, s, sf, cnt);
+  const float beta = P.output_beta ? objective_beta(C, s, sf) : 0.0f;
+  if ((P.final_gamma_threshold != -1.0 && gamma > P.final_gamma_threshold) || gamma < 0.0f) {
+    record_failed_step(f, DICEGPU_FRAME_FAILED_DUE_TO_HIGH_GAMMA, num_iterations);
+    return;
+  }
+  sf.map_to_u_v_theta(fcx, fcy, nu, nv, nt);
+  if (std::abs(nu - prev_u) > P.disp_jump_tol || std::abs(nv - prev_v) > P.disp_jump_tol ||
+      std::abs(nt - prev_t) > P.theta_jump_tol) {
+    record_failed_step(f, DICEGPU_JUMP_TOLERANCE_EXCEEDED, num_iterations);
+    return;
+  }
+  const float contrast = s.contrast_std_dev();
+  const int active_pixels = s.num_active();
+  // record_step (DICe_Schema.cpp:1986-2009)
+  sf.to_fields(f, (float)s.cx, (float)s.cy);
+  f[DICEGPU_F_SIGMA] = sigma;
+  f[DICEGPU_F_MATCH] = 0.0;
+  f[DICEGPU_F_GAMMA] = gamma;
+  f[DICEGPU_F_BETA] = beta;
+  f[DICEGPU_F_NOISE] = noise;
+  f[DICEGPU_F_CONTRAST] = contrast;
+  f[DICEGPU_F_ACTIVE_PIXELS] = active_pixels;
+  f[DICEGPU_F_STATUS] = init_status;
+  f[DICEGPU_F_ITERATIONS] = num_iterations;
+}
+
+}  // namespace oracle
+
+using namespace oracle;
+
+extern "C" int oracle_default_params(dicegpu_params* p) {
+  if (!p) return DICEGPU_ERR_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->shape_function = DICEGPU_AFFINE_SF;
+  p->enable_translation = 1;
+  p->interpolation = DICEGPU_KEYS_FOURTH;
+  p->optimization = DICEGPU_GRADIENT_BASED_THEN_SIMPLEX;
+  p->gradient_method = DICEGPU_FINITE_DIFFERENCE;
+  p->max_solver_iterations_fast = 25;
+  p->max_solver_iterations_robust = 1000;
+  p->fast_solver_tolerance = 1.0e-4;
+  p->robust_solver_tolerance = 1.0e-6;
+  p->skip_solve_gamma_threshold = 1.0e-10;
+  p->robust_delta_disp = 1.0;
+  p->robust_delta_theta = 0.1;
+  p->disp_jump_tol = 10000.0;
+  p->theta_jump_tol = 100.0;
+  p->levenberg_marquardt_regularization_factor = -1.0;
+  p->momentum_factor = 0.0;
+  p->initial_gamma_threshold = -1.0;
+  p->final_gamma_threshold = -1.0;
+  p->use_def_gradients = 1;
+  p->subset_size = 21;
+  return 0;
+}
+
+extern "C" int oracle_gradients(int w, int h, const float* img, int method, float* gx, float* gy) {
+  if (w < 3 || h < 3 || !img || !gx || !gy) return DICEGPU_ERR_ARG;
+  compute_gradients(w, h, img, method, gx, gy);
+  return 0;
+}
+
+extern "C" int oracle_interpolate(int method, int w, int h, const float* img, const float* gx,
+                                  const float* gy, int n, const float* xy, float* out_i,
+                                  float* out_gx, float* out_gy) {
+  if (!img || !xy || !out_i || n < 0) return DICEGPU_ERR_ARG;
+  Image im;
+  im.w = w; im.h = h; im.I = img; im.gx = gx; im.gy = gy;
+  im.has_gradients = gx && gy && out_gx && out_gy;
+  for (int k = 0; k < n; ++k) {
+    float iv = 0.0f, a = 0.0f, b = 0.0f;
+    interpolate(im, method, iv, a, b, im.has_gradients, xy[2 * k], xy[2 * k + 1]);
+    out_i[k] = iv;
+    if (im.has_gradients) { out_gx[k] = a; out_gy[k] = b; }
+  }
+  return 0;
+}
+
+namespace {
+struct FrameJob {
+  Ctx C;
+  int n;
+  double* fields;
+  const int32_t *offsets, *px, *py;
+  const uint8_t* force_simplex;
+  bool first_frame;
+  int32_t* gn_out;
+  int32_t* sx_out;
+};
+
+void run_range(const FrameJob& J, int b, int e) {
+  Subset s;
+  for (int i = b; i < e; ++i) {
+    double* f = J.fields + (long)i * DICEGPU_FIELD_STRIDE;
+    const int cx = (int)f[DICEGPU_F_COORD_X], cy = (int)f[DICEGPU_F_COORD_Y];
+    if (J.offsets) s.init_list(cx, cy, J.px + J.offsets[i], J.py + J.offsets[i],
+                               J.offsets[i + 1] - J.offsets[i]);
+    else s.init_square(cx, cy, J.C.P.subset_size);
+    s.init_ref(J.C.ref);
+    Counters cnt;
+    correlate_subset(J.C, s, f, J.first_frame, J.force_simplex && J.force_simplex[i], &cnt);
+    if (J.gn_out) J.gn_out[i] = cnt.gn_iters;
+    if (J.sx_out) J.sx_out[i] = cnt.simplex_evals;
+  }
+}
+}  // namespace
+
+extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, const float* ref,
+                                    const float* def, int n, double* fields,
+                                    const int32_t* offsets, const int32_t* px,
+                                    const int32_t* py, const uint8_t* force_simplex,
+                                    int first_frame, int nthreads, int32_t* gn_iters_out,
+                                    int32_t* simplex_evals_out) {
+  if (!params || !ref || !def || !fields || n < 0 || w < 16 || h < 16) return DICEGPU_ERR_ARG;
+  FrameJob J;
+  J.C.P = *params;
+  // gradients as Schema::set_ref_image / set_def_image compute them
+  std::vector<float> rgx((long)w * h), rgy((long)w * h), dgx, dgy;
+  compute_gradients(w, h, ref, params->gradient_method, rgx.data(), rgy.data());
+  J.C.ref.w = w; J.C.ref.h = h; J.C.ref.I = ref;
+  J.C.ref.gx = rgx.data(); J.C.ref.gy = rgy.data(); J.C.ref.has_gradients = true;
+  J.C.def.w = w; J.C.def.h = h; J.C.def.I = def;
+  if (params->use_def_gradients) {
+    dgx.resize((long)w * h); dgy.resize((long)w * h);
+    compute_gradients(w, h, def, params->gradient_method, dgx.data(), dgy.data());
+    J.C.def.gx = dgx.data(); J.C.def.gy = dgy.data(); J.C.def.has_gradients = true;
+  }
+  J.n = n; J.fields = fields; J.offsets = offsets; J.px = px; J.py = py;
+  J.force_simplex = force_simplex; J.first_frame = first_frame != 0;
+  J.gn_out = gn_iters_out; J.sx_out = simplex_evals_out;
+  if (nthreads <= 1 || n < 2) {
+    run_range(J, 0, n);
+    return 0;
+  }
+  if (nthreads > n) nthreads = n;
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthreads; ++t) {
+    const int b = (int)((long)n * t / nthreads), e = (int)((long)n * (t + 1) / nthreads);
+    th.emplace_back(run_range, std::cref(J), b, e);
+  }
+  for (auto& x : th) x.join();
+  return 0;
+}
+
+extern "C" int oracle_gamma(const dicegpu_params* params, int w, int h, const float* ref,
+                            const float* def, int n, const double* fields, double* gamma_out) {
+  if (!params || !ref || !def || !fields || !gamma_out) return DICEGPU_ERR_ARG;
+  Ctx C;
+  C.P = *params;
+  std::vector<float> rgx((long)w * h), rgy((long)w * h), dgx, dgy;
+  compute_gradients(w, h, ref, params->gradient_method, rgx.data(), rgy.data());
+  C.ref.w = w; C.ref.h = h; C.ref.I = ref; C.ref.gx = rgx.data(); C.ref.gy = rgy.data();
+  C.ref.has_gradients = true;
+  C.def.w = w; C.def.h = h; C.def.I = def;
+  if (params->use_def_gradients) {
+    dgx.resize((long)w * h); dgy.resize((long)w * h);
+    compute_gradients(w, h, def, params->gradient_method, dgx.data(), dgy.data());
+    C.def.gx = dgx.data(); C.def.gy = dgy.data(); C.def.has_gradients = true;
+  }
+  Subset s;
+  for (int i = 0; i < n; ++i) {
+    const double* f = fields + (long)i * DICEGPU_FIELD_STRIDE;
+    s.init_square((int)f[DICEGPU_F_COORD_X], (int)f[DICEGPU_F_COORD_Y], params->subset_size);
+    s.init_ref(C.ref);
+    ShapeFn sf;
+    sf.init(C.P);
+    sf.from_fields(f);
+    gamma_out[i] = objective_gamma(C, s, sf, nullptr);
+  }
+  return 0;
+}

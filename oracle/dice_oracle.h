@@ -1,0 +1,57 @@
+/*
+ * dice_oracle.h -- CPU oracle for the DICe local subset-correlation path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a CPU restatement of the reference
+ * algorithm (scalar_t = float, FP32 products, FP64 Hessian / RHS accumulation,
+ * FP64 LU) used as the checker in tests/, in __graft_entry__.smoke() and as
+ * the timed CPU baseline in bench.py.  The product path (libdicegpu.so) never
+ * links, loads or calls it.
+ *
+ * Parity pin: tests/test_oracle_gold.py checks it against the reference's own
+ * regression gold (tests/regression/parallel_subsets/gold/DICe_solution_0.txt,
+ * tests/regression/single_speckled_shift/gold/) and the component
+ * known-answer tests restated in tests/test_oracle_kat.py.
+ *
+ * Parameter, field and status conventions are those of include/dicegpu.h.
+ */
+#ifndef DICE_ORACLE_H
+#define DICE_ORACLE_H
+
+#include "dicegpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One frame of Schema::execute_correlation over n subsets (GENERIC_ROUTINE,
+ * USE_FIELD_VALUES).  Subsets are square (params->subset_size, centred on the
+ * COORD fields) unless offsets/px/py give pixel lists.  `first_frame` enables
+ * the frame-0 field-of-view test.  `nthreads` workers split the subsets in
+ * contiguous ranges (the reference splits them over MPI ranks).  When
+ * `oracle_gn_iters` is non-NULL it receives, per subset, the number of
+ * Gauss-Newton iterations actually executed (for FLOP accounting). */
+int oracle_execute_frame(const dicegpu_params* params, int w, int h,
+                         const float* ref, const float* def, int n, double* fields,
+                         const int32_t* offsets, const int32_t* px, const int32_t* py,
+                         const uint8_t* force_simplex, int first_frame, int nthreads,
+                         int32_t* gn_iters_out, int32_t* simplex_evals_out);
+
+/* Image_::compute_gradients (finite difference, optional 5-point smoothing). */
+int oracle_gradients(int w, int h, const float* img, int method, float* gx, float* gy);
+
+/* Image_::interpolate_*_all at n points (x,y interleaved). gx/gy may be NULL. */
+int oracle_interpolate(int method, int w, int h, const float* img, const float* gx,
+                       const float* gy, int n, const float* xy, float* out_i,
+                       float* out_gx, float* out_gy);
+
+/* Objective::gamma for each subset at the parameters in `fields`. */
+int oracle_gamma(const dicegpu_params* params, int w, int h, const float* ref,
+                 const float* def, int n, const double* fields, double* gamma_out);
+
+/* Defaults of dice_default_params (same values as dicegpu_default_params). */
+int oracle_default_params(dicegpu_params* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,107 @@
+"""ctypes binding of the CPU oracle (oracle/libdiceoracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py as the checker / CPU baseline.  The product
+(dice_b200, libdicegpu.so) never imports it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from dice_b200.abi import Params, FIELD_STRIDE
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdiceoracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("oracle not built: run `make -C oracle`")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER(Params)
+        vp, ci = ctypes.c_void_p, ctypes.c_int
+        L.oracle_execute_frame.restype = ci
+        L.oracle_execute_frame.argtypes = [P, ci, ci, vp, vp, ci, vp, vp, vp, vp, vp, ci, ci, vp, vp]
+        L.oracle_gradients.restype = ci
+        L.oracle_gradients.argtypes = [ci, ci, vp, ci, vp, vp]
+        L.oracle_interpolate.restype = ci
+        L.oracle_interpolate.argtypes = [ci, ci, ci, vp, vp, vp, ci, vp, vp, vp, vp]
+        L.oracle_gamma.restype = ci
+        L.oracle_gamma.argtypes = [P, ci, ci, vp, vp, ci, vp, vp]
+        L.oracle_default_params.restype = ci
+        L.oracle_default_params.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def execute_frame(params, ref, deff, fields, first_frame=True, nthreads=1, offsets=None,
+                  px=None, py=None, force_simplex=None, counters=False):
+    """One frame over all subsets; updates `fields` (n x FIELD_STRIDE float64) in place."""
+    ref = np.ascontiguousarray(ref, dtype=np.float32)
+    deff = np.ascontiguousarray(deff, dtype=np.float32)
+    assert fields.dtype == np.float64 and fields.flags.c_contiguous and fields.shape[1] == FIELD_STRIDE
+    h, w = ref.shape
+    n = fields.shape[0]
+    if offsets is not None:
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        px = np.ascontiguousarray(px, dtype=np.int32)
+        py = np.ascontiguousarray(py, dtype=np.int32)
+    if force_simplex is not None:
+        force_simplex = np.ascontiguousarray(force_simplex, dtype=np.uint8)
+    gn = np.zeros(n, np.int32) if counters else None
+    sx = np.zeros(n, np.int32) if counters else None
+    rc = lib().oracle_execute_frame(ctypes.byref(params), w, h, _ptr(ref), _ptr(deff), n,
+                                    _ptr(fields), _ptr(offsets), _ptr(px), _ptr(py),
+                                    _ptr(force_simplex), 1 if first_frame else 0, nthreads,
+                                    _ptr(gn), _ptr(sx))
+    if rc != 0:
+        raise RuntimeError("oracle_execute_frame failed: %d" % rc)
+    if counters:
+        return gn, sx
+    return None
+
+
+def gradients(img, method=0):
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    h, w = img.shape
+    gx = np.zeros_like(img)
+    gy = np.zeros_like(img)
+    rc = lib().oracle_gradients(w, h, _ptr(img), method, _ptr(gx), _ptr(gy))
+    assert rc == 0
+    return gx, gy
+
+
+def interpolate(method, img, xy, gx=None, gy=None):
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    xy = np.ascontiguousarray(xy, dtype=np.float32).reshape(-1, 2)
+    h, w = img.shape
+    n = xy.shape[0]
+    oi = np.zeros(n, np.float32)
+    ogx = np.zeros(n, np.float32) if gx is not None else None
+    ogy = np.zeros(n, np.float32) if gy is not None else None
+    if gx is not None:
+        gx = np.ascontiguousarray(gx, dtype=np.float32)
+        gy = np.ascontiguousarray(gy, dtype=np.float32)
+    rc = lib().oracle_interpolate(method, w, h, _ptr(img), _ptr(gx), _ptr(gy), n, _ptr(xy),
+                                  _ptr(oi), _ptr(ogx), _ptr(ogy))
+    assert rc == 0
+    return oi, ogx, ogy
+
+
+def gamma(params, ref, deff, fields):
+    ref = np.ascontiguousarray(ref, dtype=np.float32)
+    deff = np.ascontiguousarray(deff, dtype=np.float32)
+    h, w = ref.shape
+    out = np.zeros(fields.shape[0], np.float64)
+    rc = lib().oracle_gamma(ctypes.byref(params), w, h, _ptr(ref), _ptr(deff), fields.shape[0],
+                            _ptr(fields), _ptr(out))
+    assert rc == 0
+    return out

@@ -1,0 +1,72 @@
+"""Generates the committed golden fixtures from the DICe reference tree.
+
+Run in a container that has the reference checked out (read-only is fine):
+
+    python tests/golden/make_fixtures.py /path/to/dice
+
+It converts the 8-bit test images the reference's regression and component
+tests use (OpenCV IMREAD_GRAYSCALE reads them as 8-bit grey, DICe_ImageIO.cpp:454;
+Pillow's "L" mode gives the same values) and parses the reference's gold
+output files into `reference_gold.npz`.  Nothing at test time reads the
+reference tree; the tests only read the .npz written here.
+
+Sources (paths inside the DICe project):
+  tests/component/images/refSpeckled.tif, defSpeckled.tif          (512 x 512)
+  tests/component/images/refSyntheticSpeckled.tif,
+      defSyntheticSpeckled0..5.tif                                (100 x 100)
+  tests/regression/parallel_subsets/{input,params}.xml + gold/DICe_solution_0.txt
+  tests/regression/single_speckled_shift/{input,params}.xml, subsets.dat,
+      gold/single_speckled_shift_{0..6}.txt
+"""
+import os
+import sys
+
+import numpy as np
+
+
+def _img(root, name):
+    from PIL import Image
+    im = Image.open(os.path.join(root, "tests", "component", "images", name))
+    if im.mode != "L":
+        im = im.convert("L")
+    return np.asarray(im, dtype=np.uint8)
+
+
+def _rows(path):
+    rows = []
+    with open(path) as fh:
+        for line in fh:
+            line = line.strip()
+            if not line or line.startswith("***") or line[0].isalpha():
+                continue
+            rows.append([float(t) for t in line.split()])
+    return np.asarray(rows, dtype=np.float64)
+
+
+def main(root):
+    out = {}
+    out["ref_speckled"] = _img(root, "refSpeckled.tif")
+    out["def_speckled"] = _img(root, "defSpeckled.tif")
+    out["ref_synthetic"] = _img(root, "refSyntheticSpeckled.tif")
+    for k in range(6):
+        out["def_synthetic_%d" % k] = _img(root, "defSyntheticSpeckled%d.tif" % k)
+    # parallel_subsets: subset 27, step 75, translation only, KEYS_FOURTH,
+    # GRADIENT_BASED_THEN_SIMPLEX, images read from files (reference-gradient mode).
+    # columns: id x y u v exx eyy gxy gamma iterations status
+    out["parallel_subsets_gold"] = _rows(os.path.join(
+        root, "tests", "regression", "parallel_subsets", "gold", "DICe_solution_0.txt"))
+    # single_speckled_shift: 7 hand-placed subsets of size 27, frame 0 rows.
+    # columns: frame x y u v theta exx eyy gxy sigma status
+    rows = []
+    for k in range(7):
+        r = _rows(os.path.join(root, "tests", "regression", "single_speckled_shift", "gold",
+                               "single_speckled_shift_%d.txt" % k))
+        rows.append(r[0])
+    out["single_speckled_shift_gold"] = np.asarray(rows)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_gold.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, {k: v.shape for k, v in out.items()})
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
