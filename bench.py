@@ -1,0 +1,413 @@
+"""Benchmark: subset solves per second of the local DIC hot path on B200.
+
+Workload (one "step" = one frame of the sequence): a 2048 x 2048 speckle image
+in 16-bit range (speckle radius 3-5 px), imposed field
+u = 0.5 sin(2 pi x/128), v = 0.3 cos(2 pi y/96) plus 0.2 % uniform strain,
+scaled by k/10 for frame k of a 10-frame sequence; 31 x 31 subsets at step 5
+(398^2 = 158,404 subsets); affine shape function (6 parameters), ZNSSD
+Gauss-Newton with Keys-4, tolerance 1e-5, 25 iterations, simplex fallback;
+each frame initialised from the previous frame's solution.  The sequence
+restarts from zero motion after frame 10 (a device-to-device field reset
+that is part of the step).  Seeded synthetic images (no dataset).
+
+Arms
+  default            libdicegpu.so persistent batched launch (value), the same
+                     through the C ABI with host buffers (e2e), and the plain
+                     one-launch-per-subset path on a sample for comparison.
+  --impl reference   the reference algorithm's CPU restatement (the reference
+                     itself does not build here: Trilinos / OpenCV / LAPACK are
+                     absent) on all host cores, a bounded sample per step.
+
+Multi-GPU (torchrun): every rank correlates its own copy of the sequence
+(subsets are independent, no collective on the data path); value is the
+aggregate over ranks, time is the max over ranks (weak scaling).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+W = H = 2048
+SUBSET = 31
+STEP = 5
+NFRAMES = 10
+METRIC = "subset solves/sec at <=1e-4 px vs reference; batched vs plain on one B200"
+UNIT = "subsets/s"
+# algorithmic work per pixel-iteration of affine Gauss-Newton (Keys-4,
+# deformed-image gradients): 390 FP32 flop + 27 FP64 flop
+FP32_FLOP_PER_PIXEL_ITER = 390.0
+FP64_FLOP_PER_PIXEL_ITER = 27.0
+# bytes of the three interpolated planes + reference value per pixel-iteration
+# if every tap came from DRAM once per subset (compulsory traffic per frame
+# is the images: 6 planes of W*H floats)
+
+
+def params():
+    from dice_b200 import abi
+    return abi.default_params(subset_size=SUBSET, enable_rotation=1, enable_normal_strain=1,
+                              enable_shear_strain=1, fast_solver_tolerance=1e-5,
+                              max_solver_iterations_fast=25)
+
+
+def workload_config(n_subsets, n_gpus):
+    return {"workload": "2048x2048 16-bit speckle sequence, 10 frames, 31x31 affine subsets at step 5",
+            "image": [W, H], "subset_size": SUBSET, "step": STEP, "subsets_per_frame": n_subsets,
+            "frames": NFRAMES, "shape_function": "affine (6 params)", "interpolation": "keys_fourth",
+            "optimization": "gradient_based_then_simplex", "tolerance": 1e-5, "max_iterations": 25,
+            "parallelism": "replicas x%d (independent subsets, no collective)" % n_gpus,
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = []
+        for k, nm in enumerate(names):
+            if any(s[3 + k].lower().startswith("active") for s in self.samples):
+                reasons.append(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        dist.barrier(device_ids=[torch.cuda.current_device()])
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_sample(p, ref, frames, n_sample, nthreads, timed_frames=1):
+    """The oracle on a bounded sample: the first `n_sample` subsets of the
+    grid (contiguous rows), run through `timed_frames` frames from zero motion."""
+    from dice_b200 import synthetic as syn
+    from oracle import oracle as O
+    cx, cy = syn.grid_points(W, H, SUBSET, STEP)
+    f = syn.init_fields(cx[:n_sample], cy[:n_sample])
+    t0 = time.perf_counter()
+    for k in range(timed_frames):
+        O.execute_frame(p, ref, frames[k], f, first_frame=(k == 0), nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return n_sample * timed_frames / dt, dt, f
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement on all host cores."""
+    rank, world, local = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
+    if rank != 0:
+        return
+    import torch
+    from dice_b200 import synthetic as syn
+    ref, frames = syn.config2(device="cpu", nframes=NFRAMES)
+    ref = ref.numpy()
+    frames = [fr.numpy() for fr in frames]
+    p = params()
+    cores = os.cpu_count() or 1
+    n_sample = max(256, min(158404, int(args.cpu_sample)))
+    for _ in range(args.warmup):
+        cpu_sample(p, ref, frames, min(n_sample, 512), cores)
+    vals = []
+    t_all = 0.0
+    for _ in range(args.steps):
+        v, dt, _ = cpu_sample(p, ref, frames, n_sample, cores)
+        vals.append(v)
+        t_all += dt
+    value = n_sample * args.steps / t_all
+    cx, _ = syn.grid_points(W, H, SUBSET, STEP)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * len(cx) / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded speckle sequence)", "impl": "reference",
+            "config": workload_config(len(cx), world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "first %d subsets of frame 1 per step (of %d), all cores" % (n_sample, len(cx))},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def flush_l2(buf):
+    buf.zero_()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dicegpu", choices=["dicegpu", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=1200)
+    ap.add_argument("--plain-sample", type=int, default=4000)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--warps", type=int, default=0)
+    ap.add_argument("--ctas", type=int, default=0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    from dice_b200 import abi, synthetic as syn
+    from dice_b200.schema import Schema
+
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    p = params()
+    ref, frames = syn.config2(device=dev, nframes=NFRAMES)
+    torch.cuda.synchronize()
+    cx, cy = syn.grid_points(W, H, SUBSET, STEP)
+    n = len(cx)
+    f0 = syn.init_fields(cx, cy)
+    stream = torch.cuda.current_stream()
+
+    s = Schema(p, stream=stream)
+    if args.warps or args.ctas:
+        s.set_launch_shape(args.warps, args.ctas)
+    s.set_ref_image(ref)
+    s.set_fields(f0)
+    f0_dev = torch.from_numpy(f0).to(dev)
+    nbytes_fields = f0.nbytes
+    l2_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    lib = s.lib
+
+    state = {"frame": 0}
+
+    def step_device():
+        k = state["frame"]
+        if k == 0:
+            s.load_fields(f0_dev)   # sequence restart: zero motion, frame 0
+        s.set_def_image(frames[k])
+        s.execute_correlation()
+        state["frame"] = (k + 1) % NFRAMES
+
+    # warm-up (first frame includes the field-of-view test path)
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    launches0 = s.launch_count()
+
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    iters_total = 0.0
+    npix = SUBSET * SUBSET
+    fields_seen = []
+    for i in range(args.steps):
+        flush_l2(l2_buf)
+        ev[i][0].record(stream)
+        step_device()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks.stop()
+    launches = s.launch_count() - launches0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = max_over_ranks(sum(step_ms), world)
+    value = n * args.steps * world / (total_ms / 1000.0)
+
+    # accuracy / work accounting of the last frame
+    fl = s.fields()
+    st = fl[:, abi.F_STATUS]
+    ok = st < 2
+    pix_iters = float(np.sum((fl[ok, abi.F_ITERATIONS] + 1) * fl[ok, abi.F_ACTIVE_PIXELS]))
+    kernel_ms = statistics.median(step_ms)
+    fp32_tflops = pix_iters * FP32_FLOP_PER_PIXEL_ITER / (kernel_ms / 1000.0) / 1e12
+
+    # e2e through the C ABI with host buffers: H2D of the frame, D2H of the fields
+    host_frames = [fr.cpu().pin_memory() for fr in frames[:2]]
+    host_fields = torch.empty((n, abi.FIELD_STRIDE), dtype=torch.float64).pin_memory()
+    import ctypes
+    e2e_ev = []
+    s.set_fields(f0)
+    for i in range(max(3, args.steps // 2) + 2):
+        hf = host_frames[i % 2]
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush_l2(l2_buf)
+        a.record(stream)
+        abi.check(lib.dicegpu_set_def_image(s.ctx, W, H, ctypes.c_void_p(hf.data_ptr()), 0), "set_def_image")
+        abi.check(lib.dicegpu_execute_correlation(s.ctx), "execute")
+        s.store_fields(host_fields)
+        b.record(stream)
+        e2e_ev.append((a, b))
+    torch.cuda.synchronize()
+    e2e_ms = [a.elapsed_time(b) for a, b in e2e_ev[2:]]
+    e2e_total = max_over_ranks(sum(e2e_ms), world)
+    e2e_value = n * len(e2e_ms) * world / (e2e_total / 1000.0)
+
+    # plain path (one launch per subset) on a sample of subsets
+    plain = None
+    if args.plain_sample > 0:
+        ns = min(args.plain_sample, n)
+        sp = Schema(p, stream=stream)
+        sp.set_ref_image(ref)
+        sp.set_fields(f0[:ns])
+        sp.set_def_image(frames[0])
+        sp.execute_correlation_plain()
+        torch.cuda.synchronize()
+        sp.set_fields(f0[:ns])
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sp.execute_correlation_plain()
+        b.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = a.elapsed_time(b)
+        sb = Schema(p, stream=stream)
+        sb.set_ref_image(ref)
+        sb.set_fields(f0[:ns])
+        sb.set_def_image(frames[0])
+        sb.execute_correlation()
+        torch.cuda.synchronize()
+        plain = {"value": ns / (plain_ms / 1000.0), "unit": UNIT, "subsets": ns,
+                 "launches": ns, "batched_speedup": value / world / (ns / (plain_ms / 1000.0))}
+        sp.close()
+        sb.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        ref_h = ref.cpu().numpy()
+        fr_h = [fr.cpu().numpy() for fr in frames[:1]]
+        cores = os.cpu_count() or 1
+        v, dt, _ = cpu_sample(p, ref_h, fr_h, args.cpu_sample, cores)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "first %d subsets of frame 1 (of %d), %d threads, %.1f s" % (args.cpu_sample, n, cores, dt)}
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    fp32_peak = fp32_peak_tflops(dev)
+    roof = {"bound": "fp32", "achieved": fp32_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": fp32_tflops / fp32_peak if fp32_peak else None, "traffic": None,
+            "kernel": "frame_kernel (median step time incl. gradient kernel)",
+            "peak_source": "measured FP32 SGEMM on CUDA cores (TF32 off) in this run",
+            "per_unit": "390 FP32 flop per active pixel-iteration x GN pixel-iterations of the frame",
+            "hbm_peak_gbs": peaks.get("hbm_gbs")}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+                "data": "synthetic (seeded speckle sequence)", "config": workload_config(n, world),
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": W * H * 4,
+                        "d2h_bytes_per_step": nbytes_fields},
+                "gpu_launches": int(launches), "clocks": clocks.summary(), "plain": plain,
+                "accuracy": {"converged_frac": float(ok.mean()),
+                             "status_counts": {str(int(k)): int(v) for k, v in zip(*np.unique(st, return_counts=True))},
+                             "mean_iterations": float(np.mean(fl[ok, abi.F_ITERATIONS]))}}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+_FP32_PEAK = None
+
+
+def fp32_peak_tflops(dev):
+    """FP32 CUDA-core throughput measured with cuBLAS SGEMM (TF32 disabled)."""
+    global _FP32_PEAK
+    if _FP32_PEAK is not None:
+        return _FP32_PEAK
+    import torch
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn(n, n, device=dev)
+        b = torch.randn(n, n, device=dev)
+        for _ in range(2):
+            torch.mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        _FP32_PEAK = 2.0 * n ** 3 / (best / 1000.0) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+    return _FP32_PEAK
+
+
+if __name__ == "__main__":
+    main()

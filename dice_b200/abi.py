@@ -153,6 +153,8 @@ def _declare(lib):
         "dicegpu_set_force_simplex": (c_int, [c_void_p, c_int, c_void_p]),
         "dicegpu_get_fields": (c_int, [c_void_p, c_void_p]),
         "dicegpu_fields_device_ptr": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
+        "dicegpu_load_fields": (c_int, [c_void_p, c_void_p, c_int]),
+        "dicegpu_store_fields": (c_int, [c_void_p, c_void_p, c_int]),
         "dicegpu_execute_correlation": (c_int, [c_void_p]),
         "dicegpu_execute_correlation_plain": (c_int, [c_void_p]),
         "dicegpu_launch_count": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_int64)]),

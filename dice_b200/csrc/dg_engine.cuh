@@ -1,0 +1,864 @@
+// dg_engine.cuh -- the per-subset correlation engine, one warp per subset.
+//
+// Mirrors Schema::generic_correlation_routine (DICe_Schema.cpp:2026-2368)
+// for the USE_FIELD_VALUES initializer:
+//   initial guess -> Gauss-Newton (Objective_ZNSSD::computeUpdateFast,
+//   DICe_Objective.cpp:430-657) and/or Nelder-Mead (Simplex::minimize,
+//   DICe_Simplex.cpp:60-277) -> jump test -> sigma -> gamma -> record_step.
+//
+// Data flow per Gauss-Newton iteration (one "pass" over the subset pixels):
+//   lane <- pixel;  warp (map) -> round + border test -> interpolation of
+//   I (+ Gx, Gy) -> residual vector r (FP32) -> v = [r, G-F, 1]
+//   -> sum v v^T with FP64 tensor-core mma (exact products of FP32 values,
+//   FP64 sums).  The 8x8 (affine) / 16x16 (quadratic) result holds
+//   H = sum r r^T, sum r (G-F), sum r, sum (G-F) and the active count, from
+//   which the reference's q = sum r ((G - meanG) - (F - meanF)) follows as
+//   sum r (G-F) - (meanG - meanF) sum r.
+#pragma once
+
+#include "dg_device.cuh"
+
+namespace dg {
+
+enum { MODE_CORRELATE = 0, MODE_GAMMA = 1 };
+
+struct FrameArgs {
+  DevParams P;
+  DevImage ref;
+  DevImage def;
+  DevGeometry geo;
+  double* fields;        // n x DICEGPU_FIELD_STRIDE
+  int n;
+  int first_frame;
+  int mode;
+  int plain_index;       // >= 0: this launch processes only that subset (plain path)
+  double* gamma_out;     // MODE_GAMMA output
+  int* work_counter;     // persistent work queue head
+  int* status;           // device error word
+  int32_t* passes_out;   // optional: pixel passes executed per subset (GN + simplex + epilogue)
+};
+
+template <int SHAPE>
+struct Layout {
+  static constexpr int NS = SHAPE == DICEGPU_QUADRATIC_SF ? 12 : 6;   // parameter slots
+  static constexpr int VW = SHAPE == DICEGPU_QUADRATIC_SF ? 16 : 8;   // [r, d, 1] padded
+  static constexpr int VS = SHAPE == DICEGPU_QUADRATIC_SF ? 24 : 8;   // smem row stride (conflict-free)
+  static constexpr int ID = NS;      // column of d = G - F
+  static constexpr int IONE = NS + 1;  // column of 1
+  static constexpr int NMAX = NS;
+};
+
+template <int SHAPE>
+struct __align__(16) WarpSmem {
+  float vbuf[32 * Layout<SHAPE>::VS];
+  double M[Layout<SHAPE>::VW * Layout<SHAPE>::VW];
+};
+
+// Result of one pass over the subset pixels.
+struct PassOut {
+  int n;                    // active pixels
+  double sumF;              // sum of F over active pixels (shifted by K)
+  double sG, sG2, sF2, sGF; // shifted moments (gamma passes)
+  double sgx2, sgy2;        // sum of unrotated gradient^2 (sigma)
+  int minx, maxx, miny, maxy;
+};
+
+struct SubsetRef {
+  int idx, cx, cy, npix;
+  int off;          // list offset (-1 for squares)
+  float K;          // intensity shift for the moment sums
+};
+
+template <int SHAPE, int INTERP, bool DEFGRAD>
+struct Engine {
+  using L = Layout<SHAPE>;
+  const FrameArgs& A;
+  WarpSmem<SHAPE>& S;
+  const int lane;
+
+  __device__ Engine(const FrameArgs& a, WarpSmem<SHAPE>& s) : A(a), S(s), lane(threadIdx.x & 31) {}
+
+  __device__ __forceinline__ void pixel_xy(const SubsetRef& sb, int p, int& x, int& y) const {
+    if (sb.off < 0) {
+      const int side = 2 * A.geo.half + 1;
+      const int row = p / side, col = p - row * side;
+      x = sb.cx - A.geo.half + col;
+      y = sb.cy - A.geo.half + row;
+    } else {
+      x = __ldg(A.geo.px + sb.off + p);
+      y = __ldg(A.geo.py + sb.off + p);
+    }
+    x = x < 0 ? 0 : x;   // Subset ctors clamp negative coordinates (DICe_Subset.cpp:66-68, :100-101)
+    y = y < 0 ? 0 : y;
+  }
+
+  // One pass over the subset at the parameters in `slots`.
+  //   ACC_H   : accumulate sum v v^T (Gauss-Newton)
+  //   GRADS   : interpolate the deformed gradients (DEFGRAD) / read reference ones
+  //   MOMENTS : intensity moments for gamma
+  template <bool ACC_H, bool GRADS, bool MOMENTS>
+  __device__ PassOut pass(const SubsetRef& sb, const float* slots, double* C) {
+    const bool use_ref_grads = !DEFGRAD;
+    MapConst k;
+    const float fcx = (float)sb.cx, fcy = (float)sb.cy;
+    make_mapconst<SHAPE>(slots, use_ref_grads, fcx, fcy, k);
+    const int W = A.def.w, H = A.def.h;
+    PassOut o;
+    int n = 0;
+    double sumF = 0.0, sG = 0.0, sG2 = 0.0, sF2 = 0.0, sGF = 0.0, sgx2 = 0.0, sgy2 = 0.0;
+    int minx = sb.cx, maxx = sb.cx, miny = sb.cy, maxy = sb.cy;
+    double c[4][2];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) { c[b][0] = 0.0; c[b][1] = 0.0; }
+    for (int base = 0; base < sb.npix; base += 32) {
+      const int p = base + lane;
+      float v[L::VW];
+#pragma unroll
+      for (int i = 0; i < L::VW; ++i) v[i] = 0.0f;
+      if (p < sb.npix) {
+        int x, y;
+        pixel_xy(sb, p, x, y);
+        float mx, my;
+        map_point<SHAPE>(k, (float)x, (float)y, fcx, fcy, mx, my);
+        const int px = round_pixel(mx), py = round_pixel(my);
+        const bool active = !(px < 4 || px >= W - 4 || py < 4 || py >= H - 4);
+        if (active) {
+          float G, gx = 0.0f, gy = 0.0f;
+          if (GRADS && DEFGRAD) interp_interior<INTERP, true>(A.def, mx, my, G, gx, gy);
+          else interp_interior<INTERP, false>(A.def, mx, my, G, gx, gy);
+          // the reference reads intensities_[y*w+x] unchecked (row-major wrap);
+          // same element inside the array, 0 outside it
+          const long ri = (long)y * A.ref.w + x;
+          const bool rin = ri < (long)A.ref.w * A.ref.h;
+          const float F = rin ? __ldg(A.ref.I + ri) : 0.0f;
+          if (GRADS && !DEFGRAD) {
+            gx = rin ? __ldg(A.ref.gx + ri) : 0.0f;
+            gy = rin ? __ldg(A.ref.gy + ri) : 0.0f;
+          }
+          ++n;
+          const float Fs = F - sb.K, Gs = G - sb.K;
+          sumF += (double)Fs;
+          if (MOMENTS) {
+            sG += (double)Gs;
+            sG2 = fma((double)Gs, (double)Gs, sG2);
+            sF2 = fma((double)Fs, (double)Fs, sF2);
+            sGF = fma((double)Gs, (double)Fs, sGF);
+          }
+          if (GRADS) {
+            sgx2 = fma((double)gx, (double)gx, sgx2);
+            sgy2 = fma((double)gy, (double)gy, sgy2);
+            minx = min(minx, x); maxx = max(maxx, x);
+            miny = min(miny, y); maxy = max(maxy, y);
+          }
+          if (ACC_H) {
+            residuals<SHAPE>(k, (float)x, (float)y, fcx, fcy, gx, gy, use_ref_grads, v);
+            v[L::ID] = G - F;
+            v[L::IONE] = 1.0f;
+          }
+        }
+      }
+      if (ACC_H) {
+        // stage the 32 pixel vectors, then 8 groups of 4 pixels through the FP64 mma
+        float* row = S.vbuf + lane * L::VS;
+#pragma unroll
+        for (int i = 0; i < L::VW; i += 4)
+          *reinterpret_cast<float4*>(row + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        __syncwarp();
+        const int kk = lane & 3, ii = lane >> 2;
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+          const float* src = S.vbuf + (4 * g + kk) * L::VS + ii;
+          if (SHAPE == DICEGPU_QUADRATIC_SF) {
+            const double a0 = (double)src[0], a1 = (double)src[8];
+            dmma_8x8x4(c[0][0], c[0][1], a0, a0);
+            dmma_8x8x4(c[1][0], c[1][1], a0, a1);
+            dmma_8x8x4(c[2][0], c[2][1], a1, a1);
+          } else {
+            const double a0 = (double)src[0];
+            dmma_8x8x4(c[0][0], c[0][1], a0, a0);
+          }
+        }
+        __syncwarp();
+      }
+    }
+    o.n = warp_sum_i(n);
+    o.sumF = warp_sum(sumF);
+    if (MOMENTS) {
+      o.sG = warp_sum(sG); o.sG2 = warp_sum(sG2); o.sF2 = warp_sum(sF2); o.sGF = warp_sum(sGF);
+    } else {
+      o.sG = o.sG2 = o.sF2 = o.sGF = 0.0;
+    }
+    if (GRADS) {
+      o.sgx2 = warp_sum(sgx2); o.sgy2 = warp_sum(sgy2);
+      o.minx = warp_min_i(minx); o.maxx = warp_max_i(maxx);
+      o.miny = warp_min_i(miny); o.maxy = warp_max_i(maxy);
+    } else {
+      o.sgx2 = o.sgy2 = 0.0;
+      o.minx = o.maxx = sb.cx; o.miny = o.maxy = sb.cy;
+    }
+    if (ACC_H) {
+      // scatter the accumulator fragments into the dense symmetric matrix
+      __syncwarp();
+      const int r = lane >> 2, cc = 2 * (lane & 3);
+      constexpr int VW = L::VW;
+      if (SHAPE == DICEGPU_QUADRATIC_SF) {
+        C[r * VW + cc] = c[0][0];           C[r * VW + cc + 1] = c[0][1];
+        C[r * VW + 8 + cc] = c[1][0];       C[r * VW + 8 + cc + 1] = c[1][1];
+        C[(8 + cc) * VW + r] = c[1][0];     C[(8 + cc + 1) * VW + r] = c[1][1];
+        C[(8 + r) * VW + 8 + cc] = c[2][0]; C[(8 + r) * VW + 8 + cc + 1] = c[2][1];
+      } else {
+        C[r * VW + cc] = c[0][0];
+        C[r * VW + cc + 1] = c[0][1];
+      }
+      __syncwarp();
+    }
+    return o;
+  }
+
+  // Objective::gamma from the moments (Subset::gamma, DICe_Subset.cpp:323-340):
+  // gamma = sum ((G-mG)/|G-mG| - (F-mF)/|F-mF|)^2 = 2 - 2 cov / (|G-mG| |F-mF|).
+  __device__ float gamma_from(const PassOut& o, int npix) const {
+    if (o.n == 0) return -1.0f;
+    const double n = (double)o.n;
+    const double sgg = o.sG2 - o.sG * o.sG / n;
+    const double sff = o.sF2 - o.sumF * o.sumF / n;
+    const double sgf = o.sGF - o.sG * o.sumF / n;
+    if (!(sgg > 0.0) || !(sff > 0.0)) return -1.0f;
+    double g = 2.0 - 2.0 * sgf / sqrt(sgg * sff);
+    if (g < 0.0) g = 0.0;
+    float gf = (float)g;
+    if (A.P.normalize_gamma && npix > 0) gf /= (float)npix;
+    return gf;
+  }
+
+  __device__ float eval_gamma(const SubsetRef& sb, const float* slots, PassOut* out = nullptr) {
+    PassOut o = pass<false, false, true>(sb, slots, nullptr);
+    if (out) *out = o;
+    if (A.passes_out && lane == 0) A.passes_out[sb.idx] += 1;
+    return gamma_from(o, sb.npix);
+  }
+
+  __device__ void compact_to_slots(const float* comp, float* slots, const float* base) const {
+#pragma unroll
+    for (int i = 0; i < 12; ++i) slots[i] = base[i];
+    for (int k = 0; k < A.P.N; ++k) slots[A.P.slot[k]] = comp[k];
+  }
+
+  // --------------------------------------------------------------------------
+  // Gauss-Newton (Objective_ZNSSD::computeUpdateFast).  `slots` in/out.
+  // `meanF` is the reference mean at entry (Subset::mean(REF_INTENSITIES)).
+  // --------------------------------------------------------------------------
+  __device__ int gauss_newton(const SubsetRef& sb, float* slots, float meanF, int& num_iterations,
+                              float& cond_out, PassOut& last) {
+    const DevParams& P = A.P;
+    const int N = P.N;
+    float upd_old[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) upd_old[i] = 0.0f;
+    double* M = S.M;
+    int solve_it = 0;
+    for (; solve_it <= P.max_fast; ++solve_it) {
+      num_iterations = solve_it;
+      last = pass<true, true, false>(sb, slots, M);
+      if (A.passes_out && lane == 0) A.passes_out[sb.idx] += 1;
+      const int n = last.n;
+      // Subset::mean(DEF_INTENSITIES): sum G / n over the active pixels
+      const double sumG = M[L::ID * L::VW + L::IONE] + last.sumF + (double)n * (double)sb.K;
+      const float meanG = n ? (float)(sumG / (double)n) : 0.0f;
+      const double cshift = (double)meanG - (double)meanF;
+      // lane i owns row i of [H | q] in the reference's compact order
+      double h[L::NMAX];
+      double qv = 0.0;
+      const int si = lane < N ? P.slot[lane] : 0;
+#pragma unroll
+      for (int j = 0; j < L::NMAX; ++j) {
+        h[j] = 0.0;
+        if (j < N && lane < N) h[j] = M[si * L::VW + P.slot[j]];
+      }
+      if (lane < N) qv = M[si * L::VW + L::ID] - cshift * M[si * L::VW + L::IONE];
+      // Levenberg-Marquardt penalty on the displacement diagonal (:548-553)
+      if (P.lm_alpha > 0.0f) {
+        if (lane == 0) h[0] += (double)P.lm_alpha;
+        if (lane == 1) h[1] += (double)P.lm_alpha;
+      }
+      // 2x2 condition number of the displacement block (:558-564), in the
+      // reference's mix of float and double
+      const double H00 = __shfl_sync(FULL, h[0], 0), H01 = __shfl_sync(FULL, h[1], 0);
+      const double H10 = __shfl_sync(FULL, h[0], 1), H11 = __shfl_sync(FULL, h[1], 1);
+      const float det_h = (float)(H00 * H11 - H10 * H01);
+      const double nsq = H00 * H00 + H01 * H01 + H10 * H10 + H11 * H11;
+      const float norm_H = (float)sqrt(nsq);
+      float cond = -1.0f;
+      if (det_h != 0.0f) {
+        const float dd = __fmul_rn(det_h, det_h);
+        const float norm_Hi = (float)sqrt((1.0 / (double)dd) * nsq);
+        cond = norm_H * norm_Hi;
+      }
+      cond_out = cond;
+      // LU with partial pivoting (DGETRF order), q carried as an extra column
+      const double q_orig = qv;
+      int info = 0;
+#pragma unroll
+      for (int j = 0; j < L::NMAX; ++j) {
+        if (j < N) {
+          double a = (lane >= j && lane < N) ? fabs(h[j]) : -1.0;
+          int pl = lane;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            const double oa = __shfl_xor_sync(FULL, a, o);
+            const int op = __shfl_xor_sync(FULL, pl, o);
+            if (oa > a || (oa == a && op < pl)) { a = oa; pl = op; }
+          }
+          const double pv = __shfl_sync(FULL, h[j], pl);
+          if (pv != 0.0) {
+            if (pl != j) {
+              const int src = lane == j ? pl : (lane == pl ? j : lane);
+#pragma unroll
+              for (int kx = 0; kx < L::NMAX; ++kx) h[kx] = __shfl_sync(FULL, h[kx], src);
+              qv = __shfl_sync(FULL, qv, src);
+            }
+            const double rcp = 1.0 / pv;
+            if (lane > j && lane < N) h[j] *= rcp;
+          } else if (info == 0) {
+            info = j + 1;
+          }
+#pragma unroll
+          for (int kx = j + 1; kx < L::NMAX; ++kx) {
+            const double prow = __shfl_sync(FULL, h[kx], j);
+            if (kx < N && lane > j && lane < N) h[kx] -= h[j] * prow;
+          }
+          const double pq = __shfl_sync(FULL, qv, j);
+          if (lane > j && lane < N) qv -= h[j] * pq;
+        }
+      }
+      if (cond > 1.0e12f) return DICEGPU_HESSIAN_SINGULAR;
+      float upd = 0.0f;
+      if (info == 0) {
+        // back substitution: x = U^-1 y, update = -x
+        double x = 0.0;
+#pragma unroll
+        for (int j = L::NMAX - 1; j >= 0; --j) {
+          if (j < N) {
+            const double ujj = __shfl_sync(FULL, h[j], j);
+            const double yj = __shfl_sync(FULL, qv, j);
+            const double xj = yj / ujj;
+            if (lane == j) x = xj;
+            if (lane < j) qv -= h[j] * xj;
+          }
+        }
+        upd = (float)(-x);
+      } else {
+        // DGETRI returns early on a zero pivot and the LU factors themselves
+        // are applied to -q (:591, :605-607), accumulated in float
+#pragma unroll
+        for (int j = 0; j < L::NMAX; ++j) {
+          const double qj = __shfl_sync(FULL, q_orig, j);
+          if (j < N) upd = (float)((double)upd + h[j] * (-1.0) * qj);
+        }
+      }
+      float old[12];
+#pragma unroll
+      for (int i = 0; i < 12; ++i) old[i] = slots[i];
+#pragma unroll
+      for (int kx = 0; kx < 12; ++kx) {
+        float u = __shfl_sync(FULL, upd, kx);
+        if (kx < N) {
+          if (P.momentum != 0.0f) {
+            u += P.momentum * upd_old[kx];
+            upd_old[kx] = u;
+          }
+          slots[P.slot[kx]] += u;
+        }
+      }
+      // test_for_convergence (affine: u, v, theta :433-459; quadratic: all)
+      const float tol = P.fast_tol;
+      bool conv = true;
+      if (SHAPE == DICEGPU_QUADRATIC_SF) {
+#pragma unroll
+        for (int i = 0; i < 12; ++i)
+          if (fabsf(slots[i] - old[i]) >= tol) conv = false;
+      } else {
+        if (fabsf(slots[0] - old[0]) >= tol) conv = false;
+        if (fabsf(slots[1] - old[1]) >= tol) conv = false;
+        if (P.has_rot && fabsf(slots[2] - old[2]) >= tol) conv = false;
+      }
+      if (conv) break;
+    }
+    if (solve_it > P.max_fast) return DICEGPU_MAX_ITERATIONS_REACHED;
+    return DICEGPU_CORRELATION_SUCCESSFUL;
+  }
+
+  // --------------------------------------------------------------------------
+  // Nelder-Mead (Simplex::minimize, DICe_Simplex.cpp:60-277).  Every lane runs
+  // the same bookkeeping on its own private copy of the simplex (identical
+  // values in all lanes, no shared state); the gamma evaluations are
+  // warp-wide passes.  `slots` in/out: left at the last evaluated point, as
+  // the reference's aliasing of variables and shape-function parameters
+  // leaves it (DICe_LocalShapeFunction.h:259-261).  `lastp` receives that
+  // point in slot form.
+  // --------------------------------------------------------------------------
+  __device__ int simplex(const SubsetRef& sb, float* slots, int& num_iterations, float* lastp) {
+    const DevParams& P = A.P;
+    const int nd = P.N;
+    const int mpts = nd + 1;
+    float base[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) base[i] = slots[i];
+    float vars[12], init[12], pts[13][12], gv[13], psum[12], ptry[12];
+    for (int kx = 0; kx < nd; ++kx) init[kx] = base[P.slot[kx]];
+    auto evaluate = [&]() -> float {
+      float cs[12];
+      for (int kx = 0; kx < 12; ++kx) cs[kx] = kx < nd ? vars[kx] : 0.0f;
+      compact_to_slots(cs, lastp, base);
+      return eval_gamma(sb, lastp);
+    };
+    auto finish = [&]() {
+      float cs[12];
+      for (int kx = 0; kx < 12; ++kx) cs[kx] = kx < nd ? vars[kx] : 0.0f;
+      compact_to_slots(cs, slots, base);
+    };
+    // initial simplex vertex_i = x0 + delta_i e_i (:82-107)
+    for (int i = 0; i < mpts; ++i) {
+      for (int j = 0; j < nd; ++j) {
+        pts[i][j] = init[j];
+        if (i > 0 && j == i - 1) pts[i][j] += P.deltas[i - 1];
+        vars[j] = pts[i][j];
+      }
+      gv[i] = evaluate();
+      if (i == 0 && gv[i] < P.skip_thr && gv[i] >= 0.0f) {
+        num_iterations = 0;
+        finish();
+        return DICEGPU_CORRELATION_SUCCESSFUL;
+      }
+      for (int j = 0; j < nd; ++j) vars[j] = init[j];
+    }
+    for (int j = 0; j < nd; ++j) {
+      float sum = 0.0f;
+      for (int i = 0; i < mpts; ++i) sum += pts[i][j];
+      psum[j] = sum;
+    }
+    int inhi = 0;
+    float old_rtol = 0.0f, gamma_new = 0.0f, gamma_old = -1.0f;
+    int gamma_repeats = 0;
+    const float tiny = 1.0e-10f;
+    int iteration = 0;
+    for (iteration = 0; iteration < P.max_robust; iteration++) {
+      if (iteration >= P.max_robust - 1) {
+        num_iterations = iteration;
+        finish();
+        return DICEGPU_MAX_ITERATIONS_REACHED;
+      }
+      int ilo = 0;
+      int ihi;
+      if (gv[0] > gv[1]) { inhi = 1; ihi = 0; } else { inhi = 0; ihi = 1; }
+      for (int i = 0; i < mpts; i++) {
+        if (gv[i] <= gv[ilo]) ilo = i;
+        if (gv[i] > gv[ihi]) { inhi = ihi; ihi = i; }
+        else if (gv[i] > gv[inhi] && i != ihi) inhi = i;
+      }
+      const float rtol = (float)(2.0 * (double)fabsf(gv[ihi] - gv[ilo]) /
+                                 (double)(fabsf(gv[ihi]) + fabsf(gv[ilo]) + tiny));
+      const float rtol_diff = fabsf(rtol - old_rtol);
+      old_rtol = rtol;
+      if (fabsf(gamma_new - gamma_old) < 1.0e-8f) gamma_repeats++;
+      gamma_old = gamma_new;
+      if ((double)rtol < P.robust_tol || (double)rtol_diff < P.robust_tol || gamma_repeats > 15) {
+        const float g0 = gv[0];
+        gv[0] = gv[ilo];
+        gv[ilo] = g0;
+        for (int i = 0; i < nd; i++) {
+          const float t = pts[0][i];
+          pts[0][i] = pts[ilo][i];
+          pts[ilo][i] = t;
+        }
+        break;
+      }
+      auto trial = [&](float fac) -> float {
+        const float fac1 = (float)((1.0 - (double)fac) / nd);
+        const float fac2 = fac1 - fac;
+        for (int j = 0; j < nd; j++) {
+          ptry[j] = psum[j] * fac1 - pts[ihi][j] * fac2;
+          vars[j] = ptry[j];
+        }
+        const float y = evaluate();
+        if (y < gv[ihi]) {
+          gv[ihi] = y;
+          for (int j = 0; j < nd; j++) {
+            psum[j] += ptry[j] - pts[ihi][j];
+            pts[ihi][j] = ptry[j];
+          }
+        }
+        return y;
+      };
+      float ytry = trial(-1.0f);
+      if (ytry <= gv[ilo]) {
+        ytry = trial(2.0f);
+      } else if (ytry >= gv[inhi]) {
+        const float ysave = gv[ihi];
+        ytry = trial(0.5f);
+        if (ytry >= ysave) {
+          for (int i = 0; i < mpts; i++) {
+            if (i != ilo) {
+              for (int j = 0; j < nd; j++) {
+                pts[i][j] = psum[j] = (float)(0.5 * (double)(pts[i][j] + pts[ilo][j]));
+                vars[j] = psum[j];
+              }
+              gv[i] = evaluate();
+            }
+          }
+          for (int j = 0; j < nd; j++) {
+            float sum = 0.0f;
+            for (int i = 0; i < mpts; i++) sum += pts[i][j];
+            psum[j] = sum;
+          }
+        }
+      }
+      gamma_new = evaluate();
+    }
+    num_iterations = iteration;
+    finish();
+    return DICEGPU_CORRELATION_SUCCESSFUL;
+  }
+
+  // Subset::noise_std_dev (DICe_Subset.cpp:622-703) on the deformed image.
+  __device__ float noise_std_dev(const SubsetRef& sb, const PassOut& st, const float* slots) const {
+    if (st.n == 0) return -1.0f;
+    MapConst k;
+    make_mapconst<SHAPE>(slots, false, (float)sb.cx, (float)sb.cy, k);
+    float u, v, t;
+    map_to_u_v_theta<SHAPE>(k, (float)sb.cx, (float)sb.cy, u, v, t);
+    int min_x = (int)((float)st.minx + u), max_x = (int)((float)st.maxx + u);
+    int min_y = (int)((float)st.miny + v), max_y = (int)((float)st.maxy + v);
+    const int img_w = A.def.w, img_h = A.def.h;
+    if (min_x < 0) min_x = 0;
+    if (min_y < 0) min_y = 0;
+    if (max_x >= img_w) min_x = 0;
+    if (max_y >= img_h) min_y = 0;
+    int hh = max_y - min_y + 1, ww = max_x - min_x + 1;
+    if (ww < 3) ww = 3;
+    if (hh < 3) hh = 3;
+    const int rw = max_x - min_x, rh = max_y - min_y;
+    double acc = 0.0;
+    if (rw > 0 && rh > 0) {
+      const long total = (long)rw * rh;
+      const long lim = (long)img_w * img_h;
+      for (long e = lane; e < total; e += 32) {
+        const int yy = min_y + (int)(e / rw), xx = min_x + (int)(e % rw);
+        if (xx < 1 || xx >= img_w - 1 || yy < 1 || yy >= img_h - 1) {
+          const long li = (long)yy * img_w + xx;
+          const float a = (li >= 0 && li < lim) ? __ldg(A.def.I + li) : 0.0f;
+          acc += (double)fabsf(a);
+        } else {
+          const float* q = A.def.I + (size_t)(yy - 1) * img_w + (xx - 1);
+          float conv = 0.0f;
+          conv += __ldg(q) * 1.0f;  conv += __ldg(q + 1) * -2.0f;  conv += __ldg(q + 2) * 1.0f;
+          q += img_w;
+          conv += __ldg(q) * -2.0f; conv += __ldg(q + 1) * 4.0f;   conv += __ldg(q + 2) * -2.0f;
+          q += img_w;
+          conv += __ldg(q) * 1.0f;  conv += __ldg(q + 1) * -2.0f;  conv += __ldg(q + 2) * 1.0f;
+          acc += (double)fabsf(conv);
+        }
+      }
+    }
+    acc = warp_sum(acc);
+    const float var = (float)acc;
+    return (float)((double)var * (sqrt(0.5 * 3.14159265358979323846) / (6.0 * (ww - 2) * (hh - 2))));
+  }
+
+  // Objective::sigma (DICe_Objective.cpp:150-184)
+  __device__ float sigma(const SubsetRef& sb, const PassOut& st, const float* slots, float& noise) const {
+    noise = noise_std_dev(sb, st, slots);
+    if (noise < 0.0f) return -1.0f;
+    const float sgx = (float)st.sgx2, sgy = (float)st.sgy2;
+    const float sg = sgx > sgy ? sgy : sgx;
+    return sg > 0.0f ? (float)sqrt(2.0 * (double)noise * (double)noise / (double)sg) : -1.0f;
+  }
+
+  __device__ void load_slots(const double* f, float* slots) const {
+#pragma unroll
+    for (int i = 0; i < 12; ++i) slots[i] = 0.0f;
+    if (SHAPE == DICEGPU_QUADRATIC_SF) {
+#pragma unroll
+      for (int i = 0; i < 12; ++i) slots[i] = (float)f[DICEGPU_F_QUAD_A + i];
+    } else {
+      slots[0] = (float)f[DICEGPU_F_DISP_X];
+      slots[1] = (float)f[DICEGPU_F_DISP_Y];
+      for (int kx = 2; kx < A.P.N; ++kx) {
+        const int s = A.P.slot[kx];
+        slots[s] = (float)f[DICEGPU_F_DISP_X + s];   // slots 2..5 = ROT_Z..SHEAR_XY
+      }
+    }
+  }
+
+  __device__ void record_failed(double* f, int status, int num_iterations) const {
+    if (lane == 0) {
+      f[DICEGPU_F_SIGMA] = -1.0; f[DICEGPU_F_MATCH] = -1.0; f[DICEGPU_F_GAMMA] = -1.0;
+      f[DICEGPU_F_BETA] = -1.0; f[DICEGPU_F_OMEGA] = -1.0; f[DICEGPU_F_NOISE] = -1.0;
+      f[DICEGPU_F_CONTRAST] = -1.0; f[DICEGPU_F_ACTIVE_PIXELS] = -1.0;
+      f[DICEGPU_F_STATUS] = status; f[DICEGPU_F_ITERATIONS] = num_iterations;
+    }
+  }
+
+  // Objective::beta (DICe_Objective.cpp:78-148)
+  __device__ float beta(const SubsetRef& sb, const float* slots) {
+    const DevParams& P = A.P;
+    MapConst k;
+    make_mapconst<SHAPE>(slots, false, (float)sb.cx, (float)sb.cy, k);
+    float u0, v0, t0;
+    map_to_u_v_theta<SHAPE>(k, (float)sb.cx, (float)sb.cy, u0, v0, t0);
+    auto gam = [&](const float* s) {
+      PassOut o = pass<false, false, true>(sb, s, nullptr);
+      return gamma_from_unnormalised(o);
+    };
+    const float g0 = gam(slots);
+    const float eps = 0.1f;
+    const float fac[3] = {1.0e-3f, 1.0e-3f, 1.0e-1f};
+    float dir[3] = {0.0f, 0.0f, 0.0f};
+    for (int i = 0; i < 3; ++i) {
+      if (!P.has_rot && i == 2 && SHAPE != DICEGPU_QUADRATIC_SF) continue;
+      if (!P.has_rot && i == 2) continue;
+      float u = u0, v = v0, t = t0;
+      float s[12];
+      auto insert = [&]() {
+#pragma unroll
+        for (int j = 0; j < 12; ++j) s[j] = slots[j];
+        if (SHAPE == DICEGPU_QUADRATIC_SF) {
+#pragma unroll
+          for (int j = 0; j < 12; ++j) s[j] = 0.0f;
+          s[0] = cosf(t); s[1] = -sinf(t); s[6] = sinf(t); s[7] = cosf(t);
+          s[5] = u; s[11] = v;
+        } else {
+          s[0] = u; s[1] = v;
+          if (P.has_rot) s[2] = t;
+        }
+      };
+      if (i == 0) u += eps; else if (i == 1) v += eps; else t += eps;
+      insert();
+      const float gp = gam(s);
+      if (i == 0) u -= 2 * eps; else if (i == 1) v -= 2 * eps; else t -= 2 * eps;
+      insert();
+      const float gm = gam(s);
+      if (fabsf(gm - g0) < 1.0e-10f || fabsf(gp - g0) < 1.0e-10f) return -1.0f;
+      const float sm = fabsf(eps / (gm - g0)) * fac[i];
+      const float sp = fabsf(eps / (gp - g0)) * fac[i];
+      dir[i] = (float)((double)(sm + sp) / 2.0);
+    }
+    float mag = 0.0f;
+    for (int i = 0; i < 3; ++i) {
+      if (!P.has_rot && i == 2) continue;
+      mag += dir[i] * dir[i];
+    }
+    return sqrtf(mag);
+  }
+
+  __device__ float gamma_from_unnormalised(const PassOut& o) const {
+    if (o.n == 0) return -1.0f;
+    const double n = (double)o.n;
+    const double sgg = o.sG2 - o.sG * o.sG / n;
+    const double sff = o.sF2 - o.sumF * o.sumF / n;
+    const double sgf = o.sGF - o.sG * o.sumF / n;
+    if (!(sgg > 0.0) || !(sff > 0.0)) return -1.0f;
+    double g = 2.0 - 2.0 * sgf / sqrt(sgg * sff);
+    return (float)(g < 0.0 ? 0.0 : g);
+  }
+
+  // --------------------------------------------------------------------------
+  // generic_correlation_routine for one subset.
+  // --------------------------------------------------------------------------
+  __device__ void run(int idx) {
+    const DevParams& P = A.P;
+    double* f = A.fields + (size_t)idx * DICEGPU_FIELD_STRIDE;
+    SubsetRef sb;
+    sb.idx = idx;
+    sb.cx = (int)f[DICEGPU_F_COORD_X];
+    sb.cy = (int)f[DICEGPU_F_COORD_Y];
+    if (A.geo.half >= 0) {
+      const int side = 2 * A.geo.half + 1;
+      sb.npix = side * side;
+      sb.off = -1;
+    } else {
+      sb.off = A.geo.offsets[idx];
+      sb.npix = A.geo.offsets[idx + 1] - sb.off;
+    }
+    {
+      const int kx = min(max(sb.cx, 0), A.ref.w - 1), ky = min(max(sb.cy, 0), A.ref.h - 1);
+      sb.K = __ldg(A.ref.I + (size_t)ky * A.ref.w + kx);
+    }
+    float slots[12];
+    if (A.mode == MODE_GAMMA) {
+      load_slots(f, slots);
+      const float g = eval_gamma(sb, slots);
+      if (lane == 0) A.gamma_out[idx] = g;
+      return;
+    }
+    if (A.passes_out && lane == 0) A.passes_out[idx] = 0;
+    // frame-0 field-of-view test (DICe_Schema.cpp:2036-2048)
+    if (A.geo.half >= 0 && A.first_frame) {
+      const float cur_x = (float)(f[DICEGPU_F_COORD_X] + f[DICEGPU_F_DISP_X]);
+      const float cur_y = (float)(f[DICEGPU_F_COORD_Y] + f[DICEGPU_F_DISP_Y]);
+      const int hs = P.subset_size / 2;
+      if (cur_x < hs || cur_x > A.def.w - hs || cur_y < hs || cur_y > A.def.h - hs) {
+        record_failed(f, DICEGPU_INITIALIZE_FAILED_BY_EXCEPTION, -1);
+        return;
+      }
+    }
+    int num_iterations = -1;
+    // Field_Value_Initializer::initial_guess (DICe_Initializer.cpp:398-436)
+    if (f[DICEGPU_F_SIGMA] == -1.0) {
+      record_failed(f, DICEGPU_INITIALIZE_FAILED, num_iterations);
+      return;
+    }
+    load_slots(f, slots);
+    int init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+    // reference mean at Gauss-Newton entry: over the pixels active at the last
+    // deformed-state initialisation (none yet: all of them)
+    bool have_state = false;
+    PassOut last_state;
+    float last_eval[12];
+    if (P.init_gamma_thr != -1.0) {
+      PassOut o;
+      const float g0 = eval_gamma(sb, slots, &o);
+      have_state = true;
+      last_state = o;
+      if (g0 > P.init_gamma_thr || g0 < 0.0f) {
+        record_failed(f, DICEGPU_INITIALIZE_FAILED, num_iterations);
+        return;
+      }
+    }
+    const float prev_u = (float)f[DICEGPU_F_DISP_X];
+    const float prev_v = (float)f[DICEGPU_F_DISP_Y];
+    const float prev_t = (float)f[DICEGPU_F_ROT_Z];
+    const bool force_simplex = A.geo.force_simplex && A.geo.force_simplex[idx];
+    const int opt = P.opt;
+    int corr_status = DICEGPU_CORRELATION_FAILED;
+    float cond = 0.0f;
+    bool cond_set = false;
+    bool state_from_simplex = false;
+    (void)state_from_simplex;
+    auto mean_ref = [&]() -> float {
+      if (!have_state) {
+        // all pixels: reuse a moments pass of the reference values
+        double s = 0.0;
+        int cnt = 0;
+        const long lim = (long)A.ref.w * A.ref.h;
+        for (int p = lane; p < sb.npix; p += 32) {
+          int x, y;
+          pixel_xy(sb, p, x, y);
+          const long ri = (long)y * A.ref.w + x;
+          s += ri < lim ? (double)__ldg(A.ref.I + ri) : 0.0;
+          ++cnt;
+        }
+        s = warp_sum(s);
+        cnt = warp_sum_i(cnt);
+        return cnt ? (float)(s / cnt) : 0.0f;
+      }
+      const int n = last_state.n;
+      return n ? (float)((last_state.sumF + (double)n * (double)sb.K) / (double)n) : 0.0f;
+    };
+    auto run_gn = [&]() {
+      const float meanF = mean_ref();
+      corr_status = gauss_newton(sb, slots, meanF, num_iterations, cond, last_state);
+      have_state = true;
+      state_from_simplex = false;
+      cond_set = true;
+    };
+    auto run_simplex = [&]() {
+      corr_status = simplex(sb, slots, num_iterations, last_eval);
+      // state of the last evaluation: active set, gradients and bounding box
+      last_state = pass<false, true, true>(sb, last_eval, nullptr);
+      if (A.passes_out && lane == 0) A.passes_out[idx] += 1;
+      have_state = true;
+      state_from_simplex = true;
+    };
+    if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED || force_simplex) {
+      run_simplex();
+    } else {
+      run_gn();
+    }
+    MapConst kc;
+    const float fcx = (float)f[DICEGPU_F_COORD_X], fcy = (float)f[DICEGPU_F_COORD_Y];
+    float nu, nv, nt;
+    make_mapconst<SHAPE>(slots, false, fcx, fcy, kc);
+    map_to_u_v_theta<SHAPE>(kc, fcx, fcy, nu, nv, nt);
+    bool jump_pass = !(fabsf(nu - prev_u) > P.disp_jump || fabsf(nv - prev_v) > P.disp_jump ||
+                       fabsf(nt - prev_t) > P.theta_jump);
+    if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL || !jump_pass) {
+      bool second_failed = false;
+      if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_GRADIENT_BASED || force_simplex) {
+        second_failed = true;
+      } else if (opt == DICEGPU_GRADIENT_BASED_THEN_SIMPLEX) {
+        load_slots(f, slots);
+        init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+        run_simplex();
+        if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
+      } else if (opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED) {
+        load_slots(f, slots);
+        init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+        run_gn();
+        if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
+      }
+      if (second_failed && corr_status != DICEGPU_CORRELATION_SUCCESSFUL) {
+        if (cond_set && lane == 0) f[DICEGPU_F_CONDITION] = cond;
+        record_failed(f, corr_status, num_iterations);
+        return;
+      }
+    }
+    if (cond_set && lane == 0) f[DICEGPU_F_CONDITION] = cond;
+    // sigma needs the gradients of the last deformed-state initialisation
+    const PassOut st = last_state;
+    float noise = 0.0f;
+    const float sg = sigma(sb, st, slots, noise);
+    if (sg < 0.0f) {
+      record_failed(f, DICEGPU_FRAME_FAILED_DUE_TO_NEGATIVE_SIGMA, num_iterations);
+      return;
+    }
+    PassOut fin;
+    const float gamma = eval_gamma(sb, slots, &fin);
+    const float bt = P.output_beta ? beta(sb, slots) : 0.0f;
+    if ((P.final_gamma_thr != -1.0 && gamma > P.final_gamma_thr) || gamma < 0.0f) {
+      record_failed(f, DICEGPU_FRAME_FAILED_DUE_TO_HIGH_GAMMA, num_iterations);
+      return;
+    }
+    if (fabsf(nu - prev_u) > P.disp_jump || fabsf(nv - prev_v) > P.disp_jump ||
+        fabsf(nt - prev_t) > P.theta_jump) {
+      // (the parameters are unchanged since the first jump test)
+      record_failed(f, DICEGPU_JUMP_TOLERANCE_EXCEEDED, num_iterations);
+      return;
+    }
+    // contrast_std_dev and num_active_pixels at the final parameters
+    float contrast = 0.0f;
+    if (fin.n > 0) {
+      const double nn = (double)fin.n;
+      double sgg = fin.sG2 - fin.sG * fin.sG / nn;
+      if (sgg < 0.0) sgg = 0.0;
+      contrast = (float)sqrt(sgg / nn);
+    }
+    if (lane == 0) {
+      // record_step (DICe_Schema.cpp:1986-2009), save_fields
+      if (SHAPE == DICEGPU_QUADRATIC_SF) {
+        for (int i = 0; i < 12; ++i) f[DICEGPU_F_QUAD_A + i] = slots[i];
+        f[DICEGPU_F_DISP_X] = nu;
+        f[DICEGPU_F_DISP_Y] = nv;
+        f[DICEGPU_F_ROT_Z] = nt;
+      } else {
+        f[DICEGPU_F_DISP_X] = slots[0];
+        f[DICEGPU_F_DISP_Y] = slots[1];
+        for (int kx = 2; kx < P.N; ++kx) {
+          const int s = P.slot[kx];
+          f[DICEGPU_F_DISP_X + s] = slots[s];
+        }
+      }
+      f[DICEGPU_F_SIGMA] = sg;
+      f[DICEGPU_F_MATCH] = 0.0;
+      f[DICEGPU_F_GAMMA] = gamma;
+      f[DICEGPU_F_BETA] = bt;
+      f[DICEGPU_F_NOISE] = noise;
+      f[DICEGPU_F_CONTRAST] = contrast;
+      f[DICEGPU_F_ACTIVE_PIXELS] = fin.n;
+      f[DICEGPU_F_STATUS] = init_status;
+      f[DICEGPU_F_ITERATIONS] = num_iterations;
+    }
+  }
+};
+
+}  // namespace dg

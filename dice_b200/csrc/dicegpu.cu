@@ -1,0 +1,794 @@
+// dicegpu.cu -- kernels and C ABI of libdicegpu.so (sm_100a).
+//
+// Kernels
+//   gradient_kernel   Image_::compute_gradients (finite difference, optional
+//                     5x5 smoothing), DICe_Image.cpp:1015-1093
+//   frame_kernel      persistent work-stealing correlation of every subset:
+//                     one warp per subset, a global atomic queue head
+//   interp_kernel     Image_::interpolate_*_all at arbitrary points
+// The C ABI (include/dicegpu.h) owns device memory and launches on the
+// caller's stream; it never throws and never falls back to the CPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "dg_engine.cuh"
+#include "dicegpu.h"
+
+using namespace dg;
+
+// ---------------------------------------------------------------------------
+// gradients
+// ---------------------------------------------------------------------------
+// Finite differences with c1 = 1/12, c2 = -8/12 stored as float
+// (DICe_Image.cpp:214-215), one-sided within two pixels of the border.
+// Separate rounded products and sums (no contraction) so that the result is
+// bit-identical to the reference's expression order.
+__global__ void gradient_fd_kernel(int w, int h, const float* __restrict__ I, float* __restrict__ gx,
+                                   float* __restrict__ gy) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= w || y >= h) return;
+  const float c1 = (float)(1.0 / 12.0), c2 = (float)(-8.0 / 12.0);
+  const size_t i = (size_t)y * w + x;
+  float a, b;
+  if (x < 2) a = __fsub_rn(I[i + 1], I[i]);
+  else if (x >= w - 2) a = __fsub_rn(I[i], I[i - 1]);
+  else a = __fsub_rn(__fsub_rn(__fadd_rn(__fmul_rn(c1, I[i - 2]), __fmul_rn(c2, I[i - 1])),
+                               __fmul_rn(c2, I[i + 1])),
+                     __fmul_rn(c1, I[i + 2]));
+  if (y < 2) b = __fsub_rn(I[i + w], I[i]);
+  else if (y >= h - 2) b = __fsub_rn(I[i], I[i - w]);
+  else b = __fsub_rn(__fsub_rn(__fadd_rn(__fmul_rn(c1, I[i - 2 * (size_t)w]), __fmul_rn(c2, I[i - w])),
+                               __fmul_rn(c2, I[i + w])),
+                     __fmul_rn(c1, I[i + 2 * (size_t)w]));
+  gx[i] = a;
+  gy[i] = b;
+}
+
+// smooth_gradients_convolution_5_point (DICe_Image.cpp:1034-1060): outer
+// product of (1,4,6,4,1)/16 on the interior, borders copied.
+__global__ void gradient_smooth_kernel(int w, int h, const float* __restrict__ tx,
+                                       const float* __restrict__ ty, float* __restrict__ gx,
+                                       float* __restrict__ gy) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= w || y >= h) return;
+  const size_t i = (size_t)y * w + x;
+  if (x < 2 || x >= w - 2 || y < 2 || y >= h - 2) {
+    gx[i] = tx[i];
+    gy[i] = ty[i];
+    return;
+  }
+  const float k[5] = {0.0625f, 0.25f, 0.375f, 0.25f, 0.0625f};
+  float vx = 0.0f, vy = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 5; ++a)
+#pragma unroll
+    for (int b = 0; b < 5; ++b) {
+      const float c = __fmul_rn(k[a], k[b]);
+      const size_t j = (size_t)(y + a - 2) * w + x + b - 2;
+      vx = __fadd_rn(vx, __fmul_rn(c, tx[j]));
+      vy = __fadd_rn(vy, __fmul_rn(c, ty[j]));
+    }
+  gx[i] = vx;
+  gy[i] = vy;
+}
+
+// ---------------------------------------------------------------------------
+// interpolation at arbitrary points (Image_ interface; border semantics of
+// the reference: bilinear outside its range is 0; Keys / bicubic compute the
+// bilinear value near the border and then overwrite it with the kernel sum
+// read through the row-major linear index, which we reproduce where that
+// index lies inside the image and replace by the bilinear value elsewhere)
+// ---------------------------------------------------------------------------
+__device__ float lin_at(const float* a, long idx, long lim) {
+  return (idx >= 0 && idx < lim) ? a[idx] : 0.0f;
+}
+
+__device__ float bilinear_pt(const float* a, int w, int h, float lx, float ly) {
+  if (lx < 0.0f || (double)lx >= w - 1.5 || ly < 0.0f || (double)ly >= h - 1.5) return 0.0f;
+  const int x1 = (int)lx, x2 = x1 + 1, y1 = (int)ly, y2 = y1 + 1;
+  return a[y1 * w + x1] * (x2 - lx) * (y2 - ly) + a[y1 * w + x2] * (lx - x1) * (y2 - ly) +
+         a[y2 * w + x2] * (lx - x1) * (ly - y1) + a[y2 * w + x1] * (x2 - lx) * (ly - y1);
+}
+
+__global__ void interp_kernel(int method, int w, int h, const float* __restrict__ I,
+                              const float* __restrict__ gxi, const float* __restrict__ gyi, int n,
+                              const float* __restrict__ xy, float* __restrict__ oi,
+                              float* __restrict__ ogx, float* __restrict__ ogy) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const float lx = xy[2 * t], ly = xy[2 * t + 1];
+  const bool grad = gxi && gyi && ogx && ogy;
+  const long lim = (long)w * h;
+  float v = 0.0f, a = 0.0f, b = 0.0f;
+  if (method == DICEGPU_BILINEAR) {
+    v = bilinear_pt(I, w, h, lx, ly);
+    if (grad) { a = bilinear_pt(gxi, w, h, lx, ly); b = bilinear_pt(gyi, w, h, lx, ly); }
+  } else {
+    const int R = method == DICEGPU_KEYS_FOURTH ? 6 : 4;
+    const int off = method == DICEGPU_KEYS_FOURTH ? 2 : 1;
+    const int ix = (int)lx, iy = (int)ly;
+    float wx[6], wy[6];
+    if (R == 6) { keys_weights(lx - ix, wx); keys_weights(ly - iy, wy); }
+    else { cubic_weights(lx - ix, wx); cubic_weights(ly - iy, wy); }
+    bool inside = true;
+    for (int m = 0; m < R; ++m) {
+      const long r0 = (long)(iy - off + m) * w + ix - off;
+      if (r0 < 0 || r0 + R - 1 >= lim) inside = false;
+    }
+    if (!inside) {
+      v = bilinear_pt(I, w, h, lx, ly);
+      if (grad) { a = bilinear_pt(gxi, w, h, lx, ly); b = bilinear_pt(gyi, w, h, lx, ly); }
+    } else {
+      for (int m = 0; m < R; ++m) {
+        float ra = 0.0f, rb = 0.0f, rc = 0.0f;
+        const long r0 = (long)(iy - off + m) * w + ix - off;
+        for (int k = 0; k < R; ++k) {
+          ra = fmaf(wx[k], lin_at(I, r0 + k, lim), ra);
+          if (grad) {
+            rb = fmaf(wx[k], lin_at(gxi, r0 + k, lim), rb);
+            rc = fmaf(wx[k], lin_at(gyi, r0 + k, lim), rc);
+          }
+        }
+        v = fmaf(wy[m], ra, v);
+        if (grad) { a = fmaf(wy[m], rb, a); b = fmaf(wy[m], rc, b); }
+      }
+    }
+  }
+  oi[t] = v;
+  if (grad) { ogx[t] = a; ogy[t] = b; }
+}
+
+// ---------------------------------------------------------------------------
+// the persistent frame kernel
+// ---------------------------------------------------------------------------
+template <int SHAPE, int INTERP, bool DEFGRAD>
+__global__ void __launch_bounds__(256) frame_kernel(const __grid_constant__ FrameArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem<SHAPE>* ws = reinterpret_cast<WarpSmem<SHAPE>*>(smem_raw) + (threadIdx.x >> 5);
+  Engine<SHAPE, INTERP, DEFGRAD> e(a, *ws);
+  const int lane = threadIdx.x & 31;
+  if (a.plain_index >= 0) {
+    if (blockIdx.x == 0 && threadIdx.x < 32) e.run(a.plain_index);
+    return;
+  }
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(a.work_counter, 1);
+    idx = __shfl_sync(FULL, idx, 0);
+    if (idx >= a.n) break;
+    e.run(idx);
+  }
+}
+
+typedef void (*FrameKernelFn)(FrameArgs);
+
+template <int SHAPE>
+static FrameKernelFn pick_kernel(int interp, bool defgrad) {
+  if (defgrad) {
+    if (interp == DICEGPU_KEYS_FOURTH) return frame_kernel<SHAPE, DICEGPU_KEYS_FOURTH, true>;
+    if (interp == DICEGPU_BICUBIC) return frame_kernel<SHAPE, DICEGPU_BICUBIC, true>;
+    return frame_kernel<SHAPE, DICEGPU_BILINEAR, true>;
+  }
+  if (interp == DICEGPU_KEYS_FOURTH) return frame_kernel<SHAPE, DICEGPU_KEYS_FOURTH, false>;
+  if (interp == DICEGPU_BICUBIC) return frame_kernel<SHAPE, DICEGPU_BICUBIC, false>;
+  return frame_kernel<SHAPE, DICEGPU_BILINEAR, false>;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct dicegpu_ctx {
+  dicegpu_params params;
+  DevParams dp;
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  int W = 0, H = 0;
+  float* d_ref = nullptr;
+  float* d_ref_gx = nullptr;
+  float* d_ref_gy = nullptr;
+  float* d_def = nullptr;
+  float* d_def_gx = nullptr;
+  float* d_def_gy = nullptr;
+  float* d_tmp = nullptr;   // smoothing scratch (2 planes)
+  size_t img_cap = 0;       // pixels allocated per plane
+  bool has_ref = false, has_def = false;
+  int n = 0;
+  size_t fields_cap = 0;
+  double* d_fields = nullptr;
+  int32_t* d_offsets = nullptr;
+  int32_t* d_px = nullptr;
+  int32_t* d_py = nullptr;
+  size_t list_cap = 0, offs_cap = 0;
+  bool use_lists = false;
+  uint8_t* d_force = nullptr;
+  size_t force_cap = 0;
+  bool use_force = false;
+  int* d_counter = nullptr;
+  int* d_status = nullptr;
+  int32_t* d_passes = nullptr;
+  size_t passes_cap = 0;
+  int frame_index = 0;
+  int warps_per_cta = 4;
+  int ctas_per_sm = 0;   // 0: occupancy-derived
+  long long launches = 0;
+};
+
+#define CK(x)                                  \
+  do {                                         \
+    cudaError_t e_ = (x);                      \
+    if (e_ != cudaSuccess) return DICEGPU_ERR_CUDA; \
+  } while (0)
+
+static int build_devparams(const dicegpu_params& p, DevParams& d) {
+  if (!p.enable_translation) return DICEGPU_ERR_ARG;
+  if (p.shape_function != DICEGPU_AFFINE_SF && p.shape_function != DICEGPU_QUADRATIC_SF)
+    return DICEGPU_ERR_UNSUPPORTED;
+  if (p.interpolation < DICEGPU_BILINEAR || p.interpolation > DICEGPU_KEYS_FOURTH) return DICEGPU_ERR_ARG;
+  if (!(p.optimization == DICEGPU_SIMPLEX || p.optimization == DICEGPU_GRADIENT_BASED ||
+        p.optimization == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED ||
+        p.optimization == DICEGPU_GRADIENT_BASED_THEN_SIMPLEX))
+    return DICEGPU_ERR_UNSUPPORTED;
+  if (p.max_solver_iterations_fast < 0 || p.max_solver_iterations_robust < 1) return DICEGPU_ERR_ARG;
+  std::memset(&d, 0, sizeof(d));
+  d.shape = p.shape_function;
+  if (d.shape == DICEGPU_QUADRATIC_SF) {
+    d.N = 12;
+    d.NS = 12;
+    const float dl[12] = {0.001f, 0.001f, 1.0e-6f, 1.0e-6f, 1.0e-6f, 1.0f,
+                          0.001f, 0.001f, 1.0e-6f, 1.0e-6f, 1.0e-6f, 1.0f};
+    for (int i = 0; i < 12; ++i) { d.slot[i] = i; d.deltas[i] = dl[i]; }
+    d.has_rot = 0;
+  } else {
+    d.NS = 6;
+    int k = 0;
+    d.slot[k++] = 0;
+    d.slot[k++] = 1;
+    if (p.enable_rotation) d.slot[k++] = 2;
+    if (p.enable_normal_strain) { d.slot[k++] = 3; d.slot[k++] = 4; }
+    if (p.enable_shear_strain) d.slot[k++] = 5;
+    d.N = k;
+    for (int i = 0; i < k; ++i) d.deltas[i] = (float)p.robust_delta_theta;
+    d.deltas[0] = (float)p.robust_delta_disp;
+    d.deltas[1] = (float)p.robust_delta_disp;
+    d.has_rot = p.enable_rotation ? 1 : 0;
+  }
+  d.interp = p.interpolation;
+  d.opt = p.optimization;
+  d.max_fast = p.max_solver_iterations_fast;
+  d.max_robust = p.max_solver_iterations_robust;
+  d.fast_tol = (float)p.fast_solver_tolerance;
+  d.robust_tol = p.robust_solver_tolerance;
+  d.skip_thr = (float)p.skip_solve_gamma_threshold;
+  d.disp_jump = p.disp_jump_tol;
+  d.theta_jump = p.theta_jump_tol;
+  d.lm_alpha = p.levenberg_marquardt_regularization_factor > 0.0
+                   ? (float)p.levenberg_marquardt_regularization_factor : -1.0f;
+  d.momentum = (float)p.momentum_factor;
+  d.init_gamma_thr = p.initial_gamma_threshold;
+  d.final_gamma_thr = p.final_gamma_threshold;
+  d.normalize_gamma = p.normalize_gamma_with_active_pixels;
+  d.output_beta = p.output_beta;
+  d.use_def_grads = p.use_def_gradients;
+  d.subset_size = p.subset_size;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_default_params(dicegpu_params* p) {
+  if (!p) return DICEGPU_ERR_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->shape_function = DICEGPU_AFFINE_SF;
+  p->enable_translation = 1;
+  p->interpolation = DICEGPU_KEYS_FOURTH;
+  p->optimization = DICEGPU_GRADIENT_BASED_THEN_SIMPLEX;
+  p->gradient_method = DICEGPU_FINITE_DIFFERENCE;
+  p->max_solver_iterations_fast = 25;
+  p->max_solver_iterations_robust = 1000;
+  p->fast_solver_tolerance = 1.0e-4;
+  p->robust_solver_tolerance = 1.0e-6;
+  p->skip_solve_gamma_threshold = 1.0e-10;
+  p->robust_delta_disp = 1.0;
+  p->robust_delta_theta = 0.1;
+  p->disp_jump_tol = 10000.0;
+  p->theta_jump_tol = 100.0;
+  p->levenberg_marquardt_regularization_factor = -1.0;
+  p->momentum_factor = 0.0;
+  p->initial_gamma_threshold = -1.0;
+  p->final_gamma_threshold = -1.0;
+  p->use_def_gradients = 1;
+  p->subset_size = 21;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_num_params(const dicegpu_params* p) {
+  if (!p) return DICEGPU_ERR_ARG;
+  DevParams d;
+  const int rc = build_devparams(*p, d);
+  return rc ? rc : d.N;
+}
+
+extern "C" const char* dicegpu_version(void) { return "dicegpu 1.0 (sm_100a)"; }
+
+extern "C" int dicegpu_create(const dicegpu_params* params, dicegpu_ctx** out) {
+  if (!params || !out) return DICEGPU_ERR_ARG;
+  *out = nullptr;
+  dicegpu_ctx* c = new (std::nothrow) dicegpu_ctx();
+  if (!c) return DICEGPU_ERR_NOMEM;
+  c->params = *params;
+  int rc = build_devparams(*params, c->dp);
+  if (rc) { delete c; return rc; }
+  if (cudaGetDevice(&c->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
+      cudaMalloc(&c->d_counter, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess ||
+      cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
+    if (c->d_counter) cudaFree(c->d_counter);
+    delete c;
+    return DICEGPU_ERR_CUDA;
+  }
+  *out = c;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
+  if (!c) return DICEGPU_ERR_ARG;
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->d_ref); cudaFree(c->d_ref_gx); cudaFree(c->d_ref_gy);
+  cudaFree(c->d_def); cudaFree(c->d_def_gx); cudaFree(c->d_def_gy);
+  cudaFree(c->d_tmp);
+  cudaFree(c->d_fields); cudaFree(c->d_offsets); cudaFree(c->d_px); cudaFree(c->d_py);
+  cudaFree(c->d_force); cudaFree(c->d_counter); cudaFree(c->d_status); cudaFree(c->d_passes);
+  delete c;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_params(dicegpu_ctx* c, const dicegpu_params* p) {
+  if (!c || !p) return DICEGPU_ERR_ARG;
+  DevParams d;
+  const int rc = build_devparams(*p, d);
+  if (rc) return rc;
+  c->params = *p;
+  c->dp = d;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_stream(dicegpu_ctx* c, void* stream) {
+  if (!c) return DICEGPU_ERR_ARG;
+  c->stream = (cudaStream_t)stream;
+  return DICEGPU_OK;
+}
+
+static int ensure_images(dicegpu_ctx* c, int w, int h) {
+  const size_t npx = (size_t)w * h;
+  if (c->has_ref && (c->W != w || c->H != h)) {
+    // a new geometry invalidates the previous pair
+    c->has_ref = c->has_def = false;
+  }
+  if (npx > c->img_cap) {
+    cudaStreamSynchronize(c->stream);
+    float** planes[7] = {&c->d_ref, &c->d_ref_gx, &c->d_ref_gy, &c->d_def, &c->d_def_gx, &c->d_def_gy, &c->d_tmp};
+    for (float** pl : planes) { cudaFree(*pl); *pl = nullptr; }
+    for (int i = 0; i < 6; ++i)
+      if (cudaMalloc(planes[i], npx * sizeof(float)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
+    if (cudaMalloc(&c->d_tmp, 2 * npx * sizeof(float)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
+    c->img_cap = npx;
+    c->has_ref = c->has_def = false;
+  }
+  c->W = w;
+  c->H = h;
+  return DICEGPU_OK;
+}
+
+static int launch_gradients(int w, int h, const float* img, float* gx, float* gy, int method,
+                            float* tmp, cudaStream_t st, long long* launches) {
+  dim3 blk(256), grd((w + 255) / 256, h);
+  if (method == DICEGPU_CONVOLUTION_5_POINT) {
+    float* tx = tmp;
+    float* ty = tmp + (size_t)w * h;
+    gradient_fd_kernel<<<grd, blk, 0, st>>>(w, h, img, tx, ty);
+    gradient_smooth_kernel<<<grd, blk, 0, st>>>(w, h, tx, ty, gx, gy);
+    if (launches) *launches += 2;
+  } else {
+    gradient_fd_kernel<<<grd, blk, 0, st>>>(w, h, img, gx, gy);
+    if (launches) *launches += 1;
+  }
+  CK(cudaGetLastError());
+  return DICEGPU_OK;
+}
+
+static int upload_image(dicegpu_ctx* c, float* dst, const float* src, int on_device) {
+  const size_t bytes = (size_t)c->W * c->H * sizeof(float);
+  CK(cudaMemcpyAsync(dst, src, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     c->stream));
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_ref_image(dicegpu_ctx* c, int w, int h, const float* pixels, int on_device) {
+  if (!c || !pixels || w < 16 || h < 16) return DICEGPU_ERR_ARG;
+  int rc = ensure_images(c, w, h);
+  if (rc) return rc;
+  if ((rc = upload_image(c, c->d_ref, pixels, on_device))) return rc;
+  if ((rc = launch_gradients(w, h, c->d_ref, c->d_ref_gx, c->d_ref_gy, c->params.gradient_method,
+                             c->d_tmp, c->stream, &c->launches)))
+    return rc;
+  c->has_ref = true;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_def_image(dicegpu_ctx* c, int w, int h, const float* pixels, int on_device) {
+  if (!c || !pixels) return DICEGPU_ERR_ARG;
+  if (!c->has_ref) return DICEGPU_ERR_STATE;
+  if (w != c->W || h != c->H) return DICEGPU_ERR_ARG;
+  int rc;
+  if ((rc = upload_image(c, c->d_def, pixels, on_device))) return rc;
+  if (c->params.use_def_gradients) {
+    if ((rc = launch_gradients(w, h, c->d_def, c->d_def_gx, c->d_def_gy, c->params.gradient_method,
+                               c->d_tmp, c->stream, &c->launches)))
+      return rc;
+  }
+  c->has_def = true;
+  return DICEGPU_OK;
+}
+
+template <typename T>
+static int grow(T** p, size_t* cap, size_t need) {
+  if (need <= *cap && *p) return DICEGPU_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  if (cudaMalloc(p, std::max<size_t>(need, 1) * sizeof(T)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
+  *cap = need;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_subsets(dicegpu_ctx* c, int n, const double* fields) {
+  if (!c || n < 1 || !fields) return DICEGPU_ERR_ARG;
+  cudaStreamSynchronize(c->stream);
+  int rc = grow(&c->d_fields, &c->fields_cap, (size_t)n * DICEGPU_FIELD_STRIDE);
+  if (rc) return rc;
+  rc = grow(&c->d_passes, &c->passes_cap, (size_t)n);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->d_fields, fields, (size_t)n * DICEGPU_FIELD_STRIDE * sizeof(double),
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->n != n) { c->use_lists = false; c->use_force = false; }
+  c->n = n;
+  c->frame_index = 0;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_subset_pixels(dicegpu_ctx* c, int n, const int32_t* offsets,
+                                         const int32_t* px, const int32_t* py) {
+  if (!c || n != c->n || !offsets || !px || !py) return DICEGPU_ERR_ARG;
+  if (offsets[0] != 0) return DICEGPU_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (offsets[i + 1] < offsets[i]) return DICEGPU_ERR_ARG;
+  const size_t total = (size_t)offsets[n];
+  cudaStreamSynchronize(c->stream);
+  int rc;
+  if ((rc = grow(&c->d_offsets, &c->offs_cap, (size_t)n + 1))) return rc;
+  size_t cap2 = c->list_cap;
+  if ((rc = grow(&c->d_px, &c->list_cap, total))) return rc;
+  if ((rc = grow(&c->d_py, &cap2, total))) return rc;
+  c->list_cap = std::min(c->list_cap, cap2);
+  CK(cudaMemcpy(c->d_offsets, offsets, (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (total) {
+    CK(cudaMemcpy(c->d_px, px, total * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_py, py, total * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  c->use_lists = true;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_force_simplex(dicegpu_ctx* c, int n, const uint8_t* flags) {
+  if (!c) return DICEGPU_ERR_ARG;
+  if (!flags) { c->use_force = false; return DICEGPU_OK; }
+  if (n != c->n) return DICEGPU_ERR_ARG;
+  cudaStreamSynchronize(c->stream);
+  int rc = grow(&c->d_force, &c->force_cap, (size_t)n);
+  if (rc) return rc;
+  CK(cudaMemcpy(c->d_force, flags, n, cudaMemcpyHostToDevice));
+  c->use_force = true;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_get_fields(dicegpu_ctx* c, double* out) {
+  if (!c || !out || c->n < 1) return DICEGPU_ERR_ARG;
+  CK(cudaMemcpyAsync(out, c->d_fields, (size_t)c->n * DICEGPU_FIELD_STRIDE * sizeof(double),
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_load_fields(dicegpu_ctx* c, const double* src, int on_device) {
+  if (!c || !src || c->n < 1) return DICEGPU_ERR_ARG;
+  CK(cudaMemcpyAsync(c->d_fields, src, (size_t)c->n * DICEGPU_FIELD_STRIDE * sizeof(double),
+                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+  c->frame_index = 0;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_store_fields(dicegpu_ctx* c, double* dst, int on_device) {
+  if (!c || !dst || c->n < 1) return DICEGPU_ERR_ARG;
+  CK(cudaMemcpyAsync(dst, c->d_fields, (size_t)c->n * DICEGPU_FIELD_STRIDE * sizeof(double),
+                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_fields_device_ptr(dicegpu_ctx* c, double** dptr) {
+  if (!c || !dptr) return DICEGPU_ERR_ARG;
+  *dptr = c->d_fields;
+  return DICEGPU_OK;
+}
+
+static size_t warp_smem_bytes(int shape) {
+  return shape == DICEGPU_QUADRATIC_SF ? sizeof(WarpSmem<DICEGPU_QUADRATIC_SF>)
+                                       : sizeof(WarpSmem<DICEGPU_AFFINE_SF>);
+}
+
+static FrameKernelFn frame_fn(const dicegpu_ctx* c) {
+  const bool dg = c->params.use_def_gradients != 0;
+  return c->dp.shape == DICEGPU_QUADRATIC_SF ? pick_kernel<DICEGPU_QUADRATIC_SF>(c->dp.interp, dg)
+                                             : pick_kernel<DICEGPU_AFFINE_SF>(c->dp.interp, dg);
+}
+
+static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
+  std::memset(&a, 0, sizeof(a));
+  a.P = c->dp;
+  a.ref = DevImage{c->W, c->H, c->d_ref, c->d_ref_gx, c->d_ref_gy};
+  a.def = DevImage{c->W, c->H, c->d_def, c->params.use_def_gradients ? c->d_def_gx : c->d_ref_gx,
+                   c->params.use_def_gradients ? c->d_def_gy : c->d_ref_gy};
+  a.geo.half = c->use_lists ? -1 : c->params.subset_size / 2;
+  a.geo.offsets = c->use_lists ? c->d_offsets : nullptr;
+  a.geo.px = c->use_lists ? c->d_px : nullptr;
+  a.geo.py = c->use_lists ? c->d_py : nullptr;
+  a.geo.force_simplex = c->use_force ? c->d_force : nullptr;
+  a.fields = c->d_fields;
+  a.n = c->n;
+  a.first_frame = c->frame_index == 0;
+  a.mode = mode;
+  a.plain_index = -1;
+  a.work_counter = c->d_counter;
+  a.status = c->d_status;
+  a.passes_out = c->d_passes;
+}
+
+static int grid_for(dicegpu_ctx* c, FrameKernelFn fn, int* blocks, size_t* smem) {
+  const int threads = c->warps_per_cta * 32;
+  *smem = warp_smem_bytes(c->dp.shape) * c->warps_per_cta;
+  CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+  int per_sm = c->ctas_per_sm;
+  if (per_sm <= 0) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, threads, *smem));
+    if (per_sm < 1) per_sm = 1;
+  }
+  *blocks = per_sm * c->num_sms;
+  return DICEGPU_OK;
+}
+
+static int ready(dicegpu_ctx* c) {
+  if (!c) return DICEGPU_ERR_ARG;
+  if (!c->has_ref || !c->has_def || c->n < 1) return DICEGPU_ERR_STATE;
+  if (!c->use_lists && c->params.subset_size < 1) return DICEGPU_ERR_ARG;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_execute_correlation(dicegpu_ctx* c) {
+  int rc = ready(c);
+  if (rc) return rc;
+  FrameKernelFn fn = frame_fn(c);
+  int blocks;
+  size_t smem;
+  if ((rc = grid_for(c, fn, &blocks, &smem))) return rc;
+  FrameArgs a;
+  fill_args(c, a, MODE_CORRELATE);
+  CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
+  fn<<<blocks, c->warps_per_cta * 32, smem, c->stream>>>(a);
+  CK(cudaGetLastError());
+  c->launches += 1;
+  c->frame_index += 1;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
+  int rc = ready(c);
+  if (rc) return rc;
+  FrameKernelFn fn = frame_fn(c);
+  const size_t smem = warp_smem_bytes(c->dp.shape);
+  FrameArgs a;
+  fill_args(c, a, MODE_CORRELATE);
+  for (int i = 0; i < c->n; ++i) {
+    a.plain_index = i;
+    fn<<<1, 32, smem, c->stream>>>(a);
+  }
+  CK(cudaGetLastError());
+  c->launches += c->n;
+  c->frame_index += 1;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_launch_count(dicegpu_ctx* c, int64_t* count) {
+  if (!c || !count) return DICEGPU_ERR_ARG;
+  *count = c->launches;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_launch_shape(dicegpu_ctx* c, int warps_per_cta, int ctas_per_sm) {
+  if (!c || warps_per_cta < 0 || warps_per_cta > 8 || ctas_per_sm < 0) return DICEGPU_ERR_ARG;
+  if (warps_per_cta > 0) c->warps_per_cta = warps_per_cta;
+  if (ctas_per_sm >= 0) c->ctas_per_sm = ctas_per_sm;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_get_launch_shape(dicegpu_ctx* c, int* warps_per_cta, int* ctas_per_sm) {
+  if (!c || !warps_per_cta || !ctas_per_sm) return DICEGPU_ERR_ARG;
+  *warps_per_cta = c->warps_per_cta;
+  *ctas_per_sm = c->ctas_per_sm;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_device_status(dicegpu_ctx* c, int32_t* status) {
+  if (!c || !status) return DICEGPU_ERR_ARG;
+  CK(cudaMemcpyAsync(status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_gamma(dicegpu_ctx* c, const double* fields, double* gamma_out) {
+  int rc = ready(c);
+  if (rc) return rc;
+  if (!fields || !gamma_out) return DICEGPU_ERR_ARG;
+  double* d_f = nullptr;
+  double* d_g = nullptr;
+  const size_t fb = (size_t)c->n * DICEGPU_FIELD_STRIDE * sizeof(double);
+  if (cudaMalloc(&d_f, fb) != cudaSuccess) return DICEGPU_ERR_NOMEM;
+  if (cudaMalloc(&d_g, c->n * sizeof(double)) != cudaSuccess) { cudaFree(d_f); return DICEGPU_ERR_NOMEM; }
+  rc = DICEGPU_OK;
+  if (cudaMemcpyAsync(d_f, fields, fb, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+  FrameKernelFn fn = frame_fn(c);
+  int blocks;
+  size_t smem;
+  if (!rc) rc = grid_for(c, fn, &blocks, &smem);
+  if (!rc) {
+    FrameArgs a;
+    fill_args(c, a, MODE_GAMMA);
+    a.fields = d_f;
+    a.gamma_out = d_g;
+    a.passes_out = nullptr;
+    if (cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream) != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+    fn<<<blocks, c->warps_per_cta * 32, smem, c->stream>>>(a);
+    if (cudaGetLastError() != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+    c->launches += 1;
+    if (!rc && cudaMemcpyAsync(gamma_out, d_g, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+      rc = DICEGPU_ERR_CUDA;
+    if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+  }
+  cudaStreamSynchronize(c->stream);
+  cudaFree(d_f);
+  cudaFree(d_g);
+  return rc;
+}
+
+extern "C" int dicegpu_interpolate(dicegpu_ctx* c, int method, int n, const float* xy,
+                                   float* intensity, float* grad_x, float* grad_y, int on_device) {
+  if (!c || !xy || !intensity || n < 0) return DICEGPU_ERR_ARG;
+  if (!c->has_def) return DICEGPU_ERR_STATE;
+  if (method < DICEGPU_BILINEAR || method > DICEGPU_KEYS_FOURTH) return DICEGPU_ERR_ARG;
+  if (n == 0) return DICEGPU_OK;
+  const bool grad = grad_x && grad_y && c->params.use_def_gradients;
+  const float *dxy = xy;
+  float *di = intensity, *dgx = grad_x, *dgy = grad_y;
+  float* buf = nullptr;
+  if (!on_device) {
+    if (cudaMalloc(&buf, (size_t)n * 5 * sizeof(float)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
+    dxy = buf;
+    di = buf + 2 * (size_t)n;
+    dgx = buf + 3 * (size_t)n;
+    dgy = buf + 4 * (size_t)n;
+    if (cudaMemcpyAsync((void*)dxy, xy, 2 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
+      cudaFree(buf);
+      return DICEGPU_ERR_CUDA;
+    }
+  }
+  interp_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(
+      method, c->W, c->H, c->d_def, grad ? c->d_def_gx : nullptr, grad ? c->d_def_gy : nullptr, n,
+      dxy, di, grad ? dgx : nullptr, grad ? dgy : nullptr);
+  c->launches += 1;
+  int rc = cudaGetLastError() == cudaSuccess ? DICEGPU_OK : DICEGPU_ERR_CUDA;
+  if (!on_device) {
+    if (!rc && cudaMemcpyAsync(intensity, di, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+    if (!rc && grad) {
+      if (cudaMemcpyAsync(grad_x, dgx, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+      if (cudaMemcpyAsync(grad_y, dgy, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+    }
+    cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+  }
+  return rc;
+}
+
+extern "C" int dicegpu_image_gradients(int w, int h, const float* d_img, float* d_gx, float* d_gy,
+                                       int method, void* stream) {
+  if (!d_img || !d_gx || !d_gy || w < 3 || h < 3) return DICEGPU_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  float* tmp = nullptr;
+  if (method == DICEGPU_CONVOLUTION_5_POINT) {
+    if (cudaMalloc(&tmp, 2 * (size_t)w * h * sizeof(float)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
+  }
+  int rc = launch_gradients(w, h, d_img, d_gx, d_gy, method, tmp, st, nullptr);
+  if (tmp) {
+    cudaStreamSynchronize(st);
+    cudaFree(tmp);
+  }
+  return rc;
+}
+
+// dice_correlate's stride-9 interface (DICe_api.cpp:51-151) over a context
+// created for the call.
+extern "C" int dicegpu_correlate(float* points, int n_points, int subset_size, const float* ref_img,
+                                 int ref_w, int ref_h, const float* def_img, int def_w, int def_h,
+                                 const dicegpu_params* params) {
+  if (ref_w != def_w || ref_h != def_h) return -1;
+  if (subset_size < 1) return -1;
+  if (n_points < 1) return -1;
+  if (!points || !ref_img || !def_img) return -1;
+  dicegpu_params p;
+  if (params) {
+    p = *params;
+  } else {
+    // tracking_default_params (DICe_ParameterUtilities.cpp:297-361)
+    dicegpu_default_params(&p);
+    p.optimization = DICEGPU_SIMPLEX;
+    p.enable_rotation = 1;
+    p.disp_jump_tol = 8.0;
+    p.theta_jump_tol = 0.1;
+  }
+  if (p.shape_function != DICEGPU_AFFINE_SF) return DICEGPU_ERR_UNSUPPORTED;
+  p.subset_size = subset_size;
+  p.use_def_gradients = 1;   // arrays: Schema::set_def_image(w,h,array), DICe_Schema.cpp:339
+  dicegpu_ctx* c = nullptr;
+  int rc = dicegpu_create(&p, &c);
+  if (rc) return rc;
+  std::vector<double> f((size_t)n_points * DICEGPU_FIELD_STRIDE, 0.0);
+  for (int i = 0; i < n_points; ++i) {
+    double* r = &f[(size_t)i * DICEGPU_FIELD_STRIDE];
+    const float* q = points + (size_t)i * DICEGPU_API_STRIDE;
+    r[DICEGPU_F_COORD_X] = q[0];
+    r[DICEGPU_F_COORD_Y] = q[1];
+    r[DICEGPU_F_DISP_X] = q[2];
+    r[DICEGPU_F_DISP_Y] = q[3];
+    r[DICEGPU_F_ROT_Z] = q[4];
+    r[DICEGPU_F_SIGMA] = q[5];
+    r[DICEGPU_F_GAMMA] = q[6];
+    r[DICEGPU_F_BETA] = q[7];
+    r[DICEGPU_F_STATUS] = q[8];
+  }
+  if (!rc) rc = dicegpu_set_ref_image(c, ref_w, ref_h, ref_img, 0);
+  if (!rc) rc = dicegpu_set_def_image(c, def_w, def_h, def_img, 0);
+  if (!rc) rc = dicegpu_set_subsets(c, n_points, f.data());
+  if (!rc) rc = dicegpu_execute_correlation(c);
+  if (!rc) rc = dicegpu_get_fields(c, f.data());
+  if (!rc) {
+    for (int i = 0; i < n_points; ++i) {
+      const double* r = &f[(size_t)i * DICEGPU_FIELD_STRIDE];
+      float* q = points + (size_t)i * DICEGPU_API_STRIDE;
+      q[2] = (float)r[DICEGPU_F_DISP_X];
+      q[3] = (float)r[DICEGPU_F_DISP_Y];
+      q[4] = (float)r[DICEGPU_F_ROT_Z];
+      q[5] = (float)r[DICEGPU_F_SIGMA];
+      q[6] = (float)r[DICEGPU_F_GAMMA];
+      q[7] = (float)r[DICEGPU_F_BETA];
+      q[8] = (float)r[DICEGPU_F_STATUS];
+    }
+  }
+  dicegpu_destroy(c);
+  return rc;
+}

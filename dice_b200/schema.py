@@ -1,0 +1,211 @@
+"""Python mirror of the reference's Schema boundary over libdicegpu.so.
+
+    schema = Schema(params)                    # DICe::Schema(..., params)
+    schema.set_ref_image(ref)                  # Schema::set_ref_image(w, h, array)
+    schema.set_subsets(cx, cy)                 # subset centroids (COORDINATES_X/Y fields)
+    schema.set_def_image(deformed)             # Schema::set_def_image(w, h, array)
+    schema.execute_correlation()               # Schema::execute_correlation()
+    u = schema.field(abi.F_DISP_X)             # global_field_value(i, SUBSET_DISPLACEMENT_X_FS)
+
+Every call goes through the C ABI; images may be numpy arrays (host) or
+torch CUDA tensors (device pointers, no copy through the host).
+"""
+import ctypes
+
+import numpy as np
+
+from . import abi
+
+
+def _as_host_f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _is_cuda_tensor(a):
+    try:
+        import torch
+        return isinstance(a, torch.Tensor) and a.is_cuda
+    except Exception:
+        return False
+
+
+class Schema:
+    def __init__(self, params=None, stream=None):
+        self.lib = abi.load_library()
+        self.params = params.copy() if params is not None else abi.default_params()
+        self.ctx = ctypes.c_void_p()
+        abi.check(self.lib.dicegpu_create(ctypes.byref(self.params), ctypes.byref(self.ctx)),
+                  "dicegpu_create")
+        self.n = 0
+        self.w = self.h = 0
+        self._keep = []
+        if stream is not None:
+            self.set_stream(stream)
+
+    def close(self):
+        if self.ctx:
+            self.lib.dicegpu_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- configuration ------------------------------------------------------
+    def set_params(self, params):
+        self.params = params.copy()
+        abi.check(self.lib.dicegpu_set_params(self.ctx, ctypes.byref(self.params)), "set_params")
+
+    def set_stream(self, stream):
+        """stream: a cudaStream_t handle (int) or a torch.cuda.Stream."""
+        h = getattr(stream, "cuda_stream", stream)
+        abi.check(self.lib.dicegpu_set_stream(self.ctx, ctypes.c_void_p(int(h))), "set_stream")
+
+    def set_launch_shape(self, warps_per_cta=0, ctas_per_sm=0):
+        abi.check(self.lib.dicegpu_set_launch_shape(self.ctx, warps_per_cta, ctas_per_sm),
+                  "set_launch_shape")
+
+    def launch_shape(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        abi.check(self.lib.dicegpu_get_launch_shape(self.ctx, ctypes.byref(a), ctypes.byref(b)),
+                  "get_launch_shape")
+        return a.value, b.value
+
+    # ---- images ---------------------------------------------------------------
+    def _image_call(self, fn, img, what):
+        if _is_cuda_tensor(img):
+            t = img.contiguous().float()
+            h, w = t.shape
+            self._keep.append(t)
+            rc = fn(self.ctx, w, h, ctypes.c_void_p(t.data_ptr()), 1)
+        else:
+            a = _as_host_f32(img)
+            h, w = a.shape
+            rc = fn(self.ctx, w, h, a.ctypes.data_as(ctypes.c_void_p), 0)
+        abi.check(rc, what)
+        self.w, self.h = w, h
+
+    def set_ref_image(self, img):
+        self._image_call(self.lib.dicegpu_set_ref_image, img, "set_ref_image")
+
+    def set_def_image(self, img):
+        self._image_call(self.lib.dicegpu_set_def_image, img, "set_def_image")
+        if len(self._keep) > 4:
+            self._keep = self._keep[-4:]
+
+    # ---- subsets ----------------------------------------------------------------
+    def set_fields(self, fields):
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        assert f.ndim == 2 and f.shape[1] == abi.FIELD_STRIDE
+        abi.check(self.lib.dicegpu_set_subsets(self.ctx, f.shape[0], f.ctypes.data_as(ctypes.c_void_p)),
+                  "set_subsets")
+        self.n = f.shape[0]
+
+    def set_subsets(self, cx, cy, quadratic=None):
+        from .synthetic import init_fields
+        if quadratic is None:
+            quadratic = self.params.shape_function == abi.QUADRATIC_SF
+        self.set_fields(init_fields(np.asarray(cx, np.float64), np.asarray(cy, np.float64), quadratic))
+
+    def set_subset_pixels(self, offsets, px, py):
+        o = np.ascontiguousarray(offsets, dtype=np.int32)
+        x = np.ascontiguousarray(px, dtype=np.int32)
+        y = np.ascontiguousarray(py, dtype=np.int32)
+        abi.check(self.lib.dicegpu_set_subset_pixels(self.ctx, self.n, o.ctypes.data_as(ctypes.c_void_p),
+                                                     x.ctypes.data_as(ctypes.c_void_p),
+                                                     y.ctypes.data_as(ctypes.c_void_p)), "set_subset_pixels")
+
+    def set_force_simplex(self, flags):
+        if flags is None:
+            abi.check(self.lib.dicegpu_set_force_simplex(self.ctx, 0, None), "set_force_simplex")
+            return
+        a = np.ascontiguousarray(flags, dtype=np.uint8)
+        abi.check(self.lib.dicegpu_set_force_simplex(self.ctx, a.shape[0], a.ctypes.data_as(ctypes.c_void_p)),
+                  "set_force_simplex")
+
+    # ---- execution ----------------------------------------------------------------
+    def execute_correlation(self):
+        abi.check(self.lib.dicegpu_execute_correlation(self.ctx), "execute_correlation")
+
+    def execute_correlation_plain(self):
+        abi.check(self.lib.dicegpu_execute_correlation_plain(self.ctx), "execute_correlation_plain")
+
+    def fields(self):
+        out = np.zeros((self.n, abi.FIELD_STRIDE), np.float64)
+        abi.check(self.lib.dicegpu_get_fields(self.ctx, out.ctypes.data_as(ctypes.c_void_p)), "get_fields")
+        return out
+
+    def field(self, col):
+        return self.fields()[:, col]
+
+    def load_fields(self, src):
+        """Asynchronous reload of all fields (numpy host array or CUDA tensor); restarts at frame 0."""
+        if _is_cuda_tensor(src):
+            abi.check(self.lib.dicegpu_load_fields(self.ctx, ctypes.c_void_p(src.data_ptr()), 1), "load_fields")
+        else:
+            a = np.ascontiguousarray(src, dtype=np.float64)
+            self._keep.append(a)
+            abi.check(self.lib.dicegpu_load_fields(self.ctx, a.ctypes.data_as(ctypes.c_void_p), 0), "load_fields")
+
+    def store_fields(self, dst):
+        """Asynchronous copy of all fields into a CUDA tensor or pinned host tensor (no sync)."""
+        on_dev = 1 if _is_cuda_tensor(dst) else 0
+        abi.check(self.lib.dicegpu_store_fields(self.ctx, ctypes.c_void_p(dst.data_ptr()), on_dev), "store_fields")
+
+    def fields_device_ptr(self):
+        p = ctypes.c_void_p()
+        abi.check(self.lib.dicegpu_fields_device_ptr(self.ctx, ctypes.byref(p)), "fields_device_ptr")
+        return p.value
+
+    def launch_count(self):
+        c = ctypes.c_int64()
+        abi.check(self.lib.dicegpu_launch_count(self.ctx, ctypes.byref(c)), "launch_count")
+        return c.value
+
+    def device_status(self):
+        s = ctypes.c_int32()
+        abi.check(self.lib.dicegpu_device_status(self.ctx, ctypes.byref(s)), "device_status")
+        return s.value
+
+    def gamma(self, fields):
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        out = np.zeros(f.shape[0], np.float64)
+        abi.check(self.lib.dicegpu_gamma(self.ctx, f.ctypes.data_as(ctypes.c_void_p),
+                                         out.ctypes.data_as(ctypes.c_void_p)), "gamma")
+        return out
+
+    def interpolate(self, method, xy, gradients=True):
+        xy = np.ascontiguousarray(xy, dtype=np.float32).reshape(-1, 2)
+        n = xy.shape[0]
+        oi = np.zeros(n, np.float32)
+        gx = np.zeros(n, np.float32) if gradients else None
+        gy = np.zeros(n, np.float32) if gradients else None
+        p = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+        abi.check(self.lib.dicegpu_interpolate(self.ctx, method, n, p(xy), p(oi), p(gx), p(gy), 0),
+                  "interpolate")
+        return oi, gx, gy
+
+
+def correlate(points, subset_size, ref, deff, params=None):
+    """dice_correlate mirror: points is an (n, 9) float32 array updated in place."""
+    lib = abi.load_library()
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    ref = _as_host_f32(ref)
+    deff = _as_host_f32(deff)
+    h, w = ref.shape
+    dh, dw = deff.shape
+    rc = lib.dicegpu_correlate(pts.ctypes.data_as(ctypes.c_void_p), pts.shape[0], subset_size,
+                               ref.ctypes.data_as(ctypes.c_void_p), w, h,
+                               deff.ctypes.data_as(ctypes.c_void_p), dw, dh,
+                               ctypes.byref(params) if params is not None else None)
+    if rc == 0:
+        points[...] = pts
+    return rc

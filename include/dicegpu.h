@@ -196,6 +196,12 @@ int dicegpu_set_force_simplex(dicegpu_ctx* ctx, int n, const uint8_t* flags);
 int dicegpu_get_fields(dicegpu_ctx* ctx, double* fields_out);
 /* Device pointer of the field array (n * DICEGPU_FIELD_STRIDE doubles). */
 int dicegpu_fields_device_ptr(dicegpu_ctx* ctx, double** dptr);
+/* Asynchronous copies of the whole field array on the context's stream
+ * (`on_device` = 1 for device memory, 0 for host memory; pinned host memory
+ * keeps the copy asynchronous).  dicegpu_load_fields restarts the sequence:
+ * the next frame is frame 0 again.  No synchronisation. */
+int dicegpu_load_fields(dicegpu_ctx* ctx, const double* src, int on_device);
+int dicegpu_store_fields(dicegpu_ctx* ctx, double* dst, int on_device);
 
 /* One frame of local DIC over every subset: initial guess from the field
  * values (USE_FIELD_VALUES), Gauss-Newton and/or simplex per

@@ -410,11 +410,11 @@ struct Subset {
   }
   // initialize(ref_img) with no shape function (:385-389, :428-437)
   void init_ref(const Image& im) {
-    for (int i = 0; i < npix; ++i) ref[i] = im.I[(long)y[i] * im.w + x[i]];
+    for (int i = 0; i < npix; ++i) ref[i] = im.at(im.I, (long)y[i] * im.w + x[i]);
     if (im.has_gradients) {
       for (int i = 0; i < npix; ++i) {
-        gx[i] = im.gx[(long)y[i] * im.w + x[i]];
-        gy[i] = im.gy[(long)y[i] * im.w + x[i]];
+        gx[i] = im.at(im.gx, (long)y[i] * im.w + x[i]);
+        gy[i] = im.at(im.gy, (long)y[i] * im.w + x[i]);
       }
       has_gradients = true;
     }
