@@ -54,6 +54,9 @@ struct DevImage {
   const float* __restrict__ I;
   const float* __restrict__ gx;
   const float* __restrict__ gy;
+  // (I, Gx, Gy, 0) interleaved: one 16-byte load fetches all three channels
+  // of a tap (deformed image with gradients only)
+  const float4* __restrict__ p4;
 };
 
 // Subset geometry: square (`half` >= 0, centred on the COORD fields) or an
@@ -141,85 +144,66 @@ __device__ __forceinline__ void cubic_weights(float t, float w[4]) {
 // Interpolation at an interior point (the subset border test keeps every
 // active pixel at least 3.5 px from the image edge, so no tap leaves the
 // image: DICe_Subset.cpp:408).  Separable evaluation: a 6-tap (4-tap) row sum
-// per row, then the column sum.
+// per row, then the column sum.  With gradients the taps come from the
+// interleaved (I, Gx, Gy, 0) image, one 16-byte load per tap.
+template <int R, bool GRAD>
+__device__ __forceinline__ void conv_taps(const DevImage& im, int x0, int y0, const float* wx,
+                                          const float* wy, float& iv, float& gxv, float& gyv) {
+  const int w = im.w;
+  float a = 0.0f, b = 0.0f, c = 0.0f;
+  if (GRAD) {
+    const float4* q = im.p4 + (size_t)y0 * w + x0;
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      float ra = 0.0f, rb = 0.0f, rc = 0.0f;
+#pragma unroll
+      for (int n = 0; n < R; ++n) {
+        const float4 t = __ldg(q + n);
+        ra = fmaf(wx[n], t.x, ra);
+        rb = fmaf(wx[n], t.y, rb);
+        rc = fmaf(wx[n], t.z, rc);
+      }
+      a = fmaf(wy[m], ra, a);
+      b = fmaf(wy[m], rb, b);
+      c = fmaf(wy[m], rc, c);
+      q += w;
+    }
+    gxv = b;
+    gyv = c;
+  } else {
+    const float* q = im.I + (size_t)y0 * w + x0;
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      float ra = 0.0f;
+#pragma unroll
+      for (int n = 0; n < R; ++n) ra = fmaf(wx[n], __ldg(q + n), ra);
+      a = fmaf(wy[m], ra, a);
+      q += w;
+    }
+  }
+  iv = a;
+}
+
 template <int INTERP, bool GRAD>
 __device__ __forceinline__ void interp_interior(const DevImage& im, float x, float y, float& iv,
                                                 float& gxv, float& gyv) {
-  const int w = im.w;
+  const int ix = (int)x, iy = (int)y;
   if (INTERP == DICEGPU_KEYS_FOURTH) {
-    const int ix = (int)x, iy = (int)y;
     float wx[6], wy[6];
     keys_weights(x - (float)ix, wx);
     keys_weights(y - (float)iy, wy);
-    const float* pI = im.I + (size_t)(iy - 2) * w + (ix - 2);
-    const float* pX = im.gx + (size_t)(iy - 2) * w + (ix - 2);
-    const float* pY = im.gy + (size_t)(iy - 2) * w + (ix - 2);
-    float a = 0.0f, b = 0.0f, c = 0.0f;
-#pragma unroll
-    for (int m = 0; m < 6; ++m) {
-      float ra = 0.0f, rb = 0.0f, rc = 0.0f;
-#pragma unroll
-      for (int n = 0; n < 6; ++n) {
-        ra = fmaf(wx[n], __ldg(pI + n), ra);
-        if (GRAD) {
-          rb = fmaf(wx[n], __ldg(pX + n), rb);
-          rc = fmaf(wx[n], __ldg(pY + n), rc);
-        }
-      }
-      a = fmaf(wy[m], ra, a);
-      if (GRAD) {
-        b = fmaf(wy[m], rb, b);
-        c = fmaf(wy[m], rc, c);
-      }
-      pI += w;
-      if (GRAD) { pX += w; pY += w; }
-    }
-    iv = a;
-    if (GRAD) { gxv = b; gyv = c; }
+    conv_taps<6, GRAD>(im, ix - 2, iy - 2, wx, wy, iv, gxv, gyv);
   } else if (INTERP == DICEGPU_BICUBIC) {
-    const int ix = (int)x, iy = (int)y;
     float wx[4], wy[4];
     cubic_weights(x - (float)ix, wx);
     cubic_weights(y - (float)iy, wy);
-    const float* pI = im.I + (size_t)(iy - 1) * w + (ix - 1);
-    const float* pX = im.gx + (size_t)(iy - 1) * w + (ix - 1);
-    const float* pY = im.gy + (size_t)(iy - 1) * w + (ix - 1);
-    float a = 0.0f, b = 0.0f, c = 0.0f;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      float ra = 0.0f, rb = 0.0f, rc = 0.0f;
-#pragma unroll
-      for (int n = 0; n < 4; ++n) {
-        ra = fmaf(wx[n], __ldg(pI + n), ra);
-        if (GRAD) {
-          rb = fmaf(wx[n], __ldg(pX + n), rb);
-          rc = fmaf(wx[n], __ldg(pY + n), rc);
-        }
-      }
-      a = fmaf(wy[m], ra, a);
-      if (GRAD) {
-        b = fmaf(wy[m], rb, b);
-        c = fmaf(wy[m], rc, c);
-      }
-      pI += w;
-      if (GRAD) { pX += w; pY += w; }
-    }
-    iv = a;
-    if (GRAD) { gxv = b; gyv = c; }
+    conv_taps<4, GRAD>(im, ix - 1, iy - 1, wx, wy, iv, gxv, gyv);
   } else {
     // Image_::interpolate_bilinear_all (DICe_Image.cpp:394-425), interior form
-    const int x1 = (int)x, y1 = (int)y;
-    const float fx1 = (float)(x1 + 1) - x, fx0 = x - (float)x1;
-    const float fy1 = (float)(y1 + 1) - y, fy0 = y - (float)y1;
-    const size_t o = (size_t)y1 * w + x1;
-    iv = __ldg(im.I + o) * fx1 * fy1 + __ldg(im.I + o + 1) * fx0 * fy1 +
-         __ldg(im.I + o + w + 1) * fx0 * fy0 + __ldg(im.I + o + w) * fx1 * fy0;
-    if (GRAD) {
-      gxv = __ldg(im.gx + o) * fx1 * fy1 + __ldg(im.gx + o + 1) * fx0 * fy1 +
-            __ldg(im.gx + o + w + 1) * fx0 * fy0 + __ldg(im.gx + o + w) * fx1 * fy0;
-      gyv = __ldg(im.gy + o) * fx1 * fy1 + __ldg(im.gy + o + 1) * fx0 * fy1 +
-            __ldg(im.gy + o + w + 1) * fx0 * fy0 + __ldg(im.gy + o + w) * fx1 * fy0;
-    }
+    const float fx1 = (float)(ix + 1) - x, fx0 = x - (float)ix;
+    const float fy1 = (float)(iy + 1) - y, fy0 = y - (float)iy;
+    const float wx[2] = {fx1, fx0}, wy[2] = {fy1, fy0};
+    conv_taps<2, GRAD>(im, ix, iy, wx, wy, iv, gxv, gyv);
   }
 }
 
@@ -241,6 +225,61 @@ __device__ __forceinline__ void affine_D(const MapConst& k, float dx, float dy, 
                                          float& Dy) {
   Dx = (float)__dadd_rn(__dmul_rn(1.0 + (double)k.s[3], (double)dx), (double)__fmul_rn(k.s[5], dy));
   Dy = (float)__dadd_rn(__dmul_rn(1.0 + (double)k.s[4], (double)dy), (double)__fmul_rn(k.s[5], dx));
+}
+
+// Map of a pixel offset (dx, dy) = (x - cx, y - cy); for affine maps the
+// stretched offsets (Dx, Dy) are returned too (the residuals reuse them).
+template <int SHAPE>
+__device__ __forceinline__ void map_offset(const MapConst& k, float dx, float dy, float cx, float cy,
+                                           float& ox, float& oy, float& Dx, float& Dy) {
+  if (SHAPE == DICEGPU_QUADRATIC_SF) {
+    // Quadratic_Shape_Function::map (:509-520), left-to-right FP32 sums
+    float a = __fmul_rn(k.s[0], dx);
+    a = __fadd_rn(a, __fmul_rn(k.s[1], dy));
+    a = __fadd_rn(a, __fmul_rn(__fmul_rn(k.s[2], dx), dy));
+    a = __fadd_rn(a, __fmul_rn(__fmul_rn(k.s[3], dx), dx));
+    a = __fadd_rn(a, __fmul_rn(__fmul_rn(k.s[4], dy), dy));
+    a = __fadd_rn(a, k.s[5]);
+    ox = __fadd_rn(a, cx);
+    float b = __fmul_rn(k.s[6], dx);
+    b = __fadd_rn(b, __fmul_rn(k.s[7], dy));
+    b = __fadd_rn(b, __fmul_rn(__fmul_rn(k.s[8], dx), dy));
+    b = __fadd_rn(b, __fmul_rn(__fmul_rn(k.s[9], dx), dx));
+    b = __fadd_rn(b, __fmul_rn(__fmul_rn(k.s[10], dy), dy));
+    b = __fadd_rn(b, k.s[11]);
+    oy = __fadd_rn(b, cy);
+    Dx = dx;
+    Dy = dy;
+  } else {
+    affine_D(k, dx, dy, Dx, Dy);
+    ox = __fadd_rn(__fadd_rn(__fsub_rn(__fmul_rn(k.cost, Dx), __fmul_rn(k.sint, Dy)), k.s[0]), cx);
+    oy = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(k.sint, Dx), __fmul_rn(k.cost, Dy)), k.s[1]), cy);
+  }
+}
+
+// Residual vector dG/dp in slot order (affine :350-396, quadratic :580-614)
+// from the pixel offset and the stretched offset of map_offset.
+template <int SHAPE>
+__device__ __forceinline__ void residuals_D(const MapConst& k, float dx, float dy, float Dx, float Dy,
+                                            float gx, float gy, bool use_ref_grads, float* r) {
+  float Gx = gx, Gy = gy;
+  if (use_ref_grads) {
+    Gx = k.rcos * gx - k.rsin * gy;
+    Gy = k.rsin * gx + k.rcos * gy;
+  }
+  if (SHAPE == DICEGPU_QUADRATIC_SF) {
+    const float dxdy = dx * dy, dx2 = dx * dx, dy2 = dy * dy;
+    r[0] = Gx * dx; r[1] = Gx * dy; r[2] = Gx * dxdy; r[3] = Gx * dx2; r[4] = Gx * dy2; r[5] = Gx;
+    r[6] = Gy * dx; r[7] = Gy * dy; r[8] = Gy * dxdy; r[9] = Gy * dx2; r[10] = Gy * dy2; r[11] = Gy;
+  } else {
+    const float c = k.cost, s = k.sint;
+    r[0] = Gx;
+    r[1] = Gy;
+    r[2] = Gx * (-s * Dx - c * Dy) + Gy * (c * Dx - s * Dy);
+    r[3] = Gx * dx * c + Gy * dx * s;
+    r[4] = -Gx * dy * s + Gy * dy * c;
+    r[5] = Gx * (c * dy - s * dx) + Gy * (s * dy + c * dx);
+  }
 }
 
 template <int SHAPE>
@@ -344,9 +383,12 @@ __device__ __forceinline__ void make_mapconst(const float* slots, bool use_ref_g
 }
 
 // Pixel rounding of Subset::initialize (DICe_Subset.cpp:405-406).
+// The reference adds 0.5 in double; in float m + 0.5f is exact for
+// |m| < 2^22 except where the sum crosses a power of two, and there the
+// rounding cannot cross an integer, so the truncations agree.
 __device__ __forceinline__ int round_pixel(float m) {
   const int a = (int)m;
-  const int b = (int)((double)m + 0.5);
+  const int b = (int)(m + 0.5f);
   return b == a ? a : a + 1;
 }
 

@@ -54,6 +54,26 @@ struct __align__(16) WarpSmem {
   double M[Layout<SHAPE>::VW * Layout<SHAPE>::VW];
 };
 
+// Dynamic shared memory of the frame kernel: one WarpSmem per warp.  Taken
+// from the extern array in every user so the compiler keeps shared-space
+// (not generic) addressing.
+extern __shared__ __align__(16) unsigned char dg_smem[];
+
+template <int SHAPE>
+__device__ __forceinline__ WarpSmem<SHAPE>* warp_smem() {
+  return reinterpret_cast<WarpSmem<SHAPE>*>(dg_smem) + (threadIdx.x >> 5);
+}
+
+__device__ __forceinline__ void sts_v4(unsigned addr, float a, float b, float c, float d) {
+  asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+               : "memory");
+}
+__device__ __forceinline__ float lds_f(unsigned addr) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];\n" : "=f"(v) : "r"(addr) : "memory");
+  return v;
+}
+
 // Result of one pass over the subset pixels.
 struct PassOut {
   int n;                    // active pixels
@@ -73,10 +93,9 @@ template <int SHAPE, int INTERP, bool DEFGRAD>
 struct Engine {
   using L = Layout<SHAPE>;
   const FrameArgs& A;
-  WarpSmem<SHAPE>& S;
   const int lane;
 
-  __device__ Engine(const FrameArgs& a, WarpSmem<SHAPE>& s) : A(a), S(s), lane(threadIdx.x & 31) {}
+  __device__ explicit Engine(const FrameArgs& a) : A(a), lane(threadIdx.x & 31) {}
 
   __device__ __forceinline__ void pixel_xy(const SubsetRef& sb, int p, int& x, int& y) const {
     if (sb.off < 0) {
@@ -105,21 +124,50 @@ struct Engine {
     const int W = A.def.w, H = A.def.h;
     PassOut o;
     int n = 0;
-    double sumF = 0.0, sG = 0.0, sG2 = 0.0, sF2 = 0.0, sGF = 0.0, sgx2 = 0.0, sgy2 = 0.0;
-    int minx = sb.cx, maxx = sb.cx, miny = sb.cy, maxy = sb.cy;
-    double c[4][2];
+    // per-lane partial sums: FP32 over this lane's pixels (the reference sums
+    // these in FP32 over the whole subset), FP64 across the warp; the gamma
+    // moments are FP64 throughout
+    float sumF = 0.0f, sgx2 = 0.0f, sgy2 = 0.0f;
+    double sG = 0.0, sG2 = 0.0, sF2 = 0.0, sGF = 0.0, sFd = 0.0;
+    const int cxi = sb.cx, cyi = sb.cy, npix = sb.npix, off = sb.off;
+    const float K = sb.K;
+    int minx = cxi, maxx = cxi, miny = cyi, maxy = cyi;
+    // two independent accumulator sets (even / odd pixel groups) so that
+    // consecutive mma instructions do not wait on each other
+    double c[2][3][2];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) { c[b][0] = 0.0; c[b][1] = 0.0; }
-    for (int base = 0; base < sb.npix; base += 32) {
+    for (int s2 = 0; s2 < 2; ++s2)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) { c[s2][b][0] = 0.0; c[s2][b][1] = 0.0; }
+    // square subsets: (row, col) of this lane's pixel advanced by 32 per step
+    const int half = A.geo.half;
+    const int side = 2 * half + 1;
+    int row = 0, col = 0, drow = 0, dcol = 0;
+    if (off < 0) {
+      row = lane / side; col = lane - row * side;
+      drow = 32 / side; dcol = 32 - drow * side;
+    }
+    const int x0 = cxi - half, y0 = cyi - half;
+    const long ref_lim = (long)A.ref.w * A.ref.h;
+    for (int base = 0; base < npix; base += 32) {
       const int p = base + lane;
       float v[L::VW];
 #pragma unroll
       for (int i = 0; i < L::VW; ++i) v[i] = 0.0f;
-      if (p < sb.npix) {
-        int x, y;
-        pixel_xy(sb, p, x, y);
-        float mx, my;
-        map_point<SHAPE>(k, (float)x, (float)y, fcx, fcy, mx, my);
+      int x, y;
+      if (off < 0) {
+        x = max(x0 + col, 0);
+        y = max(y0 + row, 0);
+        col += dcol; row += drow;
+        if (col >= side) { col -= side; ++row; }
+      } else if (p < npix) {
+        x = max(__ldg(A.geo.px + off + p), 0);
+        y = max(__ldg(A.geo.py + off + p), 0);
+      }
+      if (p < npix) {
+        float mx, my, Dx, Dy;
+        const float dxf = __fsub_rn((float)x, fcx), dyf = __fsub_rn((float)y, fcy);
+        map_offset<SHAPE>(k, dxf, dyf, fcx, fcy, mx, my, Dx, Dy);
         const int px = round_pixel(mx), py = round_pixel(my);
         const bool active = !(px < 4 || px >= W - 4 || py < 4 || py >= H - 4);
         if (active) {
@@ -129,29 +177,30 @@ struct Engine {
           // the reference reads intensities_[y*w+x] unchecked (row-major wrap);
           // same element inside the array, 0 outside it
           const long ri = (long)y * A.ref.w + x;
-          const bool rin = ri < (long)A.ref.w * A.ref.h;
+          const bool rin = ri < ref_lim;
           const float F = rin ? __ldg(A.ref.I + ri) : 0.0f;
           if (GRADS && !DEFGRAD) {
             gx = rin ? __ldg(A.ref.gx + ri) : 0.0f;
             gy = rin ? __ldg(A.ref.gy + ri) : 0.0f;
           }
           ++n;
-          const float Fs = F - sb.K, Gs = G - sb.K;
-          sumF += (double)Fs;
+          const float Fs = F - K, Gs = G - K;
+          if (!MOMENTS) sumF += Fs;
           if (MOMENTS) {
+            sFd += (double)Fs;
             sG += (double)Gs;
             sG2 = fma((double)Gs, (double)Gs, sG2);
             sF2 = fma((double)Fs, (double)Fs, sF2);
             sGF = fma((double)Gs, (double)Fs, sGF);
           }
           if (GRADS) {
-            sgx2 = fma((double)gx, (double)gx, sgx2);
-            sgy2 = fma((double)gy, (double)gy, sgy2);
+            sgx2 = fmaf(gx, gx, sgx2);
+            sgy2 = fmaf(gy, gy, sgy2);
             minx = min(minx, x); maxx = max(maxx, x);
             miny = min(miny, y); maxy = max(maxy, y);
           }
           if (ACC_H) {
-            residuals<SHAPE>(k, (float)x, (float)y, fcx, fcy, gx, gy, use_ref_grads, v);
+            residuals_D<SHAPE>(k, dxf, dyf, Dx, Dy, gx, gy, use_ref_grads, v);
             v[L::ID] = G - F;
             v[L::IONE] = 1.0f;
           }
@@ -159,37 +208,43 @@ struct Engine {
       }
       if (ACC_H) {
         // stage the 32 pixel vectors, then 8 groups of 4 pixels through the FP64 mma
-        float* row = S.vbuf + lane * L::VS;
+        const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_smem<SHAPE>()->vbuf);
+        const unsigned vrow = vbase + (unsigned)(lane * L::VS) * 4u;
 #pragma unroll
-        for (int i = 0; i < L::VW; i += 4)
-          *reinterpret_cast<float4*>(row + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        for (int i = 0; i < L::VW; i += 4) sts_v4(vrow + 4u * i, v[i], v[i + 1], v[i + 2], v[i + 3]);
         __syncwarp();
         const int kk = lane & 3, ii = lane >> 2;
 #pragma unroll
         for (int g = 0; g < 8; ++g) {
-          const float* src = S.vbuf + (4 * g + kk) * L::VS + ii;
+          const unsigned src = vbase + (unsigned)((4 * g + kk) * L::VS + ii) * 4u;
+          double(&cs)[3][2] = c[g & 1];
           if (SHAPE == DICEGPU_QUADRATIC_SF) {
-            const double a0 = (double)src[0], a1 = (double)src[8];
-            dmma_8x8x4(c[0][0], c[0][1], a0, a0);
-            dmma_8x8x4(c[1][0], c[1][1], a0, a1);
-            dmma_8x8x4(c[2][0], c[2][1], a1, a1);
+            const double a0 = (double)lds_f(src), a1 = (double)lds_f(src + 32u);
+            dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
+            dmma_8x8x4(cs[1][0], cs[1][1], a0, a1);
+            dmma_8x8x4(cs[2][0], cs[2][1], a1, a1);
           } else {
-            const double a0 = (double)src[0];
-            dmma_8x8x4(c[0][0], c[0][1], a0, a0);
+            const double a0 = (double)lds_f(src);
+            dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
           }
         }
         __syncwarp();
       }
     }
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      c[0][b][0] += c[1][b][0];
+      c[0][b][1] += c[1][b][1];
+    }
     o.n = warp_sum_i(n);
-    o.sumF = warp_sum(sumF);
+    o.sumF = MOMENTS ? warp_sum(sFd) : warp_sum((double)sumF);
     if (MOMENTS) {
       o.sG = warp_sum(sG); o.sG2 = warp_sum(sG2); o.sF2 = warp_sum(sF2); o.sGF = warp_sum(sGF);
     } else {
       o.sG = o.sG2 = o.sF2 = o.sGF = 0.0;
     }
     if (GRADS) {
-      o.sgx2 = warp_sum(sgx2); o.sgy2 = warp_sum(sgy2);
+      o.sgx2 = warp_sum((double)sgx2); o.sgy2 = warp_sum((double)sgy2);
       o.minx = warp_min_i(minx); o.maxx = warp_max_i(maxx);
       o.miny = warp_min_i(miny); o.maxy = warp_max_i(maxy);
     } else {
@@ -201,14 +256,15 @@ struct Engine {
       __syncwarp();
       const int r = lane >> 2, cc = 2 * (lane & 3);
       constexpr int VW = L::VW;
+      const double(&cf)[3][2] = c[0];
       if (SHAPE == DICEGPU_QUADRATIC_SF) {
-        C[r * VW + cc] = c[0][0];           C[r * VW + cc + 1] = c[0][1];
-        C[r * VW + 8 + cc] = c[1][0];       C[r * VW + 8 + cc + 1] = c[1][1];
-        C[(8 + cc) * VW + r] = c[1][0];     C[(8 + cc + 1) * VW + r] = c[1][1];
-        C[(8 + r) * VW + 8 + cc] = c[2][0]; C[(8 + r) * VW + 8 + cc + 1] = c[2][1];
+        C[r * VW + cc] = cf[0][0];           C[r * VW + cc + 1] = cf[0][1];
+        C[r * VW + 8 + cc] = cf[1][0];       C[r * VW + 8 + cc + 1] = cf[1][1];
+        C[(8 + cc) * VW + r] = cf[1][0];     C[(8 + cc + 1) * VW + r] = cf[1][1];
+        C[(8 + r) * VW + 8 + cc] = cf[2][0]; C[(8 + r) * VW + 8 + cc + 1] = cf[2][1];
       } else {
-        C[r * VW + cc] = c[0][0];
-        C[r * VW + cc + 1] = c[0][1];
+        C[r * VW + cc] = cf[0][0];
+        C[r * VW + cc + 1] = cf[0][1];
       }
       __syncwarp();
     }
@@ -255,7 +311,7 @@ struct Engine {
     float upd_old[12];
 #pragma unroll
     for (int i = 0; i < 12; ++i) upd_old[i] = 0.0f;
-    double* M = S.M;
+    double* M = warp_smem<SHAPE>()->M;
     int solve_it = 0;
     for (; solve_it <= P.max_fast; ++solve_it) {
       num_iterations = solve_it;

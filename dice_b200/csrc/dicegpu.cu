@@ -80,6 +80,13 @@ __global__ void gradient_smooth_kernel(int w, int h, const float* __restrict__ t
   gy[i] = vy;
 }
 
+// (I, Gx, Gy) -> interleaved float4 (the layout the frame kernel gathers from)
+__global__ void pack_kernel(size_t n, const float* __restrict__ I, const float* __restrict__ gx,
+                            const float* __restrict__ gy, float4* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_float4(I[i], gx[i], gy[i], 0.0f);
+}
+
 // ---------------------------------------------------------------------------
 // interpolation at arbitrary points (Image_ interface; border semantics of
 // the reference: bilinear outside its range is 0; Keys / bicubic compute the
@@ -150,10 +157,8 @@ __global__ void interp_kernel(int method, int w, int h, const float* __restrict_
 // the persistent frame kernel
 // ---------------------------------------------------------------------------
 template <int SHAPE, int INTERP, bool DEFGRAD>
-__global__ void __launch_bounds__(256) frame_kernel(const __grid_constant__ FrameArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  WarpSmem<SHAPE>* ws = reinterpret_cast<WarpSmem<SHAPE>*>(smem_raw) + (threadIdx.x >> 5);
-  Engine<SHAPE, INTERP, DEFGRAD> e(a, *ws);
+__global__ void __launch_bounds__(256, 3) frame_kernel(const __grid_constant__ FrameArgs a) {
+  Engine<SHAPE, INTERP, DEFGRAD> e(a);
   const int lane = threadIdx.x & 31;
   if (a.plain_index >= 0) {
     if (blockIdx.x == 0 && threadIdx.x < 32) e.run(a.plain_index);
@@ -199,6 +204,7 @@ struct dicegpu_ctx {
   float* d_def_gx = nullptr;
   float* d_def_gy = nullptr;
   float* d_tmp = nullptr;   // smoothing scratch (2 planes)
+  float4* d_def4 = nullptr; // deformed (I, Gx, Gy, 0) interleaved
   size_t img_cap = 0;       // pixels allocated per plane
   bool has_ref = false, has_def = false;
   int n = 0;
@@ -344,6 +350,7 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   cudaFree(c->d_ref); cudaFree(c->d_ref_gx); cudaFree(c->d_ref_gy);
   cudaFree(c->d_def); cudaFree(c->d_def_gx); cudaFree(c->d_def_gy);
   cudaFree(c->d_tmp);
+  cudaFree(c->d_def4);
   cudaFree(c->d_fields); cudaFree(c->d_offsets); cudaFree(c->d_px); cudaFree(c->d_py);
   cudaFree(c->d_force); cudaFree(c->d_counter); cudaFree(c->d_status); cudaFree(c->d_passes);
   delete c;
@@ -376,6 +383,9 @@ static int ensure_images(dicegpu_ctx* c, int w, int h) {
     cudaStreamSynchronize(c->stream);
     float** planes[7] = {&c->d_ref, &c->d_ref_gx, &c->d_ref_gy, &c->d_def, &c->d_def_gx, &c->d_def_gy, &c->d_tmp};
     for (float** pl : planes) { cudaFree(*pl); *pl = nullptr; }
+    cudaFree(c->d_def4);
+    c->d_def4 = nullptr;
+    if (cudaMalloc(&c->d_def4, npx * sizeof(float4)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
     for (int i = 0; i < 6; ++i)
       if (cudaMalloc(planes[i], npx * sizeof(float)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
     if (cudaMalloc(&c->d_tmp, 2 * npx * sizeof(float)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
@@ -433,6 +443,11 @@ extern "C" int dicegpu_set_def_image(dicegpu_ctx* c, int w, int h, const float* 
     if ((rc = launch_gradients(w, h, c->d_def, c->d_def_gx, c->d_def_gy, c->params.gradient_method,
                                c->d_tmp, c->stream, &c->launches)))
       return rc;
+    const size_t npx = (size_t)w * h;
+    pack_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, c->stream>>>(npx, c->d_def, c->d_def_gx,
+                                                                      c->d_def_gy, c->d_def4);
+    CK(cudaGetLastError());
+    c->launches += 1;
   }
   c->has_def = true;
   return DICEGPU_OK;
@@ -543,9 +558,10 @@ static FrameKernelFn frame_fn(const dicegpu_ctx* c) {
 static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
   std::memset(&a, 0, sizeof(a));
   a.P = c->dp;
-  a.ref = DevImage{c->W, c->H, c->d_ref, c->d_ref_gx, c->d_ref_gy};
+  a.ref = DevImage{c->W, c->H, c->d_ref, c->d_ref_gx, c->d_ref_gy, nullptr};
   a.def = DevImage{c->W, c->H, c->d_def, c->params.use_def_gradients ? c->d_def_gx : c->d_ref_gx,
-                   c->params.use_def_gradients ? c->d_def_gy : c->d_ref_gy};
+                   c->params.use_def_gradients ? c->d_def_gy : c->d_ref_gy,
+                   c->params.use_def_gradients ? c->d_def4 : nullptr};
   a.geo.half = c->use_lists ? -1 : c->params.subset_size / 2;
   a.geo.offsets = c->use_lists ? c->d_offsets : nullptr;
   a.geo.px = c->use_lists ? c->d_px : nullptr;
