@@ -16,7 +16,7 @@
 //   sum r (G-F) - (meanG - meanF) sum r.
 #pragma once
 
-#include "dg_device.cuh"
+#include "dg_pass.cuh"
 
 namespace dg {
 
@@ -36,51 +36,6 @@ struct FrameArgs {
   int* work_counter;     // persistent work queue head
   int* status;           // device error word
   int32_t* passes_out;   // optional: pixel passes executed per subset (GN + simplex + epilogue)
-};
-
-template <int SHAPE>
-struct Layout {
-  static constexpr int NS = SHAPE == DICEGPU_QUADRATIC_SF ? 12 : 6;   // parameter slots
-  static constexpr int VW = SHAPE == DICEGPU_QUADRATIC_SF ? 16 : 8;   // [r, d, 1] padded
-  static constexpr int VS = SHAPE == DICEGPU_QUADRATIC_SF ? 24 : 8;   // smem row stride (conflict-free)
-  static constexpr int ID = NS;      // column of d = G - F
-  static constexpr int IONE = NS + 1;  // column of 1
-  static constexpr int NMAX = NS;
-};
-
-template <int SHAPE>
-struct __align__(16) WarpSmem {
-  float vbuf[32 * Layout<SHAPE>::VS];
-  double M[Layout<SHAPE>::VW * Layout<SHAPE>::VW];
-};
-
-// Dynamic shared memory of the frame kernel: one WarpSmem per warp.  Taken
-// from the extern array in every user so the compiler keeps shared-space
-// (not generic) addressing.
-extern __shared__ __align__(16) unsigned char dg_smem[];
-
-template <int SHAPE>
-__device__ __forceinline__ WarpSmem<SHAPE>* warp_smem() {
-  return reinterpret_cast<WarpSmem<SHAPE>*>(dg_smem) + (threadIdx.x >> 5);
-}
-
-__device__ __forceinline__ void sts_v4(unsigned addr, float a, float b, float c, float d) {
-  asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
-               : "memory");
-}
-__device__ __forceinline__ float lds_f(unsigned addr) {
-  float v;
-  asm volatile("ld.shared.f32 %0, [%1];\n" : "=f"(v) : "r"(addr) : "memory");
-  return v;
-}
-
-// Result of one pass over the subset pixels.
-struct PassOut {
-  int n;                    // active pixels
-  double sumF;              // sum of F over active pixels (shifted by K)
-  double sG, sG2, sF2, sGF; // shifted moments (gamma passes)
-  double sgx2, sgy2;        // sum of unrotated gradient^2 (sigma)
-  int minx, maxx, miny, maxy;
 };
 
 struct SubsetRef {
@@ -111,164 +66,27 @@ struct Engine {
     y = y < 0 ? 0 : y;
   }
 
-  // One pass over the subset at the parameters in `slots`.
-  //   ACC_H   : accumulate sum v v^T (Gauss-Newton)
-  //   GRADS   : interpolate the deformed gradients (DEFGRAD) / read reference ones
-  //   MOMENTS : intensity moments for gamma
+  // One pass over the subset at the parameters in `slots` (see subset_pass).
   template <bool ACC_H, bool GRADS, bool MOMENTS>
-  __device__ PassOut pass(const SubsetRef& sb, const float* slots, double* C) {
-    const bool use_ref_grads = !DEFGRAD;
+  __device__ __forceinline__ PassOut pass(const SubsetRef& sb, const float* slots, double* /*C*/) {
+    PassIn in;
+    in.def = A.def;
+    in.refI = A.ref.I;
+    in.refgx = A.ref.gx;
+    in.refgy = A.ref.gy;
+    in.refw = A.ref.w;
+    in.reflim = (long)A.ref.w * A.ref.h;
+    in.px = A.geo.px;
+    in.py = A.geo.py;
+    in.half = A.geo.half;
+    in.cx = sb.cx;
+    in.cy = sb.cy;
+    in.npix = sb.npix;
+    in.off = sb.off;
+    in.K = sb.K;
     MapConst k;
-    const float fcx = (float)sb.cx, fcy = (float)sb.cy;
-    make_mapconst<SHAPE>(slots, use_ref_grads, fcx, fcy, k);
-    const int W = A.def.w, H = A.def.h;
-    PassOut o;
-    int n = 0;
-    // per-lane partial sums: FP32 over this lane's pixels (the reference sums
-    // these in FP32 over the whole subset), FP64 across the warp; the gamma
-    // moments are FP64 throughout
-    float sumF = 0.0f, sgx2 = 0.0f, sgy2 = 0.0f;
-    double sG = 0.0, sG2 = 0.0, sF2 = 0.0, sGF = 0.0, sFd = 0.0;
-    const int cxi = sb.cx, cyi = sb.cy, npix = sb.npix, off = sb.off;
-    const float K = sb.K;
-    int minx = cxi, maxx = cxi, miny = cyi, maxy = cyi;
-    // two independent accumulator sets (even / odd pixel groups) so that
-    // consecutive mma instructions do not wait on each other
-    double c[2][3][2];
-#pragma unroll
-    for (int s2 = 0; s2 < 2; ++s2)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) { c[s2][b][0] = 0.0; c[s2][b][1] = 0.0; }
-    // square subsets: (row, col) of this lane's pixel advanced by 32 per step
-    const int half = A.geo.half;
-    const int side = 2 * half + 1;
-    int row = 0, col = 0, drow = 0, dcol = 0;
-    if (off < 0) {
-      row = lane / side; col = lane - row * side;
-      drow = 32 / side; dcol = 32 - drow * side;
-    }
-    const int x0 = cxi - half, y0 = cyi - half;
-    const long ref_lim = (long)A.ref.w * A.ref.h;
-    for (int base = 0; base < npix; base += 32) {
-      const int p = base + lane;
-      float v[L::VW];
-#pragma unroll
-      for (int i = 0; i < L::VW; ++i) v[i] = 0.0f;
-      int x, y;
-      if (off < 0) {
-        x = max(x0 + col, 0);
-        y = max(y0 + row, 0);
-        col += dcol; row += drow;
-        if (col >= side) { col -= side; ++row; }
-      } else if (p < npix) {
-        x = max(__ldg(A.geo.px + off + p), 0);
-        y = max(__ldg(A.geo.py + off + p), 0);
-      }
-      if (p < npix) {
-        float mx, my, Dx, Dy;
-        const float dxf = __fsub_rn((float)x, fcx), dyf = __fsub_rn((float)y, fcy);
-        map_offset<SHAPE>(k, dxf, dyf, fcx, fcy, mx, my, Dx, Dy);
-        const int px = round_pixel(mx), py = round_pixel(my);
-        const bool active = !(px < 4 || px >= W - 4 || py < 4 || py >= H - 4);
-        if (active) {
-          float G, gx = 0.0f, gy = 0.0f;
-          if (GRADS && DEFGRAD) interp_interior<INTERP, true>(A.def, mx, my, G, gx, gy);
-          else interp_interior<INTERP, false>(A.def, mx, my, G, gx, gy);
-          // the reference reads intensities_[y*w+x] unchecked (row-major wrap);
-          // same element inside the array, 0 outside it
-          const long ri = (long)y * A.ref.w + x;
-          const bool rin = ri < ref_lim;
-          const float F = rin ? __ldg(A.ref.I + ri) : 0.0f;
-          if (GRADS && !DEFGRAD) {
-            gx = rin ? __ldg(A.ref.gx + ri) : 0.0f;
-            gy = rin ? __ldg(A.ref.gy + ri) : 0.0f;
-          }
-          ++n;
-          const float Fs = F - K, Gs = G - K;
-          if (!MOMENTS) sumF += Fs;
-          if (MOMENTS) {
-            sFd += (double)Fs;
-            sG += (double)Gs;
-            sG2 = fma((double)Gs, (double)Gs, sG2);
-            sF2 = fma((double)Fs, (double)Fs, sF2);
-            sGF = fma((double)Gs, (double)Fs, sGF);
-          }
-          if (GRADS) {
-            sgx2 = fmaf(gx, gx, sgx2);
-            sgy2 = fmaf(gy, gy, sgy2);
-            minx = min(minx, x); maxx = max(maxx, x);
-            miny = min(miny, y); maxy = max(maxy, y);
-          }
-          if (ACC_H) {
-            residuals_D<SHAPE>(k, dxf, dyf, Dx, Dy, gx, gy, use_ref_grads, v);
-            v[L::ID] = G - F;
-            v[L::IONE] = 1.0f;
-          }
-        }
-      }
-      if (ACC_H) {
-        // stage the 32 pixel vectors, then 8 groups of 4 pixels through the FP64 mma
-        const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_smem<SHAPE>()->vbuf);
-        const unsigned vrow = vbase + (unsigned)(lane * L::VS) * 4u;
-#pragma unroll
-        for (int i = 0; i < L::VW; i += 4) sts_v4(vrow + 4u * i, v[i], v[i + 1], v[i + 2], v[i + 3]);
-        __syncwarp();
-        const int kk = lane & 3, ii = lane >> 2;
-#pragma unroll
-        for (int g = 0; g < 8; ++g) {
-          const unsigned src = vbase + (unsigned)((4 * g + kk) * L::VS + ii) * 4u;
-          double(&cs)[3][2] = c[g & 1];
-          if (SHAPE == DICEGPU_QUADRATIC_SF) {
-            const double a0 = (double)lds_f(src), a1 = (double)lds_f(src + 32u);
-            dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
-            dmma_8x8x4(cs[1][0], cs[1][1], a0, a1);
-            dmma_8x8x4(cs[2][0], cs[2][1], a1, a1);
-          } else {
-            const double a0 = (double)lds_f(src);
-            dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
-          }
-        }
-        __syncwarp();
-      }
-    }
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      c[0][b][0] += c[1][b][0];
-      c[0][b][1] += c[1][b][1];
-    }
-    o.n = warp_sum_i(n);
-    o.sumF = MOMENTS ? warp_sum(sFd) : warp_sum((double)sumF);
-    if (MOMENTS) {
-      o.sG = warp_sum(sG); o.sG2 = warp_sum(sG2); o.sF2 = warp_sum(sF2); o.sGF = warp_sum(sGF);
-    } else {
-      o.sG = o.sG2 = o.sF2 = o.sGF = 0.0;
-    }
-    if (GRADS) {
-      o.sgx2 = warp_sum((double)sgx2); o.sgy2 = warp_sum((double)sgy2);
-      o.minx = warp_min_i(minx); o.maxx = warp_max_i(maxx);
-      o.miny = warp_min_i(miny); o.maxy = warp_max_i(maxy);
-    } else {
-      o.sgx2 = o.sgy2 = 0.0;
-      o.minx = o.maxx = sb.cx; o.miny = o.maxy = sb.cy;
-    }
-    if (ACC_H) {
-      // scatter the accumulator fragments into the dense symmetric matrix
-      __syncwarp();
-      const int r = lane >> 2, cc = 2 * (lane & 3);
-      constexpr int VW = L::VW;
-      const double(&cf)[3][2] = c[0];
-      if (SHAPE == DICEGPU_QUADRATIC_SF) {
-        C[r * VW + cc] = cf[0][0];           C[r * VW + cc + 1] = cf[0][1];
-        C[r * VW + 8 + cc] = cf[1][0];       C[r * VW + 8 + cc + 1] = cf[1][1];
-        C[(8 + cc) * VW + r] = cf[1][0];     C[(8 + cc + 1) * VW + r] = cf[1][1];
-        C[(8 + r) * VW + 8 + cc] = cf[2][0]; C[(8 + r) * VW + 8 + cc + 1] = cf[2][1];
-      } else {
-        C[r * VW + cc] = cf[0][0];
-        C[r * VW + cc + 1] = cf[0][1];
-      }
-      __syncwarp();
-    }
-    return o;
+    make_mapconst<SHAPE>(slots, !DEFGRAD, (float)sb.cx, (float)sb.cy, k);
+    return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS>(in, k);
   }
 
   // Objective::gamma from the moments (Subset::gamma, DICe_Subset.cpp:323-340):

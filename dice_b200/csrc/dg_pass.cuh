@@ -1,0 +1,232 @@
+// dg_pass.cuh -- one warp-wide pass over the pixels of a subset.
+//
+// The hot loop of the path: Subset::initialize on the deformed image
+// (DICe_Subset.cpp:390-426) fused with the Gauss-Newton accumulation of
+// Objective_ZNSSD::computeUpdateFast (DICe_Objective.cpp:523-546) or with the
+// intensity moments of Subset::gamma (DICe_Subset.cpp:323-340).  It is a
+// separate non-inlined function taking everything it reads by value, so its
+// register allocation does not compete with the per-subset control code.
+#pragma once
+
+#include "dg_device.cuh"
+
+namespace dg {
+
+template <int SHAPE>
+struct Layout {
+  static constexpr int NS = SHAPE == DICEGPU_QUADRATIC_SF ? 12 : 6;   // parameter slots
+  static constexpr int VW = SHAPE == DICEGPU_QUADRATIC_SF ? 16 : 8;   // [r, d, 1] padded
+  static constexpr int VS = SHAPE == DICEGPU_QUADRATIC_SF ? 24 : 8;   // smem row stride (conflict-free)
+  static constexpr int ID = NS;        // column of d = G - F
+  static constexpr int IONE = NS + 1;  // column of 1
+  static constexpr int NMAX = NS;
+};
+
+template <int SHAPE>
+struct __align__(16) WarpSmem {
+  float vbuf[32 * Layout<SHAPE>::VS];
+  double M[Layout<SHAPE>::VW * Layout<SHAPE>::VW];
+};
+
+// Dynamic shared memory of the frame kernel: one WarpSmem per warp.  Taken
+// from the extern array in every user so the compiler keeps shared-space
+// (not generic) addressing.
+extern __shared__ __align__(16) unsigned char dg_smem[];
+
+template <int SHAPE>
+__device__ __forceinline__ WarpSmem<SHAPE>* warp_smem() {
+  return reinterpret_cast<WarpSmem<SHAPE>*>(dg_smem) + (threadIdx.x >> 5);
+}
+
+__device__ __forceinline__ void sts_v4(unsigned addr, float a, float b, float c, float d) {
+  asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+               : "memory");
+}
+__device__ __forceinline__ float lds_f(unsigned addr) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];\n" : "=f"(v) : "r"(addr) : "memory");
+  return v;
+}
+
+// Result of one pass over the subset pixels.
+struct PassOut {
+  int n;                    // active pixels
+  double sumF;              // sum of F over active pixels (shifted by K)
+  double sG, sG2, sF2, sGF; // shifted moments (gamma passes)
+  double sgx2, sgy2;        // sum of unrotated gradient^2 (sigma)
+  int minx, maxx, miny, maxy;
+};
+
+// Everything a pass reads, passed by value.
+struct PassIn {
+  DevImage def;
+  const float* __restrict__ refI;
+  const float* __restrict__ refgx;
+  const float* __restrict__ refgy;
+  int refw;
+  long reflim;
+  const int32_t* __restrict__ px;
+  const int32_t* __restrict__ py;
+  int half;        // square half-width (lists: unused)
+  int cx, cy, npix, off;
+  float K;         // intensity shift for the moment sums
+};
+
+//   ACC_H   : accumulate sum v v^T into the warp's smem matrix (Gauss-Newton)
+//   GRADS   : interpolate the deformed gradients (DEFGRAD) / read reference ones
+//   MOMENTS : FP64 intensity moments for gamma
+template <int SHAPE, int INTERP, bool DEFGRAD, bool ACC_H, bool GRADS, bool MOMENTS>
+__device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
+  using L = Layout<SHAPE>;
+  const int lane = threadIdx.x & 31;
+  const bool use_ref_grads = !DEFGRAD;
+  const float fcx = (float)in.cx, fcy = (float)in.cy;
+  const int W = in.def.w, H = in.def.h;
+  PassOut o;
+  int n = 0;
+  // per-lane partial sums: FP32 over this lane's pixels (the reference sums
+  // these in FP32 over the whole subset), FP64 across the warp; the gamma
+  // moments are FP64 throughout
+  float sumF = 0.0f, sgx2 = 0.0f, sgy2 = 0.0f;
+  double sG = 0.0, sG2 = 0.0, sF2 = 0.0, sGF = 0.0, sFd = 0.0;
+  int minx = in.cx, maxx = in.cx, miny = in.cy, maxy = in.cy;
+  // two independent accumulator sets (even / odd pixel groups) so that
+  // consecutive mma instructions do not wait on each other
+  double c[2][3][2];
+#pragma unroll
+  for (int s2 = 0; s2 < 2; ++s2)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) { c[s2][b][0] = 0.0; c[s2][b][1] = 0.0; }
+  // square subsets: (row, col) of this lane's pixel advanced by 32 per step
+  const int side = 2 * in.half + 1;
+  int row = 0, col = 0, drow = 0, dcol = 0;
+  if (in.off < 0) {
+    row = lane / side; col = lane - row * side;
+    drow = 32 / side; dcol = 32 - drow * side;
+  }
+  const int x0 = in.cx - in.half, y0 = in.cy - in.half;
+  const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_smem<SHAPE>()->vbuf);
+  for (int base = 0; base < in.npix; base += 32) {
+    const int p = base + lane;
+    float v[L::VW];
+#pragma unroll
+    for (int i = 0; i < L::VW; ++i) v[i] = 0.0f;
+    int x = 0, y = 0;
+    if (in.off < 0) {
+      x = max(x0 + col, 0);   // Subset ctors clamp negative coordinates (DICe_Subset.cpp:66-68, :100-101)
+      y = max(y0 + row, 0);
+      col += dcol; row += drow;
+      if (col >= side) { col -= side; ++row; }
+    } else if (p < in.npix) {
+      x = max(__ldg(in.px + in.off + p), 0);
+      y = max(__ldg(in.py + in.off + p), 0);
+    }
+    if (p < in.npix) {
+      float mx, my, Dx, Dy;
+      const float dxf = __fsub_rn((float)x, fcx), dyf = __fsub_rn((float)y, fcy);
+      map_offset<SHAPE>(k, dxf, dyf, fcx, fcy, mx, my, Dx, Dy);
+      const int px = round_pixel(mx), py = round_pixel(my);
+      // 4-pixel border deactivation (DICe_Subset.cpp:408)
+      if (!(px < 4 || px >= W - 4 || py < 4 || py >= H - 4)) {
+        float G, gx = 0.0f, gy = 0.0f;
+        if (GRADS && DEFGRAD) interp_interior<INTERP, true>(in.def, mx, my, G, gx, gy);
+        else interp_interior<INTERP, false>(in.def, mx, my, G, gx, gy);
+        // the reference reads intensities_[y*w+x] unchecked (row-major wrap);
+        // same element inside the array, 0 outside it
+        const long ri = (long)y * in.refw + x;
+        const bool rin = ri < in.reflim;
+        const float F = rin ? __ldg(in.refI + ri) : 0.0f;
+        if (GRADS && !DEFGRAD) {
+          gx = rin ? __ldg(in.refgx + ri) : 0.0f;
+          gy = rin ? __ldg(in.refgy + ri) : 0.0f;
+        }
+        ++n;
+        const float Fs = F - in.K, Gs = G - in.K;
+        if (MOMENTS) {
+          sFd += (double)Fs;
+          sG += (double)Gs;
+          sG2 = fma((double)Gs, (double)Gs, sG2);
+          sF2 = fma((double)Fs, (double)Fs, sF2);
+          sGF = fma((double)Gs, (double)Fs, sGF);
+        } else {
+          sumF += Fs;
+        }
+        if (GRADS) {
+          sgx2 = fmaf(gx, gx, sgx2);
+          sgy2 = fmaf(gy, gy, sgy2);
+          minx = min(minx, x); maxx = max(maxx, x);
+          miny = min(miny, y); maxy = max(maxy, y);
+        }
+        if (ACC_H) {
+          residuals_D<SHAPE>(k, dxf, dyf, Dx, Dy, gx, gy, use_ref_grads, v);
+          v[L::ID] = G - F;
+          v[L::IONE] = 1.0f;
+        }
+      }
+    }
+    if (ACC_H) {
+      // stage the 32 pixel vectors, then 8 groups of 4 pixels through the FP64 mma
+      const unsigned vrow = vbase + (unsigned)(lane * L::VS) * 4u;
+#pragma unroll
+      for (int i = 0; i < L::VW; i += 4) sts_v4(vrow + 4u * i, v[i], v[i + 1], v[i + 2], v[i + 3]);
+      __syncwarp();
+      const int kk = lane & 3, ii = lane >> 2;
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {
+        const unsigned src = vbase + (unsigned)((4 * g + kk) * L::VS + ii) * 4u;
+        double(&cs)[3][2] = c[g & 1];
+        if (SHAPE == DICEGPU_QUADRATIC_SF) {
+          const double a0 = (double)lds_f(src), a1 = (double)lds_f(src + 32u);
+          dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
+          dmma_8x8x4(cs[1][0], cs[1][1], a0, a1);
+          dmma_8x8x4(cs[2][0], cs[2][1], a1, a1);
+        } else {
+          const double a0 = (double)lds_f(src);
+          dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
+        }
+      }
+      __syncwarp();
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    c[0][b][0] += c[1][b][0];
+    c[0][b][1] += c[1][b][1];
+  }
+  o.n = warp_sum_i(n);
+  o.sumF = MOMENTS ? warp_sum(sFd) : warp_sum((double)sumF);
+  if (MOMENTS) {
+    o.sG = warp_sum(sG); o.sG2 = warp_sum(sG2); o.sF2 = warp_sum(sF2); o.sGF = warp_sum(sGF);
+  } else {
+    o.sG = o.sG2 = o.sF2 = o.sGF = 0.0;
+  }
+  if (GRADS) {
+    o.sgx2 = warp_sum((double)sgx2); o.sgy2 = warp_sum((double)sgy2);
+    o.minx = warp_min_i(minx); o.maxx = warp_max_i(maxx);
+    o.miny = warp_min_i(miny); o.maxy = warp_max_i(maxy);
+  } else {
+    o.sgx2 = o.sgy2 = 0.0;
+    o.minx = o.maxx = in.cx; o.miny = o.maxy = in.cy;
+  }
+  if (ACC_H) {
+    // scatter the accumulator fragments into the warp's dense symmetric matrix
+    double* C = warp_smem<SHAPE>()->M;
+    __syncwarp();
+    const int r = lane >> 2, cc = 2 * (lane & 3);
+    constexpr int VW = L::VW;
+    const double(&cf)[3][2] = c[0];
+    if (SHAPE == DICEGPU_QUADRATIC_SF) {
+      C[r * VW + cc] = cf[0][0];           C[r * VW + cc + 1] = cf[0][1];
+      C[r * VW + 8 + cc] = cf[1][0];       C[r * VW + 8 + cc + 1] = cf[1][1];
+      C[(8 + cc) * VW + r] = cf[1][0];     C[(8 + cc + 1) * VW + r] = cf[1][1];
+      C[(8 + r) * VW + 8 + cc] = cf[2][0]; C[(8 + r) * VW + 8 + cc + 1] = cf[2][1];
+    } else {
+      C[r * VW + cc] = cf[0][0];
+      C[r * VW + cc + 1] = cf[0][1];
+    }
+    __syncwarp();
+  }
+  return o;
+}
+
+}  // namespace dg
