@@ -166,6 +166,8 @@ def _declare(lib):
                                         c_void_p, c_int]),
         "dicegpu_image_gradients": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_int,
                                             c_void_p]),
+        "dicegpu_image_gradients_noalloc": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_int,
+                                                    c_void_p]),
         "dicegpu_gamma": (c_int, [c_void_p, c_void_p, c_void_p]),
         "dicegpu_device_status": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_int32)]),
         "dicegpu_version": (ctypes.c_char_p, []),

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <mutex>
 #include <vector>
 
 #include "dg_engine.cuh"
@@ -752,6 +753,57 @@ extern "C" int dicegpu_image_gradients(int w, int h, const float* d_img, float* 
     cudaFree(tmp);
   }
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Gradients without any device allocation.
+//
+// For callers that cannot allocate device memory themselves: hosts that give
+// the library a fixed device-memory budget owned by their own pool, or
+// per-frame loops that cannot afford cudaMalloc / cudaFree (cudaFree waits
+// for the whole device).  The two intermediate finite-difference planes that
+// dicegpu_image_gradients allocates for the 5-point smoothing live instead in
+// the file-scope array below, which every GPU that loads this library holds
+// until the process exits (8 MiB).
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) float g_noalloc_scratch[2 * DICEGPU_NOALLOC_MAX_PIXELS];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (the host-side symbol is only a stand-in for it).
+int noalloc_scratch(float** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DICEGPU_ERR_CUDA;
+  if (dev < 0 || dev >= kMaxDevices) return DICEGPU_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return DICEGPU_ERR_CUDA;
+    g_noalloc_ptr[dev] = static_cast<float*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return DICEGPU_OK;
+}
+}  // namespace
+
+extern "C" int dicegpu_image_gradients_noalloc(int w, int h, const float* d_img, float* d_gx,
+                                               float* d_gy, int method, void* stream) {
+  if (!d_img || !d_gx || !d_gy || w < 3 || h < 3) return DICEGPU_ERR_ARG;
+  if (method != DICEGPU_FINITE_DIFFERENCE && method != DICEGPU_CONVOLUTION_5_POINT)
+    return DICEGPU_ERR_ARG;
+  if ((long long)w * h > DICEGPU_NOALLOC_MAX_PIXELS) return DICEGPU_ERR_ARG;
+  float* tmp = nullptr;
+  if (method == DICEGPU_CONVOLUTION_5_POINT) {
+    const int rc = noalloc_scratch(&tmp);
+    if (rc) return rc;
+  }
+  // the finite-difference kernel writes every scratch element the smoothing
+  // kernel reads, so nothing needs clearing between calls
+  return launch_gradients(w, h, d_img, d_gx, d_gy, method, tmp, (cudaStream_t)stream, nullptr);
 }
 
 // dice_correlate's stride-9 interface (DICe_api.cpp:51-151) over a context

@@ -247,6 +247,23 @@ int dicegpu_interpolate(dicegpu_ctx* ctx, int method, int n, const float* xy,
 int dicegpu_image_gradients(int w, int h, const float* d_img, float* d_gx, float* d_gy,
                             int method, void* stream);
 
+/* The same gradients as dicegpu_image_gradients, computed without allocating
+ * any device memory.  No counterpart in the reference: it exists for callers
+ * that cannot call cudaMalloc -- hosts that own all device memory through
+ * their own pool or budget, and per-frame loops that cannot afford the
+ * device-wide wait of cudaFree.  The smoothing step's two intermediate
+ * planes live in a file-scope device array of 2 * DICEGPU_NOALLOC_MAX_PIXELS
+ * floats (8 MiB) that every GPU loading the library holds until exit.
+ * Images larger than DICEGPU_NOALLOC_MAX_PIXELS pixels are rejected with
+ * DICEGPU_ERR_ARG.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and caches it; make that first call before
+ * any stream capture.  All calls share the one array: calls whose GPU work
+ * overlaps (other streams, other host threads) race on it and must be
+ * serialised by the caller.  Both image pointers are device memory. */
+#define DICEGPU_NOALLOC_MAX_PIXELS (1024 * 1024)
+int dicegpu_image_gradients_noalloc(int w, int h, const float* d_img, float* d_gx, float* d_gy,
+                                    int method, void* stream);
+
 /* Objective::gamma for every subset at the parameters in `fields` (host,
  * n * stride): writes gamma per subset to gamma_out (host). */
 int dicegpu_gamma(dicegpu_ctx* ctx, const double* fields, double* gamma_out);
