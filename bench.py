@@ -84,7 +84,7 @@ class ClockSampler:
         try:
             self._proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self._proc = None
             return
@@ -172,12 +172,16 @@ def run_reference(args):
         return
     import torch
     from dice_b200 import synthetic as syn
-    ref, frames = syn.config2(device="cpu", nframes=NFRAMES)
+    ref, frames = syn.config2(device="cpu", nframes=NFRAMES, count=1)
     ref = ref.numpy()
     frames = [fr.numpy() for fr in frames]
     p = params()
     cores = os.cpu_count() or 1
-    n_sample = max(256, min(158404, int(args.cpu_sample)))
+    # each step a bounded sample sized for ~3 s of work on all cores
+    n_sample = int(args.cpu_sample) if args.cpu_sample > 0 else 0
+    if n_sample <= 0:
+        v0, _, _ = cpu_sample(p, ref, frames, 2000, cores)
+        n_sample = int(min(158404, max(2000, 3.0 * v0)))
     for _ in range(args.warmup):
         cpu_sample(p, ref, frames, min(n_sample, 512), cores)
     vals = []
@@ -209,7 +213,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dicegpu", choices=["dicegpu", "reference"])
-    ap.add_argument("--cpu-sample", type=int, default=1200)
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="subsets in the CPU sample (0: sized for ~15 s of CPU work)")
     ap.add_argument("--plain-sample", type=int, default=4000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--warps", type=int, default=0)
@@ -342,9 +347,14 @@ def main():
         ref_h = ref.cpu().numpy()
         fr_h = [fr.cpu().numpy() for fr in frames[:1]]
         cores = os.cpu_count() or 1
-        v, dt, _ = cpu_sample(p, ref_h, fr_h, args.cpu_sample, cores)
+        n_cpu = args.cpu_sample
+        if n_cpu <= 0:
+            # calibrate on a small sample, then size the timed one for ~15 s
+            v0, _, _ = cpu_sample(p, ref_h, fr_h, 2000, cores)
+            n_cpu = int(min(n, max(2000, 15.0 * v0)))
+        v, dt, _ = cpu_sample(p, ref_h, fr_h, n_cpu, cores)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": "first %d subsets of frame 1 (of %d), %d threads, %.1f s" % (args.cpu_sample, n, cores, dt)}
+               "sample": "first %d subsets of frame 1 (of %d), %d threads, %.1f s" % (n_cpu, n, cores, dt)}
 
     peaks = {}
     try:

@@ -167,10 +167,12 @@ def config2_field(k, nframes=10):
     return f
 
 
-def config2(device="cpu", w=2048, h=2048, nframes=10):
-    """2048^2 16-bit-range speckle image (radius 3-5) and `nframes` deformed frames."""
+def config2(device="cpu", w=2048, h=2048, nframes=10, count=None):
+    """2048^2 16-bit-range speckle image (radius 3-5) and the first `count`
+    (default all `nframes`) deformed frames of the sequence."""
     ref = speckle_image(w, h, seed=2, r_min=3, r_max=5, grey_lo=1000.0, grey_hi=64000.0,
                         blur_sigma=0.8, device=device)
+    count = nframes if count is None else count
     frames = [warp_image(ref, config2_field(k + 1, nframes), noise_sigma=50.0, seed=200 + k,
-                         clip=(0.0, 65535.0)) for k in range(nframes)]
+                         clip=(0.0, 65535.0)) for k in range(count)]
     return ref, frames
