@@ -33,10 +33,119 @@ struct FrameArgs {
   int mode;
   int plain_index;       // >= 0: this launch processes only that subset (plain path)
   double* gamma_out;     // MODE_GAMMA output
-  int* work_counter;     // persistent work queue head
+  int* work_counter;     // queue heads: one (queue_mode 0) or one per CTA (1)
+  int queue_mode;
   int* status;           // device error word
   int32_t* passes_out;   // optional: pixel passes executed per subset (GN + simplex + epilogue)
 };
+
+struct AffineStep {
+  float upd[6];   // parameter update per slot (0 for disabled slots)
+  float cond;     // 2x2 condition number of the displacement block
+};
+
+// Gauss-Newton step of the affine system, computed by every lane on its own
+// copy (no shuffles, all in registers).  `M` is the accumulated 8x8 matrix of
+// [r(6 slots), G-F, 1]; `em` the mask of enabled slots.  Mirrors
+// DICe_Objective.cpp:548-607: LM penalty, the 2x2 condition number in the
+// reference's float/double mix, LU with partial pivoting in DGETRF order
+// (first maximal pivot, reciprocal scaling, rank-1 updates), then
+// update = -H^-1 q, or -LU q when a pivot is exactly zero (DGETRI returns
+// early and the factors are used as the inverse).
+__device__ __noinline__ AffineStep solve_affine(const double* __restrict__ M, double cshift,
+                                                unsigned em, float lm_alpha) {
+  double H[6][6], q[6], q0[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const bool ei = (em >> i) & 1u;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const bool ej = (em >> j) & 1u;
+      H[i][j] = (ei && ej) ? M[i * 8 + j] : (i == j ? 1.0 : 0.0);
+    }
+    q[i] = ei ? M[i * 8 + 6] - cshift * M[i * 8 + 7] : 0.0;
+    q0[i] = q[i];
+  }
+  if (lm_alpha > 0.0f) {
+    H[0][0] += (double)lm_alpha;
+    H[1][1] += (double)lm_alpha;
+  }
+  AffineStep out;
+  {
+    const double nsq = H[0][0] * H[0][0] + H[0][1] * H[0][1] + H[1][0] * H[1][0] + H[1][1] * H[1][1];
+    const float det_h = (float)(H[0][0] * H[1][1] - H[1][0] * H[0][1]);
+    const float norm_H = (float)sqrt(nsq);
+    float cond = -1.0f;
+    if (det_h != 0.0f) {
+      const float dd = __fmul_rn(det_h, det_h);
+      cond = norm_H * (float)sqrt((1.0 / (double)dd) * nsq);
+    }
+    out.cond = cond;
+  }
+  int info = 0;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    int p = j;
+    double best = fabs(H[j][j]);
+#pragma unroll
+    for (int i = j + 1; i < 6; ++i) {
+      const double a = fabs(H[i][j]);
+      if (a > best) { best = a; p = i; }
+    }
+    double pv = H[j][j];
+#pragma unroll
+    for (int i = j + 1; i < 6; ++i)
+      if (i == p) pv = H[i][j];
+    if (pv != 0.0) {
+#pragma unroll
+      for (int i = j + 1; i < 6; ++i) {
+        if (i == p) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            const double t = H[j][k];
+            H[j][k] = H[i][k];
+            H[i][k] = t;
+          }
+          const double t = q[j];
+          q[j] = q[i];
+          q[i] = t;
+        }
+      }
+      const double r = 1.0 / pv;
+#pragma unroll
+      for (int i = j + 1; i < 6; ++i) H[i][j] *= r;
+    } else if (info == 0) {
+      info = j + 1;
+    }
+#pragma unroll
+    for (int i = j + 1; i < 6; ++i) {
+#pragma unroll
+      for (int k = j + 1; k < 6; ++k) H[i][k] -= H[i][j] * H[j][k];
+      q[i] -= H[i][j] * q[j];
+    }
+  }
+  if (info == 0) {
+    double x[6];
+#pragma unroll
+    for (int j = 5; j >= 0; --j) {
+      double s = q[j];
+#pragma unroll
+      for (int k = j + 1; k < 6; ++k) s -= H[j][k] * x[k];
+      x[j] = s / H[j][j];
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) out.upd[i] = (float)(-x[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      float u = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) u = (float)((double)u + H[i][j] * (-1.0) * q0[j]);
+      out.upd[i] = u;
+    }
+  }
+  return out;
+}
 
 struct SubsetRef {
   int idx, cx, cy, npix;
@@ -118,11 +227,20 @@ struct Engine {
     for (int k = 0; k < A.P.N; ++k) slots[A.P.slot[k]] = comp[k];
   }
 
+  __device__ __forceinline__ unsigned enabled_mask() const {
+    unsigned em = 0;
+    for (int k = 0; k < A.P.N; ++k) em |= 1u << A.P.slot[k];
+    return em;
+  }
+
   // --------------------------------------------------------------------------
   // Gauss-Newton (Objective_ZNSSD::computeUpdateFast).  `slots` in/out.
   // `meanF` is the reference mean at entry (Subset::mean(REF_INTENSITIES)).
   // --------------------------------------------------------------------------
-  __device__ int gauss_newton(const SubsetRef& sb, float* slots, float meanF, int& num_iterations,
+  // meanF < 0 is never a valid "not given" marker for intensities, so the
+  // all-pixel mean of a fresh subset is requested with `meanF_from_pass`.
+  __device__ int gauss_newton(const SubsetRef& sb, float* slots, float meanF, bool meanF_from_pass,
+                              int& num_iterations,
                               float& cond_out, PassOut& last) {
     const DevParams& P = A.P;
     const int N = P.N;
@@ -133,13 +251,49 @@ struct Engine {
     int solve_it = 0;
     for (; solve_it <= P.max_fast; ++solve_it) {
       num_iterations = solve_it;
+      DG_PT(t_pass);
       last = pass<true, true, false>(sb, slots, M);
+      DG_PACC(1, t_pass);
       if (A.passes_out && lane == 0) A.passes_out[sb.idx] += 1;
       const int n = last.n;
       // Subset::mean(DEF_INTENSITIES): sum G / n over the active pixels
       const double sumG = M[L::ID * L::VW + L::IONE] + last.sumF + (double)n * (double)sb.K;
       const float meanG = n ? (float)(sumG / (double)n) : 0.0f;
+      if (meanF_from_pass && solve_it == 0) {
+        // Subset::mean(REF_INTENSITIES) at entry: every pixel of a fresh subset
+        meanF = sb.npix ? (float)((last.sumFall + (double)sb.npix * (double)sb.K) / (double)sb.npix)
+                        : 0.0f;
+      }
       const double cshift = (double)meanG - (double)meanF;
+      if constexpr (SHAPE == DICEGPU_AFFINE_SF) {
+        // Every lane solves the whole (padded) 6x6 system in registers: the
+        // slots of disabled parameters get identity rows / columns and q = 0,
+        // which leaves the LU of the enabled block (same pivots, same
+        // operations) unchanged and gives them a zero update.
+        const AffineStep stp = solve_affine(M, cshift, enabled_mask(), P.lm_alpha);
+        const float* upd_s = stp.upd;
+        cond_out = stp.cond;
+        if (stp.cond > 1.0e12f) return DICEGPU_HESSIAN_SINGULAR;
+        float old[12];
+#pragma unroll
+        for (int i = 0; i < 12; ++i) old[i] = slots[i];
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+          float u = upd_s[s];
+          if (P.momentum != 0.0f) {
+            u += P.momentum * upd_old[s];
+            upd_old[s] = u;
+          }
+          slots[s] += u;   // disabled slots: u == 0
+        }
+        const float tol = P.fast_tol;
+        bool conv = true;
+        if (fabsf(slots[0] - old[0]) >= tol) conv = false;
+        if (fabsf(slots[1] - old[1]) >= tol) conv = false;
+        if (P.has_rot && fabsf(slots[2] - old[2]) >= tol) conv = false;
+        if (conv) break;
+        continue;
+      }
       // lane i owns row i of [H | q] in the reference's compact order
       double h[L::NMAX];
       double qv = 0.0;
@@ -414,23 +568,35 @@ struct Engine {
     const int rw = max_x - min_x, rh = max_y - min_y;
     double acc = 0.0;
     if (rw > 0 && rh > 0) {
-      const long total = (long)rw * rh;
+      // a lane per column, a sliding 3-row window down the rows; reads go
+      // through the row-major linear index like the reference's operator()
+      // (0 outside the array), so edge pixels need no special window
       const long lim = (long)img_w * img_h;
-      for (long e = lane; e < total; e += 32) {
-        const int yy = min_y + (int)(e / rw), xx = min_x + (int)(e % rw);
-        if (xx < 1 || xx >= img_w - 1 || yy < 1 || yy >= img_h - 1) {
-          const long li = (long)yy * img_w + xx;
-          const float a = (li >= 0 && li < lim) ? __ldg(A.def.I + li) : 0.0f;
-          acc += (double)fabsf(a);
-        } else {
-          const float* q = A.def.I + (size_t)(yy - 1) * img_w + (xx - 1);
-          float conv = 0.0f;
-          conv += __ldg(q) * 1.0f;  conv += __ldg(q + 1) * -2.0f;  conv += __ldg(q + 2) * 1.0f;
-          q += img_w;
-          conv += __ldg(q) * -2.0f; conv += __ldg(q + 1) * 4.0f;   conv += __ldg(q + 2) * -2.0f;
-          q += img_w;
-          conv += __ldg(q) * 1.0f;  conv += __ldg(q + 1) * -2.0f;  conv += __ldg(q + 2) * 1.0f;
-          acc += (double)fabsf(conv);
+      const float* I = A.def.I;
+      auto ld = [&](int x, int y) -> float {
+        const long li = (long)y * img_w + x;
+        return (li >= 0 && li < lim) ? __ldg(I + li) : 0.0f;
+      };
+      for (int xb = min_x; xb < max_x; xb += 32) {
+        const int xx = xb + lane;
+        if (xx >= max_x) continue;
+        float a0 = ld(xx - 1, min_y - 1), a1 = ld(xx, min_y - 1), a2 = ld(xx + 1, min_y - 1);
+        float b0 = ld(xx - 1, min_y), b1 = ld(xx, min_y), b2 = ld(xx + 1, min_y);
+        const bool xedge = xx < 1 || xx >= img_w - 1;
+        for (int yy = min_y; yy < max_y; ++yy) {
+          const float c0 = ld(xx - 1, yy + 1), c1 = ld(xx, yy + 1), c2 = ld(xx + 1, yy + 1);
+          if (xedge || yy < 1 || yy >= img_h - 1) {
+            acc += (double)fabsf(b1);
+          } else {
+            // mask[i][j] (i: x offset, j: y offset), j outer, i inner
+            float conv = 0.0f;
+            conv += a0 * 1.0f;  conv += a1 * -2.0f; conv += a2 * 1.0f;
+            conv += b0 * -2.0f; conv += b1 * 4.0f;  conv += b2 * -2.0f;
+            conv += c0 * 1.0f;  conv += c1 * -2.0f; conv += c2 * 1.0f;
+            acc += (double)fabsf(conv);
+          }
+          a0 = b0; a1 = b1; a2 = b2;
+          b0 = c0; b1 = c1; b2 = c2;
         }
       }
     }
@@ -448,19 +614,22 @@ struct Engine {
     return sg > 0.0f ? (float)sqrt(2.0 * (double)noise * (double)noise / (double)sg) : -1.0f;
   }
 
-  __device__ void load_slots(const double* f, float* slots) const {
-#pragma unroll
-    for (int i = 0; i < 12; ++i) slots[i] = 0.0f;
+  // initialize_parameters_from_fields from the field row held across the
+  // warp (lane c = column c): affine slots 0..5 are DISP_X, DISP_Y, ROT_Z,
+  // STRETCH_XX, STRETCH_YY, SHEAR_XY (disabled slots 0); quadratic QUAD_A..L
+  __device__ void load_slots_row(double fv, float* slots) const {
     if (SHAPE == DICEGPU_QUADRATIC_SF) {
 #pragma unroll
-      for (int i = 0; i < 12; ++i) slots[i] = (float)f[DICEGPU_F_QUAD_A + i];
+      for (int i = 0; i < 12; ++i) slots[i] = (float)__shfl_sync(FULL, fv, DICEGPU_F_QUAD_A + i);
     } else {
-      slots[0] = (float)f[DICEGPU_F_DISP_X];
-      slots[1] = (float)f[DICEGPU_F_DISP_Y];
-      for (int kx = 2; kx < A.P.N; ++kx) {
-        const int s = A.P.slot[kx];
-        slots[s] = (float)f[DICEGPU_F_DISP_X + s];   // slots 2..5 = ROT_Z..SHEAR_XY
+      const unsigned em = enabled_mask();
+#pragma unroll
+      for (int s = 0; s < 6; ++s) {
+        const float v = (float)__shfl_sync(FULL, fv, DICEGPU_F_DISP_X + s);
+        slots[s] = ((em >> s) & 1u) ? v : 0.0f;
       }
+#pragma unroll
+      for (int s = 6; s < 12; ++s) slots[s] = 0.0f;
     }
   }
 
@@ -542,10 +711,14 @@ struct Engine {
   __device__ void run(int idx) {
     const DevParams& P = A.P;
     double* f = A.fields + (size_t)idx * DICEGPU_FIELD_STRIDE;
+    // the subset's field row (32 doubles) in one coalesced load: lane c holds
+    // column c, read by shuffles
+    const double fv = f[lane];
+    auto fld = [&](int col) { return __shfl_sync(FULL, fv, col); };
     SubsetRef sb;
     sb.idx = idx;
-    sb.cx = (int)f[DICEGPU_F_COORD_X];
-    sb.cy = (int)f[DICEGPU_F_COORD_Y];
+    sb.cx = (int)fld(DICEGPU_F_COORD_X);
+    sb.cy = (int)fld(DICEGPU_F_COORD_Y);
     if (A.geo.half >= 0) {
       const int side = 2 * A.geo.half + 1;
       sb.npix = side * side;
@@ -560,7 +733,7 @@ struct Engine {
     }
     float slots[12];
     if (A.mode == MODE_GAMMA) {
-      load_slots(f, slots);
+      load_slots_row(fv, slots);
       const float g = eval_gamma(sb, slots);
       if (lane == 0) A.gamma_out[idx] = g;
       return;
@@ -568,8 +741,8 @@ struct Engine {
     if (A.passes_out && lane == 0) A.passes_out[idx] = 0;
     // frame-0 field-of-view test (DICe_Schema.cpp:2036-2048)
     if (A.geo.half >= 0 && A.first_frame) {
-      const float cur_x = (float)(f[DICEGPU_F_COORD_X] + f[DICEGPU_F_DISP_X]);
-      const float cur_y = (float)(f[DICEGPU_F_COORD_Y] + f[DICEGPU_F_DISP_Y]);
+      const float cur_x = (float)(fld(DICEGPU_F_COORD_X) + fld(DICEGPU_F_DISP_X));
+      const float cur_y = (float)(fld(DICEGPU_F_COORD_Y) + fld(DICEGPU_F_DISP_Y));
       const int hs = P.subset_size / 2;
       if (cur_x < hs || cur_x > A.def.w - hs || cur_y < hs || cur_y > A.def.h - hs) {
         record_failed(f, DICEGPU_INITIALIZE_FAILED_BY_EXCEPTION, -1);
@@ -578,11 +751,11 @@ struct Engine {
     }
     int num_iterations = -1;
     // Field_Value_Initializer::initial_guess (DICe_Initializer.cpp:398-436)
-    if (f[DICEGPU_F_SIGMA] == -1.0) {
+    if (fld(DICEGPU_F_SIGMA) == -1.0) {
       record_failed(f, DICEGPU_INITIALIZE_FAILED, num_iterations);
       return;
     }
-    load_slots(f, slots);
+    load_slots_row(fv, slots);
     int init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
     // reference mean at Gauss-Newton entry: over the pixels active at the last
     // deformed-state initialisation (none yet: all of them)
@@ -599,9 +772,9 @@ struct Engine {
         return;
       }
     }
-    const float prev_u = (float)f[DICEGPU_F_DISP_X];
-    const float prev_v = (float)f[DICEGPU_F_DISP_Y];
-    const float prev_t = (float)f[DICEGPU_F_ROT_Z];
+    const float prev_u = (float)fld(DICEGPU_F_DISP_X);
+    const float prev_v = (float)fld(DICEGPU_F_DISP_Y);
+    const float prev_t = (float)fld(DICEGPU_F_ROT_Z);
     const bool force_simplex = A.geo.force_simplex && A.geo.force_simplex[idx];
     const int opt = P.opt;
     int corr_status = DICEGPU_CORRELATION_FAILED;
@@ -609,29 +782,16 @@ struct Engine {
     bool cond_set = false;
     bool state_from_simplex = false;
     (void)state_from_simplex;
-    auto mean_ref = [&]() -> float {
-      if (!have_state) {
-        // all pixels: reuse a moments pass of the reference values
-        double s = 0.0;
-        int cnt = 0;
-        const long lim = (long)A.ref.w * A.ref.h;
-        for (int p = lane; p < sb.npix; p += 32) {
-          int x, y;
-          pixel_xy(sb, p, x, y);
-          const long ri = (long)y * A.ref.w + x;
-          s += ri < lim ? (double)__ldg(A.ref.I + ri) : 0.0;
-          ++cnt;
-        }
-        s = warp_sum(s);
-        cnt = warp_sum_i(cnt);
-        return cnt ? (float)(s / cnt) : 0.0f;
-      }
-      const int n = last_state.n;
-      return n ? (float)((last_state.sumF + (double)n * (double)sb.K) / (double)n) : 0.0f;
-    };
     auto run_gn = [&]() {
-      const float meanF = mean_ref();
-      corr_status = gauss_newton(sb, slots, meanF, num_iterations, cond, last_state);
+      // Subset::mean(REF_INTENSITIES) at entry: over the pixels active at the
+      // last deformed-state initialisation, or all pixels of a fresh subset
+      // (then taken from the first pass)
+      float meanF = 0.0f;
+      if (have_state) {
+        const int n = last_state.n;
+        meanF = n ? (float)((last_state.sumF + (double)n * (double)sb.K) / (double)n) : 0.0f;
+      }
+      corr_status = gauss_newton(sb, slots, meanF, !have_state, num_iterations, cond, last_state);
       have_state = true;
       state_from_simplex = false;
       cond_set = true;
@@ -644,13 +804,15 @@ struct Engine {
       have_state = true;
       state_from_simplex = true;
     };
+    DG_PT(t_first);
     if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED || force_simplex) {
       run_simplex();
     } else {
       run_gn();
     }
+    DG_PACC(2, t_first);
     MapConst kc;
-    const float fcx = (float)f[DICEGPU_F_COORD_X], fcy = (float)f[DICEGPU_F_COORD_Y];
+    const float fcx = (float)fld(DICEGPU_F_COORD_X), fcy = (float)fld(DICEGPU_F_COORD_Y);
     float nu, nv, nt;
     make_mapconst<SHAPE>(slots, false, fcx, fcy, kc);
     map_to_u_v_theta<SHAPE>(kc, fcx, fcy, nu, nv, nt);
@@ -661,12 +823,12 @@ struct Engine {
       if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_GRADIENT_BASED || force_simplex) {
         second_failed = true;
       } else if (opt == DICEGPU_GRADIENT_BASED_THEN_SIMPLEX) {
-        load_slots(f, slots);
+        load_slots_row(fv, slots);
         init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
         run_simplex();
         if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
       } else if (opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED) {
-        load_slots(f, slots);
+        load_slots_row(fv, slots);
         init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
         run_gn();
         if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
@@ -681,13 +843,17 @@ struct Engine {
     // sigma needs the gradients of the last deformed-state initialisation
     const PassOut st = last_state;
     float noise = 0.0f;
+    DG_PT(t_sig);
     const float sg = sigma(sb, st, slots, noise);
+    DG_PACC(3, t_sig);
     if (sg < 0.0f) {
       record_failed(f, DICEGPU_FRAME_FAILED_DUE_TO_NEGATIVE_SIGMA, num_iterations);
       return;
     }
     PassOut fin;
+    DG_PT(t_gam);
     const float gamma = eval_gamma(sb, slots, &fin);
+    DG_PACC(4, t_gam);
     const float bt = P.output_beta ? beta(sb, slots) : 0.0f;
     if ((P.final_gamma_thr != -1.0 && gamma > P.final_gamma_thr) || gamma < 0.0f) {
       record_failed(f, DICEGPU_FRAME_FAILED_DUE_TO_HIGH_GAMMA, num_iterations);

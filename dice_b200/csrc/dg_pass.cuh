@@ -12,6 +12,20 @@
 
 namespace dg {
 
+// Section timers of a profiling build (-DDG_PROFILE): warp cycles per section
+// summed over all warps.  Compiled out otherwise.
+#ifdef DG_PROFILE
+__device__ unsigned long long g_prof[8];
+#define DG_PT(var) const long long var = clock64()
+#define DG_PACC(i, t0)                                                                    \
+  do {                                                                                    \
+    if ((threadIdx.x & 31) == 0) atomicAdd(&g_prof[i], (unsigned long long)(clock64() - (t0))); \
+  } while (0)
+#else
+#define DG_PT(var)
+#define DG_PACC(i, t0)
+#endif
+
 template <int SHAPE>
 struct Layout {
   static constexpr int NS = SHAPE == DICEGPU_QUADRATIC_SF ? 12 : 6;   // parameter slots
@@ -22,9 +36,21 @@ struct Layout {
   static constexpr int NMAX = NS;
 };
 
+// Pixels per lane per step of a pass: each step maps, interpolates and
+// stages 32 * DG_PPL pixels before the mma accumulation, so that the tap
+// loads of DG_PPL independent pixels are in flight together.
+#ifndef DG_PPL
+#define DG_PPL 1
+#endif
+constexpr int PPL = DG_PPL;
+// independent FP64 mma accumulator sets of the affine pass
+#ifndef DG_NSET_AFFINE
+#define DG_NSET_AFFINE 2
+#endif
+
 template <int SHAPE>
 struct __align__(16) WarpSmem {
-  float vbuf[32 * Layout<SHAPE>::VS];
+  float vbuf[32 * PPL * Layout<SHAPE>::VS];
   double M[Layout<SHAPE>::VW * Layout<SHAPE>::VW];
 };
 
@@ -52,6 +78,7 @@ __device__ __forceinline__ float lds_f(unsigned addr) {
 struct PassOut {
   int n;                    // active pixels
   double sumF;              // sum of F over active pixels (shifted by K)
+  double sumFall;           // sum of F over all subset pixels (shifted; Gauss-Newton passes)
   double sG, sG2, sF2, sGF; // shifted moments (gamma passes)
   double sgx2, sgy2;        // sum of unrotated gradient^2 (sigma)
   int minx, maxx, miny, maxy;
@@ -87,14 +114,15 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
   // per-lane partial sums: FP32 over this lane's pixels (the reference sums
   // these in FP32 over the whole subset), FP64 across the warp; the gamma
   // moments are FP64 throughout
-  float sumF = 0.0f, sgx2 = 0.0f, sgy2 = 0.0f;
+  float sumF = 0.0f, sgx2 = 0.0f, sgy2 = 0.0f, sumFall = 0.0f;
   double sG = 0.0, sG2 = 0.0, sF2 = 0.0, sGF = 0.0, sFd = 0.0;
   int minx = in.cx, maxx = in.cx, miny = in.cy, maxy = in.cy;
-  // two independent accumulator sets (even / odd pixel groups) so that
+  // independent accumulator sets (pixel group g goes to set g % NSET) so that
   // consecutive mma instructions do not wait on each other
-  double c[2][3][2];
+  constexpr int NSET = SHAPE == DICEGPU_QUADRATIC_SF ? 2 : DG_NSET_AFFINE;
+  double c[NSET][3][2];
 #pragma unroll
-  for (int s2 = 0; s2 < 2; ++s2)
+  for (int s2 = 0; s2 < NSET; ++s2)
 #pragma unroll
     for (int b = 0; b < 3; ++b) { c[s2][b][0] = 0.0; c[s2][b][1] = 0.0; }
   // square subsets: (row, col) of this lane's pixel advanced by 32 per step
@@ -106,9 +134,12 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
   }
   const int x0 = in.cx - in.half, y0 = in.cy - in.half;
   const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_smem<SHAPE>()->vbuf);
-  for (int base = 0; base < in.npix; base += 32) {
-    const int p = base + lane;
-    float v[L::VW];
+  for (int base = 0; base < in.npix; base += 32 * PPL) {
+    float vv[PPL][L::VW];
+#pragma unroll
+    for (int u = 0; u < PPL; ++u) {
+    float* v = vv[u];
+    const int p = base + 32 * u + lane;
 #pragma unroll
     for (int i = 0; i < L::VW; ++i) v[i] = 0.0f;
     int x = 0, y = 0;
@@ -126,16 +157,17 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
       const float dxf = __fsub_rn((float)x, fcx), dyf = __fsub_rn((float)y, fcy);
       map_offset<SHAPE>(k, dxf, dyf, fcx, fcy, mx, my, Dx, Dy);
       const int px = round_pixel(mx), py = round_pixel(my);
+      // the reference reads intensities_[y*w+x] unchecked (row-major wrap);
+      // same element inside the array, 0 outside it
+      const long ri = (long)y * in.refw + x;
+      const bool rin = ri < in.reflim;
+      const float F = rin ? __ldg(in.refI + ri) : 0.0f;
+      if (ACC_H) sumFall += F - in.K;
       // 4-pixel border deactivation (DICe_Subset.cpp:408)
       if (!(px < 4 || px >= W - 4 || py < 4 || py >= H - 4)) {
         float G, gx = 0.0f, gy = 0.0f;
         if (GRADS && DEFGRAD) interp_interior<INTERP, true>(in.def, mx, my, G, gx, gy);
         else interp_interior<INTERP, false>(in.def, mx, my, G, gx, gy);
-        // the reference reads intensities_[y*w+x] unchecked (row-major wrap);
-        // same element inside the array, 0 outside it
-        const long ri = (long)y * in.refw + x;
-        const bool rin = ri < in.reflim;
-        const float F = rin ? __ldg(in.refI + ri) : 0.0f;
         if (GRADS && !DEFGRAD) {
           gx = rin ? __ldg(in.refgx + ri) : 0.0f;
           gy = rin ? __ldg(in.refgy + ri) : 0.0f;
@@ -164,17 +196,22 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
         }
       }
     }
+    }
     if (ACC_H) {
-      // stage the 32 pixel vectors, then 8 groups of 4 pixels through the FP64 mma
-      const unsigned vrow = vbase + (unsigned)(lane * L::VS) * 4u;
+      // stage the 32 * PPL pixel vectors, then groups of 4 pixels through the FP64 mma
 #pragma unroll
-      for (int i = 0; i < L::VW; i += 4) sts_v4(vrow + 4u * i, v[i], v[i + 1], v[i + 2], v[i + 3]);
+      for (int u = 0; u < PPL; ++u) {
+        const unsigned vrow = vbase + (unsigned)((32 * u + lane) * L::VS) * 4u;
+#pragma unroll
+        for (int i = 0; i < L::VW; i += 4)
+          sts_v4(vrow + 4u * i, vv[u][i], vv[u][i + 1], vv[u][i + 2], vv[u][i + 3]);
+      }
       __syncwarp();
       const int kk = lane & 3, ii = lane >> 2;
 #pragma unroll
-      for (int g = 0; g < 8; ++g) {
+      for (int g = 0; g < 8 * PPL; ++g) {
         const unsigned src = vbase + (unsigned)((4 * g + kk) * L::VS + ii) * 4u;
-        double(&cs)[3][2] = c[g & 1];
+        double(&cs)[3][2] = c[g % NSET];
         if (SHAPE == DICEGPU_QUADRATIC_SF) {
           const double a0 = (double)lds_f(src), a1 = (double)lds_f(src + 32u);
           dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
@@ -189,12 +226,15 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
     }
   }
 #pragma unroll
-  for (int b = 0; b < 3; ++b) {
-    c[0][b][0] += c[1][b][0];
-    c[0][b][1] += c[1][b][1];
-  }
+  for (int s2 = 1; s2 < NSET; ++s2)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      c[0][b][0] += c[s2][b][0];
+      c[0][b][1] += c[s2][b][1];
+    }
   o.n = warp_sum_i(n);
   o.sumF = MOMENTS ? warp_sum(sFd) : warp_sum((double)sumF);
+  o.sumFall = ACC_H ? warp_sum((double)sumFall) : 0.0;
   if (MOMENTS) {
     o.sG = warp_sum(sG); o.sG2 = warp_sum(sG2); o.sF2 = warp_sum(sF2); o.sGF = warp_sum(sGF);
   } else {

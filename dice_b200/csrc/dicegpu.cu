@@ -172,12 +172,38 @@ __global__ void __launch_bounds__(256, DG_MIN_BLOCKS) frame_kernel(const __grid_
     if (blockIdx.x == 0 && threadIdx.x < 32) e.run(a.plain_index);
     return;
   }
-  for (;;) {
+  if (a.queue_mode == 0) {
+    // one global queue head
+    for (;;) {
+      int idx = 0;
+      if (lane == 0) idx = atomicAdd(a.work_counter, 1);
+      idx = __shfl_sync(FULL, idx, 0);
+      if (idx >= a.n) break;
+      e.run(idx);
+    }
+    return;
+  }
+  // Partitioned queues: CTA r owns subsets [r n/G, (r+1) n/G) -- neighbouring
+  // subsets, so its warps share their image footprint in L1 -- and when its
+  // range is exhausted its warps take from the following CTAs' ranges.  Every
+  // index is taken exactly once (atomicAdd); a warp leaves after finding all
+  // G ranges exhausted, so no warp ever waits on another.
+  const int G = gridDim.x;
+  int q = blockIdx.x;
+  for (int visited = 0; visited < G;) {
+    const int qbeg = (int)(((long long)q * a.n) / G);
+    const int qend = (int)(((long long)(q + 1) * a.n) / G);
     int idx = 0;
-    if (lane == 0) idx = atomicAdd(a.work_counter, 1);
+    if (lane == 0) idx = qbeg + atomicAdd(a.work_counter + q, 1);
     idx = __shfl_sync(FULL, idx, 0);
-    if (idx >= a.n) break;
-    e.run(idx);
+    if (idx < qend) {
+      DG_PT(t_run);
+      e.run(idx);
+      DG_PACC(0, t_run);
+      continue;
+    }
+    ++visited;
+    q = (q + 1 == G) ? 0 : q + 1;
   }
 }
 
@@ -185,6 +211,11 @@ typedef void (*FrameKernelFn)(FrameArgs);
 
 template <int SHAPE>
 static FrameKernelFn pick_kernel(int interp, bool defgrad) {
+#ifdef DG_ONLY_BENCH_KERNEL
+  // timing experiments only: the affine / Keys-4 / deformed-gradient kernel
+  (void)interp; (void)defgrad;
+  return frame_kernel<DICEGPU_AFFINE_SF, DICEGPU_KEYS_FOURTH, true>;
+#endif
   if (defgrad) {
     if (interp == DICEGPU_KEYS_FOURTH) return frame_kernel<SHAPE, DICEGPU_KEYS_FOURTH, true>;
     if (interp == DICEGPU_BICUBIC) return frame_kernel<SHAPE, DICEGPU_BICUBIC, true>;
@@ -198,6 +229,9 @@ static FrameKernelFn pick_kernel(int interp, bool defgrad) {
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
+// upper bound on the persistent grid (and on its per-CTA queue heads)
+static const int kMaxQueues = 8192;
+
 struct dicegpu_ctx {
   dicegpu_params params;
   DevParams dp;
@@ -233,6 +267,8 @@ struct dicegpu_ctx {
   int frame_index = 0;
   int warps_per_cta = 4;
   int ctas_per_sm = 0;   // 0: occupancy-derived
+  int queue_mode = 1;    // 1: per-CTA queues with stealing, 0: one global queue
+  int carveout = -1;     // preferred shared-memory carveout (percent), -1: driver default
   long long launches = 0;
 };
 
@@ -341,13 +377,15 @@ extern "C" int dicegpu_create(const dicegpu_params* params, dicegpu_ctx** out) {
   if (rc) { delete c; return rc; }
   if (cudaGetDevice(&c->device) != cudaSuccess ||
       cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
-      cudaMalloc(&c->d_counter, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->d_counter, kMaxQueues * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess ||
       cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
     if (c->d_counter) cudaFree(c->d_counter);
     delete c;
     return DICEGPU_ERR_CUDA;
   }
+  if (const char* qm = getenv("DICEGPU_QUEUE")) c->queue_mode = atoi(qm) ? 1 : 0;
+  if (const char* cv = getenv("DICEGPU_CARVEOUT")) c->carveout = atoi(cv);
   *out = c;
   return DICEGPU_OK;
 }
@@ -581,6 +619,7 @@ static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
   a.mode = mode;
   a.plain_index = -1;
   a.work_counter = c->d_counter;
+  a.queue_mode = c->queue_mode;
   a.status = c->d_status;
   a.passes_out = c->d_passes;
 }
@@ -589,12 +628,14 @@ static int grid_for(dicegpu_ctx* c, FrameKernelFn fn, int* blocks, size_t* smem)
   const int threads = c->warps_per_cta * 32;
   *smem = warp_smem_bytes(c->dp.shape) * c->warps_per_cta;
   CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+  if (c->carveout >= 0)
+    CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributePreferredSharedMemoryCarveout, c->carveout));
   int per_sm = c->ctas_per_sm;
   if (per_sm <= 0) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, threads, *smem));
     if (per_sm < 1) per_sm = 1;
   }
-  *blocks = per_sm * c->num_sms;
+  *blocks = std::min(per_sm * c->num_sms, kMaxQueues);
   return DICEGPU_OK;
 }
 
@@ -614,7 +655,7 @@ extern "C" int dicegpu_execute_correlation(dicegpu_ctx* c) {
   if ((rc = grid_for(c, fn, &blocks, &smem))) return rc;
   FrameArgs a;
   fill_args(c, a, MODE_CORRELATE);
-  CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->d_counter, 0, (size_t)blocks * sizeof(int), c->stream));
   fn<<<blocks, c->warps_per_cta * 32, smem, c->stream>>>(a);
   CK(cudaGetLastError());
   c->launches += 1;
@@ -687,7 +728,7 @@ extern "C" int dicegpu_gamma(dicegpu_ctx* c, const double* fields, double* gamma
     a.fields = d_f;
     a.gamma_out = d_g;
     a.passes_out = nullptr;
-    if (cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream) != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+    if (cudaMemsetAsync(c->d_counter, 0, (size_t)blocks * sizeof(int), c->stream) != cudaSuccess) rc = DICEGPU_ERR_CUDA;
     fn<<<blocks, c->warps_per_cta * 32, smem, c->stream>>>(a);
     if (cudaGetLastError() != cudaSuccess) rc = DICEGPU_ERR_CUDA;
     c->launches += 1;
@@ -867,3 +908,13 @@ extern "C" int dicegpu_correlate(float* points, int n_points, int subset_size, c
   dicegpu_destroy(c);
   return rc;
 }
+
+#ifdef DG_PROFILE
+// profiling builds only: read and clear the section timers
+extern "C" int dicegpu_prof_read(unsigned long long* out8) {
+  if (cudaMemcpyFromSymbol(out8, g_prof, 8 * sizeof(unsigned long long)) != cudaSuccess) return DICEGPU_ERR_CUDA;
+  unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (cudaMemcpyToSymbol(g_prof, z, sizeof(z)) != cudaSuccess) return DICEGPU_ERR_CUDA;
+  return DICEGPU_OK;
+}
+#endif
