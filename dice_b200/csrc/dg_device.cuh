@@ -11,14 +11,6 @@
 
 #include "dicegpu.h"
 
-// build-time variants of the tap sum and the affine map (timing experiments)
-#ifndef DG_CONV_VARIANT
-#define DG_CONV_VARIANT 0
-#endif
-#ifndef DG_MAP_F32
-#define DG_MAP_F32 0
-#endif
-
 namespace dg {
 
 constexpr unsigned FULL = 0xffffffffu;
@@ -161,57 +153,21 @@ __device__ __forceinline__ void conv_taps(const DevImage& im, int x0, int y0, co
   float a = 0.0f, b = 0.0f, c = 0.0f;
   if (GRAD) {
     const float4* q = im.p4 + (size_t)y0 * w + x0;
-#if DG_CONV_VARIANT == 2
-    float4 t[R][R];
-#pragma unroll
-    for (int m = 0; m < R; ++m)
-#pragma unroll
-      for (int n = 0; n < R; ++n) t[m][n] = __ldg(q + (size_t)m * w + n);
-#pragma unroll
-    for (int m = 0; m < R; ++m) {
-      float ra = wx[0] * t[m][0].x, rb = wx[0] * t[m][0].y, rc = wx[0] * t[m][0].z;
-#pragma unroll
-      for (int n = 1; n < R; ++n) {
-        ra = fmaf(wx[n], t[m][n].x, ra);
-        rb = fmaf(wx[n], t[m][n].y, rb);
-        rc = fmaf(wx[n], t[m][n].z, rc);
-      }
-      a = fmaf(wy[m], ra, a);
-      b = fmaf(wy[m], rb, b);
-      c = fmaf(wy[m], rc, c);
-    }
-#else
 #pragma unroll
     for (int m = 0; m < R; ++m) {
       float ra = 0.0f, rb = 0.0f, rc = 0.0f;
-#if DG_CONV_VARIANT == 1
-      if (R == 6) {
-        // pairwise row sums: dependency depth 3 instead of 6
-        const float4 t0 = __ldg(q), t1 = __ldg(q + 1), t2 = __ldg(q + 2);
-        const float4 t3 = __ldg(q + 3), t4 = __ldg(q + 4), t5 = __ldg(q + 5);
-        ra = fmaf(wx[1], t1.x, wx[0] * t0.x) + fmaf(wx[3], t3.x, wx[2] * t2.x) +
-             fmaf(wx[5], t5.x, wx[4] * t4.x);
-        rb = fmaf(wx[1], t1.y, wx[0] * t0.y) + fmaf(wx[3], t3.y, wx[2] * t2.y) +
-             fmaf(wx[5], t5.y, wx[4] * t4.y);
-        rc = fmaf(wx[1], t1.z, wx[0] * t0.z) + fmaf(wx[3], t3.z, wx[2] * t2.z) +
-             fmaf(wx[5], t5.z, wx[4] * t4.z);
-      } else
-#endif
-      {
 #pragma unroll
-        for (int n = 0; n < R; ++n) {
-          const float4 t = __ldg(q + n);
-          ra = fmaf(wx[n], t.x, ra);
-          rb = fmaf(wx[n], t.y, rb);
-          rc = fmaf(wx[n], t.z, rc);
-        }
+      for (int n = 0; n < R; ++n) {
+        const float4 t = __ldg(q + n);
+        ra = fmaf(wx[n], t.x, ra);
+        rb = fmaf(wx[n], t.y, rb);
+        rc = fmaf(wx[n], t.z, rc);
       }
       a = fmaf(wy[m], ra, a);
       b = fmaf(wy[m], rb, b);
       c = fmaf(wy[m], rc, c);
       q += w;
     }
-#endif
     gxv = b;
     gyv = c;
   } else {
@@ -267,13 +223,8 @@ struct MapConst {
 // coordinate (and hence pixel rounding / deactivation) matches bit for bit.
 __device__ __forceinline__ void affine_D(const MapConst& k, float dx, float dy, float& Dx,
                                          float& Dy) {
-#if DG_MAP_F32
-  Dx = fmaf(k.s[3], dx, fmaf(k.s[5], dy, dx));
-  Dy = fmaf(k.s[4], dy, fmaf(k.s[5], dx, dy));
-#else
   Dx = (float)__dadd_rn(__dmul_rn(1.0 + (double)k.s[3], (double)dx), (double)__fmul_rn(k.s[5], dy));
   Dy = (float)__dadd_rn(__dmul_rn(1.0 + (double)k.s[4], (double)dy), (double)__fmul_rn(k.s[5], dx));
-#endif
 }
 
 // Map of a pixel offset (dx, dy) = (x - cx, y - cy); for affine maps the

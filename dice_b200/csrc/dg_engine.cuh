@@ -158,6 +158,7 @@ struct Engine {
   using L = Layout<SHAPE>;
   const FrameArgs& A;
   const int lane;
+  int npass_ = 0;   // pixel passes of the current subset (for work accounting)
 
   __device__ explicit Engine(const FrameArgs& a) : A(a), lane(threadIdx.x & 31) {}
 
@@ -217,7 +218,7 @@ struct Engine {
   __device__ float eval_gamma(const SubsetRef& sb, const float* slots, PassOut* out = nullptr) {
     PassOut o = pass<false, false, true>(sb, slots, nullptr);
     if (out) *out = o;
-    if (A.passes_out && lane == 0) A.passes_out[sb.idx] += 1;
+    ++npass_;
     return gamma_from(o, sb.npix);
   }
 
@@ -254,7 +255,7 @@ struct Engine {
       DG_PT(t_pass);
       last = pass<true, true, false>(sb, slots, M);
       DG_PACC(1, t_pass);
-      if (A.passes_out && lane == 0) A.passes_out[sb.idx] += 1;
+      ++npass_;
       const int n = last.n;
       // Subset::mean(DEF_INTENSITIES): sum G / n over the active pixels
       const double sumG = M[L::ID * L::VW + L::IONE] + last.sumF + (double)n * (double)sb.K;
@@ -709,6 +710,12 @@ struct Engine {
   // generic_correlation_routine for one subset.
   // --------------------------------------------------------------------------
   __device__ void run(int idx) {
+    npass_ = 0;
+    run_subset(idx);
+    if (A.passes_out && lane == 0 && A.mode == MODE_CORRELATE) A.passes_out[idx] = npass_;
+  }
+
+  __device__ void run_subset(int idx) {
     const DevParams& P = A.P;
     double* f = A.fields + (size_t)idx * DICEGPU_FIELD_STRIDE;
     // the subset's field row (32 doubles) in one coalesced load: lane c holds
@@ -738,7 +745,6 @@ struct Engine {
       if (lane == 0) A.gamma_out[idx] = g;
       return;
     }
-    if (A.passes_out && lane == 0) A.passes_out[idx] = 0;
     // frame-0 field-of-view test (DICe_Schema.cpp:2036-2048)
     if (A.geo.half >= 0 && A.first_frame) {
       const float cur_x = (float)(fld(DICEGPU_F_COORD_X) + fld(DICEGPU_F_DISP_X));
@@ -800,7 +806,7 @@ struct Engine {
       corr_status = simplex(sb, slots, num_iterations, last_eval);
       // state of the last evaluation: active set, gradients and bounding box
       last_state = pass<false, true, true>(sb, last_eval, nullptr);
-      if (A.passes_out && lane == 0) A.passes_out[idx] += 1;
+      ++npass_;
       have_state = true;
       state_from_simplex = true;
     };
