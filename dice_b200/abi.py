@@ -158,6 +158,10 @@ def _declare(lib):
         "dicegpu_execute_correlation": (c_int, [c_void_p]),
         "dicegpu_execute_correlation_plain": (c_int, [c_void_p]),
         "dicegpu_launch_count": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+        "dicegpu_capture_sequence": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+        "dicegpu_launch_sequence": (c_int, [c_void_p]),
+        "dicegpu_autotune": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                                     ctypes.POINTER(ctypes.c_float)]),
         "dicegpu_set_launch_shape": (c_int, [c_void_p, c_int, c_int]),
         "dicegpu_get_launch_shape": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
         "dicegpu_correlate": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p,

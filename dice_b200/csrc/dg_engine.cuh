@@ -35,6 +35,7 @@ struct FrameArgs {
   double* gamma_out;     // MODE_GAMMA output
   int* work_counter;     // queue heads: one (queue_mode 0) or one per CTA (1)
   int queue_mode;
+  int chunk;             // consecutive subsets per queue chunk (queue_mode 1)
   int* status;           // device error word
   int32_t* passes_out;   // optional: pixel passes executed per subset (GN + simplex + epilogue)
 };

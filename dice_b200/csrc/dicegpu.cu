@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -28,6 +29,10 @@ using namespace dg;
 // faster on the 2048^2 sequence despite the lower occupancy)
 #ifndef DG_MIN_BLOCKS
 #define DG_MIN_BLOCKS 2
+#endif
+// consecutive subsets per work-queue chunk (0: two per warp of a CTA)
+#ifndef DG_QUEUE_CHUNK
+#define DG_QUEUE_CHUNK 0
 #endif
 
 // ---------------------------------------------------------------------------
@@ -183,20 +188,24 @@ __global__ void __launch_bounds__(256, DG_MIN_BLOCKS) frame_kernel(const __grid_
     }
     return;
   }
-  // Partitioned queues: CTA r owns subsets [r n/G, (r+1) n/G) -- neighbouring
-  // subsets, so its warps share their image footprint in L1 -- and when its
-  // range is exhausted its warps take from the following CTAs' ranges.  Every
-  // index is taken exactly once (atomicAdd); a warp leaves after finding all
-  // G ranges exhausted, so no warp ever waits on another.
+  // Interleaved per-CTA queues: the subsets are cut into chunks of C
+  // consecutive ones and CTA r owns chunks r, r + G, r + 2G, ...  The warps of
+  // a CTA work on neighbouring subsets (shared footprint in L1) and all CTAs
+  // advance through the image together (a narrow band resident in L2).  A CTA
+  // whose chunks are exhausted takes from the following CTAs' sequences.
+  // Every index is taken exactly once (atomicAdd); a warp leaves after finding
+  // all G sequences exhausted, so no warp ever waits on another.
   const int G = gridDim.x;
+  const int C = a.chunk;
   int q = blockIdx.x;
   for (int visited = 0; visited < G;) {
-    const int qbeg = (int)(((long long)q * a.n) / G);
-    const int qend = (int)(((long long)(q + 1) * a.n) / G);
-    int idx = 0;
-    if (lane == 0) idx = qbeg + atomicAdd(a.work_counter + q, 1);
-    idx = __shfl_sync(FULL, idx, 0);
-    if (idx < qend) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(a.work_counter + q, 1);
+    t = __shfl_sync(FULL, t, 0);
+    const long long chunk = (long long)q + (long long)(t / C) * G;
+    const long long lidx = chunk * C + (t % C);
+    const int idx = lidx < a.n ? (int)lidx : a.n;
+    if (idx < a.n) {
       DG_PT(t_run);
       e.run(idx);
       DG_PACC(0, t_run);
@@ -271,7 +280,13 @@ struct dicegpu_ctx {
   int ctas_per_sm = 0;   // 0: occupancy-derived
   int queue_mode = 1;    // 1: per-CTA queues with stealing, 0: one global queue
   int carveout = -1;     // preferred shared-memory carveout (percent), -1: driver default
+  int chunk = DG_QUEUE_CHUNK;   // queue chunk (consecutive subsets); 0: 2 per warp of a CTA
   long long launches = 0;
+  // captured frame sequence
+  cudaStream_t cap_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  long long graph_launches = 0;   // kernels per replay
 };
 
 #define CK(x)                                  \
@@ -399,6 +414,9 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   cudaFree(c->d_def4);
   cudaFree(c->d_fields); cudaFree(c->d_offsets); cudaFree(c->d_px); cudaFree(c->d_py);
   cudaFree(c->d_force); cudaFree(c->d_counter); cudaFree(c->d_status); cudaFree(c->d_passes);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   delete c;
   return DICEGPU_OK;
 }
@@ -620,6 +638,7 @@ static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
   a.plain_index = -1;
   a.work_counter = c->d_counter;
   a.queue_mode = c->queue_mode;
+  a.chunk = c->chunk > 0 ? c->chunk : 2 * c->warps_per_cta;
   a.status = c->d_status;
   a.passes_out = c->d_passes;
 }
@@ -679,6 +698,160 @@ extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
   CK(cudaGetLastError());
   c->launches += c->n;
   c->frame_index += 1;
+  return DICEGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// frame sequences as CUDA graphs
+// ---------------------------------------------------------------------------
+extern "C" int dicegpu_capture_sequence(dicegpu_ctx* c, int n, const float* const* frames,
+                                        const double* reset_fields) {
+  if (!c || n < 1 || !frames) return DICEGPU_ERR_ARG;
+  for (int k = 0; k < n; ++k)
+    if (!frames[k]) return DICEGPU_ERR_ARG;
+  if (!c->has_ref || c->n < 1) return DICEGPU_ERR_STATE;
+  if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+  if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+  // record on a private stream; every call below only enqueues work
+  cudaStream_t user_stream = c->stream;
+  const int saved_frame = c->frame_index;
+  const long long saved_launches = c->launches;
+  const bool saved_has_def = c->has_def;
+  c->stream = c->cap_stream;
+  if (cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    c->stream = user_stream;
+    return DICEGPU_ERR_CUDA;
+  }
+  int rc = DICEGPU_OK;
+  if (reset_fields) {
+    if (cudaMemcpyAsync(c->d_fields, reset_fields, (size_t)c->n * DICEGPU_FIELD_STRIDE * sizeof(double),
+                        cudaMemcpyDeviceToDevice, c->cap_stream) != cudaSuccess)
+      rc = DICEGPU_ERR_CUDA;
+    c->frame_index = 0;
+  }
+  for (int k = 0; k < n && rc == DICEGPU_OK; ++k) {
+    rc = dicegpu_set_def_image(c, c->W, c->H, frames[k], 1);
+    if (rc == DICEGPU_OK) rc = dicegpu_execute_correlation(c);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->cap_stream, &g);
+  c->stream = user_stream;
+  c->frame_index = saved_frame;
+  const long long per_replay = c->launches - saved_launches;
+  c->launches = saved_launches;
+  if (rc != DICEGPU_OK || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    c->has_def = saved_has_def;
+    return rc != DICEGPU_OK ? rc : DICEGPU_ERR_CUDA;
+  }
+  if (cudaGraphInstantiate(&c->graph_exec, g, 0) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    c->graph_exec = nullptr;
+    return DICEGPU_ERR_CUDA;
+  }
+  c->graph = g;
+  c->graph_launches = per_replay;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_launch_sequence(dicegpu_ctx* c) {
+  if (!c) return DICEGPU_ERR_ARG;
+  if (!c->graph_exec) return DICEGPU_ERR_STATE;
+  CK(cudaGraphLaunch(c->graph_exec, c->stream));
+  c->launches += c->graph_launches;
+  c->frame_index = 1;   // later frames continue the sequence
+  return DICEGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch-shape autotuner
+// ---------------------------------------------------------------------------
+namespace {
+struct TuneKey {
+  int dev, shape, interp, defgrad, subset;
+  bool operator<(const TuneKey& o) const {
+    if (dev != o.dev) return dev < o.dev;
+    if (shape != o.shape) return shape < o.shape;
+    if (interp != o.interp) return interp < o.interp;
+    if (defgrad != o.defgrad) return defgrad < o.defgrad;
+    return subset < o.subset;
+  }
+};
+struct TuneVal {
+  int warps, ctas;
+  float ms;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune_cache;
+}  // namespace
+
+extern "C" int dicegpu_autotune(dicegpu_ctx* c, int* warps_per_cta, int* ctas_per_sm, float* best_ms) {
+  int rc = ready(c);
+  if (rc) return rc;
+  const TuneKey key{c->device, c->dp.shape, c->dp.interp, c->params.use_def_gradients,
+                    c->use_lists ? -1 : c->params.subset_size};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      c->warps_per_cta = it->second.warps;
+      c->ctas_per_sm = it->second.ctas;
+      if (warps_per_cta) *warps_per_cta = it->second.warps;
+      if (ctas_per_sm) *ctas_per_sm = it->second.ctas;
+      if (best_ms) *best_ms = it->second.ms;
+      return DICEGPU_OK;
+    }
+  }
+  const size_t fb = (size_t)c->n * DICEGPU_FIELD_STRIDE * sizeof(double);
+  double* saved = nullptr;
+  if (cudaMalloc(&saved, fb) != cudaSuccess) return DICEGPU_ERR_NOMEM;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  rc = DICEGPU_OK;
+  if (cudaMemcpyAsync(saved, c->d_fields, fb, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    rc = DICEGPU_ERR_CUDA;
+  const int frame0 = c->frame_index;
+  const int cand[][2] = {{8, 0}, {4, 0}, {2, 0}, {8, 1}, {4, 2}, {4, 3}};
+  TuneVal best{c->warps_per_cta, c->ctas_per_sm, 1e30f};
+  for (const auto& cd : cand) {
+    if (rc) break;
+    c->warps_per_cta = cd[0];
+    c->ctas_per_sm = cd[1];
+    float ms = 0.0f;
+    for (int rep = 0; rep < 2 && !rc; ++rep) {   // first run warms the configuration up
+      if (cudaMemcpyAsync(c->d_fields, saved, fb, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess) {
+        rc = DICEGPU_ERR_CUDA;
+        break;
+      }
+      c->frame_index = frame0;
+      cudaEventRecord(e0, c->stream);
+      rc = dicegpu_execute_correlation(c);
+      cudaEventRecord(e1, c->stream);
+      if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+      if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (!rc && ms < best.ms) best = TuneVal{cd[0], cd[1], ms};
+  }
+  // leave the fields and the sequence position as they were
+  if (cudaMemcpyAsync(c->d_fields, saved, fb, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess && !rc)
+    rc = DICEGPU_ERR_CUDA;
+  cudaStreamSynchronize(c->stream);
+  c->frame_index = frame0;
+  c->warps_per_cta = best.warps;
+  c->ctas_per_sm = best.ctas;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(saved);
+  if (rc) return rc;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  if (warps_per_cta) *warps_per_cta = best.warps;
+  if (ctas_per_sm) *ctas_per_sm = best.ctas;
+  if (best_ms) *best_ms = best.ms;
   return DICEGPU_OK;
 }
 

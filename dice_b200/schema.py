@@ -138,6 +138,24 @@ class Schema:
     def execute_correlation_plain(self):
         abi.check(self.lib.dicegpu_execute_correlation_plain(self.ctx), "execute_correlation_plain")
 
+    def capture_sequence(self, frames, reset_fields=None):
+        """Records a frame sequence (list of CUDA tensors) as one CUDA graph."""
+        self._seq = [f.contiguous().float() for f in frames]
+        ptrs = (ctypes.c_void_p * len(self._seq))(*[f.data_ptr() for f in self._seq])
+        self._seq_ptrs = ptrs
+        self._seq_reset = reset_fields
+        rp = ctypes.c_void_p(reset_fields.data_ptr()) if reset_fields is not None else None
+        abi.check(self.lib.dicegpu_capture_sequence(self.ctx, len(self._seq), ptrs, rp), "capture_sequence")
+
+    def launch_sequence(self):
+        abi.check(self.lib.dicegpu_launch_sequence(self.ctx), "launch_sequence")
+
+    def autotune(self):
+        w, c, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        abi.check(self.lib.dicegpu_autotune(self.ctx, ctypes.byref(w), ctypes.byref(c), ctypes.byref(ms)),
+                  "autotune")
+        return w.value, c.value, ms.value
+
     def fields(self):
         out = np.zeros((self.n, abi.FIELD_STRIDE), np.float64)
         abi.check(self.lib.dicegpu_get_fields(self.ctx, out.ctypes.data_as(ctypes.c_void_p)), "get_fields")

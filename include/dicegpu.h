@@ -215,6 +215,27 @@ int dicegpu_execute_correlation(dicegpu_ctx* ctx);
  * GPU path the batched launch is compared with). */
 int dicegpu_execute_correlation_plain(dicegpu_ctx* ctx);
 
+/* Frame sequences as one CUDA graph.  dicegpu_capture_sequence records, for
+ * frames k = 0..n-1, the device-to-device copy of frames[k] (device pointers
+ * to w x h float images of the reference's size), its gradients, and one
+ * frame of correlation initialised from the previous frame; when
+ * `reset_fields` (device pointer, n_subsets * DICEGPU_FIELD_STRIDE doubles)
+ * is not NULL the graph first reloads the fields from it and its first frame
+ * is frame 0.  dicegpu_launch_sequence replays the graph on the context's
+ * stream.  The frame pointers and the field source are read at every replay,
+ * so their contents may change between replays.  Replaces the host loop of
+ * set_def_image + execute_correlation (DICe_Main.cpp:324-357). */
+int dicegpu_capture_sequence(dicegpu_ctx* ctx, int n, const float* const* frames,
+                             const double* reset_fields);
+int dicegpu_launch_sequence(dicegpu_ctx* ctx);
+
+/* Chooses the persistent kernel's launch shape for the current images,
+ * subsets and parameters: times one frame for each candidate (warps per CTA
+ * x CTAs per SM), restoring the fields after each trial, keeps the fastest
+ * and caches it per (device, shape function, interpolation, subset size) for
+ * later contexts.  The result is applied to the context and returned. */
+int dicegpu_autotune(dicegpu_ctx* ctx, int* warps_per_cta, int* ctas_per_sm, float* best_ms);
+
 /* Number of kernel launches this context issued since creation. */
 int dicegpu_launch_count(dicegpu_ctx* ctx, int64_t* count);
 
