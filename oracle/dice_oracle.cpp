@@ -1026,6 +1026,16 @@ extern "C" int oracle_default_params(dicegpu_params* p) {
   return 0;
 }
 
+extern "C" int oracle_map(const dicegpu_params* params, const double* fields, int n, const float* xy,
+                          float cx, float cy, float* out_xy) {
+  if (!params || !fields || !xy || !out_xy || n < 0) return DICEGPU_ERR_ARG;
+  ShapeFn sf;
+  sf.init(*params);
+  sf.from_fields(fields);
+  for (int i = 0; i < n; ++i) sf.map(xy[2 * i], xy[2 * i + 1], cx, cy, out_xy[2 * i], out_xy[2 * i + 1]);
+  return 0;
+}
+
 extern "C" int oracle_gradients(int w, int h, const float* img, int method, float* gx, float* gy) {
   if (w < 3 || h < 3 || !img || !gx || !gy) return DICEGPU_ERR_ARG;
   compute_gradients(w, h, img, method, gx, gy);

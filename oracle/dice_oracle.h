@@ -48,6 +48,11 @@ int oracle_interpolate(int method, int w, int h, const float* img, const float* 
 int oracle_gamma(const dicegpu_params* params, int w, int h, const float* ref,
                  const float* def, int n, const double* fields, double* gamma_out);
 
+/* Local_Shape_Function::map of n points (x,y interleaved) about (cx, cy) for
+ * the parameters in the field row `fields` (DICEGPU_F_* columns). */
+int oracle_map(const dicegpu_params* params, const double* fields, int n, const float* xy,
+               float cx, float cy, float* out_xy);
+
 /* Defaults of dice_default_params (same values as dicegpu_default_params). */
 int oracle_default_params(dicegpu_params* p);
 

@@ -34,6 +34,8 @@ def lib():
         L.oracle_gamma.argtypes = [P, ci, ci, vp, vp, ci, vp, vp]
         L.oracle_default_params.restype = ci
         L.oracle_default_params.argtypes = [P]
+        L.oracle_map.restype = ci
+        L.oracle_map.argtypes = [P, vp, ci, vp, ctypes.c_float, ctypes.c_float, vp]
         _lib = L
     return _lib
 
@@ -67,6 +69,16 @@ def execute_frame(params, ref, deff, fields, first_frame=True, nthreads=1, offse
     if counters:
         return gn, sx
     return None
+
+
+def shape_map(params, field_row, xy, cx, cy):
+    """Local_Shape_Function::map of points xy (n x 2) about (cx, cy)."""
+    f = np.ascontiguousarray(field_row, dtype=np.float64)
+    xy = np.ascontiguousarray(xy, dtype=np.float32).reshape(-1, 2)
+    out = np.zeros_like(xy)
+    rc = lib().oracle_map(ctypes.byref(params), _ptr(f), xy.shape[0], _ptr(xy), cx, cy, _ptr(out))
+    assert rc == 0
+    return out
 
 
 def gradients(img, method=0):

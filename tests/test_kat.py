@@ -1,0 +1,160 @@
+"""Known-answer tests restated from the reference's component tests
+(paths inside the DICe project), run on the oracle (CPU) and through the C
+ABI on the GPU (marked gpu).
+
+  tests/component/DICe_TestSubsetGamma.cpp:58-116   stripes, gamma = 0.4 k
+  tests/component/DICe_TestObjective.cpp:177-214    quadratic map KAT
+  tests/component/DICe_TestInterpolants.cpp:60-128  bilinear / Keys on x*y
+  tests/component/DICe_TestInterpShift.cpp:60-128   sub-pixel shifts, GN
+"""
+import math
+
+import numpy as np
+import pytest
+
+from dice_b200 import abi
+from dice_b200 import synthetic as syn
+from oracle import oracle as O
+
+
+def _stripes(shift, w=199, h=199, stripes=10, width=20):
+    img = np.zeros((h, w), np.float32)
+    for s in range(stripes // 2 + 1):
+        x0 = s * 2 * width - shift
+        for x in range(x0, x0 + width):
+            if 0 <= x < w:
+                img[:, x] = 255.0
+    return img
+
+
+def test_subset_gamma_stripes_oracle():
+    """A 99x99 subset at (100,100) of 20 px stripes shifted by 2k px: gamma = 0.4 k (+-0.05)."""
+    ref = _stripes(0)
+    p = abi.default_params(subset_size=99, use_def_gradients=0)
+    f = syn.init_fields([100.0], [100.0])
+    for k in range(11):
+        g = O.gamma(p, ref, _stripes(2 * k), f)[0]
+        assert abs(g - 0.4 * k) < 0.05, (k, g)
+
+
+def test_quadratic_map_kat_oracle():
+    p = abi.default_params(shape_function=abi.QUADRATIC_SF)
+    row = np.zeros(abi.FIELD_STRIDE)
+    q = [1.0, 0.0002, 0.0003, 0.0004, 0.0005, 1.352, 0.0006, 1.0, 0.0007, 0.0008, 0.0009, -0.897]
+    row[abi.F_QUAD_A:abi.F_QUAD_A + 12] = q
+    out = O.shape_map(p, row, [[105.0, 27.0]], 250.0, 250.0)[0]
+    assert abs(out[0] - 149.282) < 1e-3 and abs(out[1] - 110.227) < 1e-3, out
+
+
+def _xy_field(w=40, h=30):
+    y, x = np.mgrid[0:h, 0:w].astype(np.float32)
+    return ((255.0 * x / w) * (255.0 * y / h)).astype(np.float32)
+
+
+def _interp_points():
+    # 11x11 subset at (20, 15) mapped by u=.3589, v=-2.89478, theta=.262
+    p = abi.default_params(enable_rotation=1)
+    row = np.zeros(abi.FIELD_STRIDE)
+    row[abi.F_DISP_X], row[abi.F_DISP_Y], row[abi.F_ROT_Z] = 0.3589, -2.89478, 0.262
+    ys, xs = np.mgrid[15 - 5:15 + 6, 20 - 5:20 + 6]
+    pts = np.stack([xs.ravel(), ys.ravel()], 1).astype(np.float32)
+    return O.shape_map(p, row, pts, 20.0, 15.0)
+
+
+def _exact(m, w=40, h=30):
+    return (255.0 * m[:, 0] / w) * (255.0 * m[:, 1] / h)
+
+
+def test_interpolants_kat_oracle():
+    img = _xy_field()
+    m = _interp_points()
+    bi, _, _ = O.interpolate(abi.BILINEAR, img, m)
+    keys, _, _ = O.interpolate(abi.KEYS_FOURTH, img, m)
+    assert np.abs(bi - _exact(m)).sum() < 1.0
+    assert np.abs(keys - _exact(m)).sum() < 2.0
+
+
+def _cos_image(shift, w=50, h=40, f=5.0):
+    y, x = np.mgrid[0:h, 0:w].astype(np.float32)
+    xv = np.abs(np.cos(((x - np.float32(shift)) / np.float32(w)) * np.float32(f * math.pi)))
+    yv = np.abs(np.cos((y / np.float32(h)) * np.float32(f * math.pi)))
+    return (xv * yv * np.float32(255.0)).astype(np.float32)
+
+
+def _interp_shift_params():
+    return abi.default_params(subset_size=21, optimization=abi.GRADIENT_BASED,
+                              max_solver_iterations_fast=100, use_def_gradients=0)
+
+
+def test_interp_shift_kat_oracle():
+    """GN with Keys-4 recovers shifts 0..1 px of |cos|*|cos| within 0.01 px."""
+    ref = _cos_image(0.0)
+    p = _interp_shift_params()
+    for k in range(11):
+        s = 0.1 * k
+        f = syn.init_fields([25.0], [20.0])
+        O.execute_frame(p, ref, _cos_image(s), f)
+        assert abs(f[0, abi.F_DISP_X] - s) < 0.01, (s, f[0, abi.F_DISP_X])
+
+
+# ---- the same through the GPU --------------------------------------------------
+def _gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+@pytest.mark.gpu
+def test_subset_gamma_stripes_gpu():
+    _gpu()
+    from dice_b200.schema import Schema
+    ref = _stripes(0)
+    p = abi.default_params(subset_size=99, use_def_gradients=0)
+    f = syn.init_fields([100.0], [100.0])
+    for k in range(11):
+        de = _stripes(2 * k)
+        with Schema(p) as s:
+            s.set_ref_image(ref)
+            s.set_def_image(de)
+            s.set_fields(f)
+            g = s.gamma(f)[0]
+        o = O.gamma(p, ref, de, f)[0]
+        assert abs(g - 0.4 * k) < 0.05, (k, g)
+        assert abs(g - o) < 1e-5 + 1e-4 * abs(o), (k, g, o)
+
+
+@pytest.mark.gpu
+def test_interpolants_kat_gpu():
+    _gpu()
+    from dice_b200.schema import Schema
+    img = _xy_field()
+    m = _interp_points()
+    with Schema(abi.default_params()) as s:
+        s.set_ref_image(img)
+        s.set_def_image(img)
+        bi, _, _ = s.interpolate(abi.BILINEAR, m, gradients=False)
+        keys, _, _ = s.interpolate(abi.KEYS_FOURTH, m, gradients=False)
+    assert np.abs(bi - _exact(m)).sum() < 1.0
+    assert np.abs(keys - _exact(m)).sum() < 2.0
+
+
+@pytest.mark.gpu
+def test_interp_shift_kat_gpu():
+    _gpu()
+    from dice_b200.schema import Schema
+    ref = _cos_image(0.0)
+    p = _interp_shift_params()
+    for k in range(11):
+        s_ = 0.1 * k
+        f = syn.init_fields([25.0], [20.0])
+        with Schema(p) as s:
+            s.set_ref_image(ref)
+            s.set_fields(f)
+            s.set_def_image(_cos_image(s_))
+            s.execute_correlation()
+            g = s.fields()
+        o = f.copy()
+        O.execute_frame(p, ref, _cos_image(s_), o)
+        assert abs(g[0, abi.F_DISP_X] - s_) < 0.01, (s_, g[0, abi.F_DISP_X])
+        assert abs(g[0, abi.F_DISP_X] - o[0, abi.F_DISP_X]) < 1e-4
+        assert g[0, abi.F_STATUS] == o[0, abi.F_STATUS]
