@@ -845,6 +845,10 @@ struct Engine {
         record_failed(f, corr_status, num_iterations);
         return;
       }
+      // the second jump test and save_fields map the parameters of the
+      // second attempt (DICe_Schema.cpp:2331-2334)
+      make_mapconst<SHAPE>(slots, false, fcx, fcy, kc);
+      map_to_u_v_theta<SHAPE>(kc, fcx, fcy, nu, nv, nt);
     }
     if (cond_set && lane == 0) f[DICEGPU_F_CONDITION] = cond;
     // sigma needs the gradients of the last deformed-state initialisation
@@ -868,7 +872,6 @@ struct Engine {
     }
     if (fabsf(nu - prev_u) > P.disp_jump || fabsf(nv - prev_v) > P.disp_jump ||
         fabsf(nt - prev_t) > P.theta_jump) {
-      // (the parameters are unchanged since the first jump test)
       record_failed(f, DICEGPU_JUMP_TOLERANCE_EXCEEDED, num_iterations);
       return;
     }

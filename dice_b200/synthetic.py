@@ -167,6 +167,104 @@ def config2_field(k, nframes=10):
     return f
 
 
+def _convex_hull(pts):
+    pts = sorted(map(tuple, pts))
+    if len(pts) < 3:
+        return pts
+
+    def cross(o, a, b):
+        return (a[0] - o[0]) * (b[1] - o[1]) - (a[1] - o[1]) * (b[0] - o[0])
+    lo, hi = [], []
+    for p in pts:
+        while len(lo) >= 2 and cross(lo[-2], lo[-1], p) <= 0:
+            lo.pop()
+        lo.append(p)
+    for p in reversed(pts):
+        while len(hi) >= 2 and cross(hi[-2], hi[-1], p) <= 0:
+            hi.pop()
+        hi.append(p)
+    return lo[:-1] + hi[:-1]
+
+
+def mixed_subsets(w, h, n, seed, margin=40):
+    """Seeded arbitrary-shape subsets: circles (radius 7-25 px), ellipses with
+    60 x 8 px axes at random orientation, and random convex polygons, 150-2000
+    pixels each, as CSR pixel lists sorted by (y, x) like the reference's
+    conformal subsets (DICe_Subset.cpp:115-142).  Returns
+    (cx, cy, offsets, px, py, kind, minor_extent) with kind 0 circle,
+    1 ellipse, 2 polygon."""
+    rng = np.random.default_rng(seed)
+    cx = rng.integers(margin, w - margin, n)
+    cy = rng.integers(margin, h - margin, n)
+    kind = rng.integers(0, 3, n)
+    offs = [0]
+    pxs, pys, minor = [], [], []
+    for i in range(n):
+        x0, y0 = int(cx[i]), int(cy[i])
+        if kind[i] == 0:
+            r = rng.uniform(7.0, 25.0)
+            R = int(np.ceil(r))
+            yy, xx = np.mgrid[-R:R + 1, -R:R + 1]
+            m = xx * xx + yy * yy <= r * r
+            minor.append(2 * r)
+        elif kind[i] == 1:
+            phi = rng.uniform(0, np.pi)
+            R = 31
+            yy, xx = np.mgrid[-R:R + 1, -R:R + 1]
+            a = (xx * np.cos(phi) + yy * np.sin(phi)) / 30.0
+            b = (-xx * np.sin(phi) + yy * np.cos(phi)) / 4.0
+            m = a * a + b * b <= 1.0
+            minor.append(8.0)
+        else:
+            rr = rng.uniform(10.0, 25.0)
+            ang = rng.uniform(0, 2 * np.pi, 9)
+            rad = rr * np.sqrt(rng.uniform(0.3, 1.0, 9))
+            hull = _convex_hull(np.stack([rad * np.cos(ang), rad * np.sin(ang)], 1))
+            R = int(np.ceil(rr)) + 1
+            yy, xx = np.mgrid[-R:R + 1, -R:R + 1]
+            m = np.ones_like(xx, dtype=bool)
+            for k in range(len(hull)):
+                ax, ay = hull[k]
+                bx, by = hull[(k + 1) % len(hull)]
+                m &= (bx - ax) * (yy - ay) - (by - ay) * (xx - ax) >= 0
+            ext = [np.ptp(xx[m]) + 1 if m.any() else 0, np.ptp(yy[m]) + 1 if m.any() else 0]
+            minor.append(float(min(ext)))
+        ys, xs = np.nonzero(m)
+        order = np.lexsort((xs, ys))
+        pys.append((ys[order] + y0 - R).astype(np.int32))
+        pxs.append((xs[order] + x0 - R).astype(np.int32))
+        offs.append(offs[-1] + int(m.sum()))
+    return (cx.astype(np.float64), cy.astype(np.float64), np.asarray(offs, np.int32),
+            np.concatenate(pxs), np.concatenate(pys), kind, np.asarray(minor))
+
+
+def config3_field(w, h, angle_deg=1.5, shear=0.005):
+    """Rigid rotation about the image centre plus simple shear (x += shear * (Y - cy))."""
+    th = np.deg2rad(angle_deg)
+    c, s = float(np.cos(th)), float(np.sin(th))
+    xc, yc = (w - 1) / 2.0, (h - 1) / 2.0
+
+    def f(X, Y):
+        dx = X - xc + shear * (Y - yc)
+        dy = Y - yc
+        x = xc + c * dx - s * dy
+        y = yc + s * dx + c * dy
+        return x - X, y - Y
+    return f
+
+
+def config5_field(h, jump=2.0, strain=0.003):
+    """Mode-I crack: a 2 px opening across the horizontal line y = h/2 plus a
+    linear far field of 0.3 % strain."""
+    yc = h / 2.0
+
+    def f(X, Y):
+        u = strain * X
+        v = strain * Y + torch.where(Y >= yc, torch.full_like(Y, jump / 2.0), torch.full_like(Y, -jump / 2.0))
+        return u, v
+    return f
+
+
 def config2(device="cpu", w=2048, h=2048, nframes=10, count=None):
     """2048^2 16-bit-range speckle image (radius 3-5) and the first `count`
     (default all `nframes`) deformed frames of the sequence."""

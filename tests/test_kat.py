@@ -120,7 +120,16 @@ def test_subset_gamma_stripes_gpu():
             g = s.gamma(f)[0]
         o = O.gamma(p, ref, de, f)[0]
         assert abs(g - 0.4 * k) < 0.05, (k, g)
-        assert abs(g - o) < 1e-5 + 1e-4 * abs(o), (k, g, o)
+        # the subset samples whole pixels, so the exact ZNSSD is a plain
+        # FP64 sum over the 99 x 99 window; the GPU's FP64 moments match it,
+        # while the reference's float running sums over 9801 pixels (which
+        # the oracle reproduces) drift by up to ~1e-4 relative
+        F = ref[51:150, 51:150].astype(np.float64)
+        G = de[51:150, 51:150].astype(np.float64)
+        a, b = F - F.mean(), G - G.mean()
+        exact = 2.0 - 2.0 * (a * b).sum() / np.sqrt((a * a).sum() * (b * b).sum())
+        assert abs(g - exact) < 1e-5 * max(1.0, exact), (k, g, exact)
+        assert abs(g - o) < 1e-5 + 3e-4 * abs(o), (k, g, o)
 
 
 @pytest.mark.gpu
