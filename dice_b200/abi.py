@@ -42,6 +42,7 @@ API_STRIDE = 9
 
 ERR_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_STATE", -4: "ERR_NOMEM",
              -5: "ERR_TIMEOUT", -6: "ERR_UNSUPPORTED", -7: "ERR_DEVICE"}
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_DEVICE = 0, -1, -2, -3, -4, -5, -6, -7
 
 
 class Params(ctypes.Structure):
@@ -72,7 +73,9 @@ class Params(ctypes.Structure):
         ("output_beta", ctypes.c_int32),
         ("use_def_gradients", ctypes.c_int32),
         ("subset_size", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("gauss_filter_images", ctypes.c_int32),
+        ("gauss_filter_mask_size", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
     def copy(self):
@@ -104,6 +107,8 @@ def default_params(**overrides):
     p.final_gamma_threshold = -1.0
     p.use_def_gradients = 1
     p.subset_size = 21
+    p.gauss_filter_images = 0
+    p.gauss_filter_mask_size = 7
     for k, v in overrides.items():
         if not hasattr(p, k):
             raise AttributeError(k)
@@ -170,6 +175,7 @@ def _declare(lib):
                                         c_void_p, c_int]),
         "dicegpu_image_gradients": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_int,
                                             c_void_p]),
+        "dicegpu_gauss_filter": (c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_void_p]),
         "dicegpu_image_gradients_noalloc": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_int,
                                                     c_void_p]),
         "dicegpu_gamma": (c_int, [c_void_p, c_void_p, c_void_p]),

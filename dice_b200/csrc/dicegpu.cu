@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <map>
@@ -91,6 +92,48 @@ __global__ void gradient_smooth_kernel(int w, int h, const float* __restrict__ t
     }
   gx[i] = vx;
   gy[i] = vy;
+}
+
+// Image_::gauss_filter (DICe_Image.cpp:1194-1230).  The M x M weights travel
+// by value in the parameter bank (uniform reads); each CTA stages its
+// (32 + M - 1) x (8 + M - 1) input tile in shared memory.  The sum runs x
+// offset outer, y offset inner, with every float product and sum rounded
+// separately, as the reference's loop does; pixels within M/2+1 of an edge
+// keep their value.
+struct GaussWeights {
+  float c[13 * 13];
+};
+
+constexpr int kGaussBX = 32, kGaussBY = 8, kGaussMaxTile = (kGaussBX + 12) * (kGaussBY + 12);
+
+__global__ void __launch_bounds__(kGaussBX * kGaussBY)
+gauss_filter_kernel(int w, int h, int M, const GaussWeights wt, const float* __restrict__ in,
+                    float* __restrict__ out) {
+  __shared__ float tile[kGaussMaxTile];
+  const int R = M / 2;                 // taps reach R pixels either side
+  const int half = M / 2 + 1;          // the reference's interior test
+  const int TW = kGaussBX + 2 * R, TH = kGaussBY + 2 * R;
+  const int x0 = blockIdx.x * kGaussBX - R, y0 = blockIdx.y * kGaussBY - R;
+  const int tid = threadIdx.y * kGaussBX + threadIdx.x;
+  for (int k = tid; k < TW * TH; k += kGaussBX * kGaussBY) {
+    const int ty = k / TW, tx = k - ty * TW;
+    const int gx = x0 + tx, gy = y0 + ty;
+    tile[k] = (gx >= 0 && gx < w && gy >= 0 && gy < h) ? in[(size_t)gy * w + gx] : 0.0f;
+  }
+  __syncthreads();
+  const int x = blockIdx.x * kGaussBX + threadIdx.x;
+  const int y = blockIdx.y * kGaussBY + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const size_t o = (size_t)y * w + x;
+  if (!(x >= half && x < w - half && y >= half && y < h - half)) {
+    out[o] = in[o];
+    return;
+  }
+  float v = 0.0f;
+  for (int i = 0; i < M; ++i)
+    for (int j = 0; j < M; ++j)
+      v = __fadd_rn(v, __fmul_rn(wt.c[i * M + j], tile[(threadIdx.y + j) * TW + threadIdx.x + i]));
+  out[o] = v;
 }
 
 // (I, Gx, Gy) -> interleaved float4 (the layout the frame kernel gathers from)
@@ -295,6 +338,8 @@ struct dicegpu_ctx {
     if (e_ != cudaSuccess) return DICEGPU_ERR_CUDA; \
   } while (0)
 
+static bool gauss_weights(int M, GaussWeights& g);
+
 static int build_devparams(const dicegpu_params& p, DevParams& d) {
   if (!p.enable_translation) return DICEGPU_ERR_ARG;
   if (p.shape_function != DICEGPU_AFFINE_SF && p.shape_function != DICEGPU_QUADRATIC_SF)
@@ -305,6 +350,10 @@ static int build_devparams(const dicegpu_params& p, DevParams& d) {
         p.optimization == DICEGPU_GRADIENT_BASED_THEN_SIMPLEX))
     return DICEGPU_ERR_UNSUPPORTED;
   if (p.max_solver_iterations_fast < 0 || p.max_solver_iterations_robust < 1) return DICEGPU_ERR_ARG;
+  if (p.gauss_filter_images) {
+    GaussWeights g;
+    if (!gauss_weights(p.gauss_filter_mask_size, g)) return DICEGPU_ERR_ARG;
+  }
   std::memset(&d, 0, sizeof(d));
   d.shape = p.shape_function;
   if (d.shape == DICEGPU_QUADRATIC_SF) {
@@ -372,6 +421,8 @@ extern "C" int dicegpu_default_params(dicegpu_params* p) {
   p->final_gamma_threshold = -1.0;
   p->use_def_gradients = 1;
   p->subset_size = 21;
+  p->gauss_filter_images = 0;
+  p->gauss_filter_mask_size = 7;
   return DICEGPU_OK;
 }
 
@@ -478,8 +529,61 @@ static int launch_gradients(int w, int h, const float* img, float* gx, float* gy
   return DICEGPU_OK;
 }
 
+// The reference's Gaussian masks are outer products of these 1-D weights
+// with every product printed to 9 significant digits (DICe_Image.cpp:54-112);
+// rounding the same way gives the identical float tables.
+static bool gauss_weights(int M, GaussWeights& g) {
+  static const double w5[] = {0.0014, 0.1574, 0.62825};
+  static const double w7[] = {0.006, 0.0606, 0.2418, 0.3831};
+  static const double w9[] = {0.0007, 0.0108, 0.0748, 0.2384, 0.3505};
+  static const double w11[] = {0.0001, 0.0017, 0.0168, 0.087, 0.2328, 0.3231};
+  static const double w13[] = {0.0001, 0.0012, 0.0085, 0.038, 0.1109, 0.2108, 0.2611};
+  const double* half;
+  switch (M) {
+    case 5: half = w5; break;
+    case 7: half = w7; break;
+    case 9: half = w9; break;
+    case 11: half = w11; break;
+    case 13: half = w13; break;
+    default: return false;
+  }
+  const int R = M / 2;
+  double w[13];
+  for (int i = 0; i < M; ++i) w[i] = half[i <= R ? i : M - 1 - i];
+  for (int i = 0; i < M; ++i)
+    for (int j = 0; j < M; ++j) {
+      char buf[32];
+      std::snprintf(buf, sizeof(buf), "%.8e", w[i] * w[j]);
+      g.c[i * M + j] = (float)std::strtod(buf, nullptr);
+    }
+  return true;
+}
+
+static int launch_gauss_filter(int w, int h, int M, const float* in, float* out, cudaStream_t st,
+                               long long* launches) {
+  GaussWeights g;
+  if (!gauss_weights(M, g)) return DICEGPU_ERR_ARG;
+  if (w < M || h < M) return DICEGPU_ERR_ARG;
+  dim3 blk(kGaussBX, kGaussBY), grd((w + kGaussBX - 1) / kGaussBX, (h + kGaussBY - 1) / kGaussBY);
+  gauss_filter_kernel<<<grd, blk, 0, st>>>(w, h, M, g, in, out);
+  CK(cudaGetLastError());
+  if (launches) *launches += 1;
+  return DICEGPU_OK;
+}
+
+// Copies the caller's image into dst; with gauss_filter_images the copy goes
+// through the filter (raw host pixels are staged in the scratch planes).
 static int upload_image(dicegpu_ctx* c, float* dst, const float* src, int on_device) {
   const size_t bytes = (size_t)c->W * c->H * sizeof(float);
+  if (c->params.gauss_filter_images) {
+    const float* raw = src;
+    if (!on_device) {
+      CK(cudaMemcpyAsync(c->d_tmp, src, bytes, cudaMemcpyHostToDevice, c->stream));
+      raw = c->d_tmp;
+    }
+    return launch_gauss_filter(c->W, c->H, c->params.gauss_filter_mask_size, raw, dst, c->stream,
+                               &c->launches);
+  }
   CK(cudaMemcpyAsync(dst, src, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                      c->stream));
   return DICEGPU_OK;
@@ -969,6 +1073,12 @@ extern "C" int dicegpu_image_gradients(int w, int h, const float* d_img, float* 
     cudaFree(tmp);
   }
   return rc;
+}
+
+extern "C" int dicegpu_gauss_filter(int w, int h, const float* d_in, float* d_out, int mask_size,
+                                    void* stream) {
+  if (!d_in || !d_out || d_in == d_out || w < 1 || h < 1) return DICEGPU_ERR_ARG;
+  return launch_gauss_filter(w, h, mask_size, d_in, d_out, (cudaStream_t)stream, nullptr);
 }
 
 // ---------------------------------------------------------------------------

@@ -144,7 +144,12 @@ typedef struct dicegpu_params {
    * DICe_Schema.cpp:185; DICe_LocalShapeFunction.cpp:375-376). */
   int32_t use_def_gradients;
   int32_t subset_size;                   /* square subsets: side length (odd) */
-  int32_t reserved[4];
+  /* Gaussian pre-filter of both images before their gradients
+   * (gauss_filter_images, gauss_filter_mask_size: 5, 7, 9, 11 or 13;
+   * Image_::post_allocation_tasks, DICe_Image.cpp:300-318). */
+  int32_t gauss_filter_images;
+  int32_t gauss_filter_mask_size;
+  int32_t reserved[2];
 } dicegpu_params;
 
 /* Fills *p with the reference defaults. Replaces dice_default_params. */
@@ -267,6 +272,15 @@ int dicegpu_interpolate(dicegpu_ctx* ctx, int method, int n, const float* xy,
  * Replaces Image_::compute_gradients (DICe_Image.cpp:1015-1093). */
 int dicegpu_image_gradients(int w, int h, const float* d_img, float* d_gx, float* d_gy,
                             int method, void* stream);
+
+/* Gaussian filter of a float image with a mask_size x mask_size mask (5, 7,
+ * 9, 11 or 13); pixels closer than mask_size/2+1 to an edge keep their
+ * value.  d_in and d_out are device pointers to different buffers.
+ * Replaces Image_::gauss_filter (DICe_Image.cpp:1194-1230).  Images smaller
+ * than the mask are rejected with DICEGPU_ERR_ARG, as the reference
+ * throws. */
+int dicegpu_gauss_filter(int w, int h, const float* d_in, float* d_out, int mask_size,
+                         void* stream);
 
 /* The same gradients as dicegpu_image_gradients, computed without allocating
  * any device memory.  No counterpart in the reference: it exists for callers

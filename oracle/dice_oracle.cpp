@@ -30,6 +30,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -207,6 +209,52 @@ static void compute_gradients(int w, int h, const float* I, int method, float* g
       }
     }
   }
+}
+
+// Mask of Image_::gauss_filter (DICe_Image.cpp:54-112): the reference's
+// tables are outer products of these 1-D weights, each printed to 9
+// significant digits, stored as float.
+static bool gauss_mask(int M, std::vector<float>& c) {
+  static const double h5[] = {0.0014, 0.1574, 0.62825};
+  static const double h7[] = {0.006, 0.0606, 0.2418, 0.3831};
+  static const double h9[] = {0.0007, 0.0108, 0.0748, 0.2384, 0.3505};
+  static const double h11[] = {0.0001, 0.0017, 0.0168, 0.087, 0.2328, 0.3231};
+  static const double h13[] = {0.0001, 0.0012, 0.0085, 0.038, 0.1109, 0.2108, 0.2611};
+  const double* hw = M == 5 ? h5 : M == 7 ? h7 : M == 9 ? h9 : M == 11 ? h11 : M == 13 ? h13 : nullptr;
+  if (!hw) return false;
+  c.assign((size_t)M * M, 0.0f);
+  for (int i = 0; i < M; ++i)
+    for (int j = 0; j < M; ++j) {
+      const double a = hw[i <= M / 2 ? i : M - 1 - i], b = hw[j <= M / 2 ? j : M - 1 - j];
+      char buf[32];
+      std::snprintf(buf, sizeof(buf), "%.8e", a * b);
+      c[(size_t)i * M + j] = (float)std::strtod(buf, nullptr);
+    }
+  return true;
+}
+
+// Image_::gauss_filter (DICe_Image.cpp:1194-1230): interior pixels (at least
+// M/2+1 from every edge) get the mask sum of the unfiltered copy, x offset
+// outer and y offset inner, in float; the rest keep their value.
+static bool gauss_filter(int w, int h, int M, const float* in, float* out) {
+  std::vector<float> c;
+  if (!gauss_mask(M, c) || w < M || h < M) return false;
+  const int half = M / 2 + 1;
+  std::vector<float> tmp(in, in + (long)w * h);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const long o = (long)y * w + x;
+      if (x >= half && x < w - half && y >= half && y < h - half) {
+        float v = 0.0f;
+        for (int i = 0; i < M; ++i)
+          for (int j = 0; j < M; ++j)
+            v += c[(size_t)i * M + j] * tmp[(long)(y + j - half + 1) * w + x + i - half + 1];
+        out[o] = v;
+      } else {
+        out[o] = tmp[o];
+      }
+    }
+  return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -1023,7 +1071,14 @@ extern "C" int oracle_default_params(dicegpu_params* p) {
   p->final_gamma_threshold = -1.0;
   p->use_def_gradients = 1;
   p->subset_size = 21;
+  p->gauss_filter_images = 0;
+  p->gauss_filter_mask_size = 7;
   return 0;
+}
+
+extern "C" int oracle_gauss_filter(int w, int h, const float* in, float* out, int mask_size) {
+  if (!in || !out || w < 1 || h < 1) return DICEGPU_ERR_ARG;
+  return gauss_filter(w, h, mask_size, in, out) ? 0 : DICEGPU_ERR_ARG;
 }
 
 extern "C" int oracle_map(const dicegpu_params* params, const double* fields, int n, const float* xy,
@@ -1094,6 +1149,17 @@ extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, 
                                     int first_frame, int nthreads, int32_t* gn_iters_out,
                                     int32_t* simplex_evals_out) {
   if (!params || !ref || !def || !fields || n < 0 || w < 16 || h < 16) return DICEGPU_ERR_ARG;
+  // the images' optional Gaussian pre-filter comes before their gradients
+  std::vector<float> fref, fdef;
+  if (params->gauss_filter_images) {
+    fref.resize((long)w * h);
+    fdef.resize((long)w * h);
+    if (!gauss_filter(w, h, params->gauss_filter_mask_size, ref, fref.data()) ||
+        !gauss_filter(w, h, params->gauss_filter_mask_size, def, fdef.data()))
+      return DICEGPU_ERR_ARG;
+    ref = fref.data();
+    def = fdef.data();
+  }
   FrameJob J;
   J.C.P = *params;
   // gradients as Schema::set_ref_image / set_def_image compute them
@@ -1127,6 +1193,16 @@ extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, 
 extern "C" int oracle_gamma(const dicegpu_params* params, int w, int h, const float* ref,
                             const float* def, int n, const double* fields, double* gamma_out) {
   if (!params || !ref || !def || !fields || !gamma_out) return DICEGPU_ERR_ARG;
+  std::vector<float> fref, fdef;
+  if (params->gauss_filter_images) {
+    fref.resize((long)w * h);
+    fdef.resize((long)w * h);
+    if (!gauss_filter(w, h, params->gauss_filter_mask_size, ref, fref.data()) ||
+        !gauss_filter(w, h, params->gauss_filter_mask_size, def, fdef.data()))
+      return DICEGPU_ERR_ARG;
+    ref = fref.data();
+    def = fdef.data();
+  }
   Ctx C;
   C.P = *params;
   std::vector<float> rgx((long)w * h), rgy((long)w * h), dgx, dgy;

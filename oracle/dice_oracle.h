@@ -39,6 +39,9 @@ int oracle_execute_frame(const dicegpu_params* params, int w, int h,
 /* Image_::compute_gradients (finite difference, optional 5-point smoothing). */
 int oracle_gradients(int w, int h, const float* img, int method, float* gx, float* gy);
 
+/* Image_::gauss_filter with a mask_size x mask_size mask (5..13, odd). */
+int oracle_gauss_filter(int w, int h, const float* in, float* out, int mask_size);
+
 /* Image_::interpolate_*_all at n points (x,y interleaved). gx/gy may be NULL. */
 int oracle_interpolate(int method, int w, int h, const float* img, const float* gx,
                        const float* gy, int n, const float* xy, float* out_i,

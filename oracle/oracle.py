@@ -28,6 +28,8 @@ def lib():
         L.oracle_execute_frame.argtypes = [P, ci, ci, vp, vp, ci, vp, vp, vp, vp, vp, ci, ci, vp, vp]
         L.oracle_gradients.restype = ci
         L.oracle_gradients.argtypes = [ci, ci, vp, ci, vp, vp]
+        L.oracle_gauss_filter.restype = ci
+        L.oracle_gauss_filter.argtypes = [ci, ci, vp, vp, ci]
         L.oracle_interpolate.restype = ci
         L.oracle_interpolate.argtypes = [ci, ci, ci, vp, vp, vp, ci, vp, vp, vp, vp]
         L.oracle_gamma.restype = ci
@@ -78,6 +80,15 @@ def shape_map(params, field_row, xy, cx, cy):
     out = np.zeros_like(xy)
     rc = lib().oracle_map(ctypes.byref(params), _ptr(f), xy.shape[0], _ptr(xy), cx, cy, _ptr(out))
     assert rc == 0
+    return out
+
+
+def gauss_filter(img, mask_size=7):
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    h, w = img.shape
+    out = np.zeros_like(img)
+    rc = lib().oracle_gauss_filter(w, h, _ptr(img), _ptr(out), mask_size)
+    assert rc == 0, rc
     return out
 
 

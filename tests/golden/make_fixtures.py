@@ -17,6 +17,7 @@ Sources (paths inside the DICe project):
   tests/regression/parallel_subsets/{input,params}.xml + gold/DICe_solution_0.txt
   tests/regression/single_speckled_shift/{input,params}.xml, subsets.dat,
       gold/single_speckled_shift_{0..6}.txt
+  tests/component/images/ImageB.tif, outFilter{5,7,9,11,13}.rawi  (240 x 161)
 """
 import os
 import sys
@@ -63,7 +64,21 @@ def main(root):
                                "single_speckled_shift_%d.txt" % k))
         rows.append(r[0])
     out["single_speckled_shift_gold"] = np.asarray(rows)
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_gold.npz")
+    # DICe_TestImage: ImageB.tif Gauss-filtered with mask 5..13 against the
+    # float-build outputs images/outFilter<M>.rawi (header: uint32 width,
+    # height, bytes per value; then row-major values).  A 64 x 64 window
+    # whose corner is stored beside the crops keeps the fixture small.
+    out["image_b"] = _img(root, "ImageB.tif")
+    y0, x0 = 40, 60
+    out["gauss_gold_origin"] = np.array([y0, x0], np.int32)
+    for m in (5, 7, 9, 11, 13):
+        with open(os.path.join(root, "tests", "component", "images", "outFilter%d.rawi" % m), "rb") as fh:
+            raw = fh.read()
+        w, h, nb = np.frombuffer(raw[:12], np.uint32)
+        assert nb == 4
+        gold = np.frombuffer(raw[12:], np.float32).reshape(h, w)
+        out["gauss_gold_%d" % m] = gold[y0:y0 + 64, x0:x0 + 64].copy()
+    path =os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_gold.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, {k: v.shape for k, v in out.items()})
 
