@@ -153,14 +153,19 @@ def max_over_ranks(x, world):
 
 def cpu_sample(p, ref, frames, n_sample, nthreads, timed_frames=1):
     """The oracle on a bounded sample: the first `n_sample` subsets of the
-    grid (contiguous rows), run through `timed_frames` frames from zero motion."""
+    grid (contiguous rows), run through `timed_frames` frames from zero motion.
+    The uncertainty fields are computed, as the reference always does
+    (Objective::computeUncertaintyFields on every converged solve); the GPU
+    arm leaves them off (params.compute_uncertainty = 0)."""
+    from dice_b200 import abi
     from dice_b200 import synthetic as syn
     from oracle import oracle as O
     cx, cy = syn.grid_points(W, H, SUBSET, STEP)
     f = syn.init_fields(cx[:n_sample], cy[:n_sample])
+    unc = np.zeros((n_sample, abi.UNCERTAINTY_STRIDE))
     t0 = time.perf_counter()
     for k in range(timed_frames):
-        O.execute_frame(p, ref, frames[k], f, first_frame=(k == 0), nthreads=nthreads)
+        O.execute_frame(p, ref, frames[k], f, first_frame=(k == 0), nthreads=nthreads, uncertainty=unc)
     dt = time.perf_counter() - t0
     return n_sample * timed_frames / dt, dt, f
 
@@ -198,7 +203,7 @@ def run_reference(args):
             "data": "synthetic (seeded speckle sequence)", "impl": "reference",
             "config": workload_config(len(cx), world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "first %d subsets of frame 1 per step (of %d), all cores" % (n_sample, len(cx))},
+                             "sample": "first %d subsets of frame 1 per step (of %d), all cores, uncertainty fields on" % (n_sample, len(cx))},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -353,8 +358,13 @@ def main():
             v0, _, _ = cpu_sample(p, ref_h, fr_h, 2000, cores)
             n_cpu = int(min(n, max(2000, 15.0 * v0)))
         v, dt, _ = cpu_sample(p, ref_h, fr_h, n_cpu, cores)
+        # the same work on one core, on a sample sized for ~5 s
+        n1 = int(min(n_cpu, max(200, 5.0 * v / cores)))
+        v1, dt1, _ = cpu_sample(p, ref_h, fr_h, n1, 1)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": "first %d subsets of frame 1 (of %d), %d threads, %.1f s" % (n_cpu, n, cores, dt)}
+               "sample": "first %d subsets of frame 1 (of %d), %d threads, %.1f s, uncertainty fields on"
+                         % (n_cpu, n, cores, dt),
+               "one_core": {"value": v1, "unit": UNIT, "sample": "first %d subsets, 1 thread, %.1f s" % (n1, dt1)}}
 
     peaks = {}
     try:

@@ -39,6 +39,7 @@ F_QUAD_A = 8
 F_SIGMA, F_GAMMA, F_BETA, F_NOISE, F_CONTRAST = 20, 21, 22, 23, 24
 F_ACTIVE_PIXELS, F_STATUS, F_ITERATIONS, F_MATCH, F_CONDITION, F_OMEGA = 25, 26, 27, 28, 29, 30
 API_STRIDE = 9
+UNCERTAINTY_STRIDE = 8
 
 ERR_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_STATE", -4: "ERR_NOMEM",
              -5: "ERR_TIMEOUT", -6: "ERR_UNSUPPORTED", -7: "ERR_DEVICE"}
@@ -75,7 +76,8 @@ class Params(ctypes.Structure):
         ("subset_size", ctypes.c_int32),
         ("gauss_filter_images", ctypes.c_int32),
         ("gauss_filter_mask_size", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("compute_uncertainty", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
     def copy(self):
@@ -157,6 +159,7 @@ def _declare(lib):
         "dicegpu_set_subset_pixels": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "dicegpu_set_force_simplex": (c_int, [c_void_p, c_int, c_void_p]),
         "dicegpu_get_fields": (c_int, [c_void_p, c_void_p]),
+        "dicegpu_get_uncertainty": (c_int, [c_void_p, c_void_p]),
         "dicegpu_fields_device_ptr": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
         "dicegpu_load_fields": (c_int, [c_void_p, c_void_p, c_int]),
         "dicegpu_store_fields": (c_int, [c_void_p, c_void_p, c_int]),

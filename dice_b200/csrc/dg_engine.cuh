@@ -38,7 +38,37 @@ struct FrameArgs {
   int chunk;             // consecutive subsets per queue chunk (queue_mode 1)
   int* status;           // device error word
   int32_t* passes_out;   // optional: pixel passes executed per subset (GN + simplex + epilogue)
+  double* unc;           // optional: n x DICEGPU_UNCERTAINTY_STRIDE uncertainty fields
 };
+
+// Image_::interpolate_keys_fourth (DICe_Image.cpp:890-924), intensity only:
+// the bilinear value (Image_::interpolate_bilinear, :432-445) near the
+// border, the 6 x 6 Keys sum (rows outer) elsewhere.
+__device__ __forceinline__ float keys_intensity(const DevImage& im, float lx, float ly) {
+  const int w = im.w, h = im.h;
+  const float* __restrict__ I = im.I;
+  // both range tests are written so that a NaN coordinate returns 0
+  if (!(lx > 2.5f && lx < (float)w - 3.5f && ly > 2.5f && ly < (float)h - 3.5f)) {
+    if (!(lx >= 0.0f && lx < (float)w - 1.5f && ly >= 0.0f && ly < (float)h - 1.5f)) return 0.0f;
+    const int x1 = (int)lx, x2 = x1 + 1, y1 = (int)ly, y2 = y1 + 1;
+    return __ldg(I + (size_t)y1 * w + x1) * ((float)x2 - lx) * ((float)y2 - ly) +
+           __ldg(I + (size_t)y1 * w + x2) * (lx - (float)x1) * ((float)y2 - ly) +
+           __ldg(I + (size_t)y2 * w + x2) * (lx - (float)x1) * (ly - (float)y1) +
+           __ldg(I + (size_t)y2 * w + x1) * ((float)x2 - lx) * (ly - (float)y1);
+  }
+  const int ix = (int)lx, iy = (int)ly;
+  float wx[6], wy[6];
+  keys_weights(lx - (float)ix, wx);
+  keys_weights(ly - (float)iy, wy);
+  float v = 0.0f;
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const float* row = I + (size_t)(iy - 2 + m) * w + ix - 2;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) v += wy[m] * wx[n] * __ldg(row + n);
+  }
+  return v;
+}
 
 struct AffineStep {
   float upd[6];   // parameter update per slot (0 for disabled slots)
@@ -235,6 +265,94 @@ struct Engine {
     return em;
   }
 
+  // Objective::computeUncertaintyFields (DICe_Objective.cpp:193-299) after a
+  // converged Gauss-Newton step, without an image deformer (exact motion 0).
+  // `before` holds the parameters of the last pass, whose gradients the
+  // reference's subset still holds; `after` the converged parameters (u, v).
+  // Every subset pixel takes part.  A pixel outside the 4-pixel border at the
+  // last pass takes the reference-image gradient (the reference keeps the
+  // gradient of the last pass in which that pixel was inside, which differs
+  // only for subsets reaching the border).  Sums in FP64; the fields are
+  // rounded to float like the reference's float fields.
+  // Arguments travel by value (registers): a pointer to the caller's arrays
+  // would move them to local memory for the whole Gauss-Newton loop.
+  struct Slots {
+    float s[12];
+  };
+  __device__ __noinline__ void write_uncertainty(const SubsetRef sb, const Slots before,
+                                                 const Slots after) {
+    const double* f = A.fields + (size_t)sb.idx * DICEGPU_FIELD_STRIDE;
+    const float ucx = (float)f[DICEGPU_F_COORD_X], ucy = (float)f[DICEGPU_F_COORD_Y];
+    MapConst kb, ka;
+    const float fcx = (float)sb.cx, fcy = (float)sb.cy;
+    make_mapconst<SHAPE>(before.s, false, fcx, fcy, kb);
+    make_mapconst<SHAPE>(after.s, false, ucx, ucy, ka);
+    float u, v, t;
+    map_to_u_v_theta<SHAPE>(ka, ucx, ucy, u, v, t);
+    const int W = A.def.w, H = A.def.h;
+    const long rlim = (long)A.ref.w * A.ref.h;
+    double s_g2 = 0.0, s_uhat = 0.0, s_ug = 0.0, s_jg = 0.0, s_r = 0.0;
+    for (int p = lane; p < sb.npix; p += 32) {
+      int x, y;
+      pixel_xy(sb, p, x, y);
+      const long ri = (long)y * A.ref.w + x;
+      const bool rin = ri < rlim;
+      float gx = rin ? __ldg(A.ref.gx + ri) : 0.0f;
+      float gy = rin ? __ldg(A.ref.gy + ri) : 0.0f;
+      if (DEFGRAD) {
+        float mx, my, Dx, Dy;
+        map_offset<SHAPE>(kb, __fsub_rn((float)x, fcx), __fsub_rn((float)y, fcy), fcx, fcy, mx, my,
+                          Dx, Dy);
+        const int px = round_pixel(mx), py = round_pixel(my);
+        if (!(px < 4 || px >= W - 4 || py < 4 || py >= H - 4)) {
+          float G;
+          interp_interior<INTERP, true>(A.def, mx, my, G, gx, gy);
+        }
+      }
+      const float g2 = gx * gx + gy * gy;
+      s_g2 += (double)g2;
+      s_uhat += (double)(u * u + v * v);
+      const float inv_g2 = g2 < 1.0e-4f ? 0.0f : (float)(1.0 / (double)g2);
+      const float a = u * gx + v * gy;
+      s_ug += (double)(a * a * inv_g2);
+      const float j = v * gx - u * gy;
+      s_jg += (double)(j * j * inv_g2);
+      const float r0 = rin ? __ldg(A.ref.I + ri) : 0.0f;
+      const float sub_r = keys_intensity(A.def, (float)x + u, (float)y + v) - r0;
+      const float sub_e = keys_intensity(A.def, (float)x, (float)y) - r0;
+      const float d = sub_r - sub_e;
+      s_r += (double)(d * d * inv_g2);
+    }
+    s_g2 = warp_sum(s_g2);
+    s_uhat = warp_sum(s_uhat);
+    s_ug = warp_sum(s_ug);
+    s_jg = warp_sum(s_jg);
+    s_r = warp_sum(s_r);
+    if (lane == 0) {
+      const float cos_hat = s_uhat == 0.0 ? 1.0f : (float)sqrt(s_ug / s_uhat);
+      double* o = A.unc + (size_t)sb.idx * DICEGPU_UNCERTAINTY_STRIDE;
+      o[DICEGPU_U_COS_THETA_HAT] = cos_hat;
+      o[DICEGPU_U_COS_THETA] = 1.0;
+      o[DICEGPU_U_ERROR_L2] = (float)sqrt(s_ug + s_jg);
+      o[DICEGPU_U_RESIDUAL_ERROR] =
+          cos_hat == 0.0f ? 0.0 : (double)(float)(1.0 / (double)cos_hat * (double)(float)sqrt(s_r));
+      o[DICEGPU_U_ERROR_GRAD_PHI] = (float)sqrt(s_ug);
+      o[DICEGPU_U_RESIDUAL] = (float)sqrt(s_r);
+      o[DICEGPU_U_SSSIG] = (float)((1.0 + s_g2) / (sb.npix ? (double)sb.npix : 1.0));
+    }
+  }
+
+  __device__ __forceinline__ void uncertainty_hook(const SubsetRef& sb, const float* before,
+                                                   const float* after) {
+    Slots b, a;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      b.s[i] = before[i];
+      a.s[i] = after[i];
+    }
+    write_uncertainty(sb, b, a);
+  }
+
   // --------------------------------------------------------------------------
   // Gauss-Newton (Objective_ZNSSD::computeUpdateFast).  `slots` in/out.
   // `meanF` is the reference mean at entry (Subset::mean(REF_INTENSITIES)).
@@ -293,7 +411,10 @@ struct Engine {
         if (fabsf(slots[0] - old[0]) >= tol) conv = false;
         if (fabsf(slots[1] - old[1]) >= tol) conv = false;
         if (P.has_rot && fabsf(slots[2] - old[2]) >= tol) conv = false;
-        if (conv) break;
+        if (conv) {
+          if (A.unc && A.mode == MODE_CORRELATE) uncertainty_hook(sb, old, slots);
+          break;
+        }
         continue;
       }
       // lane i owns row i of [H | q] in the reference's compact order
@@ -412,7 +533,10 @@ struct Engine {
         if (fabsf(slots[1] - old[1]) >= tol) conv = false;
         if (P.has_rot && fabsf(slots[2] - old[2]) >= tol) conv = false;
       }
-      if (conv) break;
+      if (conv) {
+        if (A.unc && A.mode == MODE_CORRELATE) uncertainty_hook(sb, old, slots);
+        break;
+      }
     }
     if (solve_it > P.max_fast) return DICEGPU_MAX_ITERATIONS_REACHED;
     return DICEGPU_CORRELATION_SUCCESSFUL;
@@ -739,6 +863,7 @@ struct Engine {
       const int kx = min(max(sb.cx, 0), A.ref.w - 1), ky = min(max(sb.cy, 0), A.ref.h - 1);
       sb.K = __ldg(A.ref.I + (size_t)ky * A.ref.w + kx);
     }
+
     float slots[12];
     if (A.mode == MODE_GAMMA) {
       load_slots_row(fv, slots);

@@ -318,6 +318,9 @@ struct dicegpu_ctx {
   int* d_status = nullptr;
   int32_t* d_passes = nullptr;
   size_t passes_cap = 0;
+  double* d_unc = nullptr;   // uncertainty fields (params.compute_uncertainty)
+  size_t unc_cap = 0;
+  int unc_n = 0;             // subset count the buffer was zeroed for (0: invalid)
   int frame_index = 0;
   int warps_per_cta = 8;   // measured best on the 2048^2 sequence (2 CTAs/SM at 128 registers)
   int ctas_per_sm = 0;   // 0: occupancy-derived
@@ -465,10 +468,26 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   cudaFree(c->d_def4);
   cudaFree(c->d_fields); cudaFree(c->d_offsets); cudaFree(c->d_px); cudaFree(c->d_py);
   cudaFree(c->d_force); cudaFree(c->d_counter); cudaFree(c->d_status); cudaFree(c->d_passes);
+  cudaFree(c->d_unc);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   delete c;
+  return DICEGPU_OK;
+}
+
+template <typename T>
+static int grow(T** p, size_t* cap, size_t need);
+
+// The uncertainty rows exist while params.compute_uncertainty is set; they
+// start at zero for each new set of subsets, like the reference's mesh fields.
+static int ensure_uncertainty(dicegpu_ctx* c) {
+  if (!c->params.compute_uncertainty || c->n < 1 || c->unc_n == c->n) return DICEGPU_OK;
+  const size_t cnt = (size_t)c->n * DICEGPU_UNCERTAINTY_STRIDE;
+  int rc = grow(&c->d_unc, &c->unc_cap, cnt);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(c->d_unc, 0, cnt * sizeof(double), c->stream));
+  c->unc_n = c->n;
   return DICEGPU_OK;
 }
 
@@ -479,7 +498,7 @@ extern "C" int dicegpu_set_params(dicegpu_ctx* c, const dicegpu_params* p) {
   if (rc) return rc;
   c->params = *p;
   c->dp = d;
-  return DICEGPU_OK;
+  return ensure_uncertainty(c);
 }
 
 extern "C" int dicegpu_set_stream(dicegpu_ctx* c, void* stream) {
@@ -645,7 +664,8 @@ extern "C" int dicegpu_set_subsets(dicegpu_ctx* c, int n, const double* fields) 
   if (c->n != n) { c->use_lists = false; c->use_force = false; }
   c->n = n;
   c->frame_index = 0;
-  return DICEGPU_OK;
+  c->unc_n = 0;
+  return ensure_uncertainty(c);
 }
 
 extern "C" int dicegpu_set_subset_pixels(dicegpu_ctx* c, int n, const int32_t* offsets,
@@ -686,6 +706,15 @@ extern "C" int dicegpu_set_force_simplex(dicegpu_ctx* c, int n, const uint8_t* f
 extern "C" int dicegpu_get_fields(dicegpu_ctx* c, double* out) {
   if (!c || !out || c->n < 1) return DICEGPU_ERR_ARG;
   CK(cudaMemcpyAsync(out, c->d_fields, (size_t)c->n * DICEGPU_FIELD_STRIDE * sizeof(double),
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_get_uncertainty(dicegpu_ctx* c, double* out) {
+  if (!c || !out || c->n < 1) return DICEGPU_ERR_ARG;
+  if (!c->params.compute_uncertainty || c->unc_n != c->n) return DICEGPU_ERR_STATE;
+  CK(cudaMemcpyAsync(out, c->d_unc, (size_t)c->n * DICEGPU_UNCERTAINTY_STRIDE * sizeof(double),
                      cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return DICEGPU_OK;
@@ -745,6 +774,7 @@ static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
   a.chunk = c->chunk > 0 ? c->chunk : 2 * c->warps_per_cta;
   a.status = c->d_status;
   a.passes_out = c->d_passes;
+  a.unc = (c->params.compute_uncertainty && c->unc_n == c->n) ? c->d_unc : nullptr;
 }
 
 static int grid_for(dicegpu_ctx* c, FrameKernelFn fn, int* blocks, size_t* smem) {

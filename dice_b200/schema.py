@@ -164,6 +164,14 @@ class Schema:
     def field(self, col):
         return self.fields()[:, col]
 
+    def uncertainty(self):
+        """FIELD_1..FIELD_7 of Objective::computeUncertaintyFields per subset
+        (n x UNCERTAINTY_STRIDE); needs params.compute_uncertainty = 1."""
+        out = np.zeros((self.n, abi.UNCERTAINTY_STRIDE), np.float64)
+        abi.check(self.lib.dicegpu_get_uncertainty(self.ctx, out.ctypes.data_as(ctypes.c_void_p)),
+                  "get_uncertainty")
+        return out
+
     def load_fields(self, src):
         """Asynchronous reload of all fields (numpy host array or CUDA tensor); restarts at frame 0."""
         if _is_cuda_tensor(src):

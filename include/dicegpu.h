@@ -107,6 +107,21 @@ extern "C" {
 #define DICEGPU_F_CONDITION    29   /* CONDITION_NUMBER_FS (2x2 displacement block) */
 #define DICEGPU_F_OMEGA        30
 
+/* Uncertainty fields of Objective::computeUncertaintyFields
+ * (DICe_Objective.cpp:193-299), written for a subset whenever its
+ * Gauss-Newton solve converges (params.compute_uncertainty = 1), kept across
+ * frames like the reference's mesh fields (zero until first written).  Rows
+ * of DICEGPU_UNCERTAINTY_STRIDE doubles: FIELD_1 .. FIELD_7 (FIELD_8/9 need
+ * an image deformer, which the local path has none of). */
+#define DICEGPU_UNCERTAINTY_STRIDE 8
+#define DICEGPU_U_COS_THETA_HAT    0   /* FIELD_1: cos angle(u_hat, grad phi) */
+#define DICEGPU_U_COS_THETA        1   /* FIELD_2: 1 without an exact motion */
+#define DICEGPU_U_ERROR_L2         2   /* FIELD_3 */
+#define DICEGPU_U_RESIDUAL_ERROR   3   /* FIELD_4 */
+#define DICEGPU_U_ERROR_GRAD_PHI   4   /* FIELD_5 */
+#define DICEGPU_U_RESIDUAL         5   /* FIELD_6 */
+#define DICEGPU_U_SSSIG            6   /* FIELD_7: mean squared gradient */
+
 /* dice_correlate's record, DICe_api.h:65: x, y, u, v, theta, sigma, gamma, beta, flag */
 #define DICEGPU_API_STRIDE 9
 
@@ -149,7 +164,11 @@ typedef struct dicegpu_params {
    * Image_::post_allocation_tasks, DICe_Image.cpp:300-318). */
   int32_t gauss_filter_images;
   int32_t gauss_filter_mask_size;
-  int32_t reserved[2];
+  /* 1: converged Gauss-Newton solves also write the uncertainty fields
+   * (DICEGPU_UNCERTAINTY_STRIDE rows, dicegpu_get_uncertainty); the
+   * reference always computes them, the default here is 0 (off). */
+  int32_t compute_uncertainty;
+  int32_t reserved[1];
 } dicegpu_params;
 
 /* Fills *p with the reference defaults. Replaces dice_default_params. */
@@ -199,6 +218,12 @@ int dicegpu_set_force_simplex(dicegpu_ctx* ctx, int n, const uint8_t* flags);
 /* Copies the n * DICEGPU_FIELD_STRIDE field array back to host memory
  * (waits for the context's stream). */
 int dicegpu_get_fields(dicegpu_ctx* ctx, double* fields_out);
+/* Copies the n * DICEGPU_UNCERTAINTY_STRIDE uncertainty fields to host
+ * memory (FIELD_1..FIELD_7 of Objective::computeUncertaintyFields,
+ * DICe_Objective.cpp:193-299).  DICEGPU_ERR_STATE unless
+ * params.compute_uncertainty is set. */
+int dicegpu_get_uncertainty(dicegpu_ctx* ctx, double* out);
+
 /* Device pointer of the field array (n * DICEGPU_FIELD_STRIDE doubles). */
 int dicegpu_fields_device_ptr(dicegpu_ctx* ctx, double** dptr);
 /* Asynchronous copies of the whole field array on the context's stream

@@ -628,10 +628,49 @@ struct Ctx {
   Image ref, def;
 };
 
+// Per-subset side outputs: work counters, and where the uncertainty fields of
+// a converged Gauss-Newton solve go (nullptr: not requested).
 struct Counters {
   int gn_iters = 0;
   int simplex_evals = 0;
+  double* unc = nullptr;
+  float ucx = 0.0f, ucy = 0.0f;   // the subset's COORD_X / COORD_Y fields
 };
+
+// Image_::interpolate_bilinear (DICe_Image.cpp:432-445), intensity only.
+static float bilinear_intensity(const Image& im, float lx, float ly) {
+  if (!(lx >= 0.0f && lx < im.w - 1.5 && ly >= 0.0f && ly < im.h - 1.5)) return 0.0f;   // NaN too
+  const int x1 = (int)lx, x2 = x1 + 1, y1 = (int)ly, y2 = y1 + 1;
+  return im.I[(long)y1 * im.w + x1] * (x2 - lx) * (y2 - ly) +
+         im.I[(long)y1 * im.w + x2] * (lx - x1) * (y2 - ly) +
+         im.I[(long)y2 * im.w + x2] * (lx - x1) * (ly - y1) +
+         im.I[(long)y2 * im.w + x1] * (x2 - lx) * (ly - y1);
+}
+
+// Image_::interpolate_keys_fourth (DICe_Image.cpp:890-924), intensity only:
+// unlike the _all variant it returns the bilinear value near the border.
+static float keys_intensity(const Image& im, float lx, float ly) {
+  if (!(lx > 2.5 && lx < im.w - 3.5 && ly > 2.5 && ly < im.h - 3.5)) return bilinear_intensity(im, lx, ly);
+  const int ix = (int)lx, iy = (int)ly;
+  const float dx = lx - ix, dy = ly - iy;
+  float cx[6], cy[6];
+  cx[0] = keys_f2((float)(dx + 2.0));
+  cx[1] = keys_f1((float)(dx + 1.0));
+  cx[2] = keys_f0(dx);
+  cx[3] = keys_f0((float)(1.0 - dx));
+  cx[4] = keys_f1((float)(2.0 - dx));
+  cx[5] = keys_f2((float)(3.0 - dx));
+  cy[0] = keys_f2((float)(dy + 2.0));
+  cy[1] = keys_f1((float)(dy + 1.0));
+  cy[2] = keys_f0(dy);
+  cy[3] = keys_f0((float)(1.0 - dy));
+  cy[4] = keys_f1((float)(2.0 - dy));
+  cy[5] = keys_f2((float)(3.0 - dy));
+  float v = 0.0f;
+  for (int m = 0; m < 6; ++m)
+    for (int n = 0; n < 6; ++n) v += cy[m] * cx[n] * im.I[(long)(iy - 2 + m) * im.w + ix - 2 + n];
+  return v;
+}
 
 // Objective::gamma (:58-76)
 static float objective_gamma(const Ctx& C, Subset& s, const ShapeFn& sf, Counters* cnt) {
@@ -659,6 +698,46 @@ static float objective_sigma(const Ctx& C, const Subset& s, const ShapeFn& sf, f
   }
   const float sg = sgx > sgy ? sgy : sgx;
   return sg > 0.0f ? (float)std::sqrt(2.0 * noise * noise / sg) : -1.0f;
+}
+
+// Objective::computeUncertaintyFields (DICe_Objective.cpp:193-299) without an
+// image deformer, so the exact motion (bx, by) is zero: FIELD_1..FIELD_7 go to
+// out[0..6].  Every pixel of the subset takes part, active or not, with the
+// gradients the last deformed-state initialisation left in the subset; u, v
+// are the converged parameters mapped at the subset's coordinates.  All sums
+// are float; the field store rounds to float as DICe's float fields do.
+static void uncertainty_fields(const Ctx& C, const Subset& s, const ShapeFn& sf, float fcx,
+                               float fcy, double* out) {
+  float u, v, t;
+  sf.map_to_u_v_theta(fcx, fcy, u, v, t);
+  float norm_uhat_2 = 0.0f, uhat_dot_g = 0.0f, err_dot_g = 0.0f, err_dot_jg = 0.0f, int_r = 0.0f;
+  float sssig = 1.0f;
+  for (int i = 0; i < s.npix; ++i) {
+    const float x = (float)s.x[i], y = (float)s.y[i];
+    const float gx = s.gx[i], gy = s.gy[i];
+    sssig += gx * gx + gy * gy;
+    norm_uhat_2 += u * u + v * v;
+    const float g2 = gx * gx + gy * gy;
+    const float inv_g2 = g2 < 1.0e-4 ? 0.0f : (float)(1.0 / g2);
+    const float a = u * gx + v * gy;
+    uhat_dot_g += a * a * inv_g2;
+    err_dot_g += a * a * inv_g2;
+    const float j = v * gx - u * gy;
+    err_dot_jg += j * j * inv_g2;
+    const float r0 = C.ref.at(C.ref.I, (long)s.y[i] * C.ref.w + s.x[i]);
+    const float sub_r = keys_intensity(C.def, x + u, y + v) - r0;
+    const float sub_r_exact = keys_intensity(C.def, x + 0.0f, y + 0.0f) - r0;
+    int_r += (sub_r - sub_r_exact) * (sub_r - sub_r_exact) * inv_g2;
+  }
+  sssig = (float)(sssig / (s.npix == 0 ? 1.0 : (double)s.npix));
+  const float cos_hat = norm_uhat_2 == 0.0f ? 1.0f : std::sqrt(uhat_dot_g / norm_uhat_2);
+  out[0] = cos_hat;
+  out[1] = 1.0;
+  out[2] = std::sqrt(err_dot_g + err_dot_jg);
+  out[3] = (float)(cos_hat == 0.0f ? 0.0 : 1.0 / (double)cos_hat * (double)std::sqrt(int_r));
+  out[4] = std::sqrt(err_dot_g);
+  out[5] = std::sqrt(int_r);
+  out[6] = sssig;
 }
 
 // Objective_ZNSSD::computeUpdateFast (:430-657)
@@ -726,7 +805,10 @@ static int compute_update_fast(const Ctx& C, Subset& s, ShapeFn& sf, int& num_it
       }
     }
     for (int i = 0; i < N; ++i) sf.p[i] += def_update[i];
-    if (sf.converged(def_old, tol)) break;
+    if (sf.converged(def_old, tol)) {
+      if (cnt && cnt->unc) uncertainty_fields(C, s, sf, cnt->ucx, cnt->ucy, cnt->unc);
+      break;
+    }
   }
   if (solve_it > max_its) return DICEGPU_MAX_ITERATIONS_REACHED;
   return DICEGPU_CORRELATION_SUCCESSFUL;
@@ -1123,6 +1205,7 @@ struct FrameJob {
   bool first_frame;
   int32_t* gn_out;
   int32_t* sx_out;
+  double* unc;
 };
 
 void run_range(const FrameJob& J, int b, int e) {
@@ -1135,6 +1218,11 @@ void run_range(const FrameJob& J, int b, int e) {
     else s.init_square(cx, cy, J.C.P.subset_size);
     s.init_ref(J.C.ref);
     Counters cnt;
+    if (J.unc) {
+      cnt.unc = J.unc + (long)i * DICEGPU_UNCERTAINTY_STRIDE;
+      cnt.ucx = (float)f[DICEGPU_F_COORD_X];
+      cnt.ucy = (float)f[DICEGPU_F_COORD_Y];
+    }
     correlate_subset(J.C, s, f, J.first_frame, J.force_simplex && J.force_simplex[i], &cnt);
     if (J.gn_out) J.gn_out[i] = cnt.gn_iters;
     if (J.sx_out) J.sx_out[i] = cnt.simplex_evals;
@@ -1147,7 +1235,7 @@ extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, 
                                     const int32_t* offsets, const int32_t* px,
                                     const int32_t* py, const uint8_t* force_simplex,
                                     int first_frame, int nthreads, int32_t* gn_iters_out,
-                                    int32_t* simplex_evals_out) {
+                                    int32_t* simplex_evals_out, double* uncertainty) {
   if (!params || !ref || !def || !fields || n < 0 || w < 16 || h < 16) return DICEGPU_ERR_ARG;
   // the images' optional Gaussian pre-filter comes before their gradients
   std::vector<float> fref, fdef;
@@ -1175,7 +1263,7 @@ extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, 
   }
   J.n = n; J.fields = fields; J.offsets = offsets; J.px = px; J.py = py;
   J.force_simplex = force_simplex; J.first_frame = first_frame != 0;
-  J.gn_out = gn_iters_out; J.sx_out = simplex_evals_out;
+  J.gn_out = gn_iters_out; J.sx_out = simplex_evals_out; J.unc = uncertainty;
   if (nthreads <= 1 || n < 2) {
     run_range(J, 0, n);
     return 0;

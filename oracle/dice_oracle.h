@@ -29,12 +29,15 @@ extern "C" {
  * the frame-0 field-of-view test.  `nthreads` workers split the subsets in
  * contiguous ranges (the reference splits them over MPI ranks).  When
  * `oracle_gn_iters` is non-NULL it receives, per subset, the number of
- * Gauss-Newton iterations actually executed (for FLOP accounting). */
+ * Gauss-Newton iterations actually executed (for FLOP accounting).  When
+ * `uncertainty` is non-NULL (n * DICEGPU_UNCERTAINTY_STRIDE doubles) every
+ * converged Gauss-Newton solve writes its subset's uncertainty fields there,
+ * as the reference always does. */
 int oracle_execute_frame(const dicegpu_params* params, int w, int h,
                          const float* ref, const float* def, int n, double* fields,
                          const int32_t* offsets, const int32_t* px, const int32_t* py,
                          const uint8_t* force_simplex, int first_frame, int nthreads,
-                         int32_t* gn_iters_out, int32_t* simplex_evals_out);
+                         int32_t* gn_iters_out, int32_t* simplex_evals_out, double* uncertainty);
 
 /* Image_::compute_gradients (finite difference, optional 5-point smoothing). */
 int oracle_gradients(int w, int h, const float* img, int method, float* gx, float* gy);

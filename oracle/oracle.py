@@ -9,7 +9,7 @@ import os
 
 import numpy as np
 
-from dice_b200.abi import Params, FIELD_STRIDE
+from dice_b200.abi import Params, FIELD_STRIDE, UNCERTAINTY_STRIDE
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdiceoracle.so")
@@ -25,7 +25,7 @@ def lib():
         P = ctypes.POINTER(Params)
         vp, ci = ctypes.c_void_p, ctypes.c_int
         L.oracle_execute_frame.restype = ci
-        L.oracle_execute_frame.argtypes = [P, ci, ci, vp, vp, ci, vp, vp, vp, vp, vp, ci, ci, vp, vp]
+        L.oracle_execute_frame.argtypes = [P, ci, ci, vp, vp, ci, vp, vp, vp, vp, vp, ci, ci, vp, vp, vp]
         L.oracle_gradients.restype = ci
         L.oracle_gradients.argtypes = [ci, ci, vp, ci, vp, vp]
         L.oracle_gauss_filter.restype = ci
@@ -47,8 +47,13 @@ def _ptr(a):
 
 
 def execute_frame(params, ref, deff, fields, first_frame=True, nthreads=1, offsets=None,
-                  px=None, py=None, force_simplex=None, counters=False):
-    """One frame over all subsets; updates `fields` (n x FIELD_STRIDE float64) in place."""
+                  px=None, py=None, force_simplex=None, counters=False, uncertainty=None):
+    """One frame over all subsets; updates `fields` (n x FIELD_STRIDE float64) in place.
+    `uncertainty` (n x UNCERTAINTY_STRIDE float64, optional) receives the
+    uncertainty fields of every converged Gauss-Newton solve."""
+    if uncertainty is not None:
+        assert uncertainty.dtype == np.float64 and uncertainty.flags.c_contiguous
+        assert uncertainty.shape == (fields.shape[0], UNCERTAINTY_STRIDE)
     ref = np.ascontiguousarray(ref, dtype=np.float32)
     deff = np.ascontiguousarray(deff, dtype=np.float32)
     assert fields.dtype == np.float64 and fields.flags.c_contiguous and fields.shape[1] == FIELD_STRIDE
@@ -65,7 +70,7 @@ def execute_frame(params, ref, deff, fields, first_frame=True, nthreads=1, offse
     rc = lib().oracle_execute_frame(ctypes.byref(params), w, h, _ptr(ref), _ptr(deff), n,
                                     _ptr(fields), _ptr(offsets), _ptr(px), _ptr(py),
                                     _ptr(force_simplex), 1 if first_frame else 0, nthreads,
-                                    _ptr(gn), _ptr(sx))
+                                    _ptr(gn), _ptr(sx), _ptr(uncertainty))
     if rc != 0:
         raise RuntimeError("oracle_execute_frame failed: %d" % rc)
     if counters:
