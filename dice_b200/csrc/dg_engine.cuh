@@ -20,7 +20,10 @@
 
 namespace dg {
 
-enum { MODE_CORRELATE = 0, MODE_GAMMA = 1 };
+// MODE_CORRELATE: Schema::execute_correlation for each subset.  The other
+// modes run one Objective entry point on the parameters of each field row:
+// gamma, Gauss-Newton alone, the simplex alone, sigma.
+enum { MODE_CORRELATE = 0, MODE_GAMMA = 1, MODE_GN = 2, MODE_SIMPLEX = 3, MODE_SIGMA = 4 };
 
 struct FrameArgs {
   DevParams P;
@@ -39,6 +42,9 @@ struct FrameArgs {
   int* status;           // device error word
   int32_t* passes_out;   // optional: pixel passes executed per subset (GN + simplex + epilogue)
   double* unc;           // optional: n x DICEGPU_UNCERTAINTY_STRIDE uncertainty fields
+  int32_t* iter_out;     // MODE_GN / MODE_SIMPLEX: iterations per subset
+  int32_t* status_out;   // MODE_GN / MODE_SIMPLEX: Status_Flag per subset
+  double* noise_out;     // MODE_SIGMA: noise_std_dev per subset (sigma goes to gamma_out)
 };
 
 // Image_::interpolate_keys_fourth (DICe_Image.cpp:890-924), intensity only:
@@ -412,7 +418,7 @@ struct Engine {
         if (fabsf(slots[1] - old[1]) >= tol) conv = false;
         if (P.has_rot && fabsf(slots[2] - old[2]) >= tol) conv = false;
         if (conv) {
-          if (A.unc && A.mode == MODE_CORRELATE) uncertainty_hook(sb, old, slots);
+          if (A.unc && (A.mode == MODE_CORRELATE || A.mode == MODE_GN)) uncertainty_hook(sb, old, slots);
           break;
         }
         continue;
@@ -534,7 +540,7 @@ struct Engine {
         if (P.has_rot && fabsf(slots[2] - old[2]) >= tol) conv = false;
       }
       if (conv) {
-        if (A.unc && A.mode == MODE_CORRELATE) uncertainty_hook(sb, old, slots);
+        if (A.unc && (A.mode == MODE_CORRELATE || A.mode == MODE_GN)) uncertainty_hook(sb, old, slots);
         break;
       }
     }
@@ -759,6 +765,67 @@ struct Engine {
     }
   }
 
+  // Local_Shape_Function::save_fields: the shape-function columns of a field
+  // row from the parameters (quadratic: A..L plus u, v, theta mapped at the
+  // subset's coordinates).  Lane 0 writes.
+  __device__ void save_shape_fields(double* f, const float* slots, float fcx, float fcy) const {
+    if (SHAPE == DICEGPU_QUADRATIC_SF) {
+      MapConst k;
+      make_mapconst<SHAPE>(slots, false, fcx, fcy, k);
+      float u, v, t;
+      map_to_u_v_theta<SHAPE>(k, fcx, fcy, u, v, t);
+      if (lane == 0) {
+        for (int i = 0; i < 12; ++i) f[DICEGPU_F_QUAD_A + i] = slots[i];
+        f[DICEGPU_F_DISP_X] = u;
+        f[DICEGPU_F_DISP_Y] = v;
+        f[DICEGPU_F_ROT_Z] = t;
+      }
+    } else if (lane == 0) {
+      f[DICEGPU_F_DISP_X] = slots[0];
+      f[DICEGPU_F_DISP_Y] = slots[1];
+      for (int kx = 2; kx < A.P.N; ++kx) f[DICEGPU_F_DISP_X + A.P.slot[kx]] = slots[A.P.slot[kx]];
+    }
+  }
+
+  // One Objective entry point for a fresh subset at the parameters of its
+  // field row (Objective_ZNSSD::computeUpdateFast, DICe_Objective.cpp:430-657;
+  // Objective::computeUpdateRobust, :369-388; Objective::sigma after the
+  // subset's deformed-state initialisation at those parameters, :150-184).
+  // Separate and not inlined so the correlation path keeps its registers.
+  __device__ __noinline__ void run_objective(const SubsetRef sb, const double fv) {
+    float slots[12];
+    load_slots_row(fv, slots);
+    double* f = A.fields + (size_t)sb.idx * DICEGPU_FIELD_STRIDE;
+    const float fcx = (float)__shfl_sync(FULL, fv, DICEGPU_F_COORD_X);
+    const float fcy = (float)__shfl_sync(FULL, fv, DICEGPU_F_COORD_Y);
+    if (A.mode == MODE_SIGMA) {
+      const PassOut st = pass<false, true, true>(sb, slots, nullptr);
+      float noise = 0.0f;
+      const float sg = sigma(sb, st, slots, noise);
+      if (lane == 0) {
+        A.gamma_out[sb.idx] = sg;
+        A.noise_out[sb.idx] = noise;
+      }
+      return;
+    }
+    int num_iterations = -1;
+    int status;
+    if (A.mode == MODE_GN) {
+      float cond = -1.0f;
+      PassOut last;
+      status = gauss_newton(sb, slots, 0.0f, true, num_iterations, cond, last);
+      if (lane == 0) f[DICEGPU_F_CONDITION] = cond;
+    } else {
+      float last_eval[12];
+      status = simplex(sb, slots, num_iterations, last_eval);
+    }
+    save_shape_fields(f, slots, fcx, fcy);
+    if (lane == 0) {
+      A.iter_out[sb.idx] = num_iterations;
+      A.status_out[sb.idx] = status;
+    }
+  }
+
   __device__ void record_failed(double* f, int status, int num_iterations) const {
     if (lane == 0) {
       f[DICEGPU_F_SIGMA] = -1.0; f[DICEGPU_F_MATCH] = -1.0; f[DICEGPU_F_GAMMA] = -1.0;
@@ -869,6 +936,10 @@ struct Engine {
       load_slots_row(fv, slots);
       const float g = eval_gamma(sb, slots);
       if (lane == 0) A.gamma_out[idx] = g;
+      return;
+    }
+    if (A.mode != MODE_CORRELATE) {
+      run_objective(sb, fv);
       return;
     }
     // frame-0 field-of-view test (DICe_Schema.cpp:2036-2048)

@@ -1051,6 +1051,82 @@ extern "C" int dicegpu_gamma(dicegpu_ctx* c, const double* fields, double* gamma
   return rc;
 }
 
+// One Objective entry point for every subset at the parameters of the
+// caller's field rows (host memory).  MODE_GN / MODE_SIMPLEX write the
+// updated shape-function fields back into `fields` plus iterations and
+// Status_Flag per subset; MODE_SIGMA writes sigma and noise per subset.
+static int run_objective_mode(dicegpu_ctx* c, int mode, double* fields, int32_t* iters,
+                              int32_t* status, double* sigma, double* noise) {
+  int rc = ready(c);
+  if (rc) return rc;
+  const size_t n = (size_t)c->n;
+  const size_t fb = n * DICEGPU_FIELD_STRIDE * sizeof(double);
+  const bool fit = mode == MODE_GN || mode == MODE_SIMPLEX;
+  // one scratch block: fields | iterations | status | sigma | noise
+  const size_t bytes = fb + 2 * n * sizeof(int32_t) + 2 * n * sizeof(double) + 64;
+  unsigned char* buf = nullptr;
+  if (cudaMalloc(&buf, bytes) != cudaSuccess) return DICEGPU_ERR_NOMEM;
+  double* d_f = (double*)buf;
+  int32_t* d_it = (int32_t*)(buf + fb);
+  int32_t* d_st = d_it + n;
+  double* d_sg = (double*)(((uintptr_t)(d_st + n) + 15) & ~(uintptr_t)15);
+  double* d_no = d_sg + n;
+  FrameKernelFn fn = frame_fn(c);
+  int blocks;
+  size_t smem;
+  rc = grid_for(c, fn, &blocks, &smem);
+  if (!rc && cudaMemcpyAsync(d_f, fields, fb, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    rc = DICEGPU_ERR_CUDA;
+  if (!rc) {
+    FrameArgs a;
+    fill_args(c, a, mode);
+    a.fields = d_f;
+    a.passes_out = nullptr;
+    a.iter_out = d_it;
+    a.status_out = d_st;
+    a.gamma_out = d_sg;
+    a.noise_out = d_no;
+    if (cudaMemsetAsync(c->d_counter, 0, (size_t)blocks * sizeof(int), c->stream) != cudaSuccess)
+      rc = DICEGPU_ERR_CUDA;
+    fn<<<blocks, c->warps_per_cta * 32, smem, c->stream>>>(a);
+    if (cudaGetLastError() != cudaSuccess) rc = DICEGPU_ERR_CUDA;
+    c->launches += 1;
+  }
+  auto d2h = [&](void* dst, const void* src, size_t b) {
+    if (!rc && dst && cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+      rc = DICEGPU_ERR_CUDA;
+  };
+  if (fit) {
+    d2h(fields, d_f, fb);
+    d2h(iters, d_it, n * sizeof(int32_t));
+    d2h(status, d_st, n * sizeof(int32_t));
+  } else {
+    d2h(sigma, d_sg, n * sizeof(double));
+    d2h(noise, d_no, n * sizeof(double));
+  }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess && !rc) rc = DICEGPU_ERR_CUDA;
+  cudaFree(buf);
+  return rc;
+}
+
+extern "C" int dicegpu_compute_update_fast(dicegpu_ctx* c, double* fields, int32_t* num_iterations,
+                                           int32_t* status) {
+  if (!c || !fields || !num_iterations || !status) return DICEGPU_ERR_ARG;
+  return run_objective_mode(c, MODE_GN, fields, num_iterations, status, nullptr, nullptr);
+}
+
+extern "C" int dicegpu_compute_update_robust(dicegpu_ctx* c, double* fields, int32_t* num_iterations,
+                                             int32_t* status) {
+  if (!c || !fields || !num_iterations || !status) return DICEGPU_ERR_ARG;
+  return run_objective_mode(c, MODE_SIMPLEX, fields, num_iterations, status, nullptr, nullptr);
+}
+
+extern "C" int dicegpu_sigma(dicegpu_ctx* c, const double* fields, double* sigma_out, double* noise_out) {
+  if (!c || !fields || !sigma_out) return DICEGPU_ERR_ARG;
+  return run_objective_mode(c, MODE_SIGMA, const_cast<double*>(fields), nullptr, nullptr, sigma_out,
+                            noise_out);
+}
+
 extern "C" int dicegpu_interpolate(dicegpu_ctx* c, int method, int n, const float* xy,
                                    float* intensity, float* grad_x, float* grad_y, int on_device) {
   if (!c || !xy || !intensity || n < 0) return DICEGPU_ERR_ARG;

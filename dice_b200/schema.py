@@ -164,6 +164,37 @@ class Schema:
     def field(self, col):
         return self.fields()[:, col]
 
+    def _fit(self, entry, fields):
+        f = np.ascontiguousarray(fields, dtype=np.float64).copy()
+        assert f.shape == (self.n, abi.FIELD_STRIDE)
+        it = np.zeros(self.n, np.int32)
+        st = np.zeros(self.n, np.int32)
+        vp = ctypes.c_void_p
+        abi.check(getattr(self.lib, entry)(self.ctx, f.ctypes.data_as(vp), it.ctypes.data_as(vp),
+                                            st.ctypes.data_as(vp)), entry)
+        return f, it, st
+
+    def compute_update_fast(self, fields):
+        """Objective_ZNSSD::computeUpdateFast per subset from the parameters in
+        `fields`: returns (updated fields, iterations, Status_Flag)."""
+        return self._fit("dicegpu_compute_update_fast", fields)
+
+    def compute_update_robust(self, fields):
+        """Objective::computeUpdateRobust (simplex) per subset: returns
+        (updated fields, iterations, Status_Flag)."""
+        return self._fit("dicegpu_compute_update_robust", fields)
+
+    def sigma(self, fields):
+        """Objective::sigma per subset at the parameters in `fields`:
+        returns (sigma, noise_std_dev)."""
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        sg = np.zeros(self.n, np.float64)
+        no = np.zeros(self.n, np.float64)
+        vp = ctypes.c_void_p
+        abi.check(self.lib.dicegpu_sigma(self.ctx, f.ctypes.data_as(vp), sg.ctypes.data_as(vp),
+                                         no.ctypes.data_as(vp)), "sigma")
+        return sg, no
+
     def uncertainty(self):
         """FIELD_1..FIELD_7 of Objective::computeUncertaintyFields per subset
         (n x UNCERTAINTY_STRIDE); needs params.compute_uncertainty = 1."""

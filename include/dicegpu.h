@@ -328,6 +328,32 @@ int dicegpu_image_gradients_noalloc(int w, int h, const float* d_img, float* d_g
  * n * stride): writes gamma per subset to gamma_out (host). */
 int dicegpu_gamma(dicegpu_ctx* ctx, const double* fields, double* gamma_out);
 
+/* Objective_ZNSSD::computeUpdateFast (DICe_Objective.cpp:430-657) for every
+ * subset on its own: a fresh subset, the shape function initialised from the
+ * subset's row of `fields` (host, n * DICEGPU_FIELD_STRIDE), Gauss-Newton to
+ * convergence.  The updated shape-function columns (and CONDITION) are
+ * written back into `fields`; num_iterations and the Status_Flag
+ * (CORRELATION_SUCCESSFUL, MAX_ITERATIONS_REACHED, HESSIAN_SINGULAR) per
+ * subset go to the two host arrays of n entries.  With
+ * params.compute_uncertainty a converged solve also writes the subset's
+ * uncertainty row, as the reference does. */
+int dicegpu_compute_update_fast(dicegpu_ctx* ctx, double* fields, int32_t* num_iterations,
+                                int32_t* status);
+
+/* Objective::computeUpdateRobust (DICe_Objective.cpp:369-388): the
+ * Nelder-Mead simplex (Simplex::minimize, DICe_Simplex.cpp:60-277) for every
+ * subset on its own, same in/out convention as dicegpu_compute_update_fast;
+ * the shape function is left where the simplex leaves it. */
+int dicegpu_compute_update_robust(dicegpu_ctx* ctx, double* fields, int32_t* num_iterations,
+                                  int32_t* status);
+
+/* Objective::sigma (DICe_Objective.cpp:150-184) for every subset at the
+ * parameters of its row of `fields`, after the subset has been initialised on
+ * the deformed image at those parameters (the state sigma reads in the
+ * correlation routine).  sigma_out and noise_out (noise_std_dev; may be NULL)
+ * are host arrays of n doubles. */
+int dicegpu_sigma(dicegpu_ctx* ctx, const double* fields, double* sigma_out, double* noise_out);
+
 /* Error word the device kernels write instead of trapping (0 = none). */
 int dicegpu_device_status(dicegpu_ctx* ctx, int32_t* status);
 

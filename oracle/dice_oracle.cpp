@@ -1278,6 +1278,69 @@ extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, 
   return 0;
 }
 
+// One Objective entry point per subset on a fresh square subset at the
+// parameters of its field row: op 0 computeUpdateFast (:430-657), op 1
+// computeUpdateRobust (:369-388), op 2 sigma (:150-184) after the subset's
+// deformed-state initialisation at those parameters.  Ops 0 and 1 write the
+// shape-function fields (and CONDITION for op 0) back into `fields`.
+extern "C" int oracle_objective(const dicegpu_params* params, int w, int h, const float* ref,
+                                const float* def, int n, double* fields, int op, int32_t* iters_out,
+                                int32_t* status_out, double* sigma_out, double* noise_out) {
+  if (!params || !ref || !def || !fields || op < 0 || op > 2) return DICEGPU_ERR_ARG;
+  std::vector<float> fref, fdef;
+  if (params->gauss_filter_images) {
+    fref.resize((long)w * h);
+    fdef.resize((long)w * h);
+    if (!gauss_filter(w, h, params->gauss_filter_mask_size, ref, fref.data()) ||
+        !gauss_filter(w, h, params->gauss_filter_mask_size, def, fdef.data()))
+      return DICEGPU_ERR_ARG;
+    ref = fref.data();
+    def = fdef.data();
+  }
+  Ctx C;
+  C.P = *params;
+  std::vector<float> rgx((long)w * h), rgy((long)w * h), dgx, dgy;
+  compute_gradients(w, h, ref, params->gradient_method, rgx.data(), rgy.data());
+  C.ref.w = w; C.ref.h = h; C.ref.I = ref; C.ref.gx = rgx.data(); C.ref.gy = rgy.data();
+  C.ref.has_gradients = true;
+  C.def.w = w; C.def.h = h; C.def.I = def;
+  if (params->use_def_gradients) {
+    dgx.resize((long)w * h); dgy.resize((long)w * h);
+    compute_gradients(w, h, def, params->gradient_method, dgx.data(), dgy.data());
+    C.def.gx = dgx.data(); C.def.gy = dgy.data(); C.def.has_gradients = true;
+  }
+  Subset s;
+  for (int i = 0; i < n; ++i) {
+    double* f = fields + (long)i * DICEGPU_FIELD_STRIDE;
+    s.init_square((int)f[DICEGPU_F_COORD_X], (int)f[DICEGPU_F_COORD_Y], params->subset_size);
+    s.init_ref(C.ref);
+    ShapeFn sf;
+    sf.init(C.P);
+    sf.from_fields(f);
+    const float fcx = (float)f[DICEGPU_F_COORD_X], fcy = (float)f[DICEGPU_F_COORD_Y];
+    if (op == 2) {
+      s.init_def(C.def, sf, C.P.interpolation);
+      float noise = 0.0f;
+      const float sg = objective_sigma(C, s, sf, noise);
+      if (sigma_out) sigma_out[i] = sg;
+      if (noise_out) noise_out[i] = noise;
+      continue;
+    }
+    int num_iterations = -1, st;
+    if (op == 0) {
+      double cond = 0.0;
+      st = compute_update_fast(C, s, sf, num_iterations, &cond, nullptr);
+      f[DICEGPU_F_CONDITION] = cond;
+    } else {
+      st = compute_update_robust(C, s, sf, num_iterations, nullptr);
+    }
+    sf.to_fields(f, fcx, fcy);
+    if (iters_out) iters_out[i] = num_iterations;
+    if (status_out) status_out[i] = st;
+  }
+  return 0;
+}
+
 extern "C" int oracle_gamma(const dicegpu_params* params, int w, int h, const float* ref,
                             const float* def, int n, const double* fields, double* gamma_out) {
   if (!params || !ref || !def || !fields || !gamma_out) return DICEGPU_ERR_ARG;

@@ -50,6 +50,12 @@ int oracle_interpolate(int method, int w, int h, const float* img, const float* 
                        const float* gy, int n, const float* xy, float* out_i,
                        float* out_gx, float* out_gy);
 
+/* One Objective entry point per (square) subset at the parameters of its row
+ * of `fields`: op 0 computeUpdateFast, 1 computeUpdateRobust, 2 sigma. */
+int oracle_objective(const dicegpu_params* params, int w, int h, const float* ref,
+                     const float* def, int n, double* fields, int op, int32_t* iters_out,
+                     int32_t* status_out, double* sigma_out, double* noise_out);
+
 /* Objective::gamma for each subset at the parameters in `fields`. */
 int oracle_gamma(const dicegpu_params* params, int w, int h, const float* ref,
                  const float* def, int n, const double* fields, double* gamma_out);

@@ -34,6 +34,8 @@ def lib():
         L.oracle_interpolate.argtypes = [ci, ci, ci, vp, vp, vp, ci, vp, vp, vp, vp]
         L.oracle_gamma.restype = ci
         L.oracle_gamma.argtypes = [P, ci, ci, vp, vp, ci, vp, vp]
+        L.oracle_objective.restype = ci
+        L.oracle_objective.argtypes = [P, ci, ci, vp, vp, ci, vp, ci, vp, vp, vp, vp]
         L.oracle_default_params.restype = ci
         L.oracle_default_params.argtypes = [P]
         L.oracle_map.restype = ci
@@ -133,3 +135,21 @@ def gamma(params, ref, deff, fields):
                             _ptr(fields), _ptr(out))
     assert rc == 0
     return out
+
+
+def objective(params, ref, deff, fields, op):
+    """op 0 computeUpdateFast / 1 computeUpdateRobust: updates `fields` in place
+    and returns (iterations, status); op 2 sigma: returns (sigma, noise)."""
+    ref = np.ascontiguousarray(ref, dtype=np.float32)
+    deff = np.ascontiguousarray(deff, dtype=np.float32)
+    assert fields.dtype == np.float64 and fields.flags.c_contiguous
+    h, w = ref.shape
+    n = fields.shape[0]
+    it = np.zeros(n, np.int32)
+    st = np.zeros(n, np.int32)
+    sg = np.zeros(n, np.float64)
+    no = np.zeros(n, np.float64)
+    rc = lib().oracle_objective(ctypes.byref(params), w, h, _ptr(ref), _ptr(deff), n, _ptr(fields), op,
+                                _ptr(it), _ptr(st), _ptr(sg), _ptr(no))
+    assert rc == 0, rc
+    return (sg, no) if op == 2 else (it, st)
