@@ -160,9 +160,12 @@ def _declare(lib):
         "dicegpu_set_force_simplex": (c_int, [c_void_p, c_int, c_void_p]),
         "dicegpu_get_fields": (c_int, [c_void_p, c_void_p]),
         "dicegpu_get_uncertainty": (c_int, [c_void_p, c_void_p]),
+        "dicegpu_num_subsets": (c_int, [c_void_p, ctypes.POINTER(c_int)]),
         "dicegpu_compute_update_fast": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
         "dicegpu_compute_update_robust": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
         "dicegpu_sigma": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        "dicegpu_adjoint": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
+                                    c_void_p]),
         "dicegpu_fields_device_ptr": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
         "dicegpu_load_fields": (c_int, [c_void_p, c_void_p, c_int]),
         "dicegpu_store_fields": (c_int, [c_void_p, c_void_p, c_int]),

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "dg_engine.cuh"
+#include "dg_adjoint.cuh"
 #include "dicegpu.h"
 
 using namespace dg;
@@ -711,6 +712,12 @@ extern "C" int dicegpu_get_fields(dicegpu_ctx* c, double* out) {
   return DICEGPU_OK;
 }
 
+extern "C" int dicegpu_num_subsets(dicegpu_ctx* c, int* n) {
+  if (!c || !n) return DICEGPU_ERR_ARG;
+  *n = c->n;
+  return DICEGPU_OK;
+}
+
 extern "C" int dicegpu_get_uncertainty(dicegpu_ctx* c, double* out) {
   if (!c || !out || c->n < 1) return DICEGPU_ERR_ARG;
   if (!c->params.compute_uncertainty || c->unc_n != c->n) return DICEGPU_ERR_STATE;
@@ -1125,6 +1132,47 @@ extern "C" int dicegpu_sigma(dicegpu_ctx* c, const double* fields, double* sigma
   if (!c || !fields || !sigma_out) return DICEGPU_ERR_ARG;
   return run_objective_mode(c, MODE_SIGMA, const_cast<double*>(fields), nullptr, nullptr, sigma_out,
                             noise_out);
+}
+
+extern "C" int dicegpu_adjoint(dicegpu_ctx* c, const double* d_fields, const double* d_seed,
+                               int objective, int grad_source, double* d_value, double* d_dparams,
+                               float* d_ddef) {
+  int rc = ready(c);
+  if (rc) return rc;
+  if (!d_fields || objective < 0 || objective > 1 || grad_source < 0 || grad_source > 1)
+    return DICEGPU_ERR_ARG;
+  if (c->params.interpolation != DICEGPU_KEYS_FOURTH) return DICEGPU_ERR_UNSUPPORTED;
+  if (grad_source == 1 && !c->params.use_def_gradients) return DICEGPU_ERR_STATE;
+  AdjointArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.P = c->dp;
+  a.ref = DevImage{c->W, c->H, c->d_ref, c->d_ref_gx, c->d_ref_gy, nullptr};
+  a.def = DevImage{c->W, c->H, c->d_def, c->d_def_gx, c->d_def_gy, nullptr};
+  a.geo.half = c->use_lists ? -1 : c->params.subset_size / 2;
+  a.geo.offsets = c->use_lists ? c->d_offsets : nullptr;
+  a.geo.px = c->use_lists ? c->d_px : nullptr;
+  a.geo.py = c->use_lists ? c->d_py : nullptr;
+  a.fields = d_fields;
+  a.seed = d_seed;
+  a.n = c->n;
+  a.objective = objective;
+  a.grad_source = grad_source;
+  a.value_out = d_value;
+  a.dparams_out = d_dparams;
+  a.ddef = d_ddef;
+  const void* fn = c->dp.shape == DICEGPU_QUADRATIC_SF ? (const void*)adjoint_kernel<DICEGPU_QUADRATIC_SF>
+                                                      : (const void*)adjoint_kernel<DICEGPU_AFFINE_SF>;
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
+  const int need = (c->n + 7) / 8;
+  const int blocks = std::max(1, std::min(std::max(per_sm, 1) * c->num_sms, need));
+  if (c->dp.shape == DICEGPU_QUADRATIC_SF)
+    adjoint_kernel<DICEGPU_QUADRATIC_SF><<<blocks, 256, 0, c->stream>>>(a);
+  else
+    adjoint_kernel<DICEGPU_AFFINE_SF><<<blocks, 256, 0, c->stream>>>(a);
+  CK(cudaGetLastError());
+  c->launches += 1;
+  return DICEGPU_OK;
 }
 
 extern "C" int dicegpu_interpolate(dicegpu_ctx* c, int method, int n, const float* xy,

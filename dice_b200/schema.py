@@ -195,6 +195,28 @@ class Schema:
                                          no.ctypes.data_as(vp)), "sigma")
         return sg, no
 
+    def adjoint(self, fields, seed=None, objective=0, grad_source=0, ddef=None):
+        """dicegpu_adjoint on CUDA tensors: `fields` (n x FIELD_STRIDE float64)
+        holds each subset's parameters, `seed` (n float64) weights the
+        objectives, `ddef` (H x W float32) receives the derivative with
+        respect to the deformed image (added).  Returns (value, dparams):
+        n objective values and n x 12 derivatives in parameter-slot order.
+        Ordered after the caller's current stream's work."""
+        import torch
+        assert fields.is_cuda and fields.dtype == torch.float64 and fields.is_contiguous()
+        assert fields.shape == (self.n, abi.FIELD_STRIDE)
+        value = torch.empty(self.n, dtype=torch.float64, device=fields.device)
+        dparams = torch.empty((self.n, 12), dtype=torch.float64, device=fields.device)
+        vp = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        if seed is not None:
+            assert seed.is_cuda and seed.dtype == torch.float64 and seed.is_contiguous()
+        if ddef is not None:
+            assert ddef.is_cuda and ddef.dtype == torch.float32 and ddef.is_contiguous()
+        self.set_stream(torch.cuda.current_stream())
+        abi.check(self.lib.dicegpu_adjoint(self.ctx, vp(fields), vp(seed), int(objective), int(grad_source),
+                                           vp(value), vp(dparams), vp(ddef)), "adjoint")
+        return value, dparams
+
     def uncertainty(self):
         """FIELD_1..FIELD_7 of Objective::computeUncertaintyFields per subset
         (n x UNCERTAINTY_STRIDE); needs params.compute_uncertainty = 1."""

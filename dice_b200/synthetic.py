@@ -265,6 +265,20 @@ def config5_field(h, jump=2.0, strain=0.003):
     return f
 
 
+def config4(device="cpu", w=1024, h=1024, ncontrol=16, ctrl_sigma=0.8, noise_sigma=1.0, seed=4):
+    """1024^2 speckle pair whose field is a seeded 16 x 16 cubic B-spline
+    control grid with N(0, 0.8 px) control displacements.  Returns
+    (ref, def, field, ctrl) with ctrl the (2, G, G) control tensor."""
+    from dice_b200.bspline import BSplineField
+    ref = speckle_image(w, h, seed=seed, r_min=2.0, r_max=4.0, grey_lo=20.0, grey_hi=230.0,
+                        blur_sigma=0.8, device=device)
+    g = _gen(seed + 1000, "cpu")
+    ctrl = (ctrl_sigma * torch.randn((2, ncontrol, ncontrol), generator=g, dtype=torch.float64)).to(device)
+    field = BSplineField(w, h, ncontrol)
+    deff = warp_image(ref, field.field_fn(ctrl), noise_sigma=noise_sigma, seed=seed + 100, clip=(0.0, 255.0))
+    return ref, deff, field, ctrl
+
+
 def config2(device="cpu", w=2048, h=2048, nframes=10, count=None):
     """2048^2 16-bit-range speckle image (radius 3-5) and the first `count`
     (default all `nframes`) deformed frames of the sequence."""

@@ -224,6 +224,9 @@ int dicegpu_get_fields(dicegpu_ctx* ctx, double* fields_out);
  * params.compute_uncertainty is set. */
 int dicegpu_get_uncertainty(dicegpu_ctx* ctx, double* out);
 
+/* Number of subsets of the context (0 before dicegpu_set_subsets). */
+int dicegpu_num_subsets(dicegpu_ctx* ctx, int* n);
+
 /* Device pointer of the field array (n * DICEGPU_FIELD_STRIDE doubles). */
 int dicegpu_fields_device_ptr(dicegpu_ctx* ctx, double** dptr);
 /* Asynchronous copies of the whole field array on the context's stream
@@ -353,6 +356,27 @@ int dicegpu_compute_update_robust(dicegpu_ctx* ctx, double* fields, int32_t* num
  * correlation routine).  sigma_out and noise_out (noise_std_dev; may be NULL)
  * are host arrays of n doubles. */
 int dicegpu_sigma(dicegpu_ctx* ctx, const double* fields, double* sigma_out, double* noise_out);
+
+/* Reverse-mode derivative of the subset objective (no counterpart in the
+ * reference, which has no derivative code: it differentiates the forward map
+ * the reference evaluates -- warp by the shape function, Keys fourth-order
+ * interpolation of the deformed image, Objective::gamma over the active
+ * pixels, DICe_Objective.cpp:58-76).  For every subset at the parameters of
+ * its row of d_fields (device, n * DICEGPU_FIELD_STRIDE):
+ *   objective 0: gamma;  objective 1: sum ((G - mean G) - (F - mean F))^2,
+ *   whose derivative is twice the Gauss-Newton right-hand side q.
+ *   grad_source 0: the exact derivative of the Keys interpolant;
+ *   grad_source 1: the Keys interpolation of the gradient images (needs
+ *   params.use_def_gradients), as the Gauss-Newton residuals use.
+ * d_seed (n doubles, NULL: all ones) weights each subset's objective.
+ * Outputs (device, each may be NULL): d_value n objective values (-1 where
+ * the objective is undefined), d_dparams n * 12 derivatives in parameter-slot
+ * order (affine: u, v, theta, ex, ey, gxy; quadratic: A..L), d_ddef the W * H
+ * derivative with respect to the deformed image's intensities, ADDED to what
+ * the buffer holds.  Keys interpolation only (DICEGPU_ERR_UNSUPPORTED
+ * otherwise).  Asynchronous on the context's stream. */
+int dicegpu_adjoint(dicegpu_ctx* ctx, const double* d_fields, const double* d_seed, int objective,
+                    int grad_source, double* d_value, double* d_dparams, float* d_ddef);
 
 /* Error word the device kernels write instead of trapping (0 = none). */
 int dicegpu_device_status(dicegpu_ctx* ctx, int32_t* status);

@@ -1278,6 +1278,60 @@ extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, 
   return 0;
 }
 
+// The Gauss-Newton system of Objective_ZNSSD::computeUpdateFast
+// (DICe_Objective.cpp:523-546) assembled once, for a fresh square subset at
+// the parameters of each field row: H (n x N x N) and q (n x N), compact
+// parameter order.  No solve.
+extern "C" int oracle_gn_system(const dicegpu_params* params, int w, int h, const float* ref,
+                                const float* def, int n, const double* fields, double* H_out,
+                                double* q_out) {
+  if (!params || !ref || !def || !fields || !H_out || !q_out) return DICEGPU_ERR_ARG;
+  Ctx C;
+  C.P = *params;
+  std::vector<float> rgx((long)w * h), rgy((long)w * h), dgx, dgy;
+  compute_gradients(w, h, ref, params->gradient_method, rgx.data(), rgy.data());
+  C.ref.w = w; C.ref.h = h; C.ref.I = ref; C.ref.gx = rgx.data(); C.ref.gy = rgy.data();
+  C.ref.has_gradients = true;
+  C.def.w = w; C.def.h = h; C.def.I = def;
+  if (params->use_def_gradients) {
+    dgx.resize((long)w * h); dgy.resize((long)w * h);
+    compute_gradients(w, h, def, params->gradient_method, dgx.data(), dgy.data());
+    C.def.gx = dgx.data(); C.def.gy = dgy.data(); C.def.has_gradients = true;
+  }
+  const bool use_ref_grads = !C.def.has_gradients;
+  Subset s;
+  for (int i = 0; i < n; ++i) {
+    const double* f = fields + (long)i * DICEGPU_FIELD_STRIDE;
+    s.init_square((int)f[DICEGPU_F_COORD_X], (int)f[DICEGPU_F_COORD_Y], params->subset_size);
+    s.init_ref(C.ref);
+    ShapeFn sf;
+    sf.init(C.P);
+    sf.from_fields(f);
+    const int N = sf.N;
+    double* H = H_out + (long)i * N * N;
+    double* q = q_out + (long)i * N;
+    for (int k = 0; k < N * N; ++k) H[k] = 0.0;
+    for (int k = 0; k < N; ++k) q[k] = 0.0;
+    const float meanF = s.mean(false);
+    s.init_def(C.def, sf, C.P.interpolation);
+    const float meanG = s.mean(true);
+    const float fcx = (float)s.cx, fcy = (float)s.cy;
+    float r[12];
+    for (int idx = 0; idx < s.npix; ++idx) {
+      if (s.deact[idx] || !s.active[idx]) continue;
+      const float GmF = (s.def[idx] - meanG) - (s.ref[idx] - meanF);
+      for (int k = 0; k < N; ++k) r[k] = 0.0f;
+      sf.residuals((float)s.x[idx], (float)s.y[idx], fcx, fcy, s.gx[idx], s.gy[idx], r,
+                   use_ref_grads);
+      for (int a = 0; a < N; ++a) {
+        q[a] += GmF * r[a];
+        for (int b = 0; b < N; ++b) H[a * N + b] += r[a] * r[b];
+      }
+    }
+  }
+  return 0;
+}
+
 // One Objective entry point per subset on a fresh square subset at the
 // parameters of its field row: op 0 computeUpdateFast (:430-657), op 1
 // computeUpdateRobust (:369-388), op 2 sigma (:150-184) after the subset's

@@ -50,6 +50,11 @@ int oracle_interpolate(int method, int w, int h, const float* img, const float* 
                        const float* gy, int n, const float* xy, float* out_i,
                        float* out_gx, float* out_gy);
 
+/* The Gauss-Newton system (H: n x N x N, q: n x N) of computeUpdateFast at
+ * the parameters of each (square) subset's field row, assembled once. */
+int oracle_gn_system(const dicegpu_params* params, int w, int h, const float* ref,
+                     const float* def, int n, const double* fields, double* H_out, double* q_out);
+
 /* One Objective entry point per (square) subset at the parameters of its row
  * of `fields`: op 0 computeUpdateFast, 1 computeUpdateRobust, 2 sigma. */
 int oracle_objective(const dicegpu_params* params, int w, int h, const float* ref,

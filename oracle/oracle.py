@@ -34,6 +34,8 @@ def lib():
         L.oracle_interpolate.argtypes = [ci, ci, ci, vp, vp, vp, ci, vp, vp, vp, vp]
         L.oracle_gamma.restype = ci
         L.oracle_gamma.argtypes = [P, ci, ci, vp, vp, ci, vp, vp]
+        L.oracle_gn_system.restype = ci
+        L.oracle_gn_system.argtypes = [P, ci, ci, vp, vp, ci, vp, vp, vp]
         L.oracle_objective.restype = ci
         L.oracle_objective.argtypes = [P, ci, ci, vp, vp, ci, vp, ci, vp, vp, vp, vp]
         L.oracle_default_params.restype = ci
@@ -153,3 +155,18 @@ def objective(params, ref, deff, fields, op):
                                 _ptr(it), _ptr(st), _ptr(sg), _ptr(no))
     assert rc == 0, rc
     return (sg, no) if op == 2 else (it, st)
+
+
+def gn_system(params, ref, deff, fields, nparams):
+    """(H, q) of the Gauss-Newton system at the parameters of each field row."""
+    ref = np.ascontiguousarray(ref, dtype=np.float32)
+    deff = np.ascontiguousarray(deff, dtype=np.float32)
+    f = np.ascontiguousarray(fields, dtype=np.float64)
+    h, w = ref.shape
+    n = f.shape[0]
+    H = np.zeros((n, nparams, nparams))
+    q = np.zeros((n, nparams))
+    rc = lib().oracle_gn_system(ctypes.byref(params), w, h, _ptr(ref), _ptr(deff), n, _ptr(f),
+                                _ptr(H), _ptr(q))
+    assert rc == 0, rc
+    return H, q
