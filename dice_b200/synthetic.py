@@ -102,19 +102,24 @@ def keys_sample(img, X, Y):
     return out
 
 
-def warp_image(ref, field, noise_sigma=0.0, seed=0, clip=None, iters=6):
+def warp_image(ref, field, noise_sigma=0.0, seed=0, clip=None, iters=6, block_rows=1024):
     """Deformed image def(x) = ref(X) + noise with x = X + u(X): X found by
-    fixed-point iteration X <- x - u(X).  `field(X, Y) -> (u, v)` (float64)."""
+    fixed-point iteration X <- x - u(X).  `field(X, Y) -> (u, v)` (float64).
+    Rows are processed in blocks of `block_rows` (same result, bounded
+    memory for large images)."""
     h, w = ref.shape
     dev = ref.device
-    yy, xx = torch.meshgrid(torch.arange(h, device=dev, dtype=torch.float64),
-                            torch.arange(w, device=dev, dtype=torch.float64), indexing="ij")
-    X, Y = xx.clone(), yy.clone()
-    for _ in range(iters):
-        u, v = field(X, Y)
-        X = xx - u
-        Y = yy - v
-    out = keys_sample(ref, X, Y)
+    xx = torch.arange(w, device=dev, dtype=torch.float64)
+    out = torch.empty((h, w), dtype=torch.float64, device=dev)
+    for r0 in range(0, h, block_rows):
+        r1 = min(h, r0 + block_rows)
+        yy, xb = torch.meshgrid(torch.arange(r0, r1, device=dev, dtype=torch.float64), xx, indexing="ij")
+        X, Y = xb.clone(), yy.clone()
+        for _ in range(iters):
+            u, v = field(X, Y)
+            X = xb - u
+            Y = yy - v
+        out[r0:r1] = keys_sample(ref, X, Y)
     if noise_sigma > 0:
         g = _gen(seed, dev)
         out = out + noise_sigma * torch.randn(out.shape, generator=g, dtype=torch.float64).to(dev)
@@ -263,6 +268,32 @@ def config5_field(h, jump=2.0, strain=0.003):
         v = strain * Y + torch.where(Y >= yc, torch.full_like(Y, jump / 2.0), torch.full_like(Y, -jump / 2.0))
         return u, v
     return f
+
+
+def config3(device="cpu", w=4096, h=3000, n=50000, seed=3, noise_sigma=1.0):
+    """4096 x 3000 speckle pair under a 1.5 degree rotation about the centre
+    plus 0.5 % shear, and `n` seeded mixed subsets (mixed_subsets).  Returns
+    (ref, def, field, subsets) with subsets = (cx, cy, offsets, px, py, kind,
+    minor_extent)."""
+    ref = speckle_image(w, h, seed=seed, r_min=2.0, r_max=4.0, grey_lo=20.0, grey_hi=230.0,
+                        blur_sigma=0.8, device=device)
+    field = config3_field(w, h)
+    deff = warp_image(ref, field, noise_sigma=noise_sigma, seed=seed + 300, clip=(0.0, 255.0))
+    return ref, deff, field, mixed_subsets(w, h, n, seed=seed + 30)
+
+
+def config5(device="cpu", w=8192, h=8192, nframes=8, jump=2.0, strain=0.003, count=None, seed=5,
+            noise_sigma=1.0):
+    """8192^2 speckle sequence of a mode-I crack: frame k (1..nframes) opens
+    the jump across y = h/2 to jump * k / nframes px on top of a linear far
+    field of strain * k / nframes.  Returns (ref, first `count` frames)."""
+    ref = speckle_image(w, h, seed=seed, r_min=2.0, r_max=4.0, grey_lo=20.0, grey_hi=230.0,
+                        blur_sigma=0.8, device=device)
+    count = nframes if count is None else count
+    frames = [warp_image(ref, config5_field(h, jump * (k + 1) / nframes, strain * (k + 1) / nframes),
+                         noise_sigma=noise_sigma, seed=seed + 500 + k, clip=(0.0, 255.0))
+              for k in range(count)]
+    return ref, frames
 
 
 def config4(device="cpu", w=1024, h=1024, ncontrol=16, ctrl_sigma=0.8, noise_sigma=1.0, seed=4):

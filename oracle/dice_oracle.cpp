@@ -758,7 +758,20 @@ static int compute_update_fast(const Ctx& C, Subset& s, ShapeFn& sf, int& num_it
     num_iterations = solve_it;
     s.init_def(C.def, sf, C.P.interpolation);
     if (cnt) cnt->gn_iters++;
+#ifdef ORACLE_DEF_MEAN_FP64
+    // sensitivity variant (not the reference): the deformed mean summed in
+    // double, the rounding a compiler or library change could also bring
+    float meanG = 0.0f;
+    {
+      double m = 0.0;
+      int na = 0;
+      for (int i = 0; i < s.npix; ++i)
+        if (s.active[i] && !s.deact[i]) { m += s.def[i]; ++na; }
+      meanG = na ? (float)(m / na) : 0.0f;
+    }
+#else
     const float meanG = s.mean(true);
+#endif
     for (int i = 0; i < N * N; ++i) H[i] = 0.0;
     for (int i = 0; i < N; ++i) q[i] = 0.0;
     for (int idx = 0; idx < s.npix; ++idx) {

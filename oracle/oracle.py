@@ -16,6 +16,25 @@ LIB_PATH = os.path.join(_HERE, "libdiceoracle.so")
 _lib = None
 
 
+class use_library:
+    """Context manager: route the oracle calls to another build of it (for
+    instance libdiceoracle_meanfp64.so, the rounding-sensitivity variant)."""
+
+    def __init__(self, name):
+        self.path = os.path.join(_HERE, name)
+
+    def __enter__(self):
+        global LIB_PATH, _lib
+        self._saved = (LIB_PATH, _lib)
+        LIB_PATH, _lib = self.path, None
+        return self
+
+    def __exit__(self, *exc):
+        global LIB_PATH, _lib
+        LIB_PATH, _lib = self._saved
+        return False
+
+
 def lib():
     global _lib
     if _lib is None:
