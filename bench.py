@@ -233,6 +233,349 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _line(metric, value, unit, world, args, ms_per_step, config, **extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded speckle images)",
+            "config": config}
+    line.update(extra)
+    return line
+
+
+def _timed(fn, steps, warmup, stream, flush=None):
+    """Runs fn() warmup + steps times; CUDA-event milliseconds of the timed runs."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        if flush is not None:
+            flush_l2(flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        ms.append((a, b))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ms]
+
+
+def run_crack(args):
+    """8192^2 mode-I crack sequence (8 frames, 21x21 affine subsets at step 4,
+    ~4.15M subsets): the frame loop as one CUDA graph of persistent
+    work-stealing launches; status flags compared with the oracle on the
+    subsets around the crack and a strided sample elsewhere, every frame."""
+    import torch
+    from dice_b200 import abi, synthetic as syn
+    from dice_b200.schema import Schema
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    size, nf, ss, step = args.crack_size, 8, 21, 4
+    ref, frames = syn.config5(device=dev, w=size, h=size, nframes=nf)
+    torch.cuda.synchronize()
+    cx, cy = syn.grid_points(size, size, ss, step)
+    n = len(cx)
+    p = abi.default_params(subset_size=ss, enable_rotation=1, enable_normal_strain=1, enable_shear_strain=1,
+                           final_gamma_threshold=0.02)
+    f0 = syn.init_fields(cx, cy)
+    f0_dev = torch.from_numpy(f0).to(dev)
+    stream = torch.cuda.current_stream()
+    s = Schema(p, stream=stream)
+    s.set_ref_image(ref)
+    s.set_fields(f0)
+    s.capture_sequence(frames, reset_fields=f0_dev)
+    launches0 = s.launch_count()
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier(world)
+    clocks.start()
+    ms = _timed(s.launch_sequence, args.steps, args.warmup, stream)
+    barrier(world)
+    clocks.stop()
+    per_launch = (s.launch_count() - launches0) / max(1, args.steps + args.warmup)
+    total_ms = max_over_ranks(sum(ms), world)
+    value = n * nf * args.steps * world / (total_ms / 1000.0)
+    final = s.fields()
+    st_final = final[:, abi.F_STATUS]
+    cpu = flags = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        near = np.nonzero(np.abs(cy - size / 2.0) <= 30)[0]
+        far = np.arange(0, n, 997)
+        ids = np.union1d(near, far)
+        ref_h = ref.cpu().numpy()
+        fo = syn.init_fields(cx[ids], cy[ids])
+        fdev = torch.empty((n, abi.FIELD_STRIDE), dtype=torch.float64, device=dev)
+        idt = torch.from_numpy(ids).to(dev)
+        s.load_fields(f0_dev)
+        mism = 0
+        failed = []
+        du = 0.0
+        dt = 0.0
+        cores = os.cpu_count() or 1
+        for k in range(nf):
+            s.set_def_image(frames[k])
+            s.execute_correlation()
+            s.store_fields(fdev)
+            g = fdev.index_select(0, idt).cpu().numpy()
+            fr_h = frames[k].cpu().numpy()
+            t0 = time.perf_counter()
+            O.execute_frame(p, ref_h, fr_h, fo, first_frame=(k == 0), nthreads=cores,
+                            uncertainty=np.zeros((len(ids), abi.UNCERTAINTY_STRIDE)))
+            dt += time.perf_counter() - t0
+            mism += int(np.sum(g[:, abi.F_STATUS] != fo[:, abi.F_STATUS]))
+            failed.append(int(np.sum(fo[:, abi.F_STATUS] >= 2)))
+            both = (g[:, abi.F_STATUS] < 2) & (fo[:, abi.F_STATUS] < 2) & \
+                   (g[:, abi.F_ITERATIONS] <= p.max_solver_iterations_fast) & \
+                   (fo[:, abi.F_ITERATIONS] <= p.max_solver_iterations_fast)
+            du = max(du, float(np.max(np.abs(g[both, abi.F_DISP_Y] - fo[both, abi.F_DISP_Y]), initial=0.0)))
+        flags = {"subsets": int(len(ids)), "frames": nf, "status_mismatches": mism,
+                 "oracle_failed_per_frame": failed, "max_abs_dv_px_gauss_newton_both": du,
+                 "sample": "all subsets within 30 px of the crack line plus every 997th subset"}
+        cpu = {"value": len(ids) * nf / dt, "unit": "subsets/s", "cores": cores, "kind": "port",
+               "sample": "the %d flag-check subsets through %d frames, %.1f s, uncertainty fields on"
+                         % (len(ids), nf, dt)}
+    if rank == 0:
+        cfg = {"workload": "%dx%d crack sequence, %d frames, 21x21 affine subsets at step 4" % (size, size, nf),
+               "subsets_per_frame": n, "frames": nf, "tolerance": p.fast_solver_tolerance,
+               "final_gamma_threshold": 0.02, "frame_loop": "one CUDA graph per sequence",
+               "l2": "inputs larger than L2 (8 frames x %d MB)" % (size * size * 4 >> 20),
+               "parallelism": "replicas x%d" % world}
+        print(json.dumps(_line("subset solves/sec, crack sequence", value, "subsets/s", world, args,
+                               total_ms / args.steps, cfg, cpu_baseline=cpu, flags_vs_oracle=flags,
+                               gpu_launches=int(per_launch * args.steps), clocks=clocks.summary(),
+                               accuracy={"status_counts_last_frame": {str(int(a)): int(b) for a, b in
+                                                                      zip(*np.unique(st_final, return_counts=True))}})),
+              flush=True)
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_mixed(args):
+    """4096x3000 arbitrary-shape batching: 50k seeded circles, thin ellipses
+    and convex polygons under rotation plus shear.  Subsets with a minor
+    extent of 10 px or more run quadratic Gauss-Newton over their pixel
+    lists; thinner ones run the simplex (FORCE_SIMPLEX) in an affine
+    context.  The launch shape (subsets in flight per CTA, CTAs per SM) is
+    swept for each context and the fastest is used."""
+    import torch
+    from dice_b200 import abi, synthetic as syn
+    from dice_b200.schema import Schema
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    w, h, nsub = 4096, 3000, 50000
+    ref, deff, field, sub = syn.config3(device=dev, w=w, h=h, n=nsub)
+    cx, cy, offs, px, py, kind, minor = sub
+    u0, v0 = field(torch.from_numpy(cx.astype(np.float64)).to(dev), torch.from_numpy(cy.astype(np.float64)).to(dev))
+    u0, v0 = np.round(u0.cpu().numpy()), np.round(v0.cpu().numpy())
+
+    def select(idx):
+        no, lx, ly = [0], [], []
+        for i in idx:
+            lx.append(px[offs[i]:offs[i + 1]])
+            ly.append(py[offs[i]:offs[i + 1]])
+            no.append(no[-1] + offs[i + 1] - offs[i])
+        return np.asarray(no, np.int32), np.concatenate(lx), np.concatenate(ly)
+
+    thin = minor < 10.0
+    groups = []
+    stream = torch.cuda.current_stream()
+    iq = np.nonzero(~thin)[0]
+    pq = abi.default_params(shape_function=abi.QUADRATIC_SF, subset_size=0, fast_solver_tolerance=1e-3)
+    fq = syn.init_fields(cx[iq], cy[iq], quadratic=True)
+    fq[:, abi.F_QUAD_A + 5] = u0[iq]
+    fq[:, abi.F_QUAD_A + 11] = v0[iq]
+    groups.append(("quadratic_gauss_newton", iq, pq, fq, None))
+    it = np.nonzero(thin)[0]
+    ps = abi.default_params(subset_size=0, enable_rotation=1)
+    fs = syn.init_fields(cx[it], cy[it])
+    fs[:, abi.F_DISP_X] = u0[it]
+    fs[:, abi.F_DISP_Y] = v0[it]
+    groups.append(("forced_simplex", it, ps, fs, np.ones(len(it), np.uint8)))
+    ctxs = []
+    sweep = {}
+    for name, idx, pp, ff, force in groups:
+        sc = Schema(pp, stream=stream)
+        sc.set_ref_image(ref)
+        sc.set_fields(ff)
+        sc.set_subset_pixels(*select(idx))
+        if force is not None:
+            sc.set_force_simplex(force)
+        sc.set_def_image(deff)
+        fdev = torch.from_numpy(ff).to(dev)
+        times = {}
+        for shape in ((8, 0), (4, 0), (2, 0), (8, 1), (4, 2), (4, 3)):
+            sc.set_launch_shape(*shape)
+
+            def once(sc=sc, fdev=fdev):
+                sc.load_fields(fdev)
+                sc.execute_correlation()
+            times["%dx%d" % shape] = statistics.median(_timed(once, 2, 1, stream))
+        best = min(times, key=times.get)
+        sc.set_launch_shape(*[int(t) for t in best.split("x")])
+        sweep[name] = {"ms_by_warps_x_ctas_per_sm": times, "chosen": best,
+                       "library_autotune": list(sc.autotune())}
+        ctxs.append((name, idx, pp, ff, force, sc, fdev))
+
+    def step():
+        for name, idx, pp, ff, force, sc, fdev in ctxs:
+            sc.load_fields(fdev)
+            sc.execute_correlation()
+
+    launches0 = sum(c[5].launch_count() for c in ctxs)
+    clocks = ClockSampler(torch.cuda.current_device())
+    l2 = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    barrier(world)
+    clocks.start()
+    ms = _timed(step, args.steps, args.warmup, stream, flush=l2)
+    barrier(world)
+    clocks.stop()
+    launches = sum(c[5].launch_count() for c in ctxs) - launches0
+    total_ms = max_over_ranks(sum(ms), world)
+    value = nsub * args.steps * world / (total_ms / 1000.0)
+    acc, par = {}, {}
+    cpu = None
+    dt_cpu, n_cpu = 0.0, 0
+    for name, idx, pp, ff, force, sc, fdev in ctxs:
+        g = sc.fields()
+        st = g[:, abi.F_STATUS]
+        acc[name] = {"subsets": int(len(idx)), "converged_frac": float(np.mean(st < 2)),
+                     "simplex_fallback_frac": float(np.mean((st < 2) & (g[:, abi.F_ITERATIONS] >
+                                                                        pp.max_solver_iterations_fast)))
+                     if force is None else None}
+        if rank == 0 and world == 1 and not args.no_cpu:
+            from oracle import oracle as O
+            sel = np.arange(0, len(idx), 25)
+            no, lx, ly = select(idx[sel])
+            fo = ff[sel].copy()
+            t0 = time.perf_counter()
+            O.execute_frame(pp, ref.cpu().numpy(), deff.cpu().numpy(), fo, first_frame=True,
+                            nthreads=os.cpu_count() or 1, offsets=no, px=lx, py=ly,
+                            force_simplex=None if force is None else force[sel],
+                            uncertainty=np.zeros((len(sel), abi.UNCERTAINTY_STRIDE)))
+            dt_cpu += time.perf_counter() - t0
+            n_cpu += len(sel)
+            gs = g[sel]
+            both = (gs[:, abi.F_STATUS] < 2) & (fo[:, abi.F_STATUS] < 2)
+            if force is None:
+                both &= (gs[:, abi.F_ITERATIONS] <= pp.max_solver_iterations_fast) & \
+                        (fo[:, abi.F_ITERATIONS] <= pp.max_solver_iterations_fast)
+            par[name] = {"subsets": int(len(sel)),
+                         "status_equal_frac": float(np.mean(gs[:, abi.F_STATUS] == fo[:, abi.F_STATUS])),
+                         "compared": int(both.sum()),
+                         "max_abs_du_px": float(np.max(np.abs(gs[both, abi.F_DISP_X] - fo[both, abi.F_DISP_X]),
+                                                       initial=0.0)),
+                         "max_abs_dv_px": float(np.max(np.abs(gs[both, abi.F_DISP_Y] - fo[both, abi.F_DISP_Y]),
+                                                       initial=0.0))}
+    if n_cpu:
+        cpu = {"value": n_cpu / dt_cpu, "unit": "subsets/s", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": "every 25th subset of each group (%d), %.1f s, uncertainty fields on" % (n_cpu, dt_cpu)}
+    if rank == 0:
+        cfg = {"workload": "4096x3000 mixed conformal subsets (circles r 7-25, 60x8 ellipses, convex polygons)",
+               "subsets": nsub, "groups": {k: v["subsets"] for k, v in acc.items()},
+               "quadratic_tolerance": 1e-3,
+               "tolerance_note": "1e-3: mapped coordinates up to 4096 px are spaced 4.9e-4 px in float",
+               "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas x%d" % world}
+        print(json.dumps(_line("subset solves/sec, mixed arbitrary-shape subsets", value, "subsets/s", world,
+                               args, total_ms / args.steps, cfg, cpu_baseline=cpu, launch_shape_sweep=sweep,
+                               parity_vs_oracle=par, accuracy=acc, gpu_launches=int(launches),
+                               clocks=clocks.summary())), flush=True)
+    for c in ctxs:
+        c[5].close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+ADJ_FLOP_PER_PIXEL = 560.0
+
+
+def run_adjoint(args):
+    """1024^2 pair with a 16x16 cubic B-spline field: the adjoint of the
+    subset objective (gamma, d/dparams, d/d deformed image) for 19,600
+    affine 25x25 subsets per step, then the B-spline control grid fitted by
+    gradient descent through it and compared with per-subset Gauss-Newton."""
+    import torch
+    from dice_b200 import abi, bspline, synthetic as syn
+    from dice_b200.schema import Schema
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    size = 1024
+    ref, deff, field, ctrl = syn.config4(device=dev, w=size, h=size)
+    cx, cy = syn.grid_points(size, size, 25, 7)
+    n = len(cx)
+    p = abi.default_params(subset_size=25, enable_rotation=1, enable_normal_strain=1, enable_shear_strain=1,
+                           fast_solver_tolerance=1e-5)
+    stream = torch.cuda.current_stream()
+    s = Schema(p, stream=stream)
+    s.set_ref_image(ref)
+    s.set_subsets(cx, cy)
+    s.set_def_image(deff)
+    tcx, tcy = torch.from_numpy(cx).to(dev), torch.from_numpy(cy).to(dev)
+    rows = torch.from_numpy(syn.init_fields(cx, cy)).to(dev)
+    rows[:, abi.F_DISP_X:abi.F_DISP_X + 6] = field.subset_params(ctrl, tcx, tcy)
+    rows = rows.contiguous()
+    seed = torch.ones(n, dtype=torch.float64, device=dev)
+    ddef = torch.zeros((size, size), dtype=torch.float32, device=dev)
+    l2 = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        ddef.zero_()
+        s.adjoint(rows, seed=seed, ddef=ddef)
+
+    launches0 = s.launch_count()
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier(world)
+    clocks.start()
+    ms = _timed(step, args.steps, args.warmup, stream, flush=l2)
+    barrier(world)
+    clocks.stop()
+    launches = s.launch_count() - launches0
+    total_ms = max_over_ranks(sum(ms), world)
+    value = n * args.steps * world / (total_ms / 1000.0)
+    val, _ = s.adjoint(rows)
+    torch.cuda.synchronize()
+    active = float(n * 625)
+    achieved = active * ADJ_FLOP_PER_PIXEL / (statistics.median(ms) / 1000.0) / 1e12
+    peak = fp32_peak_tflops(dev)
+    # per-subset Gauss-Newton, then the B-spline fit through the adjoint
+    s.execute_correlation()
+    gn = s.fields()
+    t0 = time.perf_counter()
+    fit = bspline.fit(s, deff, field, tcx, tcy, iters=args.fit_iters, lr=0.05)
+    torch.cuda.synchronize()
+    fit_s = time.perf_counter() - t0
+    ut, vt = field.eval(ctrl, tcx, tcy)
+    uf, vf = field.eval(fit, tcx, tcy)
+    ok = torch.from_numpy(gn[:, abi.F_STATUS] < 2).to(dev)
+    ug = torch.from_numpy(gn[:, abi.F_DISP_X]).to(dev)
+    vg = torch.from_numpy(gn[:, abi.F_DISP_Y]).to(dev)
+    fit_res = {"iterations": args.fit_iters, "seconds": fit_s, "control_grid": [2, 16, 16],
+               "rms_error_fit_px": bspline.rms(torch.cat([(uf - ut)[ok], (vf - vt)[ok]])),
+               "rms_error_gauss_newton_px": bspline.rms(torch.cat([(ug - ut)[ok], (vg - vt)[ok]])),
+               "rms_fit_minus_gauss_newton_px": bspline.rms(torch.cat([(uf - ug)[ok], (vf - vg)[ok]])),
+               "gauss_newton_converged_frac": float(ok.float().mean())}
+    if rank == 0:
+        cfg = {"workload": "1024x1024 B-spline field pair, 19,600 affine 25x25 subsets at step 7",
+               "subsets": n, "outputs": "gamma, d/dparams (6), d/d deformed image (atomic scatter)",
+               "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas x%d" % world}
+        roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None, "traffic": None,
+                "per_unit": "%d FP32 flop per subset pixel (both passes) plus 36 atomic adds" % ADJ_FLOP_PER_PIXEL,
+                "kernel": "adjoint_kernel (median step incl. clearing the image derivative)"}
+        print(json.dumps(_line("subset objective adjoints/sec (value, d/dparams, d/dimage)", value, "subsets/s",
+                               world, args, total_ms / args.steps, cfg, roofline=roof,
+                               cpu_baseline={"value": None, "note": "the reference has no derivative code"},
+                               bspline_fit=fit_res, mean_gamma=float(val.mean()),
+                               gpu_launches=int(launches), clocks=clocks.summary())), flush=True)
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def flush_l2(buf):
     buf.zero_()
 
@@ -251,9 +594,18 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--warps", type=int, default=0)
     ap.add_argument("--ctas", type=int, default=0)
+    ap.add_argument("--workload", default="sequence", choices=["sequence", "crack", "mixed", "adjoint"],
+                    help="sequence: the 2048^2 ten-frame sequence (default, the headline); crack: the "
+                         "8192^2 crack sequence; mixed: arbitrary-shape subsets; adjoint: objective "
+                         "derivatives and the B-spline fit")
+    ap.add_argument("--crack-size", type=int, default=8192)
+    ap.add_argument("--fit-iters", type=int, default=300)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload != "sequence":
+        {"crack": run_crack, "mixed": run_mixed, "adjoint": run_adjoint}[args.workload](args)
         return
     import torch
     from dice_b200 import abi, synthetic as syn
