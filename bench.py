@@ -329,7 +329,20 @@ def run_crack(args):
                    (g[:, abi.F_ITERATIONS] <= p.max_solver_iterations_fast) & \
                    (fo[:, abi.F_ITERATIONS] <= p.max_solver_iterations_fast)
             du = max(du, float(np.max(np.abs(g[both, abi.F_DISP_Y] - fo[both, abi.F_DISP_Y]), initial=0.0)))
+        # the same sample through the oracle built with one rounding change
+        # (the deformed mean summed in double): how far the reference's own
+        # flags move between builds on these subsets
+        fv = syn.init_fields(cx[ids], cy[ids])
+        fb = syn.init_fields(cx[ids], cy[ids])
+        var_mism = 0
+        for k in range(nf):
+            fr_h = frames[k].cpu().numpy()
+            O.execute_frame(p, ref_h, fr_h, fb, first_frame=(k == 0), nthreads=cores)
+            with O.use_library("libdiceoracle_meanfp64.so"):
+                O.execute_frame(p, ref_h, fr_h, fv, first_frame=(k == 0), nthreads=cores)
+            var_mism += int(np.sum(fv[:, abi.F_STATUS] != fb[:, abi.F_STATUS]))
         flags = {"subsets": int(len(ids)), "frames": nf, "status_mismatches": mism,
+                 "oracle_build_variant_status_mismatches": var_mism,
                  "oracle_failed_per_frame": failed, "max_abs_dv_px_gauss_newton_both": du,
                  "sample": "all subsets within 30 px of the crack line plus every 997th subset"}
         cpu = {"value": len(ids) * nf / dt, "unit": "subsets/s", "cores": cores, "kind": "port",
@@ -599,7 +612,7 @@ def main():
                          "8192^2 crack sequence; mixed: arbitrary-shape subsets; adjoint: objective "
                          "derivatives and the B-spline fit")
     ap.add_argument("--crack-size", type=int, default=8192)
-    ap.add_argument("--fit-iters", type=int, default=300)
+    ap.add_argument("--fit-iters", type=int, default=2000)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
