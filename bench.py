@@ -59,12 +59,14 @@ def params():
                               max_solver_iterations_fast=25)
 
 
-def workload_config(n_subsets, n_gpus):
+def workload_config(n_subsets, n_gpus, sharded=False):
     return {"workload": "2048x2048 16-bit speckle sequence, 10 frames, 31x31 affine subsets at step 5",
             "image": [W, H], "subset_size": SUBSET, "step": STEP, "subsets_per_frame": n_subsets,
             "frames": NFRAMES, "shape_function": "affine (6 params)", "interpolation": "keys_fourth",
             "optimization": "gradient_based_then_simplex", "tolerance": 1e-5, "max_iterations": 25,
-            "parallelism": "replicas x%d (independent subsets, no collective)" % n_gpus,
+            "parallelism": ("dp%d: balanced contiguous subset ranges, NCCL all-gather of the field rows "
+                            "at frame end" % n_gpus) if sharded else
+                           "replicas x%d (independent subsets, no collective)" % n_gpus,
             "l2": "flushed between timed steps (256 MiB write)"}
 
 
@@ -613,6 +615,9 @@ def main():
                          "derivatives and the B-spline fit")
     ap.add_argument("--crack-size", type=int, default=8192)
     ap.add_argument("--fit-iters", type=int, default=2000)
+    ap.add_argument("--shard", action="store_true",
+                    help="sequence workload: split the subsets over the ranks (strong scaling) "
+                         "instead of running replicas")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -630,6 +635,15 @@ def main():
     ref, frames = syn.config2(device=dev, nframes=NFRAMES)
     torch.cuda.synchronize()
     cx, cy = syn.grid_points(W, H, SUBSET, STEP)
+    n_total = len(cx)
+    # --shard: this rank's balanced contiguous range of the subsets, and an
+    # all-gather of the field rows at the end of every frame (strong
+    # scaling); otherwise every rank runs the whole frame (replicas)
+    sharded = args.shard and world > 1
+    if sharded:
+        from dice_b200 import shard
+        starts = shard.partition(np.full(n_total, float(SUBSET * SUBSET)), world)
+        cx, cy = cx[starts[rank]:starts[rank + 1]], cy[starts[rank]:starts[rank + 1]]
     n = len(cx)
     f0 = syn.init_fields(cx, cy)
     stream = torch.cuda.current_stream()
@@ -645,6 +659,7 @@ def main():
     lib = s.lib
 
     state = {"frame": 0}
+    local_rows = torch.empty((n, abi.FIELD_STRIDE), dtype=torch.float64, device=dev) if sharded else None
 
     def step_device():
         k = state["frame"]
@@ -652,6 +667,9 @@ def main():
             s.load_fields(f0_dev)   # sequence restart: zero motion, frame 0
         s.set_def_image(frames[k])
         s.execute_correlation()
+        if sharded:
+            s.store_fields(local_rows)
+            state["gathered"] = shard.gather_rows(local_rows, starts)
         state["frame"] = (k + 1) % NFRAMES
 
     # warm-up (first frame includes the field-of-view test path)
@@ -680,7 +698,7 @@ def main():
     launches = s.launch_count() - launches0
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = max_over_ranks(sum(step_ms), world)
-    value = n * args.steps * world / (total_ms / 1000.0)
+    value = (n_total if sharded else n * world) * args.steps / (total_ms / 1000.0)
 
     # accuracy of the last timed frame
     fl = s.fields()
@@ -707,7 +725,7 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = [a.elapsed_time(b) for a, b in e2e_ev[2:]]
     e2e_total = max_over_ranks(sum(e2e_ms), world)
-    e2e_value = n * len(e2e_ms) * world / (e2e_total / 1000.0)
+    e2e_value = (n_total if sharded else n * world) * len(e2e_ms) / (e2e_total / 1000.0)
 
     # plain path (one launch per subset) on a sample of subsets
     plain = None
@@ -822,8 +840,9 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-                "data": "synthetic (seeded speckle sequence)", "config": workload_config(n, world),
+                "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f32+f64",
+                "data": "synthetic (seeded speckle sequence)",
+                "config": workload_config(n_total, world, sharded),
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": W * H * 4,
                         "d2h_bytes_per_step": nbytes_fields},
