@@ -615,6 +615,9 @@ def main():
                          "derivatives and the B-spline fit")
     ap.add_argument("--crack-size", type=int, default=8192)
     ap.add_argument("--fit-iters", type=int, default=2000)
+    ap.add_argument("--profile-timed", action="store_true",
+                    help="sequence workload: bracket the timed steps with cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off)")
     ap.add_argument("--shard", action="store_true",
                     help="sequence workload: split the subsets over the ranks (strong scaling) "
                          "instead of running replicas")
@@ -687,12 +690,16 @@ def main():
     iters_total = 0.0
     npix = SUBSET * SUBSET
     fields_seen = []
+    if args.profile_timed:
+        torch.cuda.cudart().cudaProfilerStart()
     for i in range(args.steps):
         flush_l2(l2_buf)
         ev[i][0].record(stream)
         step_device()
         ev[i][1].record(stream)
     torch.cuda.synchronize()
+    if args.profile_timed:
+        torch.cuda.cudart().cudaProfilerStop()
     barrier(world)
     clocks.stop()
     launches = s.launch_count() - launches0
