@@ -173,6 +173,9 @@ def cpu_sample(p, ref, frames, n_sample, nthreads, timed_frames=1):
 
 
 SIMPLEX_FLOP_PER_PIXEL_EVAL = 200.0
+# DRAM bytes (read + write) of one frame_kernel launch of this sequence, from
+# the ncu capture summarised in profiles/frame_kernel_2048x2048_31px_step5.md
+FRAME_KERNEL_DRAM_BYTES = 258.5e6 + 1949.2e6
 
 
 def oracle_sequence_sample(p, ref_h, frames_h, stride, nthreads):
@@ -838,7 +841,11 @@ def main():
         pass
     fp32_peak = fp32_peak_tflops(dev)
     roof = {"bound": "fp32", "achieved": fp32_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
-            "frac": fp32_tflops / fp32_peak if (fp32_peak and fp32_tflops) else None, "traffic": None,
+            "frac": fp32_tflops / fp32_peak if (fp32_peak and fp32_tflops) else None,
+            "traffic": FRAME_KERNEL_DRAM_BYTES,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                              "profiles/frame_kernel_2048x2048_31px_step5.md (writes are local-memory "
+                              "write-backs; reads 258.5 MB)",
             "kernel": "frame_kernel (median step time incl. the gradient and pack kernels)",
             "peak_source": "measured FP32 SGEMM on CUDA cores (TF32 off) in this run",
             "per_unit": "390 FP32 flop per active pixel per Gauss-Newton pass + 200 per simplex evaluation, "
