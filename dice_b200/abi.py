@@ -39,6 +39,7 @@ F_QUAD_A = 8
 F_SIGMA, F_GAMMA, F_BETA, F_NOISE, F_CONTRAST = 20, 21, 22, 23, 24
 F_ACTIVE_PIXELS, F_STATUS, F_ITERATIONS, F_MATCH, F_CONDITION, F_OMEGA = 25, 26, 27, 28, 29, 30
 API_STRIDE = 9
+PIXEL_F32, PIXEL_U8, PIXEL_U16 = 0, 1, 2
 UNCERTAINTY_STRIDE = 8
 
 ERR_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_STATE", -4: "ERR_NOMEM",
@@ -155,6 +156,8 @@ def _declare(lib):
         "dicegpu_set_stream": (c_int, [c_void_p, c_void_p]),
         "dicegpu_set_ref_image": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int]),
         "dicegpu_set_def_image": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int]),
+        "dicegpu_set_ref_image_typed": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_int]),
+        "dicegpu_set_def_image_typed": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_int]),
         "dicegpu_set_subsets": (c_int, [c_void_p, c_int, c_void_p]),
         "dicegpu_set_subset_pixels": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "dicegpu_set_force_simplex": (c_int, [c_void_p, c_int, c_void_p]),

@@ -609,11 +609,46 @@ static int upload_image(dicegpu_ctx* c, float* dst, const float* src, int on_dev
   return DICEGPU_OK;
 }
 
-extern "C" int dicegpu_set_ref_image(dicegpu_ctx* c, int w, int h, const float* pixels, int on_device) {
+// 8- and 16-bit pixels become floats of the same value, as the reference's
+// image readers store them (DICe_ImageIO.cpp:480-490).
+template <typename T>
+__global__ void convert_kernel(size_t n, const T* __restrict__ in, float* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (float)in[i];
+}
+
+// Integer pixels: the raw bytes are staged in the second scratch plane, the
+// conversion writes the first (then the optional filter) or the destination.
+static int upload_typed(dicegpu_ctx* c, float* dst, const void* src, int type, int on_device) {
+  if (type == DICEGPU_PIXEL_F32) return upload_image(c, dst, (const float*)src, on_device);
+  if (type != DICEGPU_PIXEL_U8 && type != DICEGPU_PIXEL_U16) return DICEGPU_ERR_ARG;
+  const size_t npx = (size_t)c->W * c->H;
+  const size_t esz = type == DICEGPU_PIXEL_U8 ? 1 : 2;
+  const void* raw = src;
+  if (!on_device) {
+    void* stage = (void*)(c->d_tmp + npx);
+    CK(cudaMemcpyAsync(stage, src, npx * esz, cudaMemcpyHostToDevice, c->stream));
+    raw = stage;
+  }
+  float* conv = c->params.gauss_filter_images ? c->d_tmp : dst;
+  const unsigned blocks = (unsigned)((npx + 255) / 256);
+  if (type == DICEGPU_PIXEL_U8)
+    convert_kernel<uint8_t><<<blocks, 256, 0, c->stream>>>(npx, (const uint8_t*)raw, conv);
+  else
+    convert_kernel<uint16_t><<<blocks, 256, 0, c->stream>>>(npx, (const uint16_t*)raw, conv);
+  CK(cudaGetLastError());
+  c->launches += 1;
+  if (c->params.gauss_filter_images)
+    return launch_gauss_filter(c->W, c->H, c->params.gauss_filter_mask_size, conv, dst, c->stream,
+                               &c->launches);
+  return DICEGPU_OK;
+}
+
+static int set_ref(dicegpu_ctx* c, int w, int h, const void* pixels, int type, int on_device) {
   if (!c || !pixels || w < 16 || h < 16) return DICEGPU_ERR_ARG;
   int rc = ensure_images(c, w, h);
   if (rc) return rc;
-  if ((rc = upload_image(c, c->d_ref, pixels, on_device))) return rc;
+  if ((rc = upload_typed(c, c->d_ref, pixels, type, on_device))) return rc;
   if ((rc = launch_gradients(w, h, c->d_ref, c->d_ref_gx, c->d_ref_gy, c->params.gradient_method,
                              c->d_tmp, c->stream, &c->launches)))
     return rc;
@@ -621,12 +656,12 @@ extern "C" int dicegpu_set_ref_image(dicegpu_ctx* c, int w, int h, const float* 
   return DICEGPU_OK;
 }
 
-extern "C" int dicegpu_set_def_image(dicegpu_ctx* c, int w, int h, const float* pixels, int on_device) {
+static int set_def(dicegpu_ctx* c, int w, int h, const void* pixels, int type, int on_device) {
   if (!c || !pixels) return DICEGPU_ERR_ARG;
   if (!c->has_ref) return DICEGPU_ERR_STATE;
   if (w != c->W || h != c->H) return DICEGPU_ERR_ARG;
   int rc;
-  if ((rc = upload_image(c, c->d_def, pixels, on_device))) return rc;
+  if ((rc = upload_typed(c, c->d_def, pixels, type, on_device))) return rc;
   if (c->params.use_def_gradients) {
     if ((rc = launch_gradients(w, h, c->d_def, c->d_def_gx, c->d_def_gy, c->params.gradient_method,
                                c->d_tmp, c->stream, &c->launches)))
@@ -639,6 +674,21 @@ extern "C" int dicegpu_set_def_image(dicegpu_ctx* c, int w, int h, const float* 
   }
   c->has_def = true;
   return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_ref_image(dicegpu_ctx* c, int w, int h, const float* pixels, int on_device) {
+  return set_ref(c, w, h, pixels, DICEGPU_PIXEL_F32, on_device);
+}
+extern "C" int dicegpu_set_def_image(dicegpu_ctx* c, int w, int h, const float* pixels, int on_device) {
+  return set_def(c, w, h, pixels, DICEGPU_PIXEL_F32, on_device);
+}
+extern "C" int dicegpu_set_ref_image_typed(dicegpu_ctx* c, int w, int h, const void* pixels, int pixel_type,
+                                           int on_device) {
+  return set_ref(c, w, h, pixels, pixel_type, on_device);
+}
+extern "C" int dicegpu_set_def_image_typed(dicegpu_ctx* c, int w, int h, const void* pixels, int pixel_type,
+                                           int on_device) {
+  return set_def(c, w, h, pixels, pixel_type, on_device);
 }
 
 template <typename T>

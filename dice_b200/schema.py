@@ -81,6 +81,25 @@ class Schema:
 
     # ---- images ---------------------------------------------------------------
     def _image_call(self, fn, img, what):
+        # 8- and 16-bit images go through the typed entry points (converted on
+        # the device, the raw bytes are what crosses PCIe)
+        typed = {"uint8": abi.PIXEL_U8, "uint16": abi.PIXEL_U16}
+        dt = str(img.dtype).replace("torch.", "")
+        if dt in typed:
+            tfn = self.lib.dicegpu_set_ref_image_typed if "ref" in what else self.lib.dicegpu_set_def_image_typed
+            if _is_cuda_tensor(img):
+                t = img.contiguous()
+                self._keep.append(t)
+                h, w = t.shape
+                rc = tfn(self.ctx, w, h, ctypes.c_void_p(t.data_ptr()), typed[dt], 1)
+            else:
+                a = np.ascontiguousarray(img)
+                self._keep.append(a)
+                h, w = a.shape
+                rc = tfn(self.ctx, w, h, a.ctypes.data_as(ctypes.c_void_p), typed[dt], 0)
+            abi.check(rc, what)
+            self.w, self.h = w, h
+            return
         if _is_cuda_tensor(img):
             t = img.contiguous().float()
             h, w = t.shape

@@ -199,6 +199,20 @@ int dicegpu_set_stream(dicegpu_ctx* ctx, void* stream);
 int dicegpu_set_ref_image(dicegpu_ctx* ctx, int w, int h, const float* pixels, int on_device);
 int dicegpu_set_def_image(dicegpu_ctx* ctx, int w, int h, const float* pixels, int on_device);
 
+/* The same with 8- or 16-bit pixels (host or device memory), converted to
+ * float of the same value on the device, as the reference's image readers
+ * store them (DICe_ImageIO.cpp:480-490); the raw bytes cross PCIe, not the
+ * floats.  pixel_type: DICEGPU_PIXEL_U8, DICEGPU_PIXEL_U16 or
+ * DICEGPU_PIXEL_F32.  The optional Gaussian filter and the gradients follow
+ * as for float images. */
+#define DICEGPU_PIXEL_F32 0
+#define DICEGPU_PIXEL_U8  1
+#define DICEGPU_PIXEL_U16 2
+int dicegpu_set_ref_image_typed(dicegpu_ctx* ctx, int w, int h, const void* pixels, int pixel_type,
+                                int on_device);
+int dicegpu_set_def_image_typed(dicegpu_ctx* ctx, int w, int h, const void* pixels, int pixel_type,
+                                int on_device);
+
 /* Square subsets of params.subset_size centred on the COORD_X/COORD_Y field
  * columns (Subset(cx,cy,w,h), DICe_Subset.cpp:78-113).  `fields` is a host
  * array of n * DICEGPU_FIELD_STRIDE doubles: coordinates plus the initial

@@ -122,3 +122,33 @@ def test_invalid_filter_mask_rejected_by_params():
     from dice_b200.schema import Schema
     with pytest.raises(Exception):
         Schema(abi.default_params(gauss_filter_images=1, gauss_filter_mask_size=8))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16])
+@pytest.mark.parametrize("gauss", [0, 1])
+def test_integer_images_equal_their_float_values(dtype, gauss):
+    """8- and 16-bit frames uploaded as integers correlate exactly like the
+    same values uploaded as floats (host and device sources)."""
+    torch = _gpu()
+    from dice_b200.schema import Schema
+    scale = 1.0 if dtype == np.uint8 else 250.0
+    ref, deff = syn.config1(w=160, h=128)
+    ref_i = np.clip(np.round(ref.numpy() * scale), 0, np.iinfo(dtype).max).astype(dtype)
+    def_i = np.clip(np.round(deff.numpy() * scale), 0, np.iinfo(dtype).max).astype(dtype)
+    cx, cy = syn.grid_points(160, 128, 21, 12)
+    p = abi.default_params(subset_size=21, enable_rotation=1, fast_solver_tolerance=1e-5,
+                           gauss_filter_images=gauss, gauss_filter_mask_size=7)
+    out = []
+    for r, d in ((ref_i.astype(np.float32), def_i.astype(np.float32)), (ref_i, def_i),
+                 (torch.from_numpy(ref_i.astype(np.int32)).to(torch.uint16 if dtype == np.uint16 else torch.uint8).cuda(),
+                  torch.from_numpy(def_i.astype(np.int32)).to(torch.uint16 if dtype == np.uint16 else torch.uint8).cuda())):
+        with Schema(p) as s:
+            s.set_ref_image(r)
+            s.set_subsets(cx, cy)
+            s.set_def_image(d)
+            s.execute_correlation()
+            out.append(s.fields())
+    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[2])
+    assert np.mean(out[0][:, abi.F_STATUS] < 2) > 0.9
