@@ -40,6 +40,32 @@ F_SIGMA, F_GAMMA, F_BETA, F_NOISE, F_CONTRAST = 20, 21, 22, 23, 24
 F_ACTIVE_PIXELS, F_STATUS, F_ITERATIONS, F_MATCH, F_CONDITION, F_OMEGA = 25, 26, 27, 28, 29, 30
 API_STRIDE = 9
 PIXEL_F32, PIXEL_U8, PIXEL_U16 = 0, 1, 2
+SHAPE_CIRCLE, SHAPE_RECTANGLE, SHAPE_POLYGON = 0, 1, 2
+
+
+class Shape(ctypes.Structure):
+    """dicegpu_shape: one boundary (role 0) or excluded (role 1) shape of a
+    conformal subset (Conformal_Area_Def, DICe_Shape.h)."""
+    _fields_ = [("kind", ctypes.c_int32), ("subset", ctypes.c_int32), ("role", ctypes.c_int32),
+                ("cx", ctypes.c_int32), ("cy", ctypes.c_int32), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("radius", ctypes.c_float), ("vertex_offset", ctypes.c_int32),
+                ("vertex_count", ctypes.c_int32)]
+
+
+def circle(subset, cx, cy, radius, role=0):
+    return Shape(SHAPE_CIRCLE, subset, role, int(cx), int(cy), 0, 0, float(radius), 0, 0)
+
+
+def rectangle(subset, cx, cy, width, height, role=0):
+    return Shape(SHAPE_RECTANGLE, subset, role, int(cx), int(cy), int(width), int(height), 0.0, 0, 0)
+
+
+def polygon(subset, vertex_offset, vertex_count, role=0):
+    return Shape(SHAPE_POLYGON, subset, role, 0, 0, 0, 0, 0.0, int(vertex_offset), int(vertex_count))
+
+
+def shape_array(shapes):
+    return (Shape * len(shapes))(*shapes)
 UNCERTAINTY_STRIDE = 8
 
 ERR_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_STATE", -4: "ERR_NOMEM",
@@ -160,6 +186,8 @@ def _declare(lib):
         "dicegpu_set_def_image_typed": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_int]),
         "dicegpu_set_subsets": (c_int, [c_void_p, c_int, c_void_p]),
         "dicegpu_set_subset_pixels": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+        "dicegpu_set_subset_shapes": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+        "dicegpu_get_subset_pixels": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
         "dicegpu_set_force_simplex": (c_int, [c_void_p, c_int, c_void_p]),
         "dicegpu_get_fields": (c_int, [c_void_p, c_void_p]),
         "dicegpu_get_uncertainty": (c_int, [c_void_p, c_void_p]),

@@ -22,6 +22,7 @@
 
 #include "dg_engine.cuh"
 #include "dg_adjoint.cuh"
+#include "dg_raster.cuh"
 #include "dicegpu.h"
 
 using namespace dg;
@@ -739,6 +740,135 @@ extern "C" int dicegpu_set_subset_pixels(dicegpu_ctx* c, int n, const int32_t* o
     CK(cudaMemcpy(c->d_py, py, total * sizeof(int32_t), cudaMemcpyHostToDevice));
   }
   c->use_lists = true;
+  return DICEGPU_OK;
+}
+
+// Bounds of the shape arguments: every coordinate product in the pixel tests
+// stays inside int32 and a subset's bounding box stays a bounded walk.
+static const int kShapeCoordMax = 1000000;
+static const int kShapeExtentMax = 32768;
+static const int64_t kShapeAreaMax = (int64_t)1 << 26;
+
+static bool shape_box_host(const dicegpu_shape& s, const int32_t* vx, const int32_t* vy, int64_t& x0,
+                           int64_t& x1, int64_t& y0, int64_t& y1) {
+  if (s.cx < -kShapeCoordMax || s.cx > kShapeCoordMax || s.cy < -kShapeCoordMax || s.cy > kShapeCoordMax)
+    return false;
+  if (s.kind == DICEGPU_SHAPE_CIRCLE) {
+    if (!(s.radius >= 0.0f && s.radius <= 16384.0f)) return false;
+    x0 = (int)((float)s.cx - s.radius - 1.0f); x1 = (int)((float)s.cx + s.radius + 1.0f);
+    y0 = (int)((float)s.cy - s.radius - 1.0f); y1 = (int)((float)s.cy + s.radius + 1.0f);
+  } else if (s.kind == DICEGPU_SHAPE_RECTANGLE) {
+    if (s.width < 0 || s.width > kShapeExtentMax || s.height < 0 || s.height > kShapeExtentMax) return false;
+    x0 = s.cx - s.width / 2; x1 = x0 + s.width - 1;
+    y0 = s.cy - s.height / 2; y1 = y0 + s.height - 1;
+  } else if (s.kind == DICEGPU_SHAPE_POLYGON) {
+    if (!vx || !vy || s.vertex_count < 3 || s.vertex_count > 4096 || s.vertex_offset < 0) return false;
+    x0 = y0 = INT64_MAX; x1 = y1 = INT64_MIN;
+    for (int k = 0; k < s.vertex_count; ++k) {
+      const int64_t x = vx[s.vertex_offset + k], y = vy[s.vertex_offset + k];
+      if (x < -kShapeCoordMax || x > kShapeCoordMax || y < -kShapeCoordMax || y > kShapeCoordMax) return false;
+      x0 = std::min(x0, x); x1 = std::max(x1, x); y0 = std::min(y0, y); y1 = std::max(y1, y);
+    }
+  } else {
+    return false;
+  }
+  return true;
+}
+
+extern "C" int dicegpu_set_subset_shapes(dicegpu_ctx* c, int n_shapes, const dicegpu_shape* shapes,
+                                         const int32_t* vx, const int32_t* vy) {
+  if (!c || c->n < 1 || n_shapes < 1 || !shapes) return DICEGPU_ERR_ARG;
+  const int n = c->n;
+  // validate, bound every subset's box, and group the shapes by subset
+  int64_t n_vertices = 0;
+  std::vector<int64_t> bx0(n, INT64_MAX), bx1(n, INT64_MIN), by0(n, INT64_MAX), by1(n, INT64_MIN);
+  std::vector<int32_t> shape_off(n + 1, 0);
+  for (int k = 0; k < n_shapes; ++k) {
+    const dicegpu_shape& s = shapes[k];
+    if (s.subset < 0 || s.subset >= n || (s.role != 0 && s.role != 1)) return DICEGPU_ERR_ARG;
+    int64_t x0, x1, y0, y1;
+    if (!shape_box_host(s, vx, vy, x0, x1, y0, y1)) return DICEGPU_ERR_ARG;
+    if (s.kind == DICEGPU_SHAPE_POLYGON)
+      n_vertices = std::max<int64_t>(n_vertices, (int64_t)s.vertex_offset + s.vertex_count);
+    if (s.role == 0) {
+      bx0[s.subset] = std::min(bx0[s.subset], x0); bx1[s.subset] = std::max(bx1[s.subset], x1);
+      by0[s.subset] = std::min(by0[s.subset], y0); by1[s.subset] = std::max(by1[s.subset], y1);
+    }
+    ++shape_off[s.subset + 1];
+  }
+  for (int i = 0; i < n; ++i) {
+    if (bx1[i] < bx0[i]) continue;   // no boundary shape: an empty subset
+    const int64_t w = bx1[i] - bx0[i] + 1, h = by1[i] - by0[i] + 1;
+    if (w > kShapeExtentMax || h > kShapeExtentMax || w * h > kShapeAreaMax) return DICEGPU_ERR_ARG;
+  }
+  for (int i = 0; i < n; ++i) shape_off[i + 1] += shape_off[i];
+  std::vector<dicegpu_shape> grouped(n_shapes);
+  {
+    std::vector<int32_t> fill(shape_off.begin(), shape_off.end() - 1);
+    for (int k = 0; k < n_shapes; ++k) grouped[fill[shapes[k].subset]++] = shapes[k];
+  }
+  cudaStreamSynchronize(c->stream);
+  dicegpu_shape* d_shapes = nullptr;
+  int32_t *d_soff = nullptr, *d_vx = nullptr, *d_vy = nullptr, *d_counts = nullptr;
+  int rc = DICEGPU_OK;
+  auto release = [&]() { cudaFree(d_shapes); cudaFree(d_soff); cudaFree(d_vx); cudaFree(d_vy); cudaFree(d_counts); };
+  const size_t nv = (size_t)std::max<int64_t>(n_vertices, 1);
+  if (cudaMalloc(&d_shapes, n_shapes * sizeof(dicegpu_shape)) != cudaSuccess ||
+      cudaMalloc(&d_soff, (n + 1) * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&d_vx, nv * sizeof(int32_t)) != cudaSuccess || cudaMalloc(&d_vy, nv * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&d_counts, n * sizeof(int32_t)) != cudaSuccess) {
+    release();
+    return DICEGPU_ERR_NOMEM;
+  }
+  std::vector<int32_t> counts(n), offsets(n + 1, 0);
+  RasterArgs ra{d_shapes, d_soff, d_vx, d_vy, n, d_counts, nullptr, nullptr, nullptr};
+  const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)n * 32 + 255) / 256, (int64_t)c->num_sms * 8);
+  cudaError_t e = cudaMemcpy(d_shapes, grouped.data(), n_shapes * sizeof(dicegpu_shape), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_soff, shape_off.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && n_vertices) {
+    e = cudaMemcpy(d_vx, vx, n_vertices * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_vy, vy, n_vertices * sizeof(int32_t), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) {
+    raster_kernel<false><<<blocks, 256, 0, c->stream>>>(ra);
+    ++c->launches;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(counts.data(), d_counts, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) { release(); return DICEGPU_ERR_CUDA; }
+  for (int i = 0; i < n; ++i) {
+    offsets[i + 1] = offsets[i] + counts[i];
+    if (offsets[i + 1] < offsets[i]) { release(); return DICEGPU_ERR_ARG; }   // > 2^31 pixels
+  }
+  const size_t total = (size_t)offsets[n];
+  if ((rc = grow(&c->d_offsets, &c->offs_cap, (size_t)n + 1))) { release(); return rc; }
+  size_t cap2 = c->list_cap;
+  if ((rc = grow(&c->d_px, &c->list_cap, total)) || (rc = grow(&c->d_py, &cap2, total))) { release(); return rc; }
+  c->list_cap = std::min(c->list_cap, cap2);
+  e = cudaMemcpy(c->d_offsets, offsets.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    ra.offsets = c->d_offsets;
+    ra.px = c->d_px;
+    ra.py = c->d_py;
+    raster_kernel<true><<<blocks, 256, 0, c->stream>>>(ra);
+    ++c->launches;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  release();
+  if (e != cudaSuccess) return DICEGPU_ERR_CUDA;
+  c->use_lists = true;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_get_subset_pixels(dicegpu_ctx* c, int32_t* offsets, int32_t* px, int32_t* py) {
+  if (!c || !offsets || !c->use_lists || c->n < 1) return DICEGPU_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(offsets, c->d_offsets, (c->n + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  const size_t total = (size_t)offsets[c->n];
+  if (px && total) CK(cudaMemcpy(px, c->d_px, total * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (py && total) CK(cudaMemcpy(py, c->d_py, total * sizeof(int32_t), cudaMemcpyDeviceToHost));
   return DICEGPU_OK;
 }
 

@@ -142,6 +142,28 @@ class Schema:
                                                      x.ctypes.data_as(ctypes.c_void_p),
                                                      y.ctypes.data_as(ctypes.c_void_p)), "set_subset_pixels")
 
+    def set_subset_shapes(self, shapes, vx=None, vy=None):
+        """Builds every subset's pixel list on the device from its shapes
+        (abi.circle / rectangle / polygon; polygons index vx, vy)."""
+        arr = abi.shape_array(list(shapes))
+        x = np.ascontiguousarray(vx if vx is not None else [0], dtype=np.int32)
+        y = np.ascontiguousarray(vy if vy is not None else [0], dtype=np.int32)
+        abi.check(self.lib.dicegpu_set_subset_shapes(self.ctx, len(arr), ctypes.cast(arr, ctypes.c_void_p),
+                                                     x.ctypes.data_as(ctypes.c_void_p),
+                                                     y.ctypes.data_as(ctypes.c_void_p)), "set_subset_shapes")
+
+    def subset_pixels(self):
+        """(offsets, px, py) of the context's subset pixel lists."""
+        offs = np.zeros(self.n + 1, np.int32)
+        abi.check(self.lib.dicegpu_get_subset_pixels(self.ctx, offs.ctypes.data_as(ctypes.c_void_p), None, None),
+                  "get_subset_pixels")
+        px = np.zeros(max(int(offs[-1]), 1), np.int32)
+        py = np.zeros_like(px)
+        abi.check(self.lib.dicegpu_get_subset_pixels(self.ctx, offs.ctypes.data_as(ctypes.c_void_p),
+                                                     px.ctypes.data_as(ctypes.c_void_p),
+                                                     py.ctypes.data_as(ctypes.c_void_p)), "get_subset_pixels")
+        return offs, px[:offs[-1]], py[:offs[-1]]
+
     def set_force_simplex(self, flags):
         if flags is None:
             abi.check(self.lib.dicegpu_set_force_simplex(self.ctx, 0, None), "set_force_simplex")

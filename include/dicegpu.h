@@ -226,6 +226,40 @@ int dicegpu_set_subsets(dicegpu_ctx* ctx, int n, const double* fields);
  * coordinates, row-major order).  Replaces params.subset_size for these subsets. */
 int dicegpu_set_subset_pixels(dicegpu_ctx* ctx, int n, const int32_t* offsets,
                               const int32_t* px, const int32_t* py);
+
+/* Conformal subsets built on the device from shapes (Subset(cx, cy,
+ * Conformal_Area_Def), DICe_Subset.cpp:115-142, with Circle / Rectangle /
+ * Polygon::get_owned_pixels, DICe_Shape.cpp:136-420): each subset's pixels
+ * are the union of its boundary shapes (role 0), ordered by (y, x), minus
+ * the pixels inside its excluded shapes (role 1).  The reference keeps
+ * excluded pixels in the list as inactive; here they are dropped, which
+ * gives the same results except for the uncertainty fields' pixel count.
+ * Negative coordinates are clamped to 0 as the reference's constructor does.
+ * Polygons use the reference's winding-angle test (float atan2 sums against
+ * pi) with atan2 correctly rounded to float: a pixel lying exactly on an edge
+ * is decided by the last bit of atan2f, which varies between CPU math
+ * libraries; correct rounding makes that choice portable.  The
+ * subsets must already exist (dicegpu_set_subsets); shapes and vertices are
+ * host arrays.  Replaces the host-side construction of pixel lists
+ * (dicegpu_set_subset_pixels). */
+#define DICEGPU_SHAPE_CIRCLE    0
+#define DICEGPU_SHAPE_RECTANGLE 1
+#define DICEGPU_SHAPE_POLYGON   2
+typedef struct dicegpu_shape {
+  int32_t kind;            /* DICEGPU_SHAPE_* */
+  int32_t subset;          /* owning subset index */
+  int32_t role;            /* 0 boundary (union), 1 excluded */
+  int32_t cx, cy;          /* circle / rectangle centroid */
+  int32_t width, height;   /* rectangle */
+  float radius;            /* circle */
+  int32_t vertex_offset, vertex_count;   /* polygon: into vx / vy */
+} dicegpu_shape;
+int dicegpu_set_subset_shapes(dicegpu_ctx* ctx, int n_shapes, const dicegpu_shape* shapes,
+                              const int32_t* vx, const int32_t* vy);
+
+/* Copies the context's subset pixel lists to host memory: offsets[n + 1]
+ * and, when px / py are not NULL, offsets[n] coordinates each. */
+int dicegpu_get_subset_pixels(dicegpu_ctx* ctx, int32_t* offsets, int32_t* px, int32_t* py);
 /* Per-subset FORCE_SIMPLEX flags (DICe_Schema.cpp:2162-2165); NULL clears them. */
 int dicegpu_set_force_simplex(dicegpu_ctx* ctx, int n, const uint8_t* flags);
 

@@ -1345,6 +1345,117 @@ extern "C" int oracle_gn_system(const dicegpu_params* params, int w, int h, cons
   return 0;
 }
 
+// Pixel ownership of the conformal-subset shapes without deformation
+// (Circle / Rectangle / Polygon::get_owned_pixels, DICe_Shape.cpp:136-219,
+// 259-279, 322-420) and of excluded shapes (deactivate_pixels, :104-134,
+// 233-256, 298-320).  kind 0 circle (cx, cy, radius), 1 rectangle (cx, cy,
+// width, height), 2 polygon (vertices).
+namespace {
+// angle_2d (DICe_Shape.cpp:87-102): float atan2 of float arguments, the
+// wrap against the double constants, result stored as float.  The float
+// atan2 is taken correctly rounded (the double atan2 rounded to float): a
+// pixel lying exactly on a polygon edge sees that edge's term at +-pi, and
+// which side of pi it rounds to follows the last bit of atan2f, which
+// differs between math libraries (glibc 2.39's atan2f is 1 ulp off on ~16 %
+// of small integer vectors and flips ~2.5 % of on-edge pixels).  Correct
+// rounding fixes that choice everywhere and reproduces the reference's
+// conformal-subset image; off the edges no pixel depends on it.
+static float angle_2d(float x1, float y1, float x2, float y2) {
+  float t1 = (float)std::atan2((double)y1, (double)x1), t2 = (float)std::atan2((double)y2, (double)x2);
+  float d = t2 - t1;
+  while (d > 3.14159265358979323846) d -= 6.28318530717958647692;
+  while (d < -3.14159265358979323846) d += 6.28318530717958647692;
+  return d;
+}
+static bool polygon_has(const int32_t* vx, const int32_t* vy, int nv, int x, int y) {
+  float angle = 0.0f;
+  for (int i = 0; i < nv; ++i) {
+    const int j = (i + 1 == nv) ? 0 : i + 1;   // the first vertex closes the polygon
+    const float dx1 = (float)(vx[i] - x), dy1 = (float)(vy[i] - y);
+    const float dx2 = (float)(vx[j] - x), dy2 = (float)(vy[j] - y);
+    angle += angle_2d(dx1, dy1, dx2, dy2);
+  }
+  return std::abs(angle) >= 3.14159265358979323846;
+}
+static bool shape_has(const dicegpu_shape& s, const int32_t* vx, const int32_t* vy, int x, int y) {
+  if (s.kind == 0) {
+    const int lim = (int)s.radius + 1;   // outside; keeps the squares inside int
+    if (std::abs(x - s.cx) > lim || std::abs(y - s.cy) > lim) return false;
+    const float r2 = s.radius * s.radius;
+    const float dx = (float)((x - s.cx) * (x - s.cx)), dy = (float)((y - s.cy) * (y - s.cy));
+    return dx + dy <= r2;
+  }
+  if (s.kind == 1) {
+    const int ox = s.cx - s.width / 2, oy = s.cy - s.height / 2;
+    return x >= ox && x < ox + s.width && y >= oy && y < oy + s.height;
+  }
+  return polygon_has(vx + s.vertex_offset, vy + s.vertex_offset, s.vertex_count, x, y);
+}
+static void shape_box(const dicegpu_shape& s, const int32_t* vx, const int32_t* vy, int& x0, int& x1,
+                      int& y0, int& y1) {
+  if (s.kind == 0) {
+    x0 = (int)((float)s.cx - s.radius - 1.0f); x1 = (int)((float)s.cx + s.radius + 1.0f);
+    y0 = (int)((float)s.cy - s.radius - 1.0f); y1 = (int)((float)s.cy + s.radius + 1.0f);
+  } else if (s.kind == 1) {
+    x0 = s.cx - s.width / 2; x1 = x0 + s.width - 1;
+    y0 = s.cy - s.height / 2; y1 = y0 + s.height - 1;
+  } else {
+    x0 = x1 = vx[s.vertex_offset];
+    y0 = y1 = vy[s.vertex_offset];
+    for (int i = 1; i < s.vertex_count; ++i) {
+      x0 = std::min(x0, vx[s.vertex_offset + i]); x1 = std::max(x1, vx[s.vertex_offset + i]);
+      y0 = std::min(y0, vy[s.vertex_offset + i]); y1 = std::max(y1, vy[s.vertex_offset + i]);
+    }
+  }
+}
+}  // namespace
+
+// Pixel lists of n conformal subsets: the union of each subset's boundary
+// shapes ordered by (y, x) (Subset(cx, cy, Conformal_Area_Def),
+// DICe_Subset.cpp:115-142; negative coordinates clamped to 0), without the
+// pixels inside its excluded shapes.  With px == NULL only offsets[n+1] is
+// filled.
+extern "C" int oracle_rasterize(int n, int n_shapes, const dicegpu_shape* shapes, const int32_t* vx,
+                                const int32_t* vy, int32_t* offsets, int32_t* px, int32_t* py) {
+  if (n < 0 || n_shapes < 0 || !offsets || (n_shapes && !shapes)) return DICEGPU_ERR_ARG;
+  std::vector<std::vector<int>> by_subset(n);
+  for (int k = 0; k < n_shapes; ++k) {
+    if (shapes[k].subset < 0 || shapes[k].subset >= n) return DICEGPU_ERR_ARG;
+    by_subset[shapes[k].subset].push_back(k);
+  }
+  offsets[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
+    bool any = false;
+    for (int k : by_subset[i]) {
+      if (shapes[k].role != 0) continue;
+      int a, b, c, d;
+      shape_box(shapes[k], vx, vy, a, b, c, d);
+      if (!any) { x0 = a; x1 = b; y0 = c; y1 = d; any = true; }
+      else { x0 = std::min(x0, a); x1 = std::max(x1, b); y0 = std::min(y0, c); y1 = std::max(y1, d); }
+    }
+    int cnt = 0;
+    for (int y = y0; any && y <= y1; ++y)
+      for (int x = x0; x <= x1; ++x) {
+        bool in = false, out = false;
+        for (int k : by_subset[i]) {
+          const bool h = shape_has(shapes[k], vx, vy, x, y);
+          if (shapes[k].role == 0) in = in || h;
+          else out = out || h;
+        }
+        if (in && !out) {
+          if (px) {
+            px[offsets[i] + cnt] = x < 0 ? 0 : x;
+            py[offsets[i] + cnt] = y < 0 ? 0 : y;
+          }
+          ++cnt;
+        }
+      }
+    offsets[i + 1] = offsets[i] + cnt;
+  }
+  return 0;
+}
+
 // One Objective entry point per subset on a fresh square subset at the
 // parameters of its field row: op 0 computeUpdateFast (:430-657), op 1
 // computeUpdateRobust (:369-388), op 2 sigma (:150-184) after the subset's

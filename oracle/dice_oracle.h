@@ -70,6 +70,11 @@ int oracle_gamma(const dicegpu_params* params, int w, int h, const float* ref,
 int oracle_map(const dicegpu_params* params, const double* fields, int n, const float* xy,
                float cx, float cy, float* out_xy);
 
+/* Pixel lists of conformal subsets from shapes (get_owned_pixels); with
+ * px == NULL only offsets[n + 1] is filled. */
+int oracle_rasterize(int n, int n_shapes, const dicegpu_shape* shapes, const int32_t* vx,
+                     const int32_t* vy, int32_t* offsets, int32_t* px, int32_t* py);
+
 /* Defaults of dice_default_params (same values as dicegpu_default_params). */
 int oracle_default_params(dicegpu_params* p);
 

@@ -9,7 +9,7 @@ import os
 
 import numpy as np
 
-from dice_b200.abi import Params, FIELD_STRIDE, UNCERTAINTY_STRIDE
+from dice_b200.abi import Params, FIELD_STRIDE, UNCERTAINTY_STRIDE, shape_array
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdiceoracle.so")
@@ -61,6 +61,8 @@ def lib():
         L.oracle_default_params.argtypes = [P]
         L.oracle_map.restype = ci
         L.oracle_map.argtypes = [P, vp, ci, vp, ctypes.c_float, ctypes.c_float, vp]
+        L.oracle_rasterize.restype = ci
+        L.oracle_rasterize.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -109,6 +111,23 @@ def shape_map(params, field_row, xy, cx, cy):
     rc = lib().oracle_map(ctypes.byref(params), _ptr(f), xy.shape[0], _ptr(xy), cx, cy, _ptr(out))
     assert rc == 0
     return out
+
+
+def rasterize(n, shapes, vx=None, vy=None):
+    """Pixel lists (offsets, px, py) of n conformal subsets from their shapes
+    (dice_b200.abi.Shape), as get_owned_pixels builds them."""
+    arr = shape_array(list(shapes))
+    x = np.ascontiguousarray(vx if vx is not None else [0], dtype=np.int32)
+    y = np.ascontiguousarray(vy if vy is not None else [0], dtype=np.int32)
+    offs = np.zeros(n + 1, np.int32)
+    sp = ctypes.cast(arr, ctypes.c_void_p)
+    rc = lib().oracle_rasterize(n, len(arr), sp, _ptr(x), _ptr(y), _ptr(offs), None, None)
+    assert rc == 0, rc
+    px = np.zeros(max(int(offs[-1]), 1), np.int32)
+    py = np.zeros_like(px)
+    rc = lib().oracle_rasterize(n, len(arr), sp, _ptr(x), _ptr(y), _ptr(offs), _ptr(px), _ptr(py))
+    assert rc == 0, rc
+    return offs, px[:offs[-1]], py[:offs[-1]]
 
 
 def gauss_filter(img, mask_size=7):

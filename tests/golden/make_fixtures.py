@@ -18,6 +18,7 @@ Sources (paths inside the DICe project):
   tests/regression/single_speckled_shift/{input,params}.xml, subsets.dat,
       gold/single_speckled_shift_{0..6}.txt
   tests/component/images/ImageB.tif, outFilter{5,7,9,11,13}.rawi  (240 x 161)
+  tests/component/images/conformal.rawi                            (60 x 56)
 """
 import os
 import sys
@@ -78,6 +79,15 @@ def main(root):
         assert nb == 4
         gold = np.frombuffer(raw[12:], np.float32).reshape(h, w)
         out["gauss_gold_%d" % m] = gold[y0:y0 + 64, x0:x0 + 64].copy()
+    # DICe_TestSubset: the image of a conformal subset (two polygons minus
+    # a rectangle) that Subset::write_image writes over its bounding box,
+    # re-read with spread/floored intensities: 0 outside the subset, the
+    # excluded pixels at one common grey, owned pixels above it.
+    with open(os.path.join(root, "tests", "component", "images", "conformal.rawi"), "rb") as fh:
+        raw = fh.read()
+    w, h, nb = np.frombuffer(raw[:12], np.uint32)
+    assert nb == 4
+    out["conformal_subset_image"] = np.frombuffer(raw[12:], np.float32).reshape(h, w).copy()
     path =os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_gold.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, {k: v.shape for k, v in out.items()})
