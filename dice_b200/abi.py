@@ -41,6 +41,8 @@ F_ACTIVE_PIXELS, F_STATUS, F_ITERATIONS, F_MATCH, F_CONDITION, F_OMEGA = 25, 26,
 API_STRIDE = 9
 PIXEL_F32, PIXEL_U8, PIXEL_U16 = 0, 1, 2
 SHAPE_CIRCLE, SHAPE_RECTANGLE, SHAPE_POLYGON = 0, 1, 2
+ROLE_BOUNDARY, ROLE_EXCLUDED, ROLE_OBSTRUCTED = 0, 1, 2
+GENERIC_ROUTINE, TRACKING_ROUTINE = 0, 1
 
 
 class Shape(ctypes.Structure):
@@ -104,6 +106,9 @@ class Params(ctypes.Structure):
         ("gauss_filter_images", ctypes.c_int32),
         ("gauss_filter_mask_size", ctypes.c_int32),
         ("compute_uncertainty", ctypes.c_int32),
+        ("correlation_routine", ctypes.c_int32),
+        ("obstruction_skin_factor", ctypes.c_double),
+        ("override_force_simplex", ctypes.c_int32),
         ("reserved", ctypes.c_int32 * 1),
     ]
 
@@ -138,6 +143,25 @@ def default_params(**overrides):
     p.subset_size = 21
     p.gauss_filter_images = 0
     p.gauss_filter_mask_size = 7
+    p.correlation_routine = GENERIC_ROUTINE
+    p.obstruction_skin_factor = 1.0
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+def tracking_default_params(**overrides):
+    """tracking_default_params (DICe_ParameterUtilities.cpp:297-345) with overrides."""
+    p = default_params()
+    p.correlation_routine = TRACKING_ROUTINE
+    p.optimization = SIMPLEX
+    p.enable_rotation = 1
+    p.disp_jump_tol = 8.0
+    p.theta_jump_tol = 0.1
+    p.obstruction_skin_factor = 1.8
+    p.override_force_simplex = 1
     for k, v in overrides.items():
         if not hasattr(p, k):
             raise AttributeError(k)
@@ -188,6 +212,39 @@ def _declare(lib):
         "dicegpu_set_subset_pixels": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "dicegpu_set_subset_shapes": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "dicegpu_get_subset_pixels": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        "dicegpu_set_blocking": (c_int, [c_void_p, c_void_p, c_void_p]),
+        "dicegpu_get_params": (c_int, [c_void_p, P]),
+        "dicegpu_subset_file_read": (c_int, [ctypes.c_char_p, c_int, c_int, ctypes.POINTER(c_void_p),
+                                             ctypes.c_char_p, c_int]),
+        "dicegpu_subset_file_parse": (c_int, [ctypes.c_char_p, ctypes.c_size_t, c_int, c_int,
+                                              ctypes.POINTER(c_void_p), ctypes.c_char_p, c_int]),
+        "dicegpu_subset_file_free": (c_int, [c_void_p]),
+        "dicegpu_subset_file_get_info": (c_int, [c_void_p, c_void_p]),
+        "dicegpu_subset_file_coordinates": (c_int, [c_void_p, c_void_p]),
+        "dicegpu_subset_file_shapes": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        "dicegpu_subset_file_blocking": (c_int, [c_void_p, c_void_p, c_void_p]),
+        "dicegpu_subset_file_force_simplex": (c_int, [c_void_p, c_void_p]),
+        "dicegpu_subset_file_seeds": (c_int, [c_void_p, c_void_p, c_void_p]),
+        "dicegpu_subset_file_features": (c_int, [c_void_p, c_void_p]),
+        "dicegpu_subset_file_apply": (c_int, [c_void_p, c_void_p]),
+        "dicegpu_output_create": (c_int, [P, ctypes.c_char_p, ctypes.c_char_p, c_int, c_void_p,
+                                          ctypes.POINTER(c_void_p)]),
+        "dicegpu_output_destroy": (c_int, [c_void_p]),
+        "dicegpu_output_num_fields": (c_int, [c_void_p, ctypes.POINTER(c_int)]),
+        "dicegpu_output_info_text": (c_int, [c_void_p, ctypes.c_char_p, ctypes.c_size_t,
+                                             ctypes.POINTER(ctypes.c_size_t)]),
+        "dicegpu_output_header_text": (c_int, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t,
+                                               ctypes.POINTER(ctypes.c_size_t)]),
+        "dicegpu_output_row_text": (c_int, [c_void_p, c_int, c_void_p, c_void_p, ctypes.c_char_p, ctypes.c_size_t,
+                                            ctypes.POINTER(ctypes.c_size_t)]),
+        "dicegpu_output_write_frame": (c_int, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, c_int, c_int, c_int,
+                                               c_int, c_void_p, c_void_p, c_int]),
+        "dicegpu_diff_files": (c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_double, c_int,
+                                       c_int, c_int, ctypes.POINTER(c_int), ctypes.c_char_p, ctypes.c_size_t]),
+        "dicegpu_diff_text": (c_int, [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t,
+                                      ctypes.c_double, ctypes.c_double, c_int, c_int, ctypes.POINTER(c_int),
+                                      ctypes.c_char_p, ctypes.c_size_t]),
+        "dicegpu_tracking_default_params": (c_int, [P]),
         "dicegpu_set_force_simplex": (c_int, [c_void_p, c_int, c_void_p]),
         "dicegpu_get_fields": (c_int, [c_void_p, c_void_p]),
         "dicegpu_get_uncertainty": (c_int, [c_void_p, c_void_p]),

@@ -59,6 +59,10 @@ struct DevImage {
   const float4* __restrict__ p4;
 };
 
+// ints per subset mask descriptor: obstruction box (x0, y0, w, h, word
+// offset), blocked box (x0, y0, w, h, word offset)
+#define DG_MASK_DESC 10
+
 // Subset geometry: square (`half` >= 0, centred on the COORD fields) or an
 // explicit pixel list in CSR form.
 struct DevGeometry {
@@ -67,6 +71,11 @@ struct DevGeometry {
   const int32_t* __restrict__ px;
   const int32_t* __restrict__ py;
   const uint8_t* __restrict__ force_simplex;
+  // optional per-subset mask descriptors (DG_MASK_DESC ints each), the
+  // obstruction words and the blocked words
+  const int32_t* __restrict__ mask_desc;
+  const uint32_t* __restrict__ mask_bits;
+  const uint32_t* __restrict__ blocked_bits;
 };
 
 // ---------------------------------------------------------------------------

@@ -45,6 +45,8 @@ struct FrameArgs {
   int32_t* iter_out;     // MODE_GN / MODE_SIMPLEX: iterations per subset
   int32_t* status_out;   // MODE_GN / MODE_SIMPLEX: Status_Flag per subset
   double* noise_out;     // MODE_SIGMA: noise_std_dev per subset (sigma goes to gamma_out)
+  const int32_t* order;  // optional: the subsets of this launch (a tracking wave), n_order of them
+  int n_order;
 };
 
 // Image_::interpolate_keys_fourth (DICe_Image.cpp:890-924), intensity only:
@@ -188,6 +190,7 @@ struct SubsetRef {
   int idx, cx, cy, npix;
   int off;          // list offset (-1 for squares)
   float K;          // intensity shift for the moment sums
+  bool masked;      // has an obstruction or blocked bitmap
 };
 
 template <int SHAPE, int INTERP, bool DEFGRAD>
@@ -233,7 +236,16 @@ struct Engine {
     in.K = sb.K;
     MapConst k;
     make_mapconst<SHAPE>(slots, !DEFGRAD, (float)sb.cx, (float)sb.cy, k);
-    return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS>(in, k);
+    if (sb.masked) {
+      in.mdesc = A.geo.mask_desc + (size_t)sb.idx * DG_MASK_DESC;
+      in.mbits = A.geo.mask_bits;
+      in.bbits = A.geo.blocked_bits;
+      return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, true>(in, k);
+    }
+    in.mdesc = nullptr;
+    in.mbits = nullptr;
+    in.bbits = nullptr;
+    return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, false>(in, k);
   }
 
   // Objective::gamma from the moments (Subset::gamma, DICe_Subset.cpp:323-340):
@@ -930,6 +942,11 @@ struct Engine {
       const int kx = min(max(sb.cx, 0), A.ref.w - 1), ky = min(max(sb.cy, 0), A.ref.h - 1);
       sb.K = __ldg(A.ref.I + (size_t)ky * A.ref.w + kx);
     }
+    sb.masked = false;
+    if (A.geo.mask_desc) {
+      const int32_t* md = A.geo.mask_desc + (size_t)idx * DG_MASK_DESC;
+      sb.masked = md[2] > 0 || md[7] > 0;
+    }
 
     float slots[12];
     if (A.mode == MODE_GAMMA) {
@@ -942,8 +959,9 @@ struct Engine {
       run_objective(sb, fv);
       return;
     }
-    // frame-0 field-of-view test (DICe_Schema.cpp:2036-2048)
-    if (A.geo.half >= 0 && A.first_frame) {
+    // frame-0 field-of-view test (DICe_Schema.cpp:2036-2048), whenever a
+    // subset size is set (subset_dim_ > 0), whatever the subsets' shapes
+    if (P.subset_size > 0 && A.first_frame) {
       const float cur_x = (float)(fld(DICEGPU_F_COORD_X) + fld(DICEGPU_F_DISP_X));
       const float cur_y = (float)(fld(DICEGPU_F_COORD_Y) + fld(DICEGPU_F_DISP_Y));
       const int hs = P.subset_size / 2;

@@ -97,12 +97,32 @@ struct PassIn {
   int half;        // square half-width (lists: unused)
   int cx, cy, npix, off;
   float K;         // intensity shift for the moment sums
+  // MASKED passes: this subset's mask descriptor (obstruction box x0, y0,
+  // w, h, word offset; blocked box likewise), the obstruction words and the
+  // blocked words
+  const int32_t* __restrict__ mdesc;
+  const uint32_t* __restrict__ mbits;
+  const uint32_t* __restrict__ bbits;
 };
+
+// Whether pixel (px, py) is set in the mask box (x0, y0, w, h) at words.
+__device__ __forceinline__ bool mask_bit(const uint32_t* __restrict__ words, int x0, int y0, int w, int h,
+                                         int px, int py) {
+  const unsigned dx = (unsigned)(px - x0), dy = (unsigned)(py - y0);
+  if (dx >= (unsigned)w || dy >= (unsigned)h) return false;
+  const unsigned long bit = (unsigned long)dy * (unsigned)w + dx;
+  return (__ldg(words + (bit >> 5)) >> (bit & 31)) & 1u;
+}
 
 //   ACC_H   : accumulate sum v v^T into the warp's smem matrix (Gauss-Newton)
 //   GRADS   : interpolate the deformed gradients (DEFGRAD) / read reference ones
 //   MOMENTS : FP64 intensity moments for gamma
-template <int SHAPE, int INTERP, bool DEFGRAD, bool ACC_H, bool GRADS, bool MOMENTS>
+//   MASKED  : also deactivate pixels whose position rounds into the
+//             subset's obstruction or blocked bitmap (Subset::initialize,
+//             DICe_Subset.cpp:412-422); for positive coordinates, which the
+//             border test leaves, is_obstructed_pixel's rounding is the
+//             border test's
+template <int SHAPE, int INTERP, bool DEFGRAD, bool ACC_H, bool GRADS, bool MOMENTS, bool MASKED>
 __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
   using L = Layout<SHAPE>;
   const int lane = threadIdx.x & 31;
@@ -133,6 +153,11 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
     drow = 32 / side; dcol = 32 - drow * side;
   }
   const int x0 = in.cx - in.half, y0 = in.cy - in.half;
+  int m_ox = 0, m_oy = 0, m_ow = 0, m_oh = 0, m_oo = 0, m_bx = 0, m_by = 0, m_bw = 0, m_bh = 0, m_bo = 0;
+  if (MASKED) {
+    m_ox = in.mdesc[0]; m_oy = in.mdesc[1]; m_ow = in.mdesc[2]; m_oh = in.mdesc[3]; m_oo = in.mdesc[4];
+    m_bx = in.mdesc[5]; m_by = in.mdesc[6]; m_bw = in.mdesc[7]; m_bh = in.mdesc[8]; m_bo = in.mdesc[9];
+  }
   const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_smem<SHAPE>()->vbuf);
   for (int base = 0; base < in.npix; base += 32 * PPL) {
     float vv[PPL][L::VW];
@@ -164,7 +189,11 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
       const float F = rin ? __ldg(in.refI + ri) : 0.0f;
       if (ACC_H) sumFall += F - in.K;
       // 4-pixel border deactivation (DICe_Subset.cpp:408)
-      if (!(px < 4 || px >= W - 4 || py < 4 || py >= H - 4)) {
+      bool live = !(px < 4 || px >= W - 4 || py < 4 || py >= H - 4);
+      if (MASKED && live)
+        live = !mask_bit(in.mbits + m_oo, m_ox, m_oy, m_ow, m_oh, px, py) &&
+               !mask_bit(in.bbits + m_bo, m_bx, m_by, m_bw, m_bh, px, py);
+      if (live) {
         float G, gx = 0.0f, gy = 0.0f;
         if (GRADS && DEFGRAD) interp_interior<INTERP, true>(in.def, mx, my, G, gx, gy);
         else interp_interior<INTERP, false>(in.def, mx, my, G, gx, gy);

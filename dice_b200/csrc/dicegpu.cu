@@ -222,14 +222,16 @@ __global__ void __launch_bounds__(256, DG_MIN_BLOCKS) frame_kernel(const __grid_
     if (blockIdx.x == 0 && threadIdx.x < 32) e.run(a.plain_index);
     return;
   }
+  // the launch's subsets: all n, or the n_order listed in order
+  const int count = a.order ? a.n_order : a.n;
   if (a.queue_mode == 0) {
     // one global queue head
     for (;;) {
-      int idx = 0;
-      if (lane == 0) idx = atomicAdd(a.work_counter, 1);
-      idx = __shfl_sync(FULL, idx, 0);
-      if (idx >= a.n) break;
-      e.run(idx);
+      int t = 0;
+      if (lane == 0) t = atomicAdd(a.work_counter, 1);
+      t = __shfl_sync(FULL, t, 0);
+      if (t >= count) break;
+      e.run(a.order ? a.order[t] : t);
     }
     return;
   }
@@ -249,10 +251,10 @@ __global__ void __launch_bounds__(256, DG_MIN_BLOCKS) frame_kernel(const __grid_
     t = __shfl_sync(FULL, t, 0);
     const long long chunk = (long long)q + (long long)(t / C) * G;
     const long long lidx = chunk * C + (t % C);
-    const int idx = lidx < a.n ? (int)lidx : a.n;
-    if (idx < a.n) {
+    const int pos = lidx < count ? (int)lidx : count;
+    if (pos < count) {
       DG_PT(t_run);
-      e.run(idx);
+      e.run(a.order ? a.order[pos] : pos);
       DG_PACC(0, t_run);
       continue;
     }
@@ -287,6 +289,18 @@ static FrameKernelFn pick_kernel(int interp, bool defgrad) {
 // ---------------------------------------------------------------------------
 // upper bound on the persistent grid (and on its per-CTA queue heads)
 static const int kMaxQueues = 8192;
+
+template <typename T>
+static int grow(T** p, size_t* cap, size_t need);
+
+// A device array that only grows (contents are not kept across growth).
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t n) { return grow(&p, &cap, n); }
+  void release() { cudaFree(p); p = nullptr; cap = 0; }
+};
 
 struct dicegpu_ctx {
   dicegpu_params params;
@@ -335,12 +349,41 @@ struct dicegpu_ctx {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   long long graph_launches = 0;   // kernels per replay
+  // conformal shapes (dicegpu_set_subset_shapes), grouped by subset
+  std::vector<dicegpu_shape> h_shapes;
+  std::vector<int32_t> h_shape_off, h_svx, h_svy;
+  std::vector<uint8_t> h_conformal;
+  DevBuf<dicegpu_shape> d_shapes;
+  DevBuf<int32_t> d_shape_off, d_svx, d_svy;
+  DevBuf<uint8_t> d_conformal;
+  // pixel masks: descriptors (host copy kept), obstruction words, blocked words
+  std::vector<int32_t> h_mask_desc;
+  DevBuf<int32_t> d_mask_desc;
+  DevBuf<uint32_t> d_mask_bits, d_blocked_bits;
+  bool use_masks = false;
+  int blocked_W = 0, blocked_H = 0;   // image size the blocked words were sized for
+  // blocking subsets and the tracking waves
+  bool has_blocking = false;
+  std::vector<int32_t> h_blk_off, h_blk_ids;
+  DevBuf<int32_t> d_blk_off, d_blk_ids;
+  std::vector<int32_t> wave_off, bwave_off;   // wave L: d_wave[wave_off[L] ..), d_bwave[bwave_off[L] ..)
+  DevBuf<int32_t> d_wave, d_bwave, d_dv_off, d_dvx, d_dvy;
+  DevBuf<double> d_snapshot;
+  int n_blocked = 0;                   // subsets with a conformal blocker
+  std::vector<int32_t> h_blocked_slot; // their index among those, -1 otherwise
+  // forced simplex: the caller's flags and the blocking rule's
+  std::vector<uint8_t> h_force_user, h_force_block;
 };
 
+// A failed runtime call returns DICEGPU_ERR_CUDA and clears the runtime's
+// pending (non-sticky) error, so that it is not reported by a later check.
 #define CK(x)                                  \
   do {                                         \
     cudaError_t e_ = (x);                      \
-    if (e_ != cudaSuccess) return DICEGPU_ERR_CUDA; \
+    if (e_ != cudaSuccess) {                   \
+      cudaGetLastError();                      \
+      return DICEGPU_ERR_CUDA;                 \
+    }                                          \
   } while (0)
 
 static bool gauss_weights(int M, GaussWeights& g);
@@ -355,6 +398,9 @@ static int build_devparams(const dicegpu_params& p, DevParams& d) {
         p.optimization == DICEGPU_GRADIENT_BASED_THEN_SIMPLEX))
     return DICEGPU_ERR_UNSUPPORTED;
   if (p.max_solver_iterations_fast < 0 || p.max_solver_iterations_robust < 1) return DICEGPU_ERR_ARG;
+  if (p.correlation_routine != DICEGPU_GENERIC_ROUTINE && p.correlation_routine != DICEGPU_TRACKING_ROUTINE)
+    return DICEGPU_ERR_ARG;
+  if (!(std::fabs(p.obstruction_skin_factor) < 1.0e6)) return DICEGPU_ERR_ARG;
   if (p.gauss_filter_images) {
     GaussWeights g;
     if (!gauss_weights(p.gauss_filter_mask_size, g)) return DICEGPU_ERR_ARG;
@@ -428,6 +474,23 @@ extern "C" int dicegpu_default_params(dicegpu_params* p) {
   p->subset_size = 21;
   p->gauss_filter_images = 0;
   p->gauss_filter_mask_size = 7;
+  p->correlation_routine = DICEGPU_GENERIC_ROUTINE;
+  p->obstruction_skin_factor = 1.0;
+  return DICEGPU_OK;
+}
+
+// tracking_default_params (DICe_ParameterUtilities.cpp:297-345): the values
+// that differ from dice_default_params.
+extern "C" int dicegpu_tracking_default_params(dicegpu_params* p) {
+  const int rc = dicegpu_default_params(p);
+  if (rc) return rc;
+  p->correlation_routine = DICEGPU_TRACKING_ROUTINE;
+  p->optimization = DICEGPU_SIMPLEX;
+  p->enable_rotation = 1;
+  p->disp_jump_tol = 8.0;
+  p->theta_jump_tol = 0.1;
+  p->obstruction_skin_factor = 1.8;
+  p->override_force_simplex = 1;
   return DICEGPU_OK;
 }
 
@@ -471,6 +534,11 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   cudaFree(c->d_fields); cudaFree(c->d_offsets); cudaFree(c->d_px); cudaFree(c->d_py);
   cudaFree(c->d_force); cudaFree(c->d_counter); cudaFree(c->d_status); cudaFree(c->d_passes);
   cudaFree(c->d_unc);
+  c->d_shapes.release(); c->d_shape_off.release(); c->d_svx.release(); c->d_svy.release();
+  c->d_conformal.release(); c->d_mask_desc.release(); c->d_mask_bits.release();
+  c->d_blocked_bits.release(); c->d_blk_off.release(); c->d_blk_ids.release(); c->d_wave.release();
+  c->d_bwave.release(); c->d_dv_off.release(); c->d_dvx.release(); c->d_dvy.release();
+  c->d_snapshot.release();
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -493,6 +561,8 @@ static int ensure_uncertainty(dicegpu_ctx* c) {
   return DICEGPU_OK;
 }
 
+static int upload_force(dicegpu_ctx* c);
+
 extern "C" int dicegpu_set_params(dicegpu_ctx* c, const dicegpu_params* p) {
   if (!c || !p) return DICEGPU_ERR_ARG;
   DevParams d;
@@ -500,7 +570,16 @@ extern "C" int dicegpu_set_params(dicegpu_ctx* c, const dicegpu_params* p) {
   if (rc) return rc;
   c->params = *p;
   c->dp = d;
-  return ensure_uncertainty(c);
+  int rc2 = ensure_uncertainty(c);
+  if (rc2) return rc2;
+  // override_force_simplex decides whether the blocking rule's flags apply
+  return (c->n > 0 && !c->h_force_block.empty()) ? upload_force(c) : DICEGPU_OK;
+}
+
+extern "C" int dicegpu_get_params(dicegpu_ctx* c, dicegpu_params* p) {
+  if (!c || !p) return DICEGPU_ERR_ARG;
+  *p = c->params;
+  return DICEGPU_OK;
 }
 
 extern "C" int dicegpu_set_stream(dicegpu_ctx* c, void* stream) {
@@ -703,6 +782,8 @@ static int grow(T** p, size_t* cap, size_t need) {
   return DICEGPU_OK;
 }
 
+static void clear_shapes(dicegpu_ctx* c);
+
 extern "C" int dicegpu_set_subsets(dicegpu_ctx* c, int n, const double* fields) {
   if (!c || n < 1 || !fields) return DICEGPU_ERR_ARG;
   cudaStreamSynchronize(c->stream);
@@ -713,7 +794,12 @@ extern "C" int dicegpu_set_subsets(dicegpu_ctx* c, int n, const double* fields) 
   CK(cudaMemcpyAsync(c->d_fields, fields, (size_t)n * DICEGPU_FIELD_STRIDE * sizeof(double),
                      cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  if (c->n != n) { c->use_lists = false; c->use_force = false; }
+  if (c->n != n) {
+    c->use_lists = false;
+    c->use_force = false;
+    c->h_force_user.clear();
+    clear_shapes(c);
+  }
   c->n = n;
   c->frame_index = 0;
   c->unc_n = 0;
@@ -775,60 +861,111 @@ static bool shape_box_host(const dicegpu_shape& s, const int32_t* vx, const int3
   return true;
 }
 
+// The device force-simplex flags: the caller's, and those of blocked and
+// blocking subsets unless params.override_force_simplex.
+static int upload_force(dicegpu_ctx* c) {
+  const int n = c->n;
+  const bool user = (int)c->h_force_user.size() == n;
+  const bool block = (int)c->h_force_block.size() == n && !c->params.override_force_simplex;
+  if (!user && !block) {
+    c->use_force = false;
+    return DICEGPU_OK;
+  }
+  std::vector<uint8_t> f(n, 0);
+  for (int i = 0; i < n; ++i) f[i] = (user && c->h_force_user[i]) || (block && c->h_force_block[i]);
+  cudaStreamSynchronize(c->stream);
+  int rc = grow(&c->d_force, &c->force_cap, (size_t)n);
+  if (rc) return rc;
+  CK(cudaMemcpy(c->d_force, f.data(), n, cudaMemcpyHostToDevice));
+  c->use_force = true;
+  return DICEGPU_OK;
+}
+
+static void clear_shapes(dicegpu_ctx* c) {
+  c->h_shapes.clear(); c->h_shape_off.clear(); c->h_svx.clear(); c->h_svy.clear();
+  c->h_conformal.clear(); c->h_mask_desc.clear();
+  c->use_masks = false;
+  c->has_blocking = false;
+  c->h_blk_off.clear(); c->h_blk_ids.clear(); c->h_blocked_slot.clear();
+  c->wave_off.clear(); c->bwave_off.clear();
+  c->n_blocked = 0;
+  c->h_force_block.clear();
+}
+
 extern "C" int dicegpu_set_subset_shapes(dicegpu_ctx* c, int n_shapes, const dicegpu_shape* shapes,
                                          const int32_t* vx, const int32_t* vy) {
   if (!c || c->n < 1 || n_shapes < 1 || !shapes) return DICEGPU_ERR_ARG;
   const int n = c->n;
-  // validate, bound every subset's box, and group the shapes by subset
+  // validate, bound every subset's boxes, and group the shapes by subset
   int64_t n_vertices = 0;
   std::vector<int64_t> bx0(n, INT64_MAX), bx1(n, INT64_MIN), by0(n, INT64_MAX), by1(n, INT64_MIN);
+  std::vector<int64_t> ox0(n, INT64_MAX), ox1(n, INT64_MIN), oy0(n, INT64_MAX), oy1(n, INT64_MIN);
   std::vector<int32_t> shape_off(n + 1, 0);
   for (int k = 0; k < n_shapes; ++k) {
     const dicegpu_shape& s = shapes[k];
-    if (s.subset < 0 || s.subset >= n || (s.role != 0 && s.role != 1)) return DICEGPU_ERR_ARG;
+    if (s.subset < 0 || s.subset >= n || s.role < DICEGPU_ROLE_BOUNDARY || s.role > DICEGPU_ROLE_OBSTRUCTED)
+      return DICEGPU_ERR_ARG;
     int64_t x0, x1, y0, y1;
     if (!shape_box_host(s, vx, vy, x0, x1, y0, y1)) return DICEGPU_ERR_ARG;
     if (s.kind == DICEGPU_SHAPE_POLYGON)
       n_vertices = std::max<int64_t>(n_vertices, (int64_t)s.vertex_offset + s.vertex_count);
-    if (s.role == 0) {
+    if (s.role == DICEGPU_ROLE_BOUNDARY) {
       bx0[s.subset] = std::min(bx0[s.subset], x0); bx1[s.subset] = std::max(bx1[s.subset], x1);
       by0[s.subset] = std::min(by0[s.subset], y0); by1[s.subset] = std::max(by1[s.subset], y1);
+    } else if (s.role == DICEGPU_ROLE_OBSTRUCTED) {
+      ox0[s.subset] = std::min(ox0[s.subset], x0); ox1[s.subset] = std::max(ox1[s.subset], x1);
+      oy0[s.subset] = std::min(oy0[s.subset], y0); oy1[s.subset] = std::max(oy1[s.subset], y1);
     }
     ++shape_off[s.subset + 1];
   }
-  for (int i = 0; i < n; ++i) {
-    if (bx1[i] < bx0[i]) continue;   // no boundary shape: an empty subset
-    const int64_t w = bx1[i] - bx0[i] + 1, h = by1[i] - by0[i] + 1;
-    if (w > kShapeExtentMax || h > kShapeExtentMax || w * h > kShapeAreaMax) return DICEGPU_ERR_ARG;
-  }
+  auto box_ok = [](int64_t a0, int64_t a1, int64_t b0, int64_t b1) {
+    if (a1 < a0) return true;   // none
+    const int64_t w = a1 - a0 + 1, h = b1 - b0 + 1;
+    return w <= kShapeExtentMax && h <= kShapeExtentMax && w * h <= kShapeAreaMax;
+  };
+  for (int i = 0; i < n; ++i)
+    if (!box_ok(bx0[i], bx1[i], by0[i], by1[i]) || !box_ok(ox0[i], ox1[i], oy0[i], oy1[i]))
+      return DICEGPU_ERR_ARG;
   for (int i = 0; i < n; ++i) shape_off[i + 1] += shape_off[i];
   std::vector<dicegpu_shape> grouped(n_shapes);
   {
     std::vector<int32_t> fill(shape_off.begin(), shape_off.end() - 1);
     for (int k = 0; k < n_shapes; ++k) grouped[fill[shapes[k].subset]++] = shapes[k];
   }
+  // obstruction boxes and word offsets
+  std::vector<int32_t> desc((size_t)n * DG_MASK_DESC, 0), obst_list;
+  int64_t obst_words = 0;
+  for (int i = 0; i < n; ++i) {
+    if (ox1[i] < ox0[i]) continue;
+    int32_t* d = &desc[(size_t)i * DG_MASK_DESC];
+    d[0] = (int32_t)ox0[i]; d[1] = (int32_t)oy0[i];
+    d[2] = (int32_t)(ox1[i] - ox0[i] + 1); d[3] = (int32_t)(oy1[i] - oy0[i] + 1);
+    d[4] = (int32_t)obst_words;
+    obst_words += ((int64_t)d[2] * d[3] + 31) / 32;
+    obst_list.push_back(i);
+  }
+  if (obst_words > ((int64_t)1 << 31)) return DICEGPU_ERR_ARG;
+  std::vector<uint8_t> conformal(n, 0);
+  for (int i = 0; i < n; ++i) conformal[i] = bx1[i] >= bx0[i];
   cudaStreamSynchronize(c->stream);
-  dicegpu_shape* d_shapes = nullptr;
-  int32_t *d_soff = nullptr, *d_vx = nullptr, *d_vy = nullptr, *d_counts = nullptr;
-  int rc = DICEGPU_OK;
-  auto release = [&]() { cudaFree(d_shapes); cudaFree(d_soff); cudaFree(d_vx); cudaFree(d_vy); cudaFree(d_counts); };
   const size_t nv = (size_t)std::max<int64_t>(n_vertices, 1);
-  if (cudaMalloc(&d_shapes, n_shapes * sizeof(dicegpu_shape)) != cudaSuccess ||
-      cudaMalloc(&d_soff, (n + 1) * sizeof(int32_t)) != cudaSuccess ||
-      cudaMalloc(&d_vx, nv * sizeof(int32_t)) != cudaSuccess || cudaMalloc(&d_vy, nv * sizeof(int32_t)) != cudaSuccess ||
-      cudaMalloc(&d_counts, n * sizeof(int32_t)) != cudaSuccess) {
-    release();
-    return DICEGPU_ERR_NOMEM;
-  }
+  int rc;
+  if ((rc = c->d_shapes.ensure(n_shapes)) || (rc = c->d_shape_off.ensure(n + 1)) || (rc = c->d_svx.ensure(nv)) ||
+      (rc = c->d_svy.ensure(nv)) || (rc = c->d_conformal.ensure(n)))
+    return rc;
+  int32_t* d_counts = nullptr;
+  if (cudaMalloc(&d_counts, n * sizeof(int32_t)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
   std::vector<int32_t> counts(n), offsets(n + 1, 0);
-  RasterArgs ra{d_shapes, d_soff, d_vx, d_vy, n, d_counts, nullptr, nullptr, nullptr};
+  RasterArgs ra{c->d_shapes.p, c->d_shape_off.p, c->d_svx.p, c->d_svy.p, n, d_counts, nullptr, nullptr, nullptr,
+                c->d_fields, c->params.subset_size >= 1 ? c->params.subset_size / 2 : -1};
   const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)n * 32 + 255) / 256, (int64_t)c->num_sms * 8);
-  cudaError_t e = cudaMemcpy(d_shapes, grouped.data(), n_shapes * sizeof(dicegpu_shape), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d_soff, shape_off.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaMemcpy(c->d_shapes.p, grouped.data(), n_shapes * sizeof(dicegpu_shape), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_shape_off.p, shape_off.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
   if (e == cudaSuccess && n_vertices) {
-    e = cudaMemcpy(d_vx, vx, n_vertices * sizeof(int32_t), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_vy, vy, n_vertices * sizeof(int32_t), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(c->d_svx.p, vx, n_vertices * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->d_svy.p, vy, n_vertices * sizeof(int32_t), cudaMemcpyHostToDevice);
   }
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_conformal.p, conformal.data(), n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     raster_kernel<false><<<blocks, 256, 0, c->stream>>>(ra);
     ++c->launches;
@@ -836,29 +973,195 @@ extern "C" int dicegpu_set_subset_shapes(dicegpu_ctx* c, int n_shapes, const dic
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(counts.data(), d_counts, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  if (e != cudaSuccess) { release(); return DICEGPU_ERR_CUDA; }
+  cudaFree(d_counts);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return DICEGPU_ERR_CUDA;
+  }
   for (int i = 0; i < n; ++i) {
     offsets[i + 1] = offsets[i] + counts[i];
-    if (offsets[i + 1] < offsets[i]) { release(); return DICEGPU_ERR_ARG; }   // > 2^31 pixels
+    if (offsets[i + 1] < offsets[i]) return DICEGPU_ERR_ARG;   // > 2^31 pixels
   }
   const size_t total = (size_t)offsets[n];
-  if ((rc = grow(&c->d_offsets, &c->offs_cap, (size_t)n + 1))) { release(); return rc; }
+  if ((rc = grow(&c->d_offsets, &c->offs_cap, (size_t)n + 1))) return rc;
   size_t cap2 = c->list_cap;
-  if ((rc = grow(&c->d_px, &c->list_cap, total)) || (rc = grow(&c->d_py, &cap2, total))) { release(); return rc; }
+  if ((rc = grow(&c->d_px, &c->list_cap, total)) || (rc = grow(&c->d_py, &cap2, total))) return rc;
   c->list_cap = std::min(c->list_cap, cap2);
-  e = cudaMemcpy(c->d_offsets, offsets.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) {
-    ra.offsets = c->d_offsets;
-    ra.px = c->d_px;
-    ra.py = c->d_py;
-    raster_kernel<true><<<blocks, 256, 0, c->stream>>>(ra);
-    ++c->launches;
-    e = cudaGetLastError();
+  CK(cudaMemcpy(c->d_offsets, offsets.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+  ra.offsets = c->d_offsets;
+  ra.px = c->d_px;
+  ra.py = c->d_py;
+  raster_kernel<true><<<blocks, 256, 0, c->stream>>>(ra);
+  ++c->launches;
+  CK(cudaGetLastError());
+  // obstruction bitmaps
+  clear_shapes(c);
+  if (!obst_list.empty()) {
+    if ((rc = c->d_mask_bits.ensure((size_t)obst_words)) || (rc = c->d_mask_desc.ensure(desc.size()))) return rc;
+    int32_t* d_list = nullptr;
+    if (cudaMalloc(&d_list, obst_list.size() * sizeof(int32_t)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
+    e = cudaMemsetAsync(c->d_mask_bits.p, 0, (size_t)obst_words * sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c->d_mask_desc.p, desc.data(), desc.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                          c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_list, obst_list.data(), obst_list.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                          c->stream);
+    if (e == cudaSuccess) {
+      ObstArgs oa{c->d_shapes.p, c->d_shape_off.p, c->d_svx.p, c->d_svy.p, d_list, (int)obst_list.size(),
+                  c->d_mask_desc.p, c->d_mask_bits.p};
+      const unsigned ob = (unsigned)std::min<int64_t>(((int64_t)obst_list.size() * 32 + 255) / 256,
+                                                      (int64_t)c->num_sms * 8);
+      obstruction_kernel<<<ob, 256, 0, c->stream>>>(oa);
+      ++c->launches;
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_list);
+    if (e != cudaSuccess) {
+    cudaGetLastError();
+    return DICEGPU_ERR_CUDA;
   }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  release();
-  if (e != cudaSuccess) return DICEGPU_ERR_CUDA;
+    c->use_masks = true;
+  }
+  c->h_shapes.swap(grouped);
+  c->h_shape_off.swap(shape_off);
+  if (n_vertices) {
+    c->h_svx.assign(vx, vx + n_vertices);
+    c->h_svy.assign(vy, vy + n_vertices);
+  }
+  c->h_conformal.swap(conformal);
+  c->h_mask_desc.swap(desc);
+  CK(cudaStreamSynchronize(c->stream));
   c->use_lists = true;
+  return upload_force(c);
+}
+
+extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, const int32_t* ids) {
+  if (!c || c->n < 1) return DICEGPU_ERR_ARG;
+  const int n = c->n;
+  cudaStreamSynchronize(c->stream);
+  if (!offsets) {
+    c->has_blocking = false;
+    c->h_force_block.clear();
+    c->n_blocked = 0;
+    if (!c->h_mask_desc.empty()) {
+      bool any = false;
+      for (int i = 0; i < n; ++i) {
+        int32_t* d = &c->h_mask_desc[(size_t)i * DG_MASK_DESC];
+        d[5] = d[6] = d[7] = d[8] = d[9] = 0;
+        any = any || d[2] > 0;
+      }
+      // the device descriptors exist once an obstruction or a tracking frame needed them
+      if (c->d_mask_desc.p && c->d_mask_desc.cap >= c->h_mask_desc.size())
+        CK(cudaMemcpy(c->d_mask_desc.p, c->h_mask_desc.data(), c->h_mask_desc.size() * sizeof(int32_t),
+                      cudaMemcpyHostToDevice));
+      c->use_masks = any;
+      c->blocked_W = c->blocked_H = 0;
+    }
+    return upload_force(c);
+  }
+  if (offsets[0] != 0 || (offsets[n] > 0 && !ids)) return DICEGPU_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (offsets[i + 1] < offsets[i]) return DICEGPU_ERR_ARG;
+  for (int k = 0; k < offsets[n]; ++k)
+    if (ids[k] < 0 || ids[k] >= n) return DICEGPU_ERR_ARG;
+  const bool have_shapes = (int)c->h_conformal.size() == n;
+  // deformed vertices per blocked subset, and the polygon limit
+  std::vector<int32_t> dv_off, blocked_slot(n, -1);
+  std::vector<uint8_t> force(n, 0);
+  int64_t dv_total = 0;
+  int n_blocked = 0;
+  for (int i = 0; i < n; ++i) {
+    if (offsets[i + 1] > offsets[i]) force[i] = 1;   // blocked
+    int polys = 0;
+    int64_t verts = 0;
+    for (int k = offsets[i]; k < offsets[i + 1]; ++k) {
+      const int j = ids[k];
+      force[j] = 1;   // blocking
+      if (!have_shapes || !c->h_conformal[j]) continue;
+      for (int m = c->h_shape_off[j]; m < c->h_shape_off[j + 1]; ++m) {
+        const dicegpu_shape& s = c->h_shapes[m];
+        if (s.role != DICEGPU_ROLE_BOUNDARY) continue;
+        if (s.kind == DICEGPU_SHAPE_CIRCLE) return DICEGPU_ERR_UNSUPPORTED;
+        ++polys;
+        verts += s.kind == DICEGPU_SHAPE_RECTANGLE ? 4 : s.vertex_count;
+      }
+    }
+    if (polys > DG_MAX_BLOCK_POLYS) return DICEGPU_ERR_UNSUPPORTED;
+    if (polys > 0) {
+      blocked_slot[i] = n_blocked++;
+      dv_off.push_back((int32_t)dv_total);
+      dv_total += verts;
+    } else {
+      dv_off.push_back((int32_t)dv_total);
+    }
+  }
+  if (dv_total > ((int64_t)1 << 30)) return DICEGPU_ERR_ARG;
+  // waves: a subset runs after every blocker that precedes it in index order
+  std::vector<int> level(n, 0);
+  int nlev = 1;
+  for (int i = 0; i < n; ++i) {
+    for (int k = offsets[i]; k < offsets[i + 1]; ++k)
+      if (ids[k] < i) level[i] = std::max(level[i], level[ids[k]] + 1);
+    nlev = std::max(nlev, level[i] + 1);
+  }
+  std::vector<int32_t> wave, bwave, wave_off(nlev + 1, 0), bwave_off(nlev + 1, 0);
+  for (int L = 0; L < nlev; ++L) {
+    for (int i = 0; i < n; ++i)
+      if (level[i] == L) {
+        wave.push_back(i);
+        if (blocked_slot[i] >= 0) bwave.push_back(i);
+      }
+    wave_off[L + 1] = (int32_t)wave.size();
+    bwave_off[L + 1] = (int32_t)bwave.size();
+  }
+  int rc;
+  if ((rc = c->d_blk_off.ensure(n + 1)) || (rc = c->d_blk_ids.ensure(std::max(offsets[n], 1))) ||
+      (rc = c->d_wave.ensure(n)) || (rc = c->d_bwave.ensure(std::max<size_t>(bwave.size(), 1))) ||
+      (rc = c->d_dv_off.ensure(n)) || (rc = c->d_dvx.ensure((size_t)std::max<int64_t>(dv_total, 1))) ||
+      (rc = c->d_dvy.ensure((size_t)std::max<int64_t>(dv_total, 1))) ||
+      (rc = c->d_snapshot.ensure((size_t)n * DICEGPU_FIELD_STRIDE)))
+    return rc;
+  CK(cudaMemcpy(c->d_blk_off.p, offsets, (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (offsets[n]) CK(cudaMemcpy(c->d_blk_ids.p, ids, offsets[n] * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_wave.p, wave.data(), wave.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (!bwave.empty())
+    CK(cudaMemcpy(c->d_bwave.p, bwave.data(), bwave.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_dv_off.p, dv_off.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  c->h_blk_off.assign(offsets, offsets + n + 1);
+  c->h_blk_ids.assign(ids, ids + offsets[n]);
+  c->wave_off.swap(wave_off);
+  c->bwave_off.swap(bwave_off);
+  c->h_blocked_slot.swap(blocked_slot);
+  c->n_blocked = n_blocked;
+  c->blocked_W = c->blocked_H = 0;   // blocked words sized at the next tracking frame
+  c->h_force_block.swap(force);
+  c->has_blocking = true;
+  if (c->h_mask_desc.empty()) c->h_mask_desc.assign((size_t)n * DG_MASK_DESC, 0);
+  return upload_force(c);
+}
+
+// Sizes the blocked words for the current image (one full-image bitmap per
+// subset with a conformal blocker) and points the descriptors at them.
+static int ensure_blocked_words(dicegpu_ctx* c) {
+  if (c->blocked_W == c->W && c->blocked_H == c->H) return DICEGPU_OK;
+  const size_t per = ((size_t)c->W * c->H + 31) / 32;
+  const size_t total = per * (size_t)std::max(c->n_blocked, 1);
+  if (total * sizeof(uint32_t) > ((size_t)4 << 30)) return DICEGPU_ERR_NOMEM;
+  cudaStreamSynchronize(c->stream);
+  int rc;
+  if ((rc = c->d_blocked_bits.ensure(total)) || (rc = c->d_mask_desc.ensure(c->h_mask_desc.size()))) return rc;
+  for (int i = 0; i < c->n; ++i) {
+    int32_t* d = &c->h_mask_desc[(size_t)i * DG_MASK_DESC];
+    d[5] = d[6] = d[7] = d[8] = 0;
+    d[9] = c->h_blocked_slot[i] >= 0 ? (int32_t)(per * c->h_blocked_slot[i]) : 0;
+  }
+  CK(cudaMemcpy(c->d_mask_desc.p, c->h_mask_desc.data(), c->h_mask_desc.size() * sizeof(int32_t),
+                cudaMemcpyHostToDevice));
+  c->blocked_W = c->W;
+  c->blocked_H = c->H;
+  c->use_masks = true;
   return DICEGPU_OK;
 }
 
@@ -874,14 +1177,13 @@ extern "C" int dicegpu_get_subset_pixels(dicegpu_ctx* c, int32_t* offsets, int32
 
 extern "C" int dicegpu_set_force_simplex(dicegpu_ctx* c, int n, const uint8_t* flags) {
   if (!c) return DICEGPU_ERR_ARG;
-  if (!flags) { c->use_force = false; return DICEGPU_OK; }
+  if (!flags) {
+    c->h_force_user.clear();
+    return upload_force(c);
+  }
   if (n != c->n) return DICEGPU_ERR_ARG;
-  cudaStreamSynchronize(c->stream);
-  int rc = grow(&c->d_force, &c->force_cap, (size_t)n);
-  if (rc) return rc;
-  CK(cudaMemcpy(c->d_force, flags, n, cudaMemcpyHostToDevice));
-  c->use_force = true;
-  return DICEGPU_OK;
+  c->h_force_user.assign(flags, flags + n);
+  return upload_force(c);
 }
 
 extern "C" int dicegpu_get_fields(dicegpu_ctx* c, double* out) {
@@ -951,6 +1253,9 @@ static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
   a.geo.px = c->use_lists ? c->d_px : nullptr;
   a.geo.py = c->use_lists ? c->d_py : nullptr;
   a.geo.force_simplex = c->use_force ? c->d_force : nullptr;
+  a.geo.mask_desc = c->use_masks ? c->d_mask_desc.p : nullptr;
+  a.geo.mask_bits = c->d_mask_bits.p;
+  a.geo.blocked_bits = c->d_blocked_bits.p;
   a.fields = c->d_fields;
   a.n = c->n;
   a.first_frame = c->frame_index == 0;
@@ -987,6 +1292,63 @@ static int ready(dicegpu_ctx* c) {
   return DICEGPU_OK;
 }
 
+// TRACKING_ROUTINE with blocking subsets: the frame runs in waves, each
+// after the blocked bitmaps of its blocked subsets are rebuilt from their
+// blockers' parameters (this frame's for earlier subsets, the frame-start
+// snapshot's for later ones).  Everything is enqueued on the stream.
+static int run_tracking_frame(dicegpu_ctx* c, FrameKernelFn fn, int blocks, size_t smem) {
+  int rc = ensure_blocked_words(c);
+  if (rc) return rc;
+  const int n = c->n;
+  CK(cudaMemcpyAsync(c->d_snapshot.p, c->d_fields, (size_t)n * DICEGPU_FIELD_STRIDE * sizeof(double),
+                     cudaMemcpyDeviceToDevice, c->stream));
+  BlockArgs ba;
+  std::memset(&ba, 0, sizeof(ba));
+  ba.P = c->dp;
+  ba.shapes = c->d_shapes.p;
+  ba.shape_off = c->d_shape_off.p;
+  ba.vx = c->d_svx.p;
+  ba.vy = c->d_svy.p;
+  ba.fields = c->d_fields;
+  ba.snapshot = c->d_snapshot.p;
+  ba.blk_off = c->d_blk_off.p;
+  ba.blk_ids = c->d_blk_ids.p;
+  ba.conformal = c->d_conformal.p;
+  ba.dv_off = c->d_dv_off.p;
+  ba.dvx = c->d_dvx.p;
+  ba.dvy = c->d_dvy.p;
+  ba.desc = c->d_mask_desc.p;
+  ba.bits = c->d_blocked_bits.p;
+  ba.W = c->W;
+  ba.H = c->H;
+  ba.skin = (float)c->params.obstruction_skin_factor;
+  const int nlev = (int)c->wave_off.size() - 1;
+  for (int L = 0; L < nlev; ++L) {
+    const int nb = c->bwave_off[L + 1] - c->bwave_off[L];
+    if (nb > 0) {
+      ba.list = c->d_bwave.p + c->bwave_off[L];
+      ba.nlist = nb;
+      const unsigned g = (unsigned)std::min(nb, 4 * c->num_sms);
+      if (c->dp.shape == DICEGPU_QUADRATIC_SF) blocked_kernel<DICEGPU_QUADRATIC_SF><<<g, 256, 0, c->stream>>>(ba);
+      else blocked_kernel<DICEGPU_AFFINE_SF><<<g, 256, 0, c->stream>>>(ba);
+      CK(cudaGetLastError());
+      c->launches += 1;
+    }
+    const int nw = c->wave_off[L + 1] - c->wave_off[L];
+    if (nw == 0) continue;
+    FrameArgs a;
+    fill_args(c, a, MODE_CORRELATE);
+    a.order = c->d_wave.p + c->wave_off[L];
+    a.n_order = nw;
+    CK(cudaMemsetAsync(c->d_counter, 0, (size_t)blocks * sizeof(int), c->stream));
+    fn<<<blocks, c->warps_per_cta * 32, smem, c->stream>>>(a);
+    CK(cudaGetLastError());
+    c->launches += 1;
+  }
+  c->frame_index += 1;
+  return DICEGPU_OK;
+}
+
 extern "C" int dicegpu_execute_correlation(dicegpu_ctx* c) {
   int rc = ready(c);
   if (rc) return rc;
@@ -994,6 +1356,8 @@ extern "C" int dicegpu_execute_correlation(dicegpu_ctx* c) {
   int blocks;
   size_t smem;
   if ((rc = grid_for(c, fn, &blocks, &smem))) return rc;
+  if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE)
+    return run_tracking_frame(c, fn, blocks, smem);
   FrameArgs a;
   fill_args(c, a, MODE_CORRELATE);
   CK(cudaMemsetAsync(c->d_counter, 0, (size_t)blocks * sizeof(int), c->stream));
@@ -1007,6 +1371,8 @@ extern "C" int dicegpu_execute_correlation(dicegpu_ctx* c) {
 extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
   int rc = ready(c);
   if (rc) return rc;
+  if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE)
+    return DICEGPU_ERR_UNSUPPORTED;
   FrameKernelFn fn = frame_fn(c);
   if (!fn) return DICEGPU_ERR_UNSUPPORTED;
   const size_t smem = warp_smem_bytes(c->dp.shape);
@@ -1032,6 +1398,11 @@ extern "C" int dicegpu_capture_sequence(dicegpu_ctx* c, int n, const float* cons
     if (!frames[k]) return DICEGPU_ERR_ARG;
   if (!c->has_ref || c->n < 1) return DICEGPU_ERR_STATE;
   if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+  // the blocked bitmaps are sized before capture (allocation cannot be captured)
+  if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE) {
+    const int rcb = ensure_blocked_words(c);
+    if (rcb) return rcb;
+  }
   CK(cudaStreamSynchronize(c->stream));
   if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
   if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }

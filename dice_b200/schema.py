@@ -152,6 +152,22 @@ class Schema:
                                                      x.ctypes.data_as(ctypes.c_void_p),
                                                      y.ctypes.data_as(ctypes.c_void_p)), "set_subset_shapes")
 
+    def set_blocking(self, blockers):
+        """Blocking subsets: blockers[i] lists the subsets that may block
+        subset i (BLOCKING_SUBSETS); None clears them."""
+        if blockers is None:
+            abi.check(self.lib.dicegpu_set_blocking(self.ctx, None, None), "set_blocking")
+            return
+        offs = np.zeros(self.n + 1, np.int32)
+        ids = []
+        for i in range(self.n):
+            b = list(blockers[i]) if i < len(blockers) and blockers[i] is not None else []
+            ids += b
+            offs[i + 1] = offs[i] + len(b)
+        ida = np.ascontiguousarray(ids if ids else [0], dtype=np.int32)
+        abi.check(self.lib.dicegpu_set_blocking(self.ctx, offs.ctypes.data_as(ctypes.c_void_p),
+                                                ida.ctypes.data_as(ctypes.c_void_p)), "set_blocking")
+
     def subset_pixels(self):
         """(offsets, px, py) of the context's subset pixel lists."""
         offs = np.zeros(self.n + 1, np.int32)

@@ -168,11 +168,34 @@ typedef struct dicegpu_params {
    * (DICEGPU_UNCERTAINTY_STRIDE rows, dicegpu_get_uncertainty); the
    * reference always computes them, the default here is 0 (off). */
   int32_t compute_uncertainty;
+  /* Correlation_Routine (DICe.h:587-591): GENERIC_ROUTINE runs the subsets
+   * independently; TRACKING_ROUTINE runs them in index order and, before
+   * each subset with blocking subsets, deactivates the pixels its blockers
+   * cover at their current parameters (Schema::execute_correlation,
+   * DICe_Schema.cpp:1732-1762, check_for_blocking_subsets, :4529-4557). */
+  int32_t correlation_routine;
+  /* obstruction_skin_factor: stretch of a blocking subset's deformed
+   * boundary about its vertex centroid (1.0; tracking defaults 1.8). */
+  double  obstruction_skin_factor;
+  /* override_force_simplex: 0 forces the simplex on subsets that block or
+   * are blocked (DICe_Schema.cpp:2160-2185); 1 leaves them to
+   * params.optimization. */
+  int32_t override_force_simplex;
   int32_t reserved[1];
 } dicegpu_params;
 
+/* Correlation_Routine */
+#define DICEGPU_GENERIC_ROUTINE  0
+#define DICEGPU_TRACKING_ROUTINE 1
+
 /* Fills *p with the reference defaults. Replaces dice_default_params. */
 int dicegpu_default_params(dicegpu_params* p);
+/* Fills *p with the reference's tracking defaults (tracking_default_params,
+ * DICe_ParameterUtilities.cpp:297-345; use_tracking_default_params).  The
+ * subset evolution those defaults switch on changes results only for subsets
+ * with excluded shapes, whose pixels it brings back; it is not implemented,
+ * and such subsets keep their excluded pixels off. */
+int dicegpu_tracking_default_params(dicegpu_params* p);
 
 /* Number of shape-function parameters N for these params (2..6 affine, 12 quadratic). */
 int dicegpu_num_params(const dicegpu_params* p);
@@ -187,6 +210,7 @@ typedef struct dicegpu_ctx dicegpu_ctx;
 int dicegpu_create(const dicegpu_params* params, dicegpu_ctx** out);
 int dicegpu_destroy(dicegpu_ctx* ctx);
 int dicegpu_set_params(dicegpu_ctx* ctx, const dicegpu_params* params);
+int dicegpu_get_params(dicegpu_ctx* ctx, dicegpu_params* params);
 /* The stream every later call on ctx is issued on (a cudaStream_t; NULL = legacy default). */
 int dicegpu_set_stream(dicegpu_ctx* ctx, void* stream);
 
@@ -228,13 +252,20 @@ int dicegpu_set_subset_pixels(dicegpu_ctx* ctx, int n, const int32_t* offsets,
                               const int32_t* px, const int32_t* py);
 
 /* Conformal subsets built on the device from shapes (Subset(cx, cy,
- * Conformal_Area_Def), DICe_Subset.cpp:115-142, with Circle / Rectangle /
+ * Conformal_Area_Def), DICe_Subset.cpp:115-168, with Circle / Rectangle /
  * Polygon::get_owned_pixels, DICe_Shape.cpp:136-420): each subset's pixels
  * are the union of its boundary shapes (role 0), ordered by (y, x), minus
- * the pixels inside its excluded shapes (role 1).  The reference keeps
- * excluded pixels in the list as inactive; here they are dropped, which
- * gives the same results except for the uncertainty fields' pixel count.
- * Negative coordinates are clamped to 0 as the reference's constructor does.
+ * the pixels inside its excluded shapes (role 1, tested at the clamped
+ * coordinates as deactivate_pixels does).  The reference keeps excluded
+ * pixels in the list as inactive; here they are dropped, which gives the same
+ * results except for the uncertainty fields' pixel count.  Negative
+ * coordinates are clamped to 0 as the reference's constructor does.  A
+ * subset without boundary shapes is a square of params.subset_size (as a
+ * subset-file subset without a conformal definition is), empty when that is
+ * below 1.  Obstructed shapes (role 2) are static regions of the image: a
+ * subset pixel whose deformed position rounds into one is deactivated for
+ * that evaluation (Subset::is_obstructed_pixel, DICe_Subset.cpp:446-460,
+ * tested in Subset::initialize, :412-415).
  * Polygons use the reference's winding-angle test (float atan2 sums against
  * pi) with atan2 correctly rounded to float: a pixel lying exactly on an edge
  * is decided by the last bit of atan2f, which varies between CPU math
@@ -245,10 +276,13 @@ int dicegpu_set_subset_pixels(dicegpu_ctx* ctx, int n, const int32_t* offsets,
 #define DICEGPU_SHAPE_CIRCLE    0
 #define DICEGPU_SHAPE_RECTANGLE 1
 #define DICEGPU_SHAPE_POLYGON   2
+#define DICEGPU_ROLE_BOUNDARY   0
+#define DICEGPU_ROLE_EXCLUDED   1
+#define DICEGPU_ROLE_OBSTRUCTED 2
 typedef struct dicegpu_shape {
   int32_t kind;            /* DICEGPU_SHAPE_* */
   int32_t subset;          /* owning subset index */
-  int32_t role;            /* 0 boundary (union), 1 excluded */
+  int32_t role;            /* DICEGPU_ROLE_* */
   int32_t cx, cy;          /* circle / rectangle centroid */
   int32_t width, height;   /* rectangle */
   float radius;            /* circle */
@@ -256,6 +290,22 @@ typedef struct dicegpu_shape {
 } dicegpu_shape;
 int dicegpu_set_subset_shapes(dicegpu_ctx* ctx, int n_shapes, const dicegpu_shape* shapes,
                               const int32_t* vx, const int32_t* vy);
+
+/* Blocking subsets (BLOCKING_SUBSETS of a conformal subset definition,
+ * Schema::obstructing_subset_ids_): subset i is blocked by ids[offsets[i] ..
+ * offsets[i+1]).  Under DICEGPU_TRACKING_ROUTINE, before subset i runs, the
+ * pixels covered by each conformal blocker's boundary (its polygons and
+ * rectangles mapped by the blocker's parameters, rounded, and stretched by
+ * params.obstruction_skin_factor about their vertex centroid: get_owned_pixels
+ * with a shape function, DICe_Shape.cpp:136-219, 322-396) are deactivated
+ * in subset i.  A blocker earlier in index order contributes its parameters
+ * of this frame, a later one those it had when the frame started.  Square
+ * blockers cover nothing (Subset::deformed_shapes, DICe_Subset.cpp:462-476);
+ * a blocker with a circular boundary is DICEGPU_ERR_UNSUPPORTED (the
+ * reference throws there).  Blocked and blocking subsets use the simplex
+ * unless params.override_force_simplex.  offsets == NULL clears the lists.
+ * Call after dicegpu_set_subset_shapes. */
+int dicegpu_set_blocking(dicegpu_ctx* ctx, const int32_t* offsets, const int32_t* ids);
 
 /* Copies the context's subset pixel lists to host memory: offsets[n + 1]
  * and, when px / py are not NULL, offsets[n] coordinates each. */

@@ -33,7 +33,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <thread>
+#include <set>
 #include <vector>
 
 namespace oracle {
@@ -419,12 +421,16 @@ struct ShapeFn {
 // ---------------------------------------------------------------------------
 // Subset (DICe_Subset.cpp)
 // ---------------------------------------------------------------------------
+typedef std::set<std::pair<int, int>> PixelSet;   // (y, x), as the reference stores them
+
 struct Subset {
   int cx = 0, cy = 0, npix = 0;
   std::vector<int> x, y;
   std::vector<float> ref, def, gx, gy;
   std::vector<char> active, deact;
   bool has_gradients = false;
+  const PixelSet* obstructed = nullptr;   // obstructed_coords_
+  const PixelSet* blocked = nullptr;      // pixels_blocked_by_other_subsets_
 
   // Subset(cx,cy,w,h) (:78-113): odd extent, negative coordinates clamped to 0.
   void init_square(int cx_, int cy_, int size) {
@@ -476,6 +482,21 @@ struct Subset {
       const int px = ((int)(mx + 0.5) == (int)(mx)) ? (int)(mx) : (int)(mx) + 1;
       const int py = ((int)(my + 0.5) == (int)(my)) ? (int)(my) : (int)(my) + 1;
       if (px < 4 || px >= im.w - 4 || py < 4 || py >= im.h - 4) {
+        deact[i] = 1;
+        continue;
+      }
+      // is_obstructed_pixel (:446-460) with its own rounding of the position
+      if (obstructed && !obstructed->empty()) {
+        int c_x = (int)mx;
+        if (mx - (float)(int)mx >= 0.5) c_x++;
+        int c_y = (int)my;
+        if (my - (float)(int)my >= 0.5) c_y++;
+        if (obstructed->count(std::make_pair(c_y, c_x))) {
+          deact[i] = 1;
+          continue;
+        }
+      }
+      if (blocked && !blocked->empty() && blocked->count(std::make_pair(py, px))) {
         deact[i] = 1;
         continue;
       }
@@ -1168,6 +1189,8 @@ extern "C" int oracle_default_params(dicegpu_params* p) {
   p->subset_size = 21;
   p->gauss_filter_images = 0;
   p->gauss_filter_mask_size = 7;
+  p->correlation_routine = DICEGPU_GENERIC_ROUTINE;
+  p->obstruction_skin_factor = 1.0;
   return 0;
 }
 
@@ -1209,7 +1232,13 @@ extern "C" int oracle_interpolate(int method, int w, int h, const float* img, co
 }
 
 namespace {
+// buffers a frame's images and gradients live in
+struct FrameStore {
+  std::vector<float> fref, fdef, rgx, rgy, dgx, dgy;
+};
+
 struct FrameJob {
+  std::shared_ptr<FrameStore> store;
   Ctx C;
   int n;
   double* fields;
@@ -1219,6 +1248,8 @@ struct FrameJob {
   int32_t* gn_out;
   int32_t* sx_out;
   double* unc;
+  const std::vector<PixelSet>* obst = nullptr;   // per subset
+  const PixelSet* blocked = nullptr;             // the subset being run (tracking order)
 };
 
 void run_range(const FrameJob& J, int b, int e) {
@@ -1230,6 +1261,8 @@ void run_range(const FrameJob& J, int b, int e) {
                                J.offsets[i + 1] - J.offsets[i]);
     else s.init_square(cx, cy, J.C.P.subset_size);
     s.init_ref(J.C.ref);
+    s.obstructed = J.obst ? &(*J.obst)[i] : nullptr;
+    s.blocked = J.blocked;
     Counters cnt;
     if (J.unc) {
       cnt.unc = J.unc + (long)i * DICEGPU_UNCERTAINTY_STRIDE;
@@ -1243,43 +1276,43 @@ void run_range(const FrameJob& J, int b, int e) {
 }
 }  // namespace
 
-extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, const float* ref,
-                                    const float* def, int n, double* fields,
-                                    const int32_t* offsets, const int32_t* px,
-                                    const int32_t* py, const uint8_t* force_simplex,
-                                    int first_frame, int nthreads, int32_t* gn_iters_out,
-                                    int32_t* simplex_evals_out, double* uncertainty) {
-  if (!params || !ref || !def || !fields || n < 0 || w < 16 || h < 16) return DICEGPU_ERR_ARG;
-  // the images' optional Gaussian pre-filter comes before their gradients
-  std::vector<float> fref, fdef;
+// images, gradients and parameters of a frame (the images' optional Gaussian
+// pre-filter comes before their gradients)
+static int prepare_frame(const dicegpu_params* params, int w, int h, const float* ref, const float* def,
+                         FrameJob& J) {
+  if (!params || !ref || !def || w < 16 || h < 16) return DICEGPU_ERR_ARG;
+  J.store.reset(new FrameStore());
+  FrameStore& S = *J.store;
   if (params->gauss_filter_images) {
-    fref.resize((long)w * h);
-    fdef.resize((long)w * h);
-    if (!gauss_filter(w, h, params->gauss_filter_mask_size, ref, fref.data()) ||
-        !gauss_filter(w, h, params->gauss_filter_mask_size, def, fdef.data()))
+    S.fref.resize((long)w * h);
+    S.fdef.resize((long)w * h);
+    if (!gauss_filter(w, h, params->gauss_filter_mask_size, ref, S.fref.data()) ||
+        !gauss_filter(w, h, params->gauss_filter_mask_size, def, S.fdef.data()))
       return DICEGPU_ERR_ARG;
-    ref = fref.data();
-    def = fdef.data();
+    ref = S.fref.data();
+    def = S.fdef.data();
   }
-  FrameJob J;
   J.C.P = *params;
   // gradients as Schema::set_ref_image / set_def_image compute them
-  std::vector<float> rgx((long)w * h), rgy((long)w * h), dgx, dgy;
-  compute_gradients(w, h, ref, params->gradient_method, rgx.data(), rgy.data());
+  S.rgx.resize((long)w * h);
+  S.rgy.resize((long)w * h);
+  compute_gradients(w, h, ref, params->gradient_method, S.rgx.data(), S.rgy.data());
   J.C.ref.w = w; J.C.ref.h = h; J.C.ref.I = ref;
-  J.C.ref.gx = rgx.data(); J.C.ref.gy = rgy.data(); J.C.ref.has_gradients = true;
+  J.C.ref.gx = S.rgx.data(); J.C.ref.gy = S.rgy.data(); J.C.ref.has_gradients = true;
   J.C.def.w = w; J.C.def.h = h; J.C.def.I = def;
   if (params->use_def_gradients) {
-    dgx.resize((long)w * h); dgy.resize((long)w * h);
-    compute_gradients(w, h, def, params->gradient_method, dgx.data(), dgy.data());
-    J.C.def.gx = dgx.data(); J.C.def.gy = dgy.data(); J.C.def.has_gradients = true;
+    S.dgx.resize((long)w * h); S.dgy.resize((long)w * h);
+    compute_gradients(w, h, def, params->gradient_method, S.dgx.data(), S.dgy.data());
+    J.C.def.gx = S.dgx.data(); J.C.def.gy = S.dgy.data(); J.C.def.has_gradients = true;
   }
-  J.n = n; J.fields = fields; J.offsets = offsets; J.px = px; J.py = py;
-  J.force_simplex = force_simplex; J.first_frame = first_frame != 0;
-  J.gn_out = gn_iters_out; J.sx_out = simplex_evals_out; J.unc = uncertainty;
+  return 0;
+}
+
+static void run_parallel(const FrameJob& J, int nthreads) {
+  const int n = J.n;
   if (nthreads <= 1 || n < 2) {
     run_range(J, 0, n);
-    return 0;
+    return;
   }
   if (nthreads > n) nthreads = n;
   std::vector<std::thread> th;
@@ -1288,6 +1321,22 @@ extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, 
     th.emplace_back(run_range, std::cref(J), b, e);
   }
   for (auto& x : th) x.join();
+}
+
+extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, const float* ref,
+                                    const float* def, int n, double* fields,
+                                    const int32_t* offsets, const int32_t* px,
+                                    const int32_t* py, const uint8_t* force_simplex,
+                                    int first_frame, int nthreads, int32_t* gn_iters_out,
+                                    int32_t* simplex_evals_out, double* uncertainty) {
+  if (!fields || n < 0) return DICEGPU_ERR_ARG;
+  FrameJob J;
+  const int rc = prepare_frame(params, w, h, ref, def, J);
+  if (rc) return rc;
+  J.n = n; J.fields = fields; J.offsets = offsets; J.px = px; J.py = py;
+  J.force_simplex = force_simplex; J.first_frame = first_frame != 0;
+  J.gn_out = gn_iters_out; J.sx_out = simplex_evals_out; J.unc = uncertainty;
+  run_parallel(J, nthreads);
   return 0;
 }
 
@@ -1367,23 +1416,28 @@ static float angle_2d(float x1, float y1, float x2, float y2) {
   while (d < -3.14159265358979323846) d += 6.28318530717958647692;
   return d;
 }
+// the winding-angle test over a closed vertex loop (vertex nv is vertex 0)
 static bool polygon_has(const int32_t* vx, const int32_t* vy, int nv, int x, int y) {
   float angle = 0.0f;
   for (int i = 0; i < nv; ++i) {
-    const int j = (i + 1 == nv) ? 0 : i + 1;   // the first vertex closes the polygon
+    const int j = (i + 1 == nv) ? 0 : i + 1;
     const float dx1 = (float)(vx[i] - x), dy1 = (float)(vy[i] - y);
     const float dx2 = (float)(vx[j] - x), dy2 = (float)(vy[j] - y);
     angle += angle_2d(dx1, dy1, dx2, dy2);
   }
   return std::abs(angle) >= 3.14159265358979323846;
 }
-static bool shape_has(const dicegpu_shape& s, const int32_t* vx, const int32_t* vy, int x, int y) {
+// get_owned_pixels' test (excluded = false) or deactivate_pixels' (true):
+// they differ only in how the circle adds the squares
+static bool shape_has(const dicegpu_shape& s, const int32_t* vx, const int32_t* vy, int x, int y,
+                      bool excluded) {
   if (s.kind == 0) {
     const int lim = (int)s.radius + 1;   // outside; keeps the squares inside int
     if (std::abs(x - s.cx) > lim || std::abs(y - s.cy) > lim) return false;
     const float r2 = s.radius * s.radius;
-    const float dx = (float)((x - s.cx) * (x - s.cx)), dy = (float)((y - s.cy) * (y - s.cy));
-    return dx + dy <= r2;
+    const int ix = (x - s.cx) * (x - s.cx), iy = (y - s.cy) * (y - s.cy);
+    if (excluded) return (float)(ix + iy) <= r2;
+    return (float)ix + (float)iy <= r2;
   }
   if (s.kind == 1) {
     const int ox = s.cx - s.width / 2, oy = s.cy - s.height / 2;
@@ -1408,50 +1462,208 @@ static void shape_box(const dicegpu_shape& s, const int32_t* vx, const int32_t* 
     }
   }
 }
+// owned pixels of one undeformed shape
+static void owned_pixels(const dicegpu_shape& s, const int32_t* vx, const int32_t* vy, PixelSet& out) {
+  int x0, x1, y0, y1;
+  shape_box(s, vx, vy, x0, x1, y0, y1);
+  for (int y = y0; y <= y1; ++y)
+    for (int x = x0; x <= x1; ++x)
+      if (shape_has(s, vx, vy, x, y, false)) out.insert(std::make_pair(y, x));
+}
+// Polygon / Rectangle::get_owned_pixels with a shape function
+// (DICe_Shape.cpp:136-219, 322-396): the vertices mapped and rounded, then
+// stretched by skin about their integer centroid, then the winding test.  A
+// rectangle is the loop (o), (o + w, o), (o + w, o + h), (o, o + h).
+static void deformed_pixels(const dicegpu_shape& s, const int32_t* vx, const int32_t* vy,
+                            const ShapeFn& sf, int cx, int cy, float skin, PixelSet& out) {
+  std::vector<int32_t> X, Y;
+  if (s.kind == 1) {
+    const int ox = s.cx - s.width / 2, oy = s.cy - s.height / 2;
+    X = {ox, ox + s.width, ox + s.width, ox};
+    Y = {oy, oy, oy + s.height, oy + s.height};
+  } else {
+    X.assign(vx + s.vertex_offset, vx + s.vertex_offset + s.vertex_count);
+    Y.assign(vy + s.vertex_offset, vy + s.vertex_offset + s.vertex_count);
+  }
+  const int nv = (int)X.size();
+  for (int i = 0; i < nv; ++i) {
+    float mx, my;
+    sf.map((float)X[i], (float)Y[i], (float)cx, (float)cy, mx, my);
+    int nx = (int)mx;
+    if (mx - (float)(int)mx >= 0.5) nx++;
+    int ny = (int)my;
+    if (my - (float)(int)my >= 0.5) ny++;
+    X[i] = nx;
+    Y[i] = ny;
+  }
+  // integer centroid, divided as a double and truncated
+  int sx = 0, sy = 0;
+  for (int i = 0; i < nv; ++i) { sx += X[i]; sy += Y[i]; }
+  const int ccx = (int)((double)sx / (double)nv), ccy = (int)((double)sy / (double)nv);
+  int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
+  for (int i = 0; i < nv; ++i) {
+    const float fx = skin * (float)(X[i] - ccx);
+    const float fy = skin * (float)(Y[i] - ccy);
+    X[i] = (int)(fx + (float)ccx);
+    Y[i] = (int)(fy + (float)ccy);
+    if (i == 0) { x0 = x1 = X[i]; y0 = y1 = Y[i]; }
+    else {
+      x0 = std::min(x0, X[i]); x1 = std::max(x1, X[i]);
+      y0 = std::min(y0, Y[i]); y1 = std::max(y1, Y[i]);
+    }
+  }
+  for (int y = y0; y <= y1; ++y)
+    for (int x = x0; x <= x1; ++x)
+      if (polygon_has(X.data(), Y.data(), nv, x, y)) out.insert(std::make_pair(y, x));
+}
+
+// one subset's pixel list: the union of its boundary shapes in (y, x) order
+// without the excluded pixels (tested at the clamped coordinates), or the
+// square of `square_size` about its centroid when it has no boundary shape
+static void subset_pixels(const std::vector<int>& mine, const dicegpu_shape* shapes, const int32_t* vx,
+                          const int32_t* vy, int cx, int cy, int square_size, std::vector<int32_t>& px,
+                          std::vector<int32_t>& py) {
+  px.clear();
+  py.clear();
+  int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
+  bool any = false;
+  for (int k : mine) {
+    if (shapes[k].role != DICEGPU_ROLE_BOUNDARY) continue;
+    int a, b, c, d;
+    shape_box(shapes[k], vx, vy, a, b, c, d);
+    if (!any) { x0 = a; x1 = b; y0 = c; y1 = d; any = true; }
+    else { x0 = std::min(x0, a); x1 = std::max(x1, b); y0 = std::min(y0, c); y1 = std::max(y1, d); }
+  }
+  if (!any) {
+    if (square_size < 1) return;
+    const int hw = square_size / 2;
+    for (int y = cy - hw; y <= cy + hw; ++y)
+      for (int x = cx - hw; x <= cx + hw; ++x) { px.push_back(x < 0 ? 0 : x); py.push_back(y < 0 ? 0 : y); }
+    return;
+  }
+  for (int y = y0; y <= y1; ++y)
+    for (int x = x0; x <= x1; ++x) {
+      bool in = false, out = false;
+      const int ex = x < 0 ? 0 : x, ey = y < 0 ? 0 : y;
+      for (int k : mine) {
+        if (shapes[k].role == DICEGPU_ROLE_BOUNDARY) in = in || shape_has(shapes[k], vx, vy, x, y, false);
+        else if (shapes[k].role == DICEGPU_ROLE_EXCLUDED) out = out || shape_has(shapes[k], vx, vy, ex, ey, true);
+      }
+      if (in && !out) { px.push_back(ex); py.push_back(ey); }
+    }
+}
+
+static bool group_shapes(int n, int n_shapes, const dicegpu_shape* shapes, std::vector<std::vector<int>>& by) {
+  by.assign(n, {});
+  for (int k = 0; k < n_shapes; ++k) {
+    if (shapes[k].subset < 0 || shapes[k].subset >= n) return false;
+    by[shapes[k].subset].push_back(k);
+  }
+  return true;
+}
 }  // namespace
 
-// Pixel lists of n conformal subsets: the union of each subset's boundary
-// shapes ordered by (y, x) (Subset(cx, cy, Conformal_Area_Def),
-// DICe_Subset.cpp:115-142; negative coordinates clamped to 0), without the
-// pixels inside its excluded shapes.  With px == NULL only offsets[n+1] is
-// filled.
+// Pixel lists of n subsets from their shapes (Subset(cx, cy,
+// Conformal_Area_Def), DICe_Subset.cpp:115-168; negative coordinates clamped
+// to 0).  Subsets without boundary shapes are squares of square_size about
+// the field rows' coordinates (fields may be NULL when every subset has
+// boundary shapes).  With px == NULL only offsets[n+1] is filled.
 extern "C" int oracle_rasterize(int n, int n_shapes, const dicegpu_shape* shapes, const int32_t* vx,
-                                const int32_t* vy, int32_t* offsets, int32_t* px, int32_t* py) {
+                                const int32_t* vy, const double* fields, int square_size,
+                                int32_t* offsets, int32_t* px, int32_t* py) {
   if (n < 0 || n_shapes < 0 || !offsets || (n_shapes && !shapes)) return DICEGPU_ERR_ARG;
-  std::vector<std::vector<int>> by_subset(n);
-  for (int k = 0; k < n_shapes; ++k) {
-    if (shapes[k].subset < 0 || shapes[k].subset >= n) return DICEGPU_ERR_ARG;
-    by_subset[shapes[k].subset].push_back(k);
-  }
+  std::vector<std::vector<int>> by;
+  if (!group_shapes(n, n_shapes, shapes, by)) return DICEGPU_ERR_ARG;
   offsets[0] = 0;
+  std::vector<int32_t> lx, ly;
   for (int i = 0; i < n; ++i) {
-    int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
-    bool any = false;
-    for (int k : by_subset[i]) {
-      if (shapes[k].role != 0) continue;
-      int a, b, c, d;
-      shape_box(shapes[k], vx, vy, a, b, c, d);
-      if (!any) { x0 = a; x1 = b; y0 = c; y1 = d; any = true; }
-      else { x0 = std::min(x0, a); x1 = std::max(x1, b); y0 = std::min(y0, c); y1 = std::max(y1, d); }
+    const int cx = fields ? (int)fields[(long)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_X] : 0;
+    const int cy = fields ? (int)fields[(long)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_Y] : 0;
+    subset_pixels(by[i], shapes, vx, vy, cx, cy, fields ? square_size : 0, lx, ly);
+    if (px)
+      for (size_t k = 0; k < lx.size(); ++k) { px[offsets[i] + k] = lx[k]; py[offsets[i] + k] = ly[k]; }
+    offsets[i + 1] = offsets[i] + (int32_t)lx.size();
+  }
+  return 0;
+}
+
+// Schema::execute_correlation for subsets defined by shapes, with
+// obstructions and blocking subsets (see dicegpu_set_subset_shapes and
+// dicegpu_set_blocking).  The generic routine runs the subsets in threads;
+// the tracking routine with blocking runs them in index order, each blocked
+// subset's blocked pixels taken from its blockers' fields as they stand
+// (check_for_blocking_subsets, DICe_Schema.cpp:4529-4557).  Blocked and
+// blocking subsets take the simplex unless params.override_force_simplex
+// (DICe_Schema.cpp:2160-2185).
+extern "C" int oracle_execute_frame_shapes(const dicegpu_params* params, int w, int h, const float* ref,
+                                           const float* def, int n, double* fields, int n_shapes,
+                                           const dicegpu_shape* shapes, const int32_t* vx,
+                                           const int32_t* vy, const int32_t* block_offsets,
+                                           const int32_t* block_ids, const uint8_t* force_simplex,
+                                           int first_frame, int nthreads) {
+  if (!params || !fields || n < 1) return DICEGPU_ERR_ARG;
+  std::vector<std::vector<int>> by;
+  if (!group_shapes(n, n_shapes, shapes, by)) return DICEGPU_ERR_ARG;
+  // pixel lists and obstruction sets
+  std::vector<int32_t> offsets(n + 1, 0), px, py, lx, ly;
+  std::vector<PixelSet> obst(n);
+  std::vector<char> conformal(n, 0);
+  for (int i = 0; i < n; ++i) {
+    const double* f = fields + (long)i * DICEGPU_FIELD_STRIDE;
+    subset_pixels(by[i], shapes, vx, vy, (int)f[DICEGPU_F_COORD_X], (int)f[DICEGPU_F_COORD_Y],
+                  params->subset_size, lx, ly);
+    px.insert(px.end(), lx.begin(), lx.end());
+    py.insert(py.end(), ly.begin(), ly.end());
+    offsets[i + 1] = offsets[i] + (int32_t)lx.size();
+    for (int k : by[i]) {
+      if (shapes[k].role == DICEGPU_ROLE_OBSTRUCTED) owned_pixels(shapes[k], vx, vy, obst[i]);
+      if (shapes[k].role == DICEGPU_ROLE_BOUNDARY) conformal[i] = 1;
     }
-    int cnt = 0;
-    for (int y = y0; any && y <= y1; ++y)
-      for (int x = x0; x <= x1; ++x) {
-        bool in = false, out = false;
-        for (int k : by_subset[i]) {
-          const bool h = shape_has(shapes[k], vx, vy, x, y);
-          if (shapes[k].role == 0) in = in || h;
-          else out = out || h;
-        }
-        if (in && !out) {
-          if (px) {
-            px[offsets[i] + cnt] = x < 0 ? 0 : x;
-            py[offsets[i] + cnt] = y < 0 ? 0 : y;
-          }
-          ++cnt;
-        }
+  }
+  // forced simplex: the caller's flags, blocked and blocking subsets
+  std::vector<uint8_t> force(n, 0);
+  for (int i = 0; i < n; ++i) force[i] = force_simplex ? force_simplex[i] : 0;
+  bool any_block = false;
+  if (block_offsets) {
+    for (int i = 0; i < n; ++i)
+      for (int k = block_offsets[i]; k < block_offsets[i + 1]; ++k) {
+        if (block_ids[k] < 0 || block_ids[k] >= n) return DICEGPU_ERR_ARG;
+        any_block = true;
+        if (!params->override_force_simplex) { force[i] = 1; force[block_ids[k]] = 1; }
       }
-    offsets[i + 1] = offsets[i] + cnt;
+  }
+  FrameJob J;
+  const int rc = prepare_frame(params, w, h, ref, def, J);
+  if (rc) return rc;
+  J.n = n; J.fields = fields; J.offsets = offsets.data(); J.px = px.data(); J.py = py.data();
+  J.force_simplex = force.data(); J.first_frame = first_frame != 0;
+  J.gn_out = nullptr; J.sx_out = nullptr; J.unc = nullptr;
+  J.obst = &obst;
+  const bool tracking = params->correlation_routine == DICEGPU_TRACKING_ROUTINE && any_block;
+  if (!tracking) {
+    run_parallel(J, nthreads);
+    return 0;
+  }
+  ShapeFn sf;
+  sf.init(J.C.P);
+  for (int i = 0; i < n; ++i) {
+    PixelSet blocked;
+    for (int k = block_offsets[i]; k < block_offsets[i + 1]; ++k) {
+      const int j = block_ids[k];
+      if (!conformal[j]) continue;   // deformed_shapes of a square subset is empty
+      const double* fj = fields + (long)j * DICEGPU_FIELD_STRIDE;
+      ShapeFn sj = sf;
+      sj.from_fields(fj);
+      for (int m : by[j]) {
+        if (shapes[m].role != DICEGPU_ROLE_BOUNDARY) continue;
+        if (shapes[m].kind == 0) return DICEGPU_ERR_UNSUPPORTED;   // circle deformation throws
+        deformed_pixels(shapes[m], vx, vy, sj, (int)fj[DICEGPU_F_COORD_X], (int)fj[DICEGPU_F_COORD_Y],
+                        (float)params->obstruction_skin_factor, blocked);
+      }
+    }
+    J.blocked = &blocked;
+    run_range(J, i, i + 1);
+    J.blocked = nullptr;
   }
   return 0;
 }

@@ -73,7 +73,18 @@ int oracle_map(const dicegpu_params* params, const double* fields, int n, const 
 /* Pixel lists of conformal subsets from shapes (get_owned_pixels); with
  * px == NULL only offsets[n + 1] is filled. */
 int oracle_rasterize(int n, int n_shapes, const dicegpu_shape* shapes, const int32_t* vx,
-                     const int32_t* vy, int32_t* offsets, int32_t* px, int32_t* py);
+                     const int32_t* vy, const double* fields, int square_size, int32_t* offsets,
+                     int32_t* px, int32_t* py);
+
+/* Schema::execute_correlation over subsets defined by shapes (boundary,
+ * excluded, obstructed; squares where a subset has no boundary), with
+ * blocking subsets (block_offsets[n+1], block_ids; NULL for none) under the
+ * generic or tracking routine of params. */
+int oracle_execute_frame_shapes(const dicegpu_params* params, int w, int h, const float* ref,
+                                const float* def, int n, double* fields, int n_shapes,
+                                const dicegpu_shape* shapes, const int32_t* vx, const int32_t* vy,
+                                const int32_t* block_offsets, const int32_t* block_ids,
+                                const uint8_t* force_simplex, int first_frame, int nthreads);
 
 /* Defaults of dice_default_params (same values as dicegpu_default_params). */
 int oracle_default_params(dicegpu_params* p);

@@ -62,7 +62,9 @@ def lib():
         L.oracle_map.restype = ci
         L.oracle_map.argtypes = [P, vp, ci, vp, ctypes.c_float, ctypes.c_float, vp]
         L.oracle_rasterize.restype = ci
-        L.oracle_rasterize.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp]
+        L.oracle_rasterize.argtypes = [ci, ci, vp, vp, vp, vp, ci, vp, vp, vp]
+        L.oracle_execute_frame_shapes.restype = ci
+        L.oracle_execute_frame_shapes.argtypes = [P, ci, ci, vp, vp, ci, vp, ci, vp, vp, vp, vp, vp, vp, ci, ci]
         _lib = L
     return _lib
 
@@ -113,21 +115,48 @@ def shape_map(params, field_row, xy, cx, cy):
     return out
 
 
-def rasterize(n, shapes, vx=None, vy=None):
-    """Pixel lists (offsets, px, py) of n conformal subsets from their shapes
-    (dice_b200.abi.Shape), as get_owned_pixels builds them."""
+def rasterize(n, shapes, vx=None, vy=None, fields=None, square_size=0):
+    """Pixel lists (offsets, px, py) of n subsets from their shapes
+    (dice_b200.abi.Shape), as get_owned_pixels builds them; subsets without
+    boundary shapes are squares of square_size about the field rows'
+    coordinates (when fields are given)."""
     arr = shape_array(list(shapes))
     x = np.ascontiguousarray(vx if vx is not None else [0], dtype=np.int32)
     y = np.ascontiguousarray(vy if vy is not None else [0], dtype=np.int32)
+    f = None if fields is None else np.ascontiguousarray(fields, dtype=np.float64)
     offs = np.zeros(n + 1, np.int32)
     sp = ctypes.cast(arr, ctypes.c_void_p)
-    rc = lib().oracle_rasterize(n, len(arr), sp, _ptr(x), _ptr(y), _ptr(offs), None, None)
+    rc = lib().oracle_rasterize(n, len(arr), sp, _ptr(x), _ptr(y), _ptr(f), square_size, _ptr(offs), None, None)
     assert rc == 0, rc
     px = np.zeros(max(int(offs[-1]), 1), np.int32)
     py = np.zeros_like(px)
-    rc = lib().oracle_rasterize(n, len(arr), sp, _ptr(x), _ptr(y), _ptr(offs), _ptr(px), _ptr(py))
+    rc = lib().oracle_rasterize(n, len(arr), sp, _ptr(x), _ptr(y), _ptr(f), square_size, _ptr(offs),
+                                _ptr(px), _ptr(py))
     assert rc == 0, rc
     return offs, px[:offs[-1]], py[:offs[-1]]
+
+
+def execute_frame_shapes(params, ref, deff, fields, shapes, vx=None, vy=None, block_offsets=None,
+                         block_ids=None, force_simplex=None, first_frame=True, nthreads=1):
+    """Schema::execute_correlation over subsets defined by shapes with
+    obstructions and blocking subsets; updates `fields` in place."""
+    ref = np.ascontiguousarray(ref, dtype=np.float32)
+    deff = np.ascontiguousarray(deff, dtype=np.float32)
+    assert fields.dtype == np.float64 and fields.flags.c_contiguous
+    h, w = ref.shape
+    n = fields.shape[0]
+    arr = shape_array(list(shapes))
+    x = np.ascontiguousarray(vx if vx is not None else [0], dtype=np.int32)
+    y = np.ascontiguousarray(vy if vy is not None else [0], dtype=np.int32)
+    bo = None if block_offsets is None else np.ascontiguousarray(block_offsets, dtype=np.int32)
+    bi = None if block_ids is None else np.ascontiguousarray(block_ids if len(block_ids) else [0], dtype=np.int32)
+    fs = None if force_simplex is None else np.ascontiguousarray(force_simplex, dtype=np.uint8)
+    rc = lib().oracle_execute_frame_shapes(ctypes.byref(params), w, h, _ptr(ref), _ptr(deff), n, _ptr(fields),
+                                           len(arr), ctypes.cast(arr, ctypes.c_void_p), _ptr(x), _ptr(y),
+                                           _ptr(bo), _ptr(bi), _ptr(fs), int(first_frame), nthreads)
+    if rc != 0:
+        raise RuntimeError("oracle_execute_frame_shapes: %d" % rc)
+    return fields
 
 
 def gauss_filter(img, mask_size=7):

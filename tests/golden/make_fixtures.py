@@ -19,6 +19,11 @@ Sources (paths inside the DICe project):
       gold/single_speckled_shift_{0..6}.txt
   tests/component/images/ImageB.tif, outFilter{5,7,9,11,13}.rawi  (240 x 161)
   tests/component/images/conformal.rawi                            (60 x 56)
+  tests/regression/conformal_subset_def/{subset_defs.txt, gold/DICe_solution_{0..4}.txt}
+  tests/regression/simple_obstruction/{subsets.txt, images/Img_{00..36}.tif,
+      gold/DICe_solution_0.txt}
+  tests/examples/{mechanism, obstruction}/subsets.txt,
+      tests/regression/mechanism_{skip_solves, optical_flow}/subsets.txt
 """
 import os
 import sys
@@ -88,6 +93,38 @@ def main(root):
     w, h, nb = np.frombuffer(raw[:12], np.uint32)
     assert nb == 4
     out["conformal_subset_image"] = np.frombuffer(raw[12:], np.float32).reshape(h, w).copy()
+    # Subset files (read as text by the parser tests) and the regression
+    # runs that use them: conformal_subset_def (five subsets on the speckled
+    # pair, two conformal, one with excluded / obstructed shapes and blocking
+    # subsets; TRACKING_ROUTINE) and simple_obstruction (a rectangle subset
+    # moving 2 px per frame under a static obstruction, 37 frames of 200 x 200).
+    for name, rel in (("conformal_subset_def", "regression/conformal_subset_def/subset_defs.txt"),
+                      ("simple_obstruction", "regression/simple_obstruction/subsets.txt"),
+                      ("mechanism", "examples/mechanism/subsets.txt"),
+                      ("obstruction_example", "examples/obstruction/subsets.txt"),
+                      ("mechanism_skip_solves", "regression/mechanism_skip_solves/subsets.txt"),
+                      ("mechanism_optical_flow", "regression/mechanism_optical_flow/subsets.txt")):
+        with open(os.path.join(root, "tests", rel)) as fh:
+            out["subset_file_" + name] = np.array(fh.read())
+    # columns: frame x y u v theta exx eyy gxy sigma status, one row per subset
+    out["conformal_subset_def_gold"] = np.concatenate([
+        _rows(os.path.join(root, "tests", "regression", "conformal_subset_def", "gold",
+                           "DICe_solution_%d.txt" % k)) for k in range(5)])
+    # the gold files as text, for comparisons the way the reference's
+    # regression harness makes them (DICe_Diff -t 0.05 -f 5.0E-5)
+    for k in range(5):
+        with open(os.path.join(root, "tests", "regression", "conformal_subset_def", "gold",
+                               "DICe_solution_%d.txt" % k)) as fh:
+            out["conformal_subset_def_gold_text_%d" % k] = np.array(fh.read())
+    with open(os.path.join(root, "tests", "regression", "simple_obstruction", "gold", "DICe_solution_0.txt")) as fh:
+        out["simple_obstruction_gold_text"] = np.array(fh.read())
+    from PIL import Image
+    out["simple_obstruction_frames"] = np.stack([
+        np.array(Image.open(os.path.join(root, "tests", "regression", "simple_obstruction", "images",
+                                         "Img_%02d.tif" % k)).convert("L")) for k in range(37)])
+    # columns: frame x y u
+    out["simple_obstruction_gold"] = _rows(os.path.join(root, "tests", "regression", "simple_obstruction",
+                                                        "gold", "DICe_solution_0.txt"))
     path =os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_gold.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, {k: v.shape for k, v in out.items()})

@@ -145,7 +145,7 @@ def test_gpu_rasterizer_rejects_bad_shapes():
         s.set_ref_image(np.zeros((64, 64), np.float32))
         s.set_subsets(np.full(2, 32.0), np.full(2, 32.0))
         for bad in ([abi.circle(2, 5, 5, 2.0)],                    # subset out of range
-                    [abi.circle(0, 5, 5, 2.0, role=2)],            # unknown role
+                    [abi.circle(0, 5, 5, 2.0, role=3)],            # unknown role
                     [abi.circle(0, 5, 5, -1.0)],                   # negative radius
                     [abi.rectangle(0, 5, 5, 40000, 3)],            # extent above 32768
                     [abi.polygon(0, 0, 2)],                        # fewer than 3 vertices
