@@ -69,6 +69,8 @@ def polygon(subset, vertex_offset, vertex_count, role=0):
 def shape_array(shapes):
     return (Shape * len(shapes))(*shapes)
 UNCERTAINTY_STRIDE = 8
+VSG_STRIDE = 8
+VSG_STRAIN_XX, VSG_STRAIN_YY, VSG_STRAIN_XY, VSG_DUDX, VSG_DUDY, VSG_DVDX, VSG_DVDY, VSG_NEIGHBORS = range(8)
 
 ERR_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_STATE", -4: "ERR_NOMEM",
              -5: "ERR_TIMEOUT", -6: "ERR_UNSUPPORTED", -7: "ERR_DEVICE"}
@@ -230,15 +232,20 @@ def _declare(lib):
         "dicegpu_output_create": (c_int, [P, ctypes.c_char_p, ctypes.c_char_p, c_int, c_void_p,
                                           ctypes.POINTER(c_void_p)]),
         "dicegpu_output_destroy": (c_int, [c_void_p]),
+        "dicegpu_output_set_images": (c_int, [c_void_p, ctypes.c_char_p, ctypes.c_char_p]),
         "dicegpu_output_num_fields": (c_int, [c_void_p, ctypes.POINTER(c_int)]),
         "dicegpu_output_info_text": (c_int, [c_void_p, ctypes.c_char_p, ctypes.c_size_t,
                                              ctypes.POINTER(ctypes.c_size_t)]),
         "dicegpu_output_header_text": (c_int, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t,
                                                ctypes.POINTER(ctypes.c_size_t)]),
-        "dicegpu_output_row_text": (c_int, [c_void_p, c_int, c_void_p, c_void_p, ctypes.c_char_p, ctypes.c_size_t,
-                                            ctypes.POINTER(ctypes.c_size_t)]),
+        "dicegpu_output_row_text": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, ctypes.c_char_p,
+                                            ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
         "dicegpu_output_write_frame": (c_int, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, c_int, c_int, c_int,
-                                               c_int, c_void_p, c_void_p, c_int]),
+                                               c_int, c_void_p, c_void_p, c_void_p, c_int]),
+        "dicegpu_vsg_strain": (c_int, [c_void_p, c_int, c_void_p, c_int]),
+        "dicegpu_regular_grid": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
+                                         c_int, ctypes.POINTER(c_int)]),
+        "dicegpu_subset_file_apply_grid": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int]),
         "dicegpu_diff_files": (c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_double, c_int,
                                        c_int, c_int, ctypes.POINTER(c_int), ctypes.c_char_p, ctypes.c_size_t]),
         "dicegpu_diff_text": (c_int, [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t,

@@ -23,6 +23,7 @@
 #include "dg_engine.cuh"
 #include "dg_adjoint.cuh"
 #include "dg_raster.cuh"
+#include "dg_vsg.cuh"
 #include "dicegpu.h"
 
 using namespace dg;
@@ -373,6 +374,13 @@ struct dicegpu_ctx {
   std::vector<int32_t> h_blocked_slot; // their index among those, -1 otherwise
   // forced simplex: the caller's flags and the blocking rule's
   std::vector<uint8_t> h_force_user, h_force_block;
+  // VSG strain: the neighbour grid of the subset centres (rebuilt when the
+  // window or the coordinates change) and the results
+  int vsg_window = 0;
+  int vsg_ncx = 0, vsg_ncy = 0;
+  float vsg_x0 = 0.0f, vsg_y0 = 0.0f, vsg_cell = 1.0f, vsg_r2 = 0.0f;
+  DevBuf<int32_t> d_vsg_cell_off, d_vsg_cell_pts;
+  DevBuf<double> d_vsg;
 };
 
 // A failed runtime call returns DICEGPU_ERR_CUDA and clears the runtime's
@@ -539,6 +547,7 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   c->d_blocked_bits.release(); c->d_blk_off.release(); c->d_blk_ids.release(); c->d_wave.release();
   c->d_bwave.release(); c->d_dv_off.release(); c->d_dvx.release(); c->d_dvy.release();
   c->d_snapshot.release();
+  c->d_vsg_cell_off.release(); c->d_vsg_cell_pts.release(); c->d_vsg.release();
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -800,6 +809,7 @@ extern "C" int dicegpu_set_subsets(dicegpu_ctx* c, int n, const double* fields) 
     c->h_force_user.clear();
     clear_shapes(c);
   }
+  c->vsg_window = 0;
   c->n = n;
   c->frame_index = 0;
   c->unc_n = 0;
@@ -1165,6 +1175,81 @@ static int ensure_blocked_words(dicegpu_ctx* c) {
   return DICEGPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// VSG strain (VSG_Strain_Post_Processor)
+// ---------------------------------------------------------------------------
+// The uniform grid of the subset centres for a window: cell size >= the
+// search radius + 1 px, so the 3 x 3 cells around a centre hold every
+// neighbour even when a centre sits on a cell edge.
+static int build_vsg_grid(dicegpu_ctx* c, int window) {
+  const int n = c->n;
+  std::vector<double> rows((size_t)n * DICEGPU_FIELD_STRIDE);
+  CK(cudaMemcpyAsync(rows.data(), c->d_fields, rows.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // radius of the reference's neighbourhood search (initialize_neighborhood)
+  const float rad = (float)((float)window / 2.0);
+  const float r2 = rad * rad + 1.0e-5f;
+  float x0 = 0.0f, y0 = 0.0f, x1 = 0.0f, y1 = 0.0f;
+  for (int i = 0; i < n; ++i) {
+    const float x = (float)rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_X];
+    const float y = (float)rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_Y];
+    if (!std::isfinite(x) || !std::isfinite(y)) return DICEGPU_ERR_ARG;
+    if (i == 0 || x < x0) x0 = x;
+    if (i == 0 || y < y0) y0 = y;
+    if (i == 0 || x > x1) x1 = x;
+    if (i == 0 || y > y1) y1 = y;
+  }
+  float cell = std::ceil(std::sqrt(r2)) + 1.0f;
+  // at most ~4 cells per subset: sparse centres over a wide field get wider cells
+  while (((double)(x1 - x0) / cell + 1.0) * ((double)(y1 - y0) / cell + 1.0) > 4.0 * n + 16.0) cell *= 2.0f;
+  const int ncx = (int)std::floor((x1 - x0) / cell) + 1, ncy = (int)std::floor((y1 - y0) / cell) + 1;
+  std::vector<int32_t> off((size_t)ncx * ncy + 1, 0), pts(n), cell_of(n);
+  for (int i = 0; i < n; ++i) {
+    const float x = (float)rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_X];
+    const float y = (float)rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_Y];
+    const int gx = std::min(std::max((int)std::floor((x - x0) / cell), 0), ncx - 1);
+    const int gy = std::min(std::max((int)std::floor((y - y0) / cell), 0), ncy - 1);
+    cell_of[i] = gy * ncx + gx;
+    ++off[cell_of[i] + 1];
+  }
+  for (size_t k = 0; k + 1 < off.size(); ++k) off[k + 1] += off[k];
+  {
+    std::vector<int32_t> fill(off.begin(), off.end() - 1);
+    for (int i = 0; i < n; ++i) pts[fill[cell_of[i]]++] = i;
+  }
+  int rc;
+  if ((rc = c->d_vsg_cell_off.ensure(off.size())) || (rc = c->d_vsg_cell_pts.ensure(n))) return rc;
+  CK(cudaMemcpy(c->d_vsg_cell_off.p, off.data(), off.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_vsg_cell_pts.p, pts.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  c->vsg_ncx = ncx;
+  c->vsg_ncy = ncy;
+  c->vsg_x0 = x0;
+  c->vsg_y0 = y0;
+  c->vsg_cell = cell;
+  c->vsg_r2 = r2;
+  c->vsg_window = window;
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_vsg_strain(dicegpu_ctx* c, int window_size, double* out, int on_device) {
+  if (!c || c->n < 1 || window_size == 0) return DICEGPU_ERR_ARG;
+  if (window_size < 0) return DICEGPU_ERR_UNSUPPORTED;   // k-nearest neighbourhoods
+  int rc;
+  if (c->vsg_window != window_size && (rc = build_vsg_grid(c, window_size))) return rc;
+  if ((rc = c->d_vsg.ensure((size_t)c->n * DICEGPU_VSG_STRIDE))) return rc;
+  VsgArgs va{c->d_fields, c->n, c->d_vsg_cell_off.p, c->d_vsg_cell_pts.p, c->vsg_ncx, c->vsg_ncy,
+             c->vsg_x0, c->vsg_y0, c->vsg_cell, c->vsg_r2, c->d_vsg.p};
+  const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)c->n * 32 + 255) / 256, (int64_t)c->num_sms * 16);
+  vsg_kernel<<<blocks, 256, 0, c->stream>>>(va);
+  CK(cudaGetLastError());
+  c->launches += 1;
+  if (out)
+    CK(cudaMemcpyAsync(out, c->d_vsg.p, (size_t)c->n * DICEGPU_VSG_STRIDE * sizeof(double),
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+  if (out && !on_device) CK(cudaStreamSynchronize(c->stream));
+  return DICEGPU_OK;
+}
+
 extern "C" int dicegpu_get_subset_pixels(dicegpu_ctx* c, int32_t* offsets, int32_t* px, int32_t* py) {
   if (!c || !offsets || !c->use_lists || c->n < 1) return DICEGPU_ERR_ARG;
   CK(cudaStreamSynchronize(c->stream));
@@ -1214,6 +1299,7 @@ extern "C" int dicegpu_load_fields(dicegpu_ctx* c, const double* src, int on_dev
   CK(cudaMemcpyAsync(c->d_fields, src, (size_t)c->n * DICEGPU_FIELD_STRIDE * sizeof(double),
                      on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
   c->frame_index = 0;
+  c->vsg_window = 0;
   return DICEGPU_OK;
 }
 

@@ -32,10 +32,11 @@
 
 namespace {
 
-// a column of the output: a field-row column, an uncertainty column, or 0
+// a column of the output: a field-row column, an uncertainty column, a VSG
+// column, or 0
 struct Column {
   std::string name;
-  int src;   // 0: field row, 1: uncertainty row, 2: always 0
+  int src;   // 0: field row, 1: uncertainty row, 2: always 0, 3: VSG row
   int col;
 };
 
@@ -75,6 +76,10 @@ bool lookup(const std::string& name, Column& c) {
       {"STEREO_DISPLACEMENT_Y", {2, 0}}, {"MODEL_DISPLACEMENT_X", {2, 0}}, {"MODEL_DISPLACEMENT_Y", {2, 0}},
       {"MODEL_DISPLACEMENT_Z", {2, 0}}, {"CROSS_EPI_ERROR", {2, 0}}, {"EPI_A", {2, 0}}, {"EPI_B", {2, 0}},
       {"EPI_C", {2, 0}},
+      // VSG_Strain_Post_Processor fields (DICe_PostProcessor.h:105-117)
+      {"VSG_STRAIN_XX", {3, DICEGPU_VSG_STRAIN_XX}}, {"VSG_STRAIN_YY", {3, DICEGPU_VSG_STRAIN_YY}},
+      {"VSG_STRAIN_XY", {3, DICEGPU_VSG_STRAIN_XY}}, {"VSG_DUDX", {3, DICEGPU_VSG_DUDX}},
+      {"VSG_DUDY", {3, DICEGPU_VSG_DUDY}}, {"VSG_DVDX", {3, DICEGPU_VSG_DVDX}}, {"VSG_DVDY", {3, DICEGPU_VSG_DVDY}},
   };
   const auto it = table.find(name);
   if (it == table.end()) return false;
@@ -124,8 +129,8 @@ struct dicegpu_output {
   std::vector<Column> cols;
   std::string delim;
   bool omit_row_id;
-  std::string ref_image, def_image, version;
-  int subset_size, step_x, step_y, strain_window, incremental;
+  std::string ref_image, def_image, version, init_method;
+  int subset_size, step_x, step_y, strain_window, incremental, sort_rows;
 
   std::string info_text() const {
     std::string s;
@@ -141,7 +146,7 @@ struct dicegpu_output {
     appendf(s, "*** Image gradient method: %s\n", grad_name(p.gradient_method));
     appendf(s, "*** Optimization method: %s\n", opt_name(p.optimization));
     appendf(s, "*** Projection method: DISPLACEMENT_BASED\n");
-    appendf(s, "*** Guess initialization method: USE_FIELD_VALUES\n");
+    appendf(s, "*** Guess initialization method: %s\n", init_method.c_str());
     appendf(s, "*** Seed location: N/A\n");
     appendf(s, "*** Shape functions: ");
     if (p.shape_function == DICEGPU_QUADRATIC_SF) {
@@ -169,13 +174,14 @@ struct dicegpu_output {
     appendf(s, "\n");
     return s;
   }
-  std::string row_text(int row, const double* f, const double* u) const {
+  std::string row_text(int row, const double* f, const double* u, const double* g) const {
     std::string s;
     if (!omit_row_id) appendf(s, "%i%s", row, delim.c_str());
     for (size_t i = 0; i < cols.size(); ++i) {
       double v = 0.0;
       if (cols[i].src == 0) v = f[cols[i].col];
       else if (cols[i].src == 1 && u) v = u[cols[i].col];
+      else if (cols[i].src == 3 && g) v = g[cols[i].col];
       const float sv = (float)v;
       appendf(s, "%s%4.4E", i ? delim.c_str() : "", (double)sv);
     }
@@ -201,6 +207,8 @@ extern "C" int dicegpu_output_create(const dicegpu_params* params, const char* f
   o->step_y = info ? info->step_size_y : -1;
   o->strain_window = info ? info->strain_window : -1;
   o->incremental = info ? info->incremental : 0;
+  o->sort_rows = info ? info->sort_rows : 0;
+  o->init_method = info && info->initialization_method ? info->initialization_method : "USE_FIELD_VALUES";
   std::vector<std::string> names;
   if (!fields) {
     // Output_Spec's default columns (DICe_Schema.cpp:4683-4696)
@@ -246,6 +254,13 @@ extern "C" int dicegpu_output_destroy(dicegpu_output* o) {
   return DICEGPU_OK;
 }
 
+extern "C" int dicegpu_output_set_images(dicegpu_output* o, const char* ref_image, const char* def_image) {
+  if (!o) return DICEGPU_ERR_ARG;
+  if (ref_image) o->ref_image = ref_image;
+  if (def_image) o->def_image = def_image;
+  return DICEGPU_OK;
+}
+
 extern "C" int dicegpu_output_num_fields(const dicegpu_output* o, int* n) {
   if (!o || !n) return DICEGPU_ERR_ARG;
   *n = (int)o->cols.size();
@@ -264,9 +279,9 @@ extern "C" int dicegpu_output_header_text(const dicegpu_output* o, const char* r
 }
 
 extern "C" int dicegpu_output_row_text(const dicegpu_output* o, int row_index, const double* fields,
-                                       const double* unc, char* buf, size_t cap, size_t* len) {
+                                       const double* unc, const double* vsg, char* buf, size_t cap, size_t* len) {
   if (!o || !fields) return DICEGPU_ERR_ARG;
-  return give(o->row_text(row_index, fields, unc), buf, cap, len);
+  return give(o->row_text(row_index, fields, unc, vsg), buf, cap, len);
 }
 
 namespace {
@@ -285,9 +300,11 @@ bool write_all(const std::string& path, const std::string& text, const char* mod
 
 extern "C" int dicegpu_output_write_frame(const dicegpu_output* o, const char* folder, const char* prefix,
                                           int frame, int first_frame, int num_frames, int n, const double* fields,
-                                          const double* unc, int separate_files) {
+                                          const double* unc, const double* vsg, int separate_files) {
   if (!o || !folder || !prefix || !fields || n < 1) return DICEGPU_ERR_ARG;
   const std::string base = std::string(folder) + prefix + "_";
+  auto U = [&](int i) { return unc ? unc + (size_t)i * DICEGPU_UNCERTAINTY_STRIDE : nullptr; };
+  auto G = [&](int i) { return vsg ? vsg + (size_t)i * DICEGPU_VSG_STRIDE : nullptr; };
   if (separate_files) {
     const int total = digits(n);
     for (int i = 0; i < n; ++i) {
@@ -295,8 +312,7 @@ extern "C" int dicegpu_output_write_frame(const dicegpu_output* o, const char* f
       std::string name = base + std::string((size_t)std::max(total - mine, 0), '0') + std::to_string(i) + ".txt";
       if (frame == first_frame && !write_all(name, o->info_text() + o->header_text("FRAME"), "w"))
         return DICEGPU_ERR_ARG;
-      const double* u = unc ? unc + (size_t)i * DICEGPU_UNCERTAINTY_STRIDE : nullptr;
-      if (!write_all(name, o->row_text(frame, fields + (size_t)i * DICEGPU_FIELD_STRIDE, u), "a"))
+      if (!write_all(name, o->row_text(frame, fields + (size_t)i * DICEGPU_FIELD_STRIDE, U(i), G(i)), "a"))
         return DICEGPU_ERR_ARG;
     }
     return DICEGPU_OK;
@@ -308,9 +324,16 @@ extern "C" int dicegpu_output_write_frame(const dicegpu_output* o, const char* f
     zeros = std::max(total - mine, 0);
   }
   std::string text = o->info_text() + o->header_text("SUBSET_ID");
-  for (int i = 0; i < n; ++i)
-    text += o->row_text(i, fields + (size_t)i * DICEGPU_FIELD_STRIDE,
-                        unc ? unc + (size_t)i * DICEGPU_UNCERTAINTY_STRIDE : nullptr);
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  if (o->sort_rows) {
+    // sort_txt_output: by x, then y (DICe_Schema.cpp:4430-4450), on float coordinates
+    auto X = [&](int i) { return (float)fields[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_X]; };
+    auto Y = [&](int i) { return (float)fields[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_Y]; };
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return X(a) < X(b) || (X(a) == X(b) && Y(a) < Y(b)); });
+  }
+  for (int i : order) text += o->row_text(i, fields + (size_t)i * DICEGPU_FIELD_STRIDE, U(i), G(i));
   const std::string name = base + std::string((size_t)zeros, '0') + std::to_string(frame) + ".txt";
   return write_all(name, text, "w") ? DICEGPU_OK : DICEGPU_ERR_ARG;
 }

@@ -27,6 +27,7 @@ namespace {
 struct Seed {
   double v[6] = {0, 0, 0, 0, 0, 0};   // u, v, ex, ey, gxy, theta
   int flags = 0;
+  int loc_x = 0, loc_y = 0;           // LOCATION (region-of-interest seeds)
 };
 
 struct ShapeDef {
@@ -252,6 +253,8 @@ Seed read_seed(std::istream& is, bool roi) {
       if (!roi) fail("a conformal subset's seed takes no location (the centroid is used)");
       if (t.size() <= 2 || !is_number(t[1]) || !is_number(t[2])) fail("seed location needs x and y");
       has_loc = true;
+      sd.loc_x = to_int(t[1]);
+      sd.loc_y = to_int(t[2]);
     } else if (t[0] == "DISPLACEMENT" || t[0] == "NORMAL_STRAIN") {
       if (t.size() <= 2 || !is_number(t[1]) || !is_number(t[2])) fail("seed " + t[0] + " needs x and y values");
       const int k = t[0] == "DISPLACEMENT" ? 0 : 2;
@@ -554,6 +557,135 @@ extern "C" int dicegpu_subset_file_features(const dicegpu_subset_file* f, uint8_
   return DICEGPU_OK;
 }
 
+namespace {
+// Pixel ownership of an undeformed shape (get_owned_pixels,
+// DICe_Shape.cpp:136-219, 259-279, 322-420), tested per pixel; the same
+// float arithmetic as the device rasterizer, atan2 correctly rounded.
+float angle_2d(float x1, float y1, float x2, float y2) {
+  const float t1 = (float)std::atan2((double)y1, (double)x1), t2 = (float)std::atan2((double)y2, (double)x2);
+  float d = t2 - t1;
+  while (d > 3.14159265358979323846) d -= 6.28318530717958647692;
+  while (d < -3.14159265358979323846) d += 6.28318530717958647692;
+  return d;
+}
+bool owns(const ShapeDef& d, int x, int y) {
+  const dicegpu_shape& s = d.s;
+  if (s.kind == DICEGPU_SHAPE_CIRCLE) {
+    const int lim = (int)s.radius + 1;
+    if (std::abs(x - s.cx) > lim || std::abs(y - s.cy) > lim) return false;
+    const float r2 = s.radius * s.radius;
+    return (float)((x - s.cx) * (x - s.cx)) + (float)((y - s.cy) * (y - s.cy)) <= r2;
+  }
+  if (s.kind == DICEGPU_SHAPE_RECTANGLE) {
+    const int ox = s.cx - s.width / 2, oy = s.cy - s.height / 2;
+    return x >= ox && x < ox + s.width && y >= oy && y < oy + s.height;
+  }
+  const int nv = (int)d.vx.size();
+  float angle = 0.0f;
+  for (int i = 0; i < nv; ++i) {
+    const int j = (i + 1 == nv) ? 0 : i + 1;
+    angle += angle_2d((float)(d.vx[i] - x), (float)(d.vy[i] - y), (float)(d.vx[j] - x), (float)(d.vy[j] - y));
+  }
+  return std::abs(angle) >= 3.14159265358979323846;
+}
+
+// valid_correlation_point (DICe_Decomp.cpp:1070-1120) without the optional
+// gradient threshold
+bool valid_point(const ConformalDef& roi, int x, int y, int s, int w, int h) {
+  if (x < s - 1 || x > w - s || y < s - 1 || y > h - s) return false;
+  bool in = false;
+  for (const auto& d : roi.shapes)
+    if (d.s.role == DICEGPU_ROLE_BOUNDARY && owns(d, x, y)) { in = true; break; }
+  if (!in) return false;
+  const int cx0 = x - s / 2, cy0 = y - s / 2;
+  const int cxs[4] = {cx0, cx0 + s, cx0 + s, cx0}, cys[4] = {cy0, cy0, cy0 + s, cy0 + s};
+  for (int k = 0; k < 4; ++k)
+    for (const auto& d : roi.shapes)
+      if (d.s.role == DICEGPU_ROLE_EXCLUDED && owns(d, cxs[k], cys[k])) return false;
+  return true;
+}
+}  // namespace
+
+extern "C" int dicegpu_regular_grid(const dicegpu_subset_file* f, int width, int height, int step_size,
+                                    int subset_size, double* xy, int32_t* neighbor_ids, int32_t* seed_roi,
+                                    int cap, int* n_out) {
+  if (!n_out || width < 1 || height < 1 || step_size <= 0 || subset_size < 1) return DICEGPU_ERR_ARG;
+  if (f && !f->roi) return DICEGPU_ERR_ARG;
+  // the regions: the file's, or the whole image (a dummy rectangle ROI)
+  std::map<int, ConformalDef> whole;
+  const std::map<int, ConformalDef>* rois = f ? &f->conformal : &whole;
+  if (!f) {
+    ShapeDef d;
+    std::memset(&d.s, 0, sizeof(d.s));
+    d.s.kind = DICEGPU_SHAPE_RECTANGLE;
+    d.s.cx = width / 2;
+    d.s.cy = height / 2;
+    d.s.width = width;
+    d.s.height = height;
+    whole[0].shapes.push_back(d);
+  }
+  const int s = subset_size;
+  int n = 0;
+  auto push = [&](int x, int y, int neigh, int roi_of_seed) {
+    if (n < cap) {
+      if (xy) { xy[2 * n] = x; xy[2 * n + 1] = y; }
+      if (neighbor_ids) neighbor_ids[n] = neigh;
+      if (seed_roi) seed_roi[n] = roi_of_seed;
+    }
+    ++n;
+  };
+  for (const auto& kv : *rois) {
+    const ConformalDef& roi = kv.second;
+    int num_rows = 0, num_cols = 0, seed_row = 0, seed_col = 0, x = s - 1, y = s - 1;
+    int seed_x = 0, seed_y = 0;
+    bool has_seed = false;
+    if (f) {
+      const auto it = f->seeds.find(kv.first);
+      if (it != f->seeds.end()) { seed_x = it->second.loc_x; seed_y = it->second.loc_y; has_seed = true; }
+    }
+    while (x < width - s) {
+      if (x + step_size / 2 < seed_x) seed_col++;
+      x += step_size;
+      num_cols++;
+    }
+    while (y < height - s) {
+      if (y + step_size / 2 < seed_y) seed_row++;
+      y += step_size;
+      num_rows++;
+    }
+    // the seed point's id is the snakes' first neighbour only when a seed
+    // was given (seed_subset_id stays -1 otherwise)
+    int seed_id = -1;
+    x = s - 1 + seed_col * step_size;
+    y = s - 1 + seed_row * step_size;
+    if (valid_point(roi, x, y, s, width, height)) {
+      if (has_seed) seed_id = n;
+      push(x, y, -1, has_seed ? kv.first : -1);
+    } else if (!(seed_row == 0 && seed_col == 0)) {
+      return DICEGPU_ERR_ARG;   // the seed is not a valid correlation point
+    }
+    // snake right from the seed, then left
+    for (int dir0 = 1; dir0 >= -1; dir0 -= 2) {
+      const int start = n;
+      int direction = dir0, row = seed_row, col = seed_col;
+      while (row >= 0 && row < num_rows) {
+        if ((direction == 1 && row + 1 >= num_rows) || (direction == -1 && row - 1 < 0)) {
+          direction *= -1;
+          col += dir0;
+        } else {
+          row += direction;
+        }
+        if (col >= num_cols || col < 0) break;
+        x = s - 1 + col * step_size;
+        y = s - 1 + row * step_size;
+        if (valid_point(roi, x, y, s, width, height)) push(x, y, n == start ? seed_id : n - 1, -1);
+      }
+    }
+  }
+  *n_out = n;
+  return n <= cap ? DICEGPU_OK : DICEGPU_ERR_ARG;
+}
+
 extern "C" int dicegpu_subset_file_apply(const dicegpu_subset_file* f, dicegpu_ctx* ctx) {
   if (!f || !ctx) return DICEGPU_ERR_ARG;
   if (f->roi || !f->features.empty()) return DICEGPU_ERR_UNSUPPORTED;
@@ -612,4 +744,48 @@ extern "C" int dicegpu_subset_file_apply(const dicegpu_subset_file* f, dicegpu_c
     if ((rc = dicegpu_set_force_simplex(ctx, n, fl.data()))) return rc;
   }
   return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_subset_file_apply_grid(const dicegpu_subset_file* f, dicegpu_ctx* ctx, int width,
+                                              int height, int step_size) {
+  if (!ctx) return DICEGPU_ERR_ARG;
+  if (f && (!f->roi || !f->features.empty())) return DICEGPU_ERR_UNSUPPORTED;
+  dicegpu_params P;
+  int rc = dicegpu_get_params(ctx, &P);
+  if (rc) return rc;
+  if (P.subset_size < 1) return DICEGPU_ERR_ARG;
+  int n = 0;
+  rc = dicegpu_regular_grid(f, width, height, step_size, P.subset_size, nullptr, nullptr, nullptr, 0, &n);
+  if (rc != DICEGPU_OK && rc != DICEGPU_ERR_ARG) return rc;
+  if (n < 1) return DICEGPU_ERR_ARG;
+  std::vector<double> xy(2 * (size_t)n);
+  std::vector<int32_t> neigh(n), seed_roi(n);
+  if ((rc = dicegpu_regular_grid(f, width, height, step_size, P.subset_size, xy.data(), neigh.data(),
+                                 seed_roi.data(), n, &n)))
+    return rc;
+  std::vector<double> rows((size_t)n * DICEGPU_FIELD_STRIDE, 0.0);
+  for (int i = 0; i < n; ++i) {
+    double* r = &rows[(size_t)i * DICEGPU_FIELD_STRIDE];
+    r[DICEGPU_F_COORD_X] = xy[2 * i];
+    r[DICEGPU_F_COORD_Y] = xy[2 * i + 1];
+    if (P.shape_function == DICEGPU_QUADRATIC_SF) {
+      r[DICEGPU_F_QUAD_A] = 1.0;
+      r[DICEGPU_F_QUAD_A + 7] = 1.0;
+    }
+    if (!f || seed_roi[i] < 0) continue;
+    // Schema::initialize's seeding (DICe_Schema.cpp:1111-1143)
+    const Seed& sd = f->seeds.at(seed_roi[i]);
+    if ((sd.flags & (DICEGPU_SF_SEED_NORMAL_STRAIN | DICEGPU_SF_SEED_SHEAR_STRAIN)) &&
+        P.shape_function != DICEGPU_AFFINE_SF)
+      return DICEGPU_ERR_ARG;
+    r[DICEGPU_F_DISP_X] = sd.v[0];
+    r[DICEGPU_F_DISP_Y] = sd.v[1];
+    if (sd.flags & DICEGPU_SF_SEED_NORMAL_STRAIN) {
+      r[DICEGPU_F_STRETCH_XX] = sd.v[2];
+      r[DICEGPU_F_STRETCH_YY] = sd.v[3];
+    }
+    if (sd.flags & DICEGPU_SF_SEED_SHEAR_STRAIN) r[DICEGPU_F_SHEAR_XY] = sd.v[4];
+    if (sd.flags & DICEGPU_SF_SEED_ROTATION) r[DICEGPU_F_ROT_Z] = sd.v[5];
+  }
+  return dicegpu_set_subsets(ctx, n, rows.data());
 }

@@ -14,7 +14,8 @@ from . import abi
 class OutputInfo(ctypes.Structure):
     _fields_ = [("ref_image", ctypes.c_char_p), ("def_image", ctypes.c_char_p), ("version", ctypes.c_char_p),
                 ("subset_size", ctypes.c_int32), ("step_size_x", ctypes.c_int32), ("step_size_y", ctypes.c_int32),
-                ("strain_window", ctypes.c_int32), ("incremental", ctypes.c_int32)]
+                ("strain_window", ctypes.c_int32), ("incremental", ctypes.c_int32), ("sort_rows", ctypes.c_int32),
+                ("initialization_method", ctypes.c_char_p)]
 
 
 def _text(fn, *args):
@@ -30,13 +31,15 @@ class Output:
     None for the reference's default columns."""
 
     def __init__(self, params, fields=None, delimiter=" ", omit_row_id=False, ref_image="", def_image="",
-                 subset_size=None, step_size=(-1, -1), strain_window=-1, incremental=False, version=None):
+                 subset_size=None, step_size=(-1, -1), strain_window=-1, incremental=False, version=None,
+                 sort_rows=False, initialization_method=None):
         self.lib = abi.load_library()
         if isinstance(fields, (list, tuple)):
             fields = ",".join(fields)
         info = OutputInfo(ref_image.encode(), def_image.encode(), version.encode() if version else None,
                           params.subset_size if subset_size is None else subset_size, step_size[0], step_size[1],
-                          strain_window, int(incremental))
+                          strain_window, int(incremental), int(sort_rows),
+                          initialization_method.encode() if initialization_method else None)
         self._info = info
         h = ctypes.c_void_p()
         abi.check(self.lib.dicegpu_output_create(ctypes.byref(params), fields.encode() if fields else None,
@@ -44,27 +47,36 @@ class Output:
                                                  ctypes.byref(h)), "output_create")
         self.h = h
 
+    def set_images(self, ref_image=None, def_image=None):
+        abi.check(self.lib.dicegpu_output_set_images(self.h, ref_image.encode() if ref_image else None,
+                                                     def_image.encode() if def_image else None), "set_images")
+
     def info_text(self):
         return _text(self.lib.dicegpu_output_info_text, self.h)
 
     def header_text(self, row_id="FRAME"):
         return _text(self.lib.dicegpu_output_header_text, self.h, row_id.encode())
 
-    def row_text(self, row, fields_row, unc_row=None):
+    def row_text(self, row, fields_row, unc_row=None, vsg_row=None):
         f = np.ascontiguousarray(fields_row, np.float64)
         u = None if unc_row is None else np.ascontiguousarray(unc_row, np.float64)
+        g = None if vsg_row is None else np.ascontiguousarray(vsg_row, np.float64)
         return _text(self.lib.dicegpu_output_row_text, self.h, int(row), f.ctypes.data_as(ctypes.c_void_p),
-                     None if u is None else u.ctypes.data_as(ctypes.c_void_p))
+                     None if u is None else u.ctypes.data_as(ctypes.c_void_p),
+                     None if g is None else g.ctypes.data_as(ctypes.c_void_p))
 
-    def write_frame(self, folder, prefix, frame, fields, unc=None, first_frame=0, num_frames=0, separate_files=True):
+    def write_frame(self, folder, prefix, frame, fields, unc=None, vsg=None, first_frame=0, num_frames=0,
+                    separate_files=True):
         f = np.ascontiguousarray(fields, np.float64)
         u = None if unc is None else np.ascontiguousarray(unc, np.float64)
+        g = None if vsg is None else np.ascontiguousarray(vsg, np.float64)
         folder = str(folder)
         if folder and not folder.endswith("/"):
             folder += "/"
         abi.check(self.lib.dicegpu_output_write_frame(self.h, folder.encode(), prefix.encode(), frame, first_frame,
                                                       num_frames, f.shape[0], f.ctypes.data_as(ctypes.c_void_p),
                                                       None if u is None else u.ctypes.data_as(ctypes.c_void_p),
+                                                      None if g is None else g.ctypes.data_as(ctypes.c_void_p),
                                                       int(separate_files)), "output_write_frame")
 
     def close(self):

@@ -168,6 +168,15 @@ class Schema:
         abi.check(self.lib.dicegpu_set_blocking(self.ctx, offs.ctypes.data_as(ctypes.c_void_p),
                                                 ida.ctypes.data_as(ctypes.c_void_p)), "set_blocking")
 
+    def vsg_strain(self, window_size):
+        """VSG_Strain_Post_Processor on the current field rows: n x VSG_STRIDE
+        (strain xx, yy, xy, du/dx, du/dy, dv/dx, dv/dy, valid neighbours);
+        sets MATCH = -1 where the fit fails."""
+        out = np.zeros((self.n, abi.VSG_STRIDE), np.float64)
+        abi.check(self.lib.dicegpu_vsg_strain(self.ctx, int(window_size), out.ctypes.data_as(ctypes.c_void_p), 0),
+                  "vsg_strain")
+        return out
+
     def subset_pixels(self):
         """(offsets, px, py) of the context's subset pixel lists."""
         offs = np.zeros(self.n + 1, np.int32)

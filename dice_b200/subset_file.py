@@ -76,6 +76,17 @@ class SubsetFile:
         self.force_simplex = self.force_simplex[:n]
         self.seed_values, self.seed_flags, self.features = self.seed_values[:n], self.seed_flags[:n], self.features[:n]
 
+    def apply_grid(self, schema, width, height, step_size):
+        """Schema::initialize with a region-of-interest file and a step size."""
+        abi.check(self.lib.dicegpu_subset_file_apply_grid(self.h, schema.ctx, width, height, step_size),
+                  "subset_file_apply_grid")
+        n = ctypes.c_int()
+        p = abi.Params()
+        abi.check(self.lib.dicegpu_get_params(schema.ctx, ctypes.byref(p)), "get_params")
+        self.lib.dicegpu_regular_grid(self.h, width, height, step_size, p.subset_size, None, None, None, 0,
+                                      ctypes.byref(n))
+        schema.n = n.value
+
     def apply(self, schema):
         abi.check(self.lib.dicegpu_subset_file_apply(self.h, schema.ctx), "subset_file_apply")
         schema.n = self.info.n_subsets
@@ -87,3 +98,21 @@ class SubsetFile:
 
     def __del__(self):
         self.close()
+
+
+def regular_grid(subset_file, width, height, step_size, subset_size):
+    """create_regular_grid_of_correlation_points: (xy n x 2, neighbour ids,
+    seed region per point) for a region-of-interest file (or None: the whole
+    image), in the reference's order."""
+    lib = abi.load_library()
+    h = subset_file.h if subset_file is not None else None
+    n = ctypes.c_int()
+    rc = lib.dicegpu_regular_grid(h, width, height, step_size, subset_size, None, None, None, 0, ctypes.byref(n))
+    if rc not in (0, abi.ERR_ARG) or (rc == abi.ERR_ARG and n.value == 0):
+        raise SubsetFileError("regular grid: %s" % abi.ERR_NAMES.get(rc, rc))
+    xy = np.zeros((max(n.value, 1), 2), np.float64)
+    neigh = np.zeros(max(n.value, 1), np.int32)
+    seed = np.zeros(max(n.value, 1), np.int32)
+    abi.check(lib.dicegpu_regular_grid(h, width, height, step_size, subset_size, _vp(xy), _vp(neigh), _vp(seed),
+                                       n.value, ctypes.byref(n)), "regular_grid")
+    return xy[:n.value], neigh[:n.value], seed[:n.value]

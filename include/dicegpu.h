@@ -122,6 +122,19 @@ extern "C" {
 #define DICEGPU_U_RESIDUAL         5   /* FIELD_6 */
 #define DICEGPU_U_SSSIG            6   /* FIELD_7: mean squared gradient */
 
+/* VSG strain rows (dicegpu_vsg_strain), DICEGPU_VSG_STRIDE doubles: the
+ * VSG_Strain_Post_Processor fields (DICe_PostProcessor.h:105-117) and the
+ * number of valid neighbours used. */
+#define DICEGPU_VSG_STRIDE     8
+#define DICEGPU_VSG_STRAIN_XX  0   /* Green-Lagrange strains */
+#define DICEGPU_VSG_STRAIN_YY  1
+#define DICEGPU_VSG_STRAIN_XY  2
+#define DICEGPU_VSG_DUDX       3
+#define DICEGPU_VSG_DUDY       4
+#define DICEGPU_VSG_DVDX       5
+#define DICEGPU_VSG_DVDY       6
+#define DICEGPU_VSG_NEIGHBORS  7
+
 /* dice_correlate's record, DICe_api.h:65: x, y, u, v, theta, sigma, gamma, beta, flag */
 #define DICEGPU_API_STRIDE 9
 
@@ -306,6 +319,21 @@ int dicegpu_set_subset_shapes(dicegpu_ctx* ctx, int n_shapes, const dicegpu_shap
  * unless params.override_force_simplex.  offsets == NULL clears the lists.
  * Call after dicegpu_set_subset_shapes. */
 int dicegpu_set_blocking(dicegpu_ctx* ctx, const int32_t* offsets, const int32_t* ids);
+
+/* VSG_Strain_Post_Processor::execute (DICe_PostProcessor.cpp:931-1130) on
+ * the context's field rows: each subset's neighbours within window_size / 2
+ * pixels (strain_window_size_in_pixels; the reference's kd-tree radius
+ * search, squared distance in float < r^2 + 1e-5) with sigma >= 0 fit u and v
+ * by planes in double, giving du/dx .. dv/dy and the Green-Lagrange strains.
+ * Fewer than three valid neighbours, an invalid subset, or a reciprocal
+ * condition number below 1e-12 give zeros and set the subset's MATCH field
+ * to -1, as the reference does.  The reference estimates the condition
+ * number (GECON); it is computed exactly here, which differs only for
+ * nearly collinear neighbourhoods.  Writes n rows of DICEGPU_VSG_STRIDE
+ * doubles to out (device memory when on_device, else host; NULL: kept on the
+ * device only).  window_size < 0 (k nearest neighbours in the reference) is
+ * DICEGPU_ERR_UNSUPPORTED. */
+int dicegpu_vsg_strain(dicegpu_ctx* ctx, int window_size, double* out, int on_device);
 
 /* Copies the context's subset pixel lists to host memory: offsets[n + 1]
  * and, when px / py are not NULL, offsets[n] coordinates each. */

@@ -103,11 +103,36 @@ int dicegpu_subset_file_features(const dicegpu_subset_file* f, uint8_t* flags);
  * seeds' values), the conformal definitions as shapes (subsets without one
  * are squares of params.subset_size), the blocking lists and the
  * FORCE_SIMPLEX flags.  DICEGPU_ERR_UNSUPPORTED for a region-of-interest
- * file or a subset using a DICEGPU_SF_FEATURE_* option; DICEGPU_ERR_ARG when
+ * file (see dicegpu_subset_file_apply_grid) or a subset using a
+ * DICEGPU_SF_FEATURE_* option; DICEGPU_ERR_ARG when
  * a subset is neither conformal nor given a size (params.subset_size < 1)
  * or a seed sets strains under the quadratic shape function (the reference
  * throws there). */
 int dicegpu_subset_file_apply(const dicegpu_subset_file* f, dicegpu_ctx* ctx);
+
+/* create_regular_grid_of_correlation_points (DICe_Decomp.cpp:868-1050):
+ * subset centres every step_size pixels from subset_size - 1 in x and y,
+ * kept when the centre lies in a region of interest (the REGION_OF_INTEREST
+ * blocks of f in id order, or the whole image when f is NULL), no corner of
+ * the subset lies in the region's excluded shapes, and the subset is at
+ * least subset_size - 1 from the image's edges; in the reference's order:
+ * each region's seed point (its SEED LOCATION rounded onto the grid, else
+ * the first grid point), then a column-wise snake right of it, then one
+ * left.  For each point: xy (2 doubles), neighbor_ids (the previous point
+ * on its snake, the seed for a snake's first point when a seed was given,
+ * else -1) and seed_roi (the region whose seed it is, else -1); any of them
+ * may be NULL.  *n receives the number of points; DICEGPU_ERR_ARG when it
+ * exceeds cap (nothing beyond cap is written) or a given seed is not a valid
+ * point.  The reference's optional gradient threshold (sssig) is not
+ * applied. */
+int dicegpu_regular_grid(const dicegpu_subset_file* f, int width, int height, int step_size, int subset_size,
+                         double* xy, int32_t* neighbor_ids, int32_t* seed_roi, int cap, int* n);
+
+/* Schema::initialize with a region-of-interest file (or none: f NULL, the
+ * whole image) and a step size: the grid's points become square subsets of
+ * params.subset_size, the regions' seeds their field rows' initial values. */
+int dicegpu_subset_file_apply_grid(const dicegpu_subset_file* f, dicegpu_ctx* ctx, int width, int height,
+                                   int step_size);
 
 #ifdef __cplusplus
 }

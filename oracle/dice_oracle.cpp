@@ -1668,6 +1668,127 @@ extern "C" int oracle_execute_frame_shapes(const dicegpu_params* params, int w, 
   return 0;
 }
 
+// VSG_Strain_Post_Processor::execute (DICe_PostProcessor.cpp:931-1130) with
+// its neighbourhoods (Post_Processor::initialize_neighborhood, :140-236,
+// radius search): for every point the points within window/2 (float
+// squared distance < r^2 + 1e-5, the kd-tree's test), sorted by distance;
+// the neighbours with sigma >= 0 fit u and v by a plane [1, dx, dy] in
+// double; fewer than 3, an invalid point, or a condition estimate below
+// 1e-12 give zeros and MATCH = -1.  The condition number is computed
+// exactly here (||A||_1 ||A^-1||_1) where the reference estimates it with
+// GECON; the test differs only for nearly collinear neighbourhoods.
+// Field values are the reference's floats.  out: n x 7 (strain xx, yy, xy,
+// du/dx, du/dy, dv/dx, dv/dy), failed: n flags.
+namespace {
+// LU with partial pivoting and the inverse of a 3 x 3 (GETRF / GETRI);
+// false when a pivot is exactly 0
+static bool inverse3(const double A_in[3][3], double inv[3][3]) {
+  double A[3][3];
+  int piv[3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) A[i][j] = A_in[i][j];
+  for (int k = 0; k < 3; ++k) {
+    int p = k;
+    for (int i = k + 1; i < 3; ++i)
+      if (std::fabs(A[i][k]) > std::fabs(A[p][k])) p = i;
+    piv[k] = p;
+    if (A[p][k] == 0.0) return false;
+    if (p != k)
+      for (int j = 0; j < 3; ++j) std::swap(A[k][j], A[p][j]);
+    for (int i = k + 1; i < 3; ++i) {
+      A[i][k] /= A[k][k];
+      for (int j = k + 1; j < 3; ++j) A[i][j] -= A[i][k] * A[k][j];
+    }
+  }
+  // solve A X = I column by column (the row interchanges applied to I)
+  for (int c = 0; c < 3; ++c) {
+    double b[3] = {0.0, 0.0, 0.0};
+    b[c] = 1.0;
+    for (int k = 0; k < 3; ++k) std::swap(b[k], b[piv[k]]);
+    for (int i = 1; i < 3; ++i)
+      for (int j = 0; j < i; ++j) b[i] -= A[i][j] * b[j];
+    for (int i = 2; i >= 0; --i) {
+      for (int j = i + 1; j < 3; ++j) b[i] -= A[i][j] * b[j];
+      b[i] /= A[i][i];
+    }
+    for (int i = 0; i < 3; ++i) inv[i][c] = b[i];
+  }
+  return true;
+}
+static double norm1(const double M[3][3]) {
+  double a = 0.0;
+  for (int j = 0; j < 3; ++j) {
+    double c = 0.0;
+    for (int i = 0; i < 3; ++i) c += std::fabs(M[i][j]);
+    a = std::max(a, c);
+  }
+  return a;
+}
+}  // namespace
+
+extern "C" int oracle_vsg_strain(int n, const double* fields, int window, double* out, int32_t* failed) {
+  if (n < 1 || !fields || !out || !failed || window <= 0) return DICEGPU_ERR_ARG;
+  const float rad = (float)((float)window / 2.0);
+  const float r2 = rad * rad + 1.0e-5f;
+  std::vector<float> px(n), py(n), u(n), v(n), sg(n);
+  for (int i = 0; i < n; ++i) {
+    const double* f = fields + (long)i * DICEGPU_FIELD_STRIDE;
+    px[i] = (float)f[DICEGPU_F_COORD_X];
+    py[i] = (float)f[DICEGPU_F_COORD_Y];
+    u[i] = (float)f[DICEGPU_F_DISP_X];
+    v[i] = (float)f[DICEGPU_F_DISP_Y];
+    sg[i] = (float)f[DICEGPU_F_SIGMA];
+  }
+  std::vector<std::pair<float, int>> nb;
+  for (int i = 0; i < n; ++i) {
+    nb.clear();
+    for (int j = 0; j < n; ++j) {
+      const float dx = px[i] - px[j], dy = py[i] - py[j];
+      const float d2 = dx * dx + dy * dy;
+      if (d2 < r2) nb.push_back(std::make_pair(d2, j));
+    }
+    std::stable_sort(nb.begin(), nb.end(),
+                     [](const std::pair<float, int>& a, const std::pair<float, int>& b) { return a.first < b.first; });
+    double* o = out + (long)i * 7;
+    for (int k = 0; k < 7; ++k) o[k] = 0.0;
+    failed[i] = 1;
+    int valid = 0;
+    for (const auto& q : nb) valid += sg[q.second] >= 0.0f;
+    if (valid < 3 || nb.empty() || sg[nb[0].second] < 0.0f) continue;
+    double XtX[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Xu[3] = {0, 0, 0}, Xv[3] = {0, 0, 0};
+    for (const auto& q : nb) {
+      const int j = q.second;
+      if (!(sg[j] >= 0.0f)) continue;
+      const double row[3] = {1.0, (double)(px[j] - px[i]), (double)(py[j] - py[i])};
+      for (int a = 0; a < 3; ++a) {
+        for (int b = 0; b < 3; ++b) XtX[a][b] += row[a] * row[b];
+        Xu[a] += row[a] * (double)u[j];
+        Xv[a] += row[a] * (double)v[j];
+      }
+    }
+    double inv[3][3];
+    if (!inverse3(XtX, inv)) continue;
+    const double rcond = 1.0 / (norm1(XtX) * norm1(inv));
+    if (rcond < 1.0e-12) continue;
+    double cx[3] = {0, 0, 0}, cy[3] = {0, 0, 0};
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        cx[a] += inv[a][b] * Xu[b];
+        cy[a] += inv[a][b] * Xv[b];
+      }
+    const double dudx = cx[1], dudy = cx[2], dvdx = cy[1], dvdy = cy[2];
+    o[0] = (float)(0.5 * (2.0 * dudx + dudx * dudx + dvdx * dvdx));
+    o[1] = (float)(0.5 * (2.0 * dvdy + dudy * dudy + dvdy * dvdy));
+    o[2] = (float)(0.5 * (dudy + dvdx + dudx * dudy + dvdx * dvdy));
+    o[3] = (float)dudx;
+    o[4] = (float)dudy;
+    o[5] = (float)dvdx;
+    o[6] = (float)dvdy;
+    failed[i] = 0;
+  }
+  return 0;
+}
+
 // One Objective entry point per subset on a fresh square subset at the
 // parameters of its field row: op 0 computeUpdateFast (:430-657), op 1
 // computeUpdateRobust (:369-388), op 2 sigma (:150-184) after the subset's

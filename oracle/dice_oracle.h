@@ -86,6 +86,10 @@ int oracle_execute_frame_shapes(const dicegpu_params* params, int w, int h, cons
                                 const int32_t* block_offsets, const int32_t* block_ids,
                                 const uint8_t* force_simplex, int first_frame, int nthreads);
 
+/* VSG_Strain_Post_Processor on n field rows (window > 0: radius window/2):
+ * out n x 7 (strain xx, yy, xy, du/dx, du/dy, dv/dx, dv/dy), failed n flags. */
+int oracle_vsg_strain(int n, const double* fields, int window, double* out, int32_t* failed);
+
 /* Defaults of dice_default_params (same values as dicegpu_default_params). */
 int oracle_default_params(dicegpu_params* p);
 

@@ -65,6 +65,8 @@ def lib():
         L.oracle_rasterize.argtypes = [ci, ci, vp, vp, vp, vp, ci, vp, vp, vp]
         L.oracle_execute_frame_shapes.restype = ci
         L.oracle_execute_frame_shapes.argtypes = [P, ci, ci, vp, vp, ci, vp, ci, vp, vp, vp, vp, vp, vp, ci, ci]
+        L.oracle_vsg_strain.restype = ci
+        L.oracle_vsg_strain.argtypes = [ci, vp, ci, vp, vp]
         _lib = L
     return _lib
 
@@ -157,6 +159,17 @@ def execute_frame_shapes(params, ref, deff, fields, shapes, vx=None, vy=None, bl
     if rc != 0:
         raise RuntimeError("oracle_execute_frame_shapes: %d" % rc)
     return fields
+
+
+def vsg_strain(fields, window):
+    """VSG_Strain_Post_Processor on the field rows: (n x 7 values, failed flags)."""
+    f = np.ascontiguousarray(fields, dtype=np.float64)
+    n = f.shape[0]
+    out = np.zeros((n, 7), np.float64)
+    failed = np.zeros(n, np.int32)
+    rc = lib().oracle_vsg_strain(n, _ptr(f), int(window), _ptr(out), _ptr(failed))
+    assert rc == 0, rc
+    return out, failed
 
 
 def gauss_filter(img, mask_size=7):

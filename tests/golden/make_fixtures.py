@@ -22,6 +22,7 @@ Sources (paths inside the DICe project):
   tests/regression/conformal_subset_def/{subset_defs.txt, gold/DICe_solution_{0..4}.txt}
   tests/regression/simple_obstruction/{subsets.txt, images/Img_{00..36}.tif,
       gold/DICe_solution_0.txt}
+  tests/regression/dic_challenge_12{,_sorted}/{subset_file.dat, gold/DICe_solution_{01,06,11}.txt}
   tests/examples/{mechanism, obstruction}/subsets.txt,
       tests/regression/mechanism_{skip_solves, optical_flow}/subsets.txt
 """
@@ -118,6 +119,15 @@ def main(root):
             out["conformal_subset_def_gold_text_%d" % k] = np.array(fh.read())
     with open(os.path.join(root, "tests", "regression", "simple_obstruction", "gold", "DICe_solution_0.txt")) as fh:
         out["simple_obstruction_gold_text"] = np.array(fh.read())
+    # dic_challenge_12 (region-of-interest grid, step 35, subset 27; VSG strain
+    # over a 360 px window): frames 1, 6 and 11 of the unsorted and the
+    # sorted output, and the region-of-interest subset file
+    for variant in ("dic_challenge_12", "dic_challenge_12_sorted"):
+        for k in (1, 6, 11):
+            with open(os.path.join(root, "tests", "regression", variant, "gold", "DICe_solution_%02d.txt" % k)) as fh:
+                out["%s_gold_text_%02d" % (variant, k)] = np.array(fh.read())
+    with open(os.path.join(root, "tests", "regression", "dic_challenge_12", "subset_file.dat")) as fh:
+        out["subset_file_dic_challenge_12"] = np.array(fh.read())
     from PIL import Image
     out["simple_obstruction_frames"] = np.stack([
         np.array(Image.open(os.path.join(root, "tests", "regression", "simple_obstruction", "images",
