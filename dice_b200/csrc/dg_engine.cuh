@@ -91,7 +91,7 @@ struct AffineStep {
 // (first maximal pivot, reciprocal scaling, rank-1 updates), then
 // update = -H^-1 q, or -LU q when a pivot is exactly zero (DGETRI returns
 // early and the factors are used as the inverse).
-__device__ __noinline__ AffineStep solve_affine(const double* __restrict__ M, double cshift,
+static __device__ __noinline__ AffineStep solve_affine(const double* __restrict__ M, double cshift,
                                                 unsigned em, float lm_alpha) {
   double H[6][6], q[6], q0[6];
 #pragma unroll
@@ -193,7 +193,7 @@ struct SubsetRef {
   bool masked;      // has an obstruction or blocked bitmap
 };
 
-template <int SHAPE, int INTERP, bool DEFGRAD>
+template <int SHAPE, int INTERP, bool DEFGRAD, bool MASK>
 struct Engine {
   using L = Layout<SHAPE>;
   const FrameArgs& A;
@@ -236,7 +236,7 @@ struct Engine {
     in.K = sb.K;
     MapConst k;
     make_mapconst<SHAPE>(slots, !DEFGRAD, (float)sb.cx, (float)sb.cy, k);
-    if (sb.masked) {
+    if (MASK && sb.masked) {
       in.mdesc = A.geo.mask_desc + (size_t)sb.idx * DG_MASK_DESC;
       in.mbits = A.geo.mask_bits;
       in.bbits = A.geo.blocked_bits;
@@ -943,7 +943,7 @@ struct Engine {
       sb.K = __ldg(A.ref.I + (size_t)ky * A.ref.w + kx);
     }
     sb.masked = false;
-    if (A.geo.mask_desc) {
+    if (MASK && A.geo.mask_desc) {
       const int32_t* md = A.geo.mask_desc + (size_t)idx * DG_MASK_DESC;
       sb.masked = md[2] > 0 || md[7] > 0;
     }

@@ -15,7 +15,7 @@ namespace dg {
 // Section timers of a profiling build (-DDG_PROFILE): warp cycles per section
 // summed over all warps.  Compiled out otherwise.
 #ifdef DG_PROFILE
-__device__ unsigned long long g_prof[8];
+static __device__ unsigned long long g_prof[8];   // per translation unit
 #define DG_PT(var) const long long var = clock64()
 #define DG_PACC(i, t0)                                                                    \
   do {                                                                                    \

@@ -4,7 +4,8 @@
 //   gradient_kernel   Image_::compute_gradients (finite difference, optional
 //                     5x5 smoothing), DICe_Image.cpp:1015-1093
 //   frame_kernel      persistent work-stealing correlation of every subset:
-//                     one warp per subset, a global atomic queue head
+//                     one warp per subset (dg_frame.cuh; masked
+//                     instantiations in frame_masked.cu)
 //   interp_kernel     Image_::interpolate_*_all at arbitrary points
 // The C ABI (include/dicegpu.h) owns device memory and launches on the
 // caller's stream; it never throws and never falls back to the CPU.
@@ -20,7 +21,7 @@
 #include <mutex>
 #include <vector>
 
-#include "dg_engine.cuh"
+#include "dg_frame.cuh"
 #include "dg_adjoint.cuh"
 #include "dg_raster.cuh"
 #include "dg_vsg.cuh"
@@ -28,12 +29,6 @@
 
 using namespace dg;
 
-// minimum resident 256-thread blocks per SM the frame kernel is compiled for
-// (bounds its registers: 2 -> 128 per thread, 3 -> 80; 128 measured ~3 %
-// faster on the 2048^2 sequence despite the lower occupancy)
-#ifndef DG_MIN_BLOCKS
-#define DG_MIN_BLOCKS 2
-#endif
 // consecutive subsets per work-queue chunk (0: two per warp of a CTA)
 #ifndef DG_QUEUE_CHUNK
 #define DG_QUEUE_CHUNK 0
@@ -210,79 +205,6 @@ __global__ void interp_kernel(int method, int w, int h, const float* __restrict_
   }
   oi[t] = v;
   if (grad) { ogx[t] = a; ogy[t] = b; }
-}
-
-// ---------------------------------------------------------------------------
-// the persistent frame kernel
-// ---------------------------------------------------------------------------
-template <int SHAPE, int INTERP, bool DEFGRAD>
-__global__ void __launch_bounds__(256, DG_MIN_BLOCKS) frame_kernel(const __grid_constant__ FrameArgs a) {
-  Engine<SHAPE, INTERP, DEFGRAD> e(a);
-  const int lane = threadIdx.x & 31;
-  if (a.plain_index >= 0) {
-    if (blockIdx.x == 0 && threadIdx.x < 32) e.run(a.plain_index);
-    return;
-  }
-  // the launch's subsets: all n, or the n_order listed in order
-  const int count = a.order ? a.n_order : a.n;
-  if (a.queue_mode == 0) {
-    // one global queue head
-    for (;;) {
-      int t = 0;
-      if (lane == 0) t = atomicAdd(a.work_counter, 1);
-      t = __shfl_sync(FULL, t, 0);
-      if (t >= count) break;
-      e.run(a.order ? a.order[t] : t);
-    }
-    return;
-  }
-  // Interleaved per-CTA queues: the subsets are cut into chunks of C
-  // consecutive ones and CTA r owns chunks r, r + G, r + 2G, ...  The warps of
-  // a CTA work on neighbouring subsets (shared footprint in L1) and all CTAs
-  // advance through the image together (a narrow band resident in L2).  A CTA
-  // whose chunks are exhausted takes from the following CTAs' sequences.
-  // Every index is taken exactly once (atomicAdd); a warp leaves after finding
-  // all G sequences exhausted, so no warp ever waits on another.
-  const int G = gridDim.x;
-  const int C = a.chunk;
-  int q = blockIdx.x;
-  for (int visited = 0; visited < G;) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(a.work_counter + q, 1);
-    t = __shfl_sync(FULL, t, 0);
-    const long long chunk = (long long)q + (long long)(t / C) * G;
-    const long long lidx = chunk * C + (t % C);
-    const int pos = lidx < count ? (int)lidx : count;
-    if (pos < count) {
-      DG_PT(t_run);
-      e.run(a.order ? a.order[pos] : pos);
-      DG_PACC(0, t_run);
-      continue;
-    }
-    ++visited;
-    q = (q + 1 == G) ? 0 : q + 1;
-  }
-}
-
-typedef void (*FrameKernelFn)(FrameArgs);
-
-template <int SHAPE>
-static FrameKernelFn pick_kernel(int interp, bool defgrad) {
-#ifdef DG_ONLY_BENCH_KERNEL
-  // reduced build (fast compiles while tuning): only the affine / Keys-4 /
-  // deformed-gradient kernel; other configurations report UNSUPPORTED
-  if (SHAPE == DICEGPU_AFFINE_SF && interp == DICEGPU_KEYS_FOURTH && defgrad)
-    return frame_kernel<DICEGPU_AFFINE_SF, DICEGPU_KEYS_FOURTH, true>;
-  return nullptr;
-#endif
-  if (defgrad) {
-    if (interp == DICEGPU_KEYS_FOURTH) return frame_kernel<SHAPE, DICEGPU_KEYS_FOURTH, true>;
-    if (interp == DICEGPU_BICUBIC) return frame_kernel<SHAPE, DICEGPU_BICUBIC, true>;
-    return frame_kernel<SHAPE, DICEGPU_BILINEAR, true>;
-  }
-  if (interp == DICEGPU_KEYS_FOURTH) return frame_kernel<SHAPE, DICEGPU_KEYS_FOURTH, false>;
-  if (interp == DICEGPU_BICUBIC) return frame_kernel<SHAPE, DICEGPU_BICUBIC, false>;
-  return frame_kernel<SHAPE, DICEGPU_BILINEAR, false>;
 }
 
 // ---------------------------------------------------------------------------
@@ -1323,8 +1245,9 @@ static size_t warp_smem_bytes(int shape) {
 
 static FrameKernelFn frame_fn(const dicegpu_ctx* c) {
   const bool dg = c->params.use_def_gradients != 0;
-  return c->dp.shape == DICEGPU_QUADRATIC_SF ? pick_kernel<DICEGPU_QUADRATIC_SF>(c->dp.interp, dg)
-                                             : pick_kernel<DICEGPU_AFFINE_SF>(c->dp.interp, dg);
+  if (c->use_masks) return pick_masked_kernel(c->dp.shape, c->dp.interp, dg);
+  return c->dp.shape == DICEGPU_QUADRATIC_SF ? pick_kernel<DICEGPU_QUADRATIC_SF, false>(c->dp.interp, dg)
+                                             : pick_kernel<DICEGPU_AFFINE_SF, false>(c->dp.interp, dg);
 }
 
 static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
