@@ -70,6 +70,13 @@ def workload_config(n_subsets, n_gpus, sharded=False):
             "l2": "flushed between timed steps (256 MiB write)"}
 
 
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -594,6 +601,103 @@ def run_adjoint(args):
         dist.destroy_process_group()
 
 
+def run_vsg(args):
+    """VSG strain of the 2048^2 sequence's subset field (158,404 subsets at
+    step 5 after correlating frame 1; strain window 41 px): one step is one
+    VSG_Strain_Post_Processor pass over every subset (uniform-grid
+    neighbourhoods, per-subset plane fits).  e2e: the field rows uploaded from
+    host memory, the pass, and the VSG rows read back through the C ABI."""
+    import ctypes
+    import torch
+    from dice_b200 import abi, synthetic as syn
+    from dice_b200.schema import Schema
+    from oracle import oracle as O
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    window = args.vsg_window
+    p = params()
+    ref, frames = syn.config2(device=dev, nframes=2)
+    cx, cy = syn.grid_points(W, H, SUBSET, STEP)
+    n = len(cx)
+    stream = torch.cuda.current_stream()
+    s = Schema(p, stream=stream)
+    s.set_ref_image(ref)
+    s.set_fields(syn.init_fields(cx, cy))
+    s.set_def_image(frames[1])
+    s.execute_correlation()
+    fields = s.fields()
+    fields_pinned = torch.from_numpy(fields).pin_memory()
+    out_pinned = torch.empty((n, abi.VSG_STRIDE), dtype=torch.float64).pin_memory()
+    lib = s.lib
+    l2 = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        abi.check(lib.dicegpu_vsg_strain(s.ctx, window, None, 1), "vsg_strain")
+
+    def step_e2e():
+        abi.check(lib.dicegpu_load_fields(s.ctx, ctypes.c_void_p(fields_pinned.data_ptr()), 0), "load_fields")
+        abi.check(lib.dicegpu_vsg_strain(s.ctx, window, ctypes.c_void_p(out_pinned.data_ptr()), 0), "vsg")
+
+    step()   # builds the neighbour grid
+    torch.cuda.synchronize()
+    launches0 = s.launch_count()
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier(world)
+    clocks.start()
+    ms = _timed(step, args.steps, args.warmup, stream, flush=l2)
+    barrier(world)
+    clocks.stop()
+    launches = s.launch_count() - launches0
+    total_ms = max_over_ranks(sum(ms), world)
+    value = n * args.steps * world / (total_ms / 1000.0)
+    # end to end through the C ABI (the grid is rebuilt after load_fields)
+    step_e2e()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(e2e_steps):
+        step_e2e()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    got = s.vsg_strain(window)
+    # parity against the oracle on the whole field, and the CPU baseline
+    t0 = time.perf_counter()
+    want, failed = O.vsg_strain(fields, window)
+    cpu_s = time.perf_counter() - t0
+    ok = failed == 0
+    rel = float(np.max(np.abs(got[ok, :7] - want[ok]) / np.maximum(np.abs(want[ok]), 1e-9)))
+    flags_equal = bool(np.array_equal(got[:, :7][~ok], np.zeros_like(want[~ok])) and
+                       np.array_equal(s.fields()[:, abi.F_MATCH] == -1.0, (failed == 1) | (fields[:, abi.F_MATCH] == -1.0)))
+    neighbours = float(np.mean(got[:, abi.VSG_NEIGHBORS]))
+    med = statistics.median(ms)
+    # algorithmic bytes: each subset's coordinates, u, v and sigma read once
+    # (5 doubles) and its 8 VSG values written
+    alg_bytes = n * (5 + 8) * 8.0
+    peak = measured_peaks().get("hbm_gbs") or 6650.0
+    achieved = alg_bytes / (med / 1000.0) / 1e9
+    if rank == 0:
+        cfg = {"workload": "VSG strain of 158,404 subsets (2048x2048 sequence, frame 1, step 5), window %d px"
+                           % window, "subsets": n, "window": window, "mean_valid_neighbours": neighbours,
+               "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas x%d" % world}
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "vsg_kernel",
+                "per_unit": "104 B per subset (5 doubles read, 8 written); the %.0f neighbour gathers per subset "
+                            "come from L2" % neighbours}
+        print(json.dumps(_line("VSG strain subsets/sec", value, "subsets/s", world, args, total_ms / args.steps,
+                               cfg, roofline=roof,
+                               e2e={"value": n / e2e_s, "unit": "subsets/s", "h2d_bytes_per_step": fields.nbytes,
+                                    "d2h_bytes_per_step": n * abi.VSG_STRIDE * 8},
+                               cpu_baseline={"value": n / cpu_s, "unit": "subsets/s", "cores": 1, "kind": "port",
+                                             "sample": "all subsets, one core (grid neighbour search)"},
+                               parity_vs_oracle={"max_rel_diff": rel, "failed_and_match_equal": flags_equal,
+                                                 "failed": int(failed.sum())},
+                               gpu_launches=int(launches), clocks=clocks.summary())), flush=True)
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def flush_l2(buf):
     buf.zero_()
 
@@ -612,10 +716,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--warps", type=int, default=0)
     ap.add_argument("--ctas", type=int, default=0)
-    ap.add_argument("--workload", default="sequence", choices=["sequence", "crack", "mixed", "adjoint"],
+    ap.add_argument("--workload", default="sequence", choices=["sequence", "crack", "mixed", "adjoint", "vsg"],
                     help="sequence: the 2048^2 ten-frame sequence (default, the headline); crack: the "
                          "8192^2 crack sequence; mixed: arbitrary-shape subsets; adjoint: objective "
-                         "derivatives and the B-spline fit")
+                         "derivatives and the B-spline fit; vsg: VSG strain of the sequence's field")
+    ap.add_argument("--vsg-window", type=int, default=41)
     ap.add_argument("--crack-size", type=int, default=8192)
     ap.add_argument("--fit-iters", type=int, default=2000)
     ap.add_argument("--profile-timed", action="store_true",
@@ -629,7 +734,7 @@ def main():
         run_reference(args)
         return
     if args.workload != "sequence":
-        {"crack": run_crack, "mixed": run_mixed, "adjoint": run_adjoint}[args.workload](args)
+        {"crack": run_crack, "mixed": run_mixed, "adjoint": run_adjoint, "vsg": run_vsg}[args.workload](args)
         return
     import torch
     from dice_b200 import abi, synthetic as syn

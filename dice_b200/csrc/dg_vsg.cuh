@@ -10,11 +10,12 @@
 // MATCH = -1.  Field values enter as the reference's floats; results are
 // rounded to float as the reference stores them.
 //
-// One warp per subset: the neighbours come from a uniform grid of cell size
-// >= the radius (3 x 3 cells cover the disc), lanes take candidates in turn
-// and accumulate the twelve double sums of X^T X and X^T u, X^T v, a warp
-// reduction combines them, and lane 0 solves the 3 x 3 system by LU with
-// partial pivoting and an explicit inverse (the reference's GETRF / GETRI).
+// The neighbours come from a uniform grid of cell size >= the radius (3 x 3
+// cells cover the disc) whose per-subset floats are packed in cell order
+// (vsg_pack_kernel).  A warp accumulates the twelve double sums of X^T X,
+// X^T u and X^T v for 32 subsets in turn, then each lane solves one
+// subset's 3 x 3 system by LU with partial pivoting and an explicit inverse
+// (the reference's GETRF / GETRI).
 // The condition number is computed exactly where the reference estimates it
 // (GECON); the two differ only for nearly collinear neighbourhoods.
 #pragma once
@@ -25,13 +26,29 @@
 struct VsgArgs {
   double* fields;            // n x DICEGPU_FIELD_STRIDE (MATCH set to -1 where the fit fails)
   int n;
-  const int32_t* cell_off;   // [ncx * ncy + 1] into cell_pts
+  const int32_t* cell_off;   // [ncx * ncy + 1] into cell_pts / packed
   const int32_t* cell_pts;   // subset indices grouped by cell
+  const int32_t* pos_of;     // position of each subset in cell order
+  float4* packed;            // per position: x (NaN when sigma < 0), y, u, v as floats
   int ncx, ncy;
   float x0, y0, cell;        // grid origin and cell size
   float r2;                  // r^2 + 1e-5
   double* out;               // n x DICEGPU_VSG_STRIDE
 };
+
+// The per-subset values the fits read, as the reference's floats, packed in
+// cell order so that a cell's candidates are one coalesced run of 16-byte
+// loads.  An invalid subset (sigma < 0) gets x = NaN, which fails the
+// distance test exactly as the reference's validity test excludes it.
+__global__ void __launch_bounds__(256) vsg_pack_kernel(VsgArgs a) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const double* f = a.fields + (size_t)i * DICEGPU_FIELD_STRIDE;
+    const bool valid = (float)f[DICEGPU_F_SIGMA] >= 0.0f;
+    a.packed[a.pos_of[i]] = make_float4(valid ? (float)f[DICEGPU_F_COORD_X] : __int_as_float(0x7fc00000),
+                                        (float)f[DICEGPU_F_COORD_Y], (float)f[DICEGPU_F_DISP_X],
+                                        (float)f[DICEGPU_F_DISP_Y]);
+  }
+}
 
 __device__ __forceinline__ double vsg_warp_sum(double v) {
 #pragma unroll
@@ -79,31 +96,41 @@ __device__ inline double vsg_norm1(const double M[3][3]) {
   return a;
 }
 
+// One warp per batch of 32 subsets.  For each subset of the batch the lanes
+// take its candidates in turn (the three cells of a grid row are one
+// contiguous run of the packed array) and the twelve double sums are reduced
+// across the warp; lane k keeps subset k's sums, and the 32 solves then run
+// in parallel, one per lane.
 __global__ void __launch_bounds__(256) vsg_kernel(VsgArgs a) {
   const int lane = threadIdx.x & 31;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += warps) {
-    const double* fi = a.fields + (size_t)i * DICEGPU_FIELD_STRIDE;
-    const float xi = (float)fi[DICEGPU_F_COORD_X], yi = (float)fi[DICEGPU_F_COORD_Y];
-    const bool self_ok = (float)fi[DICEGPU_F_SIGMA] >= 0.0f;
-    const int gx = (int)floorf((xi - a.x0) / a.cell), gy = (int)floorf((yi - a.y0) / a.cell);
-    // sums: n, dx, dy, dx dx, dx dy, dy dy, u, dx u, dy u, v, dx v, dy v
-    double s[12];
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < a.n; base += nwarps * 32) {
+    const int cnt = min(32, a.n - base);
+    double m[12];
 #pragma unroll
-    for (int k = 0; k < 12; ++k) s[k] = 0.0;
-    int valid = 0;
-    for (int cy = max(gy - 1, 0); cy <= min(gy + 1, a.ncy - 1); ++cy)
-      for (int cx = max(gx - 1, 0); cx <= min(gx + 1, a.ncx - 1); ++cx) {
-        const int c = cy * a.ncx + cx;
-        for (int t = a.cell_off[c] + lane; t < a.cell_off[c + 1]; t += 32) {
-          const int j = a.cell_pts[t];
-          const double* fj = a.fields + (size_t)j * DICEGPU_FIELD_STRIDE;
-          const float xj = (float)fj[DICEGPU_F_COORD_X], yj = (float)fj[DICEGPU_F_COORD_Y];
-          const float ex = __fsub_rn(xi, xj), ey = __fsub_rn(yi, yj);
+    for (int k = 0; k < 12; ++k) m[k] = 0.0;
+    int mvalid = 0;
+    bool mself = false;
+    for (int k = 0; k < cnt; ++k) {
+      const int i = base + k;
+      const double* fi = a.fields + (size_t)i * DICEGPU_FIELD_STRIDE;
+      const float xi = (float)fi[DICEGPU_F_COORD_X], yi = (float)fi[DICEGPU_F_COORD_Y];
+      const int gx = (int)floorf((xi - a.x0) / a.cell), gy = (int)floorf((yi - a.y0) / a.cell);
+      // sums: n, dx, dy, dx dx, dx dy, dy dy, u, dx u, dy u, v, dx v, dy v
+      double s[12];
+#pragma unroll
+      for (int q = 0; q < 12; ++q) s[q] = 0.0;
+      int valid = 0;
+      const int cx0 = max(gx - 1, 0), cx1 = min(gx + 1, a.ncx - 1);
+      for (int cy = max(gy - 1, 0); cy <= min(gy + 1, a.ncy - 1); ++cy) {
+        const int t1 = a.cell_off[cy * a.ncx + cx1 + 1];
+        for (int t = a.cell_off[cy * a.ncx + cx0] + lane; t < t1; t += 32) {
+          const float4 pj = __ldg(a.packed + t);
+          const float ex = __fsub_rn(xi, pj.x), ey = __fsub_rn(yi, pj.y);
           const float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
-          if (!(d2 < a.r2) || !((float)fj[DICEGPU_F_SIGMA] >= 0.0f)) continue;
-          const double dx = (double)__fsub_rn(xj, xi), dy = (double)__fsub_rn(yj, yi);
-          const double u = (double)(float)fj[DICEGPU_F_DISP_X], v = (double)(float)fj[DICEGPU_F_DISP_Y];
+          if (!(d2 < a.r2)) continue;   // also an invalid neighbour (x = NaN)
+          const double dx = (double)__fsub_rn(pj.x, xi), dy = (double)__fsub_rn(pj.y, yi);
+          const double u = (double)pj.z, v = (double)pj.w;
           ++valid;
           s[0] += 1.0; s[1] += dx; s[2] += dy;
           s[3] = fma(dx, dx, s[3]); s[4] = fma(dx, dy, s[4]); s[5] = fma(dy, dy, s[5]);
@@ -112,19 +139,27 @@ __global__ void __launch_bounds__(256) vsg_kernel(VsgArgs a) {
         }
       }
 #pragma unroll
-    for (int k = 0; k < 12; ++k) s[k] = vsg_warp_sum(s[k]);
-    for (int o = 16; o > 0; o >>= 1) valid += __shfl_xor_sync(0xffffffffu, valid, o);
-    if (lane != 0) continue;
+      for (int q = 0; q < 12; ++q) s[q] = vsg_warp_sum(s[q]);
+      for (int o = 16; o > 0; o >>= 1) valid += __shfl_xor_sync(0xffffffffu, valid, o);
+      if (lane == k) {
+#pragma unroll
+        for (int q = 0; q < 12; ++q) m[q] = s[q];
+        mvalid = valid;
+        mself = (float)fi[DICEGPU_F_SIGMA] >= 0.0f;
+      }
+    }
+    if (lane >= cnt) continue;
+    const int i = base + lane;
     double* o = a.out + (size_t)i * DICEGPU_VSG_STRIDE;
     double r[7] = {0, 0, 0, 0, 0, 0, 0};
-    bool ok = self_ok && valid >= 3;
+    bool ok = mself && mvalid >= 3;
     if (ok) {
-      const double XtX[3][3] = {{s[0], s[1], s[2]}, {s[1], s[3], s[4]}, {s[2], s[4], s[5]}};
+      const double XtX[3][3] = {{m[0], m[1], m[2]}, {m[1], m[3], m[4]}, {m[2], m[4], m[5]}};
       double inv[3][3];
       ok = vsg_inverse3(XtX, inv);
       if (ok) ok = !(1.0 / (vsg_norm1(XtX) * vsg_norm1(inv)) < 1.0e-12);
       if (ok) {
-        const double Xu[3] = {s[6], s[7], s[8]}, Xv[3] = {s[9], s[10], s[11]};
+        const double Xu[3] = {m[6], m[7], m[8]}, Xv[3] = {m[9], m[10], m[11]};
         double cu[3], cv[3];
         for (int p = 0; p < 3; ++p) {
           cu[p] = inv[p][0] * Xu[0] + inv[p][1] * Xu[1] + inv[p][2] * Xu[2];
@@ -138,7 +173,7 @@ __global__ void __launch_bounds__(256) vsg_kernel(VsgArgs a) {
       }
     }
     for (int k = 0; k < 7; ++k) o[k] = r[k];
-    o[DICEGPU_VSG_NEIGHBORS] = valid;
+    o[DICEGPU_VSG_NEIGHBORS] = mvalid;
     if (!ok) a.fields[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_MATCH] = -1.0;
   }
 }

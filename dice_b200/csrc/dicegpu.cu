@@ -301,8 +301,10 @@ struct dicegpu_ctx {
   int vsg_window = 0;
   int vsg_ncx = 0, vsg_ncy = 0;
   float vsg_x0 = 0.0f, vsg_y0 = 0.0f, vsg_cell = 1.0f, vsg_r2 = 0.0f;
-  DevBuf<int32_t> d_vsg_cell_off, d_vsg_cell_pts;
+  DevBuf<int32_t> d_vsg_cell_off, d_vsg_cell_pts, d_vsg_pos;
+  DevBuf<float4> d_vsg_packed;
   DevBuf<double> d_vsg;
+  std::vector<double> h_vsg_coords;   // the coordinates the grid was built for
 };
 
 // A failed runtime call returns DICEGPU_ERR_CUDA and clears the runtime's
@@ -470,6 +472,7 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   c->d_bwave.release(); c->d_dv_off.release(); c->d_dvx.release(); c->d_dvy.release();
   c->d_snapshot.release();
   c->d_vsg_cell_off.release(); c->d_vsg_cell_pts.release(); c->d_vsg.release();
+  c->d_vsg_pos.release(); c->d_vsg_packed.release();
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -1135,14 +1138,26 @@ static int build_vsg_grid(dicegpu_ctx* c, int window) {
     ++off[cell_of[i] + 1];
   }
   for (size_t k = 0; k + 1 < off.size(); ++k) off[k + 1] += off[k];
+  std::vector<int32_t> pos(n);
   {
     std::vector<int32_t> fill(off.begin(), off.end() - 1);
-    for (int i = 0; i < n; ++i) pts[fill[cell_of[i]]++] = i;
+    for (int i = 0; i < n; ++i) {
+      pos[i] = fill[cell_of[i]]++;
+      pts[pos[i]] = i;
+    }
   }
   int rc;
-  if ((rc = c->d_vsg_cell_off.ensure(off.size())) || (rc = c->d_vsg_cell_pts.ensure(n))) return rc;
+  if ((rc = c->d_vsg_cell_off.ensure(off.size())) || (rc = c->d_vsg_cell_pts.ensure(n)) ||
+      (rc = c->d_vsg_pos.ensure(n)) || (rc = c->d_vsg_packed.ensure(n)))
+    return rc;
   CK(cudaMemcpy(c->d_vsg_cell_off.p, off.data(), off.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_vsg_cell_pts.p, pts.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_vsg_pos.p, pos.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  c->h_vsg_coords.resize(2 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    c->h_vsg_coords[2 * i] = rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_X];
+    c->h_vsg_coords[2 * i + 1] = rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_Y];
+  }
   c->vsg_ncx = ncx;
   c->vsg_ncy = ncy;
   c->vsg_x0 = x0;
@@ -1159,12 +1174,15 @@ extern "C" int dicegpu_vsg_strain(dicegpu_ctx* c, int window_size, double* out, 
   int rc;
   if (c->vsg_window != window_size && (rc = build_vsg_grid(c, window_size))) return rc;
   if ((rc = c->d_vsg.ensure((size_t)c->n * DICEGPU_VSG_STRIDE))) return rc;
-  VsgArgs va{c->d_fields, c->n, c->d_vsg_cell_off.p, c->d_vsg_cell_pts.p, c->vsg_ncx, c->vsg_ncy,
-             c->vsg_x0, c->vsg_y0, c->vsg_cell, c->vsg_r2, c->d_vsg.p};
-  const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)c->n * 32 + 255) / 256, (int64_t)c->num_sms * 16);
+  VsgArgs va{c->d_fields, c->n, c->d_vsg_cell_off.p, c->d_vsg_cell_pts.p, c->d_vsg_pos.p, c->d_vsg_packed.p,
+             c->vsg_ncx, c->vsg_ncy, c->vsg_x0, c->vsg_y0, c->vsg_cell, c->vsg_r2, c->d_vsg.p};
+  const unsigned pblocks = (unsigned)std::min<int64_t>(((int64_t)c->n + 255) / 256, (int64_t)c->num_sms * 8);
+  vsg_pack_kernel<<<pblocks, 256, 0, c->stream>>>(va);
+  // one warp per 32 subsets
+  const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)c->n + 255) / 256, (int64_t)c->num_sms * 16);
   vsg_kernel<<<blocks, 256, 0, c->stream>>>(va);
   CK(cudaGetLastError());
-  c->launches += 1;
+  c->launches += 2;
   if (out)
     CK(cudaMemcpyAsync(out, c->d_vsg.p, (size_t)c->n * DICEGPU_VSG_STRIDE * sizeof(double),
                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
@@ -1221,7 +1239,12 @@ extern "C" int dicegpu_load_fields(dicegpu_ctx* c, const double* src, int on_dev
   CK(cudaMemcpyAsync(c->d_fields, src, (size_t)c->n * DICEGPU_FIELD_STRIDE * sizeof(double),
                      on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
   c->frame_index = 0;
-  c->vsg_window = 0;
+  // the VSG neighbour grid stays valid when host rows keep its coordinates
+  bool same = !on_device && c->vsg_window != 0 && c->h_vsg_coords.size() == 2 * (size_t)c->n;
+  for (int i = 0; same && i < c->n; ++i)
+    same = src[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_X] == c->h_vsg_coords[2 * i] &&
+           src[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_Y] == c->h_vsg_coords[2 * i + 1];
+  if (!same) c->vsg_window = 0;
   return DICEGPU_OK;
 }
 

@@ -33,6 +33,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <thread>
 #include <set>
@@ -1739,16 +1740,36 @@ extern "C" int oracle_vsg_strain(int n, const double* fields, int window, double
     v[i] = (float)f[DICEGPU_F_DISP_Y];
     sg[i] = (float)f[DICEGPU_F_SIGMA];
   }
+  // candidates from a uniform grid of cell size >= the radius + 1 (the
+  // kd-tree's role: which points are tested, not how)
+  const float cell = std::ceil(std::sqrt(r2)) + 1.0f;
+  float x0 = px[0], y0 = py[0], x1 = px[0], y1 = py[0];
+  for (int i = 1; i < n; ++i) {
+    x0 = std::min(x0, px[i]); x1 = std::max(x1, px[i]);
+    y0 = std::min(y0, py[i]); y1 = std::max(y1, py[i]);
+  }
+  const long ncx = (long)std::floor((x1 - x0) / cell) + 1, ncy = (long)std::floor((y1 - y0) / cell) + 1;
+  std::map<long, std::vector<int>> cells;
+  auto cell_of = [&](int i) {
+    return (long)std::floor((py[i] - y0) / cell) * ncx + (long)std::floor((px[i] - x0) / cell);
+  };
+  for (int i = 0; i < n; ++i) cells[cell_of(i)].push_back(i);
   std::vector<std::pair<float, int>> nb;
   for (int i = 0; i < n; ++i) {
     nb.clear();
-    for (int j = 0; j < n; ++j) {
-      const float dx = px[i] - px[j], dy = py[i] - py[j];
-      const float d2 = dx * dx + dy * dy;
-      if (d2 < r2) nb.push_back(std::make_pair(d2, j));
-    }
-    std::stable_sort(nb.begin(), nb.end(),
-                     [](const std::pair<float, int>& a, const std::pair<float, int>& b) { return a.first < b.first; });
+    const long gx = (long)std::floor((px[i] - x0) / cell), gy = (long)std::floor((py[i] - y0) / cell);
+    for (long cy = std::max(gy - 1, 0L); cy <= std::min(gy + 1, ncy - 1); ++cy)
+      for (long cx = std::max(gx - 1, 0L); cx <= std::min(gx + 1, ncx - 1); ++cx) {
+        const auto it = cells.find(cy * ncx + cx);
+        if (it == cells.end()) continue;
+        for (int j : it->second) {
+          const float dx = px[i] - px[j], dy = py[i] - py[j];
+          const float d2 = dx * dx + dy * dy;
+          if (d2 < r2) nb.push_back(std::make_pair(d2, j));
+        }
+      }
+    // distance order, ties by index
+    std::sort(nb.begin(), nb.end());
     double* o = out + (long)i * 7;
     for (int k = 0; k < 7; ++k) o[k] = 0.0;
     failed[i] = 1;
