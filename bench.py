@@ -601,6 +601,164 @@ def run_adjoint(args):
         dist.destroy_process_group()
 
 
+def conformal_case(nside=50, step=40, seed=9, rmin=14, rmax=20):
+    """nside x nside conformal subsets (convex polygons or rectangles,
+    radius rmin-rmax px) on a step-px grid of the 2048^2 sequence's first
+    frame pair, 30 % with an obstructed rectangle near the centre, each
+    blocked by its right neighbour and every tenth also by its left."""
+    from dice_b200 import abi
+    rng = np.random.default_rng(seed)
+    shapes, vx, vy, cx, cy, blockers = [], [], [], [], [], []
+    x0 = (W - (nside - 1) * step) // 2
+    y0 = (H - (nside - 1) * step) // 2
+    for j in range(nside):
+        for i in range(nside):
+            k = len(cx)
+            x, y = x0 + i * step, y0 + j * step
+            cx.append(float(x))
+            cy.append(float(y))
+            if rng.random() < 0.5:
+                shapes.append(abi.rectangle(k, x, y, int(rng.integers(2 * rmin + 1, 2 * rmax + 1)),
+                                            int(rng.integers(2 * rmin + 1, 2 * rmax + 1))))
+            else:
+                m = int(rng.integers(5, 8))
+                ang = np.sort(rng.uniform(0, 2 * np.pi, m))
+                rad = rng.uniform(rmin, rmax, m)
+                shapes.append(abi.polygon(k, len(vx), m))
+                vx += list(np.round(x + rad * np.cos(ang)).astype(int))
+                vy += list(np.round(y + rad * np.sin(ang)).astype(int))
+            if rng.random() < 0.3:
+                shapes.append(abi.rectangle(k, x + int(rng.integers(-6, 7)), y + int(rng.integers(-6, 7)),
+                                            int(rng.integers(5, 10)), int(rng.integers(5, 10)),
+                                            role=abi.ROLE_OBSTRUCTED))
+            b = [k + 1] if i + 1 < nside else []
+            if i > 0 and k % 10 == 0:
+                b.append(k - 1)
+            blockers.append(b)
+    return (np.asarray(cx), np.asarray(cy), shapes, np.asarray(vx, np.int32), np.asarray(vy, np.int32), blockers)
+
+
+def run_conformal(args):
+    """Conformal subsets built on the device from shapes, with obstructed
+    regions and blocking subsets, under the tracking routine (ordered waves,
+    blocked bitmaps rebuilt per wave): one step is one frame over all
+    subsets.  Also times the rasterization and the same subsets without
+    obstructions or blocking."""
+    import torch
+    from dice_b200 import abi, synthetic as syn
+    from dice_b200.schema import Schema
+    from oracle import oracle as O
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ref, frames = syn.config2(device=dev, count=1)
+    cx, cy, shapes, vx, vy, blockers = conformal_case()
+    n = len(cx)
+    # the tracking defaults' degrees of freedom (translation, rotation); Gauss-Newton kept for every subset
+    p = abi.default_params(subset_size=0, enable_rotation=1, correlation_routine=abi.TRACKING_ROUTINE,
+                           override_force_simplex=1, fast_solver_tolerance=1e-3)
+    f0 = syn.init_fields(cx, cy)
+    stream = torch.cuda.current_stream()
+    s = Schema(p, stream=stream)
+    s.set_ref_image(ref)
+    s.set_fields(f0)
+    s.set_def_image(frames[0])
+    # rasterization: every subset's pixel list from its shapes
+    raster_ms = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.set_subset_shapes(shapes, vx, vy)
+        torch.cuda.synchronize()
+        raster_ms.append((time.perf_counter() - t0) * 1000.0)
+    offs_l, px_l, py_l = s.subset_pixels()
+    s.set_blocking(blockers)
+    f0_dev = torch.from_numpy(f0).to(dev)
+
+    def step():
+        s.load_fields(f0_dev)
+        s.execute_correlation()
+
+    l2 = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    launches0 = s.launch_count()
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier(world)
+    clocks.start()
+    ms = _timed(step, args.steps, args.warmup, stream, flush=l2)
+    barrier(world)
+    clocks.stop()
+    launches = s.launch_count() - launches0
+    total_ms = max_over_ranks(sum(ms), world)
+    value = n * args.steps * world / (total_ms / 1000.0)
+    g = s.fields()
+    # the same pixel lists without obstruction or blocking (generic, unmasked kernel)
+    p_plain = p.copy()
+    p_plain.correlation_routine = abi.GENERIC_ROUTINE
+    s2 = Schema(p_plain, stream=stream)
+    s2.set_ref_image(ref)
+    s2.set_fields(f0)
+    s2.set_subset_pixels(offs_l, px_l, py_l)
+    s2.set_def_image(frames[0])
+
+    def step_plain():
+        s2.load_fields(f0_dev)
+        s2.execute_correlation()
+    plain_ms = statistics.median(_timed(step_plain, args.steps, args.warmup, stream, flush=l2))
+    par, cpu = None, None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        fo = f0.copy()
+        offs = np.zeros(n + 1, np.int32)
+        ids = []
+        for i, b in enumerate(blockers):
+            ids += b
+            offs[i + 1] = offs[i] + len(b)
+        t0 = time.perf_counter()
+        O.execute_frame_shapes(p, ref.cpu().numpy(), frames[0].cpu().numpy(), fo, shapes, vx, vy, offs,
+                               np.asarray(ids, np.int32), first_frame=True)
+        dt = time.perf_counter() - t0
+        cpu = {"value": n / dt, "unit": "subsets/s", "cores": 1, "kind": "port",
+               "sample": "the whole frame (%d subsets; tracking order is sequential), %.1f s" % (n, dt)}
+        # where both sides take the Gauss-Newton path (the simplex stops on flat valleys by rounding)
+        both = (g[:, abi.F_STATUS] < 2) & (fo[:, abi.F_STATUS] < 2) & \
+               (g[:, abi.F_ITERATIONS] <= p.max_solver_iterations_fast) & \
+               (fo[:, abi.F_ITERATIONS] <= p.max_solver_iterations_fast)
+        par = {"status_equal_frac": float(np.mean(g[:, abi.F_STATUS] == fo[:, abi.F_STATUS])),
+               "active_pixels_equal_frac": float(np.mean(g[:, abi.F_ACTIVE_PIXELS] == fo[:, abi.F_ACTIVE_PIXELS])),
+               "active_pixels_equal_frac_gauss_newton": float(np.mean(g[both, abi.F_ACTIVE_PIXELS] ==
+                                                                      fo[both, abi.F_ACTIVE_PIXELS])),
+               "compared": int(both.sum()),
+               "max_abs_du_px": float(np.max(np.abs(g[both, abi.F_DISP_X] - fo[both, abi.F_DISP_X]), initial=0.0)),
+               "max_abs_dv_px": float(np.max(np.abs(g[both, abi.F_DISP_Y] - fo[both, abi.F_DISP_Y]), initial=0.0))}
+        # at tolerance 1e-3 a solve stopping one iteration apart differs by up to the tolerance
+        same = both & (g[:, abi.F_ITERATIONS] == fo[:, abi.F_ITERATIONS])
+        par["iterations_equal_frac"] = float(np.mean(same[both]))
+        par["max_abs_du_px_same_iterations"] = float(np.max(np.abs(g[same, abi.F_DISP_X] - fo[same, abi.F_DISP_X]),
+                                                            initial=0.0))
+    if rank == 0:
+        npix = np.diff(offs_l)
+        cfg = {"workload": "%d conformal subsets (polygons / rectangles, r 14-20 px, step 40) on the 2048x2048 "
+                           "sequence's first pair, 30 %% obstructed, blocked by right neighbours (every 10th also "
+                           "left), tracking routine, translation + rotation" % n,
+               "subsets": n, "mean_pixels": float(npix.mean()),
+               "masked_subsets": int(sum(1 for sh in shapes if sh.role == abi.ROLE_OBSTRUCTED)),
+               "blocking_lists": int(sum(1 for b in blockers if b)),
+               "tolerance": 1e-3, "l2": "flushed between timed steps (256 MiB write)",
+               "parallelism": "replicas x%d" % world}
+        print(json.dumps(_line("conformal subset solves/sec (device rasterized, obstructions, blocking, tracking)",
+                               value, "subsets/s", world, args, total_ms / args.steps, cfg,
+                               rasterize_ms={"median": statistics.median(raster_ms), "note": "set_subset_shapes: "
+                                             "host validation, count kernel, offsets, fill kernel, obstruction "
+                                             "bitmaps"},
+                               same_lists_without_masks_ms=plain_ms,
+                               active_pixels_frac=float(np.sum(g[:, abi.F_ACTIVE_PIXELS].clip(0)) / npix.sum()),
+                               cpu_baseline=cpu, parity_vs_oracle=par, gpu_launches=int(launches),
+                               clocks=clocks.summary())), flush=True)
+    s.close()
+    s2.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def run_vsg(args):
     """VSG strain of the 2048^2 sequence's subset field (158,404 subsets at
     step 5 after correlating frame 1; strain window 41 px): one step is one
@@ -716,10 +874,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--warps", type=int, default=0)
     ap.add_argument("--ctas", type=int, default=0)
-    ap.add_argument("--workload", default="sequence", choices=["sequence", "crack", "mixed", "adjoint", "vsg"],
+    ap.add_argument("--workload", default="sequence",
+                    choices=["sequence", "crack", "mixed", "adjoint", "vsg", "conformal"],
                     help="sequence: the 2048^2 ten-frame sequence (default, the headline); crack: the "
                          "8192^2 crack sequence; mixed: arbitrary-shape subsets; adjoint: objective "
-                         "derivatives and the B-spline fit; vsg: VSG strain of the sequence's field")
+                         "derivatives and the B-spline fit; vsg: VSG strain of the sequence's field; "
+                         "conformal: device-rasterized subsets with obstructions and blocking")
     ap.add_argument("--vsg-window", type=int, default=41)
     ap.add_argument("--crack-size", type=int, default=8192)
     ap.add_argument("--fit-iters", type=int, default=2000)
@@ -734,7 +894,8 @@ def main():
         run_reference(args)
         return
     if args.workload != "sequence":
-        {"crack": run_crack, "mixed": run_mixed, "adjoint": run_adjoint, "vsg": run_vsg}[args.workload](args)
+        {"crack": run_crack, "mixed": run_mixed, "adjoint": run_adjoint, "vsg": run_vsg,
+         "conformal": run_conformal}[args.workload](args)
         return
     import torch
     from dice_b200 import abi, synthetic as syn

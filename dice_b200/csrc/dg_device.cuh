@@ -60,7 +60,7 @@ struct DevImage {
 };
 
 // ints per subset mask descriptor: obstruction box (x0, y0, w, h, word
-// offset), blocked box (x0, y0, w, h, word offset)
+// offset), blocked polygons (count, table offset), three spare
 #define DG_MASK_DESC 10
 
 // Subset geometry: square (`half` >= 0, centred on the COORD fields) or an
@@ -72,10 +72,12 @@ struct DevGeometry {
   const int32_t* __restrict__ py;
   const uint8_t* __restrict__ force_simplex;
   // optional per-subset mask descriptors (DG_MASK_DESC ints each), the
-  // obstruction words and the blocked words
+  // obstruction words, and the blocked-polygon table and vertices
   const int32_t* __restrict__ mask_desc;
   const uint32_t* __restrict__ mask_bits;
-  const uint32_t* __restrict__ blocked_bits;
+  const int32_t* __restrict__ blocked_poly;
+  const int32_t* __restrict__ blocked_vx;
+  const int32_t* __restrict__ blocked_vy;
 };
 
 // ---------------------------------------------------------------------------
@@ -389,6 +391,29 @@ __device__ __forceinline__ void make_mapconst(const float* slots, bool use_ref_g
     k.rcos = k.cost;
     k.rsin = k.sint;
   }
+}
+
+// angle_2d (DICe_Shape.cpp:87-102) in the reference's precision, with the
+// float atan2 correctly rounded (the double atan2 rounded to float) so that
+// pixels lying exactly on a polygon edge, whose edge term is +-pi, are
+// decided the same way as on the host.
+__device__ __forceinline__ float polygon_angle(float x1, float y1, float x2, float y2) {
+  const float t1 = (float)atan2((double)y1, (double)x1), t2 = (float)atan2((double)y2, (double)x2);
+  float d = __fsub_rn(t2, t1);
+  for (int k = 0; k < 4 && (double)d > 3.14159265358979323846; ++k) d = (float)((double)d - 6.28318530717958647692);
+  for (int k = 0; k < 4 && (double)d < -3.14159265358979323846; ++k) d = (float)((double)d + 6.28318530717958647692);
+  return d;
+}
+
+// winding-angle test over a closed vertex loop (vertex nv is vertex 0)
+__device__ __forceinline__ bool polygon_has(const int32_t* ax, const int32_t* ay, int nv, int x, int y) {
+  float angle = 0.0f;
+  for (int i = 0; i < nv; ++i) {
+    const int j = (i + 1 == nv) ? 0 : i + 1;
+    angle = __fadd_rn(angle, polygon_angle((float)(ax[i] - x), (float)(ay[i] - y), (float)(ax[j] - x),
+                                          (float)(ay[j] - y)));
+  }
+  return (double)fabsf(angle) >= 3.14159265358979323846;
 }
 
 // Pixel rounding of Subset::initialize (DICe_Subset.cpp:405-406).

@@ -239,12 +239,16 @@ struct Engine {
     if (MASK && sb.masked) {
       in.mdesc = A.geo.mask_desc + (size_t)sb.idx * DG_MASK_DESC;
       in.mbits = A.geo.mask_bits;
-      in.bbits = A.geo.blocked_bits;
+      in.bpoly = A.geo.blocked_poly;
+      in.bvx = A.geo.blocked_vx;
+      in.bvy = A.geo.blocked_vy;
       return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, true>(in, k);
     }
     in.mdesc = nullptr;
     in.mbits = nullptr;
-    in.bbits = nullptr;
+    in.bpoly = nullptr;
+    in.bvx = nullptr;
+    in.bvy = nullptr;
     return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, false>(in, k);
   }
 
@@ -945,7 +949,7 @@ struct Engine {
     sb.masked = false;
     if (MASK && A.geo.mask_desc) {
       const int32_t* md = A.geo.mask_desc + (size_t)idx * DG_MASK_DESC;
-      sb.masked = md[2] > 0 || md[7] > 0;
+      sb.masked = md[2] > 0 || md[5] > 0;
     }
 
     float slots[12];

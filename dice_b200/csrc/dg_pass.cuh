@@ -98,11 +98,14 @@ struct PassIn {
   int cx, cy, npix, off;
   float K;         // intensity shift for the moment sums
   // MASKED passes: this subset's mask descriptor (obstruction box x0, y0,
-  // w, h, word offset; blocked box likewise), the obstruction words and the
-  // blocked words
+  // w, h, word offset; blocked polygon count and table offset), the
+  // obstruction words, the blocked-polygon table (vertex offset, count, box
+  // x0, x1, y0, y1 per polygon) and the polygons' vertices
   const int32_t* __restrict__ mdesc;
   const uint32_t* __restrict__ mbits;
-  const uint32_t* __restrict__ bbits;
+  const int32_t* __restrict__ bpoly;
+  const int32_t* __restrict__ bvx;
+  const int32_t* __restrict__ bvy;
 };
 
 // Whether pixel (px, py) is set in the mask box (x0, y0, w, h) at words.
@@ -153,10 +156,10 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
     drow = 32 / side; dcol = 32 - drow * side;
   }
   const int x0 = in.cx - in.half, y0 = in.cy - in.half;
-  int m_ox = 0, m_oy = 0, m_ow = 0, m_oh = 0, m_oo = 0, m_bx = 0, m_by = 0, m_bw = 0, m_bh = 0, m_bo = 0;
+  int m_ox = 0, m_oy = 0, m_ow = 0, m_oh = 0, m_oo = 0, m_np = 0, m_po = 0;
   if (MASKED) {
     m_ox = in.mdesc[0]; m_oy = in.mdesc[1]; m_ow = in.mdesc[2]; m_oh = in.mdesc[3]; m_oo = in.mdesc[4];
-    m_bx = in.mdesc[5]; m_by = in.mdesc[6]; m_bw = in.mdesc[7]; m_bh = in.mdesc[8]; m_bo = in.mdesc[9];
+    m_np = in.mdesc[5]; m_po = in.mdesc[6];
   }
   const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_smem<SHAPE>()->vbuf);
   for (int base = 0; base < in.npix; base += 32 * PPL) {
@@ -190,9 +193,16 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
       if (ACC_H) sumFall += F - in.K;
       // 4-pixel border deactivation (DICe_Subset.cpp:408)
       bool live = !(px < 4 || px >= W - 4 || py < 4 || py >= H - 4);
-      if (MASKED && live)
-        live = !mask_bit(in.mbits + m_oo, m_ox, m_oy, m_ow, m_oh, px, py) &&
-               !mask_bit(in.bbits + m_bo, m_bx, m_by, m_bw, m_bh, px, py);
+      if (MASKED && live) {
+        live = !mask_bit(in.mbits + m_oo, m_ox, m_oy, m_ow, m_oh, px, py);
+        // blocked: inside a blocker's deformed boundary (box first)
+        for (int q = 0; live && q < m_np; ++q) {
+          const int32_t* pd = in.bpoly + 6 * (m_po + q);
+          if (px < __ldg(pd + 2) || px > __ldg(pd + 3) || py < __ldg(pd + 4) || py > __ldg(pd + 5)) continue;
+          const int vo = __ldg(pd);
+          if (polygon_has(in.bvx + vo, in.bvy + vo, __ldg(pd + 1), px, py)) live = false;
+        }
+      }
       if (live) {
         float G, gx = 0.0f, gy = 0.0f;
         if (GRADS && DEFGRAD) interp_interior<INTERP, true>(in.def, mx, my, G, gx, gy);

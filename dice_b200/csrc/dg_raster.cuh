@@ -15,11 +15,12 @@
 //
 // Masks: a subset pixel is deactivated when its deformed position rounds
 // into the subset's obstruction bitmap (static, from its obstructed shapes)
-// or its blocked bitmap (rebuilt before each tracking wave from the deformed
-// boundaries of its blocking subsets).  Each subset has a descriptor of
-// DG_MASK_DESC ints: the obstruction box (x0, y0, w, h, word offset) and the
-// blocked box (x0, y0, w, h, word offset); a box of width 0 is no mask.  Bit
-// (y - y0) * w + (x - x0) of the words from the offset is pixel (x, y).
+// or into one of its blocked polygons (rebuilt before each tracking wave
+// from the deformed boundaries of its blocking subsets).  Each subset has a
+// descriptor of DG_MASK_DESC ints: the obstruction box (x0, y0, w, h, word
+// offset; a box of width 0 is no mask; bit (y - y0) * w + (x - x0) of the
+// words from the offset is pixel (x, y)) and the blocked polygons (count,
+// offset in the polygon table).
 #pragma once
 #include <climits>
 #include <cstdint>
@@ -44,27 +45,9 @@ struct RasterArgs {
   int square_half;               // half side of the square of a subset without boundary, -1: empty
 };
 
-// angle_2d (DICe_Shape.cpp:87-102) in the reference's precision, with the
-// float atan2 correctly rounded (the double atan2 rounded to float) so that
-// pixels lying exactly on a polygon edge, whose edge term is +-pi, are
-// decided the same way as on the host.
-__device__ __forceinline__ float raster_angle(float x1, float y1, float x2, float y2) {
-  const float t1 = (float)atan2((double)y1, (double)x1), t2 = (float)atan2((double)y2, (double)x2);
-  float d = __fsub_rn(t2, t1);
-  for (int k = 0; k < 4 && (double)d > 3.14159265358979323846; ++k) d = (float)((double)d - 6.28318530717958647692);
-  for (int k = 0; k < 4 && (double)d < -3.14159265358979323846; ++k) d = (float)((double)d + 6.28318530717958647692);
-  return d;
-}
-
-// winding-angle test over a closed vertex loop (vertex nv is vertex 0)
+// the winding test of a closed vertex loop (dg::polygon_has, dg_device.cuh)
 __device__ __forceinline__ bool raster_polygon_has(const int32_t* ax, const int32_t* ay, int nv, int x, int y) {
-  float angle = 0.0f;
-  for (int i = 0; i < nv; ++i) {
-    const int j = (i + 1 == nv) ? 0 : i + 1;
-    angle = __fadd_rn(angle, raster_angle((float)(ax[i] - x), (float)(ay[i] - y), (float)(ax[j] - x),
-                                          (float)(ay[j] - y)));
-  }
-  return (double)fabsf(angle) >= 3.14159265358979323846;
+  return dg::polygon_has(ax, ay, nv, x, y);
 }
 
 // get_owned_pixels' test, or deactivate_pixels' (excluded: the circle adds
@@ -205,16 +188,16 @@ __global__ void __launch_bounds__(256) obstruction_kernel(ObstArgs a) {
   }
 }
 
-// Blocked bitmaps of the blocked subsets of one tracking wave
+// Blocked polygons of the blocked subsets of one tracking wave
 // (Schema::check_for_blocking_subsets, DICe_Schema.cpp:4529-4557): for every
 // conformal blocker j, each boundary polygon or rectangle mapped by j's
 // parameters about j's centroid, rounded, and stretched by the skin factor
 // about its integer vertex centroid (get_owned_pixels with a shape function,
-// DICe_Shape.cpp:136-219, 322-396); the union of their winding tests over
-// their box, clipped to the image.  Blocker j's parameters come from the
-// live fields when j precedes the blocked subset in index order (it has run
-// in an earlier wave), from the frame-start snapshot otherwise.  One CTA per
-// blocked subset.
+// DICe_Shape.cpp:136-219, 322-396), stored with its vertex box in the
+// subset's slots of the polygon table; the masked pass tests pixels against
+// them.  Blocker j's parameters come from the live fields when j precedes
+// the blocked subset in index order (it has run in an earlier wave), from
+// the frame-start snapshot otherwise.  One warp per blocked subset.
 struct BlockArgs {
   dg::DevParams P;
   const dicegpu_shape* shapes;
@@ -228,131 +211,94 @@ struct BlockArgs {
   const uint8_t* conformal; // subset has boundary shapes
   const int32_t* list;      // blocked subsets of this wave
   int nlist;
-  const int32_t* dv_off;    // per blocked subset: offset of its deformed vertices
+  const int32_t* dv_off;    // per subset: offset of its deformed vertices
+  const int32_t* dp_off;    // per subset: offset of its polygons in the table
   int32_t* dvx;
   int32_t* dvy;
+  int32_t* polys;           // 6 ints per polygon: vertex offset, count, x0, x1, y0, y1
   int32_t* desc;
-  uint32_t* bits;           // blocked words
-  int W, H;
   float skin;
 };
 
 template <int SHAPE>
 __global__ void __launch_bounds__(256) blocked_kernel(BlockArgs a) {
   using namespace dg;
-  __shared__ int poly_off[DG_MAX_BLOCK_POLYS], poly_n[DG_MAX_BLOCK_POLYS], poly_box[DG_MAX_BLOCK_POLYS][4];
-  __shared__ int npoly_s, box_s[4];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int t = blockIdx.x; t < a.nlist; t += gridDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < a.nlist; t += warps) {
     const int i = a.list[t];
-    // phase 1 (warp 0): deform the blockers' boundary polygons
-    if (warp == 0) {
-      int npoly = 0, wpos = a.dv_off[i];
-      for (int b = a.blk_off[i]; b < a.blk_off[i + 1]; ++b) {
-        const int j = a.blk_ids[b];
-        if (!a.conformal[j]) continue;   // a square blocker covers nothing
-        const double* f = (j < i ? a.fields : a.snapshot) + (size_t)j * DICEGPU_FIELD_STRIDE;
-        float slots[12];
-        if (SHAPE == DICEGPU_QUADRATIC_SF) {
-          for (int q = 0; q < 12; ++q) slots[q] = (float)f[DICEGPU_F_QUAD_A + q];
-        } else {
-          for (int q = 0; q < 12; ++q) slots[q] = 0.0f;
-          for (int q = 0; q < a.P.N; ++q) slots[a.P.slot[q]] = (float)f[DICEGPU_F_DISP_X + a.P.slot[q]];
+    int npoly = 0, wpos = a.dv_off[i];
+    const int pbase = a.dp_off[i];
+    for (int b = a.blk_off[i]; b < a.blk_off[i + 1]; ++b) {
+      const int j = a.blk_ids[b];
+      if (!a.conformal[j]) continue;   // a square blocker covers nothing
+      const double* f = (j < i ? a.fields : a.snapshot) + (size_t)j * DICEGPU_FIELD_STRIDE;
+      float slots[12];
+      if (SHAPE == DICEGPU_QUADRATIC_SF) {
+        for (int q = 0; q < 12; ++q) slots[q] = (float)f[DICEGPU_F_QUAD_A + q];
+      } else {
+        for (int q = 0; q < 12; ++q) slots[q] = 0.0f;
+        for (int q = 0; q < a.P.N; ++q) slots[a.P.slot[q]] = (float)f[DICEGPU_F_DISP_X + a.P.slot[q]];
+      }
+      const float fcx = (float)(int)f[DICEGPU_F_COORD_X], fcy = (float)(int)f[DICEGPU_F_COORD_Y];
+      MapConst k;
+      make_mapconst<SHAPE>(slots, false, fcx, fcy, k);
+      for (int m = a.shape_off[j]; m < a.shape_off[j + 1]; ++m) {
+        const dicegpu_shape& s = a.shapes[m];
+        if (s.role != DICEGPU_ROLE_BOUNDARY || npoly >= DG_MAX_BLOCK_POLYS) continue;
+        const int nv = s.kind == DICEGPU_SHAPE_RECTANGLE ? 4 : s.vertex_count;
+        const int ox = s.cx - s.width / 2, oy = s.cy - s.height / 2;
+        long long sx = 0, sy = 0;
+        for (int v = lane; v < nv; v += 32) {
+          int x, y;
+          if (s.kind == DICEGPU_SHAPE_RECTANGLE) {
+            x = (v == 1 || v == 2) ? ox + s.width : ox;
+            y = (v >= 2) ? oy + s.height : oy;
+          } else {
+            x = a.vx[s.vertex_offset + v];
+            y = a.vy[s.vertex_offset + v];
+          }
+          float mx, my, Dx, Dy;
+          map_offset<SHAPE>(k, __fsub_rn((float)x, fcx), __fsub_rn((float)y, fcy), fcx, fcy, mx, my, Dx, Dy);
+          int nx = (int)mx, ny = (int)my;
+          if (__fsub_rn(mx, (float)nx) >= 0.5f) ++nx;
+          if (__fsub_rn(my, (float)ny) >= 0.5f) ++ny;
+          a.dvx[wpos + v] = nx;
+          a.dvy[wpos + v] = ny;
+          sx += nx;
+          sy += ny;
         }
-        const float fcx = (float)(int)f[DICEGPU_F_COORD_X], fcy = (float)(int)f[DICEGPU_F_COORD_Y];
-        MapConst k;
-        make_mapconst<SHAPE>(slots, false, fcx, fcy, k);
-        for (int m = a.shape_off[j]; m < a.shape_off[j + 1]; ++m) {
-          const dicegpu_shape& s = a.shapes[m];
-          if (s.role != DICEGPU_ROLE_BOUNDARY || npoly >= DG_MAX_BLOCK_POLYS) continue;
-          const int nv = s.kind == DICEGPU_SHAPE_RECTANGLE ? 4 : s.vertex_count;
-          const int ox = s.cx - s.width / 2, oy = s.cy - s.height / 2;
-          long long sx = 0, sy = 0;
-          for (int v = lane; v < nv; v += 32) {
-            int x, y;
-            if (s.kind == DICEGPU_SHAPE_RECTANGLE) {
-              x = (v == 1 || v == 2) ? ox + s.width : ox;
-              y = (v >= 2) ? oy + s.height : oy;
-            } else {
-              x = a.vx[s.vertex_offset + v];
-              y = a.vy[s.vertex_offset + v];
-            }
-            float mx, my, Dx, Dy;
-            map_offset<SHAPE>(k, __fsub_rn((float)x, fcx), __fsub_rn((float)y, fcy), fcx, fcy, mx, my, Dx, Dy);
-            int nx = (int)mx, ny = (int)my;
-            if (__fsub_rn(mx, (float)nx) >= 0.5f) ++nx;
-            if (__fsub_rn(my, (float)ny) >= 0.5f) ++ny;
-            a.dvx[wpos + v] = nx;
-            a.dvy[wpos + v] = ny;
-            sx += nx;
-            sy += ny;
-          }
-          for (int o = 16; o > 0; o >>= 1) {
-            sx += __shfl_xor_sync(0xffffffffu, sx, o);
-            sy += __shfl_xor_sync(0xffffffffu, sy, o);
-          }
-          __syncwarp();
-          const int ccx = (int)((double)sx / (double)nv), ccy = (int)((double)sy / (double)nv);
-          int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
-          for (int v = lane; v < nv; v += 32) {
-            const int nx = (int)__fadd_rn(__fmul_rn(a.skin, (float)(a.dvx[wpos + v] - ccx)), (float)ccx);
-            const int ny = (int)__fadd_rn(__fmul_rn(a.skin, (float)(a.dvy[wpos + v] - ccy)), (float)ccy);
-            a.dvx[wpos + v] = nx;
-            a.dvy[wpos + v] = ny;
-            x0 = min(x0, nx); x1 = max(x1, nx); y0 = min(y0, ny); y1 = max(y1, ny);
-          }
-          for (int o = 16; o > 0; o >>= 1) {
-            x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, o));
-            x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, o));
-            y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
-            y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
-          }
-          if (lane == 0) {
-            poly_off[npoly] = wpos;
-            poly_n[npoly] = nv;
-            poly_box[npoly][0] = x0; poly_box[npoly][1] = x1;
-            poly_box[npoly][2] = y0; poly_box[npoly][3] = y1;
-          }
-          ++npoly;
-          wpos += nv;
+        for (int o = 16; o > 0; o >>= 1) {
+          sx += __shfl_xor_sync(0xffffffffu, sx, o);
+          sy += __shfl_xor_sync(0xffffffffu, sy, o);
         }
-      }
-      // the union box, clipped to the image (pixels outside it are
-      // deactivated by the border test before this mask is consulted)
-      int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
-      __syncwarp();
-      for (int q = 0; q < npoly; ++q) {
-        x0 = min(x0, poly_box[q][0]); x1 = max(x1, poly_box[q][1]);
-        y0 = min(y0, poly_box[q][2]); y1 = max(y1, poly_box[q][3]);
-      }
-      x0 = max(x0, 0); y0 = max(y0, 0); x1 = min(x1, a.W - 1); y1 = min(y1, a.H - 1);
-      if (lane == 0) {
-        npoly_s = npoly;
-        const bool empty = npoly == 0 || x1 < x0 || y1 < y0;
-        box_s[0] = x0; box_s[1] = y0;
-        box_s[2] = empty ? 0 : x1 - x0 + 1;
-        box_s[3] = empty ? 0 : y1 - y0 + 1;
+        const int ccx = (int)((double)sx / (double)nv), ccy = (int)((double)sy / (double)nv);
+        int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
+        for (int v = lane; v < nv; v += 32) {
+          const int nx = (int)__fadd_rn(__fmul_rn(a.skin, (float)(a.dvx[wpos + v] - ccx)), (float)ccx);
+          const int ny = (int)__fadd_rn(__fmul_rn(a.skin, (float)(a.dvy[wpos + v] - ccy)), (float)ccy);
+          a.dvx[wpos + v] = nx;
+          a.dvy[wpos + v] = ny;
+          x0 = min(x0, nx); x1 = max(x1, nx); y0 = min(y0, ny); y1 = max(y1, ny);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+          x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+          y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+          y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+        }
+        if (lane == 0) {
+          int32_t* pd = a.polys + 6 * (size_t)(pbase + npoly);
+          pd[0] = wpos; pd[1] = nv; pd[2] = x0; pd[3] = x1; pd[4] = y0; pd[5] = y1;
+        }
+        ++npoly;
+        wpos += nv;
       }
     }
-    __syncthreads();
-    const int bx = box_s[0], by = box_s[1], bw = box_s[2], bh = box_s[3], npoly = npoly_s;
-    int32_t* d = a.desc + (size_t)i * DG_MASK_DESC;
-    uint32_t* words = a.bits + d[9];
-    const long nbits = (long)bw * bh, nwords = (nbits + 31) >> 5;
-    for (long w = threadIdx.x; w < nwords; w += blockDim.x) words[w] = 0u;
-    __syncthreads();
-    for (long p = threadIdx.x; p < nbits; p += blockDim.x) {
-      const int x = bx + (int)(p % bw), y = by + (int)(p / bw);
-      bool on = false;
-      for (int q = 0; q < npoly && !on; ++q) {
-        if (x < poly_box[q][0] || x > poly_box[q][1] || y < poly_box[q][2] || y > poly_box[q][3]) continue;
-        on = raster_polygon_has(a.dvx + poly_off[q], a.dvy + poly_off[q], poly_n[q], x, y);
-      }
-      if (on) atomicOr(words + (p >> 5), 1u << (p & 31));
+    if (lane == 0) {
+      int32_t* d = a.desc + (size_t)i * DG_MASK_DESC;
+      d[5] = npoly;
+      d[6] = pbase;
     }
-    if (threadIdx.x == 0) {
-      d[5] = bx; d[6] = by; d[7] = bw; d[8] = bh;
-    }
-    __syncthreads();
   }
 }

@@ -282,18 +282,17 @@ struct dicegpu_ctx {
   // pixel masks: descriptors (host copy kept), obstruction words, blocked words
   std::vector<int32_t> h_mask_desc;
   DevBuf<int32_t> d_mask_desc;
-  DevBuf<uint32_t> d_mask_bits, d_blocked_bits;
+  DevBuf<uint32_t> d_mask_bits;
   bool use_masks = false;
-  int blocked_W = 0, blocked_H = 0;   // image size the blocked words were sized for
+  bool blocking_desc_ready = false;   // descriptors on the device for the tracking waves
   // blocking subsets and the tracking waves
   bool has_blocking = false;
   std::vector<int32_t> h_blk_off, h_blk_ids;
   DevBuf<int32_t> d_blk_off, d_blk_ids;
   std::vector<int32_t> wave_off, bwave_off;   // wave L: d_wave[wave_off[L] ..), d_bwave[bwave_off[L] ..)
-  DevBuf<int32_t> d_wave, d_bwave, d_dv_off, d_dvx, d_dvy;
+  DevBuf<int32_t> d_wave, d_bwave, d_dv_off, d_dvx, d_dvy, d_dp_off, d_bpoly;
   DevBuf<double> d_snapshot;
   int n_blocked = 0;                   // subsets with a conformal blocker
-  std::vector<int32_t> h_blocked_slot; // their index among those, -1 otherwise
   // forced simplex: the caller's flags and the blocking rule's
   std::vector<uint8_t> h_force_user, h_force_block;
   // VSG strain: the neighbour grid of the subset centres (rebuilt when the
@@ -468,7 +467,8 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   cudaFree(c->d_unc);
   c->d_shapes.release(); c->d_shape_off.release(); c->d_svx.release(); c->d_svy.release();
   c->d_conformal.release(); c->d_mask_desc.release(); c->d_mask_bits.release();
-  c->d_blocked_bits.release(); c->d_blk_off.release(); c->d_blk_ids.release(); c->d_wave.release();
+  c->d_blk_off.release(); c->d_blk_ids.release(); c->d_wave.release();
+  c->d_dp_off.release(); c->d_bpoly.release();
   c->d_bwave.release(); c->d_dv_off.release(); c->d_dvx.release(); c->d_dvy.release();
   c->d_snapshot.release();
   c->d_vsg_cell_off.release(); c->d_vsg_cell_pts.release(); c->d_vsg.release();
@@ -821,7 +821,8 @@ static void clear_shapes(dicegpu_ctx* c) {
   c->h_conformal.clear(); c->h_mask_desc.clear();
   c->use_masks = false;
   c->has_blocking = false;
-  c->h_blk_off.clear(); c->h_blk_ids.clear(); c->h_blocked_slot.clear();
+  c->h_blk_off.clear(); c->h_blk_ids.clear();
+  c->blocking_desc_ready = false;
   c->wave_off.clear(); c->bwave_off.clear();
   c->n_blocked = 0;
   c->h_force_block.clear();
@@ -992,7 +993,7 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
         CK(cudaMemcpy(c->d_mask_desc.p, c->h_mask_desc.data(), c->h_mask_desc.size() * sizeof(int32_t),
                       cudaMemcpyHostToDevice));
       c->use_masks = any;
-      c->blocked_W = c->blocked_H = 0;
+      c->blocking_desc_ready = false;
     }
     return upload_force(c);
   }
@@ -1002,10 +1003,10 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
   for (int k = 0; k < offsets[n]; ++k)
     if (ids[k] < 0 || ids[k] >= n) return DICEGPU_ERR_ARG;
   const bool have_shapes = (int)c->h_conformal.size() == n;
-  // deformed vertices per blocked subset, and the polygon limit
-  std::vector<int32_t> dv_off, blocked_slot(n, -1);
-  std::vector<uint8_t> force(n, 0);
-  int64_t dv_total = 0;
+  // deformed vertices and polygon-table slots per blocked subset
+  std::vector<int32_t> dv_off, dp_off(n, 0);
+  std::vector<uint8_t> force(n, 0), has_polys(n, 0);
+  int64_t dv_total = 0, dp_total = 0;
   int n_blocked = 0;
   for (int i = 0; i < n; ++i) {
     if (offsets[i + 1] > offsets[i]) force[i] = 1;   // blocked
@@ -1024,15 +1025,16 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
       }
     }
     if (polys > DG_MAX_BLOCK_POLYS) return DICEGPU_ERR_UNSUPPORTED;
+    dv_off.push_back((int32_t)dv_total);
+    dp_off[i] = (int32_t)dp_total;
     if (polys > 0) {
-      blocked_slot[i] = n_blocked++;
-      dv_off.push_back((int32_t)dv_total);
+      has_polys[i] = 1;
+      ++n_blocked;
       dv_total += verts;
-    } else {
-      dv_off.push_back((int32_t)dv_total);
+      dp_total += polys;
     }
   }
-  if (dv_total > ((int64_t)1 << 30)) return DICEGPU_ERR_ARG;
+  if (dv_total > ((int64_t)1 << 30) || dp_total > ((int64_t)1 << 26)) return DICEGPU_ERR_ARG;
   // waves: a subset runs after every blocker that precedes it in index order
   std::vector<int> level(n, 0);
   int nlev = 1;
@@ -1046,7 +1048,7 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
     for (int i = 0; i < n; ++i)
       if (level[i] == L) {
         wave.push_back(i);
-        if (blocked_slot[i] >= 0) bwave.push_back(i);
+        if (has_polys[i]) bwave.push_back(i);
       }
     wave_off[L + 1] = (int32_t)wave.size();
     bwave_off[L + 1] = (int32_t)bwave.size();
@@ -1055,7 +1057,8 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
   if ((rc = c->d_blk_off.ensure(n + 1)) || (rc = c->d_blk_ids.ensure(std::max(offsets[n], 1))) ||
       (rc = c->d_wave.ensure(n)) || (rc = c->d_bwave.ensure(std::max<size_t>(bwave.size(), 1))) ||
       (rc = c->d_dv_off.ensure(n)) || (rc = c->d_dvx.ensure((size_t)std::max<int64_t>(dv_total, 1))) ||
-      (rc = c->d_dvy.ensure((size_t)std::max<int64_t>(dv_total, 1))) ||
+      (rc = c->d_dvy.ensure((size_t)std::max<int64_t>(dv_total, 1))) || (rc = c->d_dp_off.ensure(n)) ||
+      (rc = c->d_bpoly.ensure(6 * (size_t)std::max<int64_t>(dp_total, 1))) ||
       (rc = c->d_snapshot.ensure((size_t)n * DICEGPU_FIELD_STRIDE)))
     return rc;
   CK(cudaMemcpy(c->d_blk_off.p, offsets, (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
@@ -1064,38 +1067,33 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
   if (!bwave.empty())
     CK(cudaMemcpy(c->d_bwave.p, bwave.data(), bwave.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_dv_off.p, dv_off.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_dp_off.p, dp_off.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
   c->h_blk_off.assign(offsets, offsets + n + 1);
   c->h_blk_ids.assign(ids, ids + offsets[n]);
   c->wave_off.swap(wave_off);
   c->bwave_off.swap(bwave_off);
-  c->h_blocked_slot.swap(blocked_slot);
   c->n_blocked = n_blocked;
-  c->blocked_W = c->blocked_H = 0;   // blocked words sized at the next tracking frame
+  c->blocking_desc_ready = false;   // descriptors uploaded at the next tracking frame
   c->h_force_block.swap(force);
   c->has_blocking = true;
   if (c->h_mask_desc.empty()) c->h_mask_desc.assign((size_t)n * DG_MASK_DESC, 0);
   return upload_force(c);
 }
 
-// Sizes the blocked words for the current image (one full-image bitmap per
-// subset with a conformal blocker) and points the descriptors at them.
-static int ensure_blocked_words(dicegpu_ctx* c) {
-  if (c->blocked_W == c->W && c->blocked_H == c->H) return DICEGPU_OK;
-  const size_t per = ((size_t)c->W * c->H + 31) / 32;
-  const size_t total = per * (size_t)std::max(c->n_blocked, 1);
-  if (total * sizeof(uint32_t) > ((size_t)4 << 30)) return DICEGPU_ERR_NOMEM;
+// Puts the mask descriptors on the device for the tracking waves (the
+// blocked-polygon counts start at zero; blocked_kernel fills them).
+static int ensure_blocking_desc(dicegpu_ctx* c) {
+  if (c->blocking_desc_ready) return DICEGPU_OK;
   cudaStreamSynchronize(c->stream);
   int rc;
-  if ((rc = c->d_blocked_bits.ensure(total)) || (rc = c->d_mask_desc.ensure(c->h_mask_desc.size()))) return rc;
+  if ((rc = c->d_mask_desc.ensure(c->h_mask_desc.size()))) return rc;
   for (int i = 0; i < c->n; ++i) {
     int32_t* d = &c->h_mask_desc[(size_t)i * DG_MASK_DESC];
-    d[5] = d[6] = d[7] = d[8] = 0;
-    d[9] = c->h_blocked_slot[i] >= 0 ? (int32_t)(per * c->h_blocked_slot[i]) : 0;
+    d[5] = d[6] = d[7] = d[8] = d[9] = 0;
   }
   CK(cudaMemcpy(c->d_mask_desc.p, c->h_mask_desc.data(), c->h_mask_desc.size() * sizeof(int32_t),
                 cudaMemcpyHostToDevice));
-  c->blocked_W = c->W;
-  c->blocked_H = c->H;
+  c->blocking_desc_ready = true;
   c->use_masks = true;
   return DICEGPU_OK;
 }
@@ -1287,7 +1285,9 @@ static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
   a.geo.force_simplex = c->use_force ? c->d_force : nullptr;
   a.geo.mask_desc = c->use_masks ? c->d_mask_desc.p : nullptr;
   a.geo.mask_bits = c->d_mask_bits.p;
-  a.geo.blocked_bits = c->d_blocked_bits.p;
+  a.geo.blocked_poly = c->d_bpoly.p;
+  a.geo.blocked_vx = c->d_dvx.p;
+  a.geo.blocked_vy = c->d_dvy.p;
   a.fields = c->d_fields;
   a.n = c->n;
   a.first_frame = c->frame_index == 0;
@@ -1329,7 +1329,7 @@ static int ready(dicegpu_ctx* c) {
 // blockers' parameters (this frame's for earlier subsets, the frame-start
 // snapshot's for later ones).  Everything is enqueued on the stream.
 static int run_tracking_frame(dicegpu_ctx* c, FrameKernelFn fn, int blocks, size_t smem) {
-  int rc = ensure_blocked_words(c);
+  int rc = ensure_blocking_desc(c);
   if (rc) return rc;
   const int n = c->n;
   CK(cudaMemcpyAsync(c->d_snapshot.p, c->d_fields, (size_t)n * DICEGPU_FIELD_STRIDE * sizeof(double),
@@ -1347,12 +1347,11 @@ static int run_tracking_frame(dicegpu_ctx* c, FrameKernelFn fn, int blocks, size
   ba.blk_ids = c->d_blk_ids.p;
   ba.conformal = c->d_conformal.p;
   ba.dv_off = c->d_dv_off.p;
+  ba.dp_off = c->d_dp_off.p;
   ba.dvx = c->d_dvx.p;
   ba.dvy = c->d_dvy.p;
+  ba.polys = c->d_bpoly.p;
   ba.desc = c->d_mask_desc.p;
-  ba.bits = c->d_blocked_bits.p;
-  ba.W = c->W;
-  ba.H = c->H;
   ba.skin = (float)c->params.obstruction_skin_factor;
   const int nlev = (int)c->wave_off.size() - 1;
   for (int L = 0; L < nlev; ++L) {
@@ -1360,7 +1359,7 @@ static int run_tracking_frame(dicegpu_ctx* c, FrameKernelFn fn, int blocks, size
     if (nb > 0) {
       ba.list = c->d_bwave.p + c->bwave_off[L];
       ba.nlist = nb;
-      const unsigned g = (unsigned)std::min(nb, 4 * c->num_sms);
+      const unsigned g = (unsigned)std::min((nb * 32 + 255) / 256, 8 * c->num_sms);   // a warp per subset
       if (c->dp.shape == DICEGPU_QUADRATIC_SF) blocked_kernel<DICEGPU_QUADRATIC_SF><<<g, 256, 0, c->stream>>>(ba);
       else blocked_kernel<DICEGPU_AFFINE_SF><<<g, 256, 0, c->stream>>>(ba);
       CK(cudaGetLastError());
@@ -1430,9 +1429,9 @@ extern "C" int dicegpu_capture_sequence(dicegpu_ctx* c, int n, const float* cons
     if (!frames[k]) return DICEGPU_ERR_ARG;
   if (!c->has_ref || c->n < 1) return DICEGPU_ERR_STATE;
   if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
-  // the blocked bitmaps are sized before capture (allocation cannot be captured)
+  // the blocking descriptors are uploaded before capture (synchronous copies cannot be captured)
   if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE) {
-    const int rcb = ensure_blocked_words(c);
+    const int rcb = ensure_blocking_desc(c);
     if (rcb) return rcb;
   }
   CK(cudaStreamSynchronize(c->stream));
