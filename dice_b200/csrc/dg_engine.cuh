@@ -190,7 +190,7 @@ struct SubsetRef {
   int idx, cx, cy, npix;
   int off;          // list offset (-1 for squares)
   float K;          // intensity shift for the moment sums
-  bool masked;      // has an obstruction or blocked bitmap
+  bool masked;      // has an obstruction bitmap or blocked polygons
 };
 
 template <int SHAPE, int INTERP, bool DEFGRAD, bool MASK>

@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(256, DG_MIN_BLOCKS) frame_kernel(const __grid_
 typedef void (*FrameKernelFn)(FrameArgs);
 
 // The frame kernel of a configuration; MASK selects the instantiation whose
-// passes test obstruction and blocked bitmaps (only subsets with masks pay
+// passes test obstruction bitmaps and blocked polygons (only subsets with masks pay
 // for it, and only contexts with masks launch it).
 template <int SHAPE, bool MASK>
 static FrameKernelFn pick_kernel(int interp, bool defgrad) {

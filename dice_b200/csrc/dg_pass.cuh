@@ -121,7 +121,7 @@ __device__ __forceinline__ bool mask_bit(const uint32_t* __restrict__ words, int
 //   GRADS   : interpolate the deformed gradients (DEFGRAD) / read reference ones
 //   MOMENTS : FP64 intensity moments for gamma
 //   MASKED  : also deactivate pixels whose position rounds into the
-//             subset's obstruction or blocked bitmap (Subset::initialize,
+//             subset's obstruction bitmap or a blocked polygon (Subset::initialize,
 //             DICe_Subset.cpp:412-422); for positive coordinates, which the
 //             border test leaves, is_obstructed_pixel's rounding is the
 //             border test's

@@ -1325,7 +1325,7 @@ static int ready(dicegpu_ctx* c) {
 }
 
 // TRACKING_ROUTINE with blocking subsets: the frame runs in waves, each
-// after the blocked bitmaps of its blocked subsets are rebuilt from their
+// after the blocked polygons of its blocked subsets are rebuilt from their
 // blockers' parameters (this frame's for earlier subsets, the frame-start
 // snapshot's for later ones).  Everything is enqueued on the stream.
 static int run_tracking_frame(dicegpu_ctx* c, FrameKernelFn fn, int blocks, size_t smem) {
