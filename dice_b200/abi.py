@@ -111,7 +111,7 @@ class Params(ctypes.Structure):
         ("correlation_routine", ctypes.c_int32),
         ("obstruction_skin_factor", ctypes.c_double),
         ("override_force_simplex", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 1),
+        ("use_subset_evolution", ctypes.c_int32),
     ]
 
     def copy(self):
@@ -164,6 +164,7 @@ def tracking_default_params(**overrides):
     p.theta_jump_tol = 0.1
     p.obstruction_skin_factor = 1.8
     p.override_force_simplex = 1
+    p.use_subset_evolution = 1
     for k, v in overrides.items():
         if not hasattr(p, k):
             raise AttributeError(k)
@@ -214,6 +215,7 @@ def _declare(lib):
         "dicegpu_set_subset_pixels": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "dicegpu_set_subset_shapes": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "dicegpu_get_subset_pixels": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        "dicegpu_get_subset_pixel_state": (c_int, [c_void_p, c_void_p, c_void_p]),
         "dicegpu_set_blocking": (c_int, [c_void_p, c_void_p, c_void_p]),
         "dicegpu_get_params": (c_int, [c_void_p, P]),
         "dicegpu_subset_file_read": (c_int, [ctypes.c_char_p, c_int, c_int, ctypes.POINTER(c_void_p),

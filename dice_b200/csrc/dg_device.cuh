@@ -60,8 +60,10 @@ struct DevImage {
 };
 
 // ints per subset mask descriptor: obstruction box (x0, y0, w, h, word
-// offset), blocked polygons (count, table offset), three spare
+// offset), blocked polygons (count, table offset), subset evolution (1: the
+// subset's list keeps its excluded pixels, with per-pixel state), two spare
 #define DG_MASK_DESC 10
+#define DG_DESC_EVOLVE 7
 
 // Subset geometry: square (`half` >= 0, centred on the COORD fields) or an
 // explicit pixel list in CSR form.
@@ -78,6 +80,13 @@ struct DevGeometry {
   const int32_t* __restrict__ blocked_poly;
   const int32_t* __restrict__ blocked_vx;
   const int32_t* __restrict__ blocked_vy;
+  // subset evolution state of the list pixels of subsets whose descriptor
+  // has DG_DESC_EVOLVE set: 0 inactive (excluded), 1 active, 2 turned on
+  // with the reference intensity in pix_f; evo_nact the subsets' counts of
+  // pixels with state != 0
+  uint8_t* pix_flag;
+  float* pix_f;
+  int32_t* evo_nact;
 };
 
 // ---------------------------------------------------------------------------

@@ -47,6 +47,7 @@ struct FrameArgs {
   double* noise_out;     // MODE_SIGMA: noise_std_dev per subset (sigma goes to gamma_out)
   const int32_t* order;  // optional: the subsets of this launch (a tracking wave), n_order of them
   int n_order;
+  int evolve;            // turn on visible inactive pixels of evolving subsets after success
 };
 
 // Image_::interpolate_keys_fourth (DICe_Image.cpp:890-924), intensity only:
@@ -190,7 +191,9 @@ struct SubsetRef {
   int idx, cx, cy, npix;
   int off;          // list offset (-1 for squares)
   float K;          // intensity shift for the moment sums
-  bool masked;      // has an obstruction bitmap or blocked polygons
+  bool masked;      // has an obstruction bitmap, blocked polygons or evolution state
+  bool evo;         // evolving: its list keeps inactive pixels (per-pixel state)
+  int nact;         // pixels with is_active set (npix unless evolving)
 };
 
 template <int SHAPE, int INTERP, bool DEFGRAD, bool MASK>
@@ -242,6 +245,8 @@ struct Engine {
       in.bpoly = A.geo.blocked_poly;
       in.bvx = A.geo.blocked_vx;
       in.bvy = A.geo.blocked_vy;
+      in.pflag = sb.evo ? A.geo.pix_flag : nullptr;
+      in.pfv = sb.evo ? A.geo.pix_f : nullptr;
       return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, true>(in, k);
     }
     in.mdesc = nullptr;
@@ -249,6 +254,8 @@ struct Engine {
     in.bpoly = nullptr;
     in.bvx = nullptr;
     in.bvy = nullptr;
+    in.pflag = nullptr;
+    in.pfv = nullptr;
     return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, false>(in, k);
   }
 
@@ -272,7 +279,7 @@ struct Engine {
     PassOut o = pass<false, false, true>(sb, slots, nullptr);
     if (out) *out = o;
     ++npass_;
-    return gamma_from(o, sb.npix);
+    return gamma_from(o, sb.nact);
   }
 
   __device__ void compact_to_slots(const float* comp, float* slots, const float* base) const {
@@ -364,6 +371,38 @@ struct Engine {
     }
   }
 
+  // Subset::turn_on_previously_obstructed_pixels (DICe_Subset.cpp:506-520)
+  // after a successful solve (DICe_Schema.cpp:2354-2360): each inactive
+  // pixel that the last deformed-state initialisation (the final parameters,
+  // Objective::gamma) left visible takes the deformed intensity interpolated
+  // there as its reference intensity and becomes active.
+  __device__ __noinline__ void evolve(const SubsetRef sb, const Slots fin) {
+    MapConst k;
+    const float fcx = (float)sb.cx, fcy = (float)sb.cy;
+    make_mapconst<SHAPE>(fin.s, !DEFGRAD, fcx, fcy, k);
+    const int W = A.def.w, H = A.def.h;
+    const MaskView mv(A.geo.mask_desc + (size_t)sb.idx * DG_MASK_DESC, A.geo.mask_bits, A.geo.blocked_poly,
+                      A.geo.blocked_vx, A.geo.blocked_vy);
+    int on = 0;
+    for (int p = lane; p < sb.npix; p += 32) {
+      uint8_t* st = A.geo.pix_flag + sb.off + p;
+      if (*st != 0) continue;
+      int x, y;
+      pixel_xy(sb, p, x, y);
+      float mx, my, Dx, Dy;
+      map_offset<SHAPE>(k, __fsub_rn((float)x, fcx), __fsub_rn((float)y, fcy), fcx, fcy, mx, my, Dx, Dy);
+      const int px = round_pixel(mx), py = round_pixel(my);
+      if (px < 4 || px >= W - 4 || py < 4 || py >= H - 4 || mv.hides(px, py)) continue;
+      float G, gx, gy;
+      interp_interior<INTERP, false>(A.def, mx, my, G, gx, gy);
+      A.geo.pix_f[sb.off + p] = G;
+      *st = 2;
+      ++on;
+    }
+    on = warp_sum_i(on);
+    if (lane == 0 && on) A.geo.evo_nact[sb.idx] += on;
+  }
+
   __device__ __forceinline__ void uncertainty_hook(const SubsetRef& sb, const float* before,
                                                    const float* after) {
     Slots b, a;
@@ -402,8 +441,8 @@ struct Engine {
       const double sumG = M[L::ID * L::VW + L::IONE] + last.sumF + (double)n * (double)sb.K;
       const float meanG = n ? (float)(sumG / (double)n) : 0.0f;
       if (meanF_from_pass && solve_it == 0) {
-        // Subset::mean(REF_INTENSITIES) at entry: every pixel of a fresh subset
-        meanF = sb.npix ? (float)((last.sumFall + (double)sb.npix * (double)sb.K) / (double)sb.npix)
+        // Subset::mean(REF_INTENSITIES) at entry: every active pixel of a fresh subset
+        meanF = sb.nact ? (float)((last.sumFall + (double)sb.nact * (double)sb.K) / (double)sb.nact)
                         : 0.0f;
       }
       const double cshift = (double)meanG - (double)meanF;
@@ -947,9 +986,13 @@ struct Engine {
       sb.K = __ldg(A.ref.I + (size_t)ky * A.ref.w + kx);
     }
     sb.masked = false;
+    sb.evo = false;
+    sb.nact = sb.npix;
     if (MASK && A.geo.mask_desc) {
       const int32_t* md = A.geo.mask_desc + (size_t)idx * DG_MASK_DESC;
-      sb.masked = md[2] > 0 || md[5] > 0;
+      sb.evo = md[DG_DESC_EVOLVE] != 0 && A.geo.pix_flag != nullptr && sb.off >= 0;
+      if (sb.evo) sb.nact = A.geo.evo_nact[idx];
+      sb.masked = md[2] > 0 || md[5] > 0 || sb.evo;
     }
 
     float slots[12];
@@ -1125,6 +1168,14 @@ struct Engine {
       f[DICEGPU_F_ACTIVE_PIXELS] = fin.n;
       f[DICEGPU_F_STATUS] = init_status;
       f[DICEGPU_F_ITERATIONS] = num_iterations;
+    }
+    if constexpr (MASK) {
+      if (sb.evo && A.evolve) {
+        Slots fs;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) fs.s[i] = slots[i];
+        evolve(sb, fs);
+      }
     }
   }
 };

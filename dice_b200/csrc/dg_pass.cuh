@@ -106,6 +106,11 @@ struct PassIn {
   const int32_t* __restrict__ bpoly;
   const int32_t* __restrict__ bvx;
   const int32_t* __restrict__ bvy;
+  // MASKED passes of evolving subsets: the list pixels' evolution state
+  // (0 inactive, 1 active, 2 active with the reference intensity in pfv);
+  // nullptr otherwise
+  const uint8_t* pflag;
+  const float* pfv;
 };
 
 // Whether pixel (px, py) is set in the mask box (x0, y0, w, h) at words.
@@ -116,6 +121,37 @@ __device__ __forceinline__ bool mask_bit(const uint32_t* __restrict__ words, int
   const unsigned long bit = (unsigned long)dy * (unsigned)w + dx;
   return (__ldg(words + (bit >> 5)) >> (bit & 31)) & 1u;
 }
+
+// One subset's masks, unpacked from its descriptor.
+struct MaskView {
+  int ox, oy, ow, oh;                 // obstruction box
+  const uint32_t* __restrict__ bits;  // its words
+  int np;                             // blocked polygons
+  const int32_t* __restrict__ poly;   // their table rows
+  const int32_t* __restrict__ bvx;
+  const int32_t* __restrict__ bvy;
+
+  __device__ __forceinline__ MaskView()
+      : ox(0), oy(0), ow(0), oh(0), bits(nullptr), np(0), poly(nullptr), bvx(nullptr), bvy(nullptr) {}
+  __device__ __forceinline__ MaskView(const int32_t* md, const uint32_t* mbits, const int32_t* bpoly,
+                                      const int32_t* vx, const int32_t* vy)
+      : ox(md[0]), oy(md[1]), ow(md[2]), oh(md[3]), bits(mbits + md[4]), np(md[5]), poly(bpoly + 6 * md[6]),
+        bvx(vx), bvy(vy) {}
+
+  // is_obstructed_pixel, then the blocked-pixel test, at the rounded mapped
+  // pixel (Subset::initialize, DICe_Subset.cpp:412-422): an obstruction bit,
+  // or inside a blocker's deformed boundary (box first)
+  __device__ __forceinline__ bool hides(int px, int py) const {
+    if (mask_bit(bits, ox, oy, ow, oh, px, py)) return true;
+    for (int q = 0; q < np; ++q) {
+      const int32_t* pd = poly + 6 * q;
+      if (px < __ldg(pd + 2) || px > __ldg(pd + 3) || py < __ldg(pd + 4) || py > __ldg(pd + 5)) continue;
+      const int vo = __ldg(pd);
+      if (polygon_has(bvx + vo, bvy + vo, __ldg(pd + 1), px, py)) return true;
+    }
+    return false;
+  }
+};
 
 //   ACC_H   : accumulate sum v v^T into the warp's smem matrix (Gauss-Newton)
 //   GRADS   : interpolate the deformed gradients (DEFGRAD) / read reference ones
@@ -156,11 +192,8 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
     drow = 32 / side; dcol = 32 - drow * side;
   }
   const int x0 = in.cx - in.half, y0 = in.cy - in.half;
-  int m_ox = 0, m_oy = 0, m_ow = 0, m_oh = 0, m_oo = 0, m_np = 0, m_po = 0;
-  if (MASKED) {
-    m_ox = in.mdesc[0]; m_oy = in.mdesc[1]; m_ow = in.mdesc[2]; m_oh = in.mdesc[3]; m_oo = in.mdesc[4];
-    m_np = in.mdesc[5]; m_po = in.mdesc[6];
-  }
+  MaskView mv;
+  if (MASKED) mv = MaskView(in.mdesc, in.mbits, in.bpoly, in.bvx, in.bvy);
   const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_smem<SHAPE>()->vbuf);
   for (int base = 0; base < in.npix; base += 32 * PPL) {
     float vv[PPL][L::VW];
@@ -189,20 +222,19 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
       // same element inside the array, 0 outside it
       const long ri = (long)y * in.refw + x;
       const bool rin = ri < in.reflim;
-      const float F = rin ? __ldg(in.refI + ri) : 0.0f;
-      if (ACC_H) sumFall += F - in.K;
-      // 4-pixel border deactivation (DICe_Subset.cpp:408)
-      bool live = !(px < 4 || px >= W - 4 || py < 4 || py >= H - 4);
-      if (MASKED && live) {
-        live = !mask_bit(in.mbits + m_oo, m_ox, m_oy, m_ow, m_oh, px, py);
-        // blocked: inside a blocker's deformed boundary (box first)
-        for (int q = 0; live && q < m_np; ++q) {
-          const int32_t* pd = in.bpoly + 6 * (m_po + q);
-          if (px < __ldg(pd + 2) || px > __ldg(pd + 3) || py < __ldg(pd + 4) || py > __ldg(pd + 5)) continue;
-          const int vo = __ldg(pd);
-          if (polygon_has(in.bvx + vo, in.bvy + vo, __ldg(pd + 1), px, py)) live = false;
-        }
+      float F = rin ? __ldg(in.refI + ri) : 0.0f;
+      // subset evolution: an inactive pixel takes no part; a turned-on one
+      // has its stored reference intensity
+      bool active = true;
+      if (MASKED && in.pflag) {
+        const int st = in.pflag[in.off + p];
+        active = st != 0;
+        if (st == 2) F = in.pfv[in.off + p];
       }
+      if (ACC_H && active) sumFall += F - in.K;
+      // 4-pixel border deactivation (DICe_Subset.cpp:408)
+      bool live = active && !(px < 4 || px >= W - 4 || py < 4 || py >= H - 4);
+      if (MASKED && live) live = !mv.hides(px, py);
       if (live) {
         float G, gx = 0.0f, gy = 0.0f;
         if (GRADS && DEFGRAD) interp_interior<INTERP, true>(in.def, mx, my, G, gx, gy);

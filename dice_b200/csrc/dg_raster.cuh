@@ -21,6 +21,10 @@
 // offset; a box of width 0 is no mask; bit (y - y0) * w + (x - x0) of the
 // words from the offset is pixel (x, y)) and the blocked polygons (count,
 // offset in the polygon table).
+//
+// Subset evolution (Subset::turn_on_previously_obstructed_pixels): the
+// excluded pixels then stay in the lists, inactive, as the reference's
+// conformal Subset keeps them with is_active false (DICe_Subset.cpp:155-160).
 #pragma once
 #include <climits>
 #include <cstdint>
@@ -43,6 +47,11 @@ struct RasterArgs {
   int32_t* py;
   const double* fields;          // subset centroids (squares)
   int square_half;               // half side of the square of a subset without boundary, -1: empty
+  // subset evolution: excluded pixels stay in the lists with state 0 (the
+  // others 1); the count pass also counts the active pixels
+  int keep_excluded;
+  uint8_t* flags;                // fill pass
+  int32_t* active;               // count pass
 };
 
 // the winding test of a closed vertex loop (dg::polygon_has, dg_device.cuh)
@@ -115,15 +124,15 @@ __global__ void __launch_bounds__(256) raster_kernel(RasterArgs a) {
       x0 = cx - a.square_half; x1 = cx + a.square_half;
       y0 = cy - a.square_half; y1 = cy + a.square_half;
     }
-    int cnt = 0;
+    int cnt = 0, nact = 0;
     const int base = FILL ? a.offsets[i] : 0;
     for (int y = y0; (any || square) && y <= y1; ++y)
       for (int xs = x0; xs <= x1; xs += 32) {
         const int x = xs + lane;
-        bool own = false;
+        bool own = false, act = false;
         if (x <= x1) {
           if (square) {
-            own = true;
+            own = act = true;
           } else {
             // excluded shapes test the clamped coordinates, as
             // deactivate_pixels sees the constructed (clamped) pixel list
@@ -137,7 +146,8 @@ __global__ void __launch_bounds__(256) raster_kernel(RasterArgs a) {
                 if (!out) out = raster_has(s, a.vx, a.vy, ex, ey, true);
               }
             }
-            own = in && !out;
+            own = in && (!out || a.keep_excluded);
+            act = in && !out;
           }
         }
         const unsigned m = __ballot_sync(0xffffffffu, own);
@@ -145,10 +155,15 @@ __global__ void __launch_bounds__(256) raster_kernel(RasterArgs a) {
           const int pos = base + cnt + __popc(m & ((1u << lane) - 1u));
           a.px[pos] = x < 0 ? 0 : x;
           a.py[pos] = y < 0 ? 0 : y;
+          if (a.flags) a.flags[pos] = act ? 1 : 0;
         }
         cnt += __popc(m);
+        nact += __popc(__ballot_sync(0xffffffffu, act));
       }
-    if (!FILL && lane == 0) a.counts[i] = cnt;
+    if (!FILL && lane == 0) {
+      a.counts[i] = cnt;
+      if (a.active) a.active[i] = nact;
+    }
   }
 }
 

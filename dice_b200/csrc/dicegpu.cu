@@ -284,6 +284,16 @@ struct dicegpu_ctx {
   DevBuf<int32_t> d_mask_desc;
   DevBuf<uint32_t> d_mask_bits;
   bool use_masks = false;
+  // subset evolution (params.use_subset_evolution, tracking routine): the
+  // list pixels' state and stored reference intensities, their initial
+  // state (restored at the first frame of a sequence) and per-subset active
+  // counts
+  bool has_evo = false;
+  bool evo_suspend = false;   // the autotuner's trial frames leave the state alone
+  size_t evo_total = 0;       // list pixels (state entries)
+  DevBuf<uint8_t> d_pix_flag, d_pix_flag0;
+  DevBuf<float> d_pix_f;
+  DevBuf<int32_t> d_evo_nact, d_evo_nact0;
   bool blocking_desc_ready = false;   // descriptors on the device for the tracking waves
   // blocking subsets and the tracking waves
   bool has_blocking = false;
@@ -422,6 +432,7 @@ extern "C" int dicegpu_tracking_default_params(dicegpu_params* p) {
   p->theta_jump_tol = 0.1;
   p->obstruction_skin_factor = 1.8;
   p->override_force_simplex = 1;
+  p->use_subset_evolution = 1;
   return DICEGPU_OK;
 }
 
@@ -467,6 +478,8 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   cudaFree(c->d_unc);
   c->d_shapes.release(); c->d_shape_off.release(); c->d_svx.release(); c->d_svy.release();
   c->d_conformal.release(); c->d_mask_desc.release(); c->d_mask_bits.release();
+  c->d_pix_flag.release(); c->d_pix_flag0.release(); c->d_pix_f.release();
+  c->d_evo_nact.release(); c->d_evo_nact0.release();
   c->d_blk_off.release(); c->d_blk_ids.release(); c->d_wave.release();
   c->d_dp_off.release(); c->d_bpoly.release();
   c->d_bwave.release(); c->d_dv_off.release(); c->d_dvx.release(); c->d_dvy.release();
@@ -761,6 +774,7 @@ extern "C" int dicegpu_set_subset_pixels(dicegpu_ctx* c, int n, const int32_t* o
     CK(cudaMemcpy(c->d_py, py, total * sizeof(int32_t), cudaMemcpyHostToDevice));
   }
   c->use_lists = true;
+  c->has_evo = false;   // explicit lists carry no evolution state
   return DICEGPU_OK;
 }
 
@@ -820,6 +834,7 @@ static void clear_shapes(dicegpu_ctx* c) {
   c->h_shapes.clear(); c->h_shape_off.clear(); c->h_svx.clear(); c->h_svy.clear();
   c->h_conformal.clear(); c->h_mask_desc.clear();
   c->use_masks = false;
+  c->has_evo = false;
   c->has_blocking = false;
   c->h_blk_off.clear(); c->h_blk_ids.clear();
   c->blocking_desc_ready = false;
@@ -883,6 +898,19 @@ extern "C" int dicegpu_set_subset_shapes(dicegpu_ctx* c, int n_shapes, const dic
   if (obst_words > ((int64_t)1 << 31)) return DICEGPU_ERR_ARG;
   std::vector<uint8_t> conformal(n, 0);
   for (int i = 0; i < n; ++i) conformal[i] = bx1[i] >= bx0[i];
+  // subset evolution keeps the excluded pixels of conformal subsets with
+  // excluded shapes in their lists (the reference's static tracking
+  // objectives carry them, inactive, from frame to frame)
+  const bool evolution = c->params.use_subset_evolution && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE;
+  bool any_evo = false;
+  if (evolution)
+    for (int k = 0; k < n_shapes; ++k) {
+      const dicegpu_shape& s = grouped[k];
+      if (s.role == DICEGPU_ROLE_EXCLUDED && conformal[s.subset]) {
+        desc[(size_t)s.subset * DG_MASK_DESC + DG_DESC_EVOLVE] = 1;
+        any_evo = true;
+      }
+    }
   cudaStreamSynchronize(c->stream);
   const size_t nv = (size_t)std::max<int64_t>(n_vertices, 1);
   int rc;
@@ -892,8 +920,13 @@ extern "C" int dicegpu_set_subset_shapes(dicegpu_ctx* c, int n_shapes, const dic
   int32_t* d_counts = nullptr;
   if (cudaMalloc(&d_counts, n * sizeof(int32_t)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
   std::vector<int32_t> counts(n), offsets(n + 1, 0);
+  if (any_evo && ((rc = c->d_evo_nact0.ensure(n)) || (rc = c->d_evo_nact.ensure(n)))) {
+    cudaFree(d_counts);
+    return rc;
+  }
   RasterArgs ra{c->d_shapes.p, c->d_shape_off.p, c->d_svx.p, c->d_svy.p, n, d_counts, nullptr, nullptr, nullptr,
-                c->d_fields, c->params.subset_size >= 1 ? c->params.subset_size / 2 : -1};
+                c->d_fields, c->params.subset_size >= 1 ? c->params.subset_size / 2 : -1,
+                any_evo ? 1 : 0, nullptr, any_evo ? c->d_evo_nact0.p : nullptr};
   const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)n * 32 + 255) / 256, (int64_t)c->num_sms * 8);
   cudaError_t e = cudaMemcpy(c->d_shapes.p, grouped.data(), n_shapes * sizeof(dicegpu_shape), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_shape_off.p, shape_off.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
@@ -924,22 +957,41 @@ extern "C" int dicegpu_set_subset_shapes(dicegpu_ctx* c, int n_shapes, const dic
   if ((rc = grow(&c->d_px, &c->list_cap, total)) || (rc = grow(&c->d_py, &cap2, total))) return rc;
   c->list_cap = std::min(c->list_cap, cap2);
   CK(cudaMemcpy(c->d_offsets, offsets.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (any_evo) {
+    const size_t t1 = std::max<size_t>(total, 1);
+    if ((rc = c->d_pix_flag0.ensure(t1)) || (rc = c->d_pix_flag.ensure(t1)) || (rc = c->d_pix_f.ensure(t1)))
+      return rc;
+  }
   ra.offsets = c->d_offsets;
   ra.px = c->d_px;
   ra.py = c->d_py;
+  ra.active = nullptr;
+  ra.flags = any_evo ? c->d_pix_flag0.p : nullptr;
   raster_kernel<true><<<blocks, 256, 0, c->stream>>>(ra);
   ++c->launches;
   CK(cudaGetLastError());
   // obstruction bitmaps
   clear_shapes(c);
+  if (!obst_list.empty() || any_evo) {
+    if ((rc = c->d_mask_desc.ensure(desc.size()))) return rc;
+    CK(cudaMemcpyAsync(c->d_mask_desc.p, desc.data(), desc.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       c->stream));
+    c->use_masks = true;
+  }
+  if (any_evo) {
+    // the evolution state of a fresh sequence
+    c->evo_total = std::max<size_t>(total, 1);
+    CK(cudaMemcpyAsync(c->d_pix_flag.p, c->d_pix_flag0.p, c->evo_total, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemsetAsync(c->d_pix_f.p, 0, c->evo_total * sizeof(float), c->stream));
+    CK(cudaMemcpyAsync(c->d_evo_nact.p, c->d_evo_nact0.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                       c->stream));
+    c->has_evo = true;
+  }
   if (!obst_list.empty()) {
-    if ((rc = c->d_mask_bits.ensure((size_t)obst_words)) || (rc = c->d_mask_desc.ensure(desc.size()))) return rc;
+    if ((rc = c->d_mask_bits.ensure((size_t)obst_words))) return rc;
     int32_t* d_list = nullptr;
     if (cudaMalloc(&d_list, obst_list.size() * sizeof(int32_t)) != cudaSuccess) return DICEGPU_ERR_NOMEM;
     e = cudaMemsetAsync(c->d_mask_bits.p, 0, (size_t)obst_words * sizeof(uint32_t), c->stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c->d_mask_desc.p, desc.data(), desc.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
-                          c->stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(d_list, obst_list.data(), obst_list.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                           c->stream);
@@ -985,8 +1037,8 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
       bool any = false;
       for (int i = 0; i < n; ++i) {
         int32_t* d = &c->h_mask_desc[(size_t)i * DG_MASK_DESC];
-        d[5] = d[6] = d[7] = d[8] = d[9] = 0;
-        any = any || d[2] > 0;
+        d[5] = d[6] = 0;
+        any = any || d[2] > 0 || d[DG_DESC_EVOLVE] != 0;
       }
       // the device descriptors exist once an obstruction or a tracking frame needed them
       if (c->d_mask_desc.p && c->d_mask_desc.cap >= c->h_mask_desc.size())
@@ -1089,7 +1141,7 @@ static int ensure_blocking_desc(dicegpu_ctx* c) {
   if ((rc = c->d_mask_desc.ensure(c->h_mask_desc.size()))) return rc;
   for (int i = 0; i < c->n; ++i) {
     int32_t* d = &c->h_mask_desc[(size_t)i * DG_MASK_DESC];
-    d[5] = d[6] = d[7] = d[8] = d[9] = 0;
+    d[5] = d[6] = 0;
   }
   CK(cudaMemcpy(c->d_mask_desc.p, c->h_mask_desc.data(), c->h_mask_desc.size() * sizeof(int32_t),
                 cudaMemcpyHostToDevice));
@@ -1198,6 +1250,18 @@ extern "C" int dicegpu_get_subset_pixels(dicegpu_ctx* c, int32_t* offsets, int32
   return DICEGPU_OK;
 }
 
+extern "C" int dicegpu_get_subset_pixel_state(dicegpu_ctx* c, uint8_t* state, float* ref_values) {
+  if (!c || (!state && !ref_values)) return DICEGPU_ERR_ARG;
+  if (!c->has_evo) return DICEGPU_ERR_STATE;
+  CK(cudaStreamSynchronize(c->stream));
+  int32_t last = 0;
+  CK(cudaMemcpy(&last, c->d_offsets + c->n, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (last > 0 && state) CK(cudaMemcpy(state, c->d_pix_flag.p, (size_t)last, cudaMemcpyDeviceToHost));
+  if (last > 0 && ref_values)
+    CK(cudaMemcpy(ref_values, c->d_pix_f.p, (size_t)last * sizeof(float), cudaMemcpyDeviceToHost));
+  return DICEGPU_OK;
+}
+
 extern "C" int dicegpu_set_force_simplex(dicegpu_ctx* c, int n, const uint8_t* flags) {
   if (!c) return DICEGPU_ERR_ARG;
   if (!flags) {
@@ -1288,6 +1352,14 @@ static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
   a.geo.blocked_poly = c->d_bpoly.p;
   a.geo.blocked_vx = c->d_dvx.p;
   a.geo.blocked_vy = c->d_dvy.p;
+  a.geo.pix_flag = c->has_evo ? c->d_pix_flag.p : nullptr;
+  a.geo.pix_f = c->has_evo ? c->d_pix_f.p : nullptr;
+  a.geo.evo_nact = c->has_evo ? c->d_evo_nact.p : nullptr;
+  // turned on from the third frame of a sequence (frame_id_ > first_frame_id_
+  // + frame_skip_, DICe_Schema.cpp:2357), in the tracking routine, whose
+  // objectives persist across frames (DICe_Schema.cpp:1729-1748)
+  a.evolve = c->has_evo && !c->evo_suspend && c->params.use_subset_evolution &&
+             c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE && c->frame_index >= 2;
   a.fields = c->d_fields;
   a.n = c->n;
   a.first_frame = c->frame_index == 0;
@@ -1321,6 +1393,16 @@ static int ready(dicegpu_ctx* c) {
   if (!c) return DICEGPU_ERR_ARG;
   if (!c->has_ref || !c->has_def || c->n < 1) return DICEGPU_ERR_STATE;
   if (!c->use_lists && c->params.subset_size < 1) return DICEGPU_ERR_ARG;
+  return DICEGPU_OK;
+}
+
+// The evolution state of a fresh sequence, restored at its first frame.
+static int evo_begin_frame(dicegpu_ctx* c) {
+  if (!c->has_evo || c->frame_index != 0) return DICEGPU_OK;
+  CK(cudaMemcpyAsync(c->d_pix_flag.p, c->d_pix_flag0.p, c->evo_total, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_pix_f.p, 0, c->evo_total * sizeof(float), c->stream));
+  CK(cudaMemcpyAsync(c->d_evo_nact.p, c->d_evo_nact0.p, (size_t)c->n * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                     c->stream));
   return DICEGPU_OK;
 }
 
@@ -1387,6 +1469,7 @@ extern "C" int dicegpu_execute_correlation(dicegpu_ctx* c) {
   int blocks;
   size_t smem;
   if ((rc = grid_for(c, fn, &blocks, &smem))) return rc;
+  if ((rc = evo_begin_frame(c))) return rc;
   if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE)
     return run_tracking_frame(c, fn, blocks, smem);
   FrameArgs a;
@@ -1406,6 +1489,7 @@ extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
     return DICEGPU_ERR_UNSUPPORTED;
   FrameKernelFn fn = frame_fn(c);
   if (!fn) return DICEGPU_ERR_UNSUPPORTED;
+  if ((rc = evo_begin_frame(c))) return rc;
   const size_t smem = warp_smem_bytes(c->dp.shape);
   FrameArgs a;
   fill_args(c, a, MODE_CORRELATE);
@@ -1536,6 +1620,7 @@ extern "C" int dicegpu_autotune(dicegpu_ctx* c, int* warps_per_cta, int* ctas_pe
       cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
     rc = DICEGPU_ERR_CUDA;
   const int frame0 = c->frame_index;
+  c->evo_suspend = true;
   const int cand[][2] = {{8, 0}, {4, 0}, {2, 0}, {8, 1}, {4, 2}, {4, 3}};
   TuneVal best{c->warps_per_cta, c->ctas_per_sm, 1e30f};
   for (const auto& cd : cand) {
@@ -1562,6 +1647,7 @@ extern "C" int dicegpu_autotune(dicegpu_ctx* c, int* warps_per_cta, int* ctas_pe
     rc = DICEGPU_ERR_CUDA;
   cudaStreamSynchronize(c->stream);
   c->frame_index = frame0;
+  c->evo_suspend = false;
   c->warps_per_cta = best.warps;
   c->ctas_per_sm = best.ctas;
   if (e0) cudaEventDestroy(e0);

@@ -189,6 +189,20 @@ class Schema:
                                                      py.ctypes.data_as(ctypes.c_void_p)), "get_subset_pixels")
         return offs, px[:offs[-1]], py[:offs[-1]]
 
+    def subset_pixel_state(self):
+        """(state, ref_values) of the list pixels under subset evolution:
+        state 0 inactive, 1 active, 2 turned on with reference intensity
+        ref_values (Subset::turn_on_previously_obstructed_pixels)."""
+        offs = np.zeros(self.n + 1, np.int32)
+        abi.check(self.lib.dicegpu_get_subset_pixels(self.ctx, offs.ctypes.data_as(ctypes.c_void_p), None, None),
+                  "get_subset_pixels")
+        state = np.zeros(max(int(offs[-1]), 1), np.uint8)
+        vals = np.zeros(max(int(offs[-1]), 1), np.float32)
+        abi.check(self.lib.dicegpu_get_subset_pixel_state(self.ctx, state.ctypes.data_as(ctypes.c_void_p),
+                                                          vals.ctypes.data_as(ctypes.c_void_p)),
+                  "get_subset_pixel_state")
+        return state[:offs[-1]], vals[:offs[-1]]
+
     def set_force_simplex(self, flags):
         if flags is None:
             abi.check(self.lib.dicegpu_set_force_simplex(self.ctx, 0, None), "set_force_simplex")

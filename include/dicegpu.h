@@ -194,7 +194,18 @@ typedef struct dicegpu_params {
    * are blocked (DICe_Schema.cpp:2160-2185); 1 leaves them to
    * params.optimization. */
   int32_t override_force_simplex;
-  int32_t reserved[1];
+  /* use_subset_evolution (0; tracking defaults 1): in the tracking routine,
+   * from the third frame of a sequence on, after a successful solve, a
+   * conformal subset's excluded pixels that are visible at the solved
+   * parameters take their deformed intensity as reference and join the
+   * subset for the rest of the sequence
+   * (Subset::turn_on_previously_obstructed_pixels, DICe_Subset.cpp:506-520;
+   * DICe_Schema.cpp:2354-2360; the generic routine rebuilds its objectives
+   * every frame, so evolution has no lasting effect there).  Excluded pixels
+   * then stay in the subsets' pixel lists as inactive.  Set it, and the
+   * routine, before dicegpu_set_subset_shapes; the state restarts with each
+   * sequence (frame index 0). */
+  int32_t use_subset_evolution;
 } dicegpu_params;
 
 /* Correlation_Routine */
@@ -204,10 +215,8 @@ typedef struct dicegpu_params {
 /* Fills *p with the reference defaults. Replaces dice_default_params. */
 int dicegpu_default_params(dicegpu_params* p);
 /* Fills *p with the reference's tracking defaults (tracking_default_params,
- * DICe_ParameterUtilities.cpp:297-345; use_tracking_default_params).  The
- * subset evolution those defaults switch on changes results only for subsets
- * with excluded shapes, whose pixels it brings back; it is not implemented,
- * and such subsets keep their excluded pixels off. */
+ * DICe_ParameterUtilities.cpp:297-345; use_tracking_default_params),
+ * subset evolution included. */
 int dicegpu_tracking_default_params(dicegpu_params* p);
 
 /* Number of shape-function parameters N for these params (2..6 affine, 12 quadratic). */
@@ -338,6 +347,14 @@ int dicegpu_vsg_strain(dicegpu_ctx* ctx, int window_size, double* out, int on_de
 /* Copies the context's subset pixel lists to host memory: offsets[n + 1]
  * and, when px / py are not NULL, offsets[n] coordinates each. */
 int dicegpu_get_subset_pixels(dicegpu_ctx* ctx, int32_t* offsets, int32_t* px, int32_t* py);
+/* Subset evolution state of the list pixels (use_subset_evolution in the
+ * tracking routine, with conformal subsets that have excluded shapes):
+ * state[offsets[n]] 0 inactive (excluded and not yet seen), 1 active, 2
+ * turned on (Subset::turn_on_previously_obstructed_pixels), and
+ * ref_values[offsets[n]] the reference intensities the turned-on pixels took
+ * (Subset::ref_intensities_).  Either pointer may be NULL.  DICEGPU_ERR_STATE
+ * when the lists carry no evolution state. */
+int dicegpu_get_subset_pixel_state(dicegpu_ctx* ctx, uint8_t* state, float* ref_values);
 /* Per-subset FORCE_SIMPLEX flags (DICe_Schema.cpp:2162-2165); NULL clears them. */
 int dicegpu_set_force_simplex(dicegpu_ctx* ctx, int n, const uint8_t* flags);
 

@@ -432,6 +432,10 @@ struct Subset {
   bool has_gradients = false;
   const PixelSet* obstructed = nullptr;   // obstructed_coords_
   const PixelSet* blocked = nullptr;      // pixels_blocked_by_other_subsets_
+  // subset evolution (turn_on_previously_obstructed_pixels): per pixel 1
+  // active, 0 inactive (excluded), 2 turned on with the stored intensity
+  uint8_t* flag = nullptr;
+  float* fstore = nullptr;
 
   // Subset(cx,cy,w,h) (:78-113): odd extent, negative coordinates clamped to 0.
   void init_square(int cx_, int cy_, int size) {
@@ -466,6 +470,11 @@ struct Subset {
   // initialize(ref_img) with no shape function (:385-389, :428-437)
   void init_ref(const Image& im) {
     for (int i = 0; i < npix; ++i) ref[i] = im.at(im.I, (long)y[i] * im.w + x[i]);
+    if (flag)
+      for (int i = 0; i < npix; ++i) {
+        active[i] = flag[i] != 0;
+        if (flag[i] == 2) ref[i] = fstore[i];
+      }
     if (im.has_gradients) {
       for (int i = 0; i < npix; ++i) {
         gx[i] = im.at(im.gx, (long)y[i] * im.w + x[i]);
@@ -1060,7 +1069,7 @@ static float objective_beta(const Ctx& C, Subset& s, const ShapeFn& sf_in) {
 
 // Schema::generic_correlation_routine (DICe_Schema.cpp:2026-2368) for one subset,
 // restricted to the USE_FIELD_VALUES initializer and local DIC.
-static void correlate_subset(const Ctx& C, Subset& s, double* f, bool first_frame,
+static bool correlate_subset(const Ctx& C, Subset& s, double* f, bool first_frame,
                              bool force_simplex, Counters* cnt) {
   const dicegpu_params& P = C.P;
   if (P.subset_size > 0 && first_frame) {
@@ -1069,7 +1078,7 @@ static void correlate_subset(const Ctx& C, Subset& s, double* f, bool first_fram
     const int hs = P.subset_size / 2;
     if (cur_x < hs || cur_x > C.def.w - hs || cur_y < hs || cur_y > C.def.h - hs) {
       record_failed_step(f, DICEGPU_INITIALIZE_FAILED_BY_EXCEPTION, -1);
-      return;
+      return false;
     }
   }
   int num_iterations = -1;
@@ -1078,13 +1087,13 @@ static void correlate_subset(const Ctx& C, Subset& s, double* f, bool first_fram
   int init_status = initial_guess(f, sf);
   if (init_status == DICEGPU_INITIALIZE_FAILED) {
     record_failed_step(f, init_status, num_iterations);
-    return;
+    return false;
   }
   if (P.initial_gamma_threshold != -1.0) {
     const float g0 = objective_gamma(C, s, sf, cnt);
     if (g0 > P.initial_gamma_threshold || g0 < 0.0f) {
       record_failed_step(f, DICEGPU_INITIALIZE_FAILED, num_iterations);
-      return;
+      return false;
     }
   }
   const float prev_u = (float)f[DICEGPU_F_DISP_X];
@@ -1124,7 +1133,7 @@ static void correlate_subset(const Ctx& C, Subset& s, double* f, bool first_fram
     if (second_failed && corr_status != DICEGPU_CORRELATION_SUCCESSFUL) {
       if (cond_set) f[DICEGPU_F_CONDITION] = cond;
       record_failed_step(f, corr_status, num_iterations);
-      return;
+      return false;
     }
   }
   if (cond_set) f[DICEGPU_F_CONDITION] = cond;
@@ -1132,19 +1141,19 @@ static void correlate_subset(const Ctx& C, Subset& s, double* f, bool first_fram
   const float sigma = objective_sigma(C, s, sf, noise);
   if (sigma < 0.0f) {
     record_failed_step(f, DICEGPU_FRAME_FAILED_DUE_TO_NEGATIVE_SIGMA, num_iterations);
-    return;
+    return false;
   }
   const float gamma = objective_gamma(C, s, sf, cnt);
   const float beta = P.output_beta ? objective_beta(C, s, sf) : 0.0f;
   if ((P.final_gamma_threshold != -1.0 && gamma > P.final_gamma_threshold) || gamma < 0.0f) {
     record_failed_step(f, DICEGPU_FRAME_FAILED_DUE_TO_HIGH_GAMMA, num_iterations);
-    return;
+    return false;
   }
   sf.map_to_u_v_theta(fcx, fcy, nu, nv, nt);
   if (std::abs(nu - prev_u) > P.disp_jump_tol || std::abs(nv - prev_v) > P.disp_jump_tol ||
       std::abs(nt - prev_t) > P.theta_jump_tol) {
     record_failed_step(f, DICEGPU_JUMP_TOLERANCE_EXCEEDED, num_iterations);
-    return;
+    return false;
   }
   const float contrast = s.contrast_std_dev();
   const int active_pixels = s.num_active();
@@ -1159,6 +1168,7 @@ static void correlate_subset(const Ctx& C, Subset& s, double* f, bool first_fram
   f[DICEGPU_F_ACTIVE_PIXELS] = active_pixels;
   f[DICEGPU_F_STATUS] = init_status;
   f[DICEGPU_F_ITERATIONS] = num_iterations;
+  return true;
 }
 
 }  // namespace oracle
@@ -1251,6 +1261,9 @@ struct FrameJob {
   double* unc;
   const std::vector<PixelSet>* obst = nullptr;   // per subset
   const PixelSet* blocked = nullptr;             // the subset being run (tracking order)
+  uint8_t* pix_flag = nullptr;                   // subset evolution state per list pixel
+  float* pix_f = nullptr;
+  bool evolve = false;                           // turn on visible inactive pixels after success
 };
 
 void run_range(const FrameJob& J, int b, int e) {
@@ -1261,6 +1274,8 @@ void run_range(const FrameJob& J, int b, int e) {
     if (J.offsets) s.init_list(cx, cy, J.px + J.offsets[i], J.py + J.offsets[i],
                                J.offsets[i + 1] - J.offsets[i]);
     else s.init_square(cx, cy, J.C.P.subset_size);
+    s.flag = J.pix_flag ? J.pix_flag + J.offsets[i] : nullptr;
+    s.fstore = J.pix_f ? J.pix_f + J.offsets[i] : nullptr;
     s.init_ref(J.C.ref);
     s.obstructed = J.obst ? &(*J.obst)[i] : nullptr;
     s.blocked = J.blocked;
@@ -1270,7 +1285,15 @@ void run_range(const FrameJob& J, int b, int e) {
       cnt.ucx = (float)f[DICEGPU_F_COORD_X];
       cnt.ucy = (float)f[DICEGPU_F_COORD_Y];
     }
-    correlate_subset(J.C, s, f, J.first_frame, J.force_simplex && J.force_simplex[i], &cnt);
+    const bool ok = correlate_subset(J.C, s, f, J.first_frame, J.force_simplex && J.force_simplex[i], &cnt);
+    // Subset::turn_on_previously_obstructed_pixels (DICe_Subset.cpp:506-520)
+    // with the deformed state of the last evaluation
+    if (ok && J.evolve && s.flag)
+      for (int k = 0; k < s.npix; ++k)
+        if (!s.active[k] && !s.deact[k]) {
+          s.fstore[k] = s.def[k];
+          s.flag[k] = 2;
+        }
     if (J.gn_out) J.gn_out[i] = cnt.gn_iters;
     if (J.sx_out) J.sx_out[i] = cnt.simplex_evals;
   }
@@ -1520,12 +1543,15 @@ static void deformed_pixels(const dicegpu_shape& s, const int32_t* vx, const int
 
 // one subset's pixel list: the union of its boundary shapes in (y, x) order
 // without the excluded pixels (tested at the clamped coordinates), or the
-// square of `square_size` about its centroid when it has no boundary shape
+// square of `square_size` about its centroid when it has no boundary shape.
+// With flags, the excluded pixels stay in the list with flag 0 (inactive),
+// the others get flag 1.
 static void subset_pixels(const std::vector<int>& mine, const dicegpu_shape* shapes, const int32_t* vx,
                           const int32_t* vy, int cx, int cy, int square_size, std::vector<int32_t>& px,
-                          std::vector<int32_t>& py) {
+                          std::vector<int32_t>& py, std::vector<uint8_t>* flags = nullptr) {
   px.clear();
   py.clear();
+  if (flags) flags->clear();
   int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
   bool any = false;
   for (int k : mine) {
@@ -1539,7 +1565,11 @@ static void subset_pixels(const std::vector<int>& mine, const dicegpu_shape* sha
     if (square_size < 1) return;
     const int hw = square_size / 2;
     for (int y = cy - hw; y <= cy + hw; ++y)
-      for (int x = cx - hw; x <= cx + hw; ++x) { px.push_back(x < 0 ? 0 : x); py.push_back(y < 0 ? 0 : y); }
+      for (int x = cx - hw; x <= cx + hw; ++x) {
+        px.push_back(x < 0 ? 0 : x);
+        py.push_back(y < 0 ? 0 : y);
+        if (flags) flags->push_back(1);
+      }
     return;
   }
   for (int y = y0; y <= y1; ++y)
@@ -1550,7 +1580,11 @@ static void subset_pixels(const std::vector<int>& mine, const dicegpu_shape* sha
         if (shapes[k].role == DICEGPU_ROLE_BOUNDARY) in = in || shape_has(shapes[k], vx, vy, x, y, false);
         else if (shapes[k].role == DICEGPU_ROLE_EXCLUDED) out = out || shape_has(shapes[k], vx, vy, ex, ey, true);
       }
-      if (in && !out) { px.push_back(ex); py.push_back(ey); }
+      if (in && (!out || flags)) {
+        px.push_back(ex);
+        py.push_back(ey);
+        if (flags) flags->push_back(out ? 0 : 1);
+      }
     }
 }
 
@@ -1601,20 +1635,27 @@ extern "C" int oracle_execute_frame_shapes(const dicegpu_params* params, int w, 
                                            const dicegpu_shape* shapes, const int32_t* vx,
                                            const int32_t* vy, const int32_t* block_offsets,
                                            const int32_t* block_ids, const uint8_t* force_simplex,
-                                           int first_frame, int nthreads) {
+                                           int first_frame, int nthreads, uint8_t* pix_flag, float* pix_f,
+                                           int frame_index) {
   if (!params || !fields || n < 1) return DICEGPU_ERR_ARG;
   std::vector<std::vector<int>> by;
   if (!group_shapes(n, n_shapes, shapes, by)) return DICEGPU_ERR_ARG;
+  // the tracking routine's objectives persist across frames and carry the
+  // evolved subsets (DICe_Schema.cpp:1729-1748); the generic routine's are
+  // rebuilt every frame (:1708-1724)
+  const bool evolution = params->use_subset_evolution != 0 && params->correlation_routine == DICEGPU_TRACKING_ROUTINE;
   // pixel lists and obstruction sets
   std::vector<int32_t> offsets(n + 1, 0), px, py, lx, ly;
+  std::vector<uint8_t> flags, lf;
   std::vector<PixelSet> obst(n);
   std::vector<char> conformal(n, 0);
   for (int i = 0; i < n; ++i) {
     const double* f = fields + (long)i * DICEGPU_FIELD_STRIDE;
     subset_pixels(by[i], shapes, vx, vy, (int)f[DICEGPU_F_COORD_X], (int)f[DICEGPU_F_COORD_Y],
-                  params->subset_size, lx, ly);
+                  params->subset_size, lx, ly, evolution ? &lf : nullptr);
     px.insert(px.end(), lx.begin(), lx.end());
     py.insert(py.end(), ly.begin(), ly.end());
+    flags.insert(flags.end(), lf.begin(), lf.end());
     offsets[i + 1] = offsets[i] + (int32_t)lx.size();
     for (int k : by[i]) {
       if (shapes[k].role == DICEGPU_ROLE_OBSTRUCTED) owned_pixels(shapes[k], vx, vy, obst[i]);
@@ -1640,6 +1681,24 @@ extern "C" int oracle_execute_frame_shapes(const dicegpu_params* params, int w, 
   J.force_simplex = force.data(); J.first_frame = first_frame != 0;
   J.gn_out = nullptr; J.sx_out = nullptr; J.unc = nullptr;
   J.obst = &obst;
+  // subset evolution: the caller's state (initialised at the sequence's first frame)
+  std::vector<float> fstore;
+  if (evolution) {
+    if (pix_flag && pix_f) {
+      if (frame_index == 0) {
+        std::copy(flags.begin(), flags.end(), pix_flag);
+        std::fill(pix_f, pix_f + flags.size(), 0.0f);
+      }
+      J.pix_flag = pix_flag;
+      J.pix_f = pix_f;
+    } else {
+      fstore.assign(flags.size(), 0.0f);
+      J.pix_flag = flags.data();
+      J.pix_f = fstore.data();
+    }
+    // turned on from the third frame (frame_id_ > first_frame_id_ + frame_skip_)
+    J.evolve = frame_index >= 2;
+  }
   const bool tracking = params->correlation_routine == DICEGPU_TRACKING_ROUTINE && any_block;
   if (!tracking) {
     run_parallel(J, nthreads);

@@ -84,7 +84,8 @@ int oracle_execute_frame_shapes(const dicegpu_params* params, int w, int h, cons
                                 const float* def, int n, double* fields, int n_shapes,
                                 const dicegpu_shape* shapes, const int32_t* vx, const int32_t* vy,
                                 const int32_t* block_offsets, const int32_t* block_ids,
-                                const uint8_t* force_simplex, int first_frame, int nthreads);
+                                const uint8_t* force_simplex, int first_frame, int nthreads,
+                                uint8_t* pix_flag, float* pix_f, int frame_index);
 
 /* VSG_Strain_Post_Processor on n field rows (window > 0: radius window/2):
  * out n x 7 (strain xx, yy, xy, du/dx, du/dy, dv/dx, dv/dy), failed n flags. */

@@ -9,7 +9,7 @@ import os
 
 import numpy as np
 
-from dice_b200.abi import Params, FIELD_STRIDE, UNCERTAINTY_STRIDE, shape_array
+from dice_b200.abi import Params, FIELD_STRIDE, UNCERTAINTY_STRIDE, TRACKING_ROUTINE, shape_array
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdiceoracle.so")
@@ -64,7 +64,8 @@ def lib():
         L.oracle_rasterize.restype = ci
         L.oracle_rasterize.argtypes = [ci, ci, vp, vp, vp, vp, ci, vp, vp, vp]
         L.oracle_execute_frame_shapes.restype = ci
-        L.oracle_execute_frame_shapes.argtypes = [P, ci, ci, vp, vp, ci, vp, ci, vp, vp, vp, vp, vp, vp, ci, ci]
+        L.oracle_execute_frame_shapes.argtypes = [P, ci, ci, vp, vp, ci, vp, ci, vp, vp, vp, vp, vp, vp, ci, ci,
+                                                  vp, vp, ci]
         L.oracle_vsg_strain.restype = ci
         L.oracle_vsg_strain.argtypes = [ci, vp, ci, vp, vp]
         _lib = L
@@ -139,9 +140,12 @@ def rasterize(n, shapes, vx=None, vy=None, fields=None, square_size=0):
 
 
 def execute_frame_shapes(params, ref, deff, fields, shapes, vx=None, vy=None, block_offsets=None,
-                         block_ids=None, force_simplex=None, first_frame=True, nthreads=1):
+                         block_ids=None, force_simplex=None, first_frame=True, nthreads=1, evolution=None,
+                         frame_index=0):
     """Schema::execute_correlation over subsets defined by shapes with
-    obstructions and blocking subsets; updates `fields` in place."""
+    obstructions and blocking subsets; updates `fields` in place.  With
+    params.use_subset_evolution, `evolution` is a dict carried across the
+    frames of a sequence (the per-pixel state) and frame_index counts them."""
     ref = np.ascontiguousarray(ref, dtype=np.float32)
     deff = np.ascontiguousarray(deff, dtype=np.float32)
     assert fields.dtype == np.float64 and fields.flags.c_contiguous
@@ -153,9 +157,20 @@ def execute_frame_shapes(params, ref, deff, fields, shapes, vx=None, vy=None, bl
     bo = None if block_offsets is None else np.ascontiguousarray(block_offsets, dtype=np.int32)
     bi = None if block_ids is None else np.ascontiguousarray(block_ids if len(block_ids) else [0], dtype=np.int32)
     fs = None if force_simplex is None else np.ascontiguousarray(force_simplex, dtype=np.uint8)
+    pf = pv = None
+    if evolution is not None and params.use_subset_evolution and params.correlation_routine == TRACKING_ROUTINE:
+        if "flag" not in evolution:
+            total = int(rasterize(n, shapes, vx, vy, fields, params.subset_size)[0][-1])
+            # the lists keep the excluded pixels: size them from the boundaries alone
+            bounds = [sh for sh in shapes if sh.role == 0]
+            total = int(rasterize(n, bounds, vx, vy, fields, params.subset_size)[0][-1]) if bounds else total
+            evolution["flag"] = np.zeros(max(total, 1), np.uint8)
+            evolution["f"] = np.zeros(max(total, 1), np.float32)
+        pf, pv = evolution["flag"], evolution["f"]
     rc = lib().oracle_execute_frame_shapes(ctypes.byref(params), w, h, _ptr(ref), _ptr(deff), n, _ptr(fields),
                                            len(arr), ctypes.cast(arr, ctypes.c_void_p), _ptr(x), _ptr(y),
-                                           _ptr(bo), _ptr(bi), _ptr(fs), int(first_frame), nthreads)
+                                           _ptr(bo), _ptr(bi), _ptr(fs), int(first_frame), nthreads, _ptr(pf),
+                                           _ptr(pv), int(frame_index))
     if rc != 0:
         raise RuntimeError("oracle_execute_frame_shapes: %d" % rc)
     return fields

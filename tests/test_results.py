@@ -5,8 +5,11 @@ The regression gold files of conformal_subset_def (five subsets, two
 conformal, one obstructed and blocked) and simple_obstruction (37 frames of a
 subset sliding under an obstruction) are checked the way the reference's
 harness checks them: results written in its format, compared with
-DICe_Diff -t 0.05 -f 5.0E-5 (tests/regression/CMakeLists.txt).  The oracle
-runs them here; the GPU runs them in test_masks.py.
+DICe_Diff -t 0.05 -f 5.0E-5 (tests/regression/CMakeLists.txt).  The
+examples/obstruction run (tracking defaults with subset evolution) is checked
+with the examples' own comparison, DICe_Diff -t 10.0 -f 1E-4
+(tests/examples/CMakeLists.txt).  The oracle runs them here; the GPU runs
+them in test_masks.py.
 """
 import os
 import subprocess
@@ -24,6 +27,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLD = np.load(os.path.join(ROOT, "tests", "golden", "reference_gold.npz"))
 DIFF_BIN = os.path.join(ROOT, "dice_b200", "bin", "dicegpu_diff")
 REGRESSION_TOL, REGRESSION_FLOOR = 0.05, 5.0e-5
+# "very loose tolerances for the examples (these are not regression tests)"
+EXAMPLE_TOL, EXAMPLE_FLOOR = 10.0, 1.0e-4
 
 
 def _row(**cols):
@@ -138,6 +143,54 @@ def simple_obstruction_case():
     return sf, p, GOLD["simple_obstruction_frames"], out
 
 
+def obstruction_example_case():
+    """examples/obstruction: a conformal subset (polygon boundary, an excluded
+    and an obstructed rectangle) rotating 2 degrees per frame about (100, 100)
+    behind a static bar, blocked by a 17 x 17 subset; params.xml sets the
+    tracking defaults (subset evolution on), bilinear interpolation, simplex
+    and disp_jump_tol 5.  Its gold rows FRAME r = 1..11 are the images
+    obstruction_{r+1} against obstruction_01 (subset 1 reproduces them to the
+    printed digits)."""
+    sf = SubsetFile(text=str(GOLD["subset_file_obstruction_example"]), width=200, height=200)
+    p = abi.tracking_default_params(subset_size=-1, use_def_gradients=0, interpolation=abi.BILINEAR,
+                                    disp_jump_tol=5.0)
+    out = Output(p, fields=["COORDINATE_X", "COORDINATE_Y", "ROTATION_Z", "SIGMA", "GAMMA"], delimiter=",",
+                 ref_image="./images/obstruction_01.tif", def_image="./images/obstruction_01.tif")
+    return sf, p, GOLD["obstruction_example_frames"].astype(np.float32), out
+
+
+def oracle_obstruction_example(p, sf, frames):
+    """The oracle over the example's frames: field rows and evolution state
+    (state, reference values) after each frame."""
+    f = syn.init_fields(sf.coordinates[:, 0], sf.coordinates[:, 1])
+    offs, ids = blocking_csr(sf)
+    evo, rows, states = {}, [], []
+    for k in range(1, len(frames)):
+        O.execute_frame_shapes(p, frames[0], frames[k], f, sf.shapes, sf.vx, sf.vy, offs, ids,
+                               force_simplex=sf.force_simplex, first_frame=(k == 1), evolution=evo,
+                               frame_index=k - 1)
+        rows.append(f.copy())
+        if evo:
+            states.append((evo["flag"].copy(), evo["f"].copy()))
+    return rows, states
+
+
+def check_example_files(tmp_path, out, rows):
+    """Per-subset files (separate_output_file_for_each_subset) against the
+    example's gold: (failed lines at the example tolerance, at the
+    regression tolerance) per subset."""
+    for k, f in enumerate(rows):
+        out.write_frame(tmp_path, "DICe_solution", k + 1, f, first_frame=1, num_frames=len(rows),
+                        separate_files=True)
+    res = []
+    for i in range(2):
+        text = str(GOLD["obstruction_example_gold_text_%d" % i])
+        got = open(tmp_path / ("DICe_solution_%d.txt" % i)).read()
+        res.append((diff_text(text, got, tol=EXAMPLE_TOL, floor=EXAMPLE_FLOOR)[0],
+                    diff_text(text, got, tol=REGRESSION_TOL, floor=REGRESSION_FLOOR)[0]))
+    return res
+
+
 def blocking_csr(sf):
     offs = np.zeros(len(sf.blocking) + 1, np.int32)
     ids = []
@@ -184,3 +237,42 @@ def test_oracle_simple_obstruction_gold(tmp_path):
     check_against_gold(tmp_path, out, rows, [str(GOLD["simple_obstruction_gold_text"])])
     # the subset slides under the obstruction: its active pixels shrink
     assert active[0] == 75 * 29 and active[-1] < 200 and np.all(np.diff(active) <= 0)
+
+
+def test_oracle_obstruction_example_with_subset_evolution(tmp_path):
+    sf, p, frames, out = obstruction_example_case()
+    assert p.use_subset_evolution == 1 and p.correlation_routine == abi.TRACKING_ROUTINE
+    rows, states = oracle_obstruction_example(p, sf, frames)
+    res = check_example_files(tmp_path, out, rows)
+    # both files pass the example's comparison; the blocking subset (no
+    # excluded pixels, Gauss-Newton-free 17 x 17 square) matches its gold at
+    # the regression tolerance too
+    assert res[0][0] == 0 and res[1] == (0, 0), res
+    # the first two frames turn nothing on (frame_id_ > first_frame_id_ +
+    # frame_skip_); the excluded pixels that rotate out from under the bar do
+    # later, with image intensities as their references
+    # (36 of the subset's 4430 pixels are excluded)
+    flag0 = states[0][0]
+    assert (flag0 == 0).sum() == 36 and not (states[0][0] == 2).any() and not (states[1][0] == 2).any()
+    on = [(st == 2).sum() for st, _ in states]
+    assert on[-1] >= 5 and all(b >= a for a, b in zip(on, on[1:]))
+    last_state, last_f = states[-1]
+    assert np.all((last_f[last_state == 2] >= 0) & (last_f[last_state == 2] <= 255))
+    assert (last_f[last_state != 2] == 0).all()
+    # the turned-on pixels join the count of active pixels
+    n0 = sf.coordinates.shape[0]
+    assert n0 == 2 and rows[-1][1, abi.F_ACTIVE_PIXELS] == 289
+
+
+def test_oracle_subset_evolution_is_frame_local_in_generic_routine():
+    """The generic routine rebuilds its objectives every frame
+    (DICe_Schema.cpp:1708-1724): evolution leaves no state behind."""
+    sf, p, frames, _ = obstruction_example_case()
+    p.correlation_routine = abi.GENERIC_ROUTINE
+    sub = frames[:5]
+    rows_on, states = oracle_obstruction_example(p, sf, sub)
+    p.use_subset_evolution = 0
+    rows_off, _ = oracle_obstruction_example(p, sf, sub)
+    assert not states
+    for a, b in zip(rows_on, rows_off):
+        assert np.array_equal(a, b)
