@@ -112,6 +112,8 @@ class Params(ctypes.Structure):
         ("obstruction_skin_factor", ctypes.c_double),
         ("override_force_simplex", ctypes.c_int32),
         ("use_subset_evolution", ctypes.c_int32),
+        ("use_incremental_formulation", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
     def copy(self):
@@ -216,6 +218,7 @@ def _declare(lib):
         "dicegpu_set_subset_shapes": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "dicegpu_get_subset_pixels": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
         "dicegpu_get_subset_pixel_state": (c_int, [c_void_p, c_void_p, c_void_p]),
+        "dicegpu_set_ref_from_def": (c_int, [c_void_p]),
         "dicegpu_set_blocking": (c_int, [c_void_p, c_void_p, c_void_p]),
         "dicegpu_get_params": (c_int, [c_void_p, P]),
         "dicegpu_subset_file_read": (c_int, [ctypes.c_char_p, c_int, c_int, ctypes.POINTER(c_void_p),

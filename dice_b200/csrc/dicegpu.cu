@@ -134,6 +134,32 @@ gauss_filter_kernel(int w, int h, int M, const GaussWeights wt, const float* __r
   out[o] = v;
 }
 
+// Incremental formulation (DICe_Schema.cpp:1671-1675, 1775-1789): a frame
+// after the first starts with DISPLACEMENT_X / _Y at 0 and ends with them
+// set to the accumulated displacement.
+__global__ void incr_begin_kernel(double* __restrict__ fields, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  fields[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_DISP_X] = 0.0;
+  fields[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_DISP_Y] = 0.0;
+}
+__global__ void incr_end_kernel(double* __restrict__ fields, double* __restrict__ acc, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* f = fields + (size_t)i * DICEGPU_FIELD_STRIDE;
+  acc[2 * i] += f[DICEGPU_F_DISP_X];
+  acc[2 * i + 1] += f[DICEGPU_F_DISP_Y];
+  f[DICEGPU_F_DISP_X] = acc[2 * i];
+  f[DICEGPU_F_DISP_Y] = acc[2 * i + 1];
+}
+// The tracking routine re-reads every reference intensity from the new
+// reference each incremental frame (DICe_Schema.cpp:1757-1759): turned-on
+// pixels keep is_active and lose their stored intensity.
+__global__ void evo_rebase_kernel(uint8_t* __restrict__ state, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && state[i] == 2) state[i] = 1;
+}
+
 // (I, Gx, Gy) -> interleaved float4 (the layout the frame kernel gathers from)
 __global__ void pack_kernel(size_t n, const float* __restrict__ I, const float* __restrict__ gx,
                             const float* __restrict__ gy, float4* __restrict__ out) {
@@ -294,6 +320,10 @@ struct dicegpu_ctx {
   DevBuf<uint8_t> d_pix_flag, d_pix_flag0;
   DevBuf<float> d_pix_f;
   DevBuf<int32_t> d_evo_nact, d_evo_nact0;
+  // incremental formulation: accumulated DISPLACEMENT_X / _Y per subset, and
+  // the reference planes a captured sequence restarts from
+  DevBuf<double> d_acc;
+  DevBuf<float> d_ref_saved;
   bool blocking_desc_ready = false;   // descriptors on the device for the tracking waves
   // blocking subsets and the tracking waves
   bool has_blocking = false;
@@ -479,7 +509,7 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   c->d_shapes.release(); c->d_shape_off.release(); c->d_svx.release(); c->d_svy.release();
   c->d_conformal.release(); c->d_mask_desc.release(); c->d_mask_bits.release();
   c->d_pix_flag.release(); c->d_pix_flag0.release(); c->d_pix_f.release();
-  c->d_evo_nact.release(); c->d_evo_nact0.release();
+  c->d_evo_nact.release(); c->d_evo_nact0.release(); c->d_acc.release(); c->d_ref_saved.release();
   c->d_blk_off.release(); c->d_blk_ids.release(); c->d_wave.release();
   c->d_dp_off.release(); c->d_bpoly.release();
   c->d_bwave.release(); c->d_dv_off.release(); c->d_dvx.release(); c->d_dvy.release();
@@ -716,6 +746,14 @@ extern "C" int dicegpu_set_ref_image_typed(dicegpu_ctx* c, int w, int h, const v
 extern "C" int dicegpu_set_def_image_typed(dicegpu_ctx* c, int w, int h, const void* pixels, int pixel_type,
                                            int on_device) {
   return set_def(c, w, h, pixels, pixel_type, on_device);
+}
+
+extern "C" int dicegpu_set_ref_from_def(dicegpu_ctx* c) {
+  if (!c) return DICEGPU_ERR_ARG;
+  if (!c->has_ref || !c->has_def) return DICEGPU_ERR_STATE;
+  CK(cudaMemcpyAsync(c->d_ref, c->d_def, (size_t)c->W * c->H * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+  return launch_gradients(c->W, c->H, c->d_ref, c->d_ref_gx, c->d_ref_gy, c->params.gradient_method, c->d_tmp,
+                          c->stream, &c->launches);
 }
 
 template <typename T>
@@ -1396,13 +1434,48 @@ static int ready(dicegpu_ctx* c) {
   return DICEGPU_OK;
 }
 
-// The evolution state of a fresh sequence, restored at its first frame.
-static int evo_begin_frame(dicegpu_ctx* c) {
-  if (!c->has_evo || c->frame_index != 0) return DICEGPU_OK;
-  CK(cudaMemcpyAsync(c->d_pix_flag.p, c->d_pix_flag0.p, c->evo_total, cudaMemcpyDeviceToDevice, c->stream));
-  CK(cudaMemsetAsync(c->d_pix_f.p, 0, c->evo_total * sizeof(float), c->stream));
-  CK(cudaMemcpyAsync(c->d_evo_nact.p, c->d_evo_nact0.p, (size_t)c->n * sizeof(int32_t), cudaMemcpyDeviceToDevice,
-                     c->stream));
+// Per-frame state around the correlation kernels: at the first frame of a
+// sequence the evolution state and the accumulated displacements restart;
+// later frames of an incremental sequence zero the displacements first.
+static int frame_begin(dicegpu_ctx* c) {
+  const int n = c->n;
+  const bool incr = c->params.use_incremental_formulation != 0;
+  if (c->frame_index == 0) {
+    if (c->has_evo) {
+      CK(cudaMemcpyAsync(c->d_pix_flag.p, c->d_pix_flag0.p, c->evo_total, cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemsetAsync(c->d_pix_f.p, 0, c->evo_total * sizeof(float), c->stream));
+      CK(cudaMemcpyAsync(c->d_evo_nact.p, c->d_evo_nact0.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                         c->stream));
+    }
+    if (incr) {
+      int rc = c->d_acc.ensure(2 * (size_t)n);
+      if (rc) return rc;
+      CK(cudaMemsetAsync(c->d_acc.p, 0, 2 * (size_t)n * sizeof(double), c->stream));
+    }
+    return DICEGPU_OK;
+  }
+  if (incr) {
+    if (!c->d_acc.p || c->d_acc.cap < 2 * (size_t)n) return DICEGPU_ERR_STATE;
+    incr_begin_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->d_fields, n);
+    CK(cudaGetLastError());
+    c->launches += 1;
+    if (c->has_evo && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE) {
+      evo_rebase_kernel<<<(unsigned)((c->evo_total + 255) / 256), 256, 0, c->stream>>>(c->d_pix_flag.p,
+                                                                                      c->evo_total);
+      CK(cudaGetLastError());
+      c->launches += 1;
+    }
+  }
+  return DICEGPU_OK;
+}
+
+static int frame_end(dicegpu_ctx* c) {
+  if (c->frame_index > 0 && c->params.use_incremental_formulation) {
+    incr_end_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_fields, c->d_acc.p, c->n);
+    CK(cudaGetLastError());
+    c->launches += 1;
+  }
+  c->frame_index += 1;
   return DICEGPU_OK;
 }
 
@@ -1458,7 +1531,6 @@ static int run_tracking_frame(dicegpu_ctx* c, FrameKernelFn fn, int blocks, size
     CK(cudaGetLastError());
     c->launches += 1;
   }
-  c->frame_index += 1;
   return DICEGPU_OK;
 }
 
@@ -1469,17 +1541,18 @@ extern "C" int dicegpu_execute_correlation(dicegpu_ctx* c) {
   int blocks;
   size_t smem;
   if ((rc = grid_for(c, fn, &blocks, &smem))) return rc;
-  if ((rc = evo_begin_frame(c))) return rc;
-  if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE)
-    return run_tracking_frame(c, fn, blocks, smem);
+  if ((rc = frame_begin(c))) return rc;
+  if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE) {
+    if ((rc = run_tracking_frame(c, fn, blocks, smem))) return rc;
+    return frame_end(c);
+  }
   FrameArgs a;
   fill_args(c, a, MODE_CORRELATE);
   CK(cudaMemsetAsync(c->d_counter, 0, (size_t)blocks * sizeof(int), c->stream));
   fn<<<blocks, c->warps_per_cta * 32, smem, c->stream>>>(a);
   CK(cudaGetLastError());
   c->launches += 1;
-  c->frame_index += 1;
-  return DICEGPU_OK;
+  return frame_end(c);
 }
 
 extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
@@ -1489,7 +1562,7 @@ extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
     return DICEGPU_ERR_UNSUPPORTED;
   FrameKernelFn fn = frame_fn(c);
   if (!fn) return DICEGPU_ERR_UNSUPPORTED;
-  if ((rc = evo_begin_frame(c))) return rc;
+  if ((rc = frame_begin(c))) return rc;
   const size_t smem = warp_smem_bytes(c->dp.shape);
   FrameArgs a;
   fill_args(c, a, MODE_CORRELATE);
@@ -1499,8 +1572,7 @@ extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
   }
   CK(cudaGetLastError());
   c->launches += c->n;
-  c->frame_index += 1;
-  return DICEGPU_OK;
+  return frame_end(c);
 }
 
 // ---------------------------------------------------------------------------
@@ -1519,6 +1591,16 @@ extern "C" int dicegpu_capture_sequence(dicegpu_ctx* c, int n, const float* cons
     if (rcb) return rcb;
   }
   CK(cudaStreamSynchronize(c->stream));
+  // an incremental sequence replays from the reference it was captured with
+  const bool incr = c->params.use_incremental_formulation != 0;
+  const size_t npx = (size_t)c->W * c->H;
+  if (incr && reset_fields) {
+    const int rcs = c->d_ref_saved.ensure(3 * npx);
+    if (rcs) return rcs;
+    CK(cudaMemcpy(c->d_ref_saved.p, c->d_ref, npx * sizeof(float), cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(c->d_ref_saved.p + npx, c->d_ref_gx, npx * sizeof(float), cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(c->d_ref_saved.p + 2 * npx, c->d_ref_gy, npx * sizeof(float), cudaMemcpyDeviceToDevice));
+  }
   if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
   if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
   // record on a private stream; every call below only enqueues work
@@ -1537,9 +1619,17 @@ extern "C" int dicegpu_capture_sequence(dicegpu_ctx* c, int n, const float* cons
                         cudaMemcpyDeviceToDevice, c->cap_stream) != cudaSuccess)
       rc = DICEGPU_ERR_CUDA;
     c->frame_index = 0;
+    if (incr && rc == DICEGPU_OK) {
+      float* planes[3] = {c->d_ref, c->d_ref_gx, c->d_ref_gy};
+      for (int q = 0; q < 3 && rc == DICEGPU_OK; ++q)
+        if (cudaMemcpyAsync(planes[q], c->d_ref_saved.p + q * npx, npx * sizeof(float), cudaMemcpyDeviceToDevice,
+                            c->cap_stream) != cudaSuccess)
+          rc = DICEGPU_ERR_CUDA;
+    }
   }
   for (int k = 0; k < n && rc == DICEGPU_OK; ++k) {
-    rc = dicegpu_set_def_image(c, c->W, c->H, frames[k], 1);
+    if (incr && c->frame_index > 0) rc = dicegpu_set_ref_from_def(c);
+    if (rc == DICEGPU_OK) rc = dicegpu_set_def_image(c, c->W, c->H, frames[k], 1);
     if (rc == DICEGPU_OK) rc = dicegpu_execute_correlation(c);
   }
   cudaGraph_t g = nullptr;

@@ -206,7 +206,7 @@ extern "C" int dicegpu_output_create(const dicegpu_params* params, const char* f
   o->step_x = info ? info->step_size_x : -1;
   o->step_y = info ? info->step_size_y : -1;
   o->strain_window = info ? info->strain_window : -1;
-  o->incremental = info ? info->incremental : 0;
+  o->incremental = (info && info->incremental) || params->use_incremental_formulation;
   o->sort_rows = info ? info->sort_rows : 0;
   o->init_method = info && info->initialization_method ? info->initialization_method : "USE_FIELD_VALUES";
   std::vector<std::string> names;

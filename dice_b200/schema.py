@@ -120,6 +120,11 @@ class Schema:
         if len(self._keep) > 4:
             self._keep = self._keep[-4:]
 
+    def set_ref_from_def(self):
+        """Incremental sequences: the current deformed image becomes the
+        reference (Schema::set_ref_image(prev_img()))."""
+        abi.check(self.lib.dicegpu_set_ref_from_def(self.ctx), "set_ref_from_def")
+
     # ---- subsets ----------------------------------------------------------------
     def set_fields(self, fields):
         f = np.ascontiguousarray(fields, dtype=np.float64)

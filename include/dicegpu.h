@@ -206,6 +206,17 @@ typedef struct dicegpu_params {
    * routine, before dicegpu_set_subset_shapes; the state restarts with each
    * sequence (frame index 0). */
   int32_t use_subset_evolution;
+  /* use_incremental_formulation (0): each frame after the first of a
+   * sequence correlates against the previous frame's deformed image
+   * (dicegpu_set_ref_from_def before the new deformed image, as DICe's main
+   * sets the reference to prev_img(), DICe_Main.cpp:326-328); the subsets'
+   * DISPLACEMENT_X / _Y start the frame at 0 and end it as the accumulated
+   * displacement (DICe_Schema.cpp:1671-1675, 1775-1789); the other
+   * parameters carry over.  The tracking routine re-reads the reference
+   * intensities from the new reference (:1757-1759), evolved pixels
+   * included. */
+  int32_t use_incremental_formulation;
+  int32_t reserved;
 } dicegpu_params;
 
 /* Correlation_Routine */
@@ -347,6 +358,11 @@ int dicegpu_vsg_strain(dicegpu_ctx* ctx, int window_size, double* out, int on_de
 /* Copies the context's subset pixel lists to host memory: offsets[n + 1]
  * and, when px / py are not NULL, offsets[n] coordinates each. */
 int dicegpu_get_subset_pixels(dicegpu_ctx* ctx, int32_t* offsets, int32_t* px, int32_t* py);
+/* Schema::post_execution_tasks + set_ref_image(prev_img()) of an
+ * incremental sequence: the current deformed image (filtered, if the
+ * params filter) becomes the reference and its gradients are computed;
+ * device copies only, so it can be captured with a sequence. */
+int dicegpu_set_ref_from_def(dicegpu_ctx* ctx);
 /* Subset evolution state of the list pixels (use_subset_evolution in the
  * tracking routine, with conformal subsets that have excluded shapes):
  * state[offsets[n]] 0 inactive (excluded and not yet seen), 1 active, 2

@@ -34,7 +34,7 @@ typedef struct dicegpu_output_info {
   int32_t step_size_x;       /* -1: not a regular grid */
   int32_t step_size_y;
   int32_t strain_window;     /* -1: N/A */
-  int32_t incremental;       /* use_incremental_formulation */
+  int32_t incremental;       /* use_incremental_formulation (also on when the params set it) */
   int32_t sort_rows;         /* sort_txt_output: per-frame files' rows by x, then y */
   const char* initialization_method;  /* reported initializer name; NULL: USE_FIELD_VALUES */
 } dicegpu_output_info;

@@ -176,6 +176,38 @@ def execute_frame_shapes(params, ref, deff, fields, shapes, vx=None, vy=None, bl
     return fields
 
 
+def execute_sequence(params, ref, frames, fields, run=None, evolution=None):
+    """Schema::execute_correlation over a sequence of deformed frames
+    (DICe_Main.cpp:324-360).  With params.use_incremental_formulation, every
+    frame after the first correlates against the previous deformed frame
+    (set_ref_image(prev_img()), :326-328), starts with DISPLACEMENT_X / _Y
+    at 0 and ends with them accumulated (DICe_Schema.cpp:1671-1675,
+    1775-1789; the first frame is not accumulated), and the tracking
+    routine re-reads every reference intensity, turned-on pixels included
+    (:1757-1759).  `run(ref, deff, fields, k)` runs frame k (default: the
+    square / list path); returns the field rows after each frame."""
+    if run is None:
+        def run(r, d, f, k):
+            execute_frame(params, r, d, f, first_frame=(k == 0))
+    incr = params.use_incremental_formulation != 0
+    acc = np.zeros((fields.shape[0], 2))
+    rows = []
+    cur = ref
+    for k, d in enumerate(frames):
+        if incr and k > 0:
+            cur = frames[k - 1]
+            fields[:, 2] = 0.0   # DISPLACEMENT_X
+            fields[:, 3] = 0.0   # DISPLACEMENT_Y
+            if evolution and "flag" in evolution and params.correlation_routine == TRACKING_ROUTINE:
+                evolution["flag"][evolution["flag"] == 2] = 1
+        run(cur, d, fields, k)
+        if incr and k > 0:
+            acc += fields[:, 2:4]
+            fields[:, 2:4] = acc
+        rows.append(fields.copy())
+    return rows
+
+
 def vsg_strain(fields, window):
     """VSG_Strain_Post_Processor on the field rows: (n x 7 values, failed flags)."""
     f = np.ascontiguousarray(fields, dtype=np.float64)
