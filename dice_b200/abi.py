@@ -43,6 +43,7 @@ PIXEL_F32, PIXEL_U8, PIXEL_U16 = 0, 1, 2
 SHAPE_CIRCLE, SHAPE_RECTANGLE, SHAPE_POLYGON = 0, 1, 2
 ROLE_BOUNDARY, ROLE_EXCLUDED, ROLE_OBSTRUCTED = 0, 1, 2
 GENERIC_ROUTINE, TRACKING_ROUTINE = 0, 1
+USE_FIELD_VALUES, USE_NEIGHBOR_VALUES, USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY = 0, 1, 2
 
 
 class Shape(ctypes.Structure):
@@ -113,7 +114,7 @@ class Params(ctypes.Structure):
         ("override_force_simplex", ctypes.c_int32),
         ("use_subset_evolution", ctypes.c_int32),
         ("use_incremental_formulation", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("initialization_method", ctypes.c_int32),
     ]
 
     def copy(self):
@@ -219,6 +220,7 @@ def _declare(lib):
         "dicegpu_get_subset_pixels": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
         "dicegpu_get_subset_pixel_state": (c_int, [c_void_p, c_void_p, c_void_p]),
         "dicegpu_set_ref_from_def": (c_int, [c_void_p]),
+        "dicegpu_set_neighbors": (c_int, [c_void_p, c_void_p]),
         "dicegpu_set_blocking": (c_int, [c_void_p, c_void_p, c_void_p]),
         "dicegpu_get_params": (c_int, [c_void_p, P]),
         "dicegpu_subset_file_read": (c_int, [ctypes.c_char_p, c_int, c_int, ctypes.POINTER(c_void_p),

@@ -48,6 +48,8 @@ struct FrameArgs {
   const int32_t* order;  // optional: the subsets of this launch (a tracking wave), n_order of them
   int n_order;
   int evolve;            // turn on visible inactive pixels of evolving subsets after success
+  const int32_t* neigh;  // neighbour initialization this frame: NEIGHBOR_ID per subset
+  const double* nsnap;   // the fields at frame start (neighbours with a higher index)
 };
 
 // Image_::interpolate_keys_fourth (DICe_Image.cpp:890-924), intensity only:
@@ -820,6 +822,30 @@ struct Engine {
     }
   }
 
+  // Quadratic_Shape_Function::update_params_for_centroid_change
+  // (DICe_LocalShapeFunction.cpp:632-651) for a neighbour's parameters:
+  // float parameters and products, the 2.0 literals promote to double.
+  __device__ static void centroid_change(float* q, float dx, float dy) {
+    const float A = q[0], B = q[1], C = q[2], D = q[3], E = q[4];
+    const float G = q[6], H = q[7], I = q[8], J = q[9], K = q[10];
+    auto dbl_term = [](float c, float d1, float d, float d2) {   // c*d1 + 2.0*d*d2
+      return __dadd_rn((double)__fmul_rn(c, d1), __dmul_rn(__dmul_rn(2.0, (double)d), (double)d2));
+    };
+    auto flt_sum = [](float a, float b, float c, float d, float e, float dx_, float dy_, float sub) {
+      float t = __fadd_rn(__fmul_rn(a, dx_), __fmul_rn(b, dy_));
+      t = __fadd_rn(t, __fmul_rn(__fmul_rn(c, dx_), dy_));
+      t = __fadd_rn(t, __fmul_rn(__fmul_rn(d, dx_), dx_));
+      t = __fadd_rn(t, __fmul_rn(__fmul_rn(e, dy_), dy_));
+      return __fsub_rn(t, sub);
+    };
+    q[0] = (float)__dadd_rn((double)q[0], dbl_term(C, dy, D, dx));
+    q[1] = (float)__dadd_rn((double)q[1], dbl_term(C, dx, E, dy));
+    q[5] = __fadd_rn(q[5], flt_sum(A, B, C, D, E, dx, dy, dx));
+    q[6] = (float)__dadd_rn((double)q[6], dbl_term(I, dy, J, dx));
+    q[7] = (float)__dadd_rn((double)q[7], dbl_term(I, dx, K, dy));
+    q[11] = __fadd_rn(q[11], flt_sum(G, H, I, J, K, dx, dy, dy));
+  }
+
   // Local_Shape_Function::save_fields: the shape-function columns of a field
   // row from the parameters (quadratic: A..L plus u, v, theta mapped at the
   // subset's coordinates).  Lane 0 writes.
@@ -1018,13 +1044,31 @@ struct Engine {
       }
     }
     int num_iterations = -1;
-    // Field_Value_Initializer::initial_guess (DICe_Initializer.cpp:398-436)
-    if (fld(DICEGPU_F_SIGMA) == -1.0) {
+    // Field_Value_Initializer::initial_guess (DICe_Initializer.cpp:398-436):
+    // the subset's own row, or its neighbour's.  Subsets run in index order
+    // in the reference: a lower neighbour ran earlier this frame (an earlier
+    // wave, or this warp just before in a chain: __syncwarp orders lane 0's
+    // writes), a higher one contributes its frame-start row.
+    double gv = fv;
+    int init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+    const int nb = A.neigh ? A.neigh[idx] : -1;
+    if (nb >= 0 && nb < A.n && nb != idx) {
+      __syncwarp();
+      gv = (nb < idx ? A.fields : A.nsnap)[(size_t)nb * DICEGPU_FIELD_STRIDE + lane];
+      init_status = DICEGPU_INITIALIZE_USING_NEIGHBOR_VALUE_SUCCESSFUL;
+    }
+    if (__shfl_sync(FULL, gv, DICEGPU_F_SIGMA) == -1.0) {
       record_failed(f, DICEGPU_INITIALIZE_FAILED, num_iterations);
       return;
     }
-    load_slots_row(fv, slots);
-    int init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+    float guess[12];
+    load_slots_row(gv, guess);
+    if (SHAPE == DICEGPU_QUADRATIC_SF && init_status == DICEGPU_INITIALIZE_USING_NEIGHBOR_VALUE_SUCCESSFUL)
+      centroid_change(guess, __fsub_rn((float)fld(DICEGPU_F_COORD_X), (float)__shfl_sync(FULL, gv, DICEGPU_F_COORD_X)),
+                      __fsub_rn((float)fld(DICEGPU_F_COORD_Y), (float)__shfl_sync(FULL, gv, DICEGPU_F_COORD_Y)));
+#pragma unroll
+    for (int i = 0; i < 12; ++i) slots[i] = guess[i];
+    const int guess_status = init_status;
     // reference mean at Gauss-Newton entry: over the pixels active at the last
     // deformed-state initialisation (none yet: all of them)
     bool have_state = false;
@@ -1091,13 +1135,15 @@ struct Engine {
       if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_GRADIENT_BASED || force_simplex) {
         second_failed = true;
       } else if (opt == DICEGPU_GRADIENT_BASED_THEN_SIMPLEX) {
-        load_slots_row(fv, slots);
-        init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) slots[i] = guess[i];
+        init_status = guess_status;
         run_simplex();
         if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
       } else if (opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED) {
-        load_slots_row(fv, slots);
-        init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) slots[i] = guess[i];
+        init_status = guess_status;
         run_gn();
         if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
       }

@@ -329,8 +329,19 @@ struct dicegpu_ctx {
   bool has_blocking = false;
   std::vector<int32_t> h_blk_off, h_blk_ids;
   DevBuf<int32_t> d_blk_off, d_blk_ids;
-  std::vector<int32_t> wave_off, bwave_off;   // wave L: d_wave[wave_off[L] ..), d_bwave[bwave_off[L] ..)
-  DevBuf<int32_t> d_wave, d_bwave, d_dv_off, d_dvx, d_dvy, d_dp_off, d_bpoly;
+  std::vector<uint8_t> h_has_polys;   // blocked subsets with conformal blockers
+  DevBuf<int32_t> d_dv_off, d_dvx, d_dvy, d_dp_off, d_bpoly;
+  // neighbour initialization: NEIGHBOR_ID per subset (empty: none)
+  std::vector<int32_t> h_neigh;
+  DevBuf<int32_t> d_neigh;
+  // Dependency waves, one plan per kind (bit 0: blocking subsets of the
+  // tracking routine, bit 1: neighbour initialization): wave L is
+  // d_wave[wave_off[L] ..) in index order, its blocked subsets d_bwave[bwave_off[L] ..)
+  struct Plan {
+    bool valid = false;
+    std::vector<int32_t> wave_off, bwave_off;
+    DevBuf<int32_t> d_wave, d_bwave;
+  } plans[4];
   DevBuf<double> d_snapshot;
   int n_blocked = 0;                   // subsets with a conformal blocker
   // forced simplex: the caller's flags and the blocking rule's
@@ -372,6 +383,9 @@ static int build_devparams(const dicegpu_params& p, DevParams& d) {
   if (p.correlation_routine != DICEGPU_GENERIC_ROUTINE && p.correlation_routine != DICEGPU_TRACKING_ROUTINE)
     return DICEGPU_ERR_ARG;
   if (!(std::fabs(p.obstruction_skin_factor) < 1.0e6)) return DICEGPU_ERR_ARG;
+  if (p.initialization_method != DICEGPU_USE_FIELD_VALUES && p.initialization_method != DICEGPU_USE_NEIGHBOR_VALUES &&
+      p.initialization_method != DICEGPU_USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY)
+    return DICEGPU_ERR_UNSUPPORTED;
   if (p.gauss_filter_images) {
     GaussWeights g;
     if (!gauss_weights(p.gauss_filter_mask_size, g)) return DICEGPU_ERR_ARG;
@@ -510,9 +524,10 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   c->d_conformal.release(); c->d_mask_desc.release(); c->d_mask_bits.release();
   c->d_pix_flag.release(); c->d_pix_flag0.release(); c->d_pix_f.release();
   c->d_evo_nact.release(); c->d_evo_nact0.release(); c->d_acc.release(); c->d_ref_saved.release();
-  c->d_blk_off.release(); c->d_blk_ids.release(); c->d_wave.release();
+  c->d_blk_off.release(); c->d_blk_ids.release(); c->d_neigh.release();
+  for (auto& pl : c->plans) { pl.d_wave.release(); pl.d_bwave.release(); }
   c->d_dp_off.release(); c->d_bpoly.release();
-  c->d_bwave.release(); c->d_dv_off.release(); c->d_dvx.release(); c->d_dvy.release();
+  c->d_dv_off.release(); c->d_dvx.release(); c->d_dvy.release();
   c->d_snapshot.release();
   c->d_vsg_cell_off.release(); c->d_vsg_cell_pts.release(); c->d_vsg.release();
   c->d_vsg_pos.release(); c->d_vsg_packed.release();
@@ -748,6 +763,25 @@ extern "C" int dicegpu_set_def_image_typed(dicegpu_ctx* c, int w, int h, const v
   return set_def(c, w, h, pixels, pixel_type, on_device);
 }
 
+extern "C" int dicegpu_set_neighbors(dicegpu_ctx* c, const int32_t* neighbor_ids) {
+  if (!c || c->n < 1) return DICEGPU_ERR_ARG;
+  c->plans[2].valid = c->plans[3].valid = false;   // the plans with neighbours
+  if (!neighbor_ids) {
+    c->h_neigh.clear();
+    return DICEGPU_OK;
+  }
+  const int n = c->n;
+  std::vector<int32_t> nb(neighbor_ids, neighbor_ids + n);
+  for (auto& j : nb)
+    if (j < 0 || j >= n) j = -1;
+  cudaStreamSynchronize(c->stream);
+  int rc = c->d_neigh.ensure(n);
+  if (rc) return rc;
+  CK(cudaMemcpy(c->d_neigh.p, nb.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  c->h_neigh.swap(nb);
+  return DICEGPU_OK;
+}
+
 extern "C" int dicegpu_set_ref_from_def(dicegpu_ctx* c) {
   if (!c) return DICEGPU_ERR_ARG;
   if (!c->has_ref || !c->has_def) return DICEGPU_ERR_STATE;
@@ -783,6 +817,7 @@ extern "C" int dicegpu_set_subsets(dicegpu_ctx* c, int n, const double* fields) 
     c->use_lists = false;
     c->use_force = false;
     c->h_force_user.clear();
+    c->h_neigh.clear();
     clear_shapes(c);
   }
   c->vsg_window = 0;
@@ -876,7 +911,7 @@ static void clear_shapes(dicegpu_ctx* c) {
   c->has_blocking = false;
   c->h_blk_off.clear(); c->h_blk_ids.clear();
   c->blocking_desc_ready = false;
-  c->wave_off.clear(); c->bwave_off.clear();
+  for (auto& pl : c->plans) pl.valid = false;
   c->n_blocked = 0;
   c->h_force_block.clear();
 }
@@ -1071,6 +1106,7 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
     c->has_blocking = false;
     c->h_force_block.clear();
     c->n_blocked = 0;
+    for (auto& pl : c->plans) pl.valid = false;
     if (!c->h_mask_desc.empty()) {
       bool any = false;
       for (int i = 0; i < n; ++i) {
@@ -1125,27 +1161,8 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
     }
   }
   if (dv_total > ((int64_t)1 << 30) || dp_total > ((int64_t)1 << 26)) return DICEGPU_ERR_ARG;
-  // waves: a subset runs after every blocker that precedes it in index order
-  std::vector<int> level(n, 0);
-  int nlev = 1;
-  for (int i = 0; i < n; ++i) {
-    for (int k = offsets[i]; k < offsets[i + 1]; ++k)
-      if (ids[k] < i) level[i] = std::max(level[i], level[ids[k]] + 1);
-    nlev = std::max(nlev, level[i] + 1);
-  }
-  std::vector<int32_t> wave, bwave, wave_off(nlev + 1, 0), bwave_off(nlev + 1, 0);
-  for (int L = 0; L < nlev; ++L) {
-    for (int i = 0; i < n; ++i)
-      if (level[i] == L) {
-        wave.push_back(i);
-        if (has_polys[i]) bwave.push_back(i);
-      }
-    wave_off[L + 1] = (int32_t)wave.size();
-    bwave_off[L + 1] = (int32_t)bwave.size();
-  }
   int rc;
   if ((rc = c->d_blk_off.ensure(n + 1)) || (rc = c->d_blk_ids.ensure(std::max(offsets[n], 1))) ||
-      (rc = c->d_wave.ensure(n)) || (rc = c->d_bwave.ensure(std::max<size_t>(bwave.size(), 1))) ||
       (rc = c->d_dv_off.ensure(n)) || (rc = c->d_dvx.ensure((size_t)std::max<int64_t>(dv_total, 1))) ||
       (rc = c->d_dvy.ensure((size_t)std::max<int64_t>(dv_total, 1))) || (rc = c->d_dp_off.ensure(n)) ||
       (rc = c->d_bpoly.ensure(6 * (size_t)std::max<int64_t>(dp_total, 1))) ||
@@ -1153,15 +1170,12 @@ extern "C" int dicegpu_set_blocking(dicegpu_ctx* c, const int32_t* offsets, cons
     return rc;
   CK(cudaMemcpy(c->d_blk_off.p, offsets, (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
   if (offsets[n]) CK(cudaMemcpy(c->d_blk_ids.p, ids, offsets[n] * sizeof(int32_t), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->d_wave.p, wave.data(), wave.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-  if (!bwave.empty())
-    CK(cudaMemcpy(c->d_bwave.p, bwave.data(), bwave.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_dv_off.p, dv_off.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_dp_off.p, dp_off.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
   c->h_blk_off.assign(offsets, offsets + n + 1);
   c->h_blk_ids.assign(ids, ids + offsets[n]);
-  c->wave_off.swap(wave_off);
-  c->bwave_off.swap(bwave_off);
+  c->h_has_polys.swap(has_polys);
+  for (auto& pl : c->plans) pl.valid = false;
   c->n_blocked = n_blocked;
   c->blocking_desc_ready = false;   // descriptors uploaded at the next tracking frame
   c->h_force_block.swap(force);
@@ -1479,40 +1493,136 @@ static int frame_end(dicegpu_ctx* c) {
   return DICEGPU_OK;
 }
 
-// TRACKING_ROUTINE with blocking subsets: the frame runs in waves, each
-// after the blocked polygons of its blocked subsets are rebuilt from their
-// blockers' parameters (this frame's for earlier subsets, the frame-start
-// snapshot's for later ones).  Everything is enqueued on the stream.
-static int run_tracking_frame(dicegpu_ctx* c, FrameKernelFn fn, int blocks, size_t smem) {
-  int rc = ensure_blocking_desc(c);
-  if (rc) return rc;
+// Dependency waves of a frame (plan kind: bit 0 blocking subsets under the
+// tracking routine, bit 1 neighbour initialization).  The reference runs the
+// subsets in index order, so a subset depends on the blockers and the
+// neighbour that precede it: level(i) = 1 + the largest level among them,
+// and wave L holds the subsets of level L in index order.  Counting sort, O(n).
+static int build_plan(dicegpu_ctx* c, int kind) {
+  dicegpu_ctx::Plan& pl = c->plans[kind];
+  if (pl.valid) return DICEGPU_OK;
   const int n = c->n;
+  const bool blk = (kind & 1) && c->has_blocking && (int)c->h_blk_off.size() == n + 1;
+  const bool nbr = (kind & 2) && (int)c->h_neigh.size() == n;
+  std::vector<int32_t> level(n, 0);
+  int nlev = 1;
+  for (int i = 0; i < n; ++i) {
+    int L = 0;
+    if (blk)
+      for (int k = c->h_blk_off[i]; k < c->h_blk_off[i + 1]; ++k) {
+        const int j = c->h_blk_ids[k];
+        if (j < i) L = std::max(L, level[j] + 1);
+      }
+    if (nbr) {
+      const int j = c->h_neigh[i];
+      if (j >= 0 && j < i) L = std::max(L, level[j] + 1);
+    }
+    level[i] = L;
+    nlev = std::max(nlev, L + 1);
+  }
+  std::vector<int32_t> wave(n), wave_off(nlev + 1, 0), bwave_off(nlev + 1, 0), bwave;
+  for (int i = 0; i < n; ++i) {
+    ++wave_off[level[i] + 1];
+    if (blk && (int)c->h_has_polys.size() == n && c->h_has_polys[i]) ++bwave_off[level[i] + 1];
+  }
+  for (int L = 0; L < nlev; ++L) {
+    wave_off[L + 1] += wave_off[L];
+    bwave_off[L + 1] += bwave_off[L];
+  }
+  bwave.resize(bwave_off[nlev]);
+  {
+    std::vector<int32_t> wf(wave_off.begin(), wave_off.end() - 1), bf(bwave_off.begin(), bwave_off.end() - 1);
+    for (int i = 0; i < n; ++i) {
+      wave[wf[level[i]]++] = i;
+      if (blk && (int)c->h_has_polys.size() == n && c->h_has_polys[i]) bwave[bf[level[i]]++] = i;
+    }
+  }
+  int rc;
+  if ((rc = pl.d_wave.ensure(n)) || (rc = pl.d_bwave.ensure(std::max<size_t>(bwave.size(), 1)))) return rc;
+  CK(cudaMemcpy(pl.d_wave.p, wave.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (!bwave.empty())
+    CK(cudaMemcpy(pl.d_bwave.p, bwave.data(), bwave.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  pl.wave_off.swap(wave_off);
+  pl.bwave_off.swap(bwave_off);
+  pl.valid = true;
+  return DICEGPU_OK;
+}
+
+// The plan kind of the next frame (0: one launch over all subsets).
+static int frame_plan_kind(const dicegpu_ctx* c) {
+  int kind = 0;
+  if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE) kind |= 1;
+  const int im = c->params.initialization_method;
+  if ((int)c->h_neigh.size() == c->n &&
+      (im == DICEGPU_USE_NEIGHBOR_VALUES || (im == DICEGPU_USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY && c->frame_index == 0)))
+    kind |= 2;
+  return kind;
+}
+
+// A frame in dependency waves.  Blocked subsets get their blocked polygons
+// rebuilt before their wave from their blockers' parameters (this frame's
+// for lower indices, the frame-start snapshot's for higher ones); neighbour
+// initialization reads the same way.  Runs of waves that hold a single
+// subset without blocked polygons (a neighbour chain) go to one launch of
+// a single warp, which takes them in order.  Everything is enqueued.
+static int run_waves(dicegpu_ctx* c, int kind, FrameKernelFn fn, int blocks, size_t smem) {
+  int rc;
+  if ((kind & 1) && (rc = ensure_blocking_desc(c))) return rc;
+  if ((rc = build_plan(c, kind))) return rc;
+  const dicegpu_ctx::Plan& pl = c->plans[kind];
+  const int n = c->n;
+  if ((rc = c->d_snapshot.ensure((size_t)n * DICEGPU_FIELD_STRIDE))) return rc;
   CK(cudaMemcpyAsync(c->d_snapshot.p, c->d_fields, (size_t)n * DICEGPU_FIELD_STRIDE * sizeof(double),
                      cudaMemcpyDeviceToDevice, c->stream));
   BlockArgs ba;
   std::memset(&ba, 0, sizeof(ba));
-  ba.P = c->dp;
-  ba.shapes = c->d_shapes.p;
-  ba.shape_off = c->d_shape_off.p;
-  ba.vx = c->d_svx.p;
-  ba.vy = c->d_svy.p;
-  ba.fields = c->d_fields;
-  ba.snapshot = c->d_snapshot.p;
-  ba.blk_off = c->d_blk_off.p;
-  ba.blk_ids = c->d_blk_ids.p;
-  ba.conformal = c->d_conformal.p;
-  ba.dv_off = c->d_dv_off.p;
-  ba.dp_off = c->d_dp_off.p;
-  ba.dvx = c->d_dvx.p;
-  ba.dvy = c->d_dvy.p;
-  ba.polys = c->d_bpoly.p;
-  ba.desc = c->d_mask_desc.p;
-  ba.skin = (float)c->params.obstruction_skin_factor;
-  const int nlev = (int)c->wave_off.size() - 1;
-  for (int L = 0; L < nlev; ++L) {
-    const int nb = c->bwave_off[L + 1] - c->bwave_off[L];
+  if (kind & 1) {
+    ba.P = c->dp;
+    ba.shapes = c->d_shapes.p;
+    ba.shape_off = c->d_shape_off.p;
+    ba.vx = c->d_svx.p;
+    ba.vy = c->d_svy.p;
+    ba.fields = c->d_fields;
+    ba.snapshot = c->d_snapshot.p;
+    ba.blk_off = c->d_blk_off.p;
+    ba.blk_ids = c->d_blk_ids.p;
+    ba.conformal = c->d_conformal.p;
+    ba.dv_off = c->d_dv_off.p;
+    ba.dp_off = c->d_dp_off.p;
+    ba.dvx = c->d_dvx.p;
+    ba.dvy = c->d_dvy.p;
+    ba.polys = c->d_bpoly.p;
+    ba.desc = c->d_mask_desc.p;
+    ba.skin = (float)c->params.obstruction_skin_factor;
+  }
+  const int nlev = (int)pl.wave_off.size() - 1;
+  const size_t smem1 = warp_smem_bytes(c->dp.shape);
+  for (int L = 0; L < nlev;) {
+    const int nb = pl.bwave_off[L + 1] - pl.bwave_off[L];
+    const int nw = pl.wave_off[L + 1] - pl.wave_off[L];
+    FrameArgs a;
+    fill_args(c, a, MODE_CORRELATE);
+    if (kind & 2) {
+      a.neigh = c->d_neigh.p;
+      a.nsnap = c->d_snapshot.p;
+    }
+    if (nw == 1 && nb == 0) {
+      // a chain: consecutive single-subset waves without blocked polygons
+      int L1 = L + 1;
+      while (L1 < nlev && pl.wave_off[L1 + 1] - pl.wave_off[L1] == 1 && pl.bwave_off[L1 + 1] == pl.bwave_off[L1])
+        ++L1;
+      a.order = pl.d_wave.p + pl.wave_off[L];
+      a.n_order = pl.wave_off[L1] - pl.wave_off[L];
+      a.queue_mode = 0;
+      CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
+      fn<<<1, 32, smem1, c->stream>>>(a);
+      CK(cudaGetLastError());
+      c->launches += 1;
+      L = L1;
+      continue;
+    }
     if (nb > 0) {
-      ba.list = c->d_bwave.p + c->bwave_off[L];
+      ba.list = pl.d_bwave.p + pl.bwave_off[L];
       ba.nlist = nb;
       const unsigned g = (unsigned)std::min((nb * 32 + 255) / 256, 8 * c->num_sms);   // a warp per subset
       if (c->dp.shape == DICEGPU_QUADRATIC_SF) blocked_kernel<DICEGPU_QUADRATIC_SF><<<g, 256, 0, c->stream>>>(ba);
@@ -1520,16 +1630,15 @@ static int run_tracking_frame(dicegpu_ctx* c, FrameKernelFn fn, int blocks, size
       CK(cudaGetLastError());
       c->launches += 1;
     }
-    const int nw = c->wave_off[L + 1] - c->wave_off[L];
-    if (nw == 0) continue;
-    FrameArgs a;
-    fill_args(c, a, MODE_CORRELATE);
-    a.order = c->d_wave.p + c->wave_off[L];
-    a.n_order = nw;
-    CK(cudaMemsetAsync(c->d_counter, 0, (size_t)blocks * sizeof(int), c->stream));
-    fn<<<blocks, c->warps_per_cta * 32, smem, c->stream>>>(a);
-    CK(cudaGetLastError());
-    c->launches += 1;
+    if (nw > 0) {
+      a.order = pl.d_wave.p + pl.wave_off[L];
+      a.n_order = nw;
+      CK(cudaMemsetAsync(c->d_counter, 0, (size_t)blocks * sizeof(int), c->stream));
+      fn<<<blocks, c->warps_per_cta * 32, smem, c->stream>>>(a);
+      CK(cudaGetLastError());
+      c->launches += 1;
+    }
+    ++L;
   }
   return DICEGPU_OK;
 }
@@ -1542,8 +1651,9 @@ extern "C" int dicegpu_execute_correlation(dicegpu_ctx* c) {
   size_t smem;
   if ((rc = grid_for(c, fn, &blocks, &smem))) return rc;
   if ((rc = frame_begin(c))) return rc;
-  if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE) {
-    if ((rc = run_tracking_frame(c, fn, blocks, smem))) return rc;
+  const int kind = frame_plan_kind(c);
+  if (kind) {
+    if ((rc = run_waves(c, kind, fn, blocks, smem))) return rc;
     return frame_end(c);
   }
   FrameArgs a;
@@ -1566,6 +1676,11 @@ extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
   const size_t smem = warp_smem_bytes(c->dp.shape);
   FrameArgs a;
   fill_args(c, a, MODE_CORRELATE);
+  if (frame_plan_kind(c) & 2) {
+    // launches in index order: a higher neighbour has not run yet
+    a.neigh = c->d_neigh.p;
+    a.nsnap = c->d_fields;
+  }
   for (int i = 0; i < c->n; ++i) {
     a.plain_index = i;
     fn<<<1, 32, smem, c->stream>>>(a);
@@ -1585,9 +1700,22 @@ extern "C" int dicegpu_capture_sequence(dicegpu_ctx* c, int n, const float* cons
     if (!frames[k]) return DICEGPU_ERR_ARG;
   if (!c->has_ref || c->n < 1) return DICEGPU_ERR_STATE;
   if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
-  // the blocking descriptors are uploaded before capture (synchronous copies cannot be captured)
-  if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE) {
-    const int rcb = ensure_blocking_desc(c);
+  // everything a captured frame needs is allocated and uploaded first
+  // (allocations and synchronous copies cannot be captured): blocking
+  // descriptors, the wave plans of the first and the later frames, the
+  // snapshot and the accumulated displacements
+  {
+    int rcb = DICEGPU_OK;
+    if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE) rcb = ensure_blocking_desc(c);
+    const int saved = c->frame_index;
+    for (int fi : {reset_fields ? 0 : saved, std::max(saved, 1)}) {
+      c->frame_index = fi;
+      const int kind = frame_plan_kind(c);
+      if (!rcb && kind) rcb = build_plan(c, kind);
+    }
+    c->frame_index = saved;
+    if (!rcb) rcb = c->d_snapshot.ensure((size_t)c->n * DICEGPU_FIELD_STRIDE);
+    if (!rcb && c->params.use_incremental_formulation) rcb = c->d_acc.ensure(2 * (size_t)c->n);
     if (rcb) return rcb;
   }
   CK(cudaStreamSynchronize(c->stream));

@@ -787,5 +787,8 @@ extern "C" int dicegpu_subset_file_apply_grid(const dicegpu_subset_file* f, dice
     if (sd.flags & DICEGPU_SF_SEED_SHEAR_STRAIN) r[DICEGPU_F_SHEAR_XY] = sd.v[4];
     if (sd.flags & DICEGPU_SF_SEED_ROTATION) r[DICEGPU_F_ROT_Z] = sd.v[5];
   }
-  return dicegpu_set_subsets(ctx, n, rows.data());
+  if ((rc = dicegpu_set_subsets(ctx, n, rows.data()))) return rc;
+  // NEIGHBOR_ID_FS from the decomposition (DICe_Schema.cpp:1302), for the
+  // neighbour initializers
+  return dicegpu_set_neighbors(ctx, neigh.data());
 }

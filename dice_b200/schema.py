@@ -120,6 +120,15 @@ class Schema:
         if len(self._keep) > 4:
             self._keep = self._keep[-4:]
 
+    def set_neighbors(self, neighbor_ids):
+        """NEIGHBOR_ID per subset (None clears) for the neighbour initializers."""
+        if neighbor_ids is None:
+            abi.check(self.lib.dicegpu_set_neighbors(self.ctx, None), "set_neighbors")
+            return
+        nb = np.ascontiguousarray(neighbor_ids, dtype=np.int32)
+        assert nb.shape == (self.n,)
+        abi.check(self.lib.dicegpu_set_neighbors(self.ctx, nb.ctypes.data_as(ctypes.c_void_p)), "set_neighbors")
+
     def set_ref_from_def(self):
         """Incremental sequences: the current deformed image becomes the
         reference (Schema::set_ref_image(prev_img()))."""

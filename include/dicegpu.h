@@ -216,8 +216,23 @@ typedef struct dicegpu_params {
    * intensities from the new reference (:1757-1759), evolved pixels
    * included. */
   int32_t use_incremental_formulation;
-  int32_t reserved;
+  /* initialization_method (DICEGPU_USE_FIELD_VALUES): where a subset's
+   * initial guess comes from (Field_Value_Initializer::initial_guess,
+   * DICe_Initializer.cpp:398-436).  USE_NEIGHBOR_VALUES takes the field
+   * values of the subset's neighbour (dicegpu_set_neighbors; -1 or itself:
+   * its own), every frame; USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY at the first
+   * frame of a sequence only.  Subsets run in index order as in the
+   * reference, so a neighbour with a lower index contributes this frame's
+   * solution and one with a higher index its frame-start values; the device
+   * runs the subsets in dependency waves (a chain of single subsets as one
+   * sequential launch).  Other methods: DICEGPU_ERR_UNSUPPORTED. */
+  int32_t initialization_method;
 } dicegpu_params;
+
+/* Initialization_Method (DICe.h:473-489) */
+#define DICEGPU_USE_FIELD_VALUES                    0
+#define DICEGPU_USE_NEIGHBOR_VALUES                 1
+#define DICEGPU_USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY 2
 
 /* Correlation_Routine */
 #define DICEGPU_GENERIC_ROUTINE  0
@@ -358,6 +373,10 @@ int dicegpu_vsg_strain(dicegpu_ctx* ctx, int window_size, double* out, int on_de
 /* Copies the context's subset pixel lists to host memory: offsets[n + 1]
  * and, when px / py are not NULL, offsets[n] coordinates each. */
 int dicegpu_get_subset_pixels(dicegpu_ctx* ctx, int32_t* offsets, int32_t* px, int32_t* py);
+/* NEIGHBOR_ID per subset (the decomposition's neighbor_ids, e.g. the
+ * regular grid's snake predecessor); NULL clears them (every subset its own
+ * neighbour).  Ids outside [0, n) count as -1. */
+int dicegpu_set_neighbors(dicegpu_ctx* ctx, const int32_t* neighbor_ids);
 /* Schema::post_execution_tasks + set_ref_image(prev_img()) of an
  * incremental sequence: the current deformed image (filtered, if the
  * params filter) becomes the reference and its gradients are computed;

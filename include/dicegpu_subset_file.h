@@ -130,7 +130,9 @@ int dicegpu_regular_grid(const dicegpu_subset_file* f, int width, int height, in
 
 /* Schema::initialize with a region-of-interest file (or none: f NULL, the
  * whole image) and a step size: the grid's points become square subsets of
- * params.subset_size, the regions' seeds their field rows' initial values. */
+ * params.subset_size, the regions' seeds their field rows' initial values,
+ * and the grid's neighbor_ids the subsets' neighbours
+ * (dicegpu_set_neighbors). */
 int dicegpu_subset_file_apply_grid(const dicegpu_subset_file* f, dicegpu_ctx* ctx, int width, int height,
                                    int step_size);
 

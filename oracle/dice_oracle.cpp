@@ -1009,12 +1009,31 @@ static void record_failed_step(double* f, int status, int num_iterations) {
 }
 
 // Field_Value_Initializer::initial_guess (DICe_Initializer.cpp:398-436), own id.
-static int initial_guess(const double* f, ShapeFn& sf) {
-  if (f[DICEGPU_F_SIGMA] != -1.0) {
-    sf.from_fields(f);
-    return DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+// Field_Value_Initializer::initial_guess (DICe_Initializer.cpp:398-436):
+// the subset's own field row, or its neighbour's (nf) with neighbour
+// initialization; the quadratic parameters then move to this subset's
+// centroid (Quadratic_Shape_Function::update_params_for_centroid_change,
+// DICe_LocalShapeFunction.cpp:632-651, float parameters, the 2.0 literals
+// in double).
+static int initial_guess(const double* f, const double* nf, ShapeFn& sf) {
+  const double* g = nf ? nf : f;
+  if (g[DICEGPU_F_SIGMA] == -1.0) return DICEGPU_INITIALIZE_FAILED;
+  sf.from_fields(g);
+  if (!nf) return DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
+  if (sf.type == DICEGPU_QUADRATIC_SF) {
+    const float dx = (float)f[DICEGPU_F_COORD_X] - (float)nf[DICEGPU_F_COORD_X];
+    const float dy = (float)f[DICEGPU_F_COORD_Y] - (float)nf[DICEGPU_F_COORD_Y];
+    float* q = sf.p;
+    const float A = q[0], B = q[1], C = q[2], D = q[3], E = q[4];
+    const float G = q[6], H = q[7], I = q[8], J = q[9], K = q[10];
+    q[0] = (float)((double)q[0] + ((double)(C * dy) + 2.0 * D * dx));
+    q[1] = (float)((double)q[1] + ((double)(C * dx) + 2.0 * E * dy));
+    q[5] += A * dx + B * dy + C * dx * dy + D * dx * dx + E * dy * dy - dx;
+    q[6] = (float)((double)q[6] + ((double)(I * dy) + 2.0 * J * dx));
+    q[7] = (float)((double)q[7] + ((double)(I * dx) + 2.0 * K * dy));
+    q[11] += G * dx + H * dy + I * dx * dy + J * dx * dx + K * dy * dy - dy;
   }
-  return DICEGPU_INITIALIZE_FAILED;
+  return DICEGPU_INITIALIZE_USING_NEIGHBOR_VALUE_SUCCESSFUL;
 }
 
 // Objective::beta (DICe_Objective.cpp:78-148): finite-difference slope of gamma
@@ -1070,7 +1089,7 @@ static float objective_beta(const Ctx& C, Subset& s, const ShapeFn& sf_in) {
 // Schema::generic_correlation_routine (DICe_Schema.cpp:2026-2368) for one subset,
 // restricted to the USE_FIELD_VALUES initializer and local DIC.
 static bool correlate_subset(const Ctx& C, Subset& s, double* f, bool first_frame,
-                             bool force_simplex, Counters* cnt) {
+                             bool force_simplex, Counters* cnt, const double* nf = nullptr) {
   const dicegpu_params& P = C.P;
   if (P.subset_size > 0 && first_frame) {
     const float cur_x = (float)(f[DICEGPU_F_COORD_X] + f[DICEGPU_F_DISP_X]);
@@ -1084,7 +1103,7 @@ static bool correlate_subset(const Ctx& C, Subset& s, double* f, bool first_fram
   int num_iterations = -1;
   ShapeFn sf;
   sf.init(P);
-  int init_status = initial_guess(f, sf);
+  int init_status = initial_guess(f, nf, sf);
   if (init_status == DICEGPU_INITIALIZE_FAILED) {
     record_failed_step(f, init_status, num_iterations);
     return false;
@@ -1121,11 +1140,11 @@ static bool correlate_subset(const Ctx& C, Subset& s, double* f, bool first_fram
     if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_GRADIENT_BASED || force_simplex) {
       second_failed = true;
     } else if (opt == DICEGPU_GRADIENT_BASED_THEN_SIMPLEX) {
-      init_status = initial_guess(f, sf);
+      init_status = initial_guess(f, nf, sf);
       corr_status = compute_update_robust(C, s, sf, num_iterations, cnt);
       if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
     } else if (opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED) {
-      init_status = initial_guess(f, sf);
+      init_status = initial_guess(f, nf, sf);
       corr_status = compute_update_fast(C, s, sf, num_iterations, &cond, cnt);
       cond_set = true;
       if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
@@ -1264,6 +1283,7 @@ struct FrameJob {
   uint8_t* pix_flag = nullptr;                   // subset evolution state per list pixel
   float* pix_f = nullptr;
   bool evolve = false;                           // turn on visible inactive pixels after success
+  const int32_t* neighbors = nullptr;            // neighbour initialization this frame
 };
 
 void run_range(const FrameJob& J, int b, int e) {
@@ -1285,7 +1305,15 @@ void run_range(const FrameJob& J, int b, int e) {
       cnt.ucx = (float)f[DICEGPU_F_COORD_X];
       cnt.ucy = (float)f[DICEGPU_F_COORD_Y];
     }
-    const bool ok = correlate_subset(J.C, s, f, J.first_frame, J.force_simplex && J.force_simplex[i], &cnt);
+    // neighbour initialization: subsets run in index order, so a lower
+    // neighbour's row holds this frame's solution, a higher one's the
+    // previous frame's
+    const double* nf = nullptr;
+    if (J.neighbors) {
+      const int j = J.neighbors[i];
+      if (j >= 0 && j < J.n && j != i) nf = J.fields + (long)j * DICEGPU_FIELD_STRIDE;
+    }
+    const bool ok = correlate_subset(J.C, s, f, J.first_frame, J.force_simplex && J.force_simplex[i], &cnt, nf);
     // Subset::turn_on_previously_obstructed_pixels (DICe_Subset.cpp:506-520)
     // with the deformed state of the last evaluation
     if (ok && J.evolve && s.flag)
@@ -1334,7 +1362,7 @@ static int prepare_frame(const dicegpu_params* params, int w, int h, const float
 
 static void run_parallel(const FrameJob& J, int nthreads) {
   const int n = J.n;
-  if (nthreads <= 1 || n < 2) {
+  if (nthreads <= 1 || n < 2 || J.neighbors) {   // neighbour chains run in index order
     run_range(J, 0, n);
     return;
   }
@@ -1352,11 +1380,17 @@ extern "C" int oracle_execute_frame(const dicegpu_params* params, int w, int h, 
                                     const int32_t* offsets, const int32_t* px,
                                     const int32_t* py, const uint8_t* force_simplex,
                                     int first_frame, int nthreads, int32_t* gn_iters_out,
-                                    int32_t* simplex_evals_out, double* uncertainty) {
+                                    int32_t* simplex_evals_out, double* uncertainty, const int32_t* neighbors) {
   if (!fields || n < 0) return DICEGPU_ERR_ARG;
   FrameJob J;
   const int rc = prepare_frame(params, w, h, ref, def, J);
   if (rc) return rc;
+  const int im = params->initialization_method;
+  if (im != DICEGPU_USE_FIELD_VALUES && im != DICEGPU_USE_NEIGHBOR_VALUES &&
+      im != DICEGPU_USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY)
+    return DICEGPU_ERR_UNSUPPORTED;
+  if (neighbors && (im == DICEGPU_USE_NEIGHBOR_VALUES || (im == DICEGPU_USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY && first_frame)))
+    J.neighbors = neighbors;
   J.n = n; J.fields = fields; J.offsets = offsets; J.px = px; J.py = py;
   J.force_simplex = force_simplex; J.first_frame = first_frame != 0;
   J.gn_out = gn_iters_out; J.sx_out = simplex_evals_out; J.unc = uncertainty;

@@ -37,7 +37,8 @@ int oracle_execute_frame(const dicegpu_params* params, int w, int h,
                          const float* ref, const float* def, int n, double* fields,
                          const int32_t* offsets, const int32_t* px, const int32_t* py,
                          const uint8_t* force_simplex, int first_frame, int nthreads,
-                         int32_t* gn_iters_out, int32_t* simplex_evals_out, double* uncertainty);
+                         int32_t* gn_iters_out, int32_t* simplex_evals_out, double* uncertainty,
+                         const int32_t* neighbors);
 
 /* Image_::compute_gradients (finite difference, optional 5-point smoothing). */
 int oracle_gradients(int w, int h, const float* img, int method, float* gx, float* gy);

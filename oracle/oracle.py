@@ -44,7 +44,7 @@ def lib():
         P = ctypes.POINTER(Params)
         vp, ci = ctypes.c_void_p, ctypes.c_int
         L.oracle_execute_frame.restype = ci
-        L.oracle_execute_frame.argtypes = [P, ci, ci, vp, vp, ci, vp, vp, vp, vp, vp, ci, ci, vp, vp, vp]
+        L.oracle_execute_frame.argtypes = [P, ci, ci, vp, vp, ci, vp, vp, vp, vp, vp, ci, ci, vp, vp, vp, vp]
         L.oracle_gradients.restype = ci
         L.oracle_gradients.argtypes = [ci, ci, vp, ci, vp, vp]
         L.oracle_gauss_filter.restype = ci
@@ -77,10 +77,13 @@ def _ptr(a):
 
 
 def execute_frame(params, ref, deff, fields, first_frame=True, nthreads=1, offsets=None,
-                  px=None, py=None, force_simplex=None, counters=False, uncertainty=None):
+                  px=None, py=None, force_simplex=None, counters=False, uncertainty=None, neighbors=None):
     """One frame over all subsets; updates `fields` (n x FIELD_STRIDE float64) in place.
     `uncertainty` (n x UNCERTAINTY_STRIDE float64, optional) receives the
-    uncertainty fields of every converged Gauss-Newton solve."""
+    uncertainty fields of every converged Gauss-Newton solve.  `neighbors`
+    (NEIGHBOR_ID per subset) serve params.initialization_method."""
+    if neighbors is not None:
+        neighbors = np.ascontiguousarray(neighbors, dtype=np.int32)
     if uncertainty is not None:
         assert uncertainty.dtype == np.float64 and uncertainty.flags.c_contiguous
         assert uncertainty.shape == (fields.shape[0], UNCERTAINTY_STRIDE)
@@ -100,7 +103,7 @@ def execute_frame(params, ref, deff, fields, first_frame=True, nthreads=1, offse
     rc = lib().oracle_execute_frame(ctypes.byref(params), w, h, _ptr(ref), _ptr(deff), n,
                                     _ptr(fields), _ptr(offsets), _ptr(px), _ptr(py),
                                     _ptr(force_simplex), 1 if first_frame else 0, nthreads,
-                                    _ptr(gn), _ptr(sx), _ptr(uncertainty))
+                                    _ptr(gn), _ptr(sx), _ptr(uncertainty), _ptr(neighbors))
     if rc != 0:
         raise RuntimeError("oracle_execute_frame failed: %d" % rc)
     if counters:

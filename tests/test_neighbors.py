@@ -1,0 +1,162 @@
+"""Neighbour initialization (USE_NEIGHBOR_VALUES, _FIRST_STEP_ONLY).
+
+Field_Value_Initializer::initial_guess (DICe_Initializer.cpp:398-436) takes a
+subset's initial guess from its NEIGHBOR_ID's field values; the reference
+runs the subsets in index order, so a chain of neighbours carries a seed's
+solution across a displacement too large for a zero start.  The oracle
+restates the rule; the GPU (dependency waves, chains as one sequential
+launch, a reverse chain in one wave reading frame-start values) equals it,
+and a captured two-frame sequence equals the frame calls.
+"""
+import numpy as np
+import pytest
+import torch
+
+from dice_b200 import abi
+from dice_b200 import synthetic as syn
+from dice_b200.subset_file import SubsetFile, regular_grid
+from oracle import oracle as O
+
+W, H = 200, 160
+U, V = 9.7, -7.4          # beyond the Gauss-Newton capture range from a zero start
+SEEDED = ("BEGIN REGION_OF_INTEREST\nBEGIN BOUNDARY\nBEGIN RECTANGLE\nCENTER 100 80\nWIDTH 200\nHEIGHT 160\n"
+          "END\nEND\nBEGIN SEED\nLOCATION 100 80\nDISPLACEMENT %g %g\nEND\nEND\n" % (U, V))
+
+
+def _images():
+    ref = syn.speckle_image(W, H, seed=31, blur_sigma=0.8)
+    f1 = syn.warp_image(ref, lambda X, Y: (torch.full_like(X, U), torch.full_like(Y, V)), noise_sigma=0.5, seed=7)
+    f2 = syn.warp_image(ref, lambda X, Y: (torch.full_like(X, U + 0.4), torch.full_like(Y, V - 0.3)),
+                        noise_sigma=0.5, seed=8)
+    return ref.numpy(), f1.numpy(), f2.numpy()
+
+
+def _grid(seeded):
+    sf = SubsetFile(text=SEEDED) if seeded else None
+    xy, neigh, seed = regular_grid(sf, W, H, 12, 21)
+    f = syn.init_fields(xy[:, 0], xy[:, 1])
+    f[seed >= 0, abi.F_DISP_X] = U
+    f[seed >= 0, abi.F_DISP_Y] = V
+    if not seeded:                     # the chains' first points carry the start
+        f[neigh < 0, abi.F_DISP_X] = U
+        f[neigh < 0, abi.F_DISP_Y] = V
+    return f, neigh
+
+
+def _params(method, **kw):
+    return abi.default_params(subset_size=21, optimization=abi.GRADIENT_BASED, initialization_method=method,
+                              fast_solver_tolerance=1e-5, **kw)
+
+
+def test_oracle_neighbor_chain_carries_the_seed():
+    ref, f1, _ = _images()
+    for seeded in (False, True):
+        f, neigh = _grid(seeded)
+        g = f.copy()
+        O.execute_frame(_params(abi.USE_NEIGHBOR_VALUES), ref, f1, g, neighbors=neigh)
+        ok = g[:, abi.F_SIGMA] >= 0
+        assert ok.mean() > 0.95
+        assert np.max(np.abs(g[ok, abi.F_DISP_X] - U)) < 0.05 and np.max(np.abs(g[ok, abi.F_DISP_Y] - V)) < 0.05
+        has = (neigh >= 0) & (neigh != np.arange(len(neigh)))
+        assert (g[has & ok, abi.F_STATUS] == 3).all() and (g[~has & ok, abi.F_STATUS] == 1).all()
+        # the same grid from field values: the zero starts do not reach the solution
+        h = f.copy()
+        O.execute_frame(_params(abi.USE_FIELD_VALUES), ref, f1, h, neighbors=neigh)
+        good = (h[:, abi.F_SIGMA] >= 0) & (np.abs(h[:, abi.F_DISP_X] - U) < 0.05)
+        assert good.mean() < 0.2
+
+
+def test_oracle_first_step_only_and_index_order():
+    ref, f1, f2 = _images()
+    f, neigh = _grid(False)
+    p = _params(abi.USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY)
+    O.execute_frame(p, ref, f1, f, first_frame=True, neighbors=neigh)
+    assert (f[neigh >= 0, abi.F_STATUS] == 3).all()
+    O.execute_frame(p, ref, f2, f, first_frame=False, neighbors=neigh)
+    ok = f[:, abi.F_SIGMA] >= 0
+    assert (f[ok, abi.F_STATUS] == 1).all() and np.max(np.abs(f[ok, abi.F_DISP_X] - U - 0.4)) < 0.05
+    # a reverse chain: every neighbour has a higher index, so each start is
+    # the neighbour's frame-start row (zeros): the chain does not carry
+    g, _ = _grid(False)
+    rev = np.append(np.arange(1, len(g)), -1).astype(np.int32)
+    g[0, abi.F_DISP_X] = g[0, abi.F_DISP_Y] = 0.0
+    g[-1, abi.F_DISP_X], g[-1, abi.F_DISP_Y] = U, V
+    O.execute_frame(_params(abi.USE_NEIGHBOR_VALUES), ref, f1, g, neighbors=rev)
+    good = (g[:, abi.F_SIGMA] >= 0) & (np.abs(g[:, abi.F_DISP_X] - U) < 0.05)
+    assert good[-1] and good[-2] and good.mean() < 0.2
+
+
+def _need_gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _device(p, ref, frames, f, neigh, capture=False):
+    from dice_b200.schema import Schema
+    rows = []
+    with Schema(p) as s:
+        s.set_ref_image(ref)
+        s.set_fields(f)
+        s.set_neighbors(neigh)
+        for d in frames:
+            s.set_def_image(d)
+            s.execute_correlation()
+            rows.append(s.fields())
+        if capture:
+            s.capture_sequence([torch.from_numpy(d).cuda() for d in frames], reset_fields=torch.from_numpy(f).cuda())
+            s.launch_sequence()
+            torch.cuda.synchronize()
+            assert np.array_equal(s.fields(), rows[-1])
+        assert s.device_status() == 0
+    return rows
+
+
+def _compare(got, want):
+    assert np.array_equal(got[:, abi.F_STATUS], want[:, abi.F_STATUS])
+    assert np.array_equal(got[:, abi.F_SIGMA] < 0, want[:, abi.F_SIGMA] < 0)
+    ok = want[:, abi.F_SIGMA] >= 0
+    assert np.max(np.abs(got[ok, abi.F_DISP_X:abi.F_DISP_Y + 1] - want[ok, abi.F_DISP_X:abi.F_DISP_Y + 1])) < 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["chain", "seeded_tree", "reverse", "quadratic"])
+def test_gpu_neighbor_initialization_matches_oracle(case):
+    _need_gpu()
+    ref, f1, _ = _images()
+    f, neigh = _grid(case == "seeded_tree")
+    p = _params(abi.USE_NEIGHBOR_VALUES)
+    if case == "reverse":
+        neigh = np.append(np.arange(1, len(f)), -1).astype(np.int32)
+        f[0, abi.F_DISP_X] = f[0, abi.F_DISP_Y] = 0.0
+        f[-1, abi.F_DISP_X], f[-1, abi.F_DISP_Y] = U, V
+    if case == "quadratic":
+        p = _params(abi.USE_NEIGHBOR_VALUES, shape_function=abi.QUADRATIC_SF)
+        f = syn.init_fields(f[:, abi.F_COORD_X], f[:, abi.F_COORD_Y], quadratic=True)
+        f[neigh < 0, abi.F_QUAD_A + 5] = U
+        f[neigh < 0, abi.F_QUAD_A + 11] = V
+    want = f.copy()
+    O.execute_frame(p, ref, f1, want, neighbors=neigh)
+    got = _device(p, ref, [f1], f, neigh)[0]
+    _compare(got, want)
+    if case in ("chain", "seeded_tree"):
+        assert (want[:, abi.F_SIGMA] >= 0).mean() > 0.95
+    if case == "quadratic":
+        # a subset that fails fails every later one on its chain
+        # (INITIALIZE_FAILED from the neighbour's sigma of -1)
+        assert ((want[:, abi.F_STATUS] == 3) & (want[:, abi.F_SIGMA] >= 0)).sum() > 40
+        assert (want[:, abi.F_STATUS] == 5).any()
+
+
+@pytest.mark.gpu
+def test_gpu_first_step_only_sequence_and_graph():
+    _need_gpu()
+    ref, f1, f2 = _images()
+    f, neigh = _grid(True)
+    p = _params(abi.USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY)
+    want = f.copy()
+    O.execute_frame(p, ref, f1, want, first_frame=True, neighbors=neigh)
+    w1 = want.copy()
+    O.execute_frame(p, ref, f2, want, first_frame=False, neighbors=neigh)
+    rows = _device(p, ref, [f1, f2], f, neigh, capture=True)
+    _compare(rows[0], w1)
+    _compare(rows[1], want)
