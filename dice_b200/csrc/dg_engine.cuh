@@ -1061,14 +1061,17 @@ struct Engine {
       record_failed(f, DICEGPU_INITIALIZE_FAILED, num_iterations);
       return;
     }
-    float guess[12];
-    load_slots_row(gv, guess);
-    if (SHAPE == DICEGPU_QUADRATIC_SF && init_status == DICEGPU_INITIALIZE_USING_NEIGHBOR_VALUE_SUCCESSFUL)
-      centroid_change(guess, __fsub_rn((float)fld(DICEGPU_F_COORD_X), (float)__shfl_sync(FULL, gv, DICEGPU_F_COORD_X)),
-                      __fsub_rn((float)fld(DICEGPU_F_COORD_Y), (float)__shfl_sync(FULL, gv, DICEGPU_F_COORD_Y)));
-#pragma unroll
-    for (int i = 0; i < 12; ++i) slots[i] = guess[i];
+    // the guess is rebuilt from its row for the fallback optimizer (a
+    // second initial_guess call in the reference) rather than kept in registers
     const int guess_status = init_status;
+    auto initial_guess = [&]() {
+      load_slots_row(gv, slots);
+      if (SHAPE == DICEGPU_QUADRATIC_SF && guess_status == DICEGPU_INITIALIZE_USING_NEIGHBOR_VALUE_SUCCESSFUL)
+        centroid_change(slots,
+                        __fsub_rn((float)fld(DICEGPU_F_COORD_X), (float)__shfl_sync(FULL, gv, DICEGPU_F_COORD_X)),
+                        __fsub_rn((float)fld(DICEGPU_F_COORD_Y), (float)__shfl_sync(FULL, gv, DICEGPU_F_COORD_Y)));
+    };
+    initial_guess();
     // reference mean at Gauss-Newton entry: over the pixels active at the last
     // deformed-state initialisation (none yet: all of them)
     bool have_state = false;
@@ -1135,14 +1138,12 @@ struct Engine {
       if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_GRADIENT_BASED || force_simplex) {
         second_failed = true;
       } else if (opt == DICEGPU_GRADIENT_BASED_THEN_SIMPLEX) {
-#pragma unroll
-        for (int i = 0; i < 12; ++i) slots[i] = guess[i];
+        initial_guess();
         init_status = guess_status;
         run_simplex();
         if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
       } else if (opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED) {
-#pragma unroll
-        for (int i = 0; i < 12; ++i) slots[i] = guess[i];
+        initial_guess();
         init_status = guess_status;
         run_gn();
         if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;

@@ -27,6 +27,9 @@ Sources (paths inside the DICe project):
       tests/regression/mechanism_{skip_solves, optical_flow}/subsets.txt
   tests/examples/obstruction/{images/obstruction_{01..12}.tif,
       gold/DICe_solution_{0,1}.txt}                                (200 x 200)
+  tests/regression/{parallel_seed_first_step_only, parallel_subsets_seed}/
+      {subset_file.dat, gold/DICe_solution_*.txt}
+  tests/regression/incremental/gold/DICe_solution_{0..5}.txt
 """
 import os
 import sys
@@ -147,6 +150,19 @@ def main(root):
     for i in range(2):
         with open(os.path.join(ex, "gold", "DICe_solution_%d.txt" % i)) as fh:
             out["obstruction_example_gold_text_%d" % i] = np.array(fh.read())
+    # seeded region-of-interest grids with neighbour initialization on the
+    # speckled pair (first step only: two frames; every step: one) and the
+    # incremental formulation on the synthetic speckle sequence
+    for name, frames in (("parallel_seed_first_step_only", 2), ("parallel_subsets_seed", 1)):
+        reg = os.path.join(root, "tests", "regression", name)
+        with open(os.path.join(reg, "subset_file.dat")) as fh:
+            out["subset_file_" + name] = np.array(fh.read())
+        for k in range(frames):
+            with open(os.path.join(reg, "gold", "DICe_solution_%d.txt" % k)) as fh:
+                out["%s_gold_text_%d" % (name, k)] = np.array(fh.read())
+    for k in range(6):
+        with open(os.path.join(root, "tests", "regression", "incremental", "gold", "DICe_solution_%d.txt" % k)) as fh:
+            out["incremental_gold_text_%d" % k] = np.array(fh.read())
     path =os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_gold.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, {k: v.shape for k, v in out.items()})

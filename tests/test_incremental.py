@@ -95,3 +95,57 @@ def test_gpu_incremental_matches_oracle(first_shift):
         assert np.array_equal(rows[k][:, abi.F_STATUS], want[k][:, abi.F_STATUS]), k
         assert np.max(np.abs(rows[k][:, abi.F_DISP_X:abi.F_DISP_Y + 1] -
                              want[k][:, abi.F_DISP_X:abi.F_DISP_Y + 1])) < 1e-4, k
+
+
+# ---- the reference's incremental regression ----------------------------------
+# tests/regression/incremental: one 39 x 39 subset at (42, 42), all six affine
+# parameters, Keys-4, Gauss-Newton, reference image defSyntheticSpeckled0 and
+# frames 0..5 shifted by 1 px per frame; the result file of frame k reports
+# the previous frame as its reference image.  DICe_Diff -t 0.05 -f 5.0E-5.
+def _incremental_regression():
+    from test_results import GOLD
+    from dice_b200.results import Output
+    frames = [GOLD["def_synthetic_%d" % k].astype(np.float32) for k in range(6)]
+    p = abi.default_params(subset_size=39, interpolation=abi.KEYS_FOURTH, optimization=abi.GRADIENT_BASED,
+                           use_incremental_formulation=1, enable_rotation=1, enable_normal_strain=1,
+                           enable_shear_strain=1, use_def_gradients=0)
+    out = Output(p, fields=["COORDINATE_X", "COORDINATE_Y", "DISPLACEMENT_X", "DISPLACEMENT_Y"], delimiter=",",
+                 omit_row_id=True)
+    return frames, p, out, [str(GOLD["incremental_gold_text_%d" % k]) for k in range(6)]
+
+
+def _check_incremental_files(tmp_path, out, rows, golds):
+    from test_results import REGRESSION_FLOOR, REGRESSION_TOL
+    from dice_b200.results import diff_text
+    for k, (r, gold) in enumerate(zip(rows, golds)):
+        out.set_images(ref_image="../../component/images/defSyntheticSpeckled%d.tif" % max(k - 1, 0),
+                       def_image="../../component/images/defSyntheticSpeckled%d.tif" % k)
+        out.write_frame(tmp_path, "DICe_solution", k, r, first_frame=0, num_frames=6, separate_files=False)
+        n, rep = diff_text(gold, open(tmp_path / ("DICe_solution_%d.txt" % k)).read(), tol=REGRESSION_TOL,
+                           floor=REGRESSION_FLOOR)
+        assert n == 0, rep
+
+
+def test_oracle_incremental_regression(tmp_path):
+    frames, p, out, golds = _incremental_regression()
+    rows = O.execute_sequence(p, frames[0], frames, syn.init_fields(np.array([42.0]), np.array([42.0])))
+    _check_incremental_files(tmp_path, out, rows, golds)
+
+
+@pytest.mark.gpu
+def test_gpu_incremental_regression(tmp_path):
+    _need_gpu()
+    from dice_b200.schema import Schema
+    frames, p, out, golds = _incremental_regression()
+    rows = []
+    with Schema(p) as s:
+        s.set_ref_image(frames[0])
+        s.set_fields(syn.init_fields(np.array([42.0]), np.array([42.0])))
+        for k, d in enumerate(frames):
+            if k > 0:
+                s.set_ref_from_def()
+            s.set_def_image(d)
+            s.execute_correlation()
+            rows.append(s.fields())
+        assert s.device_status() == 0
+    _check_incremental_files(tmp_path, out, rows, golds)

@@ -160,3 +160,76 @@ def test_gpu_first_step_only_sequence_and_graph():
     rows = _device(p, ref, [f1, f2], f, neigh, capture=True)
     _compare(rows[0], w1)
     _compare(rows[1], want)
+
+
+# ---- the reference's regressions ---------------------------------------------
+# parallel_seed_first_step_only (two frames) and parallel_subsets_seed (one):
+# four seeded 50 x 50 regions of interest on the speckled pair, step 10,
+# subset 27, neighbour initialization from the seeds along the grid's snakes,
+# Keys-4, GRADIENT_BASED_THEN_SIMPLEX, translation only, file-fed images
+# (reference gradients).  Checked with DICe_Diff -t 0.05 -f 5.0E-5.
+SEED_REGRESSIONS = {"parallel_seed_first_step_only": (abi.USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY, 2),
+                    "parallel_subsets_seed": (abi.USE_NEIGHBOR_VALUES, 1)}
+
+
+def _seed_regression(name):
+    from test_results import GOLD
+    method, nframes = SEED_REGRESSIONS[name]
+    sf = SubsetFile(text=str(GOLD["subset_file_" + name]))
+    p = abi.default_params(subset_size=27, initialization_method=method, use_def_gradients=0)
+    from dice_b200.results import Output
+    out = Output(p, fields=["COORDINATE_X", "COORDINATE_Y", "DISPLACEMENT_X", "DISPLACEMENT_Y", "SIGMA"],
+                 ref_image="../../component/images/refSpeckled.tif", step_size=(10, 10),
+                 initialization_method=["USE_FIELD_VALUES", "USE_NEIGHBOR_VALUES",
+                                        "USE_NEIGHBOR_VALUES_FIRST_STEP_ONLY"][method])
+    ref = GOLD["ref_speckled"].astype(np.float32)
+    deff = GOLD["def_speckled"].astype(np.float32)
+    golds = [str(GOLD["%s_gold_text_%d" % (name, k)]) for k in range(nframes)]
+    return sf, p, out, ref, deff, golds
+
+
+def _check_seed_files(tmp_path, out, rows, golds):
+    from test_results import REGRESSION_FLOOR, REGRESSION_TOL
+    from dice_b200.results import diff_text
+    for k, (r, gold) in enumerate(zip(rows, golds)):
+        # the second frame correlates a copy of the deformed image
+        out.set_images(def_image="../../component/images/%s.tif" % ("defSpeckled" if k == 0 else "defSpeckledCopy"))
+        out.write_frame(tmp_path, "DICe_solution", k, r, first_frame=0, num_frames=len(rows), separate_files=False)
+        n, rep = diff_text(gold, open(tmp_path / ("DICe_solution_%d.txt" % k)).read(), tol=REGRESSION_TOL,
+                           floor=REGRESSION_FLOOR)
+        assert n == 0, rep
+
+
+@pytest.mark.parametrize("name", sorted(SEED_REGRESSIONS))
+def test_oracle_seed_regressions(tmp_path, name):
+    sf, p, out, ref, deff, golds = _seed_regression(name)
+    xy, neigh, seed = regular_grid(sf, 512, 512, 10, 27)
+    f = syn.init_fields(xy[:, 0], xy[:, 1])
+    f[seed >= 0, abi.F_DISP_X] = 0.4      # the regions' seeds
+    f[seed >= 0, abi.F_DISP_Y] = 0.4
+    rows = []
+    for k in range(len(golds)):
+        O.execute_frame(p, ref, deff, f, first_frame=(k == 0), neighbors=neigh)
+        rows.append(f.copy())
+    # 4 seeds start from their own rows, the other 60 from their neighbours
+    assert (rows[0][:, abi.F_STATUS] == 3).sum() == 60
+    _check_seed_files(tmp_path, out, rows, golds)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(SEED_REGRESSIONS))
+def test_gpu_seed_regressions(tmp_path, name):
+    _need_gpu()
+    from dice_b200.schema import Schema
+    sf, p, out, ref, deff, golds = _seed_regression(name)
+    rows = []
+    with Schema(p) as s:
+        s.set_ref_image(ref)
+        sf.apply_grid(s, 512, 512, 10)    # grid, seeds and neighbours
+        for _ in golds:
+            s.set_def_image(deff)
+            s.execute_correlation()
+            rows.append(s.fields())
+        assert s.device_status() == 0
+    assert (rows[0][:, abi.F_STATUS] == 3).sum() == 60
+    _check_seed_files(tmp_path, out, rows, golds)
