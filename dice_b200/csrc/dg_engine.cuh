@@ -224,7 +224,7 @@ struct Engine {
   // One pass over the subset at the parameters in `slots` (see subset_pass).
   template <bool ACC_H, bool GRADS, bool MOMENTS>
   __device__ __forceinline__ PassOut pass(const SubsetRef& sb, const float* slots, double* /*C*/) {
-    PassIn in;
+    PassInMasked in;
     in.def = A.def;
     in.refI = A.ref.I;
     in.refgx = A.ref.gx;
@@ -251,14 +251,7 @@ struct Engine {
       in.pfv = sb.evo ? A.geo.pix_f : nullptr;
       return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, true>(in, k);
     }
-    in.mdesc = nullptr;
-    in.mbits = nullptr;
-    in.bpoly = nullptr;
-    in.bvx = nullptr;
-    in.bvy = nullptr;
-    in.pflag = nullptr;
-    in.pfv = nullptr;
-    return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, false>(in, k);
+    return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, false>(static_cast<const PassIn&>(in), k);
   }
 
   // Objective::gamma from the moments (Subset::gamma, DICe_Subset.cpp:323-340):

@@ -8,6 +8,8 @@
 // register allocation does not compete with the per-subset control code.
 #pragma once
 
+#include <type_traits>
+
 #include "dg_device.cuh"
 
 namespace dg {
@@ -97,21 +99,26 @@ struct PassIn {
   int half;        // square half-width (lists: unused)
   int cx, cy, npix, off;
   float K;         // intensity shift for the moment sums
-  // MASKED passes: this subset's mask descriptor (obstruction box x0, y0,
-  // w, h, word offset; blocked polygon count and table offset), the
-  // obstruction words, the blocked-polygon table (vertex offset, count, box
-  // x0, x1, y0, y1 per polygon) and the polygons' vertices
+};
+
+// What a MASKED pass reads besides (the unmasked passes get the plain
+// PassIn, which the call passes by value): this subset's mask descriptor
+// (obstruction box x0, y0, w, h, word offset; blocked polygon count and
+// table offset), the obstruction words, the blocked-polygon table (vertex
+// offset, count, box x0, x1, y0, y1 per polygon), the polygons' vertices,
+// and for evolving subsets the list pixels' evolution state (0 inactive, 1
+// active, 2 active with the reference intensity in pfv; nullptr otherwise).
+struct PassInMasked : PassIn {
   const int32_t* __restrict__ mdesc;
   const uint32_t* __restrict__ mbits;
   const int32_t* __restrict__ bpoly;
   const int32_t* __restrict__ bvx;
   const int32_t* __restrict__ bvy;
-  // MASKED passes of evolving subsets: the list pixels' evolution state
-  // (0 inactive, 1 active, 2 active with the reference intensity in pfv);
-  // nullptr otherwise
   const uint8_t* pflag;
   const float* pfv;
 };
+template <bool MASKED>
+using PassInT = typename std::conditional<MASKED, PassInMasked, PassIn>::type;
 
 // Whether pixel (px, py) is set in the mask box (x0, y0, w, h) at words.
 __device__ __forceinline__ bool mask_bit(const uint32_t* __restrict__ words, int x0, int y0, int w, int h,
@@ -162,7 +169,7 @@ struct MaskView {
 //             border test leaves, is_obstructed_pixel's rounding is the
 //             border test's
 template <int SHAPE, int INTERP, bool DEFGRAD, bool ACC_H, bool GRADS, bool MOMENTS, bool MASKED>
-__device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
+__device__ __noinline__ PassOut subset_pass(const PassInT<MASKED> in, const MapConst k) {
   using L = Layout<SHAPE>;
   const int lane = threadIdx.x & 31;
   const bool use_ref_grads = !DEFGRAD;
@@ -193,7 +200,7 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
   }
   const int x0 = in.cx - in.half, y0 = in.cy - in.half;
   MaskView mv;
-  if (MASKED) mv = MaskView(in.mdesc, in.mbits, in.bpoly, in.bvx, in.bvy);
+  if constexpr (MASKED) mv = MaskView(in.mdesc, in.mbits, in.bpoly, in.bvx, in.bvy);
   const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_smem<SHAPE>()->vbuf);
   for (int base = 0; base < in.npix; base += 32 * PPL) {
     float vv[PPL][L::VW];
@@ -226,10 +233,12 @@ __device__ __noinline__ PassOut subset_pass(const PassIn in, const MapConst k) {
       // subset evolution: an inactive pixel takes no part; a turned-on one
       // has its stored reference intensity
       bool active = true;
-      if (MASKED && in.pflag) {
-        const int st = in.pflag[in.off + p];
-        active = st != 0;
-        if (st == 2) F = in.pfv[in.off + p];
+      if constexpr (MASKED) {
+        if (in.pflag) {
+          const int st = in.pflag[in.off + p];
+          active = st != 0;
+          if (st == 2) F = in.pfv[in.off + p];
+        }
       }
       if (ACC_H && active) sumFall += F - in.K;
       // 4-pixel border deactivation (DICe_Subset.cpp:408)
