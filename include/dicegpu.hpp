@@ -86,6 +86,27 @@ class Schema {
     fresh_ = true;
   }
 
+  // Conformal subsets (Conformal_Area_Def shapes) and obstructing subsets
+  // (obstructing_subset_ids_ in CSR form: offsets[n + 1], ids).
+  void set_subset_shapes(const std::vector<dicegpu_shape>& shapes, const std::vector<int32_t>& vx,
+                         const std::vector<int32_t>& vy) {
+    check(dicegpu_set_subset_shapes(ctx_, (int)shapes.size(), shapes.data(), vx.empty() ? nullptr : vx.data(),
+                                    vy.empty() ? nullptr : vy.data()),
+          "dicegpu_set_subset_shapes");
+  }
+  void set_blocking(const std::vector<int32_t>& offsets, const std::vector<int32_t>& ids) {
+    check(dicegpu_set_blocking(ctx_, offsets.empty() ? nullptr : offsets.data(), ids.empty() ? nullptr : ids.data()),
+          "dicegpu_set_blocking");
+  }
+  // NEIGHBOR_ID per subset for the neighbour initializers.
+  void set_neighbors(const std::vector<int32_t>& ids) {
+    if ((int)ids.size() != n_) throw Error("set_neighbors: one id per subset", DICEGPU_ERR_ARG);
+    check(dicegpu_set_neighbors(ctx_, ids.data()), "dicegpu_set_neighbors");
+  }
+  // set_ref_image(prev_img()) of an incremental sequence: the current
+  // deformed image becomes the reference on the device.
+  void set_ref_from_def() { check(dicegpu_set_ref_from_def(ctx_), "dicegpu_set_ref_from_def"); }
+
   // One frame over every subset; returns 0 as Schema::execute_correlation does.
   int execute_correlation() {
     check(dicegpu_execute_correlation(ctx_), "dicegpu_execute_correlation");
