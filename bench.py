@@ -182,7 +182,7 @@ def cpu_sample(p, ref, frames, n_sample, nthreads, timed_frames=1):
 SIMPLEX_FLOP_PER_PIXEL_EVAL = 200.0
 # DRAM bytes (read + write) of one frame_kernel launch of this sequence, from
 # the ncu capture summarised in profiles/frame_kernel_2048x2048_31px_step5.md
-FRAME_KERNEL_DRAM_BYTES = 258.5e6 + 1949.2e6
+FRAME_KERNEL_DRAM_BYTES = 290.601472e6 + 2.078065e9   # ncu capture of one launch (read + write)
 
 
 def oracle_sequence_sample(p, ref_h, frames_h, stride, nthreads):
@@ -1111,7 +1111,7 @@ def main():
             "traffic": FRAME_KERNEL_DRAM_BYTES,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
                               "profiles/frame_kernel_2048x2048_31px_step5.md (writes are local-memory "
-                              "write-backs; reads 258.5 MB)",
+                              "write-backs; reads 290.6 MB)",
             "kernel": "frame_kernel (median step time incl. the gradient and pack kernels)",
             "peak_source": "measured FP32 SGEMM on CUDA cores (TF32 off) in this run",
             "per_unit": "390 FP32 flop per active pixel per Gauss-Newton pass + 200 per simplex evaluation, "
