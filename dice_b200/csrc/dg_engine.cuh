@@ -1,7 +1,8 @@
 // dg_engine.cuh -- the per-subset correlation engine, one warp per subset.
 //
 // Mirrors Schema::generic_correlation_routine (DICe_Schema.cpp:2026-2368)
-// for the USE_FIELD_VALUES initializer:
+// with the field-value initializer (the subset's own row, or its
+// neighbour's):
 //   initial guess -> Gauss-Newton (Objective_ZNSSD::computeUpdateFast,
 //   DICe_Objective.cpp:430-657) and/or Nelder-Mead (Simplex::minimize,
 //   DICe_Simplex.cpp:60-277) -> jump test -> sigma -> gamma -> record_step.

@@ -1087,7 +1087,8 @@ static float objective_beta(const Ctx& C, Subset& s, const ShapeFn& sf_in) {
 }
 
 // Schema::generic_correlation_routine (DICe_Schema.cpp:2026-2368) for one subset,
-// restricted to the USE_FIELD_VALUES initializer and local DIC.
+// restricted to the field-value initializer (own or neighbour row, nf) and
+// local DIC.
 static bool correlate_subset(const Ctx& C, Subset& s, double* f, bool first_frame,
                              bool force_simplex, Counters* cnt, const double* nf = nullptr) {
   const dicegpu_params& P = C.P;
