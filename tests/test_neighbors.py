@@ -233,3 +233,22 @@ def test_gpu_seed_regressions(tmp_path, name):
         assert s.device_status() == 0
     assert (rows[0][:, abi.F_STATUS] == 3).sum() == 60
     _check_seed_files(tmp_path, out, rows, golds)
+
+
+def test_oracle_rejects_other_initializers():
+    """Phase correlation, optical flow, feature matching and the other
+    initializers are outside the path: DICEGPU_ERR_UNSUPPORTED."""
+    ref, f1, _ = _images()
+    f, neigh = _grid(False)
+    for method in (3, 4, 5, 6):
+        with pytest.raises(RuntimeError, match=str(abi.ERR_UNSUPPORTED)):
+            O.execute_frame(_params(method), ref, f1, f.copy(), neighbors=neigh)
+
+
+def test_abi_rejects_other_initializers():
+    """dicegpu_create validates the params before any device call."""
+    import ctypes
+    lib = abi.load_library()
+    ctx = ctypes.c_void_p()
+    for method in (3, 4, 5, 6):
+        assert lib.dicegpu_create(ctypes.byref(_params(method)), ctypes.byref(ctx)) == abi.ERR_UNSUPPORTED
