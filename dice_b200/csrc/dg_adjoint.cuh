@@ -117,7 +117,7 @@ __device__ void adjoint_subset(const AdjointArgs& A, int idx) {
     const long ri = (long)y * A.ref.w + x;
     const double F = ri < rlim ? (double)__ldg(A.ref.I + ri) : 0.0;
     float G, gdum, hdum;
-    interp_interior<DICEGPU_KEYS_FOURTH, false>(A.def, mx, my, G, gdum, hdum);
+    keys_fast_interior<false>(A.def, mx, my, G, gdum, hdum);
     n += 1.0;
     sF += F;
     sF2 += F * F;

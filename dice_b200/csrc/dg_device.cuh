@@ -1,9 +1,9 @@
 // dg_device.cuh -- device building blocks of the subset-correlation path.
 //
-// Warp-per-subset design: one warp owns one subset at a time.  Lanes take
-// 32 subset pixels per step; warp-wide results come from shuffles and from
-// FP64 tensor-core accumulation (mma.sync m8n8k4 f64), so no block-level
-// synchronisation exists anywhere on the hot path.
+// Parameters and images as the kernels see them, warp reductions, the FP64
+// tensor-core accumulation, the interpolants (in the reference's arithmetic
+// for the correlation path, in a fused FP32 form for the adjoint), the shape
+// functions and the pixel rounding of Subset::initialize.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -132,8 +132,56 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
 //   |s| < 1 :  4/3|s|^3 - 7/3|s|^2 + 1
 //   |s| < 2 : -7/12|s|^3 + 3|s|^2 - 59/12|s| + 5/2
 //   |s| < 3 :  1/12|s|^3 - 2/3|s|^2 + 7/4|s| - 3/2
-// in Horner form, FP32.
+// Two evaluations.  The *_ref ones are the reference's arithmetic: the
+// kernel's coefficients as the 14-decimal literals it writes, products and
+// sums in double, left to right, each rounded on its own, the result rounded
+// to float.  The correlation path uses them, so that every interpolated value
+// is the reference's bit for bit.  The FP32 Horner forms below them serve the
+// adjoint, whose derivative pieces they match.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float keys_f0_ref(double s) {
+  const double a = __dmul_rn(__dmul_rn(__dmul_rn(1.33333333333333, s), s), s);
+  const double b = __dmul_rn(__dmul_rn(2.33333333333333, s), s);
+  return __double2float_rn(__dadd_rn(__dsub_rn(a, b), 1.0));
+}
+__device__ __forceinline__ float keys_f1_ref(double s) {
+  const double a = __dmul_rn(__dmul_rn(__dmul_rn(-0.58333333333333, s), s), s);
+  const double b = __dmul_rn(__dmul_rn(3.0, s), s);
+  const double c = __dmul_rn(4.91666666666666, s);
+  return __double2float_rn(__dadd_rn(__dsub_rn(__dadd_rn(a, b), c), 2.5));
+}
+__device__ __forceinline__ float keys_f2_ref(double s) {
+  const double a = __dmul_rn(__dmul_rn(__dmul_rn(0.08333333333333, s), s), s);
+  const double b = __dmul_rn(__dmul_rn(0.66666666666666, s), s);
+  const double c = __dmul_rn(1.75, s);
+  return __double2float_rn(__dsub_rn(__dadd_rn(__dsub_rn(a, b), c), 1.5));
+}
+// The six weights of one axis at fractional offset d = x - (int)x, in the
+// reference's argument order (DICe_Image.cpp:858-863), where each argument
+// (d + 2.0 and so on) is rounded to float before the kernel sees it.
+// Interior form: for x >= 2 the float spacing of x is at least 2^-22, so d
+// and every k +- d (k = 0..3) is a multiple of 2^-22 in [0, 3]: exact in
+// float, and the arguments can be formed in double from one conversion.
+__device__ __forceinline__ void keys_weights_ref_interior(float d, float w[6]) {
+  const double dd = (double)d;
+  w[0] = keys_f2_ref(__dadd_rn(dd, 2.0));
+  w[1] = keys_f1_ref(__dadd_rn(dd, 1.0));
+  w[2] = keys_f0_ref(dd);
+  w[3] = keys_f0_ref(__dsub_rn(1.0, dd));
+  w[4] = keys_f1_ref(__dsub_rn(2.0, dd));
+  w[5] = keys_f2_ref(__dsub_rn(3.0, dd));
+}
+// Any d >= 0: the arguments rounded to float first.  d + k and k - d are
+// exact in double, so the float sum is the reference's (float)(d + k.0).
+__device__ __forceinline__ void keys_weights_ref_general(float d, float w[6]) {
+  w[0] = keys_f2_ref((double)__fadd_rn(d, 2.0f));
+  w[1] = keys_f1_ref((double)__fadd_rn(d, 1.0f));
+  w[2] = keys_f0_ref((double)d);
+  w[3] = keys_f0_ref((double)__fsub_rn(1.0f, d));
+  w[4] = keys_f1_ref((double)__fsub_rn(2.0f, d));
+  w[5] = keys_f2_ref((double)__fsub_rn(3.0f, d));
+}
+
 __device__ __forceinline__ float keys0(float s) {
   return fmaf(fmaf(4.0f / 3.0f, s, -7.0f / 3.0f), s * s, 1.0f);
 }
@@ -151,21 +199,163 @@ __device__ __forceinline__ void keys_weights(float t, float w[6]) {
   w[4] = keys1(2.0f - t);
   w[5] = keys2(3.0f - t);
 }
-// Catmull-Rom (a = -1/2) weights: the separable form of the bicubic
-// polynomial of Image_::interpolate_bicubic_all (DICe_Image.cpp:493-636).
-__device__ __forceinline__ void cubic_weights(float t, float w[4]) {
-  const float t2 = t * t, t3 = t2 * t;
-  w[0] = 0.5f * (-t3 + 2.0f * t2 - t);
-  w[1] = 0.5f * (3.0f * t3 - 5.0f * t2 + 2.0f);
-  w[2] = 0.5f * (-3.0f * t3 + 4.0f * t2 + t);
-  w[3] = 0.5f * (t3 - t2);
+
+// ---------------------------------------------------------------------------
+// Reference-order interpolation (Image_::interpolate_*_all) at a point whose
+// taps all lie inside the image (the subset border test keeps every active
+// pixel at least 3.5 px from the edge, DICe_Subset.cpp:408).
+// ---------------------------------------------------------------------------
+// Keys-4 (DICe_Image.cpp:834-883): cc = wy[m] * wx[n] in float, then each
+// channel += cc * tap, m outer, n inner.  With gradients the taps come from
+// the interleaved (I, Gx, Gy, 0) image, one 16-byte load per tap.
+template <bool GRAD>
+__device__ __forceinline__ void keys_ref_interior(const DevImage& im, float x, float y, float& iv, float& gxv,
+                                                  float& gyv) {
+  const int ix = (int)x, iy = (int)y;
+  float wx[6], wy[6];
+  keys_weights_ref_interior(__fsub_rn(x, (float)ix), wx);
+  keys_weights_ref_interior(__fsub_rn(y, (float)iy), wy);
+  float a = 0.0f, b = 0.0f, c = 0.0f;
+  if (GRAD) {
+    const float4* q = im.p4 + (size_t)(iy - 2) * im.w + (ix - 2);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+#pragma unroll
+      for (int n = 0; n < 6; ++n) {
+        const float4 t = __ldg(q + n);
+        const float cc = __fmul_rn(wy[m], wx[n]);
+        a = __fadd_rn(a, __fmul_rn(cc, t.x));
+        b = __fadd_rn(b, __fmul_rn(cc, t.y));
+        c = __fadd_rn(c, __fmul_rn(cc, t.z));
+      }
+      q += im.w;
+    }
+  } else {
+    const float* q = im.I + (size_t)(iy - 2) * im.w + (ix - 2);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+#pragma unroll
+      for (int n = 0; n < 6; ++n) a = __fadd_rn(a, __fmul_rn(__fmul_rn(wy[m], wx[n]), __ldg(q + n)));
+      q += im.w;
+    }
+  }
+  iv = a;
+  gxv = b;
+  gyv = c;
 }
 
-// Interpolation at an interior point (the subset border test keeps every
-// active pixel at least 3.5 px from the image edge, so no tap leaves the
-// image: DICe_Subset.cpp:408).  Separable evaluation: a 6-tap (4-tap) row sum
-// per row, then the column sum.  With gradients the taps come from the
-// interleaved (I, Gx, Gy, 0) image, one 16-byte load per tap.
+// Bilinear (DICe_Image.cpp:394-425): value = I11 (x2-x)(y2-y) + I21 (x-x1)(y2-y)
+// + I22 (x-x1)(y-y1) + I12 (x2-x)(y-y1), each product left to right.
+__device__ __forceinline__ float bilinear_ref(const float* __restrict__ a, int w, int x1, int y1, float fx2,
+                                              float fx1, float fy2, float fy1) {
+  const float* r1 = a + (size_t)y1 * w + x1;
+  const float* r2 = r1 + w;
+  float v = __fmul_rn(__fmul_rn(__ldg(r1), fx2), fy2);
+  v = __fadd_rn(v, __fmul_rn(__fmul_rn(__ldg(r1 + 1), fx1), fy2));
+  v = __fadd_rn(v, __fmul_rn(__fmul_rn(__ldg(r2 + 1), fx1), fy1));
+  v = __fadd_rn(v, __fmul_rn(__fmul_rn(__ldg(r2), fx2), fy1));
+  return v;
+}
+
+// Bicubic (DICe_Image.cpp:493-636).  The reference writes the Catmull-Rom
+// (a = -1/2) bicubic as its expanded polynomial in x and y: the coefficient
+// of x^a y^b is sum_{n,m} c_a[n] c_b[m] f(n, m) over the 4 x 4 taps, with the
+// kernel's power-coefficient vectors
+//   c_0 = (0, 1, 0, 0), c_1 = (-1/2, 0, 1/2, 0),
+//   c_2 = (1, -5/2, 2, -1/2), c_3 = (-1/2, 3/2, -3/2, 1/2)
+// (tap offsets -1, 0, 1, 2).  Each coefficient is summed over its nonzero
+// terms, x tap outer and y tap inner, and the value is
+//   f00 + C01 y + C02 y^2 + C03 y^3 + sum_{a=1..3} (Ca0 + Ca1 y + Ca2 y^2 + Ca3 y^3) x^a,
+// every product and sum in float, left to right: the reference's order.
+__device__ __forceinline__ float cr_coef(int a, int n) {
+  // c_a[n] for a, n in 0..3 (compile-time after unrolling)
+  return a == 0 ? (n == 1 ? 1.0f : 0.0f)
+       : a == 1 ? (n == 0 ? -0.5f : n == 2 ? 0.5f : 0.0f)
+       : a == 2 ? (n == 0 ? 1.0f : n == 1 ? -2.5f : n == 2 ? 2.0f : -0.5f)
+                : (n == 0 ? -0.5f : n == 1 ? 1.5f : n == 2 ? -1.5f : 0.5f);
+}
+// f[n][m]: tap at x offset n - 1, y offset m - 1
+__device__ __forceinline__ float bicubic_group(const float f[4][4], int a, int b) {
+  float s = 0.0f;
+  bool first = true;
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const float cf = cr_coef(a, n) * cr_coef(b, m);   // exact: products of the coefficients above
+      if (cf == 0.0f) continue;
+      const float t = __fmul_rn(cf, f[n][m]);
+      s = first ? t : __fadd_rn(s, t);
+      first = false;
+    }
+  return s;
+}
+__device__ __forceinline__ float bicubic_eval(const float f[4][4], float x, float y) {
+  const float x2 = __fmul_rn(x, x), x3 = __fmul_rn(x2, x);
+  const float y2 = __fmul_rn(y, y), y3 = __fmul_rn(y2, y);
+  float v = f[1][1];
+  v = __fadd_rn(v, __fmul_rn(bicubic_group(f, 0, 1), y));
+  v = __fadd_rn(v, __fmul_rn(bicubic_group(f, 0, 2), y2));
+  v = __fadd_rn(v, __fmul_rn(bicubic_group(f, 0, 3), y3));
+  const float xp[4] = {1.0f, x, x2, x3};
+#pragma unroll
+  for (int a = 1; a < 4; ++a) {
+    float g = bicubic_group(f, a, 0);
+    g = __fadd_rn(g, __fmul_rn(bicubic_group(f, a, 1), y));
+    g = __fadd_rn(g, __fmul_rn(bicubic_group(f, a, 2), y2));
+    g = __fadd_rn(g, __fmul_rn(bicubic_group(f, a, 3), y3));
+    v = __fadd_rn(v, __fmul_rn(g, xp[a]));
+  }
+  return v;
+}
+template <bool GRAD>
+__device__ __forceinline__ void bicubic_ref_interior(const DevImage& im, float lx, float ly, float& iv, float& gxv,
+                                                     float& gyv) {
+  const int x0 = (int)lx, y0 = (int)ly;
+  const float x = __fsub_rn(lx, (float)x0), y = __fsub_rn(ly, (float)y0);
+  float f[4][4];
+  const size_t base = (size_t)(y0 - 1) * im.w + (x0 - 1);
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int m = 0; m < 4; ++m) f[n][m] = __ldg(im.I + base + (size_t)m * im.w + n);
+  iv = bicubic_eval(f, x, y);
+  if (GRAD) {
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int m = 0; m < 4; ++m) f[n][m] = __ldg(im.gx + base + (size_t)m * im.w + n);
+    gxv = bicubic_eval(f, x, y);
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int m = 0; m < 4; ++m) f[n][m] = __ldg(im.gy + base + (size_t)m * im.w + n);
+    gyv = bicubic_eval(f, x, y);
+  }
+}
+
+// Interpolation of the correlation path in the reference's arithmetic.
+template <int INTERP, bool GRAD>
+__device__ __forceinline__ void interp_ref(const DevImage& im, float x, float y, float& iv, float& gxv,
+                                           float& gyv) {
+  if (INTERP == DICEGPU_KEYS_FOURTH) {
+    keys_ref_interior<GRAD>(im, x, y, iv, gxv, gyv);
+  } else if (INTERP == DICEGPU_BICUBIC) {
+    bicubic_ref_interior<GRAD>(im, x, y, iv, gxv, gyv);
+  } else {
+    const int x1 = (int)x, y1 = (int)y;
+    const float fx2 = __fsub_rn((float)(x1 + 1), x), fx1 = __fsub_rn(x, (float)x1);
+    const float fy2 = __fsub_rn((float)(y1 + 1), y), fy1 = __fsub_rn(y, (float)y1);
+    iv = bilinear_ref(im.I, im.w, x1, y1, fx2, fx1, fy2, fy1);
+    if (GRAD) {
+      gxv = bilinear_ref(im.gx, im.w, x1, y1, fx2, fx1, fy2, fy1);
+      gyv = bilinear_ref(im.gy, im.w, x1, y1, fx2, fx1, fy2, fy1);
+    }
+  }
+}
+
+// FP32 separable evaluation (fused multiply-adds, a row sum per row), the
+// adjoint's forward map.
 template <int R, bool GRAD>
 __device__ __forceinline__ void conv_taps(const DevImage& im, int x0, int y0, const float* wx,
                                           const float* wy, float& iv, float& gxv, float& gyv) {
@@ -204,28 +394,24 @@ __device__ __forceinline__ void conv_taps(const DevImage& im, int x0, int y0, co
   iv = a;
 }
 
-template <int INTERP, bool GRAD>
-__device__ __forceinline__ void interp_interior(const DevImage& im, float x, float y, float& iv,
-                                                float& gxv, float& gyv) {
+// Keys-4 in the separable FP32 form (the adjoint's forward map).
+template <bool GRAD>
+__device__ __forceinline__ void keys_fast_interior(const DevImage& im, float x, float y, float& iv, float& gxv,
+                                                   float& gyv) {
   const int ix = (int)x, iy = (int)y;
-  if (INTERP == DICEGPU_KEYS_FOURTH) {
-    float wx[6], wy[6];
-    keys_weights(x - (float)ix, wx);
-    keys_weights(y - (float)iy, wy);
-    conv_taps<6, GRAD>(im, ix - 2, iy - 2, wx, wy, iv, gxv, gyv);
-  } else if (INTERP == DICEGPU_BICUBIC) {
-    float wx[4], wy[4];
-    cubic_weights(x - (float)ix, wx);
-    cubic_weights(y - (float)iy, wy);
-    conv_taps<4, GRAD>(im, ix - 1, iy - 1, wx, wy, iv, gxv, gyv);
-  } else {
-    // Image_::interpolate_bilinear_all (DICe_Image.cpp:394-425), interior form
-    const float fx1 = (float)(ix + 1) - x, fx0 = x - (float)ix;
-    const float fy1 = (float)(iy + 1) - y, fy0 = y - (float)iy;
-    const float wx[2] = {fx1, fx0}, wy[2] = {fy1, fy0};
-    conv_taps<2, GRAD>(im, ix, iy, wx, wy, iv, gxv, gyv);
-  }
+  float wx[6], wy[6];
+  keys_weights(x - (float)ix, wx);
+  keys_weights(y - (float)iy, wy);
+  conv_taps<6, GRAD>(im, ix - 2, iy - 2, wx, wy, iv, gxv, gyv);
 }
+
+// Float cosine, sine and arc cosine as the double functions rounded to float:
+// correctly rounded but for arguments within about 2^-28 ulp of a rounding
+// boundary, like the C library's float versions the reference calls
+// (std::cos(float) and so on), so both sides agree on the float values.
+__device__ __forceinline__ float cos_f(float t) { return (float)cos((double)t); }
+__device__ __forceinline__ float sin_f(float t) { return (float)sin((double)t); }
+__device__ __forceinline__ float acos_f(float t) { return (float)acos((double)t); }
 
 // ---------------------------------------------------------------------------
 // Shape functions.
@@ -288,9 +474,9 @@ __device__ __forceinline__ void residuals_D(const MapConst& k, float dx, float d
     Gy = k.rsin * gx + k.rcos * gy;
   }
   if (SHAPE == DICEGPU_QUADRATIC_SF) {
-    const float dxdy = dx * dy, dx2 = dx * dx, dy2 = dy * dy;
-    r[0] = Gx * dx; r[1] = Gx * dy; r[2] = Gx * dxdy; r[3] = Gx * dx2; r[4] = Gx * dy2; r[5] = Gx;
-    r[6] = Gy * dx; r[7] = Gy * dy; r[8] = Gy * dxdy; r[9] = Gy * dx2; r[10] = Gy * dy2; r[11] = Gy;
+    // Gx*dx*dy is (Gx*dx)*dy, left to right, as the reference writes it
+    r[0] = Gx * dx; r[1] = Gx * dy; r[2] = Gx * dx * dy; r[3] = Gx * dx * dx; r[4] = Gx * dy * dy; r[5] = Gx;
+    r[6] = Gy * dx; r[7] = Gy * dy; r[8] = Gy * dx * dy; r[9] = Gy * dx * dx; r[10] = Gy * dy * dy; r[11] = Gy;
   } else {
     const float c = k.cost, s = k.sint;
     r[0] = Gx;
@@ -343,9 +529,9 @@ __device__ __forceinline__ void residuals(const MapConst& k, float x, float y, f
     Gy = k.rsin * gx + k.rcos * gy;
   }
   if (SHAPE == DICEGPU_QUADRATIC_SF) {
-    const float dxdy = dx * dy, dx2 = dx * dx, dy2 = dy * dy;
-    r[0] = Gx * dx; r[1] = Gx * dy; r[2] = Gx * dxdy; r[3] = Gx * dx2; r[4] = Gx * dy2; r[5] = Gx;
-    r[6] = Gy * dx; r[7] = Gy * dy; r[8] = Gy * dxdy; r[9] = Gy * dx2; r[10] = Gy * dy2; r[11] = Gy;
+    // Gx*dx*dy is (Gx*dx)*dy, left to right, as the reference writes it
+    r[0] = Gx * dx; r[1] = Gx * dy; r[2] = Gx * dx * dy; r[3] = Gx * dx * dx; r[4] = Gx * dy * dy; r[5] = Gx;
+    r[6] = Gy * dx; r[7] = Gy * dy; r[8] = Gy * dx * dy; r[9] = Gy * dx * dx; r[10] = Gy * dy * dy; r[11] = Gy;
   } else {
     float Dx, Dy;
     affine_D(k, dx, dy, Dx, Dy);
@@ -372,7 +558,7 @@ __device__ __forceinline__ void map_to_u_v_theta(const MapConst& k, float cx, fl
     const float ax = rxp - cxp, ay = ryp - cyp;
     const float mag_a = sqrtf(ax * ax + ay * ay);
     const float adb = (ax * 5.0f + ay * 0.0f) / (mag_a * 5.0f);
-    t = ay < 0.0f ? (float)(6.28318530717958647692 - (double)acosf(adb)) : acosf(adb);
+    t = ay < 0.0f ? (float)(6.28318530717958647692 - (double)acos_f(adb)) : acos_f(adb);
   } else {
     u = k.s[0];
     v = k.s[1];
@@ -391,12 +577,12 @@ __device__ __forceinline__ void make_mapconst(const float* slots, bool use_ref_g
     if (use_ref_grads) {
       float u, v, t;
       map_to_u_v_theta<SHAPE>(k, cx, cy, u, v, t);
-      k.rcos = cosf(t);
-      k.rsin = sinf(t);
+      k.rcos = cos_f(t);
+      k.rsin = sin_f(t);
     }
   } else {
-    k.cost = cosf(slots[2]);
-    k.sint = sinf(slots[2]);
+    k.cost = cos_f(slots[2]);
+    k.sint = sin_f(slots[2]);
     k.rcos = k.cost;
     k.rsin = k.sint;
   }

@@ -1,4 +1,4 @@
-// dg_engine.cuh -- the per-subset correlation engine, one warp per subset.
+// dg_engine.cuh -- the per-subset correlation engine, one CTA per subset.
 //
 // Mirrors Schema::generic_correlation_routine (DICe_Schema.cpp:2026-2368)
 // with the field-value initializer (the subset's own row, or its
@@ -7,14 +7,17 @@
 //   DICe_Objective.cpp:430-657) and/or Nelder-Mead (Simplex::minimize,
 //   DICe_Simplex.cpp:60-277) -> jump test -> sigma -> gamma -> record_step.
 //
-// Data flow per Gauss-Newton iteration (one "pass" over the subset pixels):
-//   lane <- pixel;  warp (map) -> round + border test -> interpolation of
-//   I (+ Gx, Gy) -> residual vector r (FP32) -> v = [r, G-F, 1]
-//   -> sum v v^T with FP64 tensor-core mma (exact products of FP32 values,
-//   FP64 sums).  The 8x8 (affine) / 16x16 (quadratic) result holds
-//   H = sum r r^T, sum r (G-F), sum r, sum (G-F) and the active count, from
-//   which the reference's q = sum r ((G - meanG) - (F - meanF)) follows as
-//   sum r (G-F) - (meanG - meanF) sum r.
+// Every thread of the CTA runs this control code on the same values (the
+// parameters, the pass results broadcast through shared memory), so all of
+// them take the same branches and meet at the same barriers; the passes
+// split the subset's pixels across the CTA (dg_pass.cuh).  The Gauss-Newton
+// solve runs in warp 0 and is broadcast; one thread writes the field row.
+//
+// The arithmetic is the reference's: float where it computes in float, each
+// operation rounded on its own (the library is compiled without contraction),
+// sums in the reference's order where it sums in float, the FP64 LU factors
+// and explicit inverse of LAPACK's DGETRF / DGETRI (unblocked order), and the
+// parameter update accumulated in float.
 #pragma once
 
 #include "dg_pass.cuh"
@@ -33,6 +36,9 @@ struct FrameArgs {
   DevGeometry geo;
   double* fields;        // n x DICEGPU_FIELD_STRIDE
   int n;
+  int npix_cap;          // per-pixel array capacity (>= every subset's pixel count)
+  unsigned char* pix_scratch;   // per-CTA pixel arrays in global memory (null: shared memory)
+  size_t pix_stride;            // bytes per CTA in pix_scratch
   int first_frame;
   int mode;
   int plain_index;       // >= 0: this launch processes only that subset (plain path)
@@ -55,7 +61,8 @@ struct FrameArgs {
 
 // Image_::interpolate_keys_fourth (DICe_Image.cpp:890-924), intensity only:
 // the bilinear value (Image_::interpolate_bilinear, :432-445) near the
-// border, the 6 x 6 Keys sum (rows outer) elsewhere.
+// border, the 6 x 6 Keys sum (rows outer) elsewhere, in the reference's
+// arithmetic.
 __device__ __forceinline__ float keys_intensity(const DevImage& im, float lx, float ly) {
   const int w = im.w, h = im.h;
   const float* __restrict__ I = im.I;
@@ -68,132 +75,14 @@ __device__ __forceinline__ float keys_intensity(const DevImage& im, float lx, fl
            __ldg(I + (size_t)y2 * w + x2) * (lx - (float)x1) * (ly - (float)y1) +
            __ldg(I + (size_t)y2 * w + x1) * ((float)x2 - lx) * (ly - (float)y1);
   }
-  const int ix = (int)lx, iy = (int)ly;
-  float wx[6], wy[6];
-  keys_weights(lx - (float)ix, wx);
-  keys_weights(ly - (float)iy, wy);
-  float v = 0.0f;
-#pragma unroll
-  for (int m = 0; m < 6; ++m) {
-    const float* row = I + (size_t)(iy - 2 + m) * w + ix - 2;
-#pragma unroll
-    for (int n = 0; n < 6; ++n) v += wy[m] * wx[n] * __ldg(row + n);
-  }
-  return v;
-}
-
-struct AffineStep {
-  float upd[6];   // parameter update per slot (0 for disabled slots)
-  float cond;     // 2x2 condition number of the displacement block
-};
-
-// Gauss-Newton step of the affine system, computed by every lane on its own
-// copy (no shuffles, all in registers).  `M` is the accumulated 8x8 matrix of
-// [r(6 slots), G-F, 1]; `em` the mask of enabled slots.  Mirrors
-// DICe_Objective.cpp:548-607: LM penalty, the 2x2 condition number in the
-// reference's float/double mix, LU with partial pivoting in DGETRF order
-// (first maximal pivot, reciprocal scaling, rank-1 updates), then
-// update = -H^-1 q, or -LU q when a pivot is exactly zero (DGETRI returns
-// early and the factors are used as the inverse).
-static __device__ __noinline__ AffineStep solve_affine(const double* __restrict__ M, double cshift,
-                                                unsigned em, float lm_alpha) {
-  double H[6][6], q[6], q0[6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    const bool ei = (em >> i) & 1u;
-#pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      const bool ej = (em >> j) & 1u;
-      H[i][j] = (ei && ej) ? M[i * 8 + j] : (i == j ? 1.0 : 0.0);
-    }
-    q[i] = ei ? M[i * 8 + 6] - cshift * M[i * 8 + 7] : 0.0;
-    q0[i] = q[i];
-  }
-  if (lm_alpha > 0.0f) {
-    H[0][0] += (double)lm_alpha;
-    H[1][1] += (double)lm_alpha;
-  }
-  AffineStep out;
-  {
-    const double nsq = H[0][0] * H[0][0] + H[0][1] * H[0][1] + H[1][0] * H[1][0] + H[1][1] * H[1][1];
-    const float det_h = (float)(H[0][0] * H[1][1] - H[1][0] * H[0][1]);
-    const float norm_H = (float)sqrt(nsq);
-    float cond = -1.0f;
-    if (det_h != 0.0f) {
-      const float dd = __fmul_rn(det_h, det_h);
-      cond = norm_H * (float)sqrt((1.0 / (double)dd) * nsq);
-    }
-    out.cond = cond;
-  }
-  int info = 0;
-#pragma unroll
-  for (int j = 0; j < 6; ++j) {
-    int p = j;
-    double best = fabs(H[j][j]);
-#pragma unroll
-    for (int i = j + 1; i < 6; ++i) {
-      const double a = fabs(H[i][j]);
-      if (a > best) { best = a; p = i; }
-    }
-    double pv = H[j][j];
-#pragma unroll
-    for (int i = j + 1; i < 6; ++i)
-      if (i == p) pv = H[i][j];
-    if (pv != 0.0) {
-#pragma unroll
-      for (int i = j + 1; i < 6; ++i) {
-        if (i == p) {
-#pragma unroll
-          for (int k = 0; k < 6; ++k) {
-            const double t = H[j][k];
-            H[j][k] = H[i][k];
-            H[i][k] = t;
-          }
-          const double t = q[j];
-          q[j] = q[i];
-          q[i] = t;
-        }
-      }
-      const double r = 1.0 / pv;
-#pragma unroll
-      for (int i = j + 1; i < 6; ++i) H[i][j] *= r;
-    } else if (info == 0) {
-      info = j + 1;
-    }
-#pragma unroll
-    for (int i = j + 1; i < 6; ++i) {
-#pragma unroll
-      for (int k = j + 1; k < 6; ++k) H[i][k] -= H[i][j] * H[j][k];
-      q[i] -= H[i][j] * q[j];
-    }
-  }
-  if (info == 0) {
-    double x[6];
-#pragma unroll
-    for (int j = 5; j >= 0; --j) {
-      double s = q[j];
-#pragma unroll
-      for (int k = j + 1; k < 6; ++k) s -= H[j][k] * x[k];
-      x[j] = s / H[j][j];
-    }
-#pragma unroll
-    for (int i = 0; i < 6; ++i) out.upd[i] = (float)(-x[i]);
-  } else {
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      float u = 0.0f;
-#pragma unroll
-      for (int j = 0; j < 6; ++j) u = (float)((double)u + H[i][j] * (-1.0) * q0[j]);
-      out.upd[i] = u;
-    }
-  }
-  return out;
+  float iv, a, b;
+  keys_ref_interior<false>(im, lx, ly, iv, a, b);
+  return iv;
 }
 
 struct SubsetRef {
   int idx, cx, cy, npix;
   int off;          // list offset (-1 for squares)
-  float K;          // intensity shift for the moment sums
   bool masked;      // has an obstruction bitmap, blocked polygons or evolution state
   bool evo;         // evolving: its list keeps inactive pixels (per-pixel state)
   int nact;         // pixels with is_active set (npix unless evolving)
@@ -203,10 +92,14 @@ template <int SHAPE, int INTERP, bool DEFGRAD, bool MASK>
 struct Engine {
   using L = Layout<SHAPE>;
   const FrameArgs& A;
-  const int lane;
+  const int tid, lane, warp, T;
   int npass_ = 0;   // pixel passes of the current subset (for work accounting)
 
-  __device__ explicit Engine(const FrameArgs& a) : A(a), lane(threadIdx.x & 31) {}
+  __device__ explicit Engine(const FrameArgs& a)
+      : A(a), tid(threadIdx.x), lane(threadIdx.x & 31), warp(threadIdx.x >> 5), T(blockDim.x) {}
+
+  __device__ __forceinline__ float* pix() const { return pix_base<SHAPE>(A.pix_scratch, A.pix_stride); }
+  __device__ __forceinline__ PixArrays arrays() const { return pix_arrays_at(pix(), A.npix_cap); }
 
   __device__ __forceinline__ void pixel_xy(const SubsetRef& sb, int p, int& x, int& y) const {
     if (sb.off < 0) {
@@ -222,9 +115,7 @@ struct Engine {
     y = y < 0 ? 0 : y;
   }
 
-  // One pass over the subset at the parameters in `slots` (see subset_pass).
-  template <bool ACC_H, bool GRADS, bool MOMENTS>
-  __device__ __forceinline__ PassOut pass(const SubsetRef& sb, const float* slots, double* /*C*/) {
+  __device__ __forceinline__ PassInMasked make_in(const SubsetRef& sb) const {
     PassInMasked in;
     in.def = A.def;
     in.refI = A.ref.I;
@@ -239,9 +130,15 @@ struct Engine {
     in.cy = sb.cy;
     in.npix = sb.npix;
     in.off = sb.off;
-    in.K = sb.K;
-    MapConst k;
-    make_mapconst<SHAPE>(slots, !DEFGRAD, (float)sb.cx, (float)sb.cy, k);
+    in.cap = A.npix_cap;
+    in.pix = pix();
+    in.mdesc = nullptr;
+    in.mbits = nullptr;
+    in.bpoly = nullptr;
+    in.bvx = nullptr;
+    in.bvy = nullptr;
+    in.pflag = nullptr;
+    in.pfv = nullptr;
     if (MASK && sb.masked) {
       in.mdesc = A.geo.mask_desc + (size_t)sb.idx * DG_MASK_DESC;
       in.mbits = A.geo.mask_bits;
@@ -250,38 +147,73 @@ struct Engine {
       in.bvy = A.geo.blocked_vy;
       in.pflag = sb.evo ? A.geo.pix_flag : nullptr;
       in.pfv = sb.evo ? A.geo.pix_f : nullptr;
-      return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, true>(in, k);
     }
-    return subset_pass<SHAPE, INTERP, DEFGRAD, ACC_H, GRADS, MOMENTS, false>(static_cast<const PassIn&>(in), k);
+    return in;
   }
 
-  // Objective::gamma from the moments (Subset::gamma, DICe_Subset.cpp:323-340):
-  // gamma = sum ((G-mG)/|G-mG| - (F-mF)/|F-mF|)^2 = 2 - 2 cov / (|G-mG| |F-mF|).
-  __device__ float gamma_from(const PassOut& o, int npix) const {
-    if (o.n == 0) return -1.0f;
-    const double n = (double)o.n;
-    const double sgg = o.sG2 - o.sG * o.sG / n;
-    const double sff = o.sF2 - o.sumF * o.sumF / n;
-    const double sgf = o.sGF - o.sG * o.sumF / n;
-    if (!(sgg > 0.0) || !(sff > 0.0)) return -1.0f;
-    double g = 2.0 - 2.0 * sgf / sqrt(sgg * sff);
-    if (g < 0.0) g = 0.0;
-    float gf = (float)g;
-    if (A.P.normalize_gamma && npix > 0) gf /= (float)npix;
-    return gf;
-  }
-
-  __device__ float eval_gamma(const SubsetRef& sb, const float* slots, PassOut* out = nullptr) {
-    PassOut o = pass<false, false, true>(sb, slots, nullptr);
-    if (out) *out = o;
+  // One pass over the subset at the parameters in `slots` (see cta_pass).
+  template <int KIND>
+  __device__ __forceinline__ void pass(const SubsetRef& sb, const float* slots) {
+    MapConst k;
+    make_mapconst<SHAPE>(slots, !DEFGRAD, (float)sb.cx, (float)sb.cy, k);
+    const PassInMasked in = make_in(sb);
+    if (MASK && sb.masked) {
+      cta_pass<SHAPE, INTERP, DEFGRAD, KIND, true>(in, k);
+    } else {
+      cta_pass<SHAPE, INTERP, DEFGRAD, KIND, false>(static_cast<const PassIn&>(in), k);
+    }
     ++npass_;
-    return gamma_from(o, sb.nact);
   }
 
-  __device__ void compact_to_slots(const float* comp, float* slots, const float* base) const {
-#pragma unroll
-    for (int i = 0; i < 12; ++i) slots[i] = base[i];
-    for (int k = 0; k < A.P.N; ++k) slots[A.P.slot[k]] = comp[k];
+  // Subset::gamma (DICe_Subset.cpp:323-340) over the live pixels of the last
+  // pass: mean and root sum of squares of F and of G, then the sum of
+  // squared differences of the normalised intensities, each a float sum in
+  // pixel order.  `def_sum2` receives the deformed sum of squares before
+  // its root (Subset::contrast_std_dev forms the same sum).  Uses GX, GY as
+  // scratch.
+  __device__ float gamma_exact(const SubsetRef& sb, float* def_sum2 = nullptr) {
+    const PixArrays X = arrays();
+    const int n = ctl().n;
+    const int np = sb.npix;
+    float s[2];
+    // mean(REF_INTENSITIES), mean(DEF_INTENSITIES) (:285-301); G is 0 at
+    // pixels that are not live
+    chains(2, X.F, X.G, nullptr, nullptr, X.L, 0x0101u, np, s);
+    const float mr = n ? __fdiv_rn(s[0], (float)n) : 0.0f;
+    const float md = n ? __fdiv_rn(s[1], (float)n) : 0.0f;
+    for (int p = tid; p < np; p += T) {
+      float a = 0.0f, b = 0.0f;
+      if (X.L[p] & 1) {
+        const float fa = __fsub_rn(X.F[p], mr), gb = __fsub_rn(X.G[p], md);
+        a = __fmul_rn(fa, fa);
+        b = __fmul_rn(gb, gb);
+      }
+      X.GX[p] = a;
+      X.GY[p] = b;
+    }
+    chains(2, X.GX, X.GY, nullptr, nullptr, nullptr, 0u, np, s);
+    if (def_sum2) *def_sum2 = s[1];
+    const float sr = __fsqrt_rn(s[0]), sd = __fsqrt_rn(s[1]);
+    if (sr == 0.0f || sd == 0.0f) return -1.0f;
+    for (int p = tid; p < np; p += T) {
+      float t = 0.0f;
+      if (X.L[p] & 1) {
+        const float val = __fsub_rn(__fdiv_rn(__fsub_rn(X.G[p], md), sd), __fdiv_rn(__fsub_rn(X.F[p], mr), sr));
+        t = __fmul_rn(val, val);
+      }
+      X.GX[p] = t;
+    }
+    chains(1, X.GX, nullptr, nullptr, nullptr, nullptr, 0u, np, s);
+    return s[0];
+  }
+
+  // Objective::gamma (DICe_Objective.cpp:58-76): initialise, Subset::gamma,
+  // optionally divided by the number of active pixels (in double).
+  __device__ float eval_gamma(const SubsetRef& sb, const float* slots, bool normalize, float* def_sum2 = nullptr) {
+    pass<PK_GAMMA>(sb, slots);
+    float g = gamma_exact(sb, def_sum2);
+    if (normalize && sb.nact > 0) g = (float)((double)g / (double)sb.nact);
+    return g;
   }
 
   __device__ __forceinline__ unsigned enabled_mask() const {
@@ -299,13 +231,10 @@ struct Engine {
   // gradient of the last pass in which that pixel was inside, which differs
   // only for subsets reaching the border).  Sums in FP64; the fields are
   // rounded to float like the reference's float fields.
-  // Arguments travel by value (registers): a pointer to the caller's arrays
-  // would move them to local memory for the whole Gauss-Newton loop.
   struct Slots {
     float s[12];
   };
-  __device__ __noinline__ void write_uncertainty(const SubsetRef sb, const Slots before,
-                                                 const Slots after) {
+  __device__ __noinline__ void write_uncertainty(const SubsetRef sb, const Slots before, const Slots after) {
     const double* f = A.fields + (size_t)sb.idx * DICEGPU_FIELD_STRIDE;
     const float ucx = (float)f[DICEGPU_F_COORD_X], ucy = (float)f[DICEGPU_F_COORD_Y];
     MapConst kb, ka;
@@ -317,7 +246,7 @@ struct Engine {
     const int W = A.def.w, H = A.def.h;
     const long rlim = (long)A.ref.w * A.ref.h;
     double s_g2 = 0.0, s_uhat = 0.0, s_ug = 0.0, s_jg = 0.0, s_r = 0.0;
-    for (int p = lane; p < sb.npix; p += 32) {
+    for (int p = tid; p < sb.npix; p += T) {
       int x, y;
       pixel_xy(sb, p, x, y);
       const long ri = (long)y * A.ref.w + x;
@@ -326,12 +255,11 @@ struct Engine {
       float gy = rin ? __ldg(A.ref.gy + ri) : 0.0f;
       if (DEFGRAD) {
         float mx, my, Dx, Dy;
-        map_offset<SHAPE>(kb, __fsub_rn((float)x, fcx), __fsub_rn((float)y, fcy), fcx, fcy, mx, my,
-                          Dx, Dy);
+        map_offset<SHAPE>(kb, __fsub_rn((float)x, fcx), __fsub_rn((float)y, fcy), fcx, fcy, mx, my, Dx, Dy);
         const int px = round_pixel(mx), py = round_pixel(my);
         if (!(px < 4 || px >= W - 4 || py < 4 || py >= H - 4)) {
           float G;
-          interp_interior<INTERP, true>(A.def, mx, my, G, gx, gy);
+          interp_ref<INTERP, true>(A.def, mx, my, G, gx, gy);
         }
       }
       const float g2 = gx * gx + gy * gy;
@@ -348,12 +276,12 @@ struct Engine {
       const float d = sub_r - sub_e;
       s_r += (double)(d * d * inv_g2);
     }
-    s_g2 = warp_sum(s_g2);
-    s_uhat = warp_sum(s_uhat);
-    s_ug = warp_sum(s_ug);
-    s_jg = warp_sum(s_jg);
-    s_r = warp_sum(s_r);
-    if (lane == 0) {
+    s_g2 = cta_sum(s_g2);
+    s_uhat = cta_sum(s_uhat);
+    s_ug = cta_sum(s_ug);
+    s_jg = cta_sum(s_jg);
+    s_r = cta_sum(s_r);
+    if (tid == 0) {
       const float cos_hat = s_uhat == 0.0 ? 1.0f : (float)sqrt(s_ug / s_uhat);
       double* o = A.unc + (size_t)sb.idx * DICEGPU_UNCERTAINTY_STRIDE;
       o[DICEGPU_U_COS_THETA_HAT] = cos_hat;
@@ -380,7 +308,7 @@ struct Engine {
     const MaskView mv(A.geo.mask_desc + (size_t)sb.idx * DG_MASK_DESC, A.geo.mask_bits, A.geo.blocked_poly,
                       A.geo.blocked_vx, A.geo.blocked_vy);
     int on = 0;
-    for (int p = lane; p < sb.npix; p += 32) {
+    for (int p = tid; p < sb.npix; p += T) {
       uint8_t* st = A.geo.pix_flag + sb.off + p;
       if (*st != 0) continue;
       int x, y;
@@ -390,17 +318,16 @@ struct Engine {
       const int px = round_pixel(mx), py = round_pixel(my);
       if (px < 4 || px >= W - 4 || py < 4 || py >= H - 4 || mv.hides(px, py)) continue;
       float G, gx, gy;
-      interp_interior<INTERP, false>(A.def, mx, my, G, gx, gy);
+      interp_ref<INTERP, false>(A.def, mx, my, G, gx, gy);
       A.geo.pix_f[sb.off + p] = G;
       *st = 2;
       ++on;
     }
-    on = warp_sum_i(on);
-    if (lane == 0 && on) A.geo.evo_nact[sb.idx] += on;
+    on = cta_sum_i(on);
+    if (tid == 0 && on) A.geo.evo_nact[sb.idx] += on;
   }
 
-  __device__ __forceinline__ void uncertainty_hook(const SubsetRef& sb, const float* before,
-                                                   const float* after) {
+  __device__ __forceinline__ void uncertainty_hook(const SubsetRef& sb, const float* before, const float* after) {
     Slots b, a;
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
@@ -411,187 +338,241 @@ struct Engine {
   }
 
   // --------------------------------------------------------------------------
-  // Gauss-Newton (Objective_ZNSSD::computeUpdateFast).  `slots` in/out.
-  // `meanF` is the reference mean at entry (Subset::mean(REF_INTENSITIES)).
+  // The Gauss-Newton step of one iteration, run by warp 0: the Hessian and
+  // right-hand side from the warps' sums (compact parameter order), the LM
+  // penalty, the 2x2 condition number (:558-564, float / double as the
+  // reference mixes them), LU with partial pivoting and the explicit inverse
+  // (the unblocked DGETRF / DGETRI operations, :571, :591), then
+  // def_update[i] = sum_j inv[i][j] * (-1.0) * q[j], accumulated in float
+  // (:599-601), the momentum term, the float update of the parameters and the
+  // convergence test.  A zero pivot leaves the LU factors in place and the
+  // reference applies them as the "inverse" (DGETRI returns early).  Results
+  // go to Ctl: status (0, or HESSIAN_SINGULAR), cond, conv, slots.
   // --------------------------------------------------------------------------
-  // meanF < 0 is never a valid "not given" marker for intensities, so the
-  // all-pixel mean of a fresh subset is requested with `meanF_from_pass`.
-  __device__ int gauss_newton(const SubsetRef& sb, float* slots, float meanF, bool meanF_from_pass,
-                              int& num_iterations,
-                              float& cond_out, PassOut& last) {
+  // hw0, hnw: the warps whose Hessian sums hold the subset's pixels (h_sweep)
+  __device__ __noinline__ void solve_step(const Slots cur, int hw0, int hnw) {
     const DevParams& P = A.P;
     const int N = P.N;
-    float upd_old[12];
+    Ctl& c = ctl();
+    const WarpOut<SHAPE>* wo = wouts<SHAPE>();
+    const int NW = T >> 5;
+    constexpr int NM = L::NMAX;
+    for (int e = lane; e < N * N; e += 32) {
+      const int a = e / N, b = e - a * N;
+      const int i = P.slot[a], j = P.slot[b];
+      const int lo = min(i, j), hi = max(i, j);
+      double m = 0.0, er = 0.0;
+      for (int w = hw0; w < hw0 + hnw; ++w) m += wo[w].M[lo * L::VW + hi];
+      for (int w = hw0; w < hw0 + hnw; ++w) er += wo[w].E[pair_index(lo, hi, L::NS)];
+      c.H[e] = m - er;
+    }
+    if (lane < N) {
+      double qq = 0.0;
+      for (int w = 0; w < NW; ++w) qq += wo[w].q[P.slot[lane]];
+      c.q[lane] = qq;
+    }
+    __syncwarp();
+    if (lane == 0 && P.lm_alpha > 0.0f) {
+      c.H[0] += (double)P.lm_alpha;
+      c.H[N + 1] += (double)P.lm_alpha;
+    }
+    __syncwarp();
+    // 2x2 condition number of the displacement block
+    float cond = -1.0f;
+    {
+      const double H00 = c.H[0], H01 = c.H[1], H10 = c.H[N], H11 = c.H[N + 1];
+      const float det_h = (float)(H00 * H11 - H10 * H01);
+      const double nsq = H00 * H00 + H01 * H01 + H10 * H10 + H11 * H11;
+      const float norm_H = (float)sqrt(nsq);
+      if (det_h != 0.0f) {
+        const float dd = det_h * det_h;
+        const float norm_Hi = (float)sqrt((1.0 / (double)dd) * nsq);
+        cond = norm_H * norm_Hi;
+      }
+    }
+    if (lane == 0) c.cond = cond;
+    if (cond > 1.0e12f) {
+      if (lane == 0) c.status = DICEGPU_HESSIAN_SINGULAR;
+      return;
+    }
+    // LU with partial pivoting: lane a holds row a (the unblocked DGETRF
+    // operations, lane-parallel within a column step)
+    double h[NM];
 #pragma unroll
-    for (int i = 0; i < 12; ++i) upd_old[i] = 0.0f;
-    double* M = warp_smem<SHAPE>()->M;
+    for (int j = 0; j < NM; ++j) h[j] = (lane < N && j < N) ? c.H[lane * N + j] : 0.0;
+    int info = 0;
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      if (j < N) {
+        // first row of maximal |a_ij| at or below the diagonal (IDAMAX)
+        double best = __shfl_sync(FULL, fabs(h[j]), j);
+        int p = j;
+#pragma unroll
+        for (int i = j + 1; i < NM; ++i) {
+          const double ai = __shfl_sync(FULL, fabs(h[j]), i);
+          if (i < N && ai > best) { best = ai; p = i; }
+        }
+        if (lane == 0) c.piv[j] = p;
+        const double pv = __shfl_sync(FULL, h[j], p);
+        if (pv != 0.0) {
+          if (p != j) {
+            const int src = lane == j ? p : (lane == p ? j : lane);
+#pragma unroll
+            for (int kx = 0; kx < NM; ++kx) h[kx] = __shfl_sync(FULL, h[kx], src);
+          }
+          const double r = 1.0 / pv;
+          if (lane > j && lane < N) h[j] = h[j] * r;
+        } else if (info == 0) {
+          info = j + 1;
+        }
+#pragma unroll
+        for (int kx = j + 1; kx < NM; ++kx) {
+          const double prow = __shfl_sync(FULL, h[kx], j);
+          if (kx < N && lane > j && lane < N) h[kx] = h[kx] - h[j] * prow;
+        }
+      }
+    }
+    __syncwarp();
+    if (lane < N) {
+#pragma unroll
+      for (int j = 0; j < NM; ++j)
+        if (j < N) c.H[lane * N + j] = h[j];
+    }
+    __syncwarp();
+    if (info == 0 && lane < N) {
+      // column `lane` of the inverse: x = U^-1 L^-1 P e_lane
+      double col[NM];
+#pragma unroll
+      for (int i = 0; i < NM; ++i) col[i] = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+      for (int j = 0; j < NM; ++j) {
+        if (j < N) {
+          const int pj = c.piv[j];
+          if (pj != j) {
+#pragma unroll
+            for (int i = j + 1; i < NM; ++i)
+              if (i == pj) {
+                const double t = col[i];
+                col[i] = col[j];
+                col[j] = t;
+              }
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 1; i < NM; ++i) {
+        if (i < N) {
+#pragma unroll
+          for (int j = 0; j < i; ++j) col[i] = col[i] - c.H[i * N + j] * col[j];
+        }
+      }
+#pragma unroll
+      for (int i = NM - 1; i >= 0; --i) {
+        if (i < N) {
+#pragma unroll
+          for (int j = i + 1; j < NM; ++j)
+            if (j < N) col[i] = col[i] - c.H[i * N + j] * col[j];
+          col[i] = col[i] / c.H[i * N + i];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < NM; ++i)
+        if (i < N) c.inv[i * N + lane] = col[i];
+    }
+    __syncwarp();
+    bool notc = false;
+    float nw = 0.0f;
+    if (lane < N) {
+      const double* Mrow = info == 0 ? &c.inv[lane * N] : &c.H[lane * N];
+      float du = 0.0f;
+      for (int j = 0; j < N; ++j) du = (float)((double)du + (Mrow[j] * (-1.0)) * c.q[j]);
+      if (P.momentum != 0.0f) {
+        du = du + P.momentum * c.upd_old[lane];
+        c.upd_old[lane] = du;
+      }
+      const float old = cur.s[P.slot[lane]];
+      nw = old + du;
+      // test_for_convergence: affine u, v, theta (DICe_LocalShapeFunction.cpp:433-459),
+      // quadratic every parameter (:91-102)
+      const bool tested = SHAPE == DICEGPU_QUADRATIC_SF || lane < 2 || (lane == 2 && P.has_rot);
+      notc = tested && fabsf(nw - old) >= P.fast_tol;
+    }
+    const bool conv = !__any_sync(FULL, notc);
+    if (lane < 12) c.slots[lane] = cur.s[lane];
+    __syncwarp();
+    if (lane < N) c.slots[P.slot[lane]] = nw;
+    if (lane == 0) {
+      c.status = DICEGPU_CORRELATION_SUCCESSFUL;
+      c.conv = conv ? 1 : 0;
+    }
+  }
+
+  // --------------------------------------------------------------------------
+  // Gauss-Newton (Objective_ZNSSD::computeUpdateFast).  `slots` in/out.
+  // The reference mean at entry (Subset::mean(REF_INTENSITIES), :465) is
+  // over the pixels live at the last deformed-state initialisation when
+  // `have_state`, else over all active pixels of the fresh subset.
+  // --------------------------------------------------------------------------
+  __device__ int gauss_newton(const SubsetRef& sb, float* slots, bool have_state, int& num_iterations,
+                              float& cond_out) {
+    const DevParams& P = A.P;
+    Ctl& c = ctl();
+    const PixArrays X = arrays();
+    float meanF = 0.0f;
+    if (have_state) {
+      const int na = c.n;
+      float s;
+      chains(1, X.F, nullptr, nullptr, nullptr, X.L, 0x01u, sb.npix, &s);
+      meanF = na ? __fdiv_rn(s, (float)na) : 0.0f;
+    }
+    if (tid < 12) c.upd_old[tid] = 0.0f;
     int solve_it = 0;
     for (; solve_it <= P.max_fast; ++solve_it) {
       num_iterations = solve_it;
       DG_PT(t_pass);
-      last = pass<true, true, false>(sb, slots, M);
+      pass<PK_GN>(sb, slots);
       DG_PACC(1, t_pass);
-      ++npass_;
-      const int n = last.n;
-      // Subset::mean(DEF_INTENSITIES): sum G / n over the active pixels
-      const double sumG = M[L::ID * L::VW + L::IONE] + last.sumF + (double)n * (double)sb.K;
-      const float meanG = n ? (float)(sumG / (double)n) : 0.0f;
-      if (meanF_from_pass && solve_it == 0) {
-        // Subset::mean(REF_INTENSITIES) at entry: every active pixel of a fresh subset
-        meanF = sb.nact ? (float)((last.sumFall + (double)sb.nact * (double)sb.K) / (double)sb.nact)
-                        : 0.0f;
+      const int n = c.n;
+      MapConst k;
+      make_mapconst<SHAPE>(slots, !DEFGRAD, (float)sb.cx, (float)sb.cy, k);
+      const PassInMasked in = make_in(sb);
+      const PassIn& inb = static_cast<const PassIn&>(in);
+      const bool fresh = solve_it == 0 && !have_state;
+      // Subset::mean(DEF_INTENSITIES) (and for a fresh subset the entry mean
+      // of its active reference intensities) in warp 0 while the other warps
+      // sweep the Hessian, which does not need it
+      const int NW = T >> 5;
+      const int hw0 = NW > 1 ? 1 : 0, hnw = NW > 1 ? NW - 1 : 1;
+      DG_PT(t_h);
+      if (warp == 0 && lane < (fresh ? 2 : 1))
+        c.fres[lane] = chain_sum_masked(lane ? X.F : X.G, X.L, lane ? 2u : 1u, sb.npix);
+      __syncwarp();
+      h_sweep<SHAPE, DEFGRAD>(inb, k, hw0, hnw);
+      __syncthreads();
+      DG_PACC(5, t_h);
+      if (fresh) meanF = sb.nact ? __fdiv_rn(c.fres[1], (float)sb.nact) : 0.0f;
+      const float meanG = n ? __fdiv_rn(c.fres[0], (float)n) : 0.0f;
+      DG_PT(t_q);
+      q_sweep<SHAPE, DEFGRAD>(inb, k, meanG, meanF);
+      DG_PACC(6, t_q);
+      Slots cur;
+#pragma unroll
+      for (int i = 0; i < 12; ++i) cur.s[i] = slots[i];
+      DG_PT(t_s);
+      if (warp == 0) solve_step(cur, hw0, hnw);
+      __syncthreads();
+      DG_PACC(7, t_s);
+      cond_out = c.cond;
+      if (c.status == DICEGPU_HESSIAN_SINGULAR) {
+        __syncthreads();
+        return DICEGPU_HESSIAN_SINGULAR;
       }
-      const double cshift = (double)meanG - (double)meanF;
-      if constexpr (SHAPE == DICEGPU_AFFINE_SF) {
-        // Every lane solves the whole (padded) 6x6 system in registers: the
-        // slots of disabled parameters get identity rows / columns and q = 0,
-        // which leaves the LU of the enabled block (same pivots, same
-        // operations) unchanged and gives them a zero update.
-        const AffineStep stp = solve_affine(M, cshift, enabled_mask(), P.lm_alpha);
-        const float* upd_s = stp.upd;
-        cond_out = stp.cond;
-        if (stp.cond > 1.0e12f) return DICEGPU_HESSIAN_SINGULAR;
-        float old[12];
+      const bool conv = c.conv != 0;
 #pragma unroll
-        for (int i = 0; i < 12; ++i) old[i] = slots[i];
-#pragma unroll
-        for (int s = 0; s < 6; ++s) {
-          float u = upd_s[s];
-          if (P.momentum != 0.0f) {
-            u += P.momentum * upd_old[s];
-            upd_old[s] = u;
-          }
-          slots[s] += u;   // disabled slots: u == 0
-        }
-        const float tol = P.fast_tol;
-        bool conv = true;
-        if (fabsf(slots[0] - old[0]) >= tol) conv = false;
-        if (fabsf(slots[1] - old[1]) >= tol) conv = false;
-        if (P.has_rot && fabsf(slots[2] - old[2]) >= tol) conv = false;
-        if (conv) {
-          if (A.unc && (A.mode == MODE_CORRELATE || A.mode == MODE_GN)) uncertainty_hook(sb, old, slots);
-          break;
-        }
-        continue;
-      }
-      // lane i owns row i of [H | q] in the reference's compact order
-      double h[L::NMAX];
-      double qv = 0.0;
-      const int si = lane < N ? P.slot[lane] : 0;
-#pragma unroll
-      for (int j = 0; j < L::NMAX; ++j) {
-        h[j] = 0.0;
-        if (j < N && lane < N) h[j] = M[si * L::VW + P.slot[j]];
-      }
-      if (lane < N) qv = M[si * L::VW + L::ID] - cshift * M[si * L::VW + L::IONE];
-      // Levenberg-Marquardt penalty on the displacement diagonal (:548-553)
-      if (P.lm_alpha > 0.0f) {
-        if (lane == 0) h[0] += (double)P.lm_alpha;
-        if (lane == 1) h[1] += (double)P.lm_alpha;
-      }
-      // 2x2 condition number of the displacement block (:558-564), in the
-      // reference's mix of float and double
-      const double H00 = __shfl_sync(FULL, h[0], 0), H01 = __shfl_sync(FULL, h[1], 0);
-      const double H10 = __shfl_sync(FULL, h[0], 1), H11 = __shfl_sync(FULL, h[1], 1);
-      const float det_h = (float)(H00 * H11 - H10 * H01);
-      const double nsq = H00 * H00 + H01 * H01 + H10 * H10 + H11 * H11;
-      const float norm_H = (float)sqrt(nsq);
-      float cond = -1.0f;
-      if (det_h != 0.0f) {
-        const float dd = __fmul_rn(det_h, det_h);
-        const float norm_Hi = (float)sqrt((1.0 / (double)dd) * nsq);
-        cond = norm_H * norm_Hi;
-      }
-      cond_out = cond;
-      // LU with partial pivoting (DGETRF order), q carried as an extra column
-      const double q_orig = qv;
-      int info = 0;
-#pragma unroll
-      for (int j = 0; j < L::NMAX; ++j) {
-        if (j < N) {
-          double a = (lane >= j && lane < N) ? fabs(h[j]) : -1.0;
-          int pl = lane;
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            const double oa = __shfl_xor_sync(FULL, a, o);
-            const int op = __shfl_xor_sync(FULL, pl, o);
-            if (oa > a || (oa == a && op < pl)) { a = oa; pl = op; }
-          }
-          const double pv = __shfl_sync(FULL, h[j], pl);
-          if (pv != 0.0) {
-            if (pl != j) {
-              const int src = lane == j ? pl : (lane == pl ? j : lane);
-#pragma unroll
-              for (int kx = 0; kx < L::NMAX; ++kx) h[kx] = __shfl_sync(FULL, h[kx], src);
-              qv = __shfl_sync(FULL, qv, src);
-            }
-            const double rcp = 1.0 / pv;
-            if (lane > j && lane < N) h[j] *= rcp;
-          } else if (info == 0) {
-            info = j + 1;
-          }
-#pragma unroll
-          for (int kx = j + 1; kx < L::NMAX; ++kx) {
-            const double prow = __shfl_sync(FULL, h[kx], j);
-            if (kx < N && lane > j && lane < N) h[kx] -= h[j] * prow;
-          }
-          const double pq = __shfl_sync(FULL, qv, j);
-          if (lane > j && lane < N) qv -= h[j] * pq;
-        }
-      }
-      if (cond > 1.0e12f) return DICEGPU_HESSIAN_SINGULAR;
-      float upd = 0.0f;
-      if (info == 0) {
-        // back substitution: x = U^-1 y, update = -x
-        double x = 0.0;
-#pragma unroll
-        for (int j = L::NMAX - 1; j >= 0; --j) {
-          if (j < N) {
-            const double ujj = __shfl_sync(FULL, h[j], j);
-            const double yj = __shfl_sync(FULL, qv, j);
-            const double xj = yj / ujj;
-            if (lane == j) x = xj;
-            if (lane < j) qv -= h[j] * xj;
-          }
-        }
-        upd = (float)(-x);
-      } else {
-        // DGETRI returns early on a zero pivot and the LU factors themselves
-        // are applied to -q (:591, :605-607), accumulated in float
-#pragma unroll
-        for (int j = 0; j < L::NMAX; ++j) {
-          const double qj = __shfl_sync(FULL, q_orig, j);
-          if (j < N) upd = (float)((double)upd + h[j] * (-1.0) * qj);
-        }
-      }
-      float old[12];
-#pragma unroll
-      for (int i = 0; i < 12; ++i) old[i] = slots[i];
-#pragma unroll
-      for (int kx = 0; kx < 12; ++kx) {
-        float u = __shfl_sync(FULL, upd, kx);
-        if (kx < N) {
-          if (P.momentum != 0.0f) {
-            u += P.momentum * upd_old[kx];
-            upd_old[kx] = u;
-          }
-          slots[P.slot[kx]] += u;
-        }
-      }
-      // test_for_convergence (affine: u, v, theta :433-459; quadratic: all)
-      const float tol = P.fast_tol;
-      bool conv = true;
-      if (SHAPE == DICEGPU_QUADRATIC_SF) {
-#pragma unroll
-        for (int i = 0; i < 12; ++i)
-          if (fabsf(slots[i] - old[i]) >= tol) conv = false;
-      } else {
-        if (fabsf(slots[0] - old[0]) >= tol) conv = false;
-        if (fabsf(slots[1] - old[1]) >= tol) conv = false;
-        if (P.has_rot && fabsf(slots[2] - old[2]) >= tol) conv = false;
-      }
+      for (int i = 0; i < 12; ++i) slots[i] = c.slots[i];
+      __syncthreads();
       if (conv) {
-        if (A.unc && (A.mode == MODE_CORRELATE || A.mode == MODE_GN)) uncertainty_hook(sb, old, slots);
+        if (A.unc && (A.mode == MODE_CORRELATE || A.mode == MODE_GN)) uncertainty_hook(sb, cur.s, slots);
         break;
       }
     }
@@ -600,58 +581,136 @@ struct Engine {
   }
 
   // --------------------------------------------------------------------------
-  // Nelder-Mead (Simplex::minimize, DICe_Simplex.cpp:60-277).  Every lane runs
-  // the same bookkeeping on its own private copy of the simplex (identical
-  // values in all lanes, no shared state); the gamma evaluations are
-  // warp-wide passes.  `slots` in/out: left at the last evaluated point, as
-  // the reference's aliasing of variables and shape-function parameters
-  // leaves it (DICe_LocalShapeFunction.h:259-261).  `lastp` receives that
-  // point in slot form.
+  // Nelder-Mead (Simplex::minimize, DICe_Simplex.cpp:60-277).  The vertex
+  // table and sums live in the warp's SimplexState (lane 0 writes after a
+  // __syncwarp, all lanes read after the next); every warp keeps an
+  // identical copy and all evaluate the same points together.  `slots`
+  // in/out: left at the last evaluated point, as the reference's aliasing
+  // of variables and shape-function parameters leaves it
+  // (DICe_LocalShapeFunction.h:259-261); `lastp` receives that point in slot
+  // form.  The reference evaluates gamma once more at the point it evaluated
+  // last before each convergence test; that value is the last one computed,
+  // which is taken instead of a second pass.
   // --------------------------------------------------------------------------
+  __device__ __forceinline__ void comp_to_slots(const SimplexState& S, const float* comp, float* out) const {
+    // out[s] = base[s], then the compact parameters in their slots
+#pragma unroll
+    for (int s = 0; s < 12; ++s) {
+      float v = S.base[s];
+#pragma unroll
+      for (int kx = 0; kx < 12; ++kx)
+        if (kx < A.P.N && A.P.slot[kx] == s) v = comp[kx];
+      out[s] = v;
+    }
+  }
+
   __device__ int simplex(const SubsetRef& sb, float* slots, int& num_iterations, float* lastp) {
     const DevParams& P = A.P;
     const int nd = P.N;
     const int mpts = nd + 1;
-    float base[12];
+    SimplexState& S = sx_state<SHAPE>();
+    const bool w0 = lane == 0;
+    float init[12];
 #pragma unroll
-    for (int i = 0; i < 12; ++i) base[i] = slots[i];
-    float vars[12], init[12], pts[13][12], gv[13], psum[12], ptry[12];
-    for (int kx = 0; kx < nd; ++kx) init[kx] = base[P.slot[kx]];
-    auto evaluate = [&]() -> float {
-      float cs[12];
-      for (int kx = 0; kx < 12; ++kx) cs[kx] = kx < nd ? vars[kx] : 0.0f;
-      compact_to_slots(cs, lastp, base);
-      return eval_gamma(sb, lastp);
+    for (int kx = 0; kx < 12; ++kx) {
+      float v = 0.0f;
+#pragma unroll
+      for (int s = 0; s < 12; ++s)
+        if (kx < nd && P.slot[kx] == s) v = slots[s];
+      init[kx] = v;
+    }
+    __syncwarp();
+    if (w0) {
+#pragma unroll
+      for (int s = 0; s < 12; ++s) S.base[s] = slots[s];
+#pragma unroll
+      for (int kx = 0; kx < 12; ++kx) S.init[kx] = init[kx];
+    }
+    __syncwarp();
+    float cur[12];   // the last evaluated point (compact)
+#pragma unroll
+    for (int kx = 0; kx < 12; ++kx) cur[kx] = init[kx];
+    float last_y = 0.0f;
+    auto evaluate = [&](const float* comp) -> float {
+#pragma unroll
+      for (int kx = 0; kx < 12; ++kx) cur[kx] = comp[kx];
+      comp_to_slots(S, comp, lastp);
+      last_y = eval_gamma(sb, lastp, P.normalize_gamma != 0);
+      return last_y;
     };
-    auto finish = [&]() {
-      float cs[12];
-      for (int kx = 0; kx < 12; ++kx) cs[kx] = kx < nd ? vars[kx] : 0.0f;
-      compact_to_slots(cs, slots, base);
-    };
+    auto finish = [&]() { comp_to_slots(S, cur, slots); };
     // initial simplex vertex_i = x0 + delta_i e_i (:82-107)
     for (int i = 0; i < mpts; ++i) {
-      for (int j = 0; j < nd; ++j) {
-        pts[i][j] = init[j];
-        if (i > 0 && j == i - 1) pts[i][j] += P.deltas[i - 1];
-        vars[j] = pts[i][j];
+      float v[12];
+#pragma unroll
+      for (int j = 0; j < 12; ++j) {
+        v[j] = S.init[j];
+        if (i > 0 && j == i - 1) v[j] = v[j] + P.deltas[i - 1];
       }
-      gv[i] = evaluate();
-      if (i == 0 && gv[i] < P.skip_thr && gv[i] >= 0.0f) {
+      __syncwarp();
+      if (w0) {
+#pragma unroll
+        for (int j = 0; j < 12; ++j) S.pts[i][j] = v[j];
+      }
+      __syncwarp();
+      const float g = evaluate(v);
+      __syncwarp();
+      if (w0) S.gv[i] = g;
+      __syncwarp();
+      if (i == 0 && g < P.skip_thr && g >= 0.0f) {
         num_iterations = 0;
         finish();
         return DICEGPU_CORRELATION_SUCCESSFUL;
       }
-      for (int j = 0; j < nd; ++j) vars[j] = init[j];
     }
-    for (int j = 0; j < nd; ++j) {
-      float sum = 0.0f;
-      for (int i = 0; i < mpts; ++i) sum += pts[i][j];
-      psum[j] = sum;
+    {
+      float ps[12];
+#pragma unroll
+      for (int j = 0; j < 12; ++j) {
+        float sum = 0.0f;
+        for (int i = 0; i < mpts; ++i) sum += S.pts[i][j];
+        ps[j] = sum;
+      }
+      __syncwarp();
+      if (w0) {
+#pragma unroll
+        for (int j = 0; j < 12; ++j) S.psum[j] = ps[j];
+      }
+      __syncwarp();
     }
     int inhi = 0;
     float old_rtol = 0.0f, gamma_new = 0.0f, gamma_old = -1.0f;
     int gamma_repeats = 0;
     const float tiny = 1.0e-10f;
+    int ihi = 0;
+    // a trial point psum * fac1 - pts[ihi] * fac2 (Simplex::amotry, :188-203),
+    // which replaces the worst vertex when it is better
+    auto trial = [&](float fac) -> float {
+      const float fac1 = (float)((1.0 - (double)fac) / nd);
+      const float fac2 = fac1 - fac;
+      float pt[12];
+#pragma unroll
+      for (int j = 0; j < 12; ++j) pt[j] = j < nd ? S.psum[j] * fac1 - S.pts[ihi][j] * fac2 : 0.0f;
+      const float y = evaluate(pt);
+      if (y < S.gv[ihi]) {
+        float ps[12];
+#pragma unroll
+        for (int j = 0; j < 12; ++j) ps[j] = S.psum[j] + (pt[j] - S.pts[ihi][j]);
+        __syncwarp();
+        if (w0) {
+          S.gv[ihi] = y;
+#pragma unroll
+          for (int j = 0; j < 12; ++j) {
+            if (j < nd) {
+              S.psum[j] = ps[j];
+              S.pts[ihi][j] = pt[j];
+            }
+          }
+        }
+        __syncwarp();
+      }
+      return y;
+    };
     int iteration = 0;
     for (iteration = 0; iteration < P.max_robust; iteration++) {
       if (iteration >= P.max_robust - 1) {
@@ -660,86 +719,86 @@ struct Engine {
         return DICEGPU_MAX_ITERATIONS_REACHED;
       }
       int ilo = 0;
-      int ihi;
-      if (gv[0] > gv[1]) { inhi = 1; ihi = 0; } else { inhi = 0; ihi = 1; }
+      if (S.gv[0] > S.gv[1]) { inhi = 1; ihi = 0; } else { inhi = 0; ihi = 1; }
       for (int i = 0; i < mpts; i++) {
-        if (gv[i] <= gv[ilo]) ilo = i;
-        if (gv[i] > gv[ihi]) { inhi = ihi; ihi = i; }
-        else if (gv[i] > gv[inhi] && i != ihi) inhi = i;
+        const float gi = S.gv[i];
+        if (gi <= S.gv[ilo]) ilo = i;
+        if (gi > S.gv[ihi]) { inhi = ihi; ihi = i; }
+        else if (gi > S.gv[inhi] && i != ihi) inhi = i;
       }
-      const float rtol = (float)(2.0 * (double)fabsf(gv[ihi] - gv[ilo]) /
-                                 (double)(fabsf(gv[ihi]) + fabsf(gv[ilo]) + tiny));
+      const float ghi = S.gv[ihi], glo = S.gv[ilo];
+      const float rtol = (float)(2.0 * (double)fabsf(ghi - glo) / (double)(fabsf(ghi) + fabsf(glo) + tiny));
       const float rtol_diff = fabsf(rtol - old_rtol);
       old_rtol = rtol;
       if (fabsf(gamma_new - gamma_old) < 1.0e-8f) gamma_repeats++;
       gamma_old = gamma_new;
-      if ((double)rtol < P.robust_tol || (double)rtol_diff < P.robust_tol || gamma_repeats > 15) {
-        const float g0 = gv[0];
-        gv[0] = gv[ilo];
-        gv[ilo] = g0;
-        for (int i = 0; i < nd; i++) {
-          const float t = pts[0][i];
-          pts[0][i] = pts[ilo][i];
-          pts[ilo][i] = t;
-        }
-        break;
-      }
-      auto trial = [&](float fac) -> float {
-        const float fac1 = (float)((1.0 - (double)fac) / nd);
-        const float fac2 = fac1 - fac;
-        for (int j = 0; j < nd; j++) {
-          ptry[j] = psum[j] * fac1 - pts[ihi][j] * fac2;
-          vars[j] = ptry[j];
-        }
-        const float y = evaluate();
-        if (y < gv[ihi]) {
-          gv[ihi] = y;
-          for (int j = 0; j < nd; j++) {
-            psum[j] += ptry[j] - pts[ihi][j];
-            pts[ihi][j] = ptry[j];
-          }
-        }
-        return y;
-      };
+      if ((double)rtol < P.robust_tol || (double)rtol_diff < P.robust_tol || gamma_repeats > 15) break;
       float ytry = trial(-1.0f);
-      if (ytry <= gv[ilo]) {
+      if (ytry <= S.gv[ilo]) {
         ytry = trial(2.0f);
-      } else if (ytry >= gv[inhi]) {
-        const float ysave = gv[ihi];
+      } else if (ytry >= S.gv[inhi]) {
+        const float ysave = S.gv[ihi];
         ytry = trial(0.5f);
         if (ytry >= ysave) {
           for (int i = 0; i < mpts; i++) {
             if (i != ilo) {
-              for (int j = 0; j < nd; j++) {
-                pts[i][j] = psum[j] = (float)(0.5 * (double)(pts[i][j] + pts[ilo][j]));
-                vars[j] = psum[j];
+              float v[12];
+#pragma unroll
+              for (int j = 0; j < 12; ++j) v[j] = j < nd ? (float)(0.5 * (double)(S.pts[i][j] + S.pts[ilo][j])) : 0.0f;
+              __syncwarp();
+              if (w0) {
+#pragma unroll
+                for (int j = 0; j < 12; ++j) {
+                  if (j < nd) {
+                    S.pts[i][j] = v[j];
+                    S.psum[j] = v[j];
+                  }
+                }
               }
-              gv[i] = evaluate();
+              __syncwarp();
+              const float g = evaluate(v);
+              __syncwarp();
+              if (w0) S.gv[i] = g;
+              __syncwarp();
             }
           }
-          for (int j = 0; j < nd; j++) {
+          float ps[12];
+#pragma unroll
+          for (int j = 0; j < 12; ++j) {
             float sum = 0.0f;
-            for (int i = 0; i < mpts; i++) sum += pts[i][j];
-            psum[j] = sum;
+            for (int i = 0; i < mpts; i++) sum += S.pts[i][j];
+            ps[j] = sum;
           }
+          __syncwarp();
+          if (w0) {
+#pragma unroll
+            for (int j = 0; j < 12; ++j) S.psum[j] = ps[j];
+          }
+          __syncwarp();
         }
       }
-      gamma_new = evaluate();
+      gamma_new = last_y;
     }
     num_iterations = iteration;
     finish();
     return DICEGPU_CORRELATION_SUCCESSFUL;
   }
 
-  // Subset::noise_std_dev (DICe_Subset.cpp:622-703) on the deformed image.
-  __device__ float noise_std_dev(const SubsetRef& sb, const PassOut& st, const float* slots) const {
-    if (st.n == 0) return -1.0f;
+  // Subset::noise_std_dev (DICe_Subset.cpp:622-703) on the deformed image
+  // over the box of the last pass's live pixels moved by (u, v): the 3 x 3
+  // Immerkaer mask (j outer, i inner), |.| summed in float, row by row.  The
+  // terms are computed by the CTA a chunk at a time into DX and summed in
+  // order by one thread.  Reads go through the row-major linear index like
+  // the reference's operator() (0 outside the array).
+  __device__ float noise_exact(const SubsetRef& sb, const float* slots, int n, int bminx, int bmaxx, int bminy,
+                               int bmaxy) {
+    if (n == 0) return -1.0f;
     MapConst k;
     make_mapconst<SHAPE>(slots, false, (float)sb.cx, (float)sb.cy, k);
     float u, v, t;
     map_to_u_v_theta<SHAPE>(k, (float)sb.cx, (float)sb.cy, u, v, t);
-    int min_x = (int)((float)st.minx + u), max_x = (int)((float)st.maxx + u);
-    int min_y = (int)((float)st.miny + v), max_y = (int)((float)st.maxy + v);
+    int min_x = (int)((float)bminx + u), max_x = (int)((float)bmaxx + u);
+    int min_y = (int)((float)bminy + v), max_y = (int)((float)bmaxy + v);
     const int img_w = A.def.w, img_h = A.def.h;
     if (min_x < 0) min_x = 0;
     if (min_y < 0) min_y = 0;
@@ -749,51 +808,74 @@ struct Engine {
     if (ww < 3) ww = 3;
     if (hh < 3) hh = 3;
     const int rw = max_x - min_x, rh = max_y - min_y;
-    double acc = 0.0;
+    float variance = 0.0f;
     if (rw > 0 && rh > 0) {
-      // a lane per column, a sliding 3-row window down the rows; reads go
-      // through the row-major linear index like the reference's operator()
-      // (0 outside the array), so edge pixels need no special window
       const long lim = (long)img_w * img_h;
       const float* I = A.def.I;
-      auto ld = [&](int x, int y) -> float {
-        const long li = (long)y * img_w + x;
-        return (li >= 0 && li < lim) ? __ldg(I + li) : 0.0f;
-      };
-      for (int xb = min_x; xb < max_x; xb += 32) {
-        const int xx = xb + lane;
-        if (xx >= max_x) continue;
-        float a0 = ld(xx - 1, min_y - 1), a1 = ld(xx, min_y - 1), a2 = ld(xx + 1, min_y - 1);
-        float b0 = ld(xx - 1, min_y), b1 = ld(xx, min_y), b2 = ld(xx + 1, min_y);
-        const bool xedge = xx < 1 || xx >= img_w - 1;
-        for (int yy = min_y; yy < max_y; ++yy) {
-          const float c0 = ld(xx - 1, yy + 1), c1 = ld(xx, yy + 1), c2 = ld(xx + 1, yy + 1);
-          if (xedge || yy < 1 || yy >= img_h - 1) {
-            acc += (double)fabsf(b1);
+      auto ld = [&](long li) -> float { return (li >= 0 && li < lim) ? __ldg(I + li) : 0.0f; };
+      const long total = (long)rw * rh;
+      const int chunk = A.npix_cap;
+      float* buf = arrays().DX;
+      Ctl& c = ctl();
+      for (long b0 = 0; b0 < total; b0 += chunk) {
+        const int m = (int)min((long)chunk, total - b0);
+        for (int e = tid; e < m; e += T) {
+          const long id = b0 + e;
+          const int yy = min_y + (int)(id / rw), xx = min_x + (int)(id % rw);
+          float val;
+          if (xx < 1 || xx >= img_w - 1 || yy < 1 || yy >= img_h - 1) {
+            const float a = ld((long)yy * img_w + xx);
+            val = __fsqrt_rn(a * a);
           } else {
-            // mask[i][j] (i: x offset, j: y offset), j outer, i inner
+            // mask[i][j] = {{1,-2,1},{-2,4,-2},{1,-2,1}}, i: x offset, j: y offset
+            const float* q = I + (size_t)(yy - 1) * img_w + (xx - 1);
             float conv = 0.0f;
-            conv += a0 * 1.0f;  conv += a1 * -2.0f; conv += a2 * 1.0f;
-            conv += b0 * -2.0f; conv += b1 * 4.0f;  conv += b2 * -2.0f;
-            conv += c0 * 1.0f;  conv += c1 * -2.0f; conv += c2 * 1.0f;
-            acc += (double)fabsf(conv);
+            conv = conv + __ldg(q) * 1.0f;
+            conv = conv + __ldg(q + 1) * -2.0f;
+            conv = conv + __ldg(q + 2) * 1.0f;
+            q += img_w;
+            conv = conv + __ldg(q) * -2.0f;
+            conv = conv + __ldg(q + 1) * 4.0f;
+            conv = conv + __ldg(q + 2) * -2.0f;
+            q += img_w;
+            conv = conv + __ldg(q) * 1.0f;
+            conv = conv + __ldg(q + 1) * -2.0f;
+            conv = conv + __ldg(q + 2) * 1.0f;
+            val = fabsf(conv);
           }
-          a0 = b0; a1 = b1; a2 = b2;
-          b0 = c0; b1 = c1; b2 = c2;
+          buf[e] = val;
         }
+        __syncthreads();
+        if (tid == 0) c.fres[0] = chain_sum(buf, m, variance);
+        __syncthreads();
+        variance = c.fres[0];
+        __syncthreads();
       }
     }
-    acc = warp_sum(acc);
-    const float var = (float)acc;
-    return (float)((double)var * (sqrt(0.5 * 3.14159265358979323846) / (6.0 * (ww - 2) * (hh - 2))));
+    return (float)((double)variance * (sqrt(0.5 * 3.14159265358979323846) / (6.0 * (ww - 2) * (hh - 2))));
   }
 
-  // Objective::sigma (DICe_Objective.cpp:150-184)
-  __device__ float sigma(const SubsetRef& sb, const PassOut& st, const float* slots, float& noise) const {
-    noise = noise_std_dev(sb, st, slots);
+  // Objective::sigma (DICe_Objective.cpp:150-184) at the state of the last
+  // pass with gradients: noise_std_dev, then the float sums of the squared
+  // gradients over the live pixels.
+  __device__ float sigma(const SubsetRef& sb, const float* slots, float& noise) {
+    Ctl& c = ctl();
+    const int n = c.n, bx0 = c.minx, bx1 = c.maxx, by0 = c.miny, by1 = c.maxy;
+    const PixArrays X = arrays();
+    for (int p = tid; p < sb.npix; p += T) {
+      float a = 0.0f, b = 0.0f;
+      if (X.L[p] & 1) {
+        a = X.GX[p] * X.GX[p];
+        b = X.GY[p] * X.GY[p];
+      }
+      X.DX[p] = a;
+      X.DY[p] = b;
+    }
+    float s[2];
+    chains(2, X.DX, X.DY, nullptr, nullptr, nullptr, 0u, sb.npix, s);
+    noise = noise_exact(sb, slots, n, bx0, bx1, by0, by1);
     if (noise < 0.0f) return -1.0f;
-    const float sgx = (float)st.sgx2, sgy = (float)st.sgy2;
-    const float sg = sgx > sgy ? sgy : sgx;
+    const float sg = s[0] > s[1] ? s[1] : s[0];
     return sg > 0.0f ? (float)sqrt(2.0 * (double)noise * (double)noise / (double)sg) : -1.0f;
   }
 
@@ -842,20 +924,20 @@ struct Engine {
 
   // Local_Shape_Function::save_fields: the shape-function columns of a field
   // row from the parameters (quadratic: A..L plus u, v, theta mapped at the
-  // subset's coordinates).  Lane 0 writes.
+  // subset's coordinates).  Thread 0 writes.
   __device__ void save_shape_fields(double* f, const float* slots, float fcx, float fcy) const {
     if (SHAPE == DICEGPU_QUADRATIC_SF) {
       MapConst k;
       make_mapconst<SHAPE>(slots, false, fcx, fcy, k);
       float u, v, t;
       map_to_u_v_theta<SHAPE>(k, fcx, fcy, u, v, t);
-      if (lane == 0) {
+      if (tid == 0) {
         for (int i = 0; i < 12; ++i) f[DICEGPU_F_QUAD_A + i] = slots[i];
         f[DICEGPU_F_DISP_X] = u;
         f[DICEGPU_F_DISP_Y] = v;
         f[DICEGPU_F_ROT_Z] = t;
       }
-    } else if (lane == 0) {
+    } else if (tid == 0) {
       f[DICEGPU_F_DISP_X] = slots[0];
       f[DICEGPU_F_DISP_Y] = slots[1];
       for (int kx = 2; kx < A.P.N; ++kx) f[DICEGPU_F_DISP_X + A.P.slot[kx]] = slots[A.P.slot[kx]];
@@ -874,10 +956,10 @@ struct Engine {
     const float fcx = (float)__shfl_sync(FULL, fv, DICEGPU_F_COORD_X);
     const float fcy = (float)__shfl_sync(FULL, fv, DICEGPU_F_COORD_Y);
     if (A.mode == MODE_SIGMA) {
-      const PassOut st = pass<false, true, true>(sb, slots, nullptr);
+      pass<PK_STATE>(sb, slots);
       float noise = 0.0f;
-      const float sg = sigma(sb, st, slots, noise);
-      if (lane == 0) {
+      const float sg = sigma(sb, slots, noise);
+      if (tid == 0) {
         A.gamma_out[sb.idx] = sg;
         A.noise_out[sb.idx] = noise;
       }
@@ -887,22 +969,21 @@ struct Engine {
     int status;
     if (A.mode == MODE_GN) {
       float cond = -1.0f;
-      PassOut last;
-      status = gauss_newton(sb, slots, 0.0f, true, num_iterations, cond, last);
-      if (lane == 0) f[DICEGPU_F_CONDITION] = cond;
+      status = gauss_newton(sb, slots, false, num_iterations, cond);
+      if (tid == 0) f[DICEGPU_F_CONDITION] = cond;
     } else {
       float last_eval[12];
       status = simplex(sb, slots, num_iterations, last_eval);
     }
     save_shape_fields(f, slots, fcx, fcy);
-    if (lane == 0) {
+    if (tid == 0) {
       A.iter_out[sb.idx] = num_iterations;
       A.status_out[sb.idx] = status;
     }
   }
 
   __device__ void record_failed(double* f, int status, int num_iterations) const {
-    if (lane == 0) {
+    if (tid == 0) {
       f[DICEGPU_F_SIGMA] = -1.0; f[DICEGPU_F_MATCH] = -1.0; f[DICEGPU_F_GAMMA] = -1.0;
       f[DICEGPU_F_BETA] = -1.0; f[DICEGPU_F_OMEGA] = -1.0; f[DICEGPU_F_NOISE] = -1.0;
       f[DICEGPU_F_CONTRAST] = -1.0; f[DICEGPU_F_ACTIVE_PIXELS] = -1.0;
@@ -910,23 +991,22 @@ struct Engine {
     }
   }
 
-  // Objective::beta (DICe_Objective.cpp:78-148)
+  // Objective::beta (DICe_Objective.cpp:78-148): the finite-difference slope
+  // of the unnormalised gamma in u, v (and theta with rotation), ending with
+  // the subset re-initialised at the solution.
   __device__ float beta(const SubsetRef& sb, const float* slots) {
     const DevParams& P = A.P;
     MapConst k;
     make_mapconst<SHAPE>(slots, false, (float)sb.cx, (float)sb.cy, k);
     float u0, v0, t0;
     map_to_u_v_theta<SHAPE>(k, (float)sb.cx, (float)sb.cy, u0, v0, t0);
-    auto gam = [&](const float* s) {
-      PassOut o = pass<false, false, true>(sb, s, nullptr);
-      return gamma_from_unnormalised(o);
-    };
-    const float g0 = gam(slots);
+    const float g0 = eval_gamma(sb, slots, false);
     const float eps = 0.1f;
     const float fac[3] = {1.0e-3f, 1.0e-3f, 1.0e-1f};
     float dir[3] = {0.0f, 0.0f, 0.0f};
-    for (int i = 0; i < 3; ++i) {
-      if (!P.has_rot && i == 2 && SHAPE != DICEGPU_QUADRATIC_SF) continue;
+    float result = -1.0f;
+    bool bad = false;
+    for (int i = 0; i < 3 && !bad; ++i) {
       if (!P.has_rot && i == 2) continue;
       float u = u0, v = v0, t = t0;
       float s[12];
@@ -934,9 +1014,10 @@ struct Engine {
 #pragma unroll
         for (int j = 0; j < 12; ++j) s[j] = slots[j];
         if (SHAPE == DICEGPU_QUADRATIC_SF) {
+          // Quadratic_Shape_Function::insert_motion: clear, then the rigid motion
 #pragma unroll
           for (int j = 0; j < 12; ++j) s[j] = 0.0f;
-          s[0] = cosf(t); s[1] = -sinf(t); s[6] = sinf(t); s[7] = cosf(t);
+          s[0] = cos_f(t); s[1] = -sin_f(t); s[6] = sin_f(t); s[7] = cos_f(t);
           s[5] = u; s[11] = v;
         } else {
           s[0] = u; s[1] = v;
@@ -945,32 +1026,27 @@ struct Engine {
       };
       if (i == 0) u += eps; else if (i == 1) v += eps; else t += eps;
       insert();
-      const float gp = gam(s);
+      const float gp = eval_gamma(sb, s, false);
       if (i == 0) u -= 2 * eps; else if (i == 1) v -= 2 * eps; else t -= 2 * eps;
       insert();
-      const float gm = gam(s);
-      if (fabsf(gm - g0) < 1.0e-10f || fabsf(gp - g0) < 1.0e-10f) return -1.0f;
+      const float gm = eval_gamma(sb, s, false);
+      if ((double)fabsf(gm - g0) < 1.0e-10 || (double)fabsf(gp - g0) < 1.0e-10) {
+        bad = true;
+        break;
+      }
       const float sm = fabsf(eps / (gm - g0)) * fac[i];
       const float sp = fabsf(eps / (gp - g0)) * fac[i];
       dir[i] = (float)((double)(sm + sp) / 2.0);
     }
-    float mag = 0.0f;
-    for (int i = 0; i < 3; ++i) {
-      if (!P.has_rot && i == 2) continue;
-      mag += dir[i] * dir[i];
+    if (!bad) {
+      float mag = 0.0f;
+      for (int i = 0; i < 3; ++i) {
+        if (!P.has_rot && i == 2) continue;
+        mag += dir[i] * dir[i];
+      }
+      result = __fsqrt_rn(mag);
     }
-    return sqrtf(mag);
-  }
-
-  __device__ float gamma_from_unnormalised(const PassOut& o) const {
-    if (o.n == 0) return -1.0f;
-    const double n = (double)o.n;
-    const double sgg = o.sG2 - o.sG * o.sG / n;
-    const double sff = o.sF2 - o.sumF * o.sumF / n;
-    const double sgf = o.sGF - o.sG * o.sumF / n;
-    if (!(sgg > 0.0) || !(sff > 0.0)) return -1.0f;
-    double g = 2.0 - 2.0 * sgf / sqrt(sgg * sff);
-    return (float)(g < 0.0 ? 0.0 : g);
+    return result;
   }
 
   // --------------------------------------------------------------------------
@@ -979,14 +1055,14 @@ struct Engine {
   __device__ void run(int idx) {
     npass_ = 0;
     run_subset(idx);
-    if (A.passes_out && lane == 0 && A.mode == MODE_CORRELATE) A.passes_out[idx] = npass_;
+    if (A.passes_out && tid == 0 && A.mode == MODE_CORRELATE) A.passes_out[idx] = npass_;
   }
 
   __device__ void run_subset(int idx) {
     const DevParams& P = A.P;
     double* f = A.fields + (size_t)idx * DICEGPU_FIELD_STRIDE;
-    // the subset's field row (32 doubles) in one coalesced load: lane c holds
-    // column c, read by shuffles
+    // the subset's field row (32 doubles) in one coalesced load per warp:
+    // lane c holds column c, read by shuffles
     const double fv = f[lane];
     auto fld = [&](int col) { return __shfl_sync(FULL, fv, col); };
     SubsetRef sb;
@@ -1001,10 +1077,6 @@ struct Engine {
       sb.off = A.geo.offsets[idx];
       sb.npix = A.geo.offsets[idx + 1] - sb.off;
     }
-    {
-      const int kx = min(max(sb.cx, 0), A.ref.w - 1), ky = min(max(sb.cy, 0), A.ref.h - 1);
-      sb.K = __ldg(A.ref.I + (size_t)ky * A.ref.w + kx);
-    }
     sb.masked = false;
     sb.evo = false;
     sb.nact = sb.npix;
@@ -1018,8 +1090,8 @@ struct Engine {
     float slots[12];
     if (A.mode == MODE_GAMMA) {
       load_slots_row(fv, slots);
-      const float g = eval_gamma(sb, slots);
-      if (lane == 0) A.gamma_out[idx] = g;
+      const float g = eval_gamma(sb, slots, P.normalize_gamma != 0);
+      if (tid == 0) A.gamma_out[idx] = g;
       return;
     }
     if (A.mode != MODE_CORRELATE) {
@@ -1041,13 +1113,13 @@ struct Engine {
     // Field_Value_Initializer::initial_guess (DICe_Initializer.cpp:398-436):
     // the subset's own row, or its neighbour's.  Subsets run in index order
     // in the reference: a lower neighbour ran earlier this frame (an earlier
-    // wave, or this warp just before in a chain: __syncwarp orders lane 0's
-    // writes), a higher one contributes its frame-start row.
+    // wave, or this CTA just before in a chain: the barriers at the end of
+    // the previous subset order thread 0's writes), a higher one contributes
+    // its frame-start row.
     double gv = fv;
     int init_status = DICEGPU_INITIALIZE_USING_PREVIOUS_FRAME_SUCCESSFUL;
     const int nb = A.neigh ? A.neigh[idx] : -1;
     if (nb >= 0 && nb < A.n && nb != idx) {
-      __syncwarp();
       gv = (nb < idx ? A.fields : A.nsnap)[(size_t)nb * DICEGPU_FIELD_STRIDE + lane];
       init_status = DICEGPU_INITIALIZE_USING_NEIGHBOR_VALUE_SUCCESSFUL;
     }
@@ -1066,16 +1138,13 @@ struct Engine {
                         __fsub_rn((float)fld(DICEGPU_F_COORD_Y), (float)__shfl_sync(FULL, gv, DICEGPU_F_COORD_Y)));
     };
     initial_guess();
-    // reference mean at Gauss-Newton entry: over the pixels active at the last
-    // deformed-state initialisation (none yet: all of them)
+    // the deformed state of the subset: none yet (Gauss-Newton then takes the
+    // reference mean over all its pixels)
     bool have_state = false;
-    PassOut last_state;
     float last_eval[12];
     if (P.init_gamma_thr != -1.0) {
-      PassOut o;
-      const float g0 = eval_gamma(sb, slots, &o);
+      const float g0 = eval_gamma(sb, slots, P.normalize_gamma != 0);
       have_state = true;
-      last_state = o;
       if (g0 > P.init_gamma_thr || g0 < 0.0f) {
         record_failed(f, DICEGPU_INITIALIZE_FAILED, num_iterations);
         return;
@@ -1089,29 +1158,16 @@ struct Engine {
     int corr_status = DICEGPU_CORRELATION_FAILED;
     float cond = 0.0f;
     bool cond_set = false;
-    bool state_from_simplex = false;
-    (void)state_from_simplex;
     auto run_gn = [&]() {
-      // Subset::mean(REF_INTENSITIES) at entry: over the pixels active at the
-      // last deformed-state initialisation, or all pixels of a fresh subset
-      // (then taken from the first pass)
-      float meanF = 0.0f;
-      if (have_state) {
-        const int n = last_state.n;
-        meanF = n ? (float)((last_state.sumF + (double)n * (double)sb.K) / (double)n) : 0.0f;
-      }
-      corr_status = gauss_newton(sb, slots, meanF, !have_state, num_iterations, cond, last_state);
+      corr_status = gauss_newton(sb, slots, have_state, num_iterations, cond);
       have_state = true;
-      state_from_simplex = false;
       cond_set = true;
     };
     auto run_simplex = [&]() {
       corr_status = simplex(sb, slots, num_iterations, last_eval);
       // state of the last evaluation: active set, gradients and bounding box
-      last_state = pass<false, true, true>(sb, last_eval, nullptr);
-      ++npass_;
+      pass<PK_STATE>(sb, last_eval);
       have_state = true;
-      state_from_simplex = true;
     };
     DG_PT(t_first);
     if (opt == DICEGPU_SIMPLEX || opt == DICEGPU_SIMPLEX_THEN_GRADIENT_BASED || force_simplex) {
@@ -1143,7 +1199,7 @@ struct Engine {
         if (corr_status != DICEGPU_CORRELATION_SUCCESSFUL) second_failed = true;
       }
       if (second_failed && corr_status != DICEGPU_CORRELATION_SUCCESSFUL) {
-        if (cond_set && lane == 0) f[DICEGPU_F_CONDITION] = cond;
+        if (cond_set && tid == 0) f[DICEGPU_F_CONDITION] = cond;
         record_failed(f, corr_status, num_iterations);
         return;
       }
@@ -1152,21 +1208,23 @@ struct Engine {
       make_mapconst<SHAPE>(slots, false, fcx, fcy, kc);
       map_to_u_v_theta<SHAPE>(kc, fcx, fcy, nu, nv, nt);
     }
-    if (cond_set && lane == 0) f[DICEGPU_F_CONDITION] = cond;
-    // sigma needs the gradients of the last deformed-state initialisation
-    const PassOut st = last_state;
+    if (cond_set && tid == 0) f[DICEGPU_F_CONDITION] = cond;
+    // sigma from the state of the last deformed-state initialisation
     float noise = 0.0f;
     DG_PT(t_sig);
-    const float sg = sigma(sb, st, slots, noise);
+    const float sg = sigma(sb, slots, noise);
     DG_PACC(3, t_sig);
     if (sg < 0.0f) {
       record_failed(f, DICEGPU_FRAME_FAILED_DUE_TO_NEGATIVE_SIGMA, num_iterations);
       return;
     }
-    PassOut fin;
     DG_PT(t_gam);
-    const float gamma = eval_gamma(sb, slots, &fin);
+    float def_sum2 = 0.0f;
+    const float gamma = eval_gamma(sb, slots, P.normalize_gamma != 0, &def_sum2);
+    const int fin_n = ctl().n;
     DG_PACC(4, t_gam);
+    // beta ends with the subset re-initialised at the solution, where the
+    // gamma pass just left it
     const float bt = P.output_beta ? beta(sb, slots) : 0.0f;
     if ((P.final_gamma_thr != -1.0 && gamma > P.final_gamma_thr) || gamma < 0.0f) {
       record_failed(f, DICEGPU_FRAME_FAILED_DUE_TO_HIGH_GAMMA, num_iterations);
@@ -1177,15 +1235,9 @@ struct Engine {
       record_failed(f, DICEGPU_JUMP_TOLERANCE_EXCEEDED, num_iterations);
       return;
     }
-    // contrast_std_dev and num_active_pixels at the final parameters
-    float contrast = 0.0f;
-    if (fin.n > 0) {
-      const double nn = (double)fin.n;
-      double sgg = fin.sG2 - fin.sG * fin.sG / nn;
-      if (sgg < 0.0) sgg = 0.0;
-      contrast = (float)sqrt(sgg / nn);
-    }
-    if (lane == 0) {
+    // contrast_std_dev (DICe_Subset.cpp:607-620) at the final parameters
+    const float contrast = fin_n == 0 ? 0.0f : __fsqrt_rn(__fdiv_rn(def_sum2, (float)fin_n));
+    if (tid == 0) {
       // record_step (DICe_Schema.cpp:1986-2009), save_fields
       if (SHAPE == DICEGPU_QUADRATIC_SF) {
         for (int i = 0; i < 12; ++i) f[DICEGPU_F_QUAD_A + i] = slots[i];
@@ -1206,7 +1258,7 @@ struct Engine {
       f[DICEGPU_F_BETA] = bt;
       f[DICEGPU_F_NOISE] = noise;
       f[DICEGPU_F_CONTRAST] = contrast;
-      f[DICEGPU_F_ACTIVE_PIXELS] = fin.n;
+      f[DICEGPU_F_ACTIVE_PIXELS] = fin_n;
       f[DICEGPU_F_STATUS] = init_status;
       f[DICEGPU_F_ITERATIONS] = num_iterations;
     }

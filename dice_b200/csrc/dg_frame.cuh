@@ -2,7 +2,7 @@
 //
 // frame_kernel<shape, interp, defgrad, mask> runs Schema::execute_correlation
 // (or one Objective entry point, by mode) for every subset of a launch: one
-// warp per subset from interleaved per-CTA work queues.  The unmasked
+// CTA per subset from interleaved per-CTA work queues.  The unmasked
 // instantiations are compiled with the rest of the library (dicegpu.cu), the
 // masked ones in frame_masked.cu, so that both compile in parallel and the
 // unmasked kernels are exactly what they are without masks.
@@ -10,9 +10,12 @@
 
 #include "dg_engine.cuh"
 
-// minimum resident 256-thread blocks per SM the frame kernel is compiled for
-// (bounds its registers: 2 -> 128 per thread, 3 -> 80; 128 measured ~3 %
-// faster on the 2048^2 sequence despite the lower occupancy)
+// launch bounds of the frame kernel: at most DG_MAX_THREADS threads per CTA
+// (warps per subset <= DG_MAX_THREADS / 32) and DG_MIN_BLOCKS resident CTAs
+// of that size per SM, which bounds its registers
+#ifndef DG_MAX_THREADS
+#define DG_MAX_THREADS 256
+#endif
 #ifndef DG_MIN_BLOCKS
 #define DG_MIN_BLOCKS 2
 #endif
@@ -20,14 +23,14 @@
 namespace dg {
 
 // ---------------------------------------------------------------------------
-// the persistent frame kernel
+// the persistent frame kernel: one CTA (up to 8 warps) per subset
 // ---------------------------------------------------------------------------
 template <int SHAPE, int INTERP, bool DEFGRAD, bool MASK>
-__global__ void __launch_bounds__(256, DG_MIN_BLOCKS) frame_kernel(const __grid_constant__ FrameArgs a) {
+__global__ void __launch_bounds__(DG_MAX_THREADS, DG_MIN_BLOCKS) frame_kernel(const __grid_constant__ FrameArgs a) {
   Engine<SHAPE, INTERP, DEFGRAD, MASK> e(a);
-  const int lane = threadIdx.x & 31;
+  Ctl& c = ctl();
   if (a.plain_index >= 0) {
-    if (blockIdx.x == 0 && threadIdx.x < 32) e.run(a.plain_index);
+    if (blockIdx.x == 0) e.run(a.plain_index);
     return;
   }
   // the launch's subsets: all n, or the n_order listed in order
@@ -35,28 +38,29 @@ __global__ void __launch_bounds__(256, DG_MIN_BLOCKS) frame_kernel(const __grid_
   if (a.queue_mode == 0) {
     // one global queue head
     for (;;) {
-      int t = 0;
-      if (lane == 0) t = atomicAdd(a.work_counter, 1);
-      t = __shfl_sync(FULL, t, 0);
+      if (threadIdx.x == 0) c.work = atomicAdd(a.work_counter, 1);
+      __syncthreads();
+      const int t = c.work;
+      __syncthreads();
       if (t >= count) break;
       e.run(a.order ? a.order[t] : t);
     }
     return;
   }
   // Interleaved per-CTA queues: the subsets are cut into chunks of C
-  // consecutive ones and CTA r owns chunks r, r + G, r + 2G, ...  The warps of
-  // a CTA work on neighbouring subsets (shared footprint in L1) and all CTAs
-  // advance through the image together (a narrow band resident in L2).  A CTA
-  // whose chunks are exhausted takes from the following CTAs' sequences.
-  // Every index is taken exactly once (atomicAdd); a warp leaves after finding
-  // all G sequences exhausted, so no warp ever waits on another.
+  // consecutive ones and CTA r owns chunks r, r + G, r + 2G, ...  All CTAs
+  // advance through the image together (a narrow band resident in L2).  A
+  // CTA whose chunks are exhausted takes from the following CTAs' sequences.
+  // Every index is taken exactly once (atomicAdd); a CTA leaves after finding
+  // all G sequences exhausted, so no CTA ever waits on another.
   const int G = gridDim.x;
   const int C = a.chunk;
   int q = blockIdx.x;
   for (int visited = 0; visited < G;) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(a.work_counter + q, 1);
-    t = __shfl_sync(FULL, t, 0);
+    if (threadIdx.x == 0) c.work = atomicAdd(a.work_counter + q, 1);
+    __syncthreads();
+    const int t = c.work;
+    __syncthreads();
     const long long chunk = (long long)q + (long long)(t / C) * G;
     const long long lidx = chunk * C + (t % C);
     const int pos = lidx < count ? (int)lidx : count;
@@ -84,7 +88,7 @@ static FrameKernelFn pick_kernel(int interp, bool defgrad) {
   if (SHAPE == DICEGPU_AFFINE_SF && interp == DICEGPU_KEYS_FOURTH && defgrad)
     return frame_kernel<DICEGPU_AFFINE_SF, DICEGPU_KEYS_FOURTH, true, MASK>;
   return nullptr;
-#endif
+#else
   if (defgrad) {
     if (interp == DICEGPU_KEYS_FOURTH) return frame_kernel<SHAPE, DICEGPU_KEYS_FOURTH, true, MASK>;
     if (interp == DICEGPU_BICUBIC) return frame_kernel<SHAPE, DICEGPU_BICUBIC, true, MASK>;
@@ -93,6 +97,7 @@ static FrameKernelFn pick_kernel(int interp, bool defgrad) {
   if (interp == DICEGPU_KEYS_FOURTH) return frame_kernel<SHAPE, DICEGPU_KEYS_FOURTH, false, MASK>;
   if (interp == DICEGPU_BICUBIC) return frame_kernel<SHAPE, DICEGPU_BICUBIC, false, MASK>;
   return frame_kernel<SHAPE, DICEGPU_BILINEAR, false, MASK>;
+#endif
 }
 
 // the masked instantiations live in their own translation unit (frame_masked.cu)

@@ -1,11 +1,29 @@
-// dg_pass.cuh -- one warp-wide pass over the pixels of a subset.
+// dg_pass.cuh -- CTA-wide passes over the pixels of one subset, in the
+// reference's floating-point arithmetic.
 //
-// The hot loop of the path: Subset::initialize on the deformed image
-// (DICe_Subset.cpp:390-426) fused with the Gauss-Newton accumulation of
-// Objective_ZNSSD::computeUpdateFast (DICe_Objective.cpp:523-546) or with the
-// intensity moments of Subset::gamma (DICe_Subset.cpp:323-340).  It is a
-// separate non-inlined function taking everything it reads by value, so its
-// register allocation does not compete with the per-subset control code.
+// One CTA of W warps (T = 32 W threads) owns one subset at a time; thread t
+// takes subset pixels t, t + T, t + 2T, ...  A pass is Subset::initialize on
+// the deformed image (DICe_Subset.cpp:390-426): map, round, border and mask
+// tests, interpolation of the deformed image (and its gradients).  It keeps
+// every pixel's values in shared memory (reference intensity F, deformed
+// intensity G, gradients, stretched offsets, liveness), because the reference
+// then forms sums that depend on each other in order:
+//   * Subset::mean / gamma / contrast and Objective::sigma sum in float, one
+//     pixel after the other (DICe_Subset.cpp:285-340, 597-620,
+//     DICe_Objective.cpp:150-184): here one thread sums the stored values in
+//     pixel order (chain_sum), the only way to get the same float;
+//   * Objective_ZNSSD::computeUpdateFast (DICe_Objective.cpp:523-546) adds the
+//     float products r_i r_j and GmF r_i, each rounded to float, into double
+//     sums.  H = sum fl(r_i r_j) is formed as the exact products, summed by the
+//     FP64 tensor core (mma.sync m8n8k4), minus the sum of the products'
+//     rounding errors fma(r_i, r_j, -fl(r_i r_j)) (exact floats, summed per
+//     thread in float and across threads in double), in a sweep over the
+//     stored pixels (h_sweep) that runs while one thread sums the deformed
+//     mean; q needs that mean, so a last sweep (q_sweep) adds fl(GmF r_i) in
+//     double.
+// Double sums are taken in another order than the reference's sequential one;
+// that changes them in the last bits of a double (~1e-16 relative), far below
+// the float rounding of the parameter update they feed.
 #pragma once
 
 #include <type_traits>
@@ -14,14 +32,14 @@
 
 namespace dg {
 
-// Section timers of a profiling build (-DDG_PROFILE): warp cycles per section
-// summed over all warps.  Compiled out otherwise.
+// Section timers of a profiling build (-DDG_PROFILE): cycles per section
+// summed over all CTAs (thread 0's clock).  Compiled out otherwise.
 #ifdef DG_PROFILE
 static __device__ unsigned long long g_prof[8];   // per translation unit
 #define DG_PT(var) const long long var = clock64()
 #define DG_PACC(i, t0)                                                                    \
   do {                                                                                    \
-    if ((threadIdx.x & 31) == 0) atomicAdd(&g_prof[i], (unsigned long long)(clock64() - (t0))); \
+    if (threadIdx.x == 0) atomicAdd(&g_prof[i], (unsigned long long)(clock64() - (t0))); \
   } while (0)
 #else
 #define DG_PT(var)
@@ -31,39 +49,200 @@ static __device__ unsigned long long g_prof[8];   // per translation unit
 template <int SHAPE>
 struct Layout {
   static constexpr int NS = SHAPE == DICEGPU_QUADRATIC_SF ? 12 : 6;   // parameter slots
-  static constexpr int VW = SHAPE == DICEGPU_QUADRATIC_SF ? 16 : 8;   // [r, d, 1] padded
-  static constexpr int VS = SHAPE == DICEGPU_QUADRATIC_SF ? 24 : 8;   // smem row stride (conflict-free)
-  static constexpr int ID = NS;        // column of d = G - F
-  static constexpr int IONE = NS + 1;  // column of 1
+  static constexpr int VW = SHAPE == DICEGPU_QUADRATIC_SF ? 16 : 8;   // mma vector width (padded)
+  static constexpr int VS = SHAPE == DICEGPU_QUADRATIC_SF ? 24 : 8;   // staging row stride (floats)
+  static constexpr int NP = NS * (NS + 1) / 2;                        // products r_i r_j, i <= j
   static constexpr int NMAX = NS;
 };
 
-// Pixels per lane per step of a pass: each step maps, interpolates and
-// stages 32 * DG_PPL pixels before the mma accumulation, so that the tap
-// loads of DG_PPL independent pixels are in flight together.
-#ifndef DG_PPL
-#define DG_PPL 1
-#endif
-constexpr int PPL = DG_PPL;
-// independent FP64 mma accumulator sets of the affine pass
-#ifndef DG_NSET_AFFINE
-#define DG_NSET_AFFINE 2
-#endif
+// index of the pair (i, j), i <= j, of the upper triangle in row order
+__host__ __device__ constexpr int pair_index(int i, int j, int ns) { return i * ns - i * (i - 1) / 2 + (j - i); }
 
-template <int SHAPE>
-struct __align__(16) WarpSmem {
-  float vbuf[32 * PPL * Layout<SHAPE>::VS];
-  double M[Layout<SHAPE>::VW * Layout<SHAPE>::VW];
+// ---------------------------------------------------------------------------
+// Shared memory of a frame CTA
+// ---------------------------------------------------------------------------
+// Broadcast values and the Gauss-Newton solve's workspace (one per CTA).
+struct __align__(16) Ctl {
+  int work;                      // subset of this round
+  int n, minx, maxx, miny, maxy; // live pixels and their box, last pass
+  int status, conv, info;        // solve outcome
+  int pad0;
+  float fres[4];                 // chain results
+  float slots[12];               // parameters after a solve step
+  float upd_old[12];             // momentum: the previous update (compact order)
+  float cond;
+  float pad1[3];
+  double H[144];                 // Hessian (compact order, row major), then its LU factors
+  double q[12];
+  double inv[144];               // inverse, column k written by lane k
+  int piv[12];
 };
 
-// Dynamic shared memory of the frame kernel: one WarpSmem per warp.  Taken
-// from the extern array in every user so the compiler keeps shared-space
-// (not generic) addressing.
-extern __shared__ __align__(16) unsigned char dg_smem[];
+// Per-warp partial results of a pass.
+template <int SHAPE>
+struct __align__(16) WarpOut {
+  double M[Layout<SHAPE>::VW * Layout<SHAPE>::VW];   // exact product sums
+  double E[Layout<SHAPE>::NP];                       // rounding errors of the float products
+  double q[Layout<SHAPE>::NS];                       // right-hand side (slot order)
+  int n, minx, maxx, miny, maxy, pad[3];
+};
+
+// The Nelder-Mead state of Simplex::minimize (DICe_Simplex.cpp:60-277), one
+// copy per warp: every warp runs the same bookkeeping on its own copy (lane 0
+// writes, the warp reads after __syncwarp), so all warps take the same
+// branches and evaluate the same points together.
+struct __align__(16) SimplexState {
+  float pts[13][12];
+  float gv[13];
+  float psum[12];
+  float ptry[12];
+  float init[12];
+  float base[12];
+};
+
+__host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~(size_t)15; }
+// per-pixel array capacity: a multiple of 16 pixels (16-byte aligned rows)
+__host__ __device__ inline int pix_cap(int npix_max) { return (npix_max + 15) & ~15; }
 
 template <int SHAPE>
-__device__ __forceinline__ WarpSmem<SHAPE>* warp_smem() {
-  return reinterpret_cast<WarpSmem<SHAPE>*>(dg_smem) + (threadIdx.x >> 5);
+struct SmemPlan {
+  static __host__ __device__ size_t wout(int) { return a16(sizeof(Ctl)); }
+  static __host__ __device__ size_t simplex(int W) { return wout(W) + a16((size_t)W * sizeof(WarpOut<SHAPE>)); }
+  static __host__ __device__ size_t vbuf(int W) { return simplex(W) + a16((size_t)W * sizeof(SimplexState)); }
+  static __host__ __device__ size_t pix(int W) {
+    return vbuf(W) + a16((size_t)W * 32 * Layout<SHAPE>::VS * sizeof(float));
+  }
+  // six float arrays and one byte array of `cap` pixels
+  static __host__ __device__ size_t pix_bytes(int cap) { return a16((size_t)cap * (6 * 4 + 1)); }
+  static __host__ __device__ size_t total(int W, int cap) { return pix(W) + pix_bytes(cap); }
+};
+
+extern __shared__ __align__(16) unsigned char dg_smem[];
+
+__device__ __forceinline__ Ctl& ctl() { return *reinterpret_cast<Ctl*>(dg_smem); }
+template <int SHAPE>
+__device__ __forceinline__ WarpOut<SHAPE>* wouts() {
+  return reinterpret_cast<WarpOut<SHAPE>*>(dg_smem + SmemPlan<SHAPE>::wout(blockDim.x >> 5));
+}
+template <int SHAPE>
+__device__ __forceinline__ SimplexState& sx_state() {
+  return reinterpret_cast<SimplexState*>(dg_smem + SmemPlan<SHAPE>::simplex(blockDim.x >> 5))[threadIdx.x >> 5];
+}
+template <int SHAPE>
+__device__ __forceinline__ float* warp_vbuf() {
+  return reinterpret_cast<float*>(dg_smem + SmemPlan<SHAPE>::vbuf(blockDim.x >> 5)) +
+         (threadIdx.x >> 5) * 32 * Layout<SHAPE>::VS;
+}
+
+// The per-pixel arrays: F (reference intensity), G (deformed intensity, 0 at
+// pixels that are not live), GX / GY (gradients used by the residuals), DX /
+// DY (the affine map's stretched offsets), L (bit 0 live: active and not
+// deactivated this step; bit 1 active).
+struct PixArrays {
+  float* F;
+  float* G;
+  float* GX;
+  float* GY;
+  float* DX;
+  float* DY;
+  uint8_t* L;
+};
+// Where a CTA's pixel arrays live: its shared memory, or for subsets too
+// large for it, this CTA's slice of a global scratch buffer (`stride` bytes
+// per CTA).
+template <int SHAPE>
+__device__ __forceinline__ float* pix_base(unsigned char* scratch, size_t stride) {
+  return scratch ? reinterpret_cast<float*>(scratch + (size_t)blockIdx.x * stride)
+                 : reinterpret_cast<float*>(dg_smem + SmemPlan<SHAPE>::pix(blockDim.x >> 5));
+}
+__device__ __forceinline__ PixArrays pix_arrays_at(float* b, int cap) {
+  PixArrays a;
+  a.F = b;
+  a.G = b + cap;
+  a.GX = b + 2 * (size_t)cap;
+  a.GY = b + 3 * (size_t)cap;
+  a.DX = b + 4 * (size_t)cap;
+  a.DY = b + 5 * (size_t)cap;
+  a.L = reinterpret_cast<uint8_t*>(b + 6 * (size_t)cap);
+  return a;
+}
+
+// ---------------------------------------------------------------------------
+// CTA reductions and sequential float sums (fixed order: deterministic)
+// ---------------------------------------------------------------------------
+// CTA-wide double sum of one value per thread, the same in every thread.
+// Uses Ctl's inv[] as scratch; starts and ends with a barrier.
+__device__ __forceinline__ double cta_sum(double v) {
+  Ctl& c = ctl();
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) c.inv[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  const int W = blockDim.x >> 5;
+  for (int w = 0; w < W; ++w) s += c.inv[w];
+  __syncthreads();
+  return s;
+}
+__device__ __forceinline__ int cta_sum_i(int v) {
+  return (int)cta_sum((double)v);
+}
+
+// Sequential float sum a[0] + a[1] + ... + a[n-1] starting from 0.0f, each
+// addition rounded: the reference's `sum += x` loop.  a is 16-byte aligned.
+// Zeros stand for skipped pixels: adding +0.0f leaves every running sum
+// unchanged (the sum, starting at +0.0f, is never -0.0f).
+__device__ __forceinline__ float chain_sum(const float* a, int n, float s = 0.0f) {
+  int i = 0;
+  const float4* a4 = reinterpret_cast<const float4*>(a);
+#pragma unroll 4
+  for (; i + 4 <= n; i += 4) {
+    const float4 v = a4[i >> 2];
+    s = __fadd_rn(s, v.x);
+    s = __fadd_rn(s, v.y);
+    s = __fadd_rn(s, v.z);
+    s = __fadd_rn(s, v.w);
+  }
+  for (; i < n; ++i) s = __fadd_rn(s, a[i]);
+  return s;
+}
+
+// The same over the pixels whose liveness byte has `bit` set (the others
+// count as +0.0f); a and m are 16- and 4-byte aligned.
+__device__ __forceinline__ float chain_sum_masked(const float* a, const uint8_t* m, unsigned bit, int n) {
+  float s = 0.0f;
+  int i = 0;
+  const float4* a4 = reinterpret_cast<const float4*>(a);
+  const uchar4* m4 = reinterpret_cast<const uchar4*>(m);
+#pragma unroll 4
+  for (; i + 4 <= n; i += 4) {
+    const float4 v = a4[i >> 2];
+    const uchar4 b = m4[i >> 2];
+    s = __fadd_rn(s, (b.x & bit) ? v.x : 0.0f);
+    s = __fadd_rn(s, (b.y & bit) ? v.y : 0.0f);
+    s = __fadd_rn(s, (b.z & bit) ? v.z : 0.0f);
+    s = __fadd_rn(s, (b.w & bit) ? v.w : 0.0f);
+  }
+  for (; i < n; ++i) s = __fadd_rn(s, (m[i] & bit) ? a[i] : 0.0f);
+  return s;
+}
+
+// Up to four chains at once (lanes 0..k-1 of warp 0, in lockstep), chain i
+// over the pixels whose liveness byte in m has a bit of byte i of `bits` set
+// (all pixels when m is null); results in every thread.  Barriers before
+// (the arrays are complete) and after.
+__device__ __forceinline__ void chains(int k, const float* a0, const float* a1, const float* a2, const float* a3,
+                                       const uint8_t* m, unsigned bits, int n, float* out) {
+  Ctl& c = ctl();
+  __syncthreads();
+  if (threadIdx.x < k) {
+    const float* a = threadIdx.x == 0 ? a0 : threadIdx.x == 1 ? a1 : threadIdx.x == 2 ? a2 : a3;
+    const unsigned bit = (bits >> (8 * threadIdx.x)) & 0xffu;
+    c.fres[threadIdx.x] = m ? chain_sum_masked(a, m, bit, n) : chain_sum(a, n);
+  }
+  __syncthreads();
+  for (int i = 0; i < k; ++i) out[i] = c.fres[i];
+  __syncthreads();
 }
 
 __device__ __forceinline__ void sts_v4(unsigned addr, float a, float b, float c, float d) {
@@ -76,17 +255,9 @@ __device__ __forceinline__ float lds_f(unsigned addr) {
   return v;
 }
 
-// Result of one pass over the subset pixels.
-struct PassOut {
-  int n;                    // active pixels
-  double sumF;              // sum of F over active pixels (shifted by K)
-  double sumFall;           // sum of F over all subset pixels (shifted; Gauss-Newton passes)
-  double sG, sG2, sF2, sGF; // shifted moments (gamma passes)
-  double sgx2, sgy2;        // sum of unrotated gradient^2 (sigma)
-  int minx, maxx, miny, maxy;
-};
-
-// Everything a pass reads, passed by value.
+// ---------------------------------------------------------------------------
+// Pass inputs
+// ---------------------------------------------------------------------------
 struct PassIn {
   DevImage def;
   const float* __restrict__ refI;
@@ -98,11 +269,11 @@ struct PassIn {
   const int32_t* __restrict__ py;
   int half;        // square half-width (lists: unused)
   int cx, cy, npix, off;
-  float K;         // intensity shift for the moment sums
+  int cap;         // per-pixel array capacity
+  float* pix;      // the CTA's per-pixel arrays (pix_base)
 };
 
-// What a MASKED pass reads besides (the unmasked passes get the plain
-// PassIn, which the call passes by value): this subset's mask descriptor
+// What a MASKED pass reads besides: this subset's mask descriptor
 // (obstruction box x0, y0, w, h, word offset; blocked polygon count and
 // table offset), the obstruction words, the blocked-polygon table (vertex
 // offset, count, box x0, x1, y0, y1 per polygon), the polygons' vertices,
@@ -160,150 +331,213 @@ struct MaskView {
   }
 };
 
-//   ACC_H   : accumulate sum v v^T into the warp's smem matrix (Gauss-Newton)
-//   GRADS   : interpolate the deformed gradients (DEFGRAD) / read reference ones
-//   MOMENTS : FP64 intensity moments for gamma
-//   MASKED  : also deactivate pixels whose position rounds into the
-//             subset's obstruction bitmap or a blocked polygon (Subset::initialize,
-//             DICe_Subset.cpp:412-422); for positive coordinates, which the
-//             border test leaves, is_obstructed_pixel's rounding is the
-//             border test's
-template <int SHAPE, int INTERP, bool DEFGRAD, bool ACC_H, bool GRADS, bool MOMENTS, bool MASKED>
-__device__ __noinline__ PassOut subset_pass(const PassInT<MASKED> in, const MapConst k) {
-  using L = Layout<SHAPE>;
-  const int lane = threadIdx.x & 31;
-  const bool use_ref_grads = !DEFGRAD;
+// Pixel coordinates of pixel p of a subset (clamped at 0 as the Subset
+// constructors do, DICe_Subset.cpp:66-68, :100-101).
+struct PixelWalk {
+  int side, x0, y0, row, col, drow, dcol;
+  bool square;
+  __device__ __forceinline__ PixelWalk(const PassIn& in, int first, int step) {
+    square = in.off < 0;
+    side = 2 * in.half + 1;
+    x0 = in.cx - in.half;
+    y0 = in.cy - in.half;
+    row = col = drow = dcol = 0;
+    if (square) {
+      row = first / side; col = first - row * side;
+      drow = step / side; dcol = step - drow * side;
+    }
+  }
+  __device__ __forceinline__ void xy(const PassIn& in, int p, int& x, int& y) const {
+    if (square) {
+      x = max(x0 + col, 0);
+      y = max(y0 + row, 0);
+    } else {
+      x = max(__ldg(in.px + in.off + p), 0);
+      y = max(__ldg(in.py + in.off + p), 0);
+    }
+  }
+  __device__ __forceinline__ void advance() {
+    if (square) {
+      col += dcol; row += drow;
+      if (col >= side) { col -= side; ++row; }
+    }
+  }
+};
+
+// Kinds of pass:
+//   PK_GN    : the Gauss-Newton iteration's initialisation: gradients, every
+//              per-pixel array (the sums follow in h_sweep and q_sweep)
+//   PK_STATE : deformed-state initialisation with gradients (sigma's state)
+//   PK_GAMMA : intensities only (gamma, simplex evaluations)
+enum { PK_GN = 0, PK_STATE = 1, PK_GAMMA = 2 };
+
+// One pass (Subset::initialize on the deformed image).  Ends with the live
+// count and box in Ctl (all threads may read them after the final barrier).
+template <int SHAPE, int INTERP, bool DEFGRAD, int KIND, bool MASKED>
+__device__ __noinline__ void cta_pass(const PassInT<MASKED> in, const MapConst k) {
+  constexpr bool GRADS = KIND != PK_GAMMA;
+  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
   const float fcx = (float)in.cx, fcy = (float)in.cy;
   const int W = in.def.w, H = in.def.h;
-  PassOut o;
+  const PixArrays A = pix_arrays_at(in.pix, in.cap);
   int n = 0;
-  // per-lane partial sums: FP32 over this lane's pixels (the reference sums
-  // these in FP32 over the whole subset), FP64 across the warp; the gamma
-  // moments are FP64 throughout
-  float sumF = 0.0f, sgx2 = 0.0f, sgy2 = 0.0f, sumFall = 0.0f;
-  double sG = 0.0, sG2 = 0.0, sF2 = 0.0, sGF = 0.0, sFd = 0.0;
   int minx = in.cx, maxx = in.cx, miny = in.cy, maxy = in.cy;
-  // independent accumulator sets (pixel group g goes to set g % NSET) so that
-  // consecutive mma instructions do not wait on each other
-  constexpr int NSET = SHAPE == DICEGPU_QUADRATIC_SF ? 2 : DG_NSET_AFFINE;
+  MaskView mv;
+  if constexpr (MASKED) mv = MaskView(in.mdesc, in.mbits, in.bpoly, in.bvx, in.bvy);
+  PixelWalk pw(in, tid, T);
+  for (int p = tid; p < in.npix; p += T) {
+    int x, y;
+    pw.xy(in, p, x, y);
+    pw.advance();
+    // the reference reads intensities_[y*w+x] unchecked (row-major wrap);
+    // same element inside the array, 0 outside it
+    const long ri = (long)y * in.refw + x;
+    const bool rin = ri < in.reflim;
+    float F = rin ? __ldg(in.refI + ri) : 0.0f;
+    // subset evolution: an inactive pixel takes no part; a turned-on one
+    // has its stored reference intensity
+    bool active = true;
+    if constexpr (MASKED) {
+      if (in.pflag) {
+        const int st = in.pflag[in.off + p];
+        active = st != 0;
+        if (st == 2) F = in.pfv[in.off + p];
+      }
+    }
+    float mx, my, Dx, Dy;
+    const float dxf = __fsub_rn((float)x, fcx), dyf = __fsub_rn((float)y, fcy);
+    map_offset<SHAPE>(k, dxf, dyf, fcx, fcy, mx, my, Dx, Dy);
+    const int px = round_pixel(mx), py = round_pixel(my);
+    // 4-pixel border deactivation (DICe_Subset.cpp:408)
+    bool live = active && !(px < 4 || px >= W - 4 || py < 4 || py >= H - 4);
+    if (MASKED && live) live = !mv.hides(px, py);
+    float G = 0.0f, gx = 0.0f, gy = 0.0f;
+    if (live) {
+      if (GRADS && DEFGRAD) interp_ref<INTERP, true>(in.def, mx, my, G, gx, gy);
+      else interp_ref<INTERP, false>(in.def, mx, my, G, gx, gy);
+      if (GRADS && !DEFGRAD) {
+        gx = rin ? __ldg(in.refgx + ri) : 0.0f;
+        gy = rin ? __ldg(in.refgy + ri) : 0.0f;
+      }
+      ++n;
+      minx = min(minx, x); maxx = max(maxx, x);
+      miny = min(miny, y); maxy = max(maxy, y);
+    }
+    A.F[p] = F;
+    A.G[p] = live ? G : 0.0f;
+    A.L[p] = (uint8_t)((live ? 1 : 0) | (active ? 2 : 0));
+    if (GRADS) {
+      A.GX[p] = gx;
+      A.GY[p] = gy;
+    }
+    if (KIND == PK_GN && SHAPE != DICEGPU_QUADRATIC_SF) {
+      A.DX[p] = Dx;
+      A.DY[p] = Dy;
+    }
+  }
+  // per-warp results
+  WarpOut<SHAPE>& wo = wouts<SHAPE>()[warp];
+  n = warp_sum_i(n);
+  minx = warp_min_i(minx); maxx = warp_max_i(maxx);
+  miny = warp_min_i(miny); maxy = warp_max_i(maxy);
+  if (lane == 0) {
+    wo.n = n; wo.minx = minx; wo.maxx = maxx; wo.miny = miny; wo.maxy = maxy;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    Ctl& cl = ctl();
+    const WarpOut<SHAPE>* all = wouts<SHAPE>();
+    int nn = 0, a0 = in.cx, a1 = in.cx, b0 = in.cy, b1 = in.cy;
+    const int NW = T >> 5;
+    for (int w = 0; w < NW; ++w) {
+      nn += all[w].n;
+      a0 = min(a0, all[w].minx); a1 = max(a1, all[w].maxx);
+      b0 = min(b0, all[w].miny); b1 = max(b1, all[w].maxy);
+    }
+    cl.n = nn; cl.minx = a0; cl.maxx = a1; cl.miny = b0; cl.maxy = b1;
+  }
+  __syncthreads();
+}
+
+// Residual vector of a stored pixel (the affine map's stretched offsets were
+// stored by the PK_GN pass; quadratic residuals use the plain offsets).
+template <int SHAPE>
+__device__ __forceinline__ void stored_residuals(const PassIn& in, const PixArrays& A, const MapConst& k, int p, int x,
+                                                 int y, bool use_ref_grads, float* r) {
+  const float dxf = __fsub_rn((float)x, (float)in.cx), dyf = __fsub_rn((float)y, (float)in.cy);
+  float Dx = dxf, Dy = dyf;
+  if (SHAPE != DICEGPU_QUADRATIC_SF) {
+    Dx = A.DX[p];
+    Dy = A.DY[p];
+  }
+  residuals_D<SHAPE>(k, dxf, dyf, Dx, Dy, A.GX[p], A.GY[p], use_ref_grads, r);
+}
+
+// The Hessian sweep over the stored pixels, run by warps w0 .. w0 + nw - 1
+// (full warps; pixel p goes to thread p mod 32 nw of them): the exact
+// products r_i r_j summed by the FP64 mma (WarpOut.M) and the float
+// products' rounding errors fma(r_i, r_j, -fl(r_i r_j)) (WarpOut.E), whose
+// difference is the reference's sum of float products.  Warps outside the
+// range return at once.  No barrier.
+template <int SHAPE, bool DEFGRAD>
+__device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, int nw) {
+  using L = Layout<SHAPE>;
+  constexpr int NSET = 2;   // independent mma accumulator sets
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < w0 || warp >= w0 + nw) return;
+  const int t = (warp - w0) * 32 + lane, TT = 32 * nw;
+  const bool use_ref_grads = !DEFGRAD;
+  const PixArrays A = pix_arrays_at(in.pix, in.cap);
   double c[NSET][3][2];
+  float e[L::NP];
 #pragma unroll
   for (int s2 = 0; s2 < NSET; ++s2)
 #pragma unroll
     for (int b = 0; b < 3; ++b) { c[s2][b][0] = 0.0; c[s2][b][1] = 0.0; }
-  // square subsets: (row, col) of this lane's pixel advanced by 32 per step
-  const int side = 2 * in.half + 1;
-  int row = 0, col = 0, drow = 0, dcol = 0;
-  if (in.off < 0) {
-    row = lane / side; col = lane - row * side;
-    drow = 32 / side; dcol = 32 - drow * side;
-  }
-  const int x0 = in.cx - in.half, y0 = in.cy - in.half;
-  MaskView mv;
-  if constexpr (MASKED) mv = MaskView(in.mdesc, in.mbits, in.bpoly, in.bvx, in.bvy);
-  const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_smem<SHAPE>()->vbuf);
-  for (int base = 0; base < in.npix; base += 32 * PPL) {
-    float vv[PPL][L::VW];
 #pragma unroll
-    for (int u = 0; u < PPL; ++u) {
-    float* v = vv[u];
-    const int p = base + 32 * u + lane;
+  for (int i = 0; i < L::NP; ++i) e[i] = 0.0f;
+  PixelWalk pw(in, t, TT);
+  const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_vbuf<SHAPE>());
+  for (int base = 0; base < in.npix; base += TT) {
+    const int p = base + t;
+    float v[L::VW];
 #pragma unroll
     for (int i = 0; i < L::VW; ++i) v[i] = 0.0f;
-    int x = 0, y = 0;
-    if (in.off < 0) {
-      x = max(x0 + col, 0);   // Subset ctors clamp negative coordinates (DICe_Subset.cpp:66-68, :100-101)
-      y = max(y0 + row, 0);
-      col += dcol; row += drow;
-      if (col >= side) { col -= side; ++row; }
-    } else if (p < in.npix) {
-      x = max(__ldg(in.px + in.off + p), 0);
-      y = max(__ldg(in.py + in.off + p), 0);
-    }
-    if (p < in.npix) {
-      float mx, my, Dx, Dy;
-      const float dxf = __fsub_rn((float)x, fcx), dyf = __fsub_rn((float)y, fcy);
-      map_offset<SHAPE>(k, dxf, dyf, fcx, fcy, mx, my, Dx, Dy);
-      const int px = round_pixel(mx), py = round_pixel(my);
-      // the reference reads intensities_[y*w+x] unchecked (row-major wrap);
-      // same element inside the array, 0 outside it
-      const long ri = (long)y * in.refw + x;
-      const bool rin = ri < in.reflim;
-      float F = rin ? __ldg(in.refI + ri) : 0.0f;
-      // subset evolution: an inactive pixel takes no part; a turned-on one
-      // has its stored reference intensity
-      bool active = true;
-      if constexpr (MASKED) {
-        if (in.pflag) {
-          const int st = in.pflag[in.off + p];
-          active = st != 0;
-          if (st == 2) F = in.pfv[in.off + p];
-        }
-      }
-      if (ACC_H && active) sumFall += F - in.K;
-      // 4-pixel border deactivation (DICe_Subset.cpp:408)
-      bool live = active && !(px < 4 || px >= W - 4 || py < 4 || py >= H - 4);
-      if (MASKED && live) live = !mv.hides(px, py);
-      if (live) {
-        float G, gx = 0.0f, gy = 0.0f;
-        if (GRADS && DEFGRAD) interp_interior<INTERP, true>(in.def, mx, my, G, gx, gy);
-        else interp_interior<INTERP, false>(in.def, mx, my, G, gx, gy);
-        if (GRADS && !DEFGRAD) {
-          gx = rin ? __ldg(in.refgx + ri) : 0.0f;
-          gy = rin ? __ldg(in.refgy + ri) : 0.0f;
-        }
-        ++n;
-        const float Fs = F - in.K, Gs = G - in.K;
-        if (MOMENTS) {
-          sFd += (double)Fs;
-          sG += (double)Gs;
-          sG2 = fma((double)Gs, (double)Gs, sG2);
-          sF2 = fma((double)Fs, (double)Fs, sF2);
-          sGF = fma((double)Gs, (double)Fs, sGF);
-        } else {
-          sumF += Fs;
-        }
-        if (GRADS) {
-          sgx2 = fmaf(gx, gx, sgx2);
-          sgy2 = fmaf(gy, gy, sgy2);
-          minx = min(minx, x); maxx = max(maxx, x);
-          miny = min(miny, y); maxy = max(maxy, y);
-        }
-        if (ACC_H) {
-          residuals_D<SHAPE>(k, dxf, dyf, Dx, Dy, gx, gy, use_ref_grads, v);
-          v[L::ID] = G - F;
-          v[L::IONE] = 1.0f;
-        }
-      }
-    }
-    }
-    if (ACC_H) {
-      // stage the 32 * PPL pixel vectors, then groups of 4 pixels through the FP64 mma
+    if (p < in.npix && (A.L[p] & 1)) {
+      int x, y;
+      pw.xy(in, p, x, y);
+      stored_residuals<SHAPE>(in, A, k, p, x, y, use_ref_grads, v);
+      int idx = 0;
 #pragma unroll
-      for (int u = 0; u < PPL; ++u) {
-        const unsigned vrow = vbase + (unsigned)((32 * u + lane) * L::VS) * 4u;
+      for (int i = 0; i < L::NS; ++i)
 #pragma unroll
-        for (int i = 0; i < L::VW; i += 4)
-          sts_v4(vrow + 4u * i, vv[u][i], vv[u][i + 1], vv[u][i + 2], vv[u][i + 3]);
-      }
-      __syncwarp();
-      const int kk = lane & 3, ii = lane >> 2;
-#pragma unroll
-      for (int g = 0; g < 8 * PPL; ++g) {
-        const unsigned src = vbase + (unsigned)((4 * g + kk) * L::VS + ii) * 4u;
-        double(&cs)[3][2] = c[g % NSET];
-        if (SHAPE == DICEGPU_QUADRATIC_SF) {
-          const double a0 = (double)lds_f(src), a1 = (double)lds_f(src + 32u);
-          dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
-          dmma_8x8x4(cs[1][0], cs[1][1], a0, a1);
-          dmma_8x8x4(cs[2][0], cs[2][1], a1, a1);
-        } else {
-          const double a0 = (double)lds_f(src);
-          dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
+        for (int j = i; j < L::NS; ++j, ++idx) {
+          const float pr = __fmul_rn(v[i], v[j]);
+          e[idx] = __fadd_rn(e[idx], fmaf(v[i], v[j], -pr));
         }
-      }
-      __syncwarp();
     }
+    pw.advance();
+    // stage the warp's 32 pixel vectors, then groups of 4 pixels through the FP64 mma
+    const unsigned vrow = vbase + (unsigned)(lane * L::VS) * 4u;
+#pragma unroll
+    for (int i = 0; i < L::VW; i += 4) sts_v4(vrow + 4u * i, v[i], v[i + 1], v[i + 2], v[i + 3]);
+    __syncwarp();
+    const int kk = lane & 3, ii = lane >> 2;
+#pragma unroll
+    for (int g = 0; g < 8; ++g) {
+      const unsigned src = vbase + (unsigned)((4 * g + kk) * L::VS + ii) * 4u;
+      double(&cs)[3][2] = c[g % NSET];
+      if (SHAPE == DICEGPU_QUADRATIC_SF) {
+        const double a0 = (double)lds_f(src), a1 = (double)lds_f(src + 32u);
+        dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
+        dmma_8x8x4(cs[1][0], cs[1][1], a0, a1);
+        dmma_8x8x4(cs[2][0], cs[2][1], a1, a1);
+      } else {
+        const double a0 = (double)lds_f(src);
+        dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
+      }
+    }
+    __syncwarp();
   }
 #pragma unroll
   for (int s2 = 1; s2 < NSET; ++s2)
@@ -312,41 +546,61 @@ __device__ __noinline__ PassOut subset_pass(const PassInT<MASKED> in, const MapC
       c[0][b][0] += c[s2][b][0];
       c[0][b][1] += c[s2][b][1];
     }
-  o.n = warp_sum_i(n);
-  o.sumF = MOMENTS ? warp_sum(sFd) : warp_sum((double)sumF);
-  o.sumFall = ACC_H ? warp_sum((double)sumFall) : 0.0;
-  if (MOMENTS) {
-    o.sG = warp_sum(sG); o.sG2 = warp_sum(sG2); o.sF2 = warp_sum(sF2); o.sGF = warp_sum(sGF);
+  // the accumulator fragments into the warp's dense symmetric matrix
+  WarpOut<SHAPE>& wo = wouts<SHAPE>()[warp];
+  const int r = lane >> 2, cc = 2 * (lane & 3);
+  constexpr int VW = L::VW;
+  double* C = wo.M;
+  const double(&cf)[3][2] = c[0];
+  if (SHAPE == DICEGPU_QUADRATIC_SF) {
+    C[r * VW + cc] = cf[0][0];           C[r * VW + cc + 1] = cf[0][1];
+    C[r * VW + 8 + cc] = cf[1][0];       C[r * VW + 8 + cc + 1] = cf[1][1];
+    C[(8 + cc) * VW + r] = cf[1][0];     C[(8 + cc + 1) * VW + r] = cf[1][1];
+    C[(8 + r) * VW + 8 + cc] = cf[2][0]; C[(8 + r) * VW + 8 + cc + 1] = cf[2][1];
   } else {
-    o.sG = o.sG2 = o.sF2 = o.sGF = 0.0;
+    C[r * VW + cc] = cf[0][0];
+    C[r * VW + cc + 1] = cf[0][1];
   }
-  if (GRADS) {
-    o.sgx2 = warp_sum((double)sgx2); o.sgy2 = warp_sum((double)sgy2);
-    o.minx = warp_min_i(minx); o.maxx = warp_max_i(maxx);
-    o.miny = warp_min_i(miny); o.maxy = warp_max_i(maxy);
-  } else {
-    o.sgx2 = o.sgy2 = 0.0;
-    o.minx = o.maxx = in.cx; o.miny = o.maxy = in.cy;
+#pragma unroll
+  for (int i = 0; i < L::NP; ++i) {
+    const double sm = warp_sum((double)e[i]);
+    if (lane == 0) wo.E[i] = sm;
   }
-  if (ACC_H) {
-    // scatter the accumulator fragments into the warp's dense symmetric matrix
-    double* C = warp_smem<SHAPE>()->M;
-    __syncwarp();
-    const int r = lane >> 2, cc = 2 * (lane & 3);
-    constexpr int VW = L::VW;
-    const double(&cf)[3][2] = c[0];
-    if (SHAPE == DICEGPU_QUADRATIC_SF) {
-      C[r * VW + cc] = cf[0][0];           C[r * VW + cc + 1] = cf[0][1];
-      C[r * VW + 8 + cc] = cf[1][0];       C[r * VW + 8 + cc + 1] = cf[1][1];
-      C[(8 + cc) * VW + r] = cf[1][0];     C[(8 + cc + 1) * VW + r] = cf[1][1];
-      C[(8 + r) * VW + 8 + cc] = cf[2][0]; C[(8 + r) * VW + 8 + cc + 1] = cf[2][1];
-    } else {
-      C[r * VW + cc] = cf[0][0];
-      C[r * VW + cc + 1] = cf[0][1];
+}
+
+// The right-hand side sweep: q_i = sum over live pixels of fl(GmF * r_i) in
+// double, GmF = (G - meanG) - (F - meanF) in float (DICe_Objective.cpp:
+// 528-537), by all threads.  Per-warp sums go to WarpOut.q; ends with a
+// barrier.
+template <int SHAPE, bool DEFGRAD>
+__device__ __noinline__ void q_sweep(const PassIn in, const MapConst k, float meanG, float meanF) {
+  using L = Layout<SHAPE>;
+  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31;
+  const bool use_ref_grads = !DEFGRAD;
+  const PixArrays A = pix_arrays_at(in.pix, in.cap);
+  double q[L::NS];
+#pragma unroll
+  for (int i = 0; i < L::NS; ++i) q[i] = 0.0;
+  PixelWalk pw(in, tid, T);
+  for (int p = tid; p < in.npix; p += T) {
+    if (A.L[p] & 1) {
+      int x, y;
+      pw.xy(in, p, x, y);
+      const float GmF = __fsub_rn(__fsub_rn(A.G[p], meanG), __fsub_rn(A.F[p], meanF));
+      float r[L::VW];
+      stored_residuals<SHAPE>(in, A, k, p, x, y, use_ref_grads, r);
+#pragma unroll
+      for (int i = 0; i < L::NS; ++i) q[i] = __dadd_rn(q[i], (double)__fmul_rn(GmF, r[i]));
     }
-    __syncwarp();
+    pw.advance();
   }
-  return o;
+  WarpOut<SHAPE>& wo = wouts<SHAPE>()[tid >> 5];
+#pragma unroll
+  for (int i = 0; i < L::NS; ++i) {
+    const double sm = warp_sum(q[i]);
+    if (lane == 0) wo.q[i] = sm;
+  }
+  __syncthreads();
 }
 
 }  // namespace dg

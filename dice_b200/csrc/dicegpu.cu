@@ -168,21 +168,41 @@ __global__ void pack_kernel(size_t n, const float* __restrict__ I, const float* 
 }
 
 // ---------------------------------------------------------------------------
-// interpolation at arbitrary points (Image_ interface; border semantics of
-// the reference: bilinear outside its range is 0; Keys / bicubic compute the
-// bilinear value near the border and then overwrite it with the kernel sum
-// read through the row-major linear index, which we reproduce where that
-// index lies inside the image and replace by the bilinear value elsewhere)
+// interpolation at arbitrary points (the Image_ interface), in the
+// reference's arithmetic and border semantics: bilinear outside its range is
+// 0; Keys-4 and bicubic compute the bilinear value near the border and then
+// overwrite it with the kernel sum (DICe_Image.cpp:851-857, :496-502), whose
+// taps are read through the row-major linear index.  Where that index leaves
+// the image the reference reads past its array; here such taps read 0.
 // ---------------------------------------------------------------------------
 __device__ float lin_at(const float* a, long idx, long lim) {
   return (idx >= 0 && idx < lim) ? a[idx] : 0.0f;
 }
 
+// Image_::interpolate_bilinear (DICe_Image.cpp:432-445) on one channel
 __device__ float bilinear_pt(const float* a, int w, int h, float lx, float ly) {
   if (lx < 0.0f || (double)lx >= w - 1.5 || ly < 0.0f || (double)ly >= h - 1.5) return 0.0f;
   const int x1 = (int)lx, x2 = x1 + 1, y1 = (int)ly, y2 = y1 + 1;
   return a[y1 * w + x1] * (x2 - lx) * (y2 - ly) + a[y1 * w + x2] * (lx - x1) * (y2 - ly) +
          a[y2 * w + x2] * (lx - x1) * (ly - y1) + a[y2 * w + x1] * (x2 - lx) * (ly - y1);
+}
+
+// one channel of the Keys-4 sum (cc = wy * wx in float, m outer, n inner)
+__device__ float keys_pt(const float* a, int w, long lim, int ix, int iy, const float wx[6], const float wy[6]) {
+  float v = 0.0f;
+  for (int m = 0; m < 6; ++m) {
+    const long r0 = (long)(iy - 2 + m) * w + ix - 2;
+    for (int k = 0; k < 6; ++k) v = v + (wy[m] * wx[k]) * lin_at(a, r0 + k, lim);
+  }
+  return v;
+}
+
+// one channel of the bicubic polynomial (the expanded order of dg::bicubic_eval)
+__device__ float bicubic_pt(const float* a, int w, long lim, int x0, int y0, float x, float y) {
+  float f[4][4];
+  for (int n = 0; n < 4; ++n)
+    for (int m = 0; m < 4; ++m) f[n][m] = lin_at(a, (long)(y0 - 1 + m) * w + x0 - 1 + n, lim);
+  return bicubic_eval(f, x, y);
 }
 
 __global__ void interp_kernel(int method, int w, int h, const float* __restrict__ I,
@@ -198,36 +218,18 @@ __global__ void interp_kernel(int method, int w, int h, const float* __restrict_
   if (method == DICEGPU_BILINEAR) {
     v = bilinear_pt(I, w, h, lx, ly);
     if (grad) { a = bilinear_pt(gxi, w, h, lx, ly); b = bilinear_pt(gyi, w, h, lx, ly); }
-  } else {
-    const int R = method == DICEGPU_KEYS_FOURTH ? 6 : 4;
-    const int off = method == DICEGPU_KEYS_FOURTH ? 2 : 1;
+  } else if (method == DICEGPU_KEYS_FOURTH) {
     const int ix = (int)lx, iy = (int)ly;
     float wx[6], wy[6];
-    if (R == 6) { keys_weights(lx - ix, wx); keys_weights(ly - iy, wy); }
-    else { cubic_weights(lx - ix, wx); cubic_weights(ly - iy, wy); }
-    bool inside = true;
-    for (int m = 0; m < R; ++m) {
-      const long r0 = (long)(iy - off + m) * w + ix - off;
-      if (r0 < 0 || r0 + R - 1 >= lim) inside = false;
-    }
-    if (!inside) {
-      v = bilinear_pt(I, w, h, lx, ly);
-      if (grad) { a = bilinear_pt(gxi, w, h, lx, ly); b = bilinear_pt(gyi, w, h, lx, ly); }
-    } else {
-      for (int m = 0; m < R; ++m) {
-        float ra = 0.0f, rb = 0.0f, rc = 0.0f;
-        const long r0 = (long)(iy - off + m) * w + ix - off;
-        for (int k = 0; k < R; ++k) {
-          ra = fmaf(wx[k], lin_at(I, r0 + k, lim), ra);
-          if (grad) {
-            rb = fmaf(wx[k], lin_at(gxi, r0 + k, lim), rb);
-            rc = fmaf(wx[k], lin_at(gyi, r0 + k, lim), rc);
-          }
-        }
-        v = fmaf(wy[m], ra, v);
-        if (grad) { a = fmaf(wy[m], rb, a); b = fmaf(wy[m], rc, b); }
-      }
-    }
+    keys_weights_ref_general(lx - (float)ix, wx);
+    keys_weights_ref_general(ly - (float)iy, wy);
+    v = keys_pt(I, w, lim, ix, iy, wx, wy);
+    if (grad) { a = keys_pt(gxi, w, lim, ix, iy, wx, wy); b = keys_pt(gyi, w, lim, ix, iy, wx, wy); }
+  } else {
+    const int x0 = (int)lx, y0 = (int)ly;
+    const float x = lx - (float)x0, y = ly - (float)y0;
+    v = bicubic_pt(I, w, lim, x0, y0, x, y);
+    if (grad) { a = bicubic_pt(gxi, w, lim, x0, y0, x, y); b = bicubic_pt(gyi, w, lim, x0, y0, x, y); }
   }
   oi[t] = v;
   if (grad) { ogx[t] = a; ogy[t] = b; }
@@ -256,6 +258,11 @@ struct dicegpu_ctx {
   DevParams dp;
   int device = 0;
   int num_sms = 0;
+  int smem_optin = 0;   // largest dynamic shared memory a CTA may opt in to
+  // per-pixel arrays of subsets too large for shared memory: one slice per CTA
+  bool pix_in_global = false;
+  size_t pix_stride = 0;
+  DevBuf<unsigned char> d_pix_scratch;
   cudaStream_t stream = nullptr;
   int W = 0, H = 0;
   float* d_ref = nullptr;
@@ -276,6 +283,7 @@ struct dicegpu_ctx {
   int32_t* d_py = nullptr;
   size_t list_cap = 0, offs_cap = 0;
   bool use_lists = false;
+  int list_npix_max = 0;    // largest pixel list (use_lists)
   uint8_t* d_force = nullptr;
   size_t force_cap = 0;
   bool use_force = false;
@@ -287,7 +295,7 @@ struct dicegpu_ctx {
   size_t unc_cap = 0;
   int unc_n = 0;             // subset count the buffer was zeroed for (0: invalid)
   int frame_index = 0;
-  int warps_per_cta = 8;   // measured best on the 2048^2 sequence (2 CTAs/SM at 128 registers)
+  int warps_per_cta = 4;   // warps of the CTA that solves one subset
   int ctas_per_sm = 0;   // 0: occupancy-derived
   int queue_mode = 1;    // 1: per-CTA queues with stealing, 0: one global queue
   int carveout = -1;     // preferred shared-memory carveout (percent), -1: driver default
@@ -499,6 +507,7 @@ extern "C" int dicegpu_create(const dicegpu_params* params, dicegpu_ctx** out) {
   if (rc) { delete c; return rc; }
   if (cudaGetDevice(&c->device) != cudaSuccess ||
       cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) != cudaSuccess ||
       cudaMalloc(&c->d_counter, kMaxQueues * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess ||
       cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
@@ -524,6 +533,7 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   c->d_conformal.release(); c->d_mask_desc.release(); c->d_mask_bits.release();
   c->d_pix_flag.release(); c->d_pix_flag0.release(); c->d_pix_f.release();
   c->d_evo_nact.release(); c->d_evo_nact0.release(); c->d_acc.release(); c->d_ref_saved.release();
+  c->d_pix_scratch.release();
   c->d_blk_off.release(); c->d_blk_ids.release(); c->d_neigh.release();
   for (auto& pl : c->plans) { pl.d_wave.release(); pl.d_bwave.release(); }
   c->d_dp_off.release(); c->d_bpoly.release();
@@ -847,6 +857,8 @@ extern "C" int dicegpu_set_subset_pixels(dicegpu_ctx* c, int n, const int32_t* o
     CK(cudaMemcpy(c->d_py, py, total * sizeof(int32_t), cudaMemcpyHostToDevice));
   }
   c->use_lists = true;
+  c->list_npix_max = 0;
+  for (int i = 0; i < n; ++i) c->list_npix_max = std::max(c->list_npix_max, offsets[i + 1] - offsets[i]);
   c->has_evo = false;   // explicit lists carry no evolution state
   return DICEGPU_OK;
 }
@@ -1095,6 +1107,8 @@ extern "C" int dicegpu_set_subset_shapes(dicegpu_ctx* c, int n_shapes, const dic
   c->h_mask_desc.swap(desc);
   CK(cudaStreamSynchronize(c->stream));
   c->use_lists = true;
+  c->list_npix_max = 0;
+  for (int i = 0; i < n; ++i) c->list_npix_max = std::max(c->list_npix_max, counts[i]);
   return upload_force(c);
 }
 
@@ -1375,9 +1389,25 @@ extern "C" int dicegpu_fields_device_ptr(dicegpu_ctx* c, double** dptr) {
   return DICEGPU_OK;
 }
 
-static size_t warp_smem_bytes(int shape) {
-  return shape == DICEGPU_QUADRATIC_SF ? sizeof(WarpSmem<DICEGPU_QUADRATIC_SF>)
-                                       : sizeof(WarpSmem<DICEGPU_AFFINE_SF>);
+// the largest pixel count of a subset of the context (squares: side^2)
+static int npix_max(const dicegpu_ctx* c) {
+  if (c->use_lists) return std::max(c->list_npix_max, 1);
+  const int side = 2 * (c->params.subset_size / 2) + 1;
+  return side * side;
+}
+
+// dynamic shared memory of a frame CTA of `warps` warps: the control block,
+// per-warp sums, simplex state and staging (`fixed`), and the per-pixel
+// arrays (`pix`)
+static void frame_smem_bytes(const dicegpu_ctx* c, int warps, size_t* fixed, size_t* pix) {
+  const int cap = pix_cap(npix_max(c));
+  if (c->dp.shape == DICEGPU_QUADRATIC_SF) {
+    *fixed = SmemPlan<DICEGPU_QUADRATIC_SF>::pix(warps);
+    *pix = SmemPlan<DICEGPU_QUADRATIC_SF>::pix_bytes(cap);
+  } else {
+    *fixed = SmemPlan<DICEGPU_AFFINE_SF>::pix(warps);
+    *pix = SmemPlan<DICEGPU_AFFINE_SF>::pix_bytes(cap);
+  }
 }
 
 static FrameKernelFn frame_fn(const dicegpu_ctx* c) {
@@ -1414,12 +1444,15 @@ static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
              c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE && c->frame_index >= 2;
   a.fields = c->d_fields;
   a.n = c->n;
+  a.npix_cap = pix_cap(npix_max(c));
+  a.pix_scratch = c->pix_in_global ? c->d_pix_scratch.p : nullptr;
+  a.pix_stride = c->pix_stride;
   a.first_frame = c->frame_index == 0;
   a.mode = mode;
   a.plain_index = -1;
   a.work_counter = c->d_counter;
   a.queue_mode = c->queue_mode;
-  a.chunk = c->chunk > 0 ? c->chunk : 2 * c->warps_per_cta;
+  a.chunk = c->chunk > 0 ? c->chunk : 4;
   a.status = c->d_status;
   a.passes_out = c->d_passes;
   a.unc = (c->params.compute_uncertainty && c->unc_n == c->n) ? c->d_unc : nullptr;
@@ -1428,7 +1461,13 @@ static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
 static int grid_for(dicegpu_ctx* c, FrameKernelFn fn, int* blocks, size_t* smem) {
   if (!fn) return DICEGPU_ERR_UNSUPPORTED;
   const int threads = c->warps_per_cta * 32;
-  *smem = warp_smem_bytes(c->dp.shape) * c->warps_per_cta;
+  size_t fixed, pix;
+  frame_smem_bytes(c, c->warps_per_cta, &fixed, &pix);
+  // a subset's pixel arrays live in the CTA's shared memory, or, for subsets
+  // too large for it, in a slice of a global scratch buffer per CTA
+  c->pix_in_global = fixed + pix > (size_t)c->smem_optin;
+  *smem = c->pix_in_global ? fixed : fixed + pix;
+  c->pix_stride = pix;
   CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
   if (c->carveout >= 0)
     CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributePreferredSharedMemoryCarveout, c->carveout));
@@ -1438,6 +1477,10 @@ static int grid_for(dicegpu_ctx* c, FrameKernelFn fn, int* blocks, size_t* smem)
     if (per_sm < 1) per_sm = 1;
   }
   *blocks = std::min(per_sm * c->num_sms, kMaxQueues);
+  if (c->pix_in_global) {
+    int rc = c->d_pix_scratch.ensure((size_t)*blocks * pix);
+    if (rc) return rc;
+  }
   return DICEGPU_OK;
 }
 
@@ -1596,7 +1639,6 @@ static int run_waves(dicegpu_ctx* c, int kind, FrameKernelFn fn, int blocks, siz
     ba.skin = (float)c->params.obstruction_skin_factor;
   }
   const int nlev = (int)pl.wave_off.size() - 1;
-  const size_t smem1 = warp_smem_bytes(c->dp.shape);
   for (int L = 0; L < nlev;) {
     const int nb = pl.bwave_off[L + 1] - pl.bwave_off[L];
     const int nw = pl.wave_off[L + 1] - pl.wave_off[L];
@@ -1607,7 +1649,8 @@ static int run_waves(dicegpu_ctx* c, int kind, FrameKernelFn fn, int blocks, siz
       a.nsnap = c->d_snapshot.p;
     }
     if (nw == 1 && nb == 0) {
-      // a chain: consecutive single-subset waves without blocked polygons
+      // a chain: consecutive single-subset waves without blocked polygons,
+      // taken in order by one CTA (all its warps on each subset)
       int L1 = L + 1;
       while (L1 < nlev && pl.wave_off[L1 + 1] - pl.wave_off[L1] == 1 && pl.bwave_off[L1 + 1] == pl.bwave_off[L1])
         ++L1;
@@ -1615,7 +1658,7 @@ static int run_waves(dicegpu_ctx* c, int kind, FrameKernelFn fn, int blocks, siz
       a.n_order = pl.wave_off[L1] - pl.wave_off[L];
       a.queue_mode = 0;
       CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
-      fn<<<1, 32, smem1, c->stream>>>(a);
+      fn<<<1, c->warps_per_cta * 32, smem, c->stream>>>(a);
       CK(cudaGetLastError());
       c->launches += 1;
       L = L1;
@@ -1671,9 +1714,10 @@ extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
   if (c->has_blocking && c->params.correlation_routine == DICEGPU_TRACKING_ROUTINE)
     return DICEGPU_ERR_UNSUPPORTED;
   FrameKernelFn fn = frame_fn(c);
-  if (!fn) return DICEGPU_ERR_UNSUPPORTED;
+  int blocks;
+  size_t smem;
+  if ((rc = grid_for(c, fn, &blocks, &smem))) return rc;
   if ((rc = frame_begin(c))) return rc;
-  const size_t smem = warp_smem_bytes(c->dp.shape);
   FrameArgs a;
   fill_args(c, a, MODE_CORRELATE);
   if (frame_plan_kind(c) & 2) {
@@ -1683,7 +1727,7 @@ extern "C" int dicegpu_execute_correlation_plain(dicegpu_ctx* c) {
   }
   for (int i = 0; i < c->n; ++i) {
     a.plain_index = i;
-    fn<<<1, 32, smem, c->stream>>>(a);
+    fn<<<1, c->warps_per_cta * 32, smem, c->stream>>>(a);
   }
   CK(cudaGetLastError());
   c->launches += c->n;
@@ -1839,7 +1883,7 @@ extern "C" int dicegpu_autotune(dicegpu_ctx* c, int* warps_per_cta, int* ctas_pe
     rc = DICEGPU_ERR_CUDA;
   const int frame0 = c->frame_index;
   c->evo_suspend = true;
-  const int cand[][2] = {{8, 0}, {4, 0}, {2, 0}, {8, 1}, {4, 2}, {4, 3}};
+  const int cand[][2] = {{4, 0}, {2, 0}, {8, 0}, {1, 0}, {4, 3}, {2, 6}};
   TuneVal best{c->warps_per_cta, c->ctas_per_sm, 1e30f};
   for (const auto& cd : cand) {
     if (rc) break;

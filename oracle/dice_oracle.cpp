@@ -63,16 +63,18 @@ struct Image {
 
 // Keys fourth-order cubic convolution kernel pieces (DICe_Image.cpp:114-122).
 // The published Keys (1981) 6-point kernel: for s in [0,1): 4/3 s^3 - 7/3 s^2 + 1;
-// [1,2): -7/12 s^3 + 3 s^2 - 59/12 s + 5/2; [2,3): 1/12 s^3 - 2/3 s^2 + 7/4 s - 3/2.
-// Evaluated in double and rounded to float, as the reference's double literals do.
+// [1,2): -7/12 s^3 + 3 s^2 - 59/12 s + 5/2; [2,3): 1/12 s^3 - 2/3 s^2 + 7/4 s - 3/2,
+// with the coefficients written as the 14-decimal literals the reference uses,
+// evaluated in double left to right and rounded to float, as its double
+// literals make it.
 static inline float keys_f0(float s) {
-  return (float)((4.0 / 3.0) * s * s * s - (7.0 / 3.0) * s * s + 1.0);
+  return (float)(1.33333333333333 * s * s * s - 2.33333333333333 * s * s + 1.0);
 }
 static inline float keys_f1(float s) {
-  return (float)(-(7.0 / 12.0) * s * s * s + 3.0 * s * s - (59.0 / 12.0) * s + 2.5);
+  return (float)(-0.58333333333333 * s * s * s + 3.0 * s * s - 4.91666666666666 * s + 2.5);
 }
 static inline float keys_f2(float s) {
-  return (float)((1.0 / 12.0) * s * s * s - (2.0 / 3.0) * s * s + 1.75 * s - 1.5);
+  return (float)(0.08333333333333 * s * s * s - 0.66666666666666 * s * s + 1.75 * s - 1.5);
 }
 
 // Image_::interpolate_bilinear (DICe_Image.cpp:432-445) on one channel.
@@ -94,42 +96,64 @@ static void interp_bilinear_all(const Image& im, float& iv, float& gxv, float& g
   }
 }
 
-// Catmull-Rom (a = -1/2) cubic convolution weights: the separable form of the
-// 16-tap polynomial written out in Image_::interpolate_bicubic_all
-// (DICe_Image.cpp:493-636); same kernel, summed row by row.
-static inline void catmull_rom_weights(float t, float wgt[4]) {
-  const float t2 = t * t, t3 = t2 * t;
-  wgt[0] = 0.5f * (-t3 + 2.0f * t2 - t);
-  wgt[1] = 0.5f * (3.0f * t3 - 5.0f * t2 + 2.0f);
-  wgt[2] = 0.5f * (-3.0f * t3 + 4.0f * t2 + t);
-  wgt[3] = 0.5f * (t3 - t2);
+// Image_::interpolate_bicubic_all (DICe_Image.cpp:493-636).  The reference
+// writes the Catmull-Rom (a = -1/2) bicubic as its polynomial expanded in x
+// and y: the coefficient of x^a y^b is sum_{n,m} c_a[n] c_b[m] f(n, m) over
+// the 4 x 4 taps (offsets -1..2), with the kernel's power-coefficient vectors
+//   c_0 = (0, 1, 0, 0), c_1 = (-1/2, 0, 1/2, 0),
+//   c_2 = (1, -5/2, 2, -1/2), c_3 = (-1/2, 3/2, -3/2, 1/2).
+// Each coefficient sums its nonzero terms with the x tap outer and the y
+// tap inner, and the value is
+//   f00 + C01 y + C02 y^2 + C03 y^3 + sum_{a=1..3} (Ca0 + Ca1 y + Ca2 y^2 + Ca3 y^3) x^a,
+// every product and sum in float, left to right: the reference's expression
+// order.  The coefficients' products are exact in float.
+static const float kCR[4][4] = {{0.0f, 1.0f, 0.0f, 0.0f},
+                                {-0.5f, 0.0f, 0.5f, 0.0f},
+                                {1.0f, -2.5f, 2.0f, -0.5f},
+                                {-0.5f, 1.5f, -1.5f, 0.5f}};
+static float bicubic_group(const float f[4][4], int a, int b) {
+  float s = 0.0f;
+  bool first = true;
+  for (int n = 0; n < 4; ++n)
+    for (int m = 0; m < 4; ++m) {
+      const float cf = kCR[a][n] * kCR[b][m];
+      if (cf == 0.0f) continue;
+      const float t = cf * f[n][m];
+      s = first ? t : s + t;
+      first = false;
+    }
+  return s;
 }
-
-static float bicubic_channel(const Image& im, const float* a, int x0, int y0, const float wx[4],
-                             const float wy[4]) {
-  float v = 0.0f;
-  for (int m = 0; m < 4; ++m) {
-    float row = 0.0f;
-    const long base = (long)(y0 - 1 + m) * im.w + (x0 - 1);
-    for (int n = 0; n < 4; ++n) row += wx[n] * im.at(a, base + n);
-    v += wy[m] * row;
+static float bicubic_channel(const Image& im, const float* a, int x0, int y0, float x, float y) {
+  float f[4][4];   // f[n][m]: tap at x offset n - 1, y offset m - 1
+  for (int n = 0; n < 4; ++n)
+    for (int m = 0; m < 4; ++m) f[n][m] = im.at(a, (long)(y0 - 1 + m) * im.w + (x0 - 1 + n));
+  const float x2 = x * x, x3 = x2 * x, y2 = y * y, y3 = y2 * y;
+  float v = f[1][1];
+  v = v + bicubic_group(f, 0, 1) * y;
+  v = v + bicubic_group(f, 0, 2) * y2;
+  v = v + bicubic_group(f, 0, 3) * y3;
+  const float xp[4] = {1.0f, x, x2, x3};
+  for (int a = 1; a < 4; ++a) {
+    float g = bicubic_group(f, a, 0);
+    g = g + bicubic_group(f, a, 1) * y;
+    g = g + bicubic_group(f, a, 2) * y2;
+    g = g + bicubic_group(f, a, 3) * y3;
+    v = v + g * xp[a];
   }
   return v;
 }
 
-// Image_::interpolate_bicubic_all (DICe_Image.cpp:493-636).  The reference
-// computes a bilinear fallback near the border and then falls through to the
-// bicubic expression, which overwrites it; we do the same.
+// The reference computes a bilinear fallback near the border and then falls
+// through to the bicubic expression, which overwrites it; we do the same.
 static void interp_bicubic_all(const Image& im, float& iv, float& gxv, float& gyv, bool grad,
                                float lx, float ly) {
   const int x0 = (int)lx, y0 = (int)ly;
-  float wx[4], wy[4];
-  catmull_rom_weights(lx - x0, wx);
-  catmull_rom_weights(ly - y0, wy);
-  iv = bicubic_channel(im, im.I, x0, y0, wx, wy);
+  const float x = lx - x0, y = ly - y0;
+  iv = bicubic_channel(im, im.I, x0, y0, x, y);
   if (grad) {
-    gxv = bicubic_channel(im, im.gx, x0, y0, wx, wy);
-    gyv = bicubic_channel(im, im.gy, x0, y0, wx, wy);
+    gxv = bicubic_channel(im, im.gx, x0, y0, x, y);
+    gyv = bicubic_channel(im, im.gy, x0, y0, x, y);
   }
 }
 
@@ -260,6 +284,17 @@ static bool gauss_filter(int w, int h, int M, const float* in, float* out) {
   return true;
 }
 
+// Float cosine, sine and arc cosine of the shape functions, taken correctly
+// rounded: the double function rounded to float.  The reference calls the
+// C library's float versions (std::cos(float) and so on; its affine map's
+// unqualified cos(theta) may resolve to the double one), which are not
+// correctly rounded for every argument and differ between library versions,
+// so the reference's own rotated results depend on the libm it links; the
+// correctly rounded value is the same on every platform and on the GPU.
+static inline float cos_f(float t) { return (float)std::cos((double)t); }
+static inline float sin_f(float t) { return (float)std::sin((double)t); }
+static inline float acos_f(float t) { return (float)std::acos((double)t); }
+
 // ---------------------------------------------------------------------------
 // Local shape functions (DICe_LocalShapeFunction.cpp)
 // ---------------------------------------------------------------------------
@@ -306,7 +341,7 @@ struct ShapeFn {
     const float dudx = iex >= 0 ? p[iex] : 0.0f;
     const float dvdy = iey >= 0 ? p[iey] : 0.0f;
     const float gxy = ig >= 0 ? p[ig] : 0.0f;
-    const float cost = std::cos(theta), sint = std::sin(theta);
+    const float cost = cos_f(theta), sint = sin_f(theta);
     const float Dx = (float)((1.0 + dudx) * dx + gxy * dy);
     const float Dy = (float)((1.0 + dvdy) * dy + gxy * dx);
     ox = cost * Dx - sint * Dy + p[iu] + cx;
@@ -325,7 +360,7 @@ struct ShapeFn {
       const float mag_a = std::sqrt(ax * ax + ay * ay);
       const float bx = 5.0f, by = 0.0f, mag_b = 5.0f;
       const float adb = (ax * bx + ay * by) / (mag_a * mag_b);
-      t = ay < 0.0f ? (float)(kTwoPi - std::acos(adb)) : std::acos(adb);
+      t = ay < 0.0f ? (float)(kTwoPi - (double)acos_f(adb)) : acos_f(adb);
       return;
     }
     u = p[iu];
@@ -342,7 +377,7 @@ struct ShapeFn {
       if (use_ref_grads) {
         float u, v, th;
         map_to_u_v_theta(cx, cy, u, v, th);
-        const float c = std::cos(th), s = std::sin(th);
+        const float c = cos_f(th), s = sin_f(th);
         Gx = c * gx - s * gy;
         Gy = s * gx + c * gy;
       }
@@ -356,7 +391,7 @@ struct ShapeFn {
     const float dudx = iex >= 0 ? p[iex] : 0.0f;
     const float dvdy = iey >= 0 ? p[iey] : 0.0f;
     const float gxy = ig >= 0 ? p[ig] : 0.0f;
-    const float c = std::cos(theta), s = std::sin(theta);
+    const float c = cos_f(theta), s = sin_f(theta);
     const float dx = x - cx, dy = y - cy;
     const float Dx = (float)((1.0 + dudx) * dx + gxy * dy);
     const float Dy = (float)((1.0 + dvdy) * dy + gxy * dx);
@@ -711,7 +746,8 @@ static float objective_gamma(const Ctx& C, Subset& s, const ShapeFn& sf, Counter
   if (C.P.normalize_gamma_with_active_pixels) {
     int na = 0;
     for (int i = 0; i < s.npix; ++i) if (s.active[i]) ++na;
-    if (na > 0) g /= na;
+    // gamma /= (num_active==0.0 ? 1.0 : num_active): a double divisor (:70-71)
+    if (na > 0) g = (float)(g / (double)na);
   }
   return g;
 }
@@ -1055,8 +1091,8 @@ static float objective_beta(const Ctx& C, Subset& s, const ShapeFn& sf_in) {
     auto insert = [&](ShapeFn& sfn) {
       if (sfn.type == DICEGPU_QUADRATIC_SF) {
         for (int k = 0; k < 12; ++k) sfn.p[k] = 0.0f;
-        sfn.p[0] = std::cos(th); sfn.p[1] = -std::sin(th);
-        sfn.p[6] = std::sin(th); sfn.p[7] = std::cos(th);
+        sfn.p[0] = cos_f(th); sfn.p[1] = -sin_f(th);
+        sfn.p[6] = sin_f(th); sfn.p[7] = cos_f(th);
         sfn.p[5] = u; sfn.p[11] = v;
       } else {
         sfn.p[sfn.iu] = u; sfn.p[sfn.iv] = v;

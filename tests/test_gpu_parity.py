@@ -1,10 +1,15 @@
 """GPU parity: libdicegpu.so (through its C ABI) against the CPU oracle.
 
-Bars (stated per test): bit-exact for the gradient images and the integer /
-flag outputs (status, active pixels); displacement within 1e-4 px and
-strain-like parameters within 1e-6 of the oracle on the same seeded inputs;
-iteration counts equal except where the oracle's own last update sits
-within rounding of the convergence tolerance.
+The bar is equality: the library computes the reference's float operations
+in the reference's order (interpolation weights in double, 2-D tap sums,
+sequential float means and gamma / sigma / noise sums, float-rounded products
+in the double Hessian and right-hand side, LU factors and explicit inverse,
+the update accumulated in float), so every result column -- status,
+iterations, parameters, sigma, gamma, noise, contrast, active pixels,
+condition number -- equals the oracle's bit for bit.  The double sums run in
+another order than the reference's sequential one; that moves them by about
+1e-16 relative, which decides a float rounding of the parameter update only
+with a probability of order 1e-9 per update, so none occurs in these cases.
 """
 import numpy as np
 import pytest
@@ -14,12 +19,9 @@ from dice_b200 import abi
 from dice_b200.schema import Schema, correlate
 from dice_b200 import synthetic as syn
 from oracle import oracle as O
+from tests._exact import assert_rows_equal
 
 pytestmark = pytest.mark.gpu
-
-DISP_TOL = 1e-4     # px
-STRAIN_TOL = 1e-6
-
 
 def _require_gpu():
     if not torch.cuda.is_available():
@@ -60,30 +62,8 @@ def _run_oracle(params, ref, deff, fields, frames=None, lists=None, force=None):
     return out
 
 
-def _compare(g, o, disp_tol=DISP_TOL, strain_tol=STRAIN_TOL, its_mismatch_frac=0.03, quad=False):
-    st_g, st_o = g[:, abi.F_STATUS], o[:, abi.F_STATUS]
-    assert np.array_equal(st_g, st_o), "status flags differ at %s" % np.where(st_g != st_o)[0][:10]
-    ok = st_o < 2
-    du = np.abs(g[ok, abi.F_DISP_X] - o[ok, abi.F_DISP_X])
-    dv = np.abs(g[ok, abi.F_DISP_Y] - o[ok, abi.F_DISP_Y])
-    assert du.max(initial=0) <= disp_tol, du.max()
-    assert dv.max(initial=0) <= disp_tol, dv.max()
-    same = ok & (g[:, abi.F_ITERATIONS] == o[:, abi.F_ITERATIONS])
-    if not quad:
-        # Strain-like parameters: 1e-6 where both stopped at the same
-        # iteration.  The reference's affine convergence test reads only u, v
-        # and theta (DICe_LocalShapeFunction.cpp:433-459), so where the two
-        # stop one iteration apart the strains still differ by that last,
-        # untested update (bounded here by 10x the bar).
-        for col in (abi.F_STRETCH_XX, abi.F_STRETCH_YY, abi.F_SHEAR_XY, abi.F_ROT_Z):
-            d = np.abs(g[:, col] - o[:, col])
-            assert d[same].max(initial=0) <= 1.5 * strain_tol, (col, d[same].max())
-            assert d[ok].max(initial=0) <= 10 * strain_tol, (col, d[ok].max())
-    its = int(np.sum(g[ok, abi.F_ITERATIONS] != o[ok, abi.F_ITERATIONS]))
-    assert its <= max(2, its_mismatch_frac * ok.sum()), its
-    gam = np.abs(g[ok, abi.F_GAMMA] - o[ok, abi.F_GAMMA]) / np.maximum(o[ok, abi.F_GAMMA], 1e-6)
-    assert gam.max(initial=0) < 1e-2, gam.max()
-    assert np.array_equal(g[ok, abi.F_ACTIVE_PIXELS], o[ok, abi.F_ACTIVE_PIXELS])
+def _compare(g, o):
+    assert_rows_equal(g, o)
 
 
 def test_gradients_bit_exact():
@@ -111,16 +91,18 @@ def test_interpolate_matches_oracle(method):
     ref, deff = syn.config1(w=128, h=96)
     ref, deff = ref.numpy(), deff.numpy()
     rng = np.random.default_rng(3)
-    xy = np.stack([rng.uniform(3.6, 123.4, 5000), rng.uniform(3.6, 91.4, 5000)], 1).astype(np.float32)
+    # the whole image and a margin around it: border fallbacks and the
+    # kernel sums that overwrite them, taps outside the image read as 0
+    xy = np.stack([rng.uniform(-1.5, 127.4, 20000), rng.uniform(-1.5, 95.4, 20000)], 1).astype(np.float32)
     with Schema(abi.default_params()) as s:
         s.set_ref_image(ref)
         s.set_def_image(deff)
         gi, ggx, ggy = s.interpolate(method, xy)
     dgx, dgy = O.gradients(deff)
     oi, ogx, ogy = O.interpolate(method, deff, xy, dgx, dgy)
-    np.testing.assert_allclose(gi, oi, rtol=2e-6, atol=2e-4)
-    np.testing.assert_allclose(ggx, ogx, rtol=2e-5, atol=2e-4)
-    np.testing.assert_allclose(ggy, ogy, rtol=2e-5, atol=2e-4)
+    assert np.array_equal(gi, oi)
+    assert np.array_equal(ggx, ogx)
+    assert np.array_equal(ggy, ogy)
 
 
 def test_reference_gold_on_gpu(gold):
@@ -224,13 +206,8 @@ def test_simplex_parity():
     f = syn.init_fields(cx, cy)
     gpu = _run_gpu(p, ref.numpy(), deff.numpy(), f)[0]
     ora = _run_oracle(p, ref.numpy(), deff.numpy(), f)[0]
-    st = ora[:, abi.F_STATUS]
-    assert np.array_equal(gpu[:, abi.F_STATUS], st)
-    ok = st < 2
-    # Nelder-Mead branches on comparisons of nearly equal gammas; both land
-    # within the simplex's own convergence radius of the minimum
-    assert np.max(np.abs(gpu[ok, abi.F_DISP_X] - ora[ok, abi.F_DISP_X])) < 2e-3
-    assert np.max(np.abs(gpu[ok, abi.F_DISP_Y] - ora[ok, abi.F_DISP_Y])) < 2e-3
+    _compare(gpu, ora)
+    ok = ora[:, abi.F_STATUS] < 2
     assert np.abs(np.median(gpu[ok, abi.F_DISP_X]) - 0.37) < 0.02
 
 
@@ -242,7 +219,7 @@ def test_quadratic_parity():
     f = syn.init_fields(cx, cy, quadratic=True)
     gpu = _run_gpu(p, ref.numpy(), deff.numpy(), f)[0]
     ora = _run_oracle(p, ref.numpy(), deff.numpy(), f)[0]
-    _compare(gpu, ora, quad=True, its_mismatch_frac=0.05)
+    _compare(gpu, ora)
 
 
 def test_pixel_list_subsets_parity():
@@ -323,4 +300,27 @@ def test_gamma_entry_matches_oracle():
         s.set_fields(f)
         g = s.gamma(f)
     o = O.gamma(p, ref.numpy(), deff.numpy(), f)
-    np.testing.assert_allclose(g, o, rtol=2e-3, atol=1e-6)
+    assert np.array_equal(g, o)
+
+
+def test_headline_strip_x_ge_1024_exact():
+    """The 2048^2 sequence (31 x 31 affine subsets at step 5, tolerance 1e-5)
+    on the strip x in [1024, 2048), y in [900, 1156): there the float spacing
+    of mapped coordinates (1.2e-4 px) exceeds the tolerance, the last
+    Gauss-Newton updates oscillate at that spacing and rounding decides
+    iteration counts and simplex fallbacks.  Four frames, each from the
+    previous solution; every result column equal to the oracle's."""
+    _require_gpu()
+    ref, frames = syn.config2(device="cuda", nframes=10, count=4)
+    cx, cy = syn.grid_points(2048, 2048, 31, 5)
+    sel = np.nonzero((cx >= 1024) & (cy >= 900) & (cy < 1156))[0]
+    assert len(sel) > 10000
+    p = _config1_params(subset_size=31)
+    f = syn.init_fields(cx[sel], cy[sel])
+    ref_h = ref.cpu().numpy()
+    frames_h = [fr.cpu().numpy() for fr in frames]
+    gpu = _run_gpu(p, ref, None, f, frames=frames)
+    ora = _run_oracle(p, ref_h, None, f, frames=frames_h)
+    for g, o in zip(gpu, ora):
+        _compare(g, o)
+    assert (ora[-1][:, abi.F_STATUS] < 2).all()

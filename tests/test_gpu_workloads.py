@@ -17,6 +17,7 @@ from dice_b200 import abi
 from dice_b200 import synthetic as syn
 from dice_b200.schema import Schema
 from oracle import oracle as O
+from tests._exact import assert_rows_equal
 
 pytestmark = pytest.mark.gpu
 
@@ -101,15 +102,9 @@ def test_mixed_shapes_quadratic_and_simplex():
     lq = _select(c["lists"], ib)
     g = _gpu_frames(pq, ref, [deff], fq, lists=lq)[0]
     o = _oracle_frames(pq, ref, [deff], fq, lists=lq)[0]
-    assert np.array_equal(g[:, abi.F_STATUS], o[:, abi.F_STATUS])
+    assert_rows_equal(g, o)
     ok = o[:, abi.F_STATUS] < 2
     assert ok.mean() > 0.9
-    assert np.max(np.abs(g[ok, abi.F_DISP_X] - o[ok, abi.F_DISP_X])) < 1e-4
-    assert np.max(np.abs(g[ok, abi.F_DISP_Y] - o[ok, abi.F_DISP_Y])) < 1e-4
-    assert np.max(np.abs(g[ok, abi.F_QUAD_A:abi.F_QUAD_A + 12] - o[ok, abi.F_QUAD_A:abi.F_QUAD_A + 12])) < 1e-4
-    its = g[ok, abi.F_ITERATIONS] != o[ok, abi.F_ITERATIONS]
-    assert its.sum() <= max(2, int(0.05 * ok.sum()))
-    assert np.max(np.abs(g[ok, abi.F_ITERATIONS] - o[ok, abi.F_ITERATIONS])) <= 1
     # the recovered displacement matches the imposed field at the centres
     ue, ve = c["field"](torch.from_numpy(cx[ib]), torch.from_numpy(cy[ib]))
     assert np.median(np.abs(g[ok, abi.F_DISP_X] - ue.numpy()[ok])) < 0.02
@@ -124,10 +119,7 @@ def test_mixed_shapes_quadratic_and_simplex():
     force = np.ones(len(it), np.uint8)
     g = _gpu_frames(ps, ref, [deff], fs, lists=ls, force=force)[0]
     o = _oracle_frames(ps, ref, [deff], fs, lists=ls, force=force)[0]
-    assert np.array_equal(g[:, abi.F_STATUS], o[:, abi.F_STATUS])
-    ok = o[:, abi.F_STATUS] < 2
-    assert np.max(np.abs(g[ok, abi.F_DISP_X] - o[ok, abi.F_DISP_X]), initial=0) < 2e-3
-    assert np.max(np.abs(g[ok, abi.F_DISP_Y] - o[ok, abi.F_DISP_Y]), initial=0) < 2e-3
+    assert_rows_equal(g, o)
 
 
 def test_quadratic_fallback_records_final_parameters():
@@ -171,11 +163,7 @@ def test_crack_failure_flags_match_oracle():
     gs = _gpu_frames(p, ref, frames, f)
     os_ = _oracle_frames(p, ref, frames, f)
     for g, o in zip(gs, os_):
-        st_g, st_o = g[:, abi.F_STATUS], o[:, abi.F_STATUS]
-        assert np.array_equal(st_g, st_o), np.nonzero(st_g != st_o)[0][:10]
-        assert np.array_equal(g[:, abi.F_SIGMA] == -1.0, o[:, abi.F_SIGMA] == -1.0)
-        ok = st_o < 2
-        assert np.max(np.abs(g[ok, abi.F_DISP_Y] - o[ok, abi.F_DISP_Y])) < 1e-4
+        assert_rows_equal(g, o)
     # high gamma on the crack (flag 23) sets sigma = -1, so the next frame's
     # initializer fails there (flag 5)
     st1, st2 = os_[1][:, abi.F_STATUS], os_[2][:, abi.F_STATUS]

@@ -17,6 +17,7 @@ import pytest
 from dice_b200 import abi
 from dice_b200 import synthetic as syn
 from oracle import oracle as O
+from tests._exact import assert_rows_equal
 
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_gold.npz"))
 MASKS = (5, 7, 9, 11, 13)
@@ -103,11 +104,9 @@ def test_correlation_with_filtered_images_matches_oracle(m):
         g = s.fields()
     o = f.copy()
     O.execute_frame(p, ref, deff, o, first_frame=True, nthreads=4)
-    assert np.array_equal(g[:, abi.F_STATUS], o[:, abi.F_STATUS])
+    assert_rows_equal(g, o)
     ok = o[:, abi.F_STATUS] < 2
     assert ok.mean() > 0.9
-    assert np.max(np.abs(g[ok, abi.F_DISP_X] - o[ok, abi.F_DISP_X])) < 1e-4
-    assert np.max(np.abs(g[ok, abi.F_DISP_Y] - o[ok, abi.F_DISP_Y])) < 1e-4
     # filtering changes the result (the option is not silently ignored)
     p0 = abi.default_params(subset_size=21, enable_rotation=1, enable_normal_strain=1, enable_shear_strain=1,
                             fast_solver_tolerance=1e-5)

@@ -15,6 +15,7 @@ import pytest
 from dice_b200 import abi
 from dice_b200 import synthetic as syn
 from oracle import oracle as O
+from tests._exact import assert_rows_equal
 
 
 def _stripes(shift, w=199, h=199, stripes=10, width=20):
@@ -120,16 +121,17 @@ def test_subset_gamma_stripes_gpu():
             g = s.gamma(f)[0]
         o = O.gamma(p, ref, de, f)[0]
         assert abs(g - 0.4 * k) < 0.05, (k, g)
-        # the subset samples whole pixels, so the exact ZNSSD is a plain
-        # FP64 sum over the 99 x 99 window; the GPU's FP64 moments match it,
-        # while the reference's float running sums over 9801 pixels (which
-        # the oracle reproduces) drift by up to ~1e-4 relative
+        # the GPU forms the reference's float running sums in the reference's
+        # order (the 9801-pixel subset's arrays live in global memory), so it
+        # equals the oracle exactly; the subset samples whole pixels, so the
+        # exact ZNSSD is a plain FP64 sum over the 99 x 99 window, from which
+        # those float sums drift by up to ~3e-4 relative
+        assert g == o, (k, g, o)
         F = ref[51:150, 51:150].astype(np.float64)
         G = de[51:150, 51:150].astype(np.float64)
         a, b = F - F.mean(), G - G.mean()
         exact = 2.0 - 2.0 * (a * b).sum() / np.sqrt((a * a).sum() * (b * b).sum())
-        assert abs(g - exact) < 1e-5 * max(1.0, exact), (k, g, exact)
-        assert abs(g - o) < 1e-5 + 3e-4 * abs(o), (k, g, o)
+        assert abs(g - exact) < 1e-5 + 3e-4 * exact, (k, g, exact)
 
 
 @pytest.mark.gpu
@@ -165,5 +167,5 @@ def test_interp_shift_kat_gpu():
         o = f.copy()
         O.execute_frame(p, ref, _cos_image(s_), o)
         assert abs(g[0, abi.F_DISP_X] - s_) < 0.01, (s_, g[0, abi.F_DISP_X])
-        assert abs(g[0, abi.F_DISP_X] - o[0, abi.F_DISP_X]) < 1e-4
+        assert_rows_equal(g, o)
         assert g[0, abi.F_STATUS] == o[0, abi.F_STATUS]

@@ -22,6 +22,7 @@ from dice_b200 import synthetic as syn
 from dice_b200.results import diff_text
 from dice_b200.schema import Schema
 from oracle import oracle as O
+from tests._exact import assert_rows_equal
 from test_results import (GOLD, REGRESSION_FLOOR, REGRESSION_TOL, blocking_csr, check_example_files,
                           conformal_subset_def_case, obstruction_example_case, oracle_obstruction_example,
                           simple_obstruction_case)
@@ -57,10 +58,7 @@ def test_gpu_conformal_subset_def_gold(tmp_path):
     o = syn.init_fields(sf.coordinates[:, 0], sf.coordinates[:, 1])
     offs, ids = blocking_csr(sf)
     O.execute_frame_shapes(p, ref, deff, o, sf.shapes, sf.vx, sf.vy, offs, ids, force_simplex=sf.force_simplex)
-    assert np.array_equal(g[:, abi.F_STATUS], o[:, abi.F_STATUS])
-    assert np.array_equal(g[:, abi.F_ACTIVE_PIXELS], o[:, abi.F_ACTIVE_PIXELS])
-    # Gauss-Newton subsets 1 and 2
-    assert np.max(np.abs(g[[1, 2], abi.F_DISP_X:abi.F_DISP_Y + 1] - o[[1, 2], abi.F_DISP_X:abi.F_DISP_Y + 1])) < 1e-4
+    assert_rows_equal(g, o)
 
 
 def test_gpu_simple_obstruction_gold(tmp_path):
@@ -161,12 +159,8 @@ def test_gpu_blocking_tracking_matches_oracle(seed, skin):
     for k, d in enumerate(frames):
         O.execute_frame_shapes(p, ref, d, o, shapes, vx, vy, offs, ids, first_frame=(k == 0))
         g = gs[k]
-        assert np.array_equal(g[:, abi.F_STATUS], o[:, abi.F_STATUS])
-        assert np.array_equal(g[:, abi.F_ACTIVE_PIXELS], o[:, abi.F_ACTIVE_PIXELS])
-        ok = o[:, abi.F_STATUS] < 2
-        assert ok.mean() > 0.8
-        assert np.max(np.abs(g[ok, abi.F_DISP_X] - o[ok, abi.F_DISP_X])) < 1e-4
-        assert np.max(np.abs(g[ok, abi.F_DISP_Y] - o[ok, abi.F_DISP_Y])) < 1e-4
+        assert_rows_equal(g, o)
+        assert (o[:, abi.F_STATUS] < 2).mean() > 0.8
     # blocking and obstruction deactivated pixels somewhere
     full = np.asarray(O.rasterize(len(cx), [sh for sh in shapes if sh.role == 0], vx, vy)[0])
     npix = np.diff(full)
@@ -291,23 +285,18 @@ def _device_example(p, sf, frames, graph_check=False):
 
 
 def test_gpu_obstruction_example_subset_evolution(tmp_path):
-    """The example's own parameters: the blocked subset runs the simplex,
-    whose end point on the flat valley of gamma the rounding of gamma
-    decides (device and oracle differ by up to 0.05 px and 1e-3 rad in some
-    frames, and a few knife-edge pixels); the evolution state is equal."""
+    """The example's own parameters (the blocked subset runs the simplex):
+    device and oracle agree in every result column, the evolution state and
+    the turned-on reference intensities, frame by frame."""
     _need_gpu()
     sf, p, frames, out = obstruction_example_case()
     want_rows, want_states = oracle_obstruction_example(p, sf, frames)
     rows, states = _device_example(p, sf, frames, graph_check=True)
     for k in range(len(rows)):
-        assert np.array_equal(rows[k][:, abi.F_STATUS], want_rows[k][:, abi.F_STATUS]), k
-        d_act = np.abs(rows[k][:, abi.F_ACTIVE_PIXELS] - want_rows[k][:, abi.F_ACTIVE_PIXELS])
-        assert np.all(d_act <= 0.01 * want_rows[k][:, abi.F_ACTIVE_PIXELS]), k
-        assert np.max(np.abs(rows[k][:, abi.F_ROT_Z] - want_rows[k][:, abi.F_ROT_Z])) < 2e-3, k
+        assert_rows_equal(rows[k], want_rows[k])
         assert np.array_equal(states[k][0], want_states[k][0]), k
         on = states[k][0] == 2
-        # intensities interpolated at end points up to 0.05 px apart
-        assert np.max(np.abs(states[k][1][on] - want_states[k][1][on]), initial=0.0) < 4.0, k
+        assert np.array_equal(states[k][1][on], want_states[k][1][on]), k
     assert (states[-1][0] == 2).sum() >= 5
     # the example's comparison (the simplex end points of the 17 x 17
     # subset's near-zero rotation differ beyond the regression tolerance)
@@ -326,12 +315,8 @@ def test_gpu_obstruction_example_subset_evolution_gauss_newton():
     want_rows, want_states = oracle_obstruction_example(p, sf, frames)
     rows, states = _device_example(p, sf, frames)
     for k in range(len(rows)):
-        for col in (abi.F_STATUS, abi.F_ACTIVE_PIXELS, abi.F_ITERATIONS):
-            assert np.array_equal(rows[k][:, col], want_rows[k][:, col]), (k, col)
-        assert np.max(np.abs(rows[k][:, abi.F_DISP_X:abi.F_DISP_Y + 1] -
-                             want_rows[k][:, abi.F_DISP_X:abi.F_DISP_Y + 1])) < 1e-4, k
-        assert np.max(np.abs(rows[k][:, abi.F_ROT_Z] - want_rows[k][:, abi.F_ROT_Z])) < 1e-6, k
+        assert_rows_equal(rows[k], want_rows[k])
         assert np.array_equal(states[k][0], want_states[k][0]), k
         on = states[k][0] == 2
-        assert np.max(np.abs(states[k][1][on] - want_states[k][1][on]), initial=0.0) < 1e-2, k
+        assert np.array_equal(states[k][1][on], want_states[k][1][on]), k
     assert (states[-1][0] == 2).sum() >= 5
