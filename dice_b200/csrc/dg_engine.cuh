@@ -99,7 +99,7 @@ struct Engine {
       : A(a), tid(threadIdx.x), lane(threadIdx.x & 31), warp(threadIdx.x >> 5), T(blockDim.x) {}
 
   __device__ __forceinline__ float* pix() const { return pix_base<SHAPE>(A.pix_scratch, A.pix_stride); }
-  __device__ __forceinline__ PixArrays arrays() const { return pix_arrays_at(pix(), A.npix_cap); }
+  __device__ __forceinline__ PixArrays arrays() const { return pix_arrays_at<SHAPE>(pix(), A.npix_cap); }
 
   __device__ __forceinline__ void pixel_xy(const SubsetRef& sb, int p, int& x, int& y) const {
     if (sb.off < 0) {
@@ -169,16 +169,19 @@ struct Engine {
   // pass: mean and root sum of squares of F and of G, then the sum of
   // squared differences of the normalised intensities, each a float sum in
   // pixel order.  `def_sum2` receives the deformed sum of squares before
-  // its root (Subset::contrast_std_dev forms the same sum).  Uses GX, GY as
-  // scratch.
+  // its root (Subset::contrast_std_dev forms the same sum).  Uses rows 0 and
+  // 1 as scratch.
   __device__ float gamma_exact(const SubsetRef& sb, float* def_sum2 = nullptr) {
     const PixArrays X = arrays();
+    float* T0 = X.R(0);
+    float* T1 = X.R(1);
     const int n = ctl().n;
     const int np = sb.npix;
     float s[2];
-    // mean(REF_INTENSITIES), mean(DEF_INTENSITIES) (:285-301); G is 0 at
-    // pixels that are not live
-    chains(2, X.F, X.G, nullptr, nullptr, X.L, 0x0101u, np, s);
+    // mean(REF_INTENSITIES), mean(DEF_INTENSITIES) (:285-301) over the live
+    // pixels (G is 0 at the others)
+    for (int p = tid; p < np; p += T) T0[p] = (X.L[p] & 1) ? X.F[p] : 0.0f;
+    chains(2, T0, X.G, nullptr, nullptr, nullptr, 0u, np, s);
     const float mr = n ? __fdiv_rn(s[0], (float)n) : 0.0f;
     const float md = n ? __fdiv_rn(s[1], (float)n) : 0.0f;
     for (int p = tid; p < np; p += T) {
@@ -188,10 +191,10 @@ struct Engine {
         a = __fmul_rn(fa, fa);
         b = __fmul_rn(gb, gb);
       }
-      X.GX[p] = a;
-      X.GY[p] = b;
+      T0[p] = a;
+      T1[p] = b;
     }
-    chains(2, X.GX, X.GY, nullptr, nullptr, nullptr, 0u, np, s);
+    chains(2, T0, T1, nullptr, nullptr, nullptr, 0u, np, s);
     if (def_sum2) *def_sum2 = s[1];
     const float sr = __fsqrt_rn(s[0]), sd = __fsqrt_rn(s[1]);
     if (sr == 0.0f || sd == 0.0f) return -1.0f;
@@ -201,9 +204,9 @@ struct Engine {
         const float val = __fsub_rn(__fdiv_rn(__fsub_rn(X.G[p], md), sd), __fdiv_rn(__fsub_rn(X.F[p], mr), sr));
         t = __fmul_rn(val, val);
       }
-      X.GX[p] = t;
+      T0[p] = t;
     }
-    chains(1, X.GX, nullptr, nullptr, nullptr, nullptr, 0u, np, s);
+    chains(1, T0, nullptr, nullptr, nullptr, nullptr, 0u, np, s);
     return s[0];
   }
 
@@ -544,8 +547,12 @@ struct Engine {
       const int NW = T >> 5;
       const int hw0 = NW > 1 ? 1 : 0, hnw = NW > 1 ? NW - 1 : 1;
       DG_PT(t_h);
-      if (warp == 0 && lane < (fresh ? 2 : 1))
-        c.fres[lane] = chain_sum_masked(lane ? X.F : X.G, X.L, lane ? 2u : 1u, sb.npix);
+      if (warp == 0 && lane < (fresh ? 2 : 1)) {
+        // G is 0 at the pixels that are not live, and every pixel of a subset
+        // without evolution state is active
+        c.fres[lane] = sb.evo ? chain_sum_masked(lane ? X.F : X.G, X.L, lane ? 2u : 1u, sb.npix)
+                              : chain_sum(lane ? X.F : X.G, sb.npix);
+      }
       __syncwarp();
       h_sweep<SHAPE, DEFGRAD>(inb, k, hw0, hnw);
       __syncthreads();
@@ -787,7 +794,7 @@ struct Engine {
   // Subset::noise_std_dev (DICe_Subset.cpp:622-703) on the deformed image
   // over the box of the last pass's live pixels moved by (u, v): the 3 x 3
   // Immerkaer mask (j outer, i inner), |.| summed in float, row by row.  The
-  // terms are computed by the CTA a chunk at a time into DX and summed in
+  // terms are computed by the CTA a chunk at a time into row 0 and summed in
   // order by one thread.  Reads go through the row-major linear index like
   // the reference's operator() (0 outside the array).
   __device__ float noise_exact(const SubsetRef& sb, const float* slots, int n, int bminx, int bmaxx, int bminy,
@@ -815,7 +822,7 @@ struct Engine {
       auto ld = [&](long li) -> float { return (li >= 0 && li < lim) ? __ldg(I + li) : 0.0f; };
       const long total = (long)rw * rh;
       const int chunk = A.npix_cap;
-      float* buf = arrays().DX;
+      float* buf = arrays().R(0);
       Ctl& c = ctl();
       for (long b0 = 0; b0 < total; b0 += chunk) {
         const int m = (int)min((long)chunk, total - b0);
@@ -857,22 +864,37 @@ struct Engine {
 
   // Objective::sigma (DICe_Objective.cpp:150-184) at the state of the last
   // pass with gradients: noise_std_dev, then the float sums of the squared
-  // gradients over the live pixels.
+  // gradients over the live pixels (the deformed-image gradients stored in
+  // rows 0 and 1, or the reference image's at the pixel).
   __device__ float sigma(const SubsetRef& sb, const float* slots, float& noise) {
     Ctl& c = ctl();
     const int n = c.n, bx0 = c.minx, bx1 = c.maxx, by0 = c.miny, by1 = c.maxy;
     const PixArrays X = arrays();
+    float* T0 = X.R(0);
+    float* T1 = X.R(1);
+    const long rlim = (long)A.ref.w * A.ref.h;
     for (int p = tid; p < sb.npix; p += T) {
       float a = 0.0f, b = 0.0f;
       if (X.L[p] & 1) {
-        a = X.GX[p] * X.GX[p];
-        b = X.GY[p] * X.GY[p];
+        float gx, gy;
+        if (DEFGRAD) {
+          gx = T0[p];
+          gy = T1[p];
+        } else {
+          int x, y;
+          pixel_xy(sb, p, x, y);
+          const long ri = (long)y * A.ref.w + x;
+          gx = ri < rlim ? __ldg(A.ref.gx + ri) : 0.0f;
+          gy = ri < rlim ? __ldg(A.ref.gy + ri) : 0.0f;
+        }
+        a = gx * gx;
+        b = gy * gy;
       }
-      X.DX[p] = a;
-      X.DY[p] = b;
+      T0[p] = a;
+      T1[p] = b;
     }
     float s[2];
-    chains(2, X.DX, X.DY, nullptr, nullptr, nullptr, 0u, sb.npix, s);
+    chains(2, T0, T1, nullptr, nullptr, nullptr, 0u, sb.npix, s);
     noise = noise_exact(sb, slots, n, bx0, bx1, by0, by1);
     if (noise < 0.0f) return -1.0f;
     const float sg = s[0] > s[1] ? s[1] : s[0];

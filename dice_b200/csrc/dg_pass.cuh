@@ -101,8 +101,18 @@ struct __align__(16) SimplexState {
 };
 
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~(size_t)15; }
-// per-pixel array capacity: a multiple of 16 pixels (16-byte aligned rows)
-__host__ __device__ inline int pix_cap(int npix_max) { return (npix_max + 15) & ~15; }
+// per-pixel array capacity: a multiple of 32 pixels
+__host__ __device__ inline int pix_cap(int npix_max) { return (npix_max + 31) & ~31; }
+// distance between the per-pixel float arrays: cap + 4 floats, so that the
+// same pixel's entries of the rows fall in distinct banks (and every row
+// starts on a 16-byte boundary)
+__host__ __device__ inline int pix_stride(int cap) { return cap + 4; }
+// stored per-pixel rows besides F and G: the affine residual vector r_0..r_5,
+// or the quadratic subset's gradients (its residuals are products of them)
+template <int SHAPE>
+struct PixRows {
+  static constexpr int NR = SHAPE == DICEGPU_QUADRATIC_SF ? 2 : 6;
+};
 
 template <int SHAPE>
 struct SmemPlan {
@@ -112,8 +122,10 @@ struct SmemPlan {
   static __host__ __device__ size_t pix(int W) {
     return vbuf(W) + a16((size_t)W * 32 * Layout<SHAPE>::VS * sizeof(float));
   }
-  // six float arrays and one byte array of `cap` pixels
-  static __host__ __device__ size_t pix_bytes(int cap) { return a16((size_t)cap * (6 * 4 + 1)); }
+  // F, G and the stored rows (floats, pix_stride apart), then one byte per pixel
+  static __host__ __device__ size_t pix_bytes(int cap) {
+    return a16((size_t)(2 + PixRows<SHAPE>::NR) * pix_stride(cap) * 4 + (size_t)cap);
+  }
   static __host__ __device__ size_t total(int W, int cap) { return pix(W) + pix_bytes(cap); }
 };
 
@@ -135,17 +147,18 @@ __device__ __forceinline__ float* warp_vbuf() {
 }
 
 // The per-pixel arrays: F (reference intensity), G (deformed intensity, 0 at
-// pixels that are not live), GX / GY (gradients used by the residuals), DX /
-// DY (the affine map's stretched offsets), L (bit 0 live: active and not
-// deactivated this step; bit 1 active).
+// pixels that are not live), the rows R(i) (affine: the residual vector of
+// the last Gauss-Newton pass, 0 at pixels that are not live; quadratic: the
+// gradients; after a PK_STATE pass rows 0 and 1 hold the gradients), L (bit 0
+// live: active and not deactivated this step; bit 1 active).  The arrays
+// beyond the subset's pixels up to a multiple of 32 hold zeros after a pass.
 struct PixArrays {
   float* F;
   float* G;
-  float* GX;
-  float* GY;
-  float* DX;
-  float* DY;
+  float* R0;
+  int S;        // float distance between rows
   uint8_t* L;
+  __device__ __forceinline__ float* R(int i) const { return R0 + (size_t)i * S; }
 };
 // Where a CTA's pixel arrays live: its shared memory, or for subsets too
 // large for it, this CTA's slice of a global scratch buffer (`stride` bytes
@@ -155,15 +168,15 @@ __device__ __forceinline__ float* pix_base(unsigned char* scratch, size_t stride
   return scratch ? reinterpret_cast<float*>(scratch + (size_t)blockIdx.x * stride)
                  : reinterpret_cast<float*>(dg_smem + SmemPlan<SHAPE>::pix(blockDim.x >> 5));
 }
+template <int SHAPE>
 __device__ __forceinline__ PixArrays pix_arrays_at(float* b, int cap) {
   PixArrays a;
+  const int S = pix_stride(cap);
+  a.S = S;
   a.F = b;
-  a.G = b + cap;
-  a.GX = b + 2 * (size_t)cap;
-  a.GY = b + 3 * (size_t)cap;
-  a.DX = b + 4 * (size_t)cap;
-  a.DY = b + 5 * (size_t)cap;
-  a.L = reinterpret_cast<uint8_t*>(b + 6 * (size_t)cap);
+  a.G = b + S;
+  a.R0 = b + 2 * (size_t)S;
+  a.L = reinterpret_cast<uint8_t*>(b + (size_t)(2 + PixRows<SHAPE>::NR) * S);
   return a;
 }
 
@@ -375,17 +388,31 @@ enum { PK_GN = 0, PK_STATE = 1, PK_GAMMA = 2 };
 // count and box in Ctl (all threads may read them after the final barrier).
 template <int SHAPE, int INTERP, bool DEFGRAD, int KIND, bool MASKED>
 __device__ __noinline__ void cta_pass(const PassInT<MASKED> in, const MapConst k) {
+  using L = Layout<SHAPE>;
   constexpr bool GRADS = KIND != PK_GAMMA;
+  constexpr bool AFF = SHAPE != DICEGPU_QUADRATIC_SF;
   const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const bool use_ref_grads = !DEFGRAD;
   const float fcx = (float)in.cx, fcy = (float)in.cy;
   const int W = in.def.w, H = in.def.h;
-  const PixArrays A = pix_arrays_at(in.pix, in.cap);
+  const PixArrays A = pix_arrays_at<SHAPE>(in.pix, in.cap);
   int n = 0;
   int minx = in.cx, maxx = in.cx, miny = in.cy, maxy = in.cy;
   MaskView mv;
   if constexpr (MASKED) mv = MaskView(in.mdesc, in.mbits, in.bpoly, in.bvx, in.bvy);
   PixelWalk pw(in, tid, T);
-  for (int p = tid; p < in.npix; p += T) {
+  const int npad = (in.npix + 31) & ~31;
+  for (int p = tid; p < npad; p += T) {
+    if (p >= in.npix) {
+      // the padding up to a multiple of 32 pixels: zeros for the sweeps
+      A.G[p] = 0.0f;
+      A.L[p] = 0;
+      if (KIND == PK_GN) {
+#pragma unroll
+        for (int i = 0; i < PixRows<SHAPE>::NR; ++i) A.R(i)[p] = 0.0f;
+      }
+      continue;
+    }
     int x, y;
     pw.xy(in, p, x, y);
     pw.advance();
@@ -426,13 +453,17 @@ __device__ __noinline__ void cta_pass(const PassInT<MASKED> in, const MapConst k
     A.F[p] = F;
     A.G[p] = live ? G : 0.0f;
     A.L[p] = (uint8_t)((live ? 1 : 0) | (active ? 2 : 0));
-    if (GRADS) {
-      A.GX[p] = gx;
-      A.GY[p] = gy;
-    }
-    if (KIND == PK_GN && SHAPE != DICEGPU_QUADRATIC_SF) {
-      A.DX[p] = Dx;
-      A.DY[p] = Dy;
+    if (KIND == PK_GN && AFF) {
+      // the residual vector of Objective_ZNSSD::computeUpdateFast (:538)
+      float r[L::VW];
+#pragma unroll
+      for (int i = 0; i < L::VW; ++i) r[i] = 0.0f;
+      if (live) residuals_D<SHAPE>(k, dxf, dyf, Dx, Dy, gx, gy, use_ref_grads, r);
+#pragma unroll
+      for (int i = 0; i < PixRows<SHAPE>::NR; ++i) A.R(i)[p] = r[i];
+    } else if (GRADS) {
+      A.R(0)[p] = gx;
+      A.R(1)[p] = gy;
     }
   }
   // per-warp results
@@ -459,35 +490,31 @@ __device__ __noinline__ void cta_pass(const PassInT<MASKED> in, const MapConst k
   __syncthreads();
 }
 
-// Residual vector of a stored pixel (the affine map's stretched offsets were
-// stored by the PK_GN pass; quadratic residuals use the plain offsets).
-template <int SHAPE>
-__device__ __forceinline__ void stored_residuals(const PassIn& in, const PixArrays& A, const MapConst& k, int p, int x,
-                                                 int y, bool use_ref_grads, float* r) {
+// The residual vector of a stored pixel of a quadratic subset (from its
+// stored gradients; Quadratic_Shape_Function::residuals, :580-614).
+__device__ __forceinline__ void quad_residuals(const PassIn& in, const PixArrays& A, const MapConst& k, int p, int x,
+                                               int y, bool use_ref_grads, float* r) {
   const float dxf = __fsub_rn((float)x, (float)in.cx), dyf = __fsub_rn((float)y, (float)in.cy);
-  float Dx = dxf, Dy = dyf;
-  if (SHAPE != DICEGPU_QUADRATIC_SF) {
-    Dx = A.DX[p];
-    Dy = A.DY[p];
-  }
-  residuals_D<SHAPE>(k, dxf, dyf, Dx, Dy, A.GX[p], A.GY[p], use_ref_grads, r);
+  residuals_D<DICEGPU_QUADRATIC_SF>(k, dxf, dyf, dxf, dyf, A.R(0)[p], A.R(1)[p], use_ref_grads, r);
 }
 
 // The Hessian sweep over the stored pixels, run by warps w0 .. w0 + nw - 1
-// (full warps; pixel p goes to thread p mod 32 nw of them): the exact
-// products r_i r_j summed by the FP64 mma (WarpOut.M) and the float
-// products' rounding errors fma(r_i, r_j, -fl(r_i r_j)) (WarpOut.E), whose
-// difference is the reference's sum of float products.  Warps outside the
-// range return at once.  No barrier.
+// (full warps, 32 pixels a step): the exact products r_i r_j summed by the
+// FP64 mma (WarpOut.M) and the float products' rounding errors
+// fma(r_i, r_j, -fl(r_i r_j)) (WarpOut.E), whose difference is the
+// reference's sum of float products.  The affine residual rows are read
+// straight from the stored arrays (rows pix_stride apart: conflict-free
+// fragments); quadratic residuals are formed from the stored gradients and
+// staged.  Warps outside the range return at once.  No barrier.
 template <int SHAPE, bool DEFGRAD>
 __device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, int nw) {
   using L = Layout<SHAPE>;
+  constexpr bool AFF = SHAPE != DICEGPU_QUADRATIC_SF;
   constexpr int NSET = 2;   // independent mma accumulator sets
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < w0 || warp >= w0 + nw) return;
-  const int t = (warp - w0) * 32 + lane, TT = 32 * nw;
   const bool use_ref_grads = !DEFGRAD;
-  const PixArrays A = pix_arrays_at(in.pix, in.cap);
+  const PixArrays A = pix_arrays_at<SHAPE>(in.pix, in.cap);
   double c[NSET][3][2];
   float e[L::NP];
 #pragma unroll
@@ -496,17 +523,26 @@ __device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, 
     for (int b = 0; b < 3; ++b) { c[s2][b][0] = 0.0; c[s2][b][1] = 0.0; }
 #pragma unroll
   for (int i = 0; i < L::NP; ++i) e[i] = 0.0f;
-  PixelWalk pw(in, t, TT);
+  const int nblk = (in.npix + 31) >> 5;
+  const int kk = lane & 3, ii = lane >> 2;
+  // affine: the mma fragment's row (residual index ii, zero beyond the six)
+  const float* frag = A.R(ii < PixRows<SHAPE>::NR ? ii : 0) + kk;
   const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_vbuf<SHAPE>());
-  for (int base = 0; base < in.npix; base += TT) {
-    const int p = base + t;
+  PixelWalk pw(in, (warp - w0) * 32 + lane, 32 * nw);
+  for (int blk = warp - w0; blk < nblk; blk += nw) {
+    const int p = blk * 32 + lane;
     float v[L::VW];
 #pragma unroll
     for (int i = 0; i < L::VW; ++i) v[i] = 0.0f;
-    if (p < in.npix && (A.L[p] & 1)) {
-      int x, y;
-      pw.xy(in, p, x, y);
-      stored_residuals<SHAPE>(in, A, k, p, x, y, use_ref_grads, v);
+    if (A.L[p] & 1) {
+      if (AFF) {
+#pragma unroll
+        for (int i = 0; i < L::NS; ++i) v[i] = A.R(i)[p];
+      } else {
+        int x, y;
+        pw.xy(in, p, x, y);
+        quad_residuals(in, A, k, p, x, y, use_ref_grads, v);
+      }
       int idx = 0;
 #pragma unroll
       for (int i = 0; i < L::NS; ++i)
@@ -516,28 +552,30 @@ __device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, 
           e[idx] = __fadd_rn(e[idx], fmaf(v[i], v[j], -pr));
         }
     }
-    pw.advance();
-    // stage the warp's 32 pixel vectors, then groups of 4 pixels through the FP64 mma
-    const unsigned vrow = vbase + (unsigned)(lane * L::VS) * 4u;
+    if (!AFF) {
+      pw.advance();
+      // stage the warp's 32 pixel vectors
+      const unsigned vrow = vbase + (unsigned)(lane * L::VS) * 4u;
 #pragma unroll
-    for (int i = 0; i < L::VW; i += 4) sts_v4(vrow + 4u * i, v[i], v[i + 1], v[i + 2], v[i + 3]);
-    __syncwarp();
-    const int kk = lane & 3, ii = lane >> 2;
+      for (int i = 0; i < L::VW; i += 4) sts_v4(vrow + 4u * i, v[i], v[i + 1], v[i + 2], v[i + 3]);
+      __syncwarp();
+    }
+    // groups of 4 pixels through the FP64 mma
 #pragma unroll
     for (int g = 0; g < 8; ++g) {
-      const unsigned src = vbase + (unsigned)((4 * g + kk) * L::VS + ii) * 4u;
       double(&cs)[3][2] = c[g % NSET];
-      if (SHAPE == DICEGPU_QUADRATIC_SF) {
+      if (AFF) {
+        const double a0 = ii < PixRows<SHAPE>::NR ? (double)frag[blk * 32 + 4 * g] : 0.0;
+        dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
+      } else {
+        const unsigned src = vbase + (unsigned)((4 * g + kk) * L::VS + ii) * 4u;
         const double a0 = (double)lds_f(src), a1 = (double)lds_f(src + 32u);
         dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
         dmma_8x8x4(cs[1][0], cs[1][1], a0, a1);
         dmma_8x8x4(cs[2][0], cs[2][1], a1, a1);
-      } else {
-        const double a0 = (double)lds_f(src);
-        dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
       }
     }
-    __syncwarp();
+    if (!AFF) __syncwarp();
   }
 #pragma unroll
   for (int s2 = 1; s2 < NSET; ++s2)
@@ -552,7 +590,7 @@ __device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, 
   constexpr int VW = L::VW;
   double* C = wo.M;
   const double(&cf)[3][2] = c[0];
-  if (SHAPE == DICEGPU_QUADRATIC_SF) {
+  if (!AFF) {
     C[r * VW + cc] = cf[0][0];           C[r * VW + cc + 1] = cf[0][1];
     C[r * VW + 8 + cc] = cf[1][0];       C[r * VW + 8 + cc + 1] = cf[1][1];
     C[(8 + cc) * VW + r] = cf[1][0];     C[(8 + cc + 1) * VW + r] = cf[1][1];
@@ -575,24 +613,30 @@ __device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, 
 template <int SHAPE, bool DEFGRAD>
 __device__ __noinline__ void q_sweep(const PassIn in, const MapConst k, float meanG, float meanF) {
   using L = Layout<SHAPE>;
+  constexpr bool AFF = SHAPE != DICEGPU_QUADRATIC_SF;
   const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31;
   const bool use_ref_grads = !DEFGRAD;
-  const PixArrays A = pix_arrays_at(in.pix, in.cap);
+  const PixArrays A = pix_arrays_at<SHAPE>(in.pix, in.cap);
   double q[L::NS];
 #pragma unroll
   for (int i = 0; i < L::NS; ++i) q[i] = 0.0;
   PixelWalk pw(in, tid, T);
   for (int p = tid; p < in.npix; p += T) {
     if (A.L[p] & 1) {
-      int x, y;
-      pw.xy(in, p, x, y);
       const float GmF = __fsub_rn(__fsub_rn(A.G[p], meanG), __fsub_rn(A.F[p], meanF));
       float r[L::VW];
-      stored_residuals<SHAPE>(in, A, k, p, x, y, use_ref_grads, r);
+      if (AFF) {
+#pragma unroll
+        for (int i = 0; i < L::NS; ++i) r[i] = A.R(i)[p];
+      } else {
+        int x, y;
+        pw.xy(in, p, x, y);
+        quad_residuals(in, A, k, p, x, y, use_ref_grads, r);
+      }
 #pragma unroll
       for (int i = 0; i < L::NS; ++i) q[i] = __dadd_rn(q[i], (double)__fmul_rn(GmF, r[i]));
     }
-    pw.advance();
+    if (!AFF) pw.advance();
   }
   WarpOut<SHAPE>& wo = wouts<SHAPE>()[tid >> 5];
 #pragma unroll
