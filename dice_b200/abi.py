@@ -281,7 +281,8 @@ def _declare(lib):
         "dicegpu_set_launch_shape": (c_int, [c_void_p, c_int, c_int]),
         "dicegpu_get_launch_shape": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
         "dicegpu_correlate": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p,
-                                      c_int, c_int, P]),
+                                      c_int, c_int, P, c_int]),
+        "dicegpu_correlate_reset": (c_int, []),
         "dicegpu_interpolate": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p,
                                         c_void_p, c_int]),
         "dicegpu_image_gradients": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_int,

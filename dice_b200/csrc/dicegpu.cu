@@ -2205,9 +2205,10 @@ extern "C" int dicegpu_image_gradients_noalloc(int w, int h, const float* d_img,
   if (!d_img || !d_gx || !d_gy || w < 3 || h < 3) return DICEGPU_ERR_ARG;
   if (method != DICEGPU_FINITE_DIFFERENCE && method != DICEGPU_CONVOLUTION_5_POINT)
     return DICEGPU_ERR_ARG;
-  if ((long long)w * h > DICEGPU_NOALLOC_MAX_PIXELS) return DICEGPU_ERR_ARG;
   float* tmp = nullptr;
   if (method == DICEGPU_CONVOLUTION_5_POINT) {
+    // only the smoothing step needs the intermediate planes
+    if ((long long)w * h > DICEGPU_NOALLOC_MAX_PIXELS) return DICEGPU_ERR_ARG;
     const int rc = noalloc_scratch(&tmp);
     if (rc) return rc;
   }
@@ -2216,35 +2217,85 @@ extern "C" int dicegpu_image_gradients_noalloc(int w, int h, const float* d_img,
   return launch_gradients(w, h, d_img, d_gx, d_gy, method, tmp, (cudaStream_t)stream, nullptr);
 }
 
-// dice_correlate's stride-9 interface (DICe_api.cpp:51-151) over a context
-// created for the call.
+// dice_correlate's stride-9 interface (DICe_api.cpp:51-151).  As the
+// reference keeps a static Schema, one context lives across calls: the first
+// call creates it from the parameters (tracking_default_params when NULL,
+// DICe_api.cpp:84-93), the subset size and coordinates, and the reference
+// image; every call takes a new deformed image and the nine stride-9 columns
+// of every subset, the other field columns carrying over from the previous
+// call as the Schema's fields do; the parameters are read again only when
+// update_params is set (DICe_api.cpp:114-115).  The frame count carries over
+// too, so only the first call is the sequence's first frame.
+namespace {
+std::mutex g_api_mu;
+dicegpu_ctx* g_api_ctx = nullptr;
+int g_api_device = -1;
+int g_api_subset = 0;
+std::vector<double> g_api_rows;   // the context's field rows after the last call
+
+int api_params(const dicegpu_params* in, int subset_size, dicegpu_params* p) {
+  if (in) {
+    *p = *in;
+  } else {
+    const int rc = dicegpu_tracking_default_params(p);
+    if (rc) return rc;
+  }
+  // the api routines take the affine shape function only (DICe_api.cpp:116)
+  if (p->shape_function != DICEGPU_AFFINE_SF) return DICEGPU_ERR_UNSUPPORTED;
+  p->subset_size = subset_size;
+  p->use_def_gradients = 1;   // arrays: Schema::set_def_image(w,h,array), DICe_Schema.cpp:339
+  return DICEGPU_OK;
+}
+
+void api_release() {
+  if (!g_api_ctx) return;
+  int cur = -1;
+  const bool restore = cudaGetDevice(&cur) == cudaSuccess && cur != g_api_device;
+  if (restore) cudaSetDevice(g_api_device);
+  dicegpu_destroy(g_api_ctx);
+  if (restore) cudaSetDevice(cur);
+  g_api_ctx = nullptr;
+  g_api_device = -1;
+  g_api_subset = 0;
+  g_api_rows.clear();
+}
+}  // namespace
+
 extern "C" int dicegpu_correlate(float* points, int n_points, int subset_size, const float* ref_img,
                                  int ref_w, int ref_h, const float* def_img, int def_w, int def_h,
-                                 const dicegpu_params* params) {
+                                 const dicegpu_params* params, int update_params) {
   if (ref_w != def_w || ref_h != def_h) return -1;
   if (subset_size < 1) return -1;
   if (n_points < 1) return -1;
   if (!points || !ref_img || !def_img) return -1;
-  dicegpu_params p;
-  if (params) {
-    p = *params;
+  std::lock_guard<std::mutex> lock(g_api_mu);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DICEGPU_ERR_CUDA;
+  int rc = DICEGPU_OK;
+  const bool first = g_api_ctx == nullptr;
+  if (first) {
+    dicegpu_params p;
+    rc = api_params(params, subset_size, &p);
+    if (rc) return rc;
+    rc = dicegpu_create(&p, &g_api_ctx);
+    if (rc) return rc;
+    g_api_device = dev;
+    g_api_subset = subset_size;
+    g_api_rows.assign((size_t)n_points * DICEGPU_FIELD_STRIDE, 0.0);
   } else {
-    // tracking_default_params (DICe_ParameterUtilities.cpp:297-361)
-    dicegpu_default_params(&p);
-    p.optimization = DICEGPU_SIMPLEX;
-    p.enable_rotation = 1;
-    p.disp_jump_tol = 8.0;
-    p.theta_jump_tol = 0.1;
+    // the subsets are the first call's; a context made on another device
+    // cannot be used from this one
+    if ((size_t)n_points * DICEGPU_FIELD_STRIDE != g_api_rows.size()) return DICEGPU_ERR_ARG;
+    if (dev != g_api_device) return DICEGPU_ERR_STATE;
+    if (update_params) {
+      dicegpu_params p;
+      rc = api_params(params, g_api_subset, &p);
+      if (!rc) rc = dicegpu_set_params(g_api_ctx, &p);
+      if (rc) return rc;
+    }
   }
-  if (p.shape_function != DICEGPU_AFFINE_SF) return DICEGPU_ERR_UNSUPPORTED;
-  p.subset_size = subset_size;
-  p.use_def_gradients = 1;   // arrays: Schema::set_def_image(w,h,array), DICe_Schema.cpp:339
-  dicegpu_ctx* c = nullptr;
-  int rc = dicegpu_create(&p, &c);
-  if (rc) return rc;
-  std::vector<double> f((size_t)n_points * DICEGPU_FIELD_STRIDE, 0.0);
   for (int i = 0; i < n_points; ++i) {
-    double* r = &f[(size_t)i * DICEGPU_FIELD_STRIDE];
+    double* r = &g_api_rows[(size_t)i * DICEGPU_FIELD_STRIDE];
     const float* q = points + (size_t)i * DICEGPU_API_STRIDE;
     r[DICEGPU_F_COORD_X] = q[0];
     r[DICEGPU_F_COORD_Y] = q[1];
@@ -2256,26 +2307,40 @@ extern "C" int dicegpu_correlate(float* points, int n_points, int subset_size, c
     r[DICEGPU_F_BETA] = q[7];
     r[DICEGPU_F_STATUS] = q[8];
   }
-  if (!rc) rc = dicegpu_set_ref_image(c, ref_w, ref_h, ref_img, 0);
-  if (!rc) rc = dicegpu_set_def_image(c, def_w, def_h, def_img, 0);
-  if (!rc) rc = dicegpu_set_subsets(c, n_points, f.data());
-  if (!rc) rc = dicegpu_execute_correlation(c);
-  if (!rc) rc = dicegpu_get_fields(c, f.data());
-  if (!rc) {
-    for (int i = 0; i < n_points; ++i) {
-      const double* r = &f[(size_t)i * DICEGPU_FIELD_STRIDE];
-      float* q = points + (size_t)i * DICEGPU_API_STRIDE;
-      q[2] = (float)r[DICEGPU_F_DISP_X];
-      q[3] = (float)r[DICEGPU_F_DISP_Y];
-      q[4] = (float)r[DICEGPU_F_ROT_Z];
-      q[5] = (float)r[DICEGPU_F_SIGMA];
-      q[6] = (float)r[DICEGPU_F_GAMMA];
-      q[7] = (float)r[DICEGPU_F_BETA];
-      q[8] = (float)r[DICEGPU_F_STATUS];
-    }
+  dicegpu_ctx* c = g_api_ctx;
+  if (first) {
+    rc = dicegpu_set_ref_image(c, ref_w, ref_h, ref_img, 0);
+    if (!rc) rc = dicegpu_set_subsets(c, n_points, g_api_rows.data());
+  } else if (cudaMemcpyAsync(c->d_fields, g_api_rows.data(), g_api_rows.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
+    rc = DICEGPU_ERR_CUDA;   // (dicegpu_load_fields would restart the sequence)
   }
-  dicegpu_destroy(c);
-  return rc;
+  if (!rc) rc = dicegpu_set_def_image(c, def_w, def_h, def_img, 0);
+  if (!rc) rc = dicegpu_execute_correlation(c);
+  if (!rc) rc = dicegpu_get_fields(c, g_api_rows.data());
+  if (rc) {
+    // a failed call leaves no half-made state behind
+    api_release();
+    return rc;
+  }
+  for (int i = 0; i < n_points; ++i) {
+    const double* r = &g_api_rows[(size_t)i * DICEGPU_FIELD_STRIDE];
+    float* q = points + (size_t)i * DICEGPU_API_STRIDE;
+    q[2] = (float)r[DICEGPU_F_DISP_X];
+    q[3] = (float)r[DICEGPU_F_DISP_Y];
+    q[4] = (float)r[DICEGPU_F_ROT_Z];
+    q[5] = (float)r[DICEGPU_F_SIGMA];
+    q[6] = (float)r[DICEGPU_F_GAMMA];
+    q[7] = (float)r[DICEGPU_F_BETA];
+    q[8] = (float)r[DICEGPU_F_STATUS];
+  }
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_correlate_reset(void) {
+  std::lock_guard<std::mutex> lock(g_api_mu);
+  api_release();
+  return DICEGPU_OK;
 }
 
 #ifdef DG_PROFILE

@@ -367,8 +367,12 @@ class Schema:
         return oi, gx, gy
 
 
-def correlate(points, subset_size, ref, deff, params=None):
-    """dice_correlate mirror: points is an (n, 9) float32 array updated in place."""
+def correlate(points, subset_size, ref, deff, params=None, update_params=False):
+    """dice_correlate mirror: points is an (n, 9) float32 array updated in
+    place.  The library keeps one context across calls, as the reference keeps
+    a static Schema: the first call fixes the reference image, subset size and
+    subsets; later calls correlate `deff` as the next frame and read `params`
+    again only with update_params.  correlate_reset() starts over."""
     lib = abi.load_library()
     pts = np.ascontiguousarray(points, dtype=np.float32)
     ref = _as_host_f32(ref)
@@ -378,7 +382,12 @@ def correlate(points, subset_size, ref, deff, params=None):
     rc = lib.dicegpu_correlate(pts.ctypes.data_as(ctypes.c_void_p), pts.shape[0], subset_size,
                                ref.ctypes.data_as(ctypes.c_void_p), w, h,
                                deff.ctypes.data_as(ctypes.c_void_p), dw, dh,
-                               ctypes.byref(params) if params is not None else None)
+                               ctypes.byref(params) if params is not None else None, int(bool(update_params)))
     if rc == 0:
         points[...] = pts
     return rc
+
+
+def correlate_reset():
+    """Releases the context `correlate` keeps (dicegpu_correlate_reset)."""
+    return abi.load_library().dicegpu_correlate_reset()

@@ -456,16 +456,33 @@ int dicegpu_set_launch_shape(dicegpu_ctx* ctx, int warps_per_cta, int ctas_per_s
 int dicegpu_get_launch_shape(dicegpu_ctx* ctx, int* warps_per_cta, int* ctas_per_sm);
 
 /* ---- stride-9 API (mirror of dice_correlate) ------------------------------
- * points: n * 9 floats [x, y, u, v, theta, sigma, gamma, beta, flag]; on input
- * sigma < 0 asks for an automatic guess (here: zero motion), otherwise u, v,
- * theta are the guess.  Square subsets of `subset_size`.  Images are host
- * arrays.  params may be NULL (tracking defaults as in DICe_api.cpp:96: affine
- * u,v,theta, simplex, 8 px / 0.1 rad jump tolerances).
- * Returns -1 on bad arguments like dice_correlate (DICe_api.cpp:71-76). */
+ * Replaces dice_correlate (DICe_api.cpp:51-151); update_params is its
+ * `const bool update_params`.  points: n * 9 floats [x, y, u, v, theta,
+ * sigma, gamma, beta, flag]; u, v, theta are the guess, and the results
+ * overwrite columns 2..8.  Images are host float arrays of equal size.
+ *
+ * Like the reference's static Schema, one context persists across calls (on
+ * the device current at the first call, which later calls must keep):
+ *  - the first call creates it from params (NULL: the tracking defaults of
+ *    dicegpu_tracking_default_params, as DICe_api.cpp:84-93), square subsets
+ *    of subset_size at the points' coordinates, and ref_img;
+ *  - every later call keeps that reference image, subset size and subset
+ *    count (ref_img and subset_size are not read again; another n_points is
+ *    rejected with DICEGPU_ERR_ARG), writes the nine columns of every subset
+ *    over the context's field rows (the other columns carry over), correlates
+ *    def_img as the next frame of the sequence, and re-reads params (NULL:
+ *    the tracking defaults) only when update_params is non-zero;
+ *  - dicegpu_correlate_reset releases the context; the next call starts a
+ *    new one.  A call that fails after the checks below releases it too.
+ * Calls are serialised by a lock.  Returns -1 on the reference's argument
+ * checks (DICe_api.cpp:71-76: image sizes differ, subset_size < 1,
+ * n_points < 1), DICEGPU_ERR_UNSUPPORTED for a shape function other than
+ * affine (the reference throws, DICe_api.cpp:116). */
 int dicegpu_correlate(float* points, int n_points, int subset_size,
                       const float* ref_img, int ref_w, int ref_h,
                       const float* def_img, int def_w, int def_h,
-                      const dicegpu_params* params);
+                      const dicegpu_params* params, int update_params);
+int dicegpu_correlate_reset(void);
 
 /* ---- per-call kernels for the Objective / Image interfaces --------------- */
 /* Interpolates the context's deformed image (and its gradients when present)
@@ -495,11 +512,15 @@ int dicegpu_gauss_filter(int w, int h, const float* d_in, float* d_out, int mask
  * device-wide wait of cudaFree.  The smoothing step's two intermediate
  * planes live in a file-scope device array of 2 * DICEGPU_NOALLOC_MAX_PIXELS
  * floats (8 MiB) that every GPU loading the library holds until exit.
- * Images larger than DICEGPU_NOALLOC_MAX_PIXELS pixels are rejected with
- * DICEGPU_ERR_ARG.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) and caches it; make that first call before
- * any stream capture.  All calls share the one array: calls whose GPU work
- * overlaps (other streams, other host threads) race on it and must be
+ * With DICEGPU_CONVOLUTION_5_POINT, images larger than
+ * DICEGPU_NOALLOC_MAX_PIXELS pixels are rejected with DICEGPU_ERR_ARG;
+ * DICEGPU_FINITE_DIFFERENCE uses no intermediate planes and takes any size.
+ * The first 5-point call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and caches it per device for the process; the
+ * cached address belongs to that device's context, so after a
+ * cudaDeviceReset of that device it is stale and the 5-point method must not
+ * be called on it again.  All calls share the one array: calls whose GPU
+ * work overlaps (other streams, other host threads) race on it and must be
  * serialised by the caller.  Both image pointers are device memory. */
 #define DICEGPU_NOALLOC_MAX_PIXELS (1024 * 1024)
 int dicegpu_image_gradients_noalloc(int w, int h, const float* d_img, float* d_gx, float* d_gy,

@@ -59,9 +59,9 @@ def test_correlate_rejects_bad_arguments_like_reference():
     img = np.zeros((32, 32), np.float32)
     img2 = np.zeros((32, 33), np.float32)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
-    assert lib.dicegpu_correlate(P(pts), 1, 21, P(img), 32, 32, P(img2), 33, 32, None) == -1
-    assert lib.dicegpu_correlate(P(pts), 1, 0, P(img), 32, 32, P(img), 32, 32, None) == -1
-    assert lib.dicegpu_correlate(P(pts), 0, 21, P(img), 32, 32, P(img), 32, 32, None) == -1
+    assert lib.dicegpu_correlate(P(pts), 1, 21, P(img), 32, 32, P(img2), 33, 32, None, 0) == -1
+    assert lib.dicegpu_correlate(P(pts), 1, 0, P(img), 32, 32, P(img), 32, 32, None, 0) == -1
+    assert lib.dicegpu_correlate(P(pts), 0, 21, P(img), 32, 32, P(img), 32, 32, None, 0) == -1
 
 
 def test_version_string():

@@ -268,22 +268,94 @@ def test_failure_flags_match():
         assert np.array_equal(g[:, abi.F_SIGMA] == -1, o[:, abi.F_SIGMA] == -1)
 
 
+def _api_oracle_frame(p, ref, de, rows, pts, first):
+    """One dice_correlate call on the oracle: the nine stride-9 columns
+    written over the kept rows, one frame, the results read back as floats."""
+    cols = [abi.F_COORD_X, abi.F_COORD_Y, abi.F_DISP_X, abi.F_DISP_Y, abi.F_ROT_Z, abi.F_SIGMA, abi.F_GAMMA,
+            abi.F_BETA, abi.F_STATUS]
+    rows[:, cols] = pts.astype(np.float64)
+    O.execute_frame(p, ref, de, rows, first_frame=first, nthreads=4)
+    out = pts.copy()
+    out[:, 2:] = rows[:, cols[2:]].astype(np.float32)
+    return out
+
+
 def test_correlate_stride9_api(gold):
     """DICe_TestAPI: integer shifts 0..5 of a 100x100 synthetic speckle image
-    through the stride-9 dice_correlate interface (tracking defaults)."""
+    through the stride-9 dice_correlate interface (tracking defaults), six
+    calls on the one context the library keeps (the reference's static
+    Schema): every call's results equal the oracle run as a six-frame
+    sequence, and the shifts are recovered."""
     _require_gpu()
+    from dice_b200.schema import correlate_reset
+    correlate_reset()
     ref = gold["def_synthetic_0"].astype(np.float32)
     pts = np.zeros((4, 9), np.float32)
     pts[:, 0] = [47, 51, 51, 47]
     pts[:, 1] = [47, 47, 51, 51]
-    for k in range(6):
-        de = gold["def_synthetic_%d" % k].astype(np.float32)
-        assert correlate(pts, 21, ref, de) == 0
-        assert np.all(np.abs(pts[:, 2] - k) < 1e-4), pts
-        assert np.all(np.abs(pts[:, 3] - k) < 1e-4), pts
-        assert np.all(np.abs(pts[:, 4]) < 1e-4)
-        assert np.all(pts[:, 6] < 1e-4)
-        assert np.all(pts[:, 8] == 1)
+    p = abi.tracking_default_params(subset_size=21, use_def_gradients=1)
+    rows = np.zeros((4, abi.FIELD_STRIDE))
+    want = pts.copy()
+    try:
+        for k in range(6):
+            de = gold["def_synthetic_%d" % k].astype(np.float32)
+            want = _api_oracle_frame(p, ref, de, rows, want, k == 0)
+            assert correlate(pts, 21, ref, de) == 0
+            assert np.array_equal(pts, want), (k, pts, want)
+            assert np.all(np.abs(pts[:, 2] - k) < 1e-4), pts
+            assert np.all(np.abs(pts[:, 3] - k) < 1e-4), pts
+            assert np.all(np.abs(pts[:, 4]) < 1e-4)
+            assert np.all(pts[:, 6] < 1e-4)
+            assert np.all(pts[:, 8] == 1)
+    finally:
+        correlate_reset()
+
+
+def test_correlate_keeps_its_context_until_reset(gold):
+    """What the kept context fixes: later calls ignore the reference image and
+    the subset size, reject another subset count, and read new parameters
+    only with update_params; after dicegpu_correlate_reset the next call
+    starts a new sequence."""
+    _require_gpu()
+    from dice_b200.schema import correlate_reset
+    correlate_reset()
+    ref = gold["def_synthetic_0"].astype(np.float32)
+    d1 = gold["def_synthetic_1"].astype(np.float32)
+    d2 = gold["def_synthetic_2"].astype(np.float32)
+    start = np.zeros((4, 9), np.float32)
+    start[:, 0] = [47, 51, 51, 47]
+    start[:, 1] = [47, 47, 51, 51]
+    p = abi.tracking_default_params(subset_size=21, use_def_gradients=1)
+    try:
+        pts = start.copy()
+        assert correlate(pts, 21, ref, d1) == 0
+        # another reference image and subset size are not read again
+        rows = np.zeros((4, abi.FIELD_STRIDE))
+        want = _api_oracle_frame(p, ref, d1, rows, start.copy(), True)
+        want = _api_oracle_frame(p, ref, d2, rows, want, False)
+        assert correlate(pts, 41, d1, d2) == 0
+        assert np.array_equal(pts, want)
+        # another number of subsets is rejected and leaves the context alone
+        assert correlate(pts[:3].copy(), 21, ref, d2) == abi.ERR_ARG
+        # parameters change only with update_params: without rotation theta
+        # stays at its guess
+        p_norot = abi.tracking_default_params(enable_rotation=0)
+        guess = pts.copy()
+        guess[:, 4] = 0.01
+        q = guess.copy()
+        assert correlate(q, 21, ref, d2, params=p_norot) == 0
+        assert np.all(q[:, 4] != np.float32(0.01))
+        q = guess.copy()
+        assert correlate(q, 21, ref, d2, params=p_norot, update_params=True) == 0
+        assert np.all(q[:, 4] == np.float32(0.01))
+        # a reset starts a new sequence at the first frame, as a fresh process
+        correlate_reset()
+        pts = start.copy()
+        assert correlate(pts, 21, ref, d1) == 0
+        want = _api_oracle_frame(p, ref, d1, np.zeros((4, abi.FIELD_STRIDE)), start.copy(), True)
+        assert np.array_equal(pts, want)
+    finally:
+        correlate_reset()
 
 
 def test_gamma_entry_matches_oracle():

@@ -50,7 +50,25 @@ def test_noalloc_gradients_match_allocating_entry(method):
         assert np.array_equal(gy, ref_gy)
 
 
+def test_noalloc_finite_difference_takes_any_size():
+    """The finite-difference method uses no scratch planes, so images larger
+    than the 5-point method's cap are computed, equal to the allocating
+    entry point's."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    lib = abi.load_library()
+    rng = np.random.default_rng(12)
+    h, w = 1100, 1031
+    assert h * w > MAX_PIXELS
+    img = torch.from_numpy((rng.random((h, w)) * 255).astype(np.float32)).cuda()
+    ref_gx, ref_gy = _gradients(lib.dicegpu_image_gradients, img, abi.FINITE_DIFFERENCE)
+    gx, gy = _gradients(lib.dicegpu_image_gradients_noalloc, img, abi.FINITE_DIFFERENCE)
+    assert np.array_equal(gx, ref_gx)
+    assert np.array_equal(gy, ref_gy)
+
+
 def test_noalloc_rejects_images_beyond_its_scratch():
+    """The 5-point method's cap: one row over 1024 x 1024 is rejected."""
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     lib = abi.load_library()
