@@ -106,3 +106,29 @@ def test_sigma_matches_oracle(defgrad):
     assert np.all(sg > 0)
     assert np.array_equal(sg, osg)
     assert np.array_equal(no, ono)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("optimization", [abi.GRADIENT_BASED, abi.SIMPLEX])
+def test_beta_output_matches_oracle(optimization):
+    """Objective::beta (DICe_Objective.cpp:78-148), written to the BETA
+    column when params.output_beta is set: on every converged subset of a
+    frame, equal to the oracle's, and present (non-zero somewhere)."""
+    _gpu()
+    from dice_b200.schema import Schema
+    ref, deff, p, f = _case()
+    p.output_beta = 1
+    p.optimization = optimization
+    with Schema(p) as s:
+        s.set_ref_image(ref)
+        s.set_fields(f)
+        s.set_def_image(deff)
+        s.execute_correlation()
+        g = s.fields()
+    o = f.copy()
+    O.execute_frame(p, ref, deff, o, first_frame=True, nthreads=4)
+    assert_rows_equal(g, o)
+    ok = o[:, abi.F_STATUS] < 2
+    assert ok.mean() > 0.9
+    assert np.all(np.isfinite(g[ok, abi.F_BETA]))
+    assert np.any(g[ok, abi.F_BETA] != 0)
