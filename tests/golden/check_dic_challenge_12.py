@@ -81,4 +81,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/check_dic_challenge_12.py <path to the DICe source tree>")
+    sys.exit(main(sys.argv[1]))
