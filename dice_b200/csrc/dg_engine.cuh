@@ -212,7 +212,8 @@ struct Engine {
 
   // Objective::gamma (DICe_Objective.cpp:58-76): initialise, Subset::gamma,
   // optionally divided by the number of active pixels (in double).
-  __device__ float eval_gamma(const SubsetRef& sb, const float* slots, bool normalize, float* def_sum2 = nullptr) {
+  __device__ float eval_gamma(const SubsetRef& sb, const float* slots, bool normalize,
+                                         float* def_sum2 = nullptr) {
     pass<PK_GAMMA>(sb, slots);
     float g = gamma_exact(sb, def_sum2);
     if (normalize && sb.nact > 0) g = (float)((double)g / (double)sb.nact);
@@ -353,7 +354,7 @@ struct Engine {
   // go to Ctl: status (0, or HESSIAN_SINGULAR), cond, conv, slots.
   // --------------------------------------------------------------------------
   // hw0, hnw: the warps whose Hessian sums hold the subset's pixels (h_sweep)
-  __device__ __noinline__ void solve_step(const Slots cur, int hw0, int hnw) {
+  __device__ __forceinline__ void solve_step(const Slots cur, int hw0, int hnw) {
     const DevParams& P = A.P;
     const int N = P.N;
     Ctl& c = ctl();
@@ -493,7 +494,12 @@ struct Engine {
         du = du + P.momentum * c.upd_old[lane];
         c.upd_old[lane] = du;
       }
-      const float old = cur.s[P.slot[lane]];
+      // the lane's parameter slot, selected without indexing the register array
+      const int sl = P.slot[lane];
+      float old = 0.0f;
+#pragma unroll
+      for (int i = 0; i < 12; ++i)
+        if (i == sl) old = cur.s[i];
       nw = old + du;
       // test_for_convergence: affine u, v, theta (DICe_LocalShapeFunction.cpp:433-459),
       // quadratic every parameter (:91-102)
@@ -560,7 +566,8 @@ struct Engine {
       if (fresh) meanF = sb.nact ? __fdiv_rn(c.fres[1], (float)sb.nact) : 0.0f;
       const float meanG = n ? __fdiv_rn(c.fres[0], (float)n) : 0.0f;
       DG_PT(t_q);
-      q_sweep<SHAPE, DEFGRAD>(inb, k, meanG, meanF);
+      q_sweep<SHAPE, DEFGRAD>(inb, k, meanG, meanF, tid, T);
+      __syncthreads();
       DG_PACC(6, t_q);
       Slots cur;
 #pragma unroll
@@ -611,7 +618,10 @@ struct Engine {
     }
   }
 
-  __device__ int simplex(const SubsetRef& sb, float* slots, int& num_iterations, float* lastp) {
+  // Out of line, as beta is: these fallback paths inlined into the
+  // correlation loop enlarge the code the Gauss-Newton iterations run
+  // through (instruction-cache misses) and slow every subset.
+  __device__ __noinline__ int simplex(const SubsetRef& sb, float* slots, int& num_iterations, float* lastp) {
     const DevParams& P = A.P;
     const int nd = P.N;
     const int mpts = nd + 1;
@@ -960,9 +970,12 @@ struct Engine {
         f[DICEGPU_F_ROT_Z] = t;
       }
     } else if (tid == 0) {
+      const unsigned em = enabled_mask();
       f[DICEGPU_F_DISP_X] = slots[0];
       f[DICEGPU_F_DISP_Y] = slots[1];
-      for (int kx = 2; kx < A.P.N; ++kx) f[DICEGPU_F_DISP_X + A.P.slot[kx]] = slots[A.P.slot[kx]];
+#pragma unroll
+      for (int s = 2; s < 6; ++s)
+        if ((em >> s) & 1u) f[DICEGPU_F_DISP_X + s] = slots[s];
     }
   }
 
@@ -1016,7 +1029,7 @@ struct Engine {
   // Objective::beta (DICe_Objective.cpp:78-148): the finite-difference slope
   // of the unnormalised gamma in u, v (and theta with rotation), ending with
   // the subset re-initialised at the solution.
-  __device__ float beta(const SubsetRef& sb, const float* slots) {
+  __device__ __noinline__ float beta(const SubsetRef& sb, const float* slots) {
     const DevParams& P = A.P;
     MapConst k;
     make_mapconst<SHAPE>(slots, false, (float)sb.cx, (float)sb.cy, k);
@@ -1267,12 +1280,12 @@ struct Engine {
         f[DICEGPU_F_DISP_Y] = nv;
         f[DICEGPU_F_ROT_Z] = nt;
       } else {
+        const unsigned em = enabled_mask();
         f[DICEGPU_F_DISP_X] = slots[0];
         f[DICEGPU_F_DISP_Y] = slots[1];
-        for (int kx = 2; kx < P.N; ++kx) {
-          const int s = P.slot[kx];
-          f[DICEGPU_F_DISP_X + s] = slots[s];
-        }
+#pragma unroll
+        for (int s = 2; s < 6; ++s)
+          if ((em >> s) & 1u) f[DICEGPU_F_DISP_X + s] = slots[s];
       }
       f[DICEGPU_F_SIGMA] = sg;
       f[DICEGPU_F_MATCH] = 0.0;

@@ -2,10 +2,9 @@
 //
 // frame_kernel<shape, interp, defgrad, mask> runs Schema::execute_correlation
 // (or one Objective entry point, by mode) for every subset of a launch: one
-// CTA per subset from interleaved per-CTA work queues.  The unmasked
-// instantiations are compiled with the rest of the library (dicegpu.cu), the
-// masked ones in frame_masked.cu, so that both compile in parallel and the
-// unmasked kernels are exactly what they are without masks.
+// CTA per subset from interleaved per-CTA work queues.  The instantiations
+// live in frame_inst.cu (one unit per shape function, interpolation and
+// mask); the unmasked kernels are exactly what they are without masks.
 #pragma once
 
 #include "dg_engine.cuh"
@@ -77,30 +76,33 @@ __global__ void __launch_bounds__(DG_MAX_THREADS, DG_MIN_BLOCKS) frame_kernel(co
 
 typedef void (*FrameKernelFn)(FrameArgs);
 
-// The frame kernel of a configuration; MASK selects the instantiation whose
-// passes test obstruction bitmaps and blocked polygons (only subsets with masks pay
-// for it, and only contexts with masks launch it).
-template <int SHAPE, bool MASK>
-static FrameKernelFn pick_kernel(int interp, bool defgrad) {
-#ifdef DG_ONLY_BENCH_KERNEL
-  // reduced build (fast compiles while tuning): only the affine / Keys-4 /
-  // deformed-gradient kernel; other configurations report UNSUPPORTED
-  if (SHAPE == DICEGPU_AFFINE_SF && interp == DICEGPU_KEYS_FOURTH && defgrad)
-    return frame_kernel<DICEGPU_AFFINE_SF, DICEGPU_KEYS_FOURTH, true, MASK>;
-  return nullptr;
-#else
-  if (defgrad) {
-    if (interp == DICEGPU_KEYS_FOURTH) return frame_kernel<SHAPE, DICEGPU_KEYS_FOURTH, true, MASK>;
-    if (interp == DICEGPU_BICUBIC) return frame_kernel<SHAPE, DICEGPU_BICUBIC, true, MASK>;
-    return frame_kernel<SHAPE, DICEGPU_BILINEAR, true, MASK>;
-  }
-  if (interp == DICEGPU_KEYS_FOURTH) return frame_kernel<SHAPE, DICEGPU_KEYS_FOURTH, false, MASK>;
-  if (interp == DICEGPU_BICUBIC) return frame_kernel<SHAPE, DICEGPU_BICUBIC, false, MASK>;
-  return frame_kernel<SHAPE, DICEGPU_BILINEAR, false, MASK>;
-#endif
-}
+// The frame kernels are instantiated in frame_inst.cu, compiled once per
+// (shape function, interpolation, mask) so that the units build in
+// parallel: frame_fn_s<shape>_i<interp>_m<mask>(defgrad) returns the kernel
+// with or without deformed-image gradients.  MASK selects the instantiation
+// whose passes test obstruction bitmaps and blocked polygons (only contexts
+// with masks launch it).
+#define DG_FRAME_FN_NAME(S, I, M) frame_fn_s##S##_i##I##_m##M
+#define DG_DECLARE_FRAME_FN(S, I, M) FrameKernelFn DG_FRAME_FN_NAME(S, I, M)(bool defgrad);
+DG_DECLARE_FRAME_FN(0, 0, 0) DG_DECLARE_FRAME_FN(0, 1, 0) DG_DECLARE_FRAME_FN(0, 2, 0)
+DG_DECLARE_FRAME_FN(1, 0, 0) DG_DECLARE_FRAME_FN(1, 1, 0) DG_DECLARE_FRAME_FN(1, 2, 0)
+DG_DECLARE_FRAME_FN(0, 0, 1) DG_DECLARE_FRAME_FN(0, 1, 1) DG_DECLARE_FRAME_FN(0, 2, 1)
+DG_DECLARE_FRAME_FN(1, 0, 1) DG_DECLARE_FRAME_FN(1, 1, 1) DG_DECLARE_FRAME_FN(1, 2, 1)
 
-// the masked instantiations live in their own translation unit (frame_masked.cu)
-FrameKernelFn pick_masked_kernel(int shape, int interp, bool defgrad);
+// The frame kernel of a configuration (nullptr for one this build leaves
+// out: a unit compiled with DG_ONLY_BENCH_KERNEL returns only the affine /
+// Keys-4 / deformed-gradient kernel).
+inline FrameKernelFn pick_frame_kernel(int shape, int interp, bool defgrad, bool mask) {
+  typedef FrameKernelFn (*Pick)(bool);
+  static const Pick table[2][3][2] = {
+      {{DG_FRAME_FN_NAME(0, 0, 0), DG_FRAME_FN_NAME(0, 0, 1)},
+       {DG_FRAME_FN_NAME(0, 1, 0), DG_FRAME_FN_NAME(0, 1, 1)},
+       {DG_FRAME_FN_NAME(0, 2, 0), DG_FRAME_FN_NAME(0, 2, 1)}},
+      {{DG_FRAME_FN_NAME(1, 0, 0), DG_FRAME_FN_NAME(1, 0, 1)},
+       {DG_FRAME_FN_NAME(1, 1, 0), DG_FRAME_FN_NAME(1, 1, 1)},
+       {DG_FRAME_FN_NAME(1, 2, 0), DG_FRAME_FN_NAME(1, 2, 1)}}};
+  if (shape < 0 || shape > 1 || interp < 0 || interp > 2) return nullptr;
+  return table[shape][interp][mask ? 1 : 0](defgrad);
+}
 
 }  // namespace dg

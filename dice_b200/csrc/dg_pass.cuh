@@ -30,19 +30,22 @@
 
 #include "dg_device.cuh"
 
+
 namespace dg {
 
 // Section timers of a profiling build (-DDG_PROFILE): cycles per section
 // summed over all CTAs (thread 0's clock).  Compiled out otherwise.
 #ifdef DG_PROFILE
-static __device__ unsigned long long g_prof[8];   // per translation unit
+static __device__ unsigned long long g_prof[16];   // per translation unit
 #define DG_PT(var) const long long var = clock64()
-#define DG_PACC(i, t0)                                                                    \
-  do {                                                                                    \
-    if (threadIdx.x == 0) atomicAdd(&g_prof[i], (unsigned long long)(clock64() - (t0))); \
+#define DG_PACC_T(i, t0, thr)                                                               \
+  do {                                                                                      \
+    if (threadIdx.x == (thr)) atomicAdd(&g_prof[i], (unsigned long long)(clock64() - (t0))); \
   } while (0)
+#define DG_PACC(i, t0) DG_PACC_T(i, t0, 0)
 #else
 #define DG_PT(var)
+#define DG_PACC_T(i, t0, thr)
 #define DG_PACC(i, t0)
 #endif
 
@@ -109,11 +112,18 @@ __host__ __device__ inline int pix_cap(int npix_max) { return (npix_max + 31) & 
 __host__ __device__ inline int pix_stride(int cap) { return cap + 4; }
 // stored per-pixel rows besides F and G: the affine residual vector r_0..r_5,
 // or the quadratic subset's gradients (its residuals are products of them)
+// Stored rows of an affine subset (DG_AFF_ROWS): 6, its residual vector;
+// 4, the gradients and the stretched offsets Dx, Dy; 2, the gradients only
+// (the sweeps form the residuals from them).
+#ifndef DG_AFF_ROWS
+#define DG_AFF_ROWS 6
+#endif
 template <int SHAPE>
 struct PixRows {
-  static constexpr int NR = SHAPE == DICEGPU_QUADRATIC_SF ? 2 : 6;
+  static constexpr int NR = SHAPE == DICEGPU_QUADRATIC_SF ? 2 : DG_AFF_ROWS;
+  // the sweeps read the residual vector straight from the rows
+  static constexpr bool RESID = SHAPE != DICEGPU_QUADRATIC_SF && DG_AFF_ROWS == 6;
 };
-
 template <int SHAPE>
 struct SmemPlan {
   static __host__ __device__ size_t wout(int) { return a16(sizeof(Ctl)); }
@@ -387,7 +397,7 @@ enum { PK_GN = 0, PK_STATE = 1, PK_GAMMA = 2 };
 // One pass (Subset::initialize on the deformed image).  Ends with the live
 // count and box in Ctl (all threads may read them after the final barrier).
 template <int SHAPE, int INTERP, bool DEFGRAD, int KIND, bool MASKED>
-__device__ __noinline__ void cta_pass(const PassInT<MASKED> in, const MapConst k) {
+__device__ __forceinline__ void cta_pass(const PassInT<MASKED> in, const MapConst k) {
   using L = Layout<SHAPE>;
   constexpr bool GRADS = KIND != PK_GAMMA;
   constexpr bool AFF = SHAPE != DICEGPU_QUADRATIC_SF;
@@ -453,7 +463,7 @@ __device__ __noinline__ void cta_pass(const PassInT<MASKED> in, const MapConst k
     A.F[p] = F;
     A.G[p] = live ? G : 0.0f;
     A.L[p] = (uint8_t)((live ? 1 : 0) | (active ? 2 : 0));
-    if (KIND == PK_GN && AFF) {
+    if (KIND == PK_GN && PixRows<SHAPE>::RESID) {
       // the residual vector of Objective_ZNSSD::computeUpdateFast (:538)
       float r[L::VW];
 #pragma unroll
@@ -464,6 +474,10 @@ __device__ __noinline__ void cta_pass(const PassInT<MASKED> in, const MapConst k
     } else if (GRADS) {
       A.R(0)[p] = gx;
       A.R(1)[p] = gy;
+      if (KIND == PK_GN && AFF && PixRows<SHAPE>::NR == 4) {
+        A.R(2)[p] = Dx;
+        A.R(3)[p] = Dy;
+      }
     }
   }
   // per-warp results
@@ -490,12 +504,25 @@ __device__ __noinline__ void cta_pass(const PassInT<MASKED> in, const MapConst k
   __syncthreads();
 }
 
-// The residual vector of a stored pixel of a quadratic subset (from its
-// stored gradients; Quadratic_Shape_Function::residuals, :580-614).
-__device__ __forceinline__ void quad_residuals(const PassIn& in, const PixArrays& A, const MapConst& k, int p, int x,
-                                               int y, bool use_ref_grads, float* r) {
+// The residual vector of a stored pixel formed from its stored gradients
+// (Quadratic_Shape_Function::residuals, :580-614; the affine one, :350-396,
+// with the stretched offsets stored or formed again as the pass formed them).
+template <int SHAPE>
+__device__ __forceinline__ void stored_residuals(const PassIn& in, const PixArrays& A, const MapConst& k, int p, int x,
+                                                 int y, bool use_ref_grads, float* r) {
   const float dxf = __fsub_rn((float)x, (float)in.cx), dyf = __fsub_rn((float)y, (float)in.cy);
-  residuals_D<DICEGPU_QUADRATIC_SF>(k, dxf, dyf, dxf, dyf, A.R(0)[p], A.R(1)[p], use_ref_grads, r);
+  if (SHAPE == DICEGPU_QUADRATIC_SF) {
+    residuals_D<SHAPE>(k, dxf, dyf, dxf, dyf, A.R(0)[p], A.R(1)[p], use_ref_grads, r);
+  } else {
+    float Dx, Dy;
+    if (PixRows<SHAPE>::NR >= 4) {
+      Dx = A.R(2)[p];
+      Dy = A.R(3)[p];
+    } else {
+      affine_D(k, dxf, dyf, Dx, Dy);
+    }
+    residuals_D<SHAPE>(k, dxf, dyf, Dx, Dy, A.R(0)[p], A.R(1)[p], use_ref_grads, r);
+  }
 }
 
 // The Hessian sweep over the stored pixels, run by warps w0 .. w0 + nw - 1
@@ -507,26 +534,28 @@ __device__ __forceinline__ void quad_residuals(const PassIn& in, const PixArrays
 // fragments); quadratic residuals are formed from the stored gradients and
 // staged.  Warps outside the range return at once.  No barrier.
 template <int SHAPE, bool DEFGRAD>
-__device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, int nw) {
+__device__ __forceinline__ void h_sweep(const PassIn in, const MapConst k, int w0, int nw) {
   using L = Layout<SHAPE>;
   constexpr bool AFF = SHAPE != DICEGPU_QUADRATIC_SF;
+  constexpr bool ROWS = PixRows<SHAPE>::RESID;   // residual vectors stored per pixel
   constexpr int NSET = 2;   // independent mma accumulator sets
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < w0 || warp >= w0 + nw) return;
   const bool use_ref_grads = !DEFGRAD;
   const PixArrays A = pix_arrays_at<SHAPE>(in.pix, in.cap);
   double c[NSET][3][2];
-  float e[L::NP];
 #pragma unroll
   for (int s2 = 0; s2 < NSET; ++s2)
 #pragma unroll
     for (int b = 0; b < 3; ++b) { c[s2][b][0] = 0.0; c[s2][b][1] = 0.0; }
+  float e[L::NP];
 #pragma unroll
   for (int i = 0; i < L::NP; ++i) e[i] = 0.0f;
   const int nblk = (in.npix + 31) >> 5;
   const int kk = lane & 3, ii = lane >> 2;
-  // affine: the mma fragment's row (residual index ii, zero beyond the six)
-  const float* frag = A.R(ii < PixRows<SHAPE>::NR ? ii : 0) + kk;
+  // stored residual rows: the mma fragment's row (residual index ii, zero
+  // beyond the six)
+  const float* frag = A.R(ROWS && ii < PixRows<SHAPE>::NR ? ii : 0) + kk;
   const unsigned vbase = (unsigned)__cvta_generic_to_shared(warp_vbuf<SHAPE>());
   PixelWalk pw(in, (warp - w0) * 32 + lane, 32 * nw);
   for (int blk = warp - w0; blk < nblk; blk += nw) {
@@ -535,13 +564,13 @@ __device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, 
 #pragma unroll
     for (int i = 0; i < L::VW; ++i) v[i] = 0.0f;
     if (A.L[p] & 1) {
-      if (AFF) {
+      if (ROWS) {
 #pragma unroll
         for (int i = 0; i < L::NS; ++i) v[i] = A.R(i)[p];
       } else {
         int x, y;
         pw.xy(in, p, x, y);
-        quad_residuals(in, A, k, p, x, y, use_ref_grads, v);
+        stored_residuals<SHAPE>(in, A, k, p, x, y, use_ref_grads, v);
       }
       int idx = 0;
 #pragma unroll
@@ -552,7 +581,7 @@ __device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, 
           e[idx] = __fadd_rn(e[idx], fmaf(v[i], v[j], -pr));
         }
     }
-    if (!AFF) {
+    if (!ROWS) {
       pw.advance();
       // stage the warp's 32 pixel vectors
       const unsigned vrow = vbase + (unsigned)(lane * L::VS) * 4u;
@@ -564,18 +593,21 @@ __device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, 
 #pragma unroll
     for (int g = 0; g < 8; ++g) {
       double(&cs)[3][2] = c[g % NSET];
-      if (AFF) {
+      if (ROWS) {
         const double a0 = ii < PixRows<SHAPE>::NR ? (double)frag[blk * 32 + 4 * g] : 0.0;
         dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
       } else {
         const unsigned src = vbase + (unsigned)((4 * g + kk) * L::VS + ii) * 4u;
-        const double a0 = (double)lds_f(src), a1 = (double)lds_f(src + 32u);
+        const double a0 = (double)lds_f(src);
         dmma_8x8x4(cs[0][0], cs[0][1], a0, a0);
-        dmma_8x8x4(cs[1][0], cs[1][1], a0, a1);
-        dmma_8x8x4(cs[2][0], cs[2][1], a1, a1);
+        if (!AFF) {
+          const double a1 = (double)lds_f(src + 32u);
+          dmma_8x8x4(cs[1][0], cs[1][1], a0, a1);
+          dmma_8x8x4(cs[2][0], cs[2][1], a1, a1);
+        }
       }
     }
-    if (!AFF) __syncwarp();
+    if (!ROWS) __syncwarp();
   }
 #pragma unroll
   for (int s2 = 1; s2 < NSET; ++s2)
@@ -608,43 +640,42 @@ __device__ __noinline__ void h_sweep(const PassIn in, const MapConst k, int w0, 
 
 // The right-hand side sweep: q_i = sum over live pixels of fl(GmF * r_i) in
 // double, GmF = (G - meanG) - (F - meanF) in float (DICe_Objective.cpp:
-// 528-537), by all threads.  Per-warp sums go to WarpOut.q; ends with a
-// barrier.
+// 528-537), by nt threads of whole warps, this one the vt-th.  Per-warp sums
+// go to WarpOut.q.  No barrier.
 template <int SHAPE, bool DEFGRAD>
-__device__ __noinline__ void q_sweep(const PassIn in, const MapConst k, float meanG, float meanF) {
+__device__ __forceinline__ void q_sweep(const PassIn in, const MapConst k, float meanG, float meanF, int vt, int nt) {
   using L = Layout<SHAPE>;
-  constexpr bool AFF = SHAPE != DICEGPU_QUADRATIC_SF;
-  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31;
+  constexpr bool ROWS = PixRows<SHAPE>::RESID;
+  const int lane = threadIdx.x & 31;
   const bool use_ref_grads = !DEFGRAD;
   const PixArrays A = pix_arrays_at<SHAPE>(in.pix, in.cap);
   double q[L::NS];
 #pragma unroll
   for (int i = 0; i < L::NS; ++i) q[i] = 0.0;
-  PixelWalk pw(in, tid, T);
-  for (int p = tid; p < in.npix; p += T) {
+  PixelWalk pw(in, vt, nt);
+  for (int p = vt; p < in.npix; p += nt) {
     if (A.L[p] & 1) {
       const float GmF = __fsub_rn(__fsub_rn(A.G[p], meanG), __fsub_rn(A.F[p], meanF));
       float r[L::VW];
-      if (AFF) {
+      if (ROWS) {
 #pragma unroll
         for (int i = 0; i < L::NS; ++i) r[i] = A.R(i)[p];
       } else {
         int x, y;
         pw.xy(in, p, x, y);
-        quad_residuals(in, A, k, p, x, y, use_ref_grads, r);
+        stored_residuals<SHAPE>(in, A, k, p, x, y, use_ref_grads, r);
       }
 #pragma unroll
       for (int i = 0; i < L::NS; ++i) q[i] = __dadd_rn(q[i], (double)__fmul_rn(GmF, r[i]));
     }
-    if (!AFF) pw.advance();
+    if (!ROWS) pw.advance();
   }
-  WarpOut<SHAPE>& wo = wouts<SHAPE>()[tid >> 5];
+  WarpOut<SHAPE>& wo = wouts<SHAPE>()[threadIdx.x >> 5];
 #pragma unroll
   for (int i = 0; i < L::NS; ++i) {
     const double sm = warp_sum(q[i]);
     if (lane == 0) wo.q[i] = sm;
   }
-  __syncthreads();
 }
 
 }  // namespace dg

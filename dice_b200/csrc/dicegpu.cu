@@ -4,8 +4,8 @@
 //   gradient_kernel   Image_::compute_gradients (finite difference, optional
 //                     5x5 smoothing), DICe_Image.cpp:1015-1093
 //   frame_kernel      persistent work-stealing correlation of every subset:
-//                     one warp per subset (dg_frame.cuh; masked
-//                     instantiations in frame_masked.cu)
+//                     one CTA per subset (dg_frame.cuh; instantiated in
+//                     frame_inst.cu)
 //   interp_kernel     Image_::interpolate_*_all at arbitrary points
 // The C ABI (include/dicegpu.h) owns device memory and launches on the
 // caller's stream; it never throws and never falls back to the CPU.
@@ -1412,9 +1412,7 @@ static void frame_smem_bytes(const dicegpu_ctx* c, int warps, size_t* fixed, siz
 
 static FrameKernelFn frame_fn(const dicegpu_ctx* c) {
   const bool dg = c->params.use_def_gradients != 0;
-  if (c->use_masks) return pick_masked_kernel(c->dp.shape, c->dp.interp, dg);
-  return c->dp.shape == DICEGPU_QUADRATIC_SF ? pick_kernel<DICEGPU_QUADRATIC_SF, false>(c->dp.interp, dg)
-                                             : pick_kernel<DICEGPU_AFFINE_SF, false>(c->dp.interp, dg);
+  return pick_frame_kernel(c->dp.shape, c->dp.interp, dg, c->use_masks);
 }
 
 static void fill_args(dicegpu_ctx* c, FrameArgs& a, int mode) {
@@ -2345,9 +2343,9 @@ extern "C" int dicegpu_correlate_reset(void) {
 
 #ifdef DG_PROFILE
 // profiling builds only: read and clear the section timers
-extern "C" int dicegpu_prof_read(unsigned long long* out8) {
-  if (cudaMemcpyFromSymbol(out8, g_prof, 8 * sizeof(unsigned long long)) != cudaSuccess) return DICEGPU_ERR_CUDA;
-  unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+extern "C" int dicegpu_prof_read(unsigned long long* out16) {
+  if (cudaMemcpyFromSymbol(out16, g_prof, 16 * sizeof(unsigned long long)) != cudaSuccess) return DICEGPU_ERR_CUDA;
+  unsigned long long z[16] = {};
   if (cudaMemcpyToSymbol(g_prof, z, sizeof(z)) != cudaSuccess) return DICEGPU_ERR_CUDA;
   return DICEGPU_OK;
 }
