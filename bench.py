@@ -398,30 +398,35 @@ def run_crack(args):
         ids = np.nonzero(np.abs(cy - size / 2.0) < half)[0]
         ref_h = ref.cpu().numpy()
         fdev = torch.empty((n, abi.FIELD_STRIDE), dtype=torch.float64, device=dev)
-        idt = torch.from_numpy(ids).to(dev)
-        s.load_fields(f0_dev)
         cores = os.cpu_count() or 1
         mx = p.max_solver_iterations_fast
         gpu_vs, var_vs = RowComparison(mx), RowComparison(mx)
-        fo = syn.init_fields(cx[ids], cy[ids])
-        fv = fo.copy()
-        failed = []
+        failed = [0] * nf
         dt = 0.0
-        # frame by frame (the band's rows of one frame at a time in host memory)
-        for k in range(nf):
-            s.set_def_image(frames[k])
-            s.execute_correlation()
-            s.store_fields(fdev)
-            g = fdev.index_select(0, idt).cpu().numpy()
-            fr_h = frames[k].cpu().numpy()
-            t0 = time.perf_counter()
-            O.execute_frame(p, ref_h, fr_h, fo, first_frame=(k == 0), nthreads=cores)
-            dt += time.perf_counter() - t0
-            with O.use_library("libdiceoracle_meanfp64.so"):
-                O.execute_frame(p, ref_h, fr_h, fv, first_frame=(k == 0), nthreads=cores)
-            gpu_vs.add(g, fo)
-            var_vs.add(fv, fo)
-            failed.append(int(np.sum(fo[:, abi.F_STATUS] >= 2)))
+        # the band in chunks of subsets (bounded host memory), each chunk
+        # through the whole sequence on the GPU, the oracle and the variant
+        for c0 in range(0, len(ids), args.flags_chunk):
+            cid = ids[c0:c0 + args.flags_chunk]
+            idt = torch.from_numpy(cid).to(dev)
+            s.load_fields(f0_dev)
+            fo = syn.init_fields(cx[cid], cy[cid])
+            fv = fo.copy()
+            for k in range(nf):
+                s.set_def_image(frames[k])
+                s.execute_correlation()
+                s.store_fields(fdev)
+                g = fdev.index_select(0, idt).cpu().numpy()
+                fr_h = frames[k].cpu().numpy()
+                t0 = time.perf_counter()
+                O.execute_frame(p, ref_h, fr_h, fo, first_frame=(k == 0), nthreads=cores)
+                dt += time.perf_counter() - t0
+                with O.use_library("libdiceoracle_meanfp64.so"):
+                    O.execute_frame(p, ref_h, fr_h, fv, first_frame=(k == 0), nthreads=cores)
+                del fr_h
+                gpu_vs.add(g, fo)
+                var_vs.add(fv, fo)
+                failed[k] += int(np.sum(fo[:, abi.F_STATUS] >= 2))
+            del g, fo, fv
         flags = dict(gpu_vs.result(), subsets=int(len(ids)), frames=nf,
                      columns=RESULT_COLUMNS_TEXT, bar="every column equal to the oracle's, bit for bit",
                      oracle_failed_per_frame=failed,
@@ -958,6 +963,8 @@ def main():
     ap.add_argument("--crack-size", type=int, default=8192)
     ap.add_argument("--flags-band", type=int, default=4096,
                     help="crack workload: height in px of the band of rows checked against the oracle")
+    ap.add_argument("--flags-chunk", type=int, default=400000,
+                    help="crack workload: subsets of the band per pass through the sequence")
     ap.add_argument("--fit-iters", type=int, default=2000)
     ap.add_argument("--profile-timed", action="store_true",
                     help="sequence workload: bracket the timed steps with cudaProfilerStart/Stop "
