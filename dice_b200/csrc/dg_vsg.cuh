@@ -177,3 +177,65 @@ __global__ void __launch_bounds__(256) vsg_kernel(VsgArgs a) {
     if (!ok) a.fields[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_MATCH] = -1.0;
   }
 }
+
+// k nearest neighbourhoods (a negative window: Post_Processor::
+// initialize_neighborhood's knnSearch, DICe_PostProcessor.cpp:185-205): the
+// k nearest subsets, valid or not, listed per subset in ascending float
+// squared distance (ties by index) by the host.  One thread per subset
+// forms the same sums as the oracle, neighbour by neighbour in list order,
+// each product and sum rounded on its own; the nearest (the subset itself)
+// must be valid, as the reference tests neighbour 0.
+struct VsgKnnArgs {
+  double* fields;
+  int n, k;
+  const int32_t* nbr;        // n x k neighbour indices
+  double* out;               // n x DICEGPU_VSG_STRIDE
+};
+
+__global__ void __launch_bounds__(256) vsg_knn_kernel(VsgKnnArgs a) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const int32_t* nb = a.nbr + (size_t)i * a.k;
+    const double* fi = a.fields + (size_t)i * DICEGPU_FIELD_STRIDE;
+    const float xi = (float)fi[DICEGPU_F_COORD_X], yi = (float)fi[DICEGPU_F_COORD_Y];
+    int valid = 0;
+    for (int q = 0; q < a.k; ++q) valid += (float)a.fields[(size_t)nb[q] * DICEGPU_FIELD_STRIDE + DICEGPU_F_SIGMA] >= 0.0f;
+    bool ok = valid >= 3 && (float)a.fields[(size_t)nb[0] * DICEGPU_FIELD_STRIDE + DICEGPU_F_SIGMA] >= 0.0f;
+    double r[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (ok) {
+      double XtX[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Xu[3] = {0, 0, 0}, Xv[3] = {0, 0, 0};
+      for (int q = 0; q < a.k; ++q) {
+        const double* fj = a.fields + (size_t)nb[q] * DICEGPU_FIELD_STRIDE;
+        if (!((float)fj[DICEGPU_F_SIGMA] >= 0.0f)) continue;
+        const double row[3] = {1.0, (double)__fsub_rn((float)fj[DICEGPU_F_COORD_X], xi),
+                               (double)__fsub_rn((float)fj[DICEGPU_F_COORD_Y], yi)};
+        const double u = (double)(float)fj[DICEGPU_F_DISP_X], v = (double)(float)fj[DICEGPU_F_DISP_Y];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+#pragma unroll
+          for (int b = 0; b < 3; ++b) XtX[p][b] = __dadd_rn(XtX[p][b], __dmul_rn(row[p], row[b]));
+          Xu[p] = __dadd_rn(Xu[p], __dmul_rn(row[p], u));
+          Xv[p] = __dadd_rn(Xv[p], __dmul_rn(row[p], v));
+        }
+      }
+      double inv[3][3];
+      ok = vsg_inverse3(XtX, inv);
+      if (ok) ok = !(1.0 / (vsg_norm1(XtX) * vsg_norm1(inv)) < 1.0e-12);
+      if (ok) {
+        double cu[3], cv[3];
+        for (int p = 0; p < 3; ++p) {
+          cu[p] = inv[p][0] * Xu[0] + inv[p][1] * Xu[1] + inv[p][2] * Xu[2];
+          cv[p] = inv[p][0] * Xv[0] + inv[p][1] * Xv[1] + inv[p][2] * Xv[2];
+        }
+        const double dudx = cu[1], dudy = cu[2], dvdx = cv[1], dvdy = cv[2];
+        r[0] = (float)(0.5 * (2.0 * dudx + dudx * dudx + dvdx * dvdx));
+        r[1] = (float)(0.5 * (2.0 * dvdy + dudy * dudy + dvdy * dvdy));
+        r[2] = (float)(0.5 * (dudy + dvdx + dudx * dudy + dvdx * dvdy));
+        r[3] = (float)dudx; r[4] = (float)dudy; r[5] = (float)dvdx; r[6] = (float)dvdy;
+      }
+    }
+    double* o = a.out + (size_t)i * DICEGPU_VSG_STRIDE;
+    for (int q = 0; q < 7; ++q) o[q] = r[q];
+    o[DICEGPU_VSG_NEIGHBORS] = valid;
+    if (!ok) a.fields[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_MATCH] = -1.0;
+  }
+}

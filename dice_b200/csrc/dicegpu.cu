@@ -361,6 +361,7 @@ struct dicegpu_ctx {
   float vsg_x0 = 0.0f, vsg_y0 = 0.0f, vsg_cell = 1.0f, vsg_r2 = 0.0f;
   DevBuf<int32_t> d_vsg_cell_off, d_vsg_cell_pts, d_vsg_pos;
   DevBuf<float4> d_vsg_packed;
+  DevBuf<int32_t> d_vsg_nbr;   // k nearest neighbours per subset (negative windows)
   DevBuf<double> d_vsg;
   std::vector<double> h_vsg_coords;   // the coordinates the grid was built for
 };
@@ -540,7 +541,7 @@ extern "C" int dicegpu_destroy(dicegpu_ctx* c) {
   c->d_dv_off.release(); c->d_dvx.release(); c->d_dvy.release();
   c->d_snapshot.release();
   c->d_vsg_cell_off.release(); c->d_vsg_cell_pts.release(); c->d_vsg.release();
-  c->d_vsg_pos.release(); c->d_vsg_packed.release();
+  c->d_vsg_pos.release(); c->d_vsg_packed.release(); c->d_vsg_nbr.release();
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -1284,10 +1285,97 @@ static int build_vsg_grid(dicegpu_ctx* c, int window) {
   return DICEGPU_OK;
 }
 
+// The k nearest subsets of every subset (a negative VSG window), valid or
+// not, in ascending float squared distance (query minus point, as the
+// kd-tree's L2 adaptor forms it), ties by index.  Candidates come from a
+// uniform grid of about k / 4 subsets per cell, searched in growing squares
+// of cells until the k-th distance is below the square's inner radius, so
+// no closer point lies outside it.
+static int build_vsg_knn(dicegpu_ctx* c, int k) {
+  const int n = c->n;
+  if (k > n) return DICEGPU_ERR_ARG;
+  std::vector<double> rows((size_t)n * DICEGPU_FIELD_STRIDE);
+  CK(cudaMemcpyAsync(rows.data(), c->d_fields, rows.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<float> px(n), py(n);
+  float x0 = 0.0f, y0 = 0.0f, x1 = 0.0f, y1 = 0.0f;
+  for (int i = 0; i < n; ++i) {
+    px[i] = (float)rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_X];
+    py[i] = (float)rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_Y];
+    if (!std::isfinite(px[i]) || !std::isfinite(py[i])) return DICEGPU_ERR_ARG;
+    if (i == 0 || px[i] < x0) x0 = px[i];
+    if (i == 0 || py[i] < y0) y0 = py[i];
+    if (i == 0 || px[i] > x1) x1 = px[i];
+    if (i == 0 || py[i] > y1) y1 = py[i];
+  }
+  const double area = std::max(1.0, ((double)x1 - x0 + 1.0) * ((double)y1 - y0 + 1.0));
+  const double cell = std::max(1.0, std::sqrt(area / n * std::max(k, 4) / 4.0));
+  const int ncx = (int)std::floor((x1 - x0) / cell) + 1, ncy = (int)std::floor((y1 - y0) / cell) + 1;
+  std::vector<int32_t> off((size_t)ncx * ncy + 1, 0), pts(n), cell_of(n);
+  for (int i = 0; i < n; ++i) {
+    const int gx = std::min((int)std::floor((px[i] - x0) / cell), ncx - 1);
+    const int gy = std::min((int)std::floor((py[i] - y0) / cell), ncy - 1);
+    cell_of[i] = gy * ncx + gx;
+    ++off[cell_of[i] + 1];
+  }
+  for (size_t q = 0; q + 1 < off.size(); ++q) off[q + 1] += off[q];
+  {
+    std::vector<int32_t> fill(off.begin(), off.end() - 1);
+    for (int i = 0; i < n; ++i) pts[fill[cell_of[i]]++] = i;
+  }
+  std::vector<int32_t> nbr((size_t)n * k);
+  std::vector<std::pair<float, int32_t>> cand;
+  for (int i = 0; i < n; ++i) {
+    const int gx = cell_of[i] % ncx, gy = cell_of[i] / ncx;
+    for (int R = 1;; ++R) {
+      cand.clear();
+      for (int cy = std::max(gy - R, 0); cy <= std::min(gy + R, ncy - 1); ++cy) {
+        const int q0 = off[(size_t)cy * ncx + std::max(gx - R, 0)];
+        const int q1 = off[(size_t)cy * ncx + std::min(gx + R, ncx - 1) + 1];
+        for (int q = q0; q < q1; ++q) {
+          const int j = pts[q];
+          const float dx = px[i] - px[j], dy = py[i] - py[j];
+          cand.push_back(std::make_pair(dx * dx + dy * dy, j));
+        }
+      }
+      const bool all = gx - R <= 0 && gy - R <= 0 && gx + R >= ncx - 1 && gy + R >= ncy - 1;
+      if ((int)cand.size() < k && !all) continue;
+      std::partial_sort(cand.begin(), cand.begin() + k, cand.end());
+      // a point outside the square is at least R cells away in x or y
+      const double inner = R * cell;
+      if (all || (double)cand[k - 1].first < inner * inner * (1.0 - 1e-6)) break;
+    }
+    for (int q = 0; q < k; ++q) nbr[(size_t)i * k + q] = cand[q].second;
+  }
+  int rc;
+  if ((rc = c->d_vsg_nbr.ensure(nbr.size()))) return rc;
+  CK(cudaMemcpy(c->d_vsg_nbr.p, nbr.data(), nbr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  c->h_vsg_coords.resize(2 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    c->h_vsg_coords[2 * i] = rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_X];
+    c->h_vsg_coords[2 * i + 1] = rows[(size_t)i * DICEGPU_FIELD_STRIDE + DICEGPU_F_COORD_Y];
+  }
+  c->vsg_window = -k;
+  return DICEGPU_OK;
+}
+
 extern "C" int dicegpu_vsg_strain(dicegpu_ctx* c, int window_size, double* out, int on_device) {
   if (!c || c->n < 1 || window_size == 0) return DICEGPU_ERR_ARG;
-  if (window_size < 0) return DICEGPU_ERR_UNSUPPORTED;   // k-nearest neighbourhoods
   int rc;
+  if (window_size < 0) {
+    if (c->vsg_window != window_size && (rc = build_vsg_knn(c, -window_size))) return rc;
+    if ((rc = c->d_vsg.ensure((size_t)c->n * DICEGPU_VSG_STRIDE))) return rc;
+    VsgKnnArgs ka{c->d_fields, c->n, -window_size, c->d_vsg_nbr.p, c->d_vsg.p};
+    const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)c->n + 255) / 256, (int64_t)c->num_sms * 8);
+    vsg_knn_kernel<<<blocks, 256, 0, c->stream>>>(ka);
+    CK(cudaGetLastError());
+    c->launches += 1;
+    if (out)
+      CK(cudaMemcpyAsync(out, c->d_vsg.p, (size_t)c->n * DICEGPU_VSG_STRIDE * sizeof(double),
+                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+    if (out && !on_device) CK(cudaStreamSynchronize(c->stream));
+    return DICEGPU_OK;
+  }
   if (c->vsg_window != window_size && (rc = build_vsg_grid(c, window_size))) return rc;
   if ((rc = c->d_vsg.ensure((size_t)c->n * DICEGPU_VSG_STRIDE))) return rc;
   VsgArgs va{c->d_fields, c->n, c->d_vsg_cell_off.p, c->d_vsg_cell_pts.p, c->d_vsg_pos.p, c->d_vsg_packed.p,

@@ -185,7 +185,8 @@ class Schema:
     def vsg_strain(self, window_size):
         """VSG_Strain_Post_Processor on the current field rows: n x VSG_STRIDE
         (strain xx, yy, xy, du/dx, du/dy, dv/dx, dv/dy, valid neighbours);
-        sets MATCH = -1 where the fit fails."""
+        sets MATCH = -1 where the fit fails.  A negative window_size takes the
+        -window_size nearest subsets as the neighbourhood."""
         out = np.zeros((self.n, abi.VSG_STRIDE), np.float64)
         abi.check(self.lib.dicegpu_vsg_strain(self.ctx, int(window_size), out.ctypes.data_as(ctypes.c_void_p), 0),
                   "vsg_strain")

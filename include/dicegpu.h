@@ -366,8 +366,13 @@ int dicegpu_set_blocking(dicegpu_ctx* ctx, const int32_t* offsets, const int32_t
  * number (GECON); it is computed exactly here, which differs only for
  * nearly collinear neighbourhoods.  Writes n rows of DICEGPU_VSG_STRIDE
  * doubles to out (device memory when on_device, else host; NULL: kept on the
- * device only).  window_size < 0 (k nearest neighbours in the reference) is
- * DICEGPU_ERR_UNSUPPORTED. */
+ * device only).  window_size < 0: the -window_size nearest subsets, valid or
+ * not, form the neighbourhood (the reference's knnSearch,
+ * DICe_PostProcessor.cpp:185-205) and the nearest (the subset itself) must
+ * be valid; distances are the float squared distances, ties broken by
+ * subset index where the reference's kd-tree breaks them by its traversal
+ * order, so the two can differ only when several subsets tie at the k-th
+ * distance.  -window_size larger than the subset count is DICEGPU_ERR_ARG. */
 int dicegpu_vsg_strain(dicegpu_ctx* ctx, int window_size, double* out, int on_device);
 
 /* Copies the context's subset pixel lists to host memory: offsets[n + 1]

@@ -1857,9 +1857,15 @@ static double norm1(const double M[3][3]) {
 }
 }  // namespace
 
+// window > 0: the neighbours within window / 2 (the kd-tree radius search,
+// DICe_PostProcessor.cpp:207-231); window < 0: the -window nearest points,
+// valid or not (knnSearch, :185-205), by float squared distance, ties by
+// index (the kd-tree breaks ties by its traversal order).
 extern "C" int oracle_vsg_strain(int n, const double* fields, int window, double* out, int32_t* failed) {
-  if (n < 1 || !fields || !out || !failed || window <= 0) return DICEGPU_ERR_ARG;
-  const float rad = (float)((float)window / 2.0);
+  if (n < 1 || !fields || !out || !failed || window == 0) return DICEGPU_ERR_ARG;
+  if (window < 0 && -(long)window > n) return DICEGPU_ERR_ARG;
+  const int knn = window < 0 ? -window : 0;
+  const float rad = (float)((float)(window < 0 ? 1 : window) / 2.0);
   const float r2 = rad * rad + 1.0e-5f;
   std::vector<float> px(n), py(n), u(n), v(n), sg(n);
   for (int i = 0; i < n; ++i) {
@@ -1883,23 +1889,34 @@ extern "C" int oracle_vsg_strain(int n, const double* fields, int window, double
   auto cell_of = [&](int i) {
     return (long)std::floor((py[i] - y0) / cell) * ncx + (long)std::floor((px[i] - x0) / cell);
   };
-  for (int i = 0; i < n; ++i) cells[cell_of(i)].push_back(i);
+  if (knn == 0)
+    for (int i = 0; i < n; ++i) cells[cell_of(i)].push_back(i);
   std::vector<std::pair<float, int>> nb;
   for (int i = 0; i < n; ++i) {
     nb.clear();
-    const long gx = (long)std::floor((px[i] - x0) / cell), gy = (long)std::floor((py[i] - y0) / cell);
-    for (long cy = std::max(gy - 1, 0L); cy <= std::min(gy + 1, ncy - 1); ++cy)
-      for (long cx = std::max(gx - 1, 0L); cx <= std::min(gx + 1, ncx - 1); ++cx) {
-        const auto it = cells.find(cy * ncx + cx);
-        if (it == cells.end()) continue;
-        for (int j : it->second) {
-          const float dx = px[i] - px[j], dy = py[i] - py[j];
-          const float d2 = dx * dx + dy * dy;
-          if (d2 < r2) nb.push_back(std::make_pair(d2, j));
-        }
+    if (knn > 0) {
+      // every point, the knn smallest
+      for (int j = 0; j < n; ++j) {
+        const float dx = px[i] - px[j], dy = py[i] - py[j];
+        nb.push_back(std::make_pair(dx * dx + dy * dy, j));
       }
-    // distance order, ties by index
-    std::sort(nb.begin(), nb.end());
+      std::sort(nb.begin(), nb.end());
+      nb.resize(knn);
+    } else {
+      const long gx = (long)std::floor((px[i] - x0) / cell), gy = (long)std::floor((py[i] - y0) / cell);
+      for (long cy = std::max(gy - 1, 0L); cy <= std::min(gy + 1, ncy - 1); ++cy)
+        for (long cx = std::max(gx - 1, 0L); cx <= std::min(gx + 1, ncx - 1); ++cx) {
+          const auto it = cells.find(cy * ncx + cx);
+          if (it == cells.end()) continue;
+          for (int j : it->second) {
+            const float dx = px[i] - px[j], dy = py[i] - py[j];
+            const float d2 = dx * dx + dy * dy;
+            if (d2 < r2) nb.push_back(std::make_pair(d2, j));
+          }
+        }
+      // distance order, ties by index
+      std::sort(nb.begin(), nb.end());
+    }
     double* o = out + (long)i * 7;
     for (int k = 0; k < 7; ++k) o[k] = 0.0;
     failed[i] = 1;

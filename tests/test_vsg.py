@@ -200,3 +200,63 @@ def test_oracle_vsg_regression_files(tmp_path, variant):
         n, rep = diff_text(str(GOLD["%s_gold_text_%s" % (variant, k)]),
                            open(tmp_path / ("DICe_solution_%s.txt" % k)).read(), tol=0.05, floor=5.0e-5)
         assert n == 0, rep
+
+
+def _scattered(n, seed, fail_frac=0.05):
+    rng = np.random.default_rng(seed)
+    f = np.zeros((n, abi.FIELD_STRIDE))
+    f[:, abi.F_COORD_X] = np.round(rng.uniform(0, 600, n))
+    f[:, abi.F_COORD_Y] = np.round(rng.uniform(0, 400, n))
+    f[:, abi.F_DISP_X] = 1e-3 * f[:, abi.F_COORD_X] + rng.normal(0, 0.01, n)
+    f[:, abi.F_DISP_Y] = -2e-3 * f[:, abi.F_COORD_Y] + rng.normal(0, 0.01, n)
+    f[rng.random(n) < fail_frac, abi.F_SIGMA] = -1.0
+    return f
+
+
+def test_oracle_vsg_k_nearest_shells_equal_radius():
+    """k nearest neighbourhoods (negative windows, the reference's knnSearch):
+    on a square grid, k = 9 and k = 25 take whole shells of neighbours (self,
+    4 + 4 at 1 and sqrt(2) steps; then 4 + 8 at 2 and sqrt(5), 4 at sqrt(8)),
+    so they equal the radius windows that hold exactly those shells, bit for
+    bit.  The nearest must be valid, as the reference tests neighbour 0."""
+    ys, xs = np.mgrid[0:14, 0:17]
+    x, y = 30.0 + 10 * xs.ravel(), 40.0 + 10 * ys.ravel()
+    f = np.zeros((len(x), abi.FIELD_STRIDE))
+    f[:, abi.F_COORD_X], f[:, abi.F_COORD_Y] = x, y
+    rng = np.random.default_rng(3)
+    f[:, abi.F_DISP_X] = 0.5 + 0.0025 * (x - 100) + rng.normal(0, 1e-3, len(x))
+    f[:, abi.F_DISP_Y] = -0.25 + 0.004 * (y - 90) + rng.normal(0, 1e-3, len(x))
+    f[11, abi.F_SIGMA] = -1.0
+    interior = (xs.ravel() >= 2) & (xs.ravel() <= 14) & (ys.ravel() >= 2) & (ys.ravel() <= 11)
+    for k, window in ((9, 30), (25, 58)):   # radius 15 px: the 3 x 3 block; 29 px: the 5 x 5 block
+        ok_k, fail_k = O.vsg_strain(f, -k)
+        ok_r, fail_r = O.vsg_strain(f, window)
+        assert np.array_equal(ok_k[interior], ok_r[interior])
+        assert np.array_equal(fail_k[interior], fail_r[interior])
+    out, failed = O.vsg_strain(f, -9)
+    assert failed[11] == 1 and (failed == 0).sum() > 200
+    assert np.max(np.abs(out[failed == 0, 3] - 0.0025)) < 1e-3
+    with pytest.raises(AssertionError):
+        O.vsg_strain(f[:5], -6)     # more neighbours than subsets
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [5, 9, 16, 40])
+def test_gpu_vsg_k_nearest_matches_oracle(k):
+    """The GPU's k nearest neighbourhoods (host lists, float squared distance,
+    ties by index) equal the oracle's, and so do the fits, bit for bit, on a
+    scattered cloud with failed subsets and on a square grid, where ties at
+    the k-th distance are common."""
+    _gpu()
+    ys, xs = np.mgrid[0:20, 0:25]
+    grid = np.zeros((xs.size, abi.FIELD_STRIDE))
+    grid[:, abi.F_COORD_X], grid[:, abi.F_COORD_Y] = 5.0 + 7 * xs.ravel(), 9.0 + 7 * ys.ravel()
+    grid[:, abi.F_DISP_X] = 1e-3 * grid[:, abi.F_COORD_X]
+    grid[:, abi.F_DISP_Y] = 3e-3 * grid[:, abi.F_COORD_Y]
+    grid[::13, abi.F_SIGMA] = -1.0
+    for fields in (_scattered(2500, 11), grid):
+        want, failed = O.vsg_strain(fields, -k)
+        got, g = _device_vsg(fields, -k)
+        assert np.array_equal(got[:, :7], want)
+        assert np.array_equal(g[:, abi.F_MATCH] == -1.0, (failed == 1) | (fields[:, abi.F_MATCH] == -1.0))
+        assert (failed == 0).any()
