@@ -184,9 +184,9 @@ def cpu_sample(p, ref, frames, n_sample, nthreads, timed_frames=1, uncertainty=F
 
 SIMPLEX_FLOP_PER_PIXEL_EVAL = 200.0
 # DRAM bytes (read + write) of one frame_kernel launch of the full frame
-# (158,404 subsets, first frame of the sequence), from an ncu capture of that
-# launch: dram__bytes_read.sum 154.8 MB + dram__bytes_write.sum 131.7 MB
-FRAME_KERNEL_DRAM_BYTES = 154.848e6 + 131.709e6
+# (158,404 subsets, a frame of the sequence), from an ncu capture of that
+# launch: dram__bytes_read.sum 156.0 MB + dram__bytes_write.sum 31.4 MB
+FRAME_KERNEL_DRAM_BYTES = 156.004e6 + 31.382e6
 
 
 def oracle_sequence_sample(p, ref_h, frames_h, stride, nthreads, uncertainty=False, library=None):
@@ -1211,7 +1211,10 @@ def main():
             "frac": fp32_tflops / fp32_peak if (fp32_peak and fp32_tflops) else None,
             "traffic": FRAME_KERNEL_DRAM_BYTES,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one frame_kernel launch "
-                              "on the full first frame (reads 154.8 MB, writes 131.7 MB)",
+                              "on a full frame (reads 156.0 MB, writes 31.4 MB)",
+            "issue": {"inst_per_cycle_per_scheduler": 0.41, "warp_instructions_per_frame": 29.0e9,
+                      "source": "ncu smsp__issue_active / smsp__inst_executed.sum of the same capture; the "
+                                "binding resource is instruction issue, not a math pipe or DRAM"},
             "kernel": "frame_kernel (median step time incl. the gradient and pack kernels)",
             "peak_source": "measured FP32 SGEMM on CUDA cores (TF32 off) in this run",
             "per_unit": "390 FP32 flop per active pixel per Gauss-Newton pass + 200 per simplex evaluation, "
