@@ -225,6 +225,18 @@ RESULT_COLUMNS_TEXT = ("u, v, theta, strains, sigma, gamma, noise, contrast, act
                        "condition number")
 
 
+COLUMN_NAMES = {}
+
+
+def _column_names():
+    from dice_b200 import abi
+    if not COLUMN_NAMES:
+        for name in ("DISP_X", "DISP_Y", "ROT_Z", "STRETCH_XX", "STRETCH_YY", "SHEAR_XY", "SIGMA", "GAMMA", "NOISE",
+                     "CONTRAST", "ACTIVE_PIXELS", "STATUS", "ITERATIONS", "CONDITION"):
+            COLUMN_NAMES[getattr(abi, "F_" + name)] = name.lower()
+    return COLUMN_NAMES
+
+
 class RowComparison:
     """Rows of one run against the oracle's, frame by frame (n x stride
     each): the fractions of subset-frames with equal status, equal
@@ -234,8 +246,10 @@ class RowComparison:
     each group."""
 
     def __init__(self, max_fast_iterations):
+        _column_names()
         self.mx = max_fast_iterations
         self.eq_status = self.eq_iters = self.eq_all = self.tot = 0
+        self.col_bad = {}
         self.groups = {"gn_both": [0, 0.0, 0.0], "simplex_both": [0, 0.0, 0.0], "path_differs": [0, 0.0, 0.0]}
 
     def add(self, g, o):
@@ -248,6 +262,13 @@ class RowComparison:
         self.eq_iters += int(np.sum(g[:, abi.F_ITERATIONS] == o[:, abi.F_ITERATIONS]))
         same = (g[:, cols] == o[:, cols]) | (np.isnan(g[:, cols]) & np.isnan(o[:, cols]))
         self.eq_all += int(np.sum(np.all(same, axis=1)))
+        for ci, c in enumerate(cols):
+            bad = ~same[:, ci]
+            if bad.any():
+                name = COLUMN_NAMES.get(c, str(c))
+                cnt, mag = self.col_bad.get(name, (0, 0.0))
+                diff = np.abs(g[bad, c] - o[bad, c])
+                self.col_bad[name] = (cnt + int(bad.sum()), max(mag, float(np.nanmax(diff, initial=0.0))))
         self.tot += len(g)
         gs, os_ = g[:, abi.F_ITERATIONS] > self.mx, o[:, abi.F_ITERATIONS] > self.mx
         for name, m in (("gn_both", both & ~gs & ~os_), ("simplex_both", both & gs & os_),
@@ -262,6 +283,8 @@ class RowComparison:
         t = max(self.tot, 1)
         return {"status_equal_frac": self.eq_status / t, "iterations_equal_frac": self.eq_iters / t,
                 "all_columns_equal_frac": self.eq_all / t, "status_mismatches": self.tot - self.eq_status,
+                "differing_by_column": {k: {"subset_frames": v[0], "max_abs_diff": v[1]}
+                                        for k, v in self.col_bad.items()},
                 "by_path": {k: {"subset_frames": v[0], "max_abs_du_px": v[1], "max_abs_dv_px": v[2]}
                             for k, v in self.groups.items()}}
 
