@@ -25,6 +25,7 @@ JUMP_TOLERANCE_EXCEEDED = 16
 HESSIAN_SINGULAR = 21
 FRAME_FAILED_DUE_TO_HIGH_GAMMA = 23
 FRAME_FAILED_DUE_TO_NEGATIVE_SIGMA = 24
+FRAME_SKIPPED = 30
 
 BILINEAR, BICUBIC, KEYS_FOURTH = 0, 1, 2
 SIMPLEX, GRADIENT_BASED, SIMPLEX_THEN_GRADIENT_BASED, GRADIENT_BASED_THEN_SIMPLEX = 0, 1, 3, 4
@@ -115,6 +116,7 @@ class Params(ctypes.Structure):
         ("use_subset_evolution", ctypes.c_int32),
         ("use_incremental_formulation", ctypes.c_int32),
         ("initialization_method", ctypes.c_int32),
+        ("skip_all_solves", ctypes.c_int32),
     ]
 
     def copy(self):
@@ -235,6 +237,7 @@ def _declare(lib):
         "dicegpu_subset_file_force_simplex": (c_int, [c_void_p, c_void_p]),
         "dicegpu_subset_file_seeds": (c_int, [c_void_p, c_void_p, c_void_p]),
         "dicegpu_subset_file_features": (c_int, [c_void_p, c_void_p]),
+        "dicegpu_subset_file_skip_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
         "dicegpu_subset_file_apply": (c_int, [c_void_p, c_void_p]),
         "dicegpu_output_create": (c_int, [P, ctypes.c_char_p, ctypes.c_char_p, c_int, c_void_p,
                                           ctypes.POINTER(c_void_p)]),
@@ -283,6 +286,8 @@ def _declare(lib):
         "dicegpu_correlate": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p,
                                       c_int, c_int, P, c_int]),
         "dicegpu_correlate_reset": (c_int, []),
+        "dicegpu_set_skip_solve": (c_int, [c_void_p, c_int, c_void_p]),
+        "dicegpu_skip_solve_frame": (c_int, [c_void_p, c_int, c_int]),
         "dicegpu_interpolate": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p,
                                         c_void_p, c_int]),
         "dicegpu_image_gradients": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_int,

@@ -47,6 +47,7 @@ struct DevParams {
   int output_beta;
   int use_def_grads;
   int subset_size;
+  int skip_all;      // skip_all_solves
 };
 
 struct DevImage {
@@ -72,7 +73,7 @@ struct DevGeometry {
   const int32_t* __restrict__ offsets;
   const int32_t* __restrict__ px;
   const int32_t* __restrict__ py;
-  const uint8_t* __restrict__ force_simplex;
+  const uint8_t* __restrict__ force_simplex;   // per subset: bit 0 force the simplex, bit 1 skip the solve
   // optional per-subset mask descriptors (DG_MASK_DESC ints each), the
   // obstruction words, and the blocked-polygon table and vertices
   const int32_t* __restrict__ mask_desc;

@@ -1084,6 +1084,110 @@ struct Engine {
     return result;
   }
 
+  // Schema::record_step (DICe_Schema.cpp:1986-2009) with save_fields: the
+  // shape-function columns (quadratic: A..L and the mapped u, v, theta) and
+  // the solve's results.  Thread 0 writes.
+  __device__ void record_step(double* f, const float* slots, float nu, float nv, float nt, float sg, float gamma,
+                              float bt, float noise, float contrast, int active, int status, int num_iterations) const {
+    if (tid != 0) return;
+    if (SHAPE == DICEGPU_QUADRATIC_SF) {
+      for (int i = 0; i < 12; ++i) f[DICEGPU_F_QUAD_A + i] = slots[i];
+      f[DICEGPU_F_DISP_X] = nu;
+      f[DICEGPU_F_DISP_Y] = nv;
+      f[DICEGPU_F_ROT_Z] = nt;
+    } else {
+      const unsigned em = enabled_mask();
+      f[DICEGPU_F_DISP_X] = slots[0];
+      f[DICEGPU_F_DISP_Y] = slots[1];
+#pragma unroll
+      for (int s = 2; s < 6; ++s)
+        if ((em >> s) & 1u) f[DICEGPU_F_DISP_X + s] = slots[s];
+    }
+    f[DICEGPU_F_SIGMA] = sg;
+    f[DICEGPU_F_MATCH] = 0.0;
+    f[DICEGPU_F_GAMMA] = gamma;
+    f[DICEGPU_F_BETA] = bt;
+    f[DICEGPU_F_NOISE] = noise;
+    f[DICEGPU_F_CONTRAST] = contrast;
+    f[DICEGPU_F_ACTIVE_PIXELS] = active;
+    f[DICEGPU_F_STATUS] = status;
+    f[DICEGPU_F_ITERATIONS] = num_iterations;
+  }
+
+  // The per-pixel state of a subset as constructed (before any deformed-state
+  // initialisation): liveness = activity, the rows 0 and 1 = the reference
+  // image's gradients at the pixels, live count and box of the active pixels.
+  __device__ void fresh_state(const SubsetRef& sb) {
+    const PixArrays X = arrays();
+    const long rlim = (long)A.ref.w * A.ref.h;
+    int n = 0, minx = sb.cx, maxx = sb.cx, miny = sb.cy, maxy = sb.cy;
+    for (int p = tid; p < sb.npix; p += T) {
+      int x, y;
+      pixel_xy(sb, p, x, y);
+      bool active = true;
+      if (MASK && sb.evo) active = A.geo.pix_flag[sb.off + p] != 0;
+      const long ri = (long)y * A.ref.w + x;
+      X.R(0)[p] = ri < rlim ? __ldg(A.ref.gx + ri) : 0.0f;
+      X.R(1)[p] = ri < rlim ? __ldg(A.ref.gy + ri) : 0.0f;
+      X.L[p] = (uint8_t)(active ? 3 : 0);
+      if (active) {
+        ++n;
+        minx = min(minx, x); maxx = max(maxx, x);
+        miny = min(miny, y); maxy = max(maxy, y);
+      }
+    }
+    WarpOut<SHAPE>& wo = wouts<SHAPE>()[warp];
+    n = warp_sum_i(n);
+    minx = warp_min_i(minx); maxx = warp_max_i(maxx);
+    miny = warp_min_i(miny); maxy = warp_max_i(maxy);
+    if (lane == 0) {
+      wo.n = n; wo.minx = minx; wo.maxx = maxx; wo.miny = miny; wo.maxy = maxy;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      Ctl& cl = ctl();
+      const WarpOut<SHAPE>* all = wouts<SHAPE>();
+      int nn = 0, a0 = sb.cx, a1 = sb.cx, b0 = sb.cy, b1 = sb.cy;
+      for (int w = 0; w < (T >> 5); ++w) {
+        nn += all[w].n;
+        a0 = min(a0, all[w].minx); a1 = max(a1, all[w].maxx);
+        b0 = min(b0, all[w].miny); b1 = max(b1, all[w].maxy);
+      }
+      cl.n = nn; cl.minx = a0; cl.maxx = a1; cl.miny = b0; cl.maxy = b1;
+    }
+    __syncthreads();
+  }
+
+  // A subset whose solve is skipped (SKIP_SOLVE, skip_all_solves;
+  // DICe_Schema.cpp:2118-2143): sigma, gamma, beta, contrast and the active
+  // pixels at the initial guess, recorded as FRAME_SKIPPED.  Out of line: a
+  // path outside the correlation loop.
+  __device__ __noinline__ void skip_solve(const SubsetRef sb, double* f, const Slots init, int num_iterations) {
+    const DevParams& P = A.P;
+    float slots[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) slots[i] = init.s[i];
+    // Objective::sigma reads the subset as constructed: no deformed-state
+    // initialisation has run, so every active pixel counts, with the
+    // reference image's gradients, and the noise box is the active pixels'
+    fresh_state(sb);
+    float noise = 0.0f;
+    const float sg = sigma(sb, slots, noise);
+    float def_sum2 = 0.0f;
+    const float gamma = eval_gamma(sb, slots, P.normalize_gamma != 0, &def_sum2);
+    const int fin_n = ctl().n;
+    const float bt = P.output_beta ? beta(sb, slots) : 0.0f;
+    const float contrast = fin_n == 0 ? 0.0f : __fsqrt_rn(__fdiv_rn(def_sum2, (float)fin_n));
+    MapConst kc;
+    float nu = 0.0f, nv = 0.0f, nt = 0.0f;
+    make_mapconst<SHAPE>(slots, false, (float)sb.cx, (float)sb.cy, kc);
+    map_to_u_v_theta<SHAPE>(kc, (float)sb.cx, (float)sb.cy, nu, nv, nt);
+    record_step(f, slots, nu, nv, nt, sg, gamma, bt, noise, contrast, fin_n, DICEGPU_FRAME_SKIPPED, num_iterations);
+    if constexpr (MASK) {
+      if (sb.evo && A.evolve) evolve(sb, init);
+    }
+  }
+
   // --------------------------------------------------------------------------
   // generic_correlation_routine for one subset.
   // --------------------------------------------------------------------------
@@ -1173,6 +1277,14 @@ struct Engine {
                         __fsub_rn((float)fld(DICEGPU_F_COORD_Y), (float)__shfl_sync(FULL, gv, DICEGPU_F_COORD_Y)));
     };
     initial_guess();
+    const uint8_t subset_flags = A.geo.force_simplex ? A.geo.force_simplex[idx] : 0;
+    if ((subset_flags & 2u) || P.skip_all) {
+      Slots init;
+#pragma unroll
+      for (int i = 0; i < 12; ++i) init.s[i] = slots[i];
+      skip_solve(sb, f, init, num_iterations);
+      return;
+    }
     // the deformed state of the subset: none yet (Gauss-Newton then takes the
     // reference mean over all its pixels)
     bool have_state = false;
@@ -1188,7 +1300,7 @@ struct Engine {
     const float prev_u = (float)fld(DICEGPU_F_DISP_X);
     const float prev_v = (float)fld(DICEGPU_F_DISP_Y);
     const float prev_t = (float)fld(DICEGPU_F_ROT_Z);
-    const bool force_simplex = A.geo.force_simplex && A.geo.force_simplex[idx];
+    const bool force_simplex = (subset_flags & 1u) != 0;
     const int opt = P.opt;
     int corr_status = DICEGPU_CORRELATION_FAILED;
     float cond = 0.0f;
@@ -1272,31 +1384,7 @@ struct Engine {
     }
     // contrast_std_dev (DICe_Subset.cpp:607-620) at the final parameters
     const float contrast = fin_n == 0 ? 0.0f : __fsqrt_rn(__fdiv_rn(def_sum2, (float)fin_n));
-    if (tid == 0) {
-      // record_step (DICe_Schema.cpp:1986-2009), save_fields
-      if (SHAPE == DICEGPU_QUADRATIC_SF) {
-        for (int i = 0; i < 12; ++i) f[DICEGPU_F_QUAD_A + i] = slots[i];
-        f[DICEGPU_F_DISP_X] = nu;
-        f[DICEGPU_F_DISP_Y] = nv;
-        f[DICEGPU_F_ROT_Z] = nt;
-      } else {
-        const unsigned em = enabled_mask();
-        f[DICEGPU_F_DISP_X] = slots[0];
-        f[DICEGPU_F_DISP_Y] = slots[1];
-#pragma unroll
-        for (int s = 2; s < 6; ++s)
-          if ((em >> s) & 1u) f[DICEGPU_F_DISP_X + s] = slots[s];
-      }
-      f[DICEGPU_F_SIGMA] = sg;
-      f[DICEGPU_F_MATCH] = 0.0;
-      f[DICEGPU_F_GAMMA] = gamma;
-      f[DICEGPU_F_BETA] = bt;
-      f[DICEGPU_F_NOISE] = noise;
-      f[DICEGPU_F_CONTRAST] = contrast;
-      f[DICEGPU_F_ACTIVE_PIXELS] = fin_n;
-      f[DICEGPU_F_STATUS] = init_status;
-      f[DICEGPU_F_ITERATIONS] = num_iterations;
-    }
+    record_step(f, slots, nu, nv, nt, sg, gamma, bt, noise, contrast, fin_n, init_status, num_iterations);
     if constexpr (MASK) {
       if (sb.evo && A.evolve) {
         Slots fs;

@@ -354,6 +354,7 @@ struct dicegpu_ctx {
   int n_blocked = 0;                   // subsets with a conformal blocker
   // forced simplex: the caller's flags and the blocking rule's
   std::vector<uint8_t> h_force_user, h_force_block;
+  std::vector<uint8_t> h_skip_user;   // dicegpu_set_skip_solve
   // VSG strain: the neighbour grid of the subset centres (rebuilt when the
   // window or the coordinates change) and the results
   int vsg_window = 0;
@@ -429,6 +430,7 @@ static int build_devparams(const dicegpu_params& p, DevParams& d) {
   d.fast_tol = (float)p.fast_solver_tolerance;
   d.robust_tol = p.robust_solver_tolerance;
   d.skip_thr = (float)p.skip_solve_gamma_threshold;
+  d.skip_all = p.skip_all_solves != 0;
   d.disp_jump = p.disp_jump_tol;
   d.theta_jump = p.theta_jump_tol;
   d.lm_alpha = p.levenberg_marquardt_regularization_factor > 0.0
@@ -828,6 +830,7 @@ extern "C" int dicegpu_set_subsets(dicegpu_ctx* c, int n, const double* fields) 
     c->use_lists = false;
     c->use_force = false;
     c->h_force_user.clear();
+    c->h_skip_user.clear();
     c->h_neigh.clear();
     clear_shapes(c);
   }
@@ -902,12 +905,16 @@ static int upload_force(dicegpu_ctx* c) {
   const int n = c->n;
   const bool user = (int)c->h_force_user.size() == n;
   const bool block = (int)c->h_force_block.size() == n && !c->params.override_force_simplex;
-  if (!user && !block) {
+  const bool skip = (int)c->h_skip_user.size() == n;
+  if (!user && !block && !skip) {
     c->use_force = false;
     return DICEGPU_OK;
   }
+  // per subset: bit 0 force the simplex, bit 1 skip the solve
   std::vector<uint8_t> f(n, 0);
-  for (int i = 0; i < n; ++i) f[i] = (user && c->h_force_user[i]) || (block && c->h_force_block[i]);
+  for (int i = 0; i < n; ++i)
+    f[i] = (uint8_t)(((user && c->h_force_user[i]) || (block && c->h_force_block[i]) ? 1 : 0) |
+                     (skip && c->h_skip_user[i] ? 2 : 0));
   cudaStreamSynchronize(c->stream);
   int rc = grow(&c->d_force, &c->force_cap, (size_t)n);
   if (rc) return rc;
@@ -1414,6 +1421,29 @@ extern "C" int dicegpu_get_subset_pixel_state(dicegpu_ctx* c, uint8_t* state, fl
   if (last > 0 && ref_values)
     CK(cudaMemcpy(ref_values, c->d_pix_f.p, (size_t)last * sizeof(float), cudaMemcpyDeviceToHost));
   return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_set_skip_solve(dicegpu_ctx* c, int n, const uint8_t* flags) {
+  if (!c) return DICEGPU_ERR_ARG;
+  if (!flags) {
+    c->h_skip_user.clear();
+    return upload_force(c);
+  }
+  if (n != c->n) return DICEGPU_ERR_ARG;
+  c->h_skip_user.assign(flags, flags + n);
+  return upload_force(c);
+}
+
+extern "C" int dicegpu_skip_solve_frame(const int32_t* frame_ids, int count, int frame) {
+  if (count < 0 || (count > 0 && !frame_ids)) return DICEGPU_ERR_ARG;
+  if (count == 0) return 1;
+  int index = count;
+  for (int i = 0; i < count; ++i)
+    if (frame < frame_ids[i]) {
+      index = i;
+      break;
+    }
+  return index % 2 == 0 ? 0 : 1;
 }
 
 extern "C" int dicegpu_set_force_simplex(dicegpu_ctx* c, int n, const uint8_t* flags) {

@@ -49,6 +49,7 @@ struct dicegpu_subset_file {
   std::set<int> force_simplex;
   std::map<int, Seed> seeds;
   std::map<int, int> features;
+  std::map<int, std::vector<int32_t>> skip_solve;   // SKIP_SOLVE frame ids, ascending
   int n_roi = 0;
 };
 
@@ -328,8 +329,9 @@ void read_roi(std::istream& is, dicegpu_subset_file& F) {
 // BEGIN CONFORMAL_SUBSET (DICe_Parser.cpp:1366-1600)
 void read_conformal(std::istream& is, dicegpu_subset_file& F) {
   int id = -1;
-  bool has_seed = false, force = false, test_motion = false, motion_window = false;
+  bool has_seed = false, force = false, test_motion = false, motion_window = false, has_skip = false;
   int features = 0;
+  std::vector<int32_t> skip;
   Seed seed;
   ConformalDef def;
   std::vector<int> blocking;
@@ -354,10 +356,19 @@ void read_conformal(std::istream& is, dicegpu_subset_file& F) {
           if (!is_number(t[m])) fail("MOTION_WINDOW parameters should be numbers");
       }
     } else if (t[0] == "SKIP_SOLVE") {
-      features |= DICEGPU_SF_FEATURE_SKIP_SOLVE;
-      if (t.size() > 1 && is_number(t[1]))
-        for (std::size_t m = 1; m < t.size(); ++m)
+      if (t.size() > 1 && !is_number(t[1])) {
+        // the frame ids in a file (DICe_Parser.cpp:1440-1452): not read here
+        features |= DICEGPU_SF_FEATURE_SKIP_SOLVE;
+      } else {
+        // frame ids that turn solving off and on (DICe_Parser.cpp:1454-1463)
+        has_skip = true;
+        skip.clear();
+        for (std::size_t m = 1; m < t.size(); ++m) {
           if (!is_number(t[m])) fail("SKIP_SOLVE ids should be numbers");
+          skip.push_back((int32_t)to_int(t[m]));
+        }
+        std::sort(skip.begin(), skip.end());
+      }
     } else if (t[0] == "USE_OPTICAL_FLOW") {
       features |= DICEGPU_SF_FEATURE_OPTICAL_FLOW;
     } else if (t[0] == "FORCE_SIMPLEX") {
@@ -401,6 +412,7 @@ void read_conformal(std::istream& is, dicegpu_subset_file& F) {
   if (force) F.force_simplex.insert(id);
   if (has_seed) F.seeds.insert(std::make_pair(id, seed));
   if (features) F.features[id] |= features;
+  if (has_skip) F.skip_solve[id] = skip;
 }
 
 void parse(std::istream& is, int width, int height, dicegpu_subset_file& F) {
@@ -491,6 +503,26 @@ extern "C" int dicegpu_subset_file_get_info(const dicegpu_subset_file* f, dicegp
   info->region_of_interest = f->roi ? 1 : 0;
   info->n_seeds = (int32_t)f->seeds.size();
   info->n_unsupported = (int32_t)f->features.size();
+  info->n_skip_solve_ids = 0;
+  for (const auto& kv : f->skip_solve) info->n_skip_solve_ids += (int32_t)kv.second.size();
+  return DICEGPU_OK;
+}
+
+extern "C" int dicegpu_subset_file_skip_solve(const dicegpu_subset_file* f, uint8_t* has_skip, int32_t* offsets,
+                                              int32_t* frame_ids) {
+  if (!f || !has_skip || !offsets) return DICEGPU_ERR_ARG;
+  const int n = (int)(f->coords.size() / 2);
+  int32_t k = 0;
+  for (int i = 0; i < n; ++i) {
+    offsets[i] = k;
+    const auto it = f->skip_solve.find(i);
+    has_skip[i] = it != f->skip_solve.end();
+    if (has_skip[i]) {
+      if (!it->second.empty() && !frame_ids) return DICEGPU_ERR_ARG;
+      for (int32_t v : it->second) frame_ids[k++] = v;
+    }
+  }
+  offsets[n] = k;
   return DICEGPU_OK;
 }
 

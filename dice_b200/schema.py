@@ -226,6 +226,16 @@ class Schema:
         abi.check(self.lib.dicegpu_set_force_simplex(self.ctx, a.shape[0], a.ctypes.data_as(ctypes.c_void_p)),
                   "set_force_simplex")
 
+    def set_skip_solve(self, flags):
+        """Per-subset flags (non-zero: only evaluate the initial guess and
+        record FRAME_SKIPPED) for the following frames; None clears them."""
+        if flags is None:
+            abi.check(self.lib.dicegpu_set_skip_solve(self.ctx, 0, None), "set_skip_solve")
+            return
+        a = np.ascontiguousarray(np.asarray(flags) != 0, dtype=np.uint8)
+        abi.check(self.lib.dicegpu_set_skip_solve(self.ctx, a.shape[0], a.ctypes.data_as(ctypes.c_void_p)),
+                  "set_skip_solve")
+
     # ---- execution ----------------------------------------------------------------
     def execute_correlation(self):
         abi.check(self.lib.dicegpu_execute_correlation(self.ctx), "execute_correlation")

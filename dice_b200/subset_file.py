@@ -19,7 +19,8 @@ FEATURE_SKIP_SOLVE, FEATURE_OPTICAL_FLOW, FEATURE_PATH_FILE, FEATURE_MOTION_WIND
 
 class Info(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int32) for k in ("n_subsets", "n_shapes", "n_vertices", "n_blocking_ids",
-                                                "n_conformal", "region_of_interest", "n_seeds", "n_unsupported")]
+                                                "n_conformal", "region_of_interest", "n_seeds", "n_unsupported",
+                                                "n_skip_solve_ids")]
 
 
 class SubsetFileError(ValueError):
@@ -75,6 +76,23 @@ class SubsetFile:
             abi.check(self.lib.dicegpu_subset_file_features(self.h, _vp(self.features)), "features")
         self.force_simplex = self.force_simplex[:n]
         self.seed_values, self.seed_flags, self.features = self.seed_values[:n], self.seed_flags[:n], self.features[:n]
+        # SKIP_SOLVE frame lists (None: the subset has none)
+        has = np.zeros(max(n, 1), np.uint8)
+        soff = np.zeros(n + 1, np.int32)
+        sids = np.zeros(max(info.n_skip_solve_ids, 1), np.int32)
+        abi.check(self.lib.dicegpu_subset_file_skip_solve(self.h, _vp(has), _vp(soff), _vp(sids)), "skip_solve")
+        self.skip_solve = [list(sids[soff[i]:soff[i + 1]]) if has[i] else None for i in range(n)]
+
+    def skip_solve_flags(self, frame):
+        """Per-subset flags for dicegpu_set_skip_solve at frame id `frame`
+        (frame_should_be_skipped over each subset's SKIP_SOLVE list)."""
+        out = np.zeros(len(self.skip_solve), np.uint8)
+        for i, ids in enumerate(self.skip_solve):
+            if ids is None:
+                continue
+            a = np.ascontiguousarray(ids, dtype=np.int32)
+            out[i] = self.lib.dicegpu_skip_solve_frame(_vp(a) if len(a) else None, len(a), int(frame))
+        return out
 
     def apply_grid(self, schema, width, height, step_size):
         """Schema::initialize with a region-of-interest file and a step size."""

@@ -64,6 +64,7 @@ extern "C" {
 #define DICEGPU_HESSIAN_SINGULAR                      21
 #define DICEGPU_FRAME_FAILED_DUE_TO_HIGH_GAMMA        23
 #define DICEGPU_FRAME_FAILED_DUE_TO_NEGATIVE_SIGMA    24
+#define DICEGPU_FRAME_SKIPPED                         30
 
 /* Interpolation_Method, DICe.h:549-555 */
 #define DICEGPU_BILINEAR    0
@@ -227,6 +228,11 @@ typedef struct dicegpu_params {
    * runs the subsets in dependency waves (a chain of single subsets as one
    * sequential launch).  Other methods: DICEGPU_ERR_UNSUPPORTED. */
   int32_t initialization_method;
+  /* skip_all_solves (0): every subset is only initialised, as for a subset
+   * whose solve is skipped (dicegpu_set_skip_solve): sigma, gamma (and beta)
+   * at its initial guess, STATUS_FLAG = FRAME_SKIPPED, ITERATIONS = -1
+   * (Schema::generic_correlation_routine, DICe_Schema.cpp:2118-2143). */
+  int32_t skip_all_solves;
 } dicegpu_params;
 
 /* Initialization_Method (DICe.h:473-489) */
@@ -387,6 +393,21 @@ int dicegpu_set_neighbors(dicegpu_ctx* ctx, const int32_t* neighbor_ids);
  * params filter) becomes the reference and its gradients are computed;
  * device copies only, so it can be captured with a sequence. */
 int dicegpu_set_ref_from_def(dicegpu_ctx* ctx);
+/* Per-subset "skip the solve" flags for the following frames (n bytes,
+ * non-zero: skip; NULL clears them): a skipped subset is initialised from
+ * its field values as usual, then only evaluated there -- sigma, gamma,
+ * beta, contrast, active pixels -- and recorded with STATUS_FLAG =
+ * FRAME_SKIPPED and ITERATIONS = -1, without the jump or gamma tests
+ * (DICe_Schema.cpp:2051-2059, 2118-2143; SKIP_SOLVE in a subset file).
+ * dicegpu_skip_solve_frame gives a subset's flag for a frame from its
+ * SKIP_SOLVE frame list. */
+int dicegpu_set_skip_solve(dicegpu_ctx* ctx, int n, const uint8_t* flags);
+/* frame_should_be_skipped (DICe_Schema.cpp:4945-4960): with the ascending
+ * frame ids of a SKIP_SOLVE list (count 0: always skip), 1 when the solve
+ * of frame `frame` is skipped -- frame ids toggle solving off and on,
+ * starting on. */
+int dicegpu_skip_solve_frame(const int32_t* frame_ids, int count, int frame);
+
 /* Subset evolution state of the list pixels (use_subset_evolution in the
  * tracking routine, with conformal subsets that have excluded shapes):
  * state[offsets[n]] 0 inactive (excluded and not yet seen), 1 active, 2

@@ -56,11 +56,14 @@ typedef struct dicegpu_subset_file_info {
   int32_t region_of_interest; /* 1: a REGION_OF_INTEREST file */
   int32_t n_seeds;            /* definitions with a SEED */
   int32_t n_unsupported;      /* subsets using a feature listed under DICEGPU_SF_FEATURE_* */
+  int32_t n_skip_solve_ids;   /* frame ids of all SKIP_SOLVE lists */
 } dicegpu_subset_file_info;
 
 /* Feature bits of dicegpu_subset_file_features: subset-file options that
  * select parts of the reference outside this library's correlation path
- * (other initializers, motion detection, frame skipping). */
+ * (other initializers, motion detection, a SKIP_SOLVE whose frame ids are in
+ * another file).  A SKIP_SOLVE with its frame ids on the line is read:
+ * dicegpu_subset_file_skip_solve. */
 #define DICEGPU_SF_FEATURE_SKIP_SOLVE    1
 #define DICEGPU_SF_FEATURE_OPTICAL_FLOW  2
 #define DICEGPU_SF_FEATURE_PATH_FILE     4
@@ -95,6 +98,13 @@ int dicegpu_subset_file_force_simplex(const dicegpu_subset_file* f, uint8_t* fla
 /* Seeds per subset: values[6 * i ..] = u, v, normal strain x, y, shear
  * strain, rotation; flags[i] = DICEGPU_SF_SEED_* bits present. */
 int dicegpu_subset_file_seeds(const dicegpu_subset_file* f, double* values, uint8_t* flags);
+/* SKIP_SOLVE per subset (DICe_Parser.cpp:1435-1463): has_skip[i] non-zero
+ * when subset i has one; its ascending frame ids are frame_ids[offsets[i] ..
+ * offsets[i + 1]) (offsets: n_subsets + 1 entries; frame_ids:
+ * n_skip_solve_ids).  dicegpu_skip_solve_frame turns a list into the flag
+ * of a frame for dicegpu_set_skip_solve. */
+int dicegpu_subset_file_skip_solve(const dicegpu_subset_file* f, uint8_t* has_skip, int32_t* offsets,
+                                   int32_t* frame_ids);
 /* DICEGPU_SF_FEATURE_* bits per subset (n_subsets bytes). */
 int dicegpu_subset_file_features(const dicegpu_subset_file* f, uint8_t* flags);
 

@@ -1125,8 +1125,10 @@ static float objective_beta(const Ctx& C, Subset& s, const ShapeFn& sf_in) {
 // Schema::generic_correlation_routine (DICe_Schema.cpp:2026-2368) for one subset,
 // restricted to the field-value initializer (own or neighbour row, nf) and
 // local DIC.
+// flags: bit 0 forces the simplex, bit 1 skips the solve (SKIP_SOLVE).
 static bool correlate_subset(const Ctx& C, Subset& s, double* f, bool first_frame,
-                             bool force_simplex, Counters* cnt, const double* nf = nullptr) {
+                             unsigned flags, Counters* cnt, const double* nf = nullptr) {
+  const bool force_simplex = (flags & 1u) != 0;
   const dicegpu_params& P = C.P;
   if (P.subset_size > 0 && first_frame) {
     const float cur_x = (float)(f[DICEGPU_F_COORD_X] + f[DICEGPU_F_DISP_X]);
@@ -1144,6 +1146,27 @@ static bool correlate_subset(const Ctx& C, Subset& s, double* f, bool first_fram
   if (init_status == DICEGPU_INITIALIZE_FAILED) {
     record_failed_step(f, init_status, num_iterations);
     return false;
+  }
+  // the solve skipped (DICe_Schema.cpp:2118-2143): the initial guess
+  // evaluated and recorded as FRAME_SKIPPED
+  if ((flags & 2u) || P.skip_all_solves) {
+    float noise = 0.0f;
+    const float sigma = objective_sigma(C, s, sf, noise);
+    const float gamma = objective_gamma(C, s, sf, cnt);
+    const float beta = P.output_beta ? objective_beta(C, s, sf) : 0.0f;
+    const float contrast = s.contrast_std_dev();
+    const int active_pixels = s.num_active();
+    sf.to_fields(f, (float)s.cx, (float)s.cy);
+    f[DICEGPU_F_SIGMA] = sigma;
+    f[DICEGPU_F_MATCH] = 0.0;
+    f[DICEGPU_F_GAMMA] = gamma;
+    f[DICEGPU_F_BETA] = beta;
+    f[DICEGPU_F_NOISE] = noise;
+    f[DICEGPU_F_CONTRAST] = contrast;
+    f[DICEGPU_F_ACTIVE_PIXELS] = active_pixels;
+    f[DICEGPU_F_STATUS] = DICEGPU_FRAME_SKIPPED;
+    f[DICEGPU_F_ITERATIONS] = num_iterations;
+    return true;
   }
   if (P.initial_gamma_threshold != -1.0) {
     const float g0 = objective_gamma(C, s, sf, cnt);
@@ -1350,7 +1373,7 @@ void run_range(const FrameJob& J, int b, int e) {
       const int j = J.neighbors[i];
       if (j >= 0 && j < J.n && j != i) nf = J.fields + (long)j * DICEGPU_FIELD_STRIDE;
     }
-    const bool ok = correlate_subset(J.C, s, f, J.first_frame, J.force_simplex && J.force_simplex[i], &cnt, nf);
+    const bool ok = correlate_subset(J.C, s, f, J.first_frame, J.force_simplex ? J.force_simplex[i] : 0u, &cnt, nf);
     // Subset::turn_on_previously_obstructed_pixels (DICe_Subset.cpp:506-520)
     // with the deformed state of the last evaluation
     if (ok && J.evolve && s.flag)
@@ -1742,7 +1765,7 @@ extern "C" int oracle_execute_frame_shapes(const dicegpu_params* params, int w, 
       for (int k = block_offsets[i]; k < block_offsets[i + 1]; ++k) {
         if (block_ids[k] < 0 || block_ids[k] >= n) return DICEGPU_ERR_ARG;
         any_block = true;
-        if (!params->override_force_simplex) { force[i] = 1; force[block_ids[k]] = 1; }
+        if (!params->override_force_simplex) { force[i] |= 1; force[block_ids[k]] |= 1; }
       }
   }
   FrameJob J;

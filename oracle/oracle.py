@@ -76,12 +76,28 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
 
+def _subset_flags(n, force_simplex, skip_solve):
+    """Per-subset flag bytes of the oracle: bit 0 forces the simplex, bit 1
+    skips the solve."""
+    if force_simplex is None and skip_solve is None:
+        return None
+    f = np.zeros(n, np.uint8)
+    if force_simplex is not None:
+        f |= (np.asarray(force_simplex) != 0).astype(np.uint8)
+    if skip_solve is not None:
+        f |= 2 * (np.asarray(skip_solve) != 0).astype(np.uint8)
+    return np.ascontiguousarray(f)
+
+
 def execute_frame(params, ref, deff, fields, first_frame=True, nthreads=1, offsets=None,
-                  px=None, py=None, force_simplex=None, counters=False, uncertainty=None, neighbors=None):
+                  px=None, py=None, force_simplex=None, counters=False, uncertainty=None, neighbors=None,
+                  skip_solve=None):
     """One frame over all subsets; updates `fields` (n x FIELD_STRIDE float64) in place.
     `uncertainty` (n x UNCERTAINTY_STRIDE float64, optional) receives the
     uncertainty fields of every converged Gauss-Newton solve.  `neighbors`
-    (NEIGHBOR_ID per subset) serve params.initialization_method."""
+    (NEIGHBOR_ID per subset) serve params.initialization_method.
+    `skip_solve` (per subset, non-zero: skip) only evaluates those subsets at
+    their initial guess (FRAME_SKIPPED)."""
     if neighbors is not None:
         neighbors = np.ascontiguousarray(neighbors, dtype=np.int32)
     if uncertainty is not None:
@@ -96,8 +112,7 @@ def execute_frame(params, ref, deff, fields, first_frame=True, nthreads=1, offse
         offsets = np.ascontiguousarray(offsets, dtype=np.int32)
         px = np.ascontiguousarray(px, dtype=np.int32)
         py = np.ascontiguousarray(py, dtype=np.int32)
-    if force_simplex is not None:
-        force_simplex = np.ascontiguousarray(force_simplex, dtype=np.uint8)
+    force_simplex = _subset_flags(n, force_simplex, skip_solve)
     gn = np.zeros(n, np.int32) if counters else None
     sx = np.zeros(n, np.int32) if counters else None
     rc = lib().oracle_execute_frame(ctypes.byref(params), w, h, _ptr(ref), _ptr(deff), n,
@@ -144,7 +159,7 @@ def rasterize(n, shapes, vx=None, vy=None, fields=None, square_size=0):
 
 def execute_frame_shapes(params, ref, deff, fields, shapes, vx=None, vy=None, block_offsets=None,
                          block_ids=None, force_simplex=None, first_frame=True, nthreads=1, evolution=None,
-                         frame_index=0):
+                         frame_index=0, skip_solve=None):
     """Schema::execute_correlation over subsets defined by shapes with
     obstructions and blocking subsets; updates `fields` in place.  With
     params.use_subset_evolution, `evolution` is a dict carried across the
@@ -159,7 +174,7 @@ def execute_frame_shapes(params, ref, deff, fields, shapes, vx=None, vy=None, bl
     y = np.ascontiguousarray(vy if vy is not None else [0], dtype=np.int32)
     bo = None if block_offsets is None else np.ascontiguousarray(block_offsets, dtype=np.int32)
     bi = None if block_ids is None else np.ascontiguousarray(block_ids if len(block_ids) else [0], dtype=np.int32)
-    fs = None if force_simplex is None else np.ascontiguousarray(force_simplex, dtype=np.uint8)
+    fs = _subset_flags(n, force_simplex, skip_solve)
     pf = pv = None
     if evolution is not None and params.use_subset_evolution and params.correlation_routine == TRACKING_ROUTINE:
         if "flag" not in evolution:

@@ -61,7 +61,12 @@ def test_obstruction_and_mechanism_files():
     assert kinds == [(0, abi.SHAPE_POLYGON), (0, abi.SHAPE_POLYGON), (1, abi.SHAPE_RECTANGLE),
                      (2, abi.SHAPE_CIRCLE), (3, abi.SHAPE_RECTANGLE)]
     skip = SubsetFile(text=_text("mechanism_skip_solves"))
-    assert (skip.features == FEATURE_SKIP_SOLVE).all()
+    # subset 0 reads its frame ids from another file (not read here: an
+    # unsupported feature); subset 1 lists them on the line
+    assert skip.features.tolist() == [FEATURE_SKIP_SOLVE, 0]
+    assert skip.skip_solve == [None, [4903, 4912, 4915]]
+    # frame_should_be_skipped: solving starts on; each id toggles it
+    assert [skip.skip_solve_flags(fr)[1] for fr in (4900, 4903, 4911, 4912, 4914, 4915, 5000)] == [0, 1, 1, 0, 0, 1, 1]
     assert not SubsetFile(text=_text("mechanism_optical_flow")).features.any()
 
 
