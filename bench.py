@@ -185,8 +185,8 @@ def cpu_sample(p, ref, frames, n_sample, nthreads, timed_frames=1, uncertainty=F
 SIMPLEX_FLOP_PER_PIXEL_EVAL = 200.0
 # DRAM bytes (read + write) of one frame_kernel launch of the full frame
 # (158,404 subsets, a frame of the sequence), from an ncu capture of that
-# launch: dram__bytes_read.sum 156.0 MB + dram__bytes_write.sum 31.4 MB
-FRAME_KERNEL_DRAM_BYTES = 156.004e6 + 31.382e6
+# launch: dram__bytes_read.sum 157.6 MB + dram__bytes_write.sum 38.2 MB
+FRAME_KERNEL_DRAM_BYTES = 157.641e6 + 38.175e6
 
 
 def oracle_sequence_sample(p, ref_h, frames_h, stride, nthreads, uncertainty=False, library=None):
@@ -1234,8 +1234,8 @@ def main():
             "frac": fp32_tflops / fp32_peak if (fp32_peak and fp32_tflops) else None,
             "traffic": FRAME_KERNEL_DRAM_BYTES,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one frame_kernel launch "
-                              "on a full frame (reads 156.0 MB, writes 31.4 MB)",
-            "issue": {"inst_per_cycle_per_scheduler": 0.41, "warp_instructions_per_frame": 29.0e9,
+                              "on a full frame (reads 157.6 MB, writes 38.2 MB)",
+            "issue": {"inst_per_cycle_per_scheduler": 0.43, "warp_instructions_per_frame": 28.9e9,
                       "source": "ncu smsp__issue_active / smsp__inst_executed.sum of the same capture; the "
                                 "binding resource is instruction issue, not a math pipe or DRAM"},
             "kernel": "frame_kernel (median step time incl. the gradient and pack kernels)",

@@ -360,7 +360,6 @@ struct Engine {
     Ctl& c = ctl();
     const WarpOut<SHAPE>* wo = wouts<SHAPE>();
     const int NW = T >> 5;
-    constexpr int NM = L::NMAX;
     for (int e = lane; e < N * N; e += 32) {
       const int a = e / N, b = e - a * N;
       const int i = P.slot[a], j = P.slot[b];
@@ -399,95 +398,76 @@ struct Engine {
       if (lane == 0) c.status = DICEGPU_HESSIAN_SINGULAR;
       return;
     }
-    // LU with partial pivoting: lane a holds row a (the unblocked DGETRF
-    // operations, lane-parallel within a column step)
-    double h[NM];
-#pragma unroll
-    for (int j = 0; j < NM; ++j) h[j] = (lane < N && j < N) ? c.H[lane * N + j] : 0.0;
+    // LU with partial pivoting in place in c.H (the unblocked DGETRF steps:
+    // IDAMAX, the row swap, the scaling by the pivot's reciprocal, the rank-1
+    // update), then the inverse a column per lane, x = U^-1 L^-1 P e_lane.
+    // Rolled loops over shared memory: the solve runs once per iteration on
+    // one warp, and a short loop stays in the instruction cache.
     int info = 0;
-#pragma unroll
-    for (int j = 0; j < NM; ++j) {
-      if (j < N) {
-        // first row of maximal |a_ij| at or below the diagonal (IDAMAX)
-        double best = __shfl_sync(FULL, fabs(h[j]), j);
-        int p = j;
-#pragma unroll
-        for (int i = j + 1; i < NM; ++i) {
-          const double ai = __shfl_sync(FULL, fabs(h[j]), i);
-          if (i < N && ai > best) { best = ai; p = i; }
-        }
-        if (lane == 0) c.piv[j] = p;
-        const double pv = __shfl_sync(FULL, h[j], p);
-        if (pv != 0.0) {
-          if (p != j) {
-            const int src = lane == j ? p : (lane == p ? j : lane);
-#pragma unroll
-            for (int kx = 0; kx < NM; ++kx) h[kx] = __shfl_sync(FULL, h[kx], src);
-          }
-          const double r = 1.0 / pv;
-          if (lane > j && lane < N) h[j] = h[j] * r;
-        } else if (info == 0) {
-          info = j + 1;
-        }
-#pragma unroll
-        for (int kx = j + 1; kx < NM; ++kx) {
-          const double prow = __shfl_sync(FULL, h[kx], j);
-          if (kx < N && lane > j && lane < N) h[kx] = h[kx] - h[j] * prow;
-        }
+#pragma unroll 1
+    for (int j = 0; j < N; ++j) {
+      double best = fabs(c.H[j * N + j]);
+      int p = j;
+#pragma unroll 1
+      for (int i = j + 1; i < N; ++i) {
+        const double ai = fabs(c.H[i * N + j]);
+        if (ai > best) { best = ai; p = i; }
       }
+      const double pv = c.H[p * N + j];
+      __syncwarp();
+      if (lane == 0) c.piv[j] = p;
+      if (pv != 0.0) {
+        if (p != j && lane < N) {
+          const double t = c.H[j * N + lane];
+          c.H[j * N + lane] = c.H[p * N + lane];
+          c.H[p * N + lane] = t;
+        }
+        __syncwarp();
+        const double r = 1.0 / pv;
+        if (lane > j && lane < N) c.H[lane * N + j] = c.H[lane * N + j] * r;
+      } else if (info == 0) {
+        info = j + 1;
+      }
+      __syncwarp();
+      const int m = N - 1 - j;
+#pragma unroll 1
+      for (int e = lane; e < m * m; e += 32) {
+        const int i = j + 1 + e / m, kx = j + 1 + (e - (e / m) * m);
+        c.H[i * N + kx] = c.H[i * N + kx] - c.H[i * N + j] * c.H[j * N + kx];
+      }
+      __syncwarp();
     }
-    __syncwarp();
-    if (lane < N) {
-#pragma unroll
-      for (int j = 0; j < NM; ++j)
-        if (j < N) c.H[lane * N + j] = h[j];
-    }
-    __syncwarp();
     if (info == 0 && lane < N) {
-      // column `lane` of the inverse: x = U^-1 L^-1 P e_lane
-      double col[NM];
-#pragma unroll
-      for (int i = 0; i < NM; ++i) col[i] = (i == lane) ? 1.0 : 0.0;
-#pragma unroll
-      for (int j = 0; j < NM; ++j) {
-        if (j < N) {
-          const int pj = c.piv[j];
-          if (pj != j) {
-#pragma unroll
-            for (int i = j + 1; i < NM; ++i)
-              if (i == pj) {
-                const double t = col[i];
-                col[i] = col[j];
-                col[j] = t;
-              }
-          }
-        }
+      double* x = ctl_inv<SHAPE>(c) + lane;     // column `lane`, stride N
+      int pos = lane;                           // P e_lane is a unit vector
+#pragma unroll 1
+      for (int j = 0; j < N; ++j) {
+        const int pj = c.piv[j];
+        if (pos == j) pos = pj;
+        else if (pos == pj) pos = j;
       }
-#pragma unroll
-      for (int i = 1; i < NM; ++i) {
-        if (i < N) {
-#pragma unroll
-          for (int j = 0; j < i; ++j) col[i] = col[i] - c.H[i * N + j] * col[j];
-        }
+#pragma unroll 1
+      for (int i = 0; i < N; ++i) x[i * N] = i == pos ? 1.0 : 0.0;
+#pragma unroll 1
+      for (int i = 1; i < N; ++i) {
+        double acc = x[i * N];
+#pragma unroll 1
+        for (int j = 0; j < i; ++j) acc = acc - c.H[i * N + j] * x[j * N];
+        x[i * N] = acc;
       }
-#pragma unroll
-      for (int i = NM - 1; i >= 0; --i) {
-        if (i < N) {
-#pragma unroll
-          for (int j = i + 1; j < NM; ++j)
-            if (j < N) col[i] = col[i] - c.H[i * N + j] * col[j];
-          col[i] = col[i] / c.H[i * N + i];
-        }
+#pragma unroll 1
+      for (int i = N - 1; i >= 0; --i) {
+        double acc = x[i * N];
+#pragma unroll 1
+        for (int j = i + 1; j < N; ++j) acc = acc - c.H[i * N + j] * x[j * N];
+        x[i * N] = acc / c.H[i * N + i];
       }
-#pragma unroll
-      for (int i = 0; i < NM; ++i)
-        if (i < N) c.inv[i * N + lane] = col[i];
     }
     __syncwarp();
     bool notc = false;
     float nw = 0.0f;
     if (lane < N) {
-      const double* Mrow = info == 0 ? &c.inv[lane * N] : &c.H[lane * N];
+      const double* Mrow = info == 0 ? ctl_inv<SHAPE>(c) + lane * N : &c.H[lane * N];
       float du = 0.0f;
       for (int j = 0; j < N; ++j) du = (float)((double)du + (Mrow[j] * (-1.0)) * c.q[j]);
       if (P.momentum != 0.0f) {
@@ -804,12 +784,15 @@ struct Engine {
   // Subset::noise_std_dev (DICe_Subset.cpp:622-703) on the deformed image
   // over the box of the last pass's live pixels moved by (u, v): the 3 x 3
   // Immerkaer mask (j outer, i inner), |.| summed in float, row by row.  The
-  // terms are computed by the CTA a chunk at a time into row 0 and summed in
-  // order by one thread.  Reads go through the row-major linear index like
-  // the reference's operator() (0 outside the array).
-  __device__ float noise_exact(const SubsetRef& sb, const float* slots, int n, int bminx, int bmaxx, int bminy,
-                               int bmaxy) {
-    if (n == 0) return -1.0f;
+  // terms are computed by the CTA a chunk at a time and summed in order by
+  // one thread.  Reads go through the row-major linear index like the
+  // reference's operator() (0 outside the array).
+  struct NoiseBox {
+    int min_x, min_y, rw, rh, ww, hh;
+    __device__ long total() const { return (rw > 0 && rh > 0) ? (long)rw * rh : 0; }
+  };
+  __device__ NoiseBox noise_box(const SubsetRef& sb, const float* slots, int bminx, int bmaxx, int bminy,
+                                int bmaxy) const {
     MapConst k;
     make_mapconst<SHAPE>(slots, false, (float)sb.cx, (float)sb.cy, k);
     float u, v, t;
@@ -821,55 +804,63 @@ struct Engine {
     if (min_y < 0) min_y = 0;
     if (max_x >= img_w) min_x = 0;
     if (max_y >= img_h) min_y = 0;
-    int hh = max_y - min_y + 1, ww = max_x - min_x + 1;
-    if (ww < 3) ww = 3;
-    if (hh < 3) hh = 3;
-    const int rw = max_x - min_x, rh = max_y - min_y;
-    float variance = 0.0f;
-    if (rw > 0 && rh > 0) {
-      const long lim = (long)img_w * img_h;
-      const float* I = A.def.I;
-      auto ld = [&](long li) -> float { return (li >= 0 && li < lim) ? __ldg(I + li) : 0.0f; };
-      const long total = (long)rw * rh;
-      const int chunk = A.npix_cap;
-      float* buf = arrays().R(0);
-      Ctl& c = ctl();
-      for (long b0 = 0; b0 < total; b0 += chunk) {
-        const int m = (int)min((long)chunk, total - b0);
-        for (int e = tid; e < m; e += T) {
-          const long id = b0 + e;
-          const int yy = min_y + (int)(id / rw), xx = min_x + (int)(id % rw);
-          float val;
-          if (xx < 1 || xx >= img_w - 1 || yy < 1 || yy >= img_h - 1) {
-            const float a = ld((long)yy * img_w + xx);
-            val = __fsqrt_rn(a * a);
-          } else {
-            // mask[i][j] = {{1,-2,1},{-2,4,-2},{1,-2,1}}, i: x offset, j: y offset
-            const float* q = I + (size_t)(yy - 1) * img_w + (xx - 1);
-            float conv = 0.0f;
-            conv = conv + __ldg(q) * 1.0f;
-            conv = conv + __ldg(q + 1) * -2.0f;
-            conv = conv + __ldg(q + 2) * 1.0f;
-            q += img_w;
-            conv = conv + __ldg(q) * -2.0f;
-            conv = conv + __ldg(q + 1) * 4.0f;
-            conv = conv + __ldg(q + 2) * -2.0f;
-            q += img_w;
-            conv = conv + __ldg(q) * 1.0f;
-            conv = conv + __ldg(q + 1) * -2.0f;
-            conv = conv + __ldg(q + 2) * 1.0f;
-            val = fabsf(conv);
-          }
-          buf[e] = val;
-        }
-        __syncthreads();
-        if (tid == 0) c.fres[0] = chain_sum(buf, m, variance);
-        __syncthreads();
-        variance = c.fres[0];
-        __syncthreads();
-      }
+    NoiseBox nb;
+    nb.hh = max(max_y - min_y + 1, 3);
+    nb.ww = max(max_x - min_x + 1, 3);
+    nb.min_x = min_x;
+    nb.min_y = min_y;
+    nb.rw = max_x - min_x;
+    nb.rh = max_y - min_y;
+    return nb;
+  }
+  // The term of box element `id` (row-major over rw x rh).
+  __device__ float noise_term(const NoiseBox& nb, long id) const {
+    const int img_w = A.def.w, img_h = A.def.h;
+    const float* I = A.def.I;
+    const int yy = nb.min_y + (int)(id / nb.rw), xx = nb.min_x + (int)(id % nb.rw);
+    if (xx < 1 || xx >= img_w - 1 || yy < 1 || yy >= img_h - 1) {
+      const long li = (long)yy * img_w + xx;
+      const float a = (li >= 0 && li < (long)img_w * img_h) ? __ldg(I + li) : 0.0f;
+      return __fsqrt_rn(a * a);
     }
-    return (float)((double)variance * (sqrt(0.5 * 3.14159265358979323846) / (6.0 * (ww - 2) * (hh - 2))));
+    // mask[i][j] = {{1,-2,1},{-2,4,-2},{1,-2,1}}, i: x offset, j: y offset
+    const float* q = I + (size_t)(yy - 1) * img_w + (xx - 1);
+    float conv = 0.0f;
+    conv = conv + __ldg(q) * 1.0f;
+    conv = conv + __ldg(q + 1) * -2.0f;
+    conv = conv + __ldg(q + 2) * 1.0f;
+    q += img_w;
+    conv = conv + __ldg(q) * -2.0f;
+    conv = conv + __ldg(q + 1) * 4.0f;
+    conv = conv + __ldg(q + 2) * -2.0f;
+    q += img_w;
+    conv = conv + __ldg(q) * 1.0f;
+    conv = conv + __ldg(q + 1) * -2.0f;
+    conv = conv + __ldg(q + 2) * 1.0f;
+    return fabsf(conv);
+  }
+  __device__ static float noise_scale(const NoiseBox& nb, float variance) {
+    return (float)((double)variance * (sqrt(0.5 * 3.14159265358979323846) / (6.0 * (nb.ww - 2) * (nb.hh - 2))));
+  }
+  __device__ float noise_exact(const SubsetRef& sb, const float* slots, int n, int bminx, int bmaxx, int bminy,
+                               int bmaxy) {
+    if (n == 0) return -1.0f;
+    const NoiseBox nb = noise_box(sb, slots, bminx, bmaxx, bminy, bmaxy);
+    float variance = 0.0f;
+    const long total = nb.total();
+    const int chunk = A.npix_cap;
+    float* buf = arrays().R(0);
+    Ctl& c = ctl();
+    for (long b0 = 0; b0 < total; b0 += chunk) {
+      const int m = (int)min((long)chunk, total - b0);
+      for (int e = tid; e < m; e += T) buf[e] = noise_term(nb, b0 + e);
+      __syncthreads();
+      if (tid == 0) c.fres[0] = chain_sum(buf, m, variance);
+      __syncthreads();
+      variance = c.fres[0];
+      __syncthreads();
+    }
+    return noise_scale(nb, variance);
   }
 
   // Objective::sigma (DICe_Objective.cpp:150-184) at the state of the last
@@ -904,8 +895,24 @@ struct Engine {
       T1[p] = b;
     }
     float s[2];
-    chains(2, T0, T1, nullptr, nullptr, nullptr, 0u, sb.npix, s);
-    noise = noise_exact(sb, slots, n, bx0, bx1, by0, by1);
+    const NoiseBox nb = noise_box(sb, slots, bx0, bx1, by0, by1);
+    if (PixRows<SHAPE>::NR >= 3 && n > 0 && nb.total() <= A.npix_cap) {
+      // the noise terms in row 2, and the three sums side by side
+      float* T2 = X.R(2);
+      const int nt = (int)nb.total();
+      for (int e = tid; e < nt; e += T) T2[e] = noise_term(nb, e);
+      Ctl& cl = ctl();
+      __syncthreads();
+      if (tid < 3) cl.fres[tid] = chain_sum(tid == 0 ? T0 : tid == 1 ? T1 : T2, tid == 2 ? nt : sb.npix);
+      __syncthreads();
+      s[0] = cl.fres[0];
+      s[1] = cl.fres[1];
+      noise = noise_scale(nb, cl.fres[2]);
+      __syncthreads();
+    } else {
+      chains(2, T0, T1, nullptr, nullptr, nullptr, 0u, sb.npix, s);
+      noise = noise_exact(sb, slots, n, bx0, bx1, by0, by1);
+    }
     if (noise < 0.0f) return -1.0f;
     const float sg = s[0] > s[1] ? s[1] : s[0];
     return sg > 0.0f ? (float)sqrt(2.0 * (double)noise * (double)noise / (double)sg) : -1.0f;
@@ -1197,7 +1204,7 @@ struct Engine {
     if (A.passes_out && tid == 0 && A.mode == MODE_CORRELATE) A.passes_out[idx] = npass_;
   }
 
-  __device__ void run_subset(int idx) {
+  __device__ __noinline__ void run_subset(int idx) {
     const DevParams& P = A.P;
     double* f = A.fields + (size_t)idx * DICEGPU_FIELD_STRIDE;
     // the subset's field row (32 doubles) in one coalesced load per warp:

@@ -75,11 +75,19 @@ struct __align__(16) Ctl {
   float upd_old[12];             // momentum: the previous update (compact order)
   float cond;
   float pad1[3];
-  double H[144];                 // Hessian (compact order, row major), then its LU factors
+  double red[8];                 // cta_sum's per-warp partial sums
   double q[12];
-  double inv[144];               // inverse, column k written by lane k
   int piv[12];
+  // the Hessian (compact order, row major, then its LU factors) in the first
+  // NS * NS entries, its inverse (column k written by lane k) in the next
+  // NS * NS; the CTA's shared memory holds only the shape function's share
+  double H[2 * 144];
 };
+// the inverse's place in Ctl::H
+template <int SHAPE>
+__device__ __forceinline__ double* ctl_inv(Ctl& c) {
+  return c.H + Layout<SHAPE>::NS * Layout<SHAPE>::NS;
+}
 
 // Per-warp partial results of a pass.
 template <int SHAPE>
@@ -126,11 +134,15 @@ struct PixRows {
 };
 template <int SHAPE>
 struct SmemPlan {
-  static __host__ __device__ size_t wout(int) { return a16(sizeof(Ctl)); }
+  // Ctl up to the shape function's share of H (Hessian and inverse)
+  static __host__ __device__ size_t wout(int) {
+    return a16(offsetof(Ctl, H) + 2 * sizeof(double) * Layout<SHAPE>::NS * Layout<SHAPE>::NS);
+  }
   static __host__ __device__ size_t simplex(int W) { return wout(W) + a16((size_t)W * sizeof(WarpOut<SHAPE>)); }
   static __host__ __device__ size_t vbuf(int W) { return simplex(W) + a16((size_t)W * sizeof(SimplexState)); }
+  // the sweeps' staging rows: only when the residual vectors are not stored
   static __host__ __device__ size_t pix(int W) {
-    return vbuf(W) + a16((size_t)W * 32 * Layout<SHAPE>::VS * sizeof(float));
+    return vbuf(W) + (PixRows<SHAPE>::RESID ? 0 : a16((size_t)W * 32 * Layout<SHAPE>::VS * sizeof(float)));
   }
   // F, G and the stored rows (floats, pix_stride apart), then one byte per pixel
   static __host__ __device__ size_t pix_bytes(int cap) {
@@ -194,16 +206,16 @@ __device__ __forceinline__ PixArrays pix_arrays_at(float* b, int cap) {
 // CTA reductions and sequential float sums (fixed order: deterministic)
 // ---------------------------------------------------------------------------
 // CTA-wide double sum of one value per thread, the same in every thread.
-// Uses Ctl's inv[] as scratch; starts and ends with a barrier.
+// Uses Ctl's red[] as scratch; starts and ends with a barrier.
 __device__ __forceinline__ double cta_sum(double v) {
   Ctl& c = ctl();
   v = warp_sum(v);
   __syncthreads();
-  if ((threadIdx.x & 31) == 0) c.inv[threadIdx.x >> 5] = v;
+  if ((threadIdx.x & 31) == 0) c.red[threadIdx.x >> 5] = v;
   __syncthreads();
   double s = 0.0;
   const int W = blockDim.x >> 5;
-  for (int w = 0; w < W; ++w) s += c.inv[w];
+  for (int w = 0; w < W; ++w) s += c.red[w];
   __syncthreads();
   return s;
 }
@@ -214,41 +226,66 @@ __device__ __forceinline__ int cta_sum_i(int v) {
 // Sequential float sum a[0] + a[1] + ... + a[n-1] starting from 0.0f, each
 // addition rounded: the reference's `sum += x` loop.  a is 16-byte aligned.
 // Zeros stand for skipped pixels: adding +0.0f leaves every running sum
-// unchanged (the sum, starting at +0.0f, is never -0.0f).
-__device__ __forceinline__ float chain_sum(const float* a, int n, float s = 0.0f) {
-  int i = 0;
+// unchanged (the sum, starting at +0.0f, is never -0.0f).  The next 16
+// values are loaded while the current 16 are added, so the chain runs at the
+// addition's latency rather than the shared-memory load's.
+#define DG_ADD4(s, v)        \
+  s = __fadd_rn(s, (v).x); \
+  s = __fadd_rn(s, (v).y); \
+  s = __fadd_rn(s, (v).z); \
+  s = __fadd_rn(s, (v).w)
+static __device__ __noinline__ float chain_sum(const float* a, int n, float s = 0.0f) {
   const float4* a4 = reinterpret_cast<const float4*>(a);
-#pragma unroll 4
-  for (; i + 4 <= n; i += 4) {
-    const float4 v = a4[i >> 2];
-    s = __fadd_rn(s, v.x);
-    s = __fadd_rn(s, v.y);
-    s = __fadd_rn(s, v.z);
-    s = __fadd_rn(s, v.w);
+  const int nq = n >> 2;
+  int q = 0;
+  if (nq >= 4) {
+    float4 v0 = a4[0], v1 = a4[1], v2 = a4[2], v3 = a4[3];
+    for (q = 4; q + 4 <= nq; q += 4) {
+      const float4 w0 = a4[q], w1 = a4[q + 1], w2 = a4[q + 2], w3 = a4[q + 3];
+      DG_ADD4(s, v0); DG_ADD4(s, v1); DG_ADD4(s, v2); DG_ADD4(s, v3);
+      v0 = w0; v1 = w1; v2 = w2; v3 = w3;
+    }
+    DG_ADD4(s, v0); DG_ADD4(s, v1); DG_ADD4(s, v2); DG_ADD4(s, v3);
   }
-  for (; i < n; ++i) s = __fadd_rn(s, a[i]);
+  for (; q < nq; ++q) {
+    const float4 v = a4[q];
+    DG_ADD4(s, v);
+  }
+  for (int i = nq << 2; i < n; ++i) s = __fadd_rn(s, a[i]);
   return s;
 }
 
 // The same over the pixels whose liveness byte has `bit` set (the others
 // count as +0.0f); a and m are 16- and 4-byte aligned.
-__device__ __forceinline__ float chain_sum_masked(const float* a, const uint8_t* m, unsigned bit, int n) {
+__device__ __forceinline__ float4 masked4(float4 v, uchar4 b, unsigned bit) {
+  return make_float4((b.x & bit) ? v.x : 0.0f, (b.y & bit) ? v.y : 0.0f, (b.z & bit) ? v.z : 0.0f,
+                     (b.w & bit) ? v.w : 0.0f);
+}
+static __device__ __noinline__ float chain_sum_masked(const float* a, const uint8_t* m, unsigned bit, int n) {
   float s = 0.0f;
-  int i = 0;
   const float4* a4 = reinterpret_cast<const float4*>(a);
   const uchar4* m4 = reinterpret_cast<const uchar4*>(m);
-#pragma unroll 4
-  for (; i + 4 <= n; i += 4) {
-    const float4 v = a4[i >> 2];
-    const uchar4 b = m4[i >> 2];
-    s = __fadd_rn(s, (b.x & bit) ? v.x : 0.0f);
-    s = __fadd_rn(s, (b.y & bit) ? v.y : 0.0f);
-    s = __fadd_rn(s, (b.z & bit) ? v.z : 0.0f);
-    s = __fadd_rn(s, (b.w & bit) ? v.w : 0.0f);
+  const int nq = n >> 2;
+  int q = 0;
+  if (nq >= 4) {
+    float4 v0 = masked4(a4[0], m4[0], bit), v1 = masked4(a4[1], m4[1], bit);
+    float4 v2 = masked4(a4[2], m4[2], bit), v3 = masked4(a4[3], m4[3], bit);
+    for (q = 4; q + 4 <= nq; q += 4) {
+      const float4 w0 = masked4(a4[q], m4[q], bit), w1 = masked4(a4[q + 1], m4[q + 1], bit);
+      const float4 w2 = masked4(a4[q + 2], m4[q + 2], bit), w3 = masked4(a4[q + 3], m4[q + 3], bit);
+      DG_ADD4(s, v0); DG_ADD4(s, v1); DG_ADD4(s, v2); DG_ADD4(s, v3);
+      v0 = w0; v1 = w1; v2 = w2; v3 = w3;
+    }
+    DG_ADD4(s, v0); DG_ADD4(s, v1); DG_ADD4(s, v2); DG_ADD4(s, v3);
   }
-  for (; i < n; ++i) s = __fadd_rn(s, (m[i] & bit) ? a[i] : 0.0f);
+  for (; q < nq; ++q) {
+    const float4 v = masked4(a4[q], m4[q], bit);
+    DG_ADD4(s, v);
+  }
+  for (int i = nq << 2; i < n; ++i) s = __fadd_rn(s, (m[i] & bit) ? a[i] : 0.0f);
   return s;
 }
+#undef DG_ADD4
 
 // Up to four chains at once (lanes 0..k-1 of warp 0, in lockstep), chain i
 // over the pixels whose liveness byte in m has a bit of byte i of `bits` set
