@@ -1724,6 +1724,24 @@ static int frame_plan_kind(const dicegpu_ctx* c) {
 // initialization reads the same way.  Runs of waves that hold a single
 // subset without blocked polygons (a neighbour chain) go to one launch of
 // a single warp, which takes them in order.  Everything is enqueued.
+// A chain of single-subset waves runs alone on the GPU, one subset after the
+// other: its CTA takes the most warps the frame kernel allows (the passes and
+// sweeps split over more warps; the sequential sums and the solve do not),
+// when their shared memory fits.
+static void chain_shape(dicegpu_ctx* c, FrameKernelFn fn, int* warps, size_t* smem) {
+  const int w = DG_MAX_THREADS / 32;
+  if (w <= *warps) return;
+  size_t fixed, pix;
+  frame_smem_bytes(c, w, &fixed, &pix);
+  const size_t s = c->pix_in_global ? fixed : fixed + pix;
+  if (s > (size_t)c->smem_optin) return;
+  if (s > *smem &&
+      cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s) != cudaSuccess)
+    return;
+  *warps = w;
+  *smem = s;
+}
+
 static int run_waves(dicegpu_ctx* c, int kind, FrameKernelFn fn, int blocks, size_t smem) {
   int rc;
   if ((kind & 1) && (rc = ensure_blocking_desc(c))) return rc;
@@ -1773,8 +1791,11 @@ static int run_waves(dicegpu_ctx* c, int kind, FrameKernelFn fn, int blocks, siz
       a.order = pl.d_wave.p + pl.wave_off[L];
       a.n_order = pl.wave_off[L1] - pl.wave_off[L];
       a.queue_mode = 0;
+      int cw = c->warps_per_cta;
+      size_t csmem = smem;
+      chain_shape(c, fn, &cw, &csmem);
       CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
-      fn<<<1, c->warps_per_cta * 32, smem, c->stream>>>(a);
+      fn<<<1, cw * 32, csmem, c->stream>>>(a);
       CK(cudaGetLastError());
       c->launches += 1;
       L = L1;
