@@ -476,8 +476,12 @@ int dicegpu_autotune(dicegpu_ctx* ctx, int* warps_per_cta, int* ctas_per_sm, flo
 /* Number of kernel launches this context issued since creation. */
 int dicegpu_launch_count(dicegpu_ctx* ctx, int64_t* count);
 
-/* Launch shape of the persistent kernel: warps (subsets in flight) per CTA
- * and CTAs per SM; 0 keeps the current value.  The tile capacity is derived. */
+/* Launch shape of the persistent kernel: warps per CTA (one CTA solves one
+ * subset at a time; 1-8, default 4) and CTAs per SM (0: as many as fit); 0
+ * keeps the current value.  Until a shape is set here or by
+ * dicegpu_autotune, a launch with at most six subsets per default-shape CTA
+ * (small tracking waves, small frames, per-subset launches) and a chain of
+ * single-subset waves run on CTAs of eight warps. */
 int dicegpu_set_launch_shape(dicegpu_ctx* ctx, int warps_per_cta, int ctas_per_sm);
 int dicegpu_get_launch_shape(dicegpu_ctx* ctx, int* warps_per_cta, int* ctas_per_sm);
 
