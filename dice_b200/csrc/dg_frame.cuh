@@ -89,6 +89,16 @@ DG_DECLARE_FRAME_FN(1, 0, 0) DG_DECLARE_FRAME_FN(1, 1, 0) DG_DECLARE_FRAME_FN(1,
 DG_DECLARE_FRAME_FN(0, 0, 1) DG_DECLARE_FRAME_FN(0, 1, 1) DG_DECLARE_FRAME_FN(0, 2, 1)
 DG_DECLARE_FRAME_FN(1, 0, 1) DG_DECLARE_FRAME_FN(1, 1, 1) DG_DECLARE_FRAME_FN(1, 2, 1)
 
+#ifdef DG_PROFILE
+// profiling builds: each unit adds its section timers into acc16 and clears them
+#define DG_FRAME_PROF_NAME(S, I, M) frame_prof_s##S##_i##I##_m##M
+#define DG_DECLARE_FRAME_PROF(S, I, M) int DG_FRAME_PROF_NAME(S, I, M)(unsigned long long* acc16);
+DG_DECLARE_FRAME_PROF(0, 0, 0) DG_DECLARE_FRAME_PROF(0, 1, 0) DG_DECLARE_FRAME_PROF(0, 2, 0)
+DG_DECLARE_FRAME_PROF(1, 0, 0) DG_DECLARE_FRAME_PROF(1, 1, 0) DG_DECLARE_FRAME_PROF(1, 2, 0)
+DG_DECLARE_FRAME_PROF(0, 0, 1) DG_DECLARE_FRAME_PROF(0, 1, 1) DG_DECLARE_FRAME_PROF(0, 2, 1)
+DG_DECLARE_FRAME_PROF(1, 0, 1) DG_DECLARE_FRAME_PROF(1, 1, 1) DG_DECLARE_FRAME_PROF(1, 2, 1)
+#endif
+
 // The frame kernel of a configuration (nullptr for one this build leaves
 // out: a unit compiled with DG_ONLY_BENCH_KERNEL returns only the affine /
 // Keys-4 / deformed-gradient kernel).

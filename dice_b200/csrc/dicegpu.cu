@@ -2516,11 +2516,16 @@ extern "C" int dicegpu_correlate_reset(void) {
 }
 
 #ifdef DG_PROFILE
-// profiling builds only: read and clear the section timers
+// profiling builds only: read and clear the section timers of every frame
+// kernel unit (cycles summed over the units)
 extern "C" int dicegpu_prof_read(unsigned long long* out16) {
-  if (cudaMemcpyFromSymbol(out16, g_prof, 16 * sizeof(unsigned long long)) != cudaSuccess) return DICEGPU_ERR_CUDA;
-  unsigned long long z[16] = {};
-  if (cudaMemcpyToSymbol(g_prof, z, sizeof(z)) != cudaSuccess) return DICEGPU_ERR_CUDA;
-  return DICEGPU_OK;
+  unsigned long long acc[16] = {};
+  int bad = 0;
+  bad |= DG_FRAME_PROF_NAME(0, 0, 0)(acc) | DG_FRAME_PROF_NAME(0, 1, 0)(acc) | DG_FRAME_PROF_NAME(0, 2, 0)(acc);
+  bad |= DG_FRAME_PROF_NAME(1, 0, 0)(acc) | DG_FRAME_PROF_NAME(1, 1, 0)(acc) | DG_FRAME_PROF_NAME(1, 2, 0)(acc);
+  bad |= DG_FRAME_PROF_NAME(0, 0, 1)(acc) | DG_FRAME_PROF_NAME(0, 1, 1)(acc) | DG_FRAME_PROF_NAME(0, 2, 1)(acc);
+  bad |= DG_FRAME_PROF_NAME(1, 0, 1)(acc) | DG_FRAME_PROF_NAME(1, 1, 1)(acc) | DG_FRAME_PROF_NAME(1, 2, 1)(acc);
+  std::memcpy(out16, acc, sizeof(acc));
+  return bad ? DICEGPU_ERR_CUDA : DICEGPU_OK;
 }
 #endif

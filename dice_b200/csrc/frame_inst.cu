@@ -27,4 +27,15 @@ FrameKernelFn DG_CAT_FN(DG_INST_SHAPE, DG_INST_INTERP, DG_INST_MASK)(bool defgra
 #endif
 }
 
+#ifdef DG_PROFILE
+#define DG_CAT_PROF(S, I, M) DG_FRAME_PROF_NAME(S, I, M)
+int DG_CAT_PROF(DG_INST_SHAPE, DG_INST_INTERP, DG_INST_MASK)(unsigned long long* acc16) {
+  unsigned long long v[16];
+  if (cudaMemcpyFromSymbol(v, g_prof, sizeof(v)) != cudaSuccess) return 1;
+  for (int i = 0; i < 16; ++i) acc16[i] += v[i];
+  const unsigned long long z[16] = {};
+  return cudaMemcpyToSymbol(g_prof, z, sizeof(z)) != cudaSuccess ? 1 : 0;
+}
+#endif
+
 }  // namespace dg
