@@ -30,6 +30,8 @@ Sources (paths inside the DICe project):
   tests/regression/{parallel_seed_first_step_only, parallel_subsets_seed}/
       {subset_file.dat, gold/DICe_solution_*.txt}
   tests/regression/incremental/gold/DICe_solution_{0..5}.txt
+  tests/regression/bitmap_star/{images/DIC_Challenge_Wave_*_Noisy.bmp,
+      gold/DICe_solution_0.txt}                                   (2000 x 501)
 """
 import os
 import sys
@@ -163,7 +165,29 @@ def main(root):
     for k in range(6):
         with open(os.path.join(root, "tests", "regression", "incremental", "gold", "DICe_solution_%d.txt" % k)) as fh:
             out["incremental_gold_text_%d" % k] = np.array(fh.read())
-    path =os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_gold.npz")
+    # bitmap_star: the DIC challenge wave pair (8-bit BMP, 2000 x 501; the
+    # reference image is the "Deformed" file, as its input.xml names them),
+    # subset 31 at step 25, KEYS_FOURTH, GRADIENT_BASED, translation only.
+    # Its gold prints UNCERTAINTY = SIGMA / FIELD_1 (Uncertainty_Post_Processor,
+    # DICe_PostProcessor.cpp:1507-1537).  Kept: every 20th gold row and a
+    # 45 x 45 patch of each image centred on those subsets (the subset's
+    # pixels, the interpolation taps, the gradient stencil and the noise box
+    # all fit), cut from the images padded by 22 zero pixels.
+    bs = os.path.join(root, "tests", "regression", "bitmap_star")
+    from PIL import Image
+    pair = [np.asarray(Image.open(os.path.join(bs, "images", nm)).convert("L"), dtype=np.uint8)
+            for nm in ("DIC_Challenge_Wave_Deformed_Noisy.bmp", "DIC_Challenge_Wave_Reference_Noisy.bmp")]
+    with open(os.path.join(bs, "gold", "DICe_solution_0.txt")) as fh:
+        lines = fh.read().strip().splitlines()
+    gold = np.array([[float(t) for t in ln.split(",")] for ln in lines[1:]])[::20]
+    out["bitmap_star_columns"] = np.array(lines[0])
+    out["bitmap_star_gold"] = gold
+    out["bitmap_star_shape"] = np.array(pair[0].shape, np.int32)
+    for key, img in zip(("ref", "def"), pair):
+        padded = np.pad(img, 22)
+        out["bitmap_star_%s_patches" % key] = np.stack([
+            padded[int(y):int(y) + 45, int(x):int(x) + 45] for x, y in gold[:, 1:3]])
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_gold.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, {k: v.shape for k, v in out.items()})
 

@@ -4,7 +4,8 @@ Gauss-Newton solve converges.
 
 CPU: the oracle's restatement against an independent numpy evaluation of the
 same formulas (reference-gradient mode, where the subset's gradients are the
-reference image's at the pixel).  GPU: parity with the oracle in both gradient
+reference image's at the pixel), and both against the bitmap_star regression's
+gold (its UNCERTAINTY column is SIGMA / FIELD_1).  GPU: parity with the oracle in both gradient
 modes through the C ABI.
 """
 import ctypes
@@ -72,6 +73,62 @@ def test_oracle_uncertainty_matches_formulas():
         assert np.allclose(got, want, rtol=2e-4, atol=1e-6), (i, got, want)
 
 
+# ---- pinned to the reference: bitmap_star --------------------------------------
+# The regression's gold prints UNCERTAINTY = SIGMA / FIELD_1 for 2-D results
+# (Uncertainty_Post_Processor::execute, DICe_PostProcessor.cpp:1507-1537), so
+# FIELD_1 = SIGMA / UNCERTAINTY is a reference vector of computeUncertaintyFields'
+# first field.  Fixture: every 20th gold row and 45 x 45 patches of the DIC
+# challenge wave pair around those subsets (tests/golden/make_fixtures.py).
+
+def _bitmap_star():
+    import os
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_gold.npz"))
+    cols = {c: i for i, c in enumerate(str(gold["bitmap_star_columns"]).split(","))}
+    rows = gold["bitmap_star_gold"]
+    h, w = (int(v) for v in gold["bitmap_star_shape"])
+    imgs = []
+    for key in ("ref", "def"):
+        canvas = np.zeros((h + 44, w + 44), np.float32)
+        for (x, y), patch in zip(rows[:, 1:3].astype(int), gold["bitmap_star_%s_patches" % key]):
+            canvas[y:y + 45, x:x + 45] = patch
+        imgs.append(canvas[22:22 + h, 22:22 + w].copy())
+    # file-fed images: the subsets keep the reference image's gradients
+    p = abi.default_params(subset_size=31, use_def_gradients=0, compute_uncertainty=1,
+                           optimization=abi.GRADIENT_BASED)
+    return imgs[0], imgs[1], rows, cols, p
+
+
+def test_uncertainty_formula_pinned_to_bitmap_star_gold():
+    ref, deff, rows, cols, p = _bitmap_star()
+    implied = rows[:, cols["SIGMA"]] / rows[:, cols["UNCERTAINTY"]]
+    got = []
+    for r in rows:
+        row = np.zeros(abi.FIELD_STRIDE)
+        row[abi.F_COORD_X], row[abi.F_COORD_Y] = r[cols["COORDINATE_X"]], r[cols["COORDINATE_Y"]]
+        row[abi.F_DISP_X], row[abi.F_DISP_Y] = r[cols["DISPLACEMENT_X"]], r[cols["DISPLACEMENT_Y"]]
+        got.append(_numpy_fields(ref, deff, p, row)[0])
+    rel = np.abs(np.array(got) - implied) / implied
+    # five printed digits of SIGMA, UNCERTAINTY, u and v (4.8e-5 reached)
+    assert rel.max() < 1e-4, rel.max()
+
+
+def test_oracle_uncertainty_against_bitmap_star_gold():
+    ref, deff, rows, cols, p = _bitmap_star()
+    f = np.zeros((len(rows), abi.FIELD_STRIDE))
+    f[:, abi.F_COORD_X] = rows[:, cols["COORDINATE_X"]]
+    f[:, abi.F_COORD_Y] = rows[:, cols["COORDINATE_Y"]]
+    unc = np.zeros((len(rows), U))
+    O.execute_frame(p, ref, deff, f, first_frame=True, nthreads=4, uncertainty=unc)
+    assert np.all(f[:, abi.F_STATUS] < 2)
+    # the reference started each solve from feature matching, these from zero:
+    # the solves stop within the 1e-4 px tolerance of each other
+    assert np.abs(f[:, abi.F_DISP_X] - rows[:, cols["DISPLACEMENT_X"]]).max() < 1e-4
+    assert np.abs(f[:, abi.F_DISP_Y] - rows[:, cols["DISPLACEMENT_Y"]]).max() < 1e-4
+    # where u and v stop apart, FIELD_1 moves with their direction
+    rel = np.abs(f[:, abi.F_SIGMA] / unc[:, 0] - rows[:, cols["UNCERTAINTY"]]) / rows[:, cols["UNCERTAINTY"]]
+    assert (rel < 1e-4).mean() > 0.95 and rel.max() < 1e-2, (np.median(rel), rel.max())
+
+
 def test_oracle_uncertainty_untouched_without_convergence():
     ref, deff, cx, cy, p = _case(use_def_gradients=0, optimization=abi.SIMPLEX)
     f = syn.init_fields(cx, cy)
@@ -116,6 +173,25 @@ def test_gpu_uncertainty_matches_oracle(defgrad):
         # agreement (FIELD_4/6 scale with the displacement)
         assert np.allclose(gu[ok, :7], unc[ok, :7], rtol=2e-3, atol=1e-5)
         assert np.all(gu[ok, 1] == 1.0)
+
+
+@pytest.mark.gpu
+def test_gpu_uncertainty_against_bitmap_star_gold():
+    _gpu()
+    from dice_b200.schema import Schema
+    ref, deff, rows, cols, p = _bitmap_star()
+    f = np.zeros((len(rows), abi.FIELD_STRIDE))
+    f[:, abi.F_COORD_X] = rows[:, cols["COORDINATE_X"]]
+    f[:, abi.F_COORD_Y] = rows[:, cols["COORDINATE_Y"]]
+    with Schema(p) as s:
+        s.set_ref_image(ref)
+        s.set_fields(f)
+        s.set_def_image(deff)
+        s.execute_correlation()
+        g, gu = s.fields(), s.uncertainty()
+    assert np.all(g[:, abi.F_STATUS] < 2)
+    rel = np.abs(g[:, abi.F_SIGMA] / gu[:, 0] - rows[:, cols["UNCERTAINTY"]]) / rows[:, cols["UNCERTAINTY"]]
+    assert (rel < 1e-4).mean() > 0.95 and rel.max() < 1e-2, (np.median(rel), rel.max())
 
 
 @pytest.mark.gpu
