@@ -127,6 +127,13 @@ def test_oracle_uncertainty_against_bitmap_star_gold():
     # where u and v stop apart, FIELD_1 moves with their direction
     rel = np.abs(f[:, abi.F_SIGMA] / unc[:, 0] - rows[:, cols["UNCERTAINTY"]]) / rows[:, cols["UNCERTAINTY"]]
     assert (rel < 1e-4).mean() > 0.95 and rel.max() < 1e-2, (np.median(rel), rel.max())
+    _check_sigma_gamma(f, rows, cols)
+
+
+def _check_sigma_gamma(f, rows, cols):
+    for name, c in (("SIGMA", abi.F_SIGMA), ("GAMMA", abi.F_GAMMA)):
+        rel = np.abs(f[:, c] - rows[:, cols[name]]) / rows[:, cols[name]]
+        assert (rel < 1e-4).mean() > 0.95 and rel.max() < 1e-2, (name, rel.max())
 
 
 def test_oracle_uncertainty_untouched_without_convergence():
@@ -192,6 +199,7 @@ def test_gpu_uncertainty_against_bitmap_star_gold():
     assert np.all(g[:, abi.F_STATUS] < 2)
     rel = np.abs(g[:, abi.F_SIGMA] / gu[:, 0] - rows[:, cols["UNCERTAINTY"]]) / rows[:, cols["UNCERTAINTY"]]
     assert (rel < 1e-4).mean() > 0.95 and rel.max() < 1e-2, (np.median(rel), rel.max())
+    _check_sigma_gamma(g, rows, cols)
 
 
 @pytest.mark.gpu
