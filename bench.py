@@ -992,6 +992,9 @@ def main():
     ap.add_argument("--profile-timed", action="store_true",
                     help="sequence workload: bracket the timed steps with cudaProfilerStart/Stop "
                          "(for ncu --profile-from-start off)")
+    ap.add_argument("--section-timers", action="store_true",
+                    help="sequence workload, with a library built with -DDG_PROFILE: add the frame "
+                         "kernel's section timers over the timed steps (cycles per subset) to the line")
     ap.add_argument("--shard", action="store_true",
                     help="sequence workload: split the subsets over the ranks (strong scaling) "
                          "instead of running replicas")
@@ -1071,6 +1074,14 @@ def main():
     fields_seen = []
     if args.profile_timed:
         torch.cuda.cudart().cudaProfilerStart()
+    timers = None
+    if args.section_timers:
+        import ctypes
+        if not hasattr(lib, "dicegpu_prof_read"):
+            raise SystemExit("--section-timers needs a library built with -DDG_PROFILE")
+        timers = (ctypes.c_ulonglong * 16)()
+        torch.cuda.synchronize()
+        abi.check(lib.dicegpu_prof_read(timers), "prof_read")   # clears the warm-up's
     for i in range(args.steps):
         flush_l2(l2_buf)
         ev[i][0].record(stream)
@@ -1079,6 +1090,8 @@ def main():
     torch.cuda.synchronize()
     if args.profile_timed:
         torch.cuda.cudart().cudaProfilerStop()
+    if timers is not None:
+        abi.check(lib.dicegpu_prof_read(timers), "prof_read")
     barrier(world)
     clocks.stop()
     launches = s.launch_count() - launches0
@@ -1260,6 +1273,13 @@ def main():
                 "accuracy": {"converged_frac": float(ok.mean()),
                              "status_counts": {str(int(k)): int(v) for k, v in zip(*np.unique(st, return_counts=True))},
                              "mean_iterations": float(np.mean(fl[ok, abi.F_ITERATIONS]))}}
+        if timers is not None:
+            # cycles of thread 0 of each subset's CTA, per subset of the timed steps
+            names = ["subset", "gauss_newton_passes", "first_attempt", "sigma", "final_gamma",
+                     "deformed_sum_beside_hessian_sweep", "q_sweep", "solve"]
+            per = float(n) * args.steps
+            line["section_timers"] = {"unit": "cycles per subset", "subsets": int(per),
+                                      **{nm: timers[i] / per for i, nm in enumerate(names)}}
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:
