@@ -298,6 +298,10 @@ struct dicegpu_ctx {
   int warps_per_cta = 4;   // warps of the CTA that solves one subset
   int ctas_per_sm = 0;   // 0: occupancy-derived
   bool shape_set = false;  // the caller (or the autotuner) chose the launch shape
+  // occupancy of the eight-warp shape, for the last kernel and shared memory asked
+  const void* wide_fn = nullptr;
+  size_t wide_smem = 0;
+  int wide_per_sm = 0;
   int queue_mode = 1;    // 1: per-CTA queues with stealing, 0: one global queue
   int carveout = -1;     // preferred shared-memory carveout (percent), -1: driver default
   int chunk = DG_QUEUE_CHUNK;   // queue chunk (consecutive subsets); 0: 2 per warp of a CTA
@@ -1759,9 +1763,16 @@ static void wide_launch(dicegpu_ctx* c, FrameKernelFn fn, long n, int* warps, in
   if (s > *smem &&
       cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s) != cudaSuccess)
     return;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, w * 32, s) != cudaSuccess || per_sm < 1)
-    return;
+  if (c->wide_fn != (const void*)fn || c->wide_smem != s) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, w * 32, s) != cudaSuccess)
+      per_sm = 0;
+    c->wide_fn = (const void*)fn;
+    c->wide_smem = s;
+    c->wide_per_sm = per_sm;
+  }
+  const int per_sm = c->wide_per_sm;
+  if (per_sm < 1) return;
   *warps = w;
   *blocks = std::min(std::min(per_sm * c->num_sms, kMaxQueues), *blocks);
   *smem = s;
