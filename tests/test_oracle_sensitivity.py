@@ -10,7 +10,7 @@ depends on rounding.  The oracle built with one legitimate rounding change,
 the mean of the deformed intensities summed in double
 (libdiceoracle_meanfp64.so), changes the iteration count of ~2 % of such
 subsets and the optimiser path of some; solves that converge in both agree
-to far inside 1e-4 px.  GPU-vs-oracle parity is judged the same way.
+to far inside 1e-4 px.  GPU-vs-oracle parity is assessed the same way.
 """
 import numpy as np
 
